@@ -1,0 +1,286 @@
+"""Benchmark: DOF-timesteps/s of the RK4 free-surface step (4 Laplace solves
+per step) on the 1025 x 257 x 17 irregular-sea workload, mixed precision
+(FP32 multigrid, FP64 FGMRES/RK4) against the all-FP64 GPU path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One process per GPU; every rank advances its own replica of the workload
+(the path does not shard: replicas only) and rank 0 prints one JSON line.
+The reference arm times the CPU restatement of the reference algorithm
+(lexicographic Gauss-Seidel multigrid, left-preconditioned GMRES) on the
+host cores, on a bounded sub-basin of the same workload.
+"""
+import argparse
+import importlib.util
+import json
+import os
+import pathlib
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+PKG_DIR = ROOT / "oceanwave3d-fortran90_b200"
+WORKLOAD = dict(Nx=1025, Ny=257, Nz=17)
+METRIC = "DOF-timesteps/s (mixed FP32-MG/FP64 vs FP64, eta err <= 1e-6)"
+UNIT = "DOF-timesteps/s"
+CPU_SAMPLE = dict(Nx=129, Ny=33, Nz=17)
+
+
+def package():
+    if "ow3d_b200" in sys.modules:
+        return sys.modules["ow3d_b200"]
+    spec = importlib.util.spec_from_file_location("ow3d_b200", PKG_DIR / "__init__.py",
+                                                  submodule_search_locations=[str(PKG_DIR)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["ow3d_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def peaks():
+    try:
+        d = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu=0):
+        self.gpu, self.rows, self.proc = gpu, [], None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) >= 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dof(p):
+    return p.Nx * p.Ny * p.Nz
+
+
+def run_gpu(args, rank, world):
+    import torch
+    pkg = package()
+    W = pkg.workloads
+    lib = pkg.lib()
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    res = {}
+    states = {}
+    for prec in ("fp64", "mixed"):
+        p, geo, E0, P0 = W.irregular_sea(**WORKLOAD, precision=(1 if prec == "mixed" else 0), seed=1234 + rank)
+        p.device = dev
+        sim = pkg.Simulation(p, **geo)
+        sim.set_state(E0, P0)
+        sim.step(args.warmup)
+        sim.reset_stats()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        with ClockSampler(dev) as clk:
+            st, ms = sim.step_timed(args.steps)
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+        s = sim.stats()
+        E, P, Wv, phi, tt = sim.get_state()
+        states[prec] = (E, phi)
+        res[prec] = dict(ms=ms, stats=s, clocks=clk.summary(), params=p, bytes=sim.device_bytes())
+        if prec == "mixed":
+            res["sim"] = sim
+        else:
+            sim.close()
+    # e2e through the public API with host buffers: per step, push E and P from
+    # pinned host memory, one RK4 step, read E, P, W back.
+    sim = res.pop("sim")
+    pm = res["mixed"]["params"]
+    C = sim.C
+    hostE = torch.empty(C, dtype=torch.float64).pin_memory().numpy()
+    hostP = torch.empty(C, dtype=torch.float64).pin_memory().numpy()
+    outW = torch.empty(C, dtype=torch.float64).pin_memory().numpy()
+    E, P, Wv, phi, tt = sim.get_state()
+    hostE[:] = E; hostP[:] = P
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sim.put_surface(hostE, hostP)
+        sim.step(1)
+        lib.ow3d_get_state(sim.h, pkg._d(hostE), pkg._d(hostP), pkg._d(outW), None, None)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    e2e_s = float(t.item())
+    sim.close()
+    # eta / phi error of the mixed path against the FP64 path after the same steps
+    Ef, phif = states["fp64"]; Em, phim = states["mixed"]
+    err_eta = float(np.max(np.abs(Em - Ef)) / np.max(np.abs(Ef)))
+    err_phi = float(np.max(np.abs(phim - phif)) / np.max(np.abs(phif)))
+    return res, e2e_s, err_eta, err_phi, pm
+
+
+def kernel_roofline(pkg, p, dev):
+    """Dominant kernel (high-order operator) timed alone with CUDA events."""
+    lib = pkg.lib()
+    import ctypes as C
+    p2 = pkg.default_params(Nx=p.Nx, Ny=p.Ny, Nz=p.Nz, Lx=p.Lx, Ly=p.Ly, Lz=p.Lz, GridZ=1, device=dev)
+    Nxg, Nyg, Nzg = pkg.dims(p2)
+    sim = pkg.Simulation(p2, np.ones(Nxg * Nyg))
+    ms = C.c_double()
+    reps = 50
+    r = lib.ow3d_bench_kernel(sim.h, 0, reps, C.byref(ms))
+    sim.close()
+    if r != 0:
+        return None
+    N, Cc = Nxg * Nyg * Nzg, Nxg * Nyg
+    alg = 2 * 8 * N + 10 * 8 * Cc
+    return ms.value / reps, alg
+
+
+def cpu_baseline(threads, steps=1):
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    pkg = package()
+    W = pkg.workloads
+    O.set_threads(threads)
+    p, geo, E0, P0 = W.irregular_sea(**CPU_SAMPLE, precision=0, seed=1234)
+    orc = O.Oracle(p, **geo, mode=O.MODE_REFERENCE)
+    orc.set_state(E0, P0)
+    t0 = time.perf_counter()
+    orc.step(steps)
+    dt = time.perf_counter() - t0
+    return dof(p) * steps / dt, dt, p
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        nthreads = os.cpu_count() or 1
+        vals = []
+        for _ in range(args.warmup):
+            pass
+        for _ in range(max(args.steps, 1)):
+            v, dt, p = cpu_baseline(nthreads, 1)
+            vals.append(v)
+        v = float(np.median(vals))
+        sample = f"{p.Nx}x{p.Ny}x{p.Nz} sub-basin of the irregular-sea workload (same dx, Nz, spectrum), 1 RK4 step per sample"
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "config": {"workload": "irregular sea 1025x257x17 (sampled on host)", "sample": sample},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "dtype": "f64", "data": "synthetic (seeded JONSWAP sea)"}))
+        return
+    if world > 1:
+        import torch
+        torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    res, e2e_s, err_eta, err_phi, pm = run_gpu(args, rank, world)
+    if rank != 0:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+        return
+    pkg = package()
+    D = dof(pm)
+    ms_mixed, ms_fp64 = res["mixed"]["ms"], res["fp64"]["ms"]
+    v_mixed = D * args.steps * world / (ms_mixed / 1e3)
+    v_fp64 = D * args.steps * world / (ms_fp64 / 1e3)
+    peak, peak_kind = peaks()
+    roof = None
+    kr = kernel_roofline(pkg, pm, int(os.environ.get("LOCAL_RANK", "0")))
+    if kr:
+        kms, alg = kr
+        ach = alg / (kms / 1e3) / 1e9
+        roof = {"bound": "hbm", "kernel": "k_ho_matvec (6th-order sigma operator, FP64)", "achieved": ach,
+                "peak": peak, "unit": "GB/s", "frac": ach / peak, "traffic": None,
+                "peak_kind": peak_kind, "alg_bytes_per_launch": alg, "ms_per_launch": kms}
+    cpu = None
+    if not args.no_cpu:
+        nthreads = os.cpu_count() or 1
+        v, dt, p = cpu_baseline(nthreads, 1)
+        cpu = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port",
+               "sample": f"{p.Nx}x{p.Ny}x{p.Nz} sub-basin of the same workload, 1 RK4 step ({dt:.1f} s)"}
+    C = (pm.Nx + 2) * (pm.Ny + 2)
+    sm = res["mixed"]["stats"]; sf = res["fp64"]["stats"]
+    out = {
+        "metric": METRIC, "value": v_mixed, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_mixed / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 (FP32 multigrid)", "data": "synthetic (seeded JONSWAP sea)",
+        "config": {"workload": "irregular sea 1025x257x17, flat 1 m, JONSWAP Hs=0.05 Tp=1.5 gamma=3.3, "
+                               "GMRES rtol 1e-8, Courant 0.5", "DOF": D, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (phi 38 MB + Krylov basis ~1.8 GB per replica)"},
+        "fp64": {"value": v_fp64, "ms_per_step": ms_fp64 / args.steps,
+                 "avg_iterations": sf["total_iterations"] / max(sf["solves"], 1)},
+        "mixed": {"value": v_mixed, "ms_per_step": ms_mixed / args.steps,
+                  "avg_iterations": sm["total_iterations"] / max(sm["solves"], 1),
+                  "eta_rel_err_vs_fp64": err_eta, "phi_rel_err_vs_fp64": err_phi},
+        "speedup_mixed_vs_fp64": v_mixed / v_fp64,
+        "laplace_solves_per_s": sm["solves"] * world / (ms_mixed / 1e3),
+        "e2e": {"value": D * args.steps * world / e2e_s, "unit": UNIT,
+                "h2d_bytes_per_step": 2 * 8 * C, "d2h_bytes_per_step": 3 * 8 * C},
+        "roofline": roof, "cpu_baseline": cpu, "clocks": res["mixed"]["clocks"],
+        "gpu_launches": None,
+    }
+    print(json.dumps(out))
+    if world > 1:
+        import torch
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,268 @@
+/*
+ * ow3d.h -- C ABI of the B200-native OceanWave3D hot path.
+ *
+ * The library replaces two call sites of the reference Fortran program:
+ *
+ *   (1) the per-stage Laplace solve
+ *         CALL iterative_solution(RHS, n_rows, BuildLinearSystem, PHI, FineGrid)
+ *       (src/wrappers/iterative_solution.f90:1-136, called from
+ *        src/timeintegration/Runge_Kutta_4.f90:129,216,309,419)
+ *       -> ow3d_solve / ow3d_solve_device
+ *
+ *   (2) the whole RK4 free-surface time step
+ *         CALL timeintegration_fsbc   (src/timeintegration/timeintegration_fsbc.f90:1-45)
+ *       -> ow3d_step
+ *
+ * The set-up half of the reference (OceanWave3DT0Setup, src/main/OceanWave3DT0Setup.f90)
+ * maps to ow3d_read_deck + ow3d_create.
+ *
+ * Conventions shared with the reference:
+ *   - All arrays are caller-owned, column-major Fortran arrays with ghost points
+ *     included:  3-D fields are PHI(k,i,j), k (sigma) fastest, size
+ *     Nzg*Nxg*Nyg with Nzg = Nz+GhostGridZ, Nxg = Nx+2*GhostGridX,
+ *     Nyg = Ny+2*GhostGridY (src/initialization/InitializeVariables.f90:24);
+ *     2-D free-surface fields are E(i,j), size Nxg*Nyg.
+ *   - Pointers are only read or written during the call; nothing is retained.
+ *   - Every function returns an int status: 0 = OK, > 0 = warning, < 0 = error.
+ *     No function calls exit() or aborts the process.
+ *   - One handle per host thread; calls on one handle are not thread-safe.
+ */
+#ifndef OW3D_H
+#define OW3D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define OW3D_OK                 0
+#define OW3D_NOT_CONVERGED      1   /* GMRES hit its matvec limit; solution kept
+                                       (the reference accepts this silently,
+                                       iterative_solution.f90:117-134)          */
+#define OW3D_ERR_BAD_INPUT     -1
+#define OW3D_ERR_CUDA          -2
+#define OW3D_ERR_OOM           -3   /* device allocation failed / admission denied */
+#define OW3D_ERR_UNSTABLE      -4   /* max|eta| > 10 max h (OceanWave3DTakeATimeStep.f90:54) */
+#define OW3D_ERR_TIMEOUT       -5
+#define OW3D_ERR_NO_DEVICE     -6
+#define OW3D_ERR_IO            -7
+#define OW3D_ERR_UNSUPPORTED   -8
+
+/* ------------------------------------------------------- build-only knobs */
+#define OW3D_PREC_FP64          0   /* everything FP64 ("plain" form)                 */
+#define OW3D_PREC_MIXED         1   /* MG hierarchy + smoother FP32, Krylov/RK4 FP64  */
+
+#define OW3D_KRYLOV_FGMRES      0   /* right-preconditioned flexible GMRES (default)   */
+#define OW3D_KRYLOV_LGMRES      1   /* left-preconditioned GMRES, stopping test on the
+                                       preconditioned residual (SPARSKIT2 semantics
+                                       used by iterative_solution.f90:23-24)            */
+
+#define OW3D_MAX_ZONES          8
+
+/* One relaxation zone: deck line 13 continuation
+ * "x1 x2 y1 y2 ftype param XorY WavegenONOFF XorYgen degrees"
+ * (src/IO/ReadInputFileParameters.f90:505-517,
+ *  src/initialization/PreprocessRelaxationZones.f90). */
+typedef struct ow3d_zone {
+    double x1, x2, y1, y2;
+    int    ftype;        /* +/-9 (sponge 1->0), +/-10 (3rd-order 0->1), 11..14  */
+    double param;
+    char   XorY;         /* 'X' or 'Y' */
+    int    WavegenONOFF; /* 0: absorption (sponge), 1: generation              */
+    char   XorYgen;
+    double degrees;
+    int    PhiOnOff;     /* sponge relaxes phi too when 1 (default 1)          */
+} ow3d_zone;
+
+/* Parameters of the positional input deck (src/IO/ReadInputFileParameters.f90),
+ * restricted to the fields the hot path reads, plus build-only knobs. */
+typedef struct ow3d_params {
+    /* line 2 */
+    int    IC, IncWaveType;
+    /* line 3 */
+    double Lx, Ly, Lz;
+    int    Nx, Ny, Nz;
+    int    GridX, GridY, GridZ;
+    int    GhostGridX, GhostGridY, GhostGridZ;
+    /* line 4 */
+    int    alpha, beta, gamma;
+    int    alphaprecond, betaprecond, gammaprecond;
+    /* line 5 */
+    int    Nsteps;
+    double dt;
+    int    timemethod;
+    double CFL;
+    int    extrapolationONOFF;
+    double time0;
+    /* line 6 */
+    double g;
+    /* line 7 */
+    int    solver;                /* 1 = GMRES (0 = defect correction: unsupported) */
+    int    Precond;               /* 3 = multigrid, 0 = none                         */
+    int    MGCoarseningStrategy;  /* 0 (default), 1, 2                               */
+    int    GMRESmaxiterations;
+    double reltol, abstol;
+    int    maxit;                 /* V-cycles per preconditioner application         */
+    char   cyclet;                /* 'V' (W/F: unsupported)                          */
+    int    nu1, nu2;
+    int    MGmaxgrids;
+    /* line 10 */
+    int    LinearONOFF;           /* 1 = nonlinear, 0 = linear (reference naming)    */
+    int    PressureTermOnOff;     /* must be 0                                       */
+    /* line 11 */
+    int    filteringONOFF, filterALPHA, filterORDER;
+    double sigma_filt[3];
+    /* line 13 */
+    int    relaxONOFF;
+    double relaxTransientTime;
+    int    relaxNo;
+    char   relaxXorY;
+    double relaxDegrees;
+    ow3d_zone zones[OW3D_MAX_ZONES];
+    /* build-only knobs (not part of the deck; defaults from ow3d_default_params) */
+    int    precision;             /* OW3D_PREC_*   */
+    int    krylov;                /* OW3D_KRYLOV_* */
+    int    device;                /* CUDA device ordinal */
+} ow3d_params;
+
+typedef struct ow3d_handle ow3d_handle;
+
+/* Solver statistics: the counters of OceanWave3DTakeATimeStep.f90:76-122 plus
+ * device timings. Iterations are counted as matvec requests, including the
+ * initial residual, exactly as iterative_solution.f90:58-60 counts them. */
+typedef struct ow3d_stats {
+    int64_t solves;
+    int64_t total_iterations;
+    int     min_iterations, max_iterations;
+    int     last_iterations;
+    int64_t not_converged;
+    double  last_residual;        /* final residual estimate of the last solve */
+    double  time;                 /* simulation time                           */
+    int64_t tstep;                /* number of completed time steps            */
+} ow3d_stats;
+
+/* ------------------------------------------------------------- set-up */
+
+/* Fill *p with the defaults the reference uses when a deck omits optional
+ * fields, plus precision = FP64, krylov = FGMRES, device = 0. */
+int ow3d_default_params(ow3d_params* p);
+
+/* Parse a positional OceanWave3D input deck (ReadInputFileParameters.f90:18-747)
+ * into *p. Fields beyond line 13 that the hot path does not use are skipped.
+ * Replaces: ReadInputFileParameters (src/IO/ReadInputFileParameters.f90:1). */
+int ow3d_read_deck(const char* path, ow3d_params* p);
+
+/* Create a simulation on the device: grid, stencils, sigma levels, multigrid
+ * hierarchy and workspaces. h..hyy are the bathymetry and its derivatives,
+ * Nxg*Nyg each, ghosts included (SetupInitialConditions.f90:51-111).
+ * Replaces: the device-relevant part of OceanWave3DT0Setup
+ * (OceanWave3DT0Setup.f90:35-444: SetupCompDomain, PreProcessDiffStencils,
+ *  ConstructTableCrossDerivatives, MGPreProcess, FilterInit,
+ *  PreprocessRelaxationZones). */
+int ow3d_create(const ow3d_params* p,
+                const double* h, const double* hx, const double* hxx,
+                const double* hy, const double* hyy,
+                ow3d_handle** out);
+
+int ow3d_destroy(ow3d_handle* h);
+
+/* Grid dimensions including ghosts and the device bytes the handle holds. */
+int ow3d_dims(const ow3d_handle* h, int* Nxg, int* Nyg, int* Nzg, size_t* device_bytes);
+
+/* Estimated device bytes a handle with parameters *p would allocate
+ * (used by the serving loop's admission gate). */
+int ow3d_estimate_bytes(const ow3d_params* p, size_t* bytes);
+
+/* ------------------------------------------------- the Laplace solve */
+
+/* One Laplace solve A(eta) phi = rhs with the 6th-order sigma-transformed
+ * operator, preconditioned by the low-order multigrid V-cycle.
+ *   rhs       : Nzg*Nxg*Nyg, host, read
+ *   phi_inout : Nzg*Nxg*Nyg, host, initial guess in, solution out
+ *   E,Ex,Exx,Ey,Eyy : the free-surface elevation and its horizontal
+ *               derivatives (Nxg*Nyg each, host) that define the sigma
+ *               coefficients (DetermineTransformationConstantsArray.f90);
+ *               Ey/Eyy may be NULL in 2-D.
+ *   iterations: out, matvec count as iterative_solution.f90:58-60 counts it.
+ * Replaces: iterative_solution(rhss, n_rows, BuildLinearSystem, sol, FineGrid)
+ *   (src/wrappers/iterative_solution.f90:1, matvec callback
+ *    src/functions/BuildLinearSystem.f90:1). */
+int ow3d_solve(ow3d_handle* h, const double* rhs, double* phi_inout,
+               const double* E, const double* Ex, const double* Exx,
+               const double* Ey, const double* Eyy, int* iterations);
+
+/* Same, with all pointers in device memory of the handle's device. Runs on the
+ * handle's stream; returns after the solve completed. */
+int ow3d_solve_device(ow3d_handle* h, const double* d_rhs, double* d_phi_inout,
+                      const double* d_E, const double* d_Ex, const double* d_Exx,
+                      const double* d_Ey, const double* d_Eyy, int* iterations);
+
+/* y = A phi with the high-order operator (BuildLinearSystem.f90:1-290) for the
+ * surface state (E..Eyy). Host pointers. Probe/unit-test entry point. */
+int ow3d_matvec(ow3d_handle* h, const double* phi, double* y,
+                const double* E, const double* Ex, const double* Exx,
+                const double* Ey, const double* Eyy);
+
+/* u = M^{-1} r: maxit V-cycles of the low-order multigrid preconditioner from
+ * u = 0 (MultiGridSolveLinearSystem.f90:1-95). Host pointers. */
+int ow3d_precondition(ow3d_handle* h, const double* r, double* u);
+
+/* ------------------------------------------------- the time step */
+
+/* Set the free-surface state: E, P (surface potential) and W (vertical surface
+ * velocity), Nxg*Nyg each, and the 3-D potential phi (may be NULL: zero), at
+ * simulation time t. Mirrors the state OceanWave3DT0Setup leaves behind. */
+int ow3d_set_state(ow3d_handle* h, const double* E, const double* P,
+                   const double* W, const double* phi, double t);
+
+/* Overwrite the surface elevation E and surface potential P (Nxg*Nyg, host)
+ * between time steps without touching phi, W or the extrapolation history,
+ * e.g. when a coupled host modifies the surface (the reference's global
+ * Wavefield%E, Wavefield%P). Recomputes the surface derivatives. */
+int ow3d_put_surface(ow3d_handle* h, const double* E, const double* P);
+
+/* Read back E, P, W (Nxg*Nyg) and phi (Nzg*Nxg*Nyg); any pointer may be NULL. */
+int ow3d_get_state(ow3d_handle* h, double* E, double* P, double* W,
+                   double* phi, double* t);
+
+/* Relaxation-zone target signal for generation zone `zone` (0-based):
+ * nt samples of eta and surface phi on the zone rectangle (i fastest, then j,
+ * ghost-inclusive index box of the zone), sampled every dt_sample from t=0.
+ * mode 0: dt_sample = dt and mid-stage targets are the average of the two
+ *         neighbouring samples (AnalyticWaveMaker2D.f90:26-33, IncWaveType 2);
+ * mode 1: dt_sample = dt/2, every RK stage time is a sample (IncWaveType 1). */
+int ow3d_set_relax_target(ow3d_handle* h, int zone, int mode, int nt,
+                          double dt_sample, const double* eta, const double* phis);
+
+/* Advance nsteps RK4 steps (Runge_Kutta_4.f90:1-429 with rhsFreeSurface3D or
+ * rhsLinearFreeSurface3D, relaxation, SG filtering), device resident.
+ * Replaces: timeintegration_fsbc (timeintegration_fsbc.f90:1-45) called from
+ * OceanWave3DTakeATimeStep.f90:27. Returns OW3D_ERR_UNSTABLE on the
+ * reference's instability test; OW3D_NOT_CONVERGED if any solve hit the limit. */
+int ow3d_step(ow3d_handle* h, int nsteps);
+
+/* ow3d_step, plus the device time of the steps measured with CUDA events on
+ * the handle's stream (milliseconds). */
+int ow3d_step_timed(ow3d_handle* h, int nsteps, double* device_ms);
+
+int ow3d_get_stats(const ow3d_handle* h, ow3d_stats* s);
+int ow3d_reset_stats(ow3d_handle* h);
+
+/* Capture each RK stage as a CUDA graph (1) or launch kernels directly (0). */
+int ow3d_set_graphs(ow3d_handle* h, int on);
+
+/* Zone-box of relaxation zone `zone` in 1-based ghost-inclusive indices. */
+int ow3d_zone_box(const ow3d_handle* h, int zone, int* i0, int* i1, int* j0, int* j1);
+
+const char* ow3d_strerror(int status);
+/* Message of the last failing call on this host thread (empty if none). */
+const char* ow3d_last_error(void);
+const char* ow3d_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OW3D_H */

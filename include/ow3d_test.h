@@ -1,0 +1,37 @@
+/*
+ * ow3d_test.h -- probe entry points used by the parity tests. They expose the
+ * set-up tables and the individual multigrid components of a handle so that
+ * each can be compared with the CPU restatement of the reference; they have no
+ * counterpart in the reference program and are not part of the drop-in API.
+ */
+#ifndef OW3D_TEST_H
+#define OW3D_TEST_H
+#include "ow3d.h"
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+int ow3d_test_level_count(const ow3d_handle* h);
+int ow3d_test_level_dims(const ow3d_handle* h, int level, int* Nx, int* Ny, int* Nz, int* ncolor);
+/* High-order stencil tables [order-1][pos][7] for x (2*Nxg*7), y (2*Nyg*7), sigma (2*Nzg*7). */
+int ow3d_test_stencils(const ow3d_handle* h, double* SX, double* SY, double* SZ);
+int ow3d_test_level_z(const ow3d_handle* h, int level, double* z);
+int ow3d_test_zone_gamma(const ow3d_handle* h, int zone, double* gamma);
+int ow3d_test_filter_coeffs(const ow3d_handle* h, double* centre, double* boundary);
+/* Multigrid component on level `level` (0 = coarsest), in the handle's precision:
+ * op 0: out = A_l in1;  op 1: out = smoothed in1 with rhs in2 (nu steps);
+ * op 2: out = restriction of the fine residual in1 to level-1;
+ * op 3: out = prolongation of the level-1 vector in1 (added to zero);
+ * op 4: out = coarsest-level solve of in1 (level 0 only). */
+int ow3d_test_level_op(ow3d_handle* h, int level, int op, int nu, const double* in1, const double* in2, double* out);
+/* Time `reps` back-to-back launches of one kernel group with CUDA events on
+ * the handle's stream: which 0 = high-order operator, 1 = one preconditioner
+ * application (V-cycle). Returns the total milliseconds. */
+int ow3d_bench_kernel(ow3d_handle* h, int which, int reps, double* ms_total);
+/* sizeof the C structs: 0 ow3d_params, 1 ow3d_zone, 2 ow3d_stats. */
+int ow3d_test_sizeof(int which);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,216 @@
+"""B200-native OceanWave3D hot path: the per-stage sigma-grid Laplace solve and
+the RK4 free-surface update, as CUDA kernels for sm_100a behind the C ABI of
+include/ow3d.h.
+
+This module is the Python host side of that ABI (the reference's driver is
+Fortran; a Fortran host binds the same symbols through iso_c_binding, see
+INTEGRATION.md). It mirrors the reference's split into a set-up call
+(OceanWave3DT0Setup) and a time-step call (OceanWave3DTakeATimeStep) and
+exposes the drop-in Laplace solve (iterative_solution).
+
+Arrays follow the reference's Fortran layout, flattened column-major:
+3-D fields PHI(k,i,j) with k fastest, 2-D fields E(i,j) with i fastest, ghost
+points included. numpy arrays of shape (Nyg, Nxg, Nzg) / (Nyg, Nxg) in C order
+have exactly that memory layout.
+"""
+import ctypes as _C
+import pathlib as _pathlib
+
+import numpy as _np
+
+from . import capi
+from . import workloads  # noqa: F401
+from .capi import Params, Zone, Stats, default_params, dims, set_zone  # noqa: F401
+
+LIB_PATH = _pathlib.Path(__file__).resolve().parent / "libow3d.so"
+_lib = None
+
+
+class OW3DError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        msg = f"{what}: status {status}"
+        if _lib is not None:
+            msg += f" ({_lib.ow3d_strerror(status).decode()}; {_lib.ow3d_last_error().decode()})"
+        super().__init__(msg)
+
+
+def lib():
+    """The loaded CUDA library. There is no CPU fallback: a missing library is an error."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise OW3DError(-8, f"{LIB_PATH} is missing; build it with build.py (there is no CPU fallback)")
+        L = _C.CDLL(str(LIB_PATH))
+        capi.declare(L)
+        D = _C.POINTER(_C.c_double)
+        L.ow3d_test_level_count.argtypes = [_C.c_void_p]
+        L.ow3d_test_level_dims.argtypes = [_C.c_void_p, _C.c_int] + [_C.POINTER(_C.c_int)] * 4
+        L.ow3d_test_stencils.argtypes = [_C.c_void_p, D, D, D]
+        L.ow3d_test_level_z.argtypes = [_C.c_void_p, _C.c_int, D]
+        L.ow3d_test_zone_gamma.argtypes = [_C.c_void_p, _C.c_int, D]
+        L.ow3d_test_filter_coeffs.argtypes = [_C.c_void_p, D, D]
+        L.ow3d_test_level_op.argtypes = [_C.c_void_p, _C.c_int, _C.c_int, _C.c_int, D, D, D]
+        L.ow3d_test_sizeof.argtypes = [_C.c_int]
+        L.ow3d_bench_kernel.argtypes = [_C.c_void_p, _C.c_int, _C.c_int, D]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return None if a is None else a.ctypes.data_as(_C.POINTER(_C.c_double))
+
+
+def _f64(a):
+    return None if a is None else _np.ascontiguousarray(a, dtype=_np.float64)
+
+
+def _check(st, what):
+    if st < 0:
+        raise OW3DError(st, what)
+    return st
+
+
+def read_deck(path):
+    """Parse an OceanWave3D input deck (ReadInputFileParameters.f90) into Params."""
+    p = Params()
+    _check(lib().ow3d_read_deck(str(path).encode(), _C.byref(p)), "ow3d_read_deck")
+    return p
+
+
+class Simulation:
+    """One simulation resident on one GPU (an ow3d_handle)."""
+
+    def __init__(self, params, h, hx=None, hxx=None, hy=None, hyy=None):
+        self.params = params
+        L = lib()
+        self.Nxg, self.Nyg, self.Nzg = dims(params)
+        self.C = self.Nxg * self.Nyg
+        self.N = self.C * self.Nzg
+        z = _np.zeros(self.C)
+        self._geo = [_f64(h).ravel()] + [(_f64(a).ravel() if a is not None else z) for a in (hx, hxx, hy, hyy)]
+        for a in self._geo:
+            if a.size != self.C:
+                raise ValueError(f"bathymetry arrays must have Nxg*Nyg = {self.C} entries")
+        hnd = _C.c_void_p()
+        _check(L.ow3d_create(_C.byref(params), *[_d(a) for a in self._geo], _C.byref(hnd)), "ow3d_create")
+        self.h = hnd
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ow3d_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- sizes
+    def device_bytes(self):
+        n = _C.c_size_t()
+        lib().ow3d_dims(self.h, None, None, None, _C.byref(n))
+        return n.value
+
+    # ---- the drop-in solve (iterative_solution.f90)
+    def solve(self, rhs, phi0, E=None, Ex=None, Exx=None, Ey=None, Eyy=None):
+        """Returns (phi, iterations, status)."""
+        phi = _f64(phi0).ravel().copy()
+        rhs = _f64(rhs).ravel()
+        surf = [_f64(a).ravel() if a is not None else None for a in (E, Ex, Exx, Ey, Eyy)]
+        it = _C.c_int()
+        st = _check(lib().ow3d_solve(self.h, _d(rhs), _d(phi), *[_d(a) for a in surf], _C.byref(it)), "ow3d_solve")
+        return phi, it.value, st
+
+    def matvec(self, phi, E=None, Ex=None, Exx=None, Ey=None, Eyy=None):
+        phi = _f64(phi).ravel()
+        y = _np.zeros(self.N)
+        surf = [_f64(a).ravel() if a is not None else None for a in (E, Ex, Exx, Ey, Eyy)]
+        _check(lib().ow3d_matvec(self.h, _d(phi), _d(y), *[_d(a) for a in surf]), "ow3d_matvec")
+        return y
+
+    def precondition(self, r):
+        r = _f64(r).ravel()
+        u = _np.zeros(self.N)
+        _check(lib().ow3d_precondition(self.h, _d(r), _d(u)), "ow3d_precondition")
+        return u
+
+    # ---- the time step (timeintegration_fsbc / Runge_Kutta_4.f90)
+    def set_state(self, E, P, W=None, phi=None, t=0.0):
+        arrs = [_f64(E).ravel(), _f64(P).ravel(), None if W is None else _f64(W).ravel(),
+                None if phi is None else _f64(phi).ravel()]
+        _check(lib().ow3d_set_state(self.h, *[_d(a) for a in arrs], float(t)), "ow3d_set_state")
+
+    def get_state(self):
+        E = _np.zeros(self.C); P = _np.zeros(self.C); W = _np.zeros(self.C); phi = _np.zeros(self.N)
+        t = _C.c_double()
+        _check(lib().ow3d_get_state(self.h, _d(E), _d(P), _d(W), _d(phi), _C.byref(t)), "ow3d_get_state")
+        return E, P, W, phi, t.value
+
+    def step(self, n=1):
+        return _check(lib().ow3d_step(self.h, int(n)), "ow3d_step")
+
+    def step_timed(self, n=1):
+        """Advance n steps; returns (status, device milliseconds from CUDA events)."""
+        ms = _C.c_double()
+        st = _check(lib().ow3d_step_timed(self.h, int(n), _C.byref(ms)), "ow3d_step_timed")
+        return st, ms.value
+
+    def put_surface(self, E, P):
+        _check(lib().ow3d_put_surface(self.h, _d(_f64(E).ravel()), _d(_f64(P).ravel())), "ow3d_put_surface")
+
+    def set_relax_target(self, zone, mode, nt, dt_sample, eta, phis):
+        _check(lib().ow3d_set_relax_target(self.h, zone, mode, nt, float(dt_sample), _d(_f64(eta).ravel()),
+                                           _d(_f64(phis).ravel())), "ow3d_set_relax_target")
+
+    def zone_box(self, zone):
+        a, b, c, d = (_C.c_int() for _ in range(4))
+        _check(lib().ow3d_zone_box(self.h, zone, _C.byref(a), _C.byref(b), _C.byref(c), _C.byref(d)), "ow3d_zone_box")
+        return a.value, b.value, c.value, d.value
+
+    def stats(self):
+        s = Stats()
+        _check(lib().ow3d_get_stats(self.h, _C.byref(s)), "ow3d_get_stats")
+        return {f: getattr(s, f) for f, _ in Stats._fields_}
+
+    def reset_stats(self):
+        lib().ow3d_reset_stats(self.h)
+
+    # ---- probes (include/ow3d_test.h)
+    def level_count(self):
+        return lib().ow3d_test_level_count(self.h)
+
+    def level_dims(self, l):
+        a, b, c, d = (_C.c_int() for _ in range(4))
+        _check(lib().ow3d_test_level_dims(self.h, l, _C.byref(a), _C.byref(b), _C.byref(c), _C.byref(d)), "level_dims")
+        return a.value, b.value, c.value, d.value
+
+    def level_size(self, l):
+        nx, ny, nz, _ = self.level_dims(l)
+        gy = 1 if self.params.Ny > 1 else 0
+        return (nx + 2) * (ny + 2 * gy) * (nz + 1)
+
+    def level_op(self, l, op, in1, in2=None, nu=1):
+        n_out = {0: self.level_size(l), 1: self.level_size(l), 2: self.level_size(l - 1) if l > 0 else 0,
+                 3: self.level_size(l), 4: self.level_size(l)}[op]
+        out = _np.zeros(n_out)
+        a = _f64(in1).ravel(); b = None if in2 is None else _f64(in2).ravel()
+        _check(lib().ow3d_test_level_op(self.h, l, op, nu, _d(a), _d(b), _d(out)), "level_op")
+        return out
+
+    def stencils(self):
+        SX = _np.zeros((2, self.Nxg, 7)); SY = _np.zeros((2, self.Nyg, 7 if self.params.Ny > 1 else 1))
+        SZ = _np.zeros((2, self.Nzg, 7))
+        _check(lib().ow3d_test_stencils(self.h, _d(SX), _d(SY), _d(SZ)), "stencils")
+        return SX, SY, SZ
+
+
+def version():
+    return lib().ow3d_version().decode()

@@ -1,0 +1,913 @@
+// C ABI and drivers of the B200 OceanWave3D hot path (include/ow3d.h).
+//
+// One ow3d_handle owns one simulation on one device: grid and stencils, the
+// multigrid hierarchy, the Krylov workspace and the free-surface state, all
+// resident in device memory for the handle's lifetime. Host pointers passed
+// to the API are only read or written during the call.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "ow3d_fs.h"
+#include "ow3d_internal.h"
+#include "../../include/ow3d_test.h"
+#include "setup.h"
+
+using namespace ow3d;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+#define CK(call)                                                                           \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            g_last_error = std::string(#call) + ": " + cudaGetErrorString(e_);             \
+            return (e_ == cudaErrorMemoryAllocation) ? OW3D_ERR_OOM : OW3D_ERR_CUDA;       \
+        }                                                                                  \
+    } while (0)
+
+template <typename T>
+struct MgSet {
+    std::vector<LevelDev<T>> lev;
+    T* coarse_inv = nullptr;
+    T* fine_b = nullptr;    // right-hand side of the finest level
+    T* fine_x = nullptr;    // iterate of the finest level when not written in place
+};
+
+}  // namespace
+
+struct ow3d_handle {
+    ow3d_params p;
+    GridHost G;
+    std::vector<ZoneHost> zones_h;
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    size_t bytes = 0;
+    std::vector<void*> allocs;
+    bool mixed = false;
+    // geometry
+    double *SX = nullptr, *SY = nullptr, *SZ = nullptr, *zs = nullptr;
+    double *h = nullptr, *hx = nullptr, *hxx = nullptr, *hy = nullptr, *hyy = nullptr;
+    HoGrid hg;
+    FsArgs fa;
+    // multigrid
+    MgSet<double> mg64;
+    MgSet<float> mg32;
+    int nlev = 0;
+    // Krylov
+    int m = 0;
+    int64_t ldv = 0;
+    double* V = nullptr;      // (m+1) vectors, stride ldv
+    void* Z = nullptr;        // m vectors (FGMRES), element type of the preconditioner
+    double* w = nullptr;      // scratch vector
+    KrylovState* ks = nullptr;
+    KrylovState* ks_host = nullptr;   // pinned
+    DotScratch dsc;
+    // state
+    double *E, *P, *W, *Ex, *Exx, *Ey, *Eyy, *Px, *Py;
+    double *tE, *tP, *tW, *tEx, *tExx, *tEy, *tEyy, *tPx, *tPy;
+    double *kE[4], *kP[4], *ftmp;
+    double *PHI, *LP[2], *RHS;
+    double* zerosC = nullptr;
+    // host-API staging (allocated on first use)
+    double *s_rhs = nullptr, *s_phi = nullptr, *s_E[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    // relaxation and filtering
+    std::vector<RelaxZoneDev> zones;
+    double *fc = nullptr, *F2 = nullptr;
+    int* flag = nullptr;
+    int* flag_host = nullptr;
+    double hmax = 0;
+    // bookkeeping
+    double time = 0;
+    int64_t tstep = 0;
+    ow3d_stats stats{};
+    int graphs = 0;
+};
+
+namespace {
+
+template <typename T>
+int dalloc(ow3d_handle* H, T** p, size_t n) {
+    void* q = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc(&q, n * sizeof(T));
+    if (e != cudaSuccess) {
+        g_last_error = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+        return OW3D_ERR_OOM;
+    }
+    H->allocs.push_back(q);
+    H->bytes += n * sizeof(T);
+    *p = (T*)q;
+    return OW3D_OK;
+}
+
+template <typename T>
+int upload(ow3d_handle* H, T** p, const std::vector<double>& v) {
+    int r = dalloc(H, p, v.size());
+    if (r) return r;
+    std::vector<T> t(v.begin(), v.end());
+    CK(cudaMemcpy(*p, t.data(), t.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return OW3D_OK;
+}
+
+#define TRY(x) do { int r_ = (x); if (r_) return r_; } while (0)
+
+template <typename T>
+int build_levels(ow3d_handle* H, MgSet<T>& S, bool alloc_fine_x) {
+    const int L = (int)H->G.levels.size();
+    S.lev.resize(L);
+    for (int l = 0; l < L; ++l) {
+        const LevelHost& h = H->G.levels[l];
+        LevelDev<T>& d = S.lev[l];
+        d.Nx = h.Nx; d.Ny = h.Ny; d.Nz = h.Nz; d.Nxg = h.Nxg; d.Nyg = h.Nyg; d.Nzg = h.Nzg;
+        d.N = (int64_t)h.Nxg * h.Nyg * h.Nzg;
+        d.ncolor = h.ncolor; d.xc = h.xc; d.yc = h.yc; d.zc = h.zc;
+        T *sx, *sy, *sz, *zs, *hh, *hx, *hxx, *hy, *hyy;
+        TRY(upload(H, &sx, h.SX.w)); TRY(upload(H, &sy, h.SY.w.empty() ? std::vector<double>(1, 0.0) : h.SY.w));
+        TRY(upload(H, &sz, h.SZ.w)); TRY(upload(H, &zs, h.zs));
+        TRY(upload(H, &hh, h.h)); TRY(upload(H, &hx, h.hx)); TRY(upload(H, &hxx, h.hxx));
+        TRY(upload(H, &hy, h.hy)); TRY(upload(H, &hyy, h.hyy));
+        d.SX = sx; d.SY = sy; d.SZ = sz; d.zs = zs; d.h = hh; d.hx = hx; d.hxx = hxx; d.hy = hy; d.hyy = hyy;
+        double *x, *y, *z;
+        TRY(upload(H, &x, h.x)); TRY(upload(H, &y, h.y)); TRY(upload(H, &z, h.z));
+        d.x = x; d.y = y; d.z = z;
+        T* r;
+        TRY(dalloc(H, &r, d.N)); d.rv = r;
+        if (l < L - 1) {
+            T *xv, *bv;
+            TRY(dalloc(H, &xv, d.N)); TRY(dalloc(H, &bv, d.N));
+            d.xv = xv; d.bv = bv;
+        }
+    }
+    LevelDev<T>& F = S.lev[L - 1];
+    TRY(dalloc(H, &S.fine_b, F.N));
+    F.bv = S.fine_b;
+    if (alloc_fine_x) TRY(dalloc(H, &S.fine_x, F.N));
+    F.xv = S.fine_x;
+    return OW3D_OK;
+}
+
+// Dense inverse of the coarsest-level operator, probing the matrix-free
+// operator with unit vectors (FP64), Gauss-Jordan with partial pivoting.
+template <typename T>
+int coarse_inverse(ow3d_handle* H, MgSet<T>& S) {
+    // FP64 probe on a temporary FP64 copy of the coarsest level
+    MgSet<double> tmp;
+    ow3d_handle& h = *H;
+    const LevelHost& Lh = h.G.levels[0];
+    const int n = Lh.Nxg * Lh.Nyg * Lh.Nzg;
+    if (n > 4096) { g_last_error = "coarsest multigrid level too large for the dense solve (raise MGmaxgrids)"; return OW3D_ERR_UNSUPPORTED; }
+    std::vector<LevelHost> keep = h.G.levels;
+    h.G.levels.assign(1, Lh);
+    int r = build_levels<double>(H, tmp, false);
+    h.G.levels = keep;
+    if (r) return r;
+    LevelDev<double> L0 = tmp.lev[0];
+    double *X, *Y;
+    TRY(dalloc(H, &X, (size_t)n * n)); TRY(dalloc(H, &Y, (size_t)n * n));
+    std::vector<double> I((size_t)n * n, 0.0);
+    for (int c = 0; c < n; ++c) I[(size_t)c * n + c] = 1.0;
+    CK(cudaMemcpy(X, I.data(), I.size() * sizeof(double), cudaMemcpyHostToDevice));
+    for (int c = 0; c < n; ++c) launch_lo_matvec<double>(L0, X + (size_t)c * n, Y + (size_t)c * n, h.st);
+    CK(cudaStreamSynchronize(h.st));
+    std::vector<double> A((size_t)n * n), colmaj((size_t)n * n);
+    CK(cudaMemcpy(colmaj.data(), Y, colmaj.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int c = 0; c < n; ++c) for (int rr = 0; rr < n; ++rr) A[(size_t)rr * n + c] = colmaj[(size_t)c * n + rr];
+    std::vector<double> inv((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) inv[(size_t)i * n + i] = 1.0;
+    for (int k = 0; k < n; ++k) {
+        int pr = k;
+        for (int rr = k + 1; rr < n; ++rr) if (std::fabs(A[(size_t)rr * n + k]) > std::fabs(A[(size_t)pr * n + k])) pr = rr;
+        if (A[(size_t)pr * n + k] == 0.0) { g_last_error = "singular coarsest-level operator"; return OW3D_ERR_BAD_INPUT; }
+        if (pr != k)
+            for (int c = 0; c < n; ++c) { std::swap(A[(size_t)k * n + c], A[(size_t)pr * n + c]); std::swap(inv[(size_t)k * n + c], inv[(size_t)pr * n + c]); }
+        const double d = A[(size_t)k * n + k];
+        for (int c = 0; c < n; ++c) { A[(size_t)k * n + c] /= d; inv[(size_t)k * n + c] /= d; }
+        for (int rr = 0; rr < n; ++rr) {
+            if (rr == k) continue;
+            const double f = A[(size_t)rr * n + k];
+            if (f == 0.0) continue;
+            for (int c = 0; c < n; ++c) { A[(size_t)rr * n + c] -= f * A[(size_t)k * n + c]; inv[(size_t)rr * n + c] -= f * inv[(size_t)k * n + c]; }
+        }
+    }
+    TRY(upload(H, &S.coarse_inv, inv));
+    return OW3D_OK;
+}
+
+int alloc_state(ow3d_handle* H) {
+    const size_t C = (size_t)H->G.C, N = (size_t)H->G.N;
+    double** cs[] = {&H->E, &H->P, &H->W, &H->Ex, &H->Exx, &H->Ey, &H->Eyy, &H->Px, &H->Py,
+                     &H->tE, &H->tP, &H->tW, &H->tEx, &H->tExx, &H->tEy, &H->tEyy, &H->tPx, &H->tPy,
+                     &H->kE[0], &H->kE[1], &H->kE[2], &H->kE[3], &H->kP[0], &H->kP[1], &H->kP[2], &H->kP[3],
+                     &H->ftmp, &H->zerosC};
+    for (double** q : cs) { TRY(dalloc(H, q, C)); CK(cudaMemset(*q, 0, C * sizeof(double))); }
+    double** ns[] = {&H->PHI, &H->LP[0], &H->LP[1], &H->RHS};
+    for (double** q : ns) { TRY(dalloc(H, q, N)); CK(cudaMemset(*q, 0, N * sizeof(double))); }
+    return OW3D_OK;
+}
+
+Surface surface_of(const ow3d_handle* H, const double* E, const double* Ex, const double* Exx, const double* Ey,
+                   const double* Eyy) {
+    Surface s{E, Ex, Exx, Ey, Eyy};
+    return s;
+}
+
+template <typename T>
+void run_precond(ow3d_handle* H, MgSet<T>& S, const double* src, const double* dscale, T* out) {
+    LevelDev<T>* lev = S.lev.data();
+    const int L = (int)S.lev.size();
+    LevelDev<T>& F = lev[L - 1];
+    launch_scale_copy_dev<T>(src, dscale, S.fine_b, F.N, H->st);
+    F.xv = out;
+    launch_mg_vcycle<T>(lev, L, S.coarse_inv, H->p.nu1, H->p.nu2, H->p.maxit, H->st);
+}
+
+// Apply M^{-1} to src (times *dscale) into the FP64 vector dst.
+void precond_into(ow3d_handle* H, const double* src, const double* dscale, double* dst) {
+    if (H->nlev == 0) {  // no preconditioner
+        launch_scale_copy_dev<double>(src, dscale, dst, H->G.N, H->st);
+        return;
+    }
+    if (!H->mixed) run_precond<double>(H, H->mg64, src, dscale, dst);
+    else {
+        run_precond<float>(H, H->mg32, src, dscale, H->mg32.fine_x);
+        launch_convert(H->mg32.fine_x, dst, H->G.N, H->st);
+    }
+}
+
+int sync_ks(ow3d_handle* H) {
+    CK(cudaMemcpyAsync(H->ks_host, H->ks, sizeof(KrylovState), cudaMemcpyDeviceToHost, H->st));
+    CK(cudaStreamSynchronize(H->st));
+    return OW3D_OK;
+}
+
+int sync_ks_small(ow3d_handle* H) {
+    // the scalars after the Hessenberg/rotation arrays
+    const size_t off = offsetof(KrylovState, w0);
+    CK(cudaMemcpyAsync((char*)H->ks_host + off, (char*)H->ks + off, sizeof(KrylovState) - off,
+                       cudaMemcpyDeviceToHost, H->st));
+    CK(cudaStreamSynchronize(H->st));
+    return OW3D_OK;
+}
+
+// One Laplace solve on the device: phi <- A^{-1} rhs, initial guess in phi.
+int solve_device(ow3d_handle* H, const double* rhs, double* phi, const Surface& s, int* iters_out) {
+    const int64_t N = H->G.N;
+    const int m = H->m, maxmv = H->p.GMRESmaxiterations;
+    const bool left = (H->p.krylov == OW3D_KRYLOV_LGMRES);
+    launch_krylov_reset(H->ks, H->st);
+    int status = OW3D_OK;
+    for (int cycle = 0; cycle < 1000; ++cycle) {
+        // initial residual
+        if (!left) {
+            launch_ho_matvec<double>(H->hg, s, phi, nullptr, rhs, H->V, 1, H->st);
+        } else {
+            launch_ho_matvec<double>(H->hg, s, phi, nullptr, rhs, H->w, 1, H->st);
+            precond_into(H, H->w, nullptr, H->V);
+        }
+        launch_norm_init(H->V, N, H->dsc, H->ks, H->p.reltol, H->p.abstol, H->st);
+        TRY(sync_ks_small(H));
+        int j = 0;
+        while (!H->ks_host->done) {
+            double* Vj = H->V + (int64_t)j * H->ldv;
+            double* Vn = H->V + (int64_t)(j + 1) * H->ldv;
+            const double* sj = &H->ks->scale[j];
+            if (!left) {
+                if (H->nlev == 0) {
+                    launch_scale_copy_dev<double>(Vj, sj, (double*)H->Z + (int64_t)j * H->ldv, N, H->st);
+                    launch_ho_matvec<double>(H->hg, s, (double*)H->Z + (int64_t)j * H->ldv, nullptr, nullptr, Vn, 0, H->st);
+                } else if (!H->mixed) {
+                    double* Zj = (double*)H->Z + (int64_t)j * H->ldv;
+                    run_precond<double>(H, H->mg64, Vj, sj, Zj);
+                    launch_ho_matvec<double>(H->hg, s, Zj, nullptr, nullptr, Vn, 0, H->st);
+                } else {
+                    float* Zj = (float*)H->Z + (int64_t)j * H->ldv;
+                    run_precond<float>(H, H->mg32, Vj, sj, Zj);
+                    launch_ho_matvec<float>(H->hg, s, Zj, nullptr, nullptr, Vn, 0, H->st);
+                }
+            } else {
+                launch_ho_matvec<double>(H->hg, s, Vj, sj, nullptr, H->w, 0, H->st);
+                precond_into(H, H->w, nullptr, Vn);
+            }
+            launch_multidot(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 0, H->st);
+            launch_project(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 0, H->st);
+            launch_multidot(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 1, H->st);
+            launch_project(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 1, H->st);
+            launch_arnoldi_finish(H->ks, maxmv, m, H->st);
+            TRY(sync_ks_small(H));
+            ++j;
+        }
+        if (H->ks_host->k > 0) {
+            launch_backsolve(H->ks, H->st);
+            if (!left) {
+                if (!H->mixed) launch_solution_update<double>(phi, (const double*)H->Z, H->ldv, N, H->ks, 0, H->st);
+                else launch_solution_update<float>(phi, (const float*)H->Z, H->ldv, N, H->ks, 0, H->st);
+            } else {
+                launch_solution_update<double>(phi, H->V, H->ldv, N, H->ks, 1, H->st);
+            }
+        }
+        TRY(sync_ks_small(H));
+        if (H->ks_host->converged) break;
+        if (H->ks_host->iters >= maxmv) { status = OW3D_NOT_CONVERGED; break; }
+        // restart: the subspace filled before the matvec limit
+        launch_krylov_restart(H->ks, H->st);
+    }
+    const int it = H->ks_host->iters;
+    if (iters_out) *iters_out = it;
+    ow3d_stats& S = H->stats;
+    S.solves++;
+    S.total_iterations += it;
+    S.min_iterations = (S.solves == 1) ? it : std::min(S.min_iterations, it);
+    S.max_iterations = std::max(S.max_iterations, it);
+    S.last_iterations = it;
+    S.last_residual = H->ks_host->resid;
+    if (status == OW3D_NOT_CONVERGED) S.not_converged++;
+    CK(cudaGetLastError());
+    return status;
+}
+
+int check_dims(const ow3d_params* p) {
+    if (!p) return OW3D_ERR_BAD_INPUT;
+    if (p->solver != 1) { g_last_error = "only GMRES (solver = 1) is supported"; return OW3D_ERR_UNSUPPORTED; }
+    if (p->Precond != 3 && p->Precond != 0) { g_last_error = "Precond must be 3 (multigrid) or 0"; return OW3D_ERR_UNSUPPORTED; }
+    if (p->cyclet != 'V' && p->cyclet != 'v') { g_last_error = "only V cycles are supported"; return OW3D_ERR_UNSUPPORTED; }
+    if (p->GMRESmaxiterations < 2 || p->GMRESmaxiterations > kMaxKrylov) { g_last_error = "GMRESmaxiterations out of range"; return OW3D_ERR_BAD_INPUT; }
+    if (p->timemethod != 1) { g_last_error = "only RK4 (timemethod = 1) is supported"; return OW3D_ERR_UNSUPPORTED; }
+    if (p->PressureTermOnOff != 0) { g_last_error = "applied surface pressure is not supported"; return OW3D_ERR_UNSUPPORTED; }
+    return OW3D_OK;
+}
+
+int create_impl(const ow3d_params* p, const double* h, const double* hx, const double* hxx, const double* hy,
+                const double* hyy, ow3d_handle** out) {
+    TRY(check_dims(p));
+    std::unique_ptr<ow3d_handle> H(new ow3d_handle());
+    H->p = *p;
+    H->mixed = (p->precision == OW3D_PREC_MIXED);
+    std::string err;
+    int r = build_grid(*p, h, hx, hxx, hy, hyy, H->G, &err);
+    if (r) { g_last_error = err; return r; }
+    H->dev = p->device;
+    CK(cudaSetDevice(H->dev));
+    CK(cudaStreamCreateWithFlags(&H->st, cudaStreamNonBlocking));
+    GridHost& G = H->G;
+    TRY(upload(H.get(), &H->SX, G.SX.w));
+    TRY(upload(H.get(), &H->SY, G.SY.w.empty() ? std::vector<double>(1, 0.0) : G.SY.w));
+    TRY(upload(H.get(), &H->SZ, G.SZ.w));
+    TRY(upload(H.get(), &H->zs, G.zs));
+    TRY(upload(H.get(), &H->h, G.h)); TRY(upload(H.get(), &H->hx, G.hx)); TRY(upload(H.get(), &H->hxx, G.hxx));
+    TRY(upload(H.get(), &H->hy, G.hy)); TRY(upload(H.get(), &H->hyy, G.hyy));
+    HoGrid& hg = H->hg;
+    hg.Nxg = G.Nxg; hg.Nyg = G.Nyg; hg.Nzg = G.Nzg; hg.gx = G.gx; hg.gy = G.gy; hg.three = G.three;
+    hg.nonlinear = (p->LinearONOFF == 1); hg.SX = H->SX; hg.SY = H->SY; hg.SZ = H->SZ; hg.zs = H->zs;
+    hg.h = H->h; hg.hx = H->hx; hg.hxx = H->hxx; hg.hy = H->hy; hg.hyy = H->hyy;
+    FsArgs& fa = H->fa;
+    fa.Nxg = G.Nxg; fa.Nyg = G.Nyg; fa.Nzg = G.Nzg; fa.three = G.three; fa.nonlinear = hg.nonlinear; fa.g = p->g;
+    fa.SX = H->SX; fa.SY = H->SY; fa.SZ = H->SZ; fa.h = H->h;
+    H->hmax = *std::max_element(G.h.begin(), G.h.end());
+    // multigrid
+    H->nlev = (int)G.levels.size();
+    if (H->nlev > 0) {
+        if (!H->mixed) { TRY(build_levels<double>(H.get(), H->mg64, true)); TRY(coarse_inverse<double>(H.get(), H->mg64)); }
+        else { TRY(build_levels<float>(H.get(), H->mg32, true)); TRY(coarse_inverse<float>(H.get(), H->mg32)); }
+    }
+    // Krylov workspace
+    H->m = p->GMRESmaxiterations;
+    H->ldv = (G.N + 31) / 32 * 32;
+    TRY(dalloc(H.get(), &H->V, (size_t)(H->m + 1) * H->ldv));
+    if (p->krylov == OW3D_KRYLOV_FGMRES) {
+        if (H->mixed) { float* z; TRY(dalloc(H.get(), &z, (size_t)H->m * H->ldv)); H->Z = z; }
+        else { double* z; TRY(dalloc(H.get(), &z, (size_t)H->m * H->ldv)); H->Z = z; }
+    }
+    TRY(dalloc(H.get(), &H->w, (size_t)H->ldv));
+    TRY(dalloc(H.get(), &H->ks, 1));
+    CK(cudaMallocHost(&H->ks_host, sizeof(KrylovState)));
+    std::memset(H->ks_host, 0, sizeof(KrylovState));
+    H->dsc.nblocks = 148 * 4;
+    TRY(dalloc(H.get(), &H->dsc.partial, (size_t)(kMaxKrylov + 2) * H->dsc.nblocks));
+    TRY(dalloc(H.get(), &H->dsc.counter, 1));
+    CK(cudaMemset(H->dsc.counter, 0, sizeof(unsigned int)));
+    TRY(alloc_state(H.get()));
+    // relaxation zones and filter
+    H->zones_h = build_zones(*p, G);
+    for (const ZoneHost& z : H->zones_h) {
+        RelaxZoneDev d{};
+        d.i0 = z.i0; d.i1 = z.i1; d.j0 = z.j0; d.j1 = z.j1; d.xdir = z.xdir; d.wavegen = z.wavegen; d.phion = z.phion;
+        double* g;
+        TRY(upload(H.get(), &g, z.gam));
+        d.gam = g; d.tmode = 0; d.nt = 0; d.tdt = 1.0; d.eta = nullptr; d.phis = nullptr;
+        H->zones.push_back(d);
+    }
+    if (p->filteringONOFF > 0) {
+        std::vector<double> fc, F2;
+        filter_coeffs(*p, fc, F2);
+        TRY(upload(H.get(), &H->fc, fc)); TRY(upload(H.get(), &H->F2, F2));
+    }
+    TRY(dalloc(H.get(), &H->flag, 1));
+    CK(cudaMemset(H->flag, 0, sizeof(int)));
+    CK(cudaMallocHost(&H->flag_host, sizeof(int)));
+    H->time = p->time0;
+    H->stats.time = H->time;
+    CK(cudaStreamSynchronize(H->st));
+    CK(cudaGetLastError());
+    *out = H.release();
+    return OW3D_OK;
+}
+
+int ensure_staging(ow3d_handle* H) {
+    if (H->s_rhs) return OW3D_OK;
+    TRY(dalloc(H, &H->s_rhs, (size_t)H->G.N));
+    TRY(dalloc(H, &H->s_phi, (size_t)H->G.N));
+    for (int q = 0; q < 5; ++q) TRY(dalloc(H, &H->s_E[q], (size_t)H->G.C));
+    return OW3D_OK;
+}
+
+int stage_surface(ow3d_handle* H, const double* E, const double* Ex, const double* Exx, const double* Ey,
+                  const double* Eyy, Surface& s) {
+    const double* src[5] = {E, Ex, Exx, Ey, Eyy};
+    const double* dst[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    for (int q = 0; q < 5; ++q) {
+        if (!src[q]) continue;
+        CK(cudaMemcpyAsync(H->s_E[q], src[q], sizeof(double) * H->G.C, cudaMemcpyHostToDevice, H->st));
+        dst[q] = H->s_E[q];
+    }
+    s = Surface{dst[0], dst[1], dst[2], dst[3], dst[4]};
+    return OW3D_OK;
+}
+
+// ------------------------------------------------------------- RK4 step
+// Runge_Kutta_4.f90:1-429 with the stage sequence of the reference.
+int rk4_step(ow3d_handle* H) {
+    cudaStream_t st = H->st;
+    const double dt = H->p.dt, half = 0.5, time = H->time;
+    const int64_t N = H->G.N;
+    H->tstep++;
+    const int64_t tstep = H->tstep;
+    double* LPnew = H->LP[(tstep - 1) % 2];
+    double* LPlast = H->LP[tstep % 2];
+    CK(cudaMemcpyAsync(LPnew, H->PHI, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+    const FsArgs& fa = H->fa;
+    int status = OW3D_OK;
+    auto relax = [&](double* E, double* P, double RKtime) {
+        if (H->p.relaxONOFF == 1)
+            fs_relax(fa, H->zones.data(), (int)H->zones.size(), E, P, RKtime, time, H->p.relaxTransientTime, st);
+    };
+    auto derivs = [&](double* E, double* P, double* Ex, double* Exx, double* Px, double* Ey, double* Eyy, double* Py) {
+        fs_derivs(fa, E, P, Ex, Exx, Px, Ey, Eyy, Py, st);
+    };
+    auto solve = [&](const Surface& s) -> int {
+        int it = 0;
+        int r = solve_device(H, H->RHS, H->PHI, s, &it);
+        if (r < 0) return r;
+        if (r == OW3D_NOT_CONVERGED) status = OW3D_NOT_CONVERGED;
+        return OW3D_OK;
+    };
+    const bool nl = H->p.LinearONOFF == 1;
+    auto surf = [&](const double* E, const double* Ex, const double* Exx, const double* Ey, const double* Eyy) {
+        return nl ? Surface{E, Ex, Exx, Ey, Eyy} : Surface{nullptr, nullptr, nullptr, nullptr, nullptr};
+    };
+    // stage 1
+    fs_stage(fa, H->E, H->P, H->W, H->Ex, H->Px, H->Ey, H->Py, H->E, H->P, half * dt, H->kE[0], H->kP[0], H->tE, H->tP, st);
+    relax(H->tE, H->tP, time + half * dt);
+    derivs(H->tE, H->tP, H->tEx, H->tExx, H->tPx, H->tEy, H->tEyy, H->tPy);
+    fs_set_rhs(fa, H->tP, H->RHS, st);
+    if (H->p.extrapolationONOFF == 1) fs_extrap(H->PHI, LPnew, LPlast, N, 0, st);
+    TRY(solve(surf(H->tE, H->tEx, H->tExx, H->tEy, H->tEyy)));
+    fs_wvel(fa, H->PHI, H->tE, H->tW, st);
+    // stage 2
+    fs_stage(fa, H->tE, H->tP, H->tW, H->tEx, H->tPx, H->tEy, H->tPy, H->E, H->P, half * dt, H->kE[1], H->kP[1], H->tE, H->tP, st);
+    relax(H->tE, H->tP, time + half * dt);
+    derivs(H->tE, H->tP, H->tEx, H->tExx, H->tPx, H->tEy, H->tEyy, H->tPy);
+    fs_set_rhs(fa, H->tP, H->RHS, st);
+    TRY(solve(surf(H->tE, H->tEx, H->tExx, H->tEy, H->tEyy)));
+    fs_wvel(fa, H->PHI, H->tE, H->tW, st);
+    // stage 3
+    fs_stage(fa, H->tE, H->tP, H->tW, H->tEx, H->tPx, H->tEy, H->tPy, H->E, H->P, dt, H->kE[2], H->kP[2], H->tE, H->tP, st);
+    relax(H->tE, H->tP, time + dt);
+    derivs(H->tE, H->tP, H->tEx, H->tExx, H->tPx, H->tEy, H->tEyy, H->tPy);
+    fs_set_rhs(fa, H->tP, H->RHS, st);
+    if (H->p.extrapolationONOFF == 1 && tstep > 1) fs_extrap(H->PHI, LPnew, LPlast, N, 1, st);
+    TRY(solve(surf(H->tE, H->tEx, H->tExx, H->tEy, H->tEyy)));
+    fs_wvel(fa, H->PHI, H->tE, H->tW, st);
+    // stage 4 and the new time level
+    fs_stage(fa, H->tE, H->tP, H->tW, H->tEx, H->tPx, H->tEy, H->tPy, nullptr, nullptr, 0.0, H->kE[3], H->kP[3], nullptr, nullptr, st);
+    fs_rk_final(fa, H->E, H->P, H->kE, H->kP, dt, st);
+    if (H->p.filteringONOFF > 0 && (tstep % H->p.filteringONOFF) == 0) {
+        FilterDev f{H->p.filterALPHA, H->fc, H->F2};
+        fs_filter(fa, f, H->E, H->ftmp, st);
+        fs_filter(fa, f, H->P, H->ftmp, st);
+    }
+    relax(H->E, H->P, time + dt);
+    derivs(H->E, H->P, H->Ex, H->Exx, H->Px, H->Ey, H->Eyy, H->Py);
+    fs_set_rhs(fa, H->P, H->RHS, st);
+    TRY(solve(surf(H->E, H->Ex, H->Exx, H->Ey, H->Eyy)));
+    fs_wvel(fa, H->PHI, H->E, H->W, st);
+    // OceanWave3DTakeATimeStep.f90:54-70
+    fs_unstable(fa, H->E, 10.0 * H->hmax, H->flag, st);
+    CK(cudaMemcpyAsync(H->flag_host, H->flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (*H->flag_host) { g_last_error = "max|eta| > 10 max h: the solution went unstable"; return OW3D_ERR_UNSTABLE; }
+    H->time = time + dt;
+    H->stats.time = H->time;
+    H->stats.tstep = H->tstep;
+    CK(cudaGetLastError());
+    return status;
+}
+
+}  // namespace
+
+namespace {
+template <typename T>
+int level_op_t(ow3d_handle* H, MgSet<T>& S, int l, int op, int nu, const double* in1, const double* in2, double* out) {
+    const int L = (int)S.lev.size();
+    LevelDev<T> Lv = S.lev[l];
+    const size_t n = (size_t)Lv.N;
+    T *a, *b, *c;
+    // temporary device buffers for the probe (freed at the end of the call)
+    size_t nmax = n;
+    if (l > 0) nmax = std::max(nmax, (size_t)S.lev[l - 1].N);
+    CK(cudaMalloc(&a, nmax * sizeof(T))); CK(cudaMalloc(&b, nmax * sizeof(T))); CK(cudaMalloc(&c, nmax * sizeof(T)));
+    auto put = [&](T* d, const double* h, size_t k) -> int {
+        std::vector<T> t(h, h + k);
+        CK(cudaMemcpy(d, t.data(), k * sizeof(T), cudaMemcpyHostToDevice));
+        return OW3D_OK;
+    };
+    auto get = [&](double* h, const T* d, size_t k) -> int {
+        std::vector<T> t(k);
+        CK(cudaMemcpy(t.data(), d, k * sizeof(T), cudaMemcpyDeviceToHost));
+        for (size_t q = 0; q < k; ++q) h[q] = (double)t[q];
+        return OW3D_OK;
+    };
+    int r = OW3D_OK;
+    if (op == 0) {  // y = A_l x
+        r = put(a, in1, n);
+        if (!r) { launch_lo_matvec<T>(Lv, a, b, H->st); cudaStreamSynchronize(H->st); r = get(out, b, n); }
+    } else if (op == 1) {  // smoothing: x <- S(x, b), nu steps
+        r = put(a, in1, n); if (!r) r = put(b, in2, n);
+        if (!r) { Lv.xv = a; Lv.bv = b; launch_lo_smooth<T>(Lv, nu, H->st); cudaStreamSynchronize(H->st); r = get(out, a, n); }
+    } else if (op == 2 && l > 0) {  // restriction of a fine residual to level l-1
+        LevelDev<T> Cc = S.lev[l - 1];
+        r = put(a, in1, n);
+        if (!r) { Cc.xv = c; launch_restrict<T>(Lv, Cc, a, b, H->st); cudaStreamSynchronize(H->st); r = get(out, b, (size_t)Cc.N); }
+    } else if (op == 3 && l > 0) {  // prolongation of a level l-1 vector, added to zero
+        LevelDev<T> Cc = S.lev[l - 1];
+        r = put(a, in1, (size_t)Cc.N);
+        if (!r) {
+            cudaMemsetAsync(b, 0, n * sizeof(T), H->st);
+            launch_prolong_add<T>(Lv, Cc, a, b, H->st); cudaStreamSynchronize(H->st); r = get(out, b, n);
+        }
+    } else if (op == 4 && l == 0) {  // coarse solve
+        r = put(b, in1, n);
+        if (!r) { Lv.bv = b; Lv.xv = a; launch_coarse_solve<T>(Lv, S.coarse_inv, H->st); cudaStreamSynchronize(H->st); r = get(out, a, n); }
+    } else r = OW3D_ERR_BAD_INPUT;
+    cudaFree(a); cudaFree(b); cudaFree(c);
+    (void)L;
+    CK(cudaGetLastError());
+    return r;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+int ow3d_default_params(ow3d_params* p) { return default_params(p); }
+
+int ow3d_read_deck(const char* path, ow3d_params* p) {
+    if (!path || !p) return OW3D_ERR_BAD_INPUT;
+    std::string err;
+    int r = read_deck(path, p, &err);
+    if (r) g_last_error = err;
+    return r;
+}
+
+int ow3d_create(const ow3d_params* p, const double* h, const double* hx, const double* hxx, const double* hy,
+                const double* hyy, ow3d_handle** out) {
+    if (!out) return OW3D_ERR_BAD_INPUT;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) { g_last_error = "no CUDA device"; return OW3D_ERR_NO_DEVICE; }
+    return create_impl(p, h, hx, hxx, hy, hyy, out);
+}
+
+int ow3d_destroy(ow3d_handle* H) {
+    if (!H) return OW3D_OK;
+    cudaSetDevice(H->dev);
+    if (H->st) cudaStreamSynchronize(H->st);
+    for (void* q : H->allocs) cudaFree(q);
+    if (H->ks_host) cudaFreeHost(H->ks_host);
+    if (H->flag_host) cudaFreeHost(H->flag_host);
+    if (H->st) cudaStreamDestroy(H->st);
+    delete H;
+    return OW3D_OK;
+}
+
+int ow3d_dims(const ow3d_handle* H, int* Nxg, int* Nyg, int* Nzg, size_t* bytes) {
+    if (!H) return OW3D_ERR_BAD_INPUT;
+    if (Nxg) *Nxg = H->G.Nxg;
+    if (Nyg) *Nyg = H->G.Nyg;
+    if (Nzg) *Nzg = H->G.Nzg;
+    if (bytes) *bytes = H->bytes;
+    return OW3D_OK;
+}
+
+int ow3d_estimate_bytes(const ow3d_params* p, size_t* bytes) {
+    if (!p || !bytes) return OW3D_ERR_BAD_INPUT;
+    const int gx = p->Nx > 1 ? 1 : 0, gy = p->Ny > 1 ? 1 : 0;
+    const double C = (double)(p->Nx + 2 * gx) * (p->Ny + 2 * gy);
+    const double N = C * (p->Nz + 1);
+    const double s = (p->precision == OW3D_PREC_MIXED) ? 4.0 : 8.0;
+    const int m = p->GMRESmaxiterations;
+    double b = 8.0 * N * (m + 1) + s * N * m + 8.0 * N * 5 + 3.0 * s * N * 1.6 + 8.0 * C * 60;
+    *bytes = (size_t)(b * 1.05) + ((size_t)64 << 20);
+    return OW3D_OK;
+}
+
+int ow3d_solve_device(ow3d_handle* H, const double* rhs, double* phi, const double* E, const double* Ex,
+                      const double* Exx, const double* Ey, const double* Eyy, int* iterations) {
+    if (!H || !rhs || !phi) return OW3D_ERR_BAD_INPUT;
+    CK(cudaSetDevice(H->dev));
+    const bool nl = H->p.LinearONOFF == 1;
+    Surface s = nl ? Surface{E, Ex, Exx, Ey, Eyy} : Surface{nullptr, nullptr, nullptr, nullptr, nullptr};
+    return solve_device(H, rhs, phi, s, iterations);
+}
+
+int ow3d_solve(ow3d_handle* H, const double* rhs, double* phi, const double* E, const double* Ex, const double* Exx,
+               const double* Ey, const double* Eyy, int* iterations) {
+    if (!H || !rhs || !phi) return OW3D_ERR_BAD_INPUT;
+    CK(cudaSetDevice(H->dev));
+    TRY(ensure_staging(H));
+    const size_t nb = sizeof(double) * (size_t)H->G.N;
+    CK(cudaMemcpyAsync(H->s_rhs, rhs, nb, cudaMemcpyHostToDevice, H->st));
+    CK(cudaMemcpyAsync(H->s_phi, phi, nb, cudaMemcpyHostToDevice, H->st));
+    Surface s;
+    TRY(stage_surface(H, E, Ex, Exx, Ey, Eyy, s));
+    if (H->p.LinearONOFF != 1) s = Surface{nullptr, nullptr, nullptr, nullptr, nullptr};
+    int r = solve_device(H, H->s_rhs, H->s_phi, s, iterations);
+    if (r < 0) return r;
+    CK(cudaMemcpyAsync(phi, H->s_phi, nb, cudaMemcpyDeviceToHost, H->st));
+    CK(cudaStreamSynchronize(H->st));
+    return r;
+}
+
+int ow3d_matvec(ow3d_handle* H, const double* phi, double* y, const double* E, const double* Ex, const double* Exx,
+                const double* Ey, const double* Eyy) {
+    if (!H || !phi || !y) return OW3D_ERR_BAD_INPUT;
+    CK(cudaSetDevice(H->dev));
+    TRY(ensure_staging(H));
+    const size_t nb = sizeof(double) * (size_t)H->G.N;
+    CK(cudaMemcpyAsync(H->s_phi, phi, nb, cudaMemcpyHostToDevice, H->st));
+    Surface s;
+    TRY(stage_surface(H, E, Ex, Exx, Ey, Eyy, s));
+    if (H->p.LinearONOFF != 1) s = Surface{nullptr, nullptr, nullptr, nullptr, nullptr};
+    launch_ho_matvec<double>(H->hg, s, H->s_phi, nullptr, nullptr, H->s_rhs, 0, H->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(y, H->s_rhs, nb, cudaMemcpyDeviceToHost, H->st));
+    CK(cudaStreamSynchronize(H->st));
+    return OW3D_OK;
+}
+
+int ow3d_precondition(ow3d_handle* H, const double* r, double* u) {
+    if (!H || !r || !u) return OW3D_ERR_BAD_INPUT;
+    CK(cudaSetDevice(H->dev));
+    TRY(ensure_staging(H));
+    const size_t nb = sizeof(double) * (size_t)H->G.N;
+    CK(cudaMemcpyAsync(H->s_rhs, r, nb, cudaMemcpyHostToDevice, H->st));
+    precond_into(H, H->s_rhs, nullptr, H->s_phi);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(u, H->s_phi, nb, cudaMemcpyDeviceToHost, H->st));
+    CK(cudaStreamSynchronize(H->st));
+    return OW3D_OK;
+}
+
+int ow3d_set_state(ow3d_handle* H, const double* E, const double* P, const double* W, const double* phi, double t) {
+    if (!H) return OW3D_ERR_BAD_INPUT;
+    CK(cudaSetDevice(H->dev));
+    const size_t cb = sizeof(double) * (size_t)H->G.C, nb = sizeof(double) * (size_t)H->G.N;
+    if (E) CK(cudaMemcpyAsync(H->E, E, cb, cudaMemcpyHostToDevice, H->st)); else CK(cudaMemsetAsync(H->E, 0, cb, H->st));
+    if (P) CK(cudaMemcpyAsync(H->P, P, cb, cudaMemcpyHostToDevice, H->st)); else CK(cudaMemsetAsync(H->P, 0, cb, H->st));
+    if (W) CK(cudaMemcpyAsync(H->W, W, cb, cudaMemcpyHostToDevice, H->st)); else CK(cudaMemsetAsync(H->W, 0, cb, H->st));
+    if (phi) CK(cudaMemcpyAsync(H->PHI, phi, nb, cudaMemcpyHostToDevice, H->st)); else CK(cudaMemsetAsync(H->PHI, 0, nb, H->st));
+    CK(cudaMemsetAsync(H->LP[0], 0, nb, H->st));
+    CK(cudaMemsetAsync(H->LP[1], 0, nb, H->st));
+    CK(cudaMemsetAsync(H->RHS, 0, nb, H->st));
+    // OceanWave3DT0Setup.f90:444 -- surface derivatives of the initial state
+    fs_derivs(H->fa, H->E, H->P, H->Ex, H->Exx, H->Px, H->Ey, H->Eyy, H->Py, H->st);
+    H->time = t;
+    H->tstep = 0;
+    H->stats.time = t;
+    H->stats.tstep = 0;
+    CK(cudaStreamSynchronize(H->st));
+    return OW3D_OK;
+}
+
+int ow3d_put_surface(ow3d_handle* H, const double* E, const double* P) {
+    if (!H || !E || !P) return OW3D_ERR_BAD_INPUT;
+    CK(cudaSetDevice(H->dev));
+    const size_t cb = sizeof(double) * (size_t)H->G.C;
+    CK(cudaMemcpyAsync(H->E, E, cb, cudaMemcpyHostToDevice, H->st));
+    CK(cudaMemcpyAsync(H->P, P, cb, cudaMemcpyHostToDevice, H->st));
+    fs_derivs(H->fa, H->E, H->P, H->Ex, H->Exx, H->Px, H->Ey, H->Eyy, H->Py, H->st);
+    CK(cudaGetLastError());
+    return OW3D_OK;
+}
+
+int ow3d_get_state(ow3d_handle* H, double* E, double* P, double* W, double* phi, double* t) {
+    if (!H) return OW3D_ERR_BAD_INPUT;
+    CK(cudaSetDevice(H->dev));
+    const size_t cb = sizeof(double) * (size_t)H->G.C, nb = sizeof(double) * (size_t)H->G.N;
+    if (E) CK(cudaMemcpyAsync(E, H->E, cb, cudaMemcpyDeviceToHost, H->st));
+    if (P) CK(cudaMemcpyAsync(P, H->P, cb, cudaMemcpyDeviceToHost, H->st));
+    if (W) CK(cudaMemcpyAsync(W, H->W, cb, cudaMemcpyDeviceToHost, H->st));
+    if (phi) CK(cudaMemcpyAsync(phi, H->PHI, nb, cudaMemcpyDeviceToHost, H->st));
+    CK(cudaStreamSynchronize(H->st));
+    if (t) *t = H->time;
+    return OW3D_OK;
+}
+
+int ow3d_set_relax_target(ow3d_handle* H, int zone, int mode, int nt, double dts, const double* eta, const double* phis) {
+    if (!H || zone < 0 || zone >= (int)H->zones.size() || nt <= 0 || !eta || !phis || dts <= 0) return OW3D_ERR_BAD_INPUT;
+    CK(cudaSetDevice(H->dev));
+    RelaxZoneDev& z = H->zones[zone];
+    const size_t box = (size_t)(z.i1 - z.i0 + 1) * (z.j1 - z.j0 + 1);
+    double *de, *dp;
+    TRY(dalloc(H, &de, box * nt)); TRY(dalloc(H, &dp, box * nt));
+    CK(cudaMemcpy(de, eta, box * nt * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dp, phis, box * nt * sizeof(double), cudaMemcpyHostToDevice));
+    z.eta = de; z.phis = dp; z.nt = nt; z.tdt = dts; z.tmode = mode;
+    return OW3D_OK;
+}
+
+int ow3d_zone_box(const ow3d_handle* H, int zone, int* i0, int* i1, int* j0, int* j1) {
+    if (!H || zone < 0 || zone >= (int)H->zones.size()) return OW3D_ERR_BAD_INPUT;
+    const RelaxZoneDev& z = H->zones[zone];
+    *i0 = z.i0; *i1 = z.i1; *j0 = z.j0; *j1 = z.j1;
+    return OW3D_OK;
+}
+
+int ow3d_step(ow3d_handle* H, int nsteps) {
+    if (!H || nsteps < 0) return OW3D_ERR_BAD_INPUT;
+    CK(cudaSetDevice(H->dev));
+    int st = OW3D_OK;
+    for (int i = 0; i < nsteps; ++i) {
+        int r = rk4_step(H);
+        if (r < 0) return r;
+        if (r > 0) st = r;
+    }
+    return st;
+}
+
+int ow3d_step_timed(ow3d_handle* H, int nsteps, double* device_ms) {
+    if (!H || nsteps < 0) return OW3D_ERR_BAD_INPUT;
+    CK(cudaSetDevice(H->dev));
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a)); CK(cudaEventCreate(&b));
+    CK(cudaEventRecord(a, H->st));
+    int st = OW3D_OK;
+    for (int i = 0; i < nsteps; ++i) {
+        int r = rk4_step(H);
+        if (r < 0) { cudaEventDestroy(a); cudaEventDestroy(b); return r; }
+        if (r > 0) st = r;
+    }
+    CK(cudaEventRecord(b, H->st));
+    CK(cudaEventSynchronize(b));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a); cudaEventDestroy(b);
+    if (device_ms) *device_ms = ms;
+    return st;
+}
+
+int ow3d_get_stats(const ow3d_handle* H, ow3d_stats* s) {
+    if (!H || !s) return OW3D_ERR_BAD_INPUT;
+    *s = H->stats;
+    return OW3D_OK;
+}
+
+int ow3d_reset_stats(ow3d_handle* H) {
+    if (!H) return OW3D_ERR_BAD_INPUT;
+    const double t = H->stats.time;
+    const int64_t ts = H->stats.tstep;
+    std::memset(&H->stats, 0, sizeof(H->stats));
+    H->stats.time = t;
+    H->stats.tstep = ts;
+    return OW3D_OK;
+}
+
+int ow3d_set_graphs(ow3d_handle* H, int on) {
+    if (!H) return OW3D_ERR_BAD_INPUT;
+    H->graphs = on;
+    return OW3D_OK;
+}
+
+const char* ow3d_strerror(int s) {
+    switch (s) {
+        case OW3D_OK: return "ok";
+        case OW3D_NOT_CONVERGED: return "GMRES reached its matvec limit before the tolerance (solution kept)";
+        case OW3D_ERR_BAD_INPUT: return "bad input";
+        case OW3D_ERR_CUDA: return "CUDA error";
+        case OW3D_ERR_OOM: return "out of device memory";
+        case OW3D_ERR_UNSTABLE: return "solution unstable (max|eta| > 10 max h)";
+        case OW3D_ERR_TIMEOUT: return "timeout";
+        case OW3D_ERR_NO_DEVICE: return "no CUDA device";
+        case OW3D_ERR_IO: return "I/O error";
+        case OW3D_ERR_UNSUPPORTED: return "unsupported configuration";
+        default: return "unknown status";
+    }
+}
+
+const char* ow3d_version(void) { return "ow3d-b200 0.1 (sm_100a)"; }
+
+const char* ow3d_last_error(void) { return g_last_error.c_str(); }
+
+// --------------------------------------------------------- test hooks
+int ow3d_test_level_count(const ow3d_handle* H) { return H ? H->nlev : -1; }
+
+int ow3d_test_level_dims(const ow3d_handle* H, int l, int* Nx, int* Ny, int* Nz, int* ncolor) {
+    if (!H || l < 0 || l >= H->nlev) return OW3D_ERR_BAD_INPUT;
+    const LevelHost& L = H->G.levels[l];
+    *Nx = L.Nx; *Ny = L.Ny; *Nz = L.Nz; *ncolor = L.ncolor;
+    return OW3D_OK;
+}
+
+int ow3d_test_stencils(const ow3d_handle* H, double* SX, double* SY, double* SZ) {
+    if (!H) return OW3D_ERR_BAD_INPUT;
+    if (SX) std::copy(H->G.SX.w.begin(), H->G.SX.w.end(), SX);
+    if (SY) std::copy(H->G.SY.w.begin(), H->G.SY.w.end(), SY);
+    if (SZ) std::copy(H->G.SZ.w.begin(), H->G.SZ.w.end(), SZ);
+    return OW3D_OK;
+}
+
+int ow3d_test_level_z(const ow3d_handle* H, int l, double* z) {
+    if (!H || l < 0 || l >= H->nlev) return OW3D_ERR_BAD_INPUT;
+    std::copy(H->G.levels[l].z.begin(), H->G.levels[l].z.end(), z);
+    return OW3D_OK;
+}
+
+int ow3d_test_zone_gamma(const ow3d_handle* H, int zone, double* g) {
+    if (!H || zone < 0 || zone >= (int)H->zones_h.size()) return OW3D_ERR_BAD_INPUT;
+    std::copy(H->zones_h[zone].gam.begin(), H->zones_h[zone].gam.end(), g);
+    return OW3D_OK;
+}
+
+int ow3d_test_filter_coeffs(const ow3d_handle* H, double* fc, double* F2) {
+    if (!H) return OW3D_ERR_BAD_INPUT;
+    std::vector<double> a, b;
+    filter_coeffs(H->p, a, b);
+    std::copy(a.begin(), a.end(), fc);
+    std::copy(b.begin(), b.end(), F2);
+    return OW3D_OK;
+}
+
+int ow3d_test_level_op(ow3d_handle* H, int l, int op, int nu, const double* in1, const double* in2, double* out) {
+    if (!H || l < 0 || l >= H->nlev) return OW3D_ERR_BAD_INPUT;
+    CK(cudaSetDevice(H->dev));
+    if (!H->mixed) return level_op_t<double>(H, H->mg64, l, op, nu, in1, in2, out);
+    return level_op_t<float>(H, H->mg32, l, op, nu, in1, in2, out);
+}
+
+int ow3d_bench_kernel(ow3d_handle* H, int which, int reps, double* ms_total) {
+    if (!H || reps < 1) return OW3D_ERR_BAD_INPUT;
+    CK(cudaSetDevice(H->dev));
+    TRY(ensure_staging(H));
+    const size_t nb = sizeof(double) * (size_t)H->G.N;
+    std::vector<double> host(H->G.N);
+    for (size_t q = 0; q < host.size(); ++q) host[q] = std::sin(0.001 * (double)q);
+    CK(cudaMemcpy(H->s_phi, host.data(), nb, cudaMemcpyHostToDevice));
+    Surface s{nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a)); CK(cudaEventCreate(&b));
+    auto once = [&]() {
+        if (which == 0) launch_ho_matvec<double>(H->hg, s, H->s_phi, nullptr, nullptr, H->s_rhs, 0, H->st);
+        else precond_into(H, H->s_phi, nullptr, H->s_rhs);
+    };
+    once();
+    CK(cudaEventRecord(a, H->st));
+    for (int r = 0; r < reps; ++r) once();
+    CK(cudaEventRecord(b, H->st));
+    CK(cudaEventSynchronize(b));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a); cudaEventDestroy(b);
+    *ms_total = ms;
+    CK(cudaGetLastError());
+    return OW3D_OK;
+}
+
+int ow3d_test_sizeof(int which) {
+    switch (which) {
+        case 0: return (int)sizeof(ow3d_params);
+        case 1: return (int)sizeof(ow3d_zone);
+        case 2: return (int)sizeof(ow3d_stats);
+        default: return -1;
+    }
+}
+
+}  // extern "C"

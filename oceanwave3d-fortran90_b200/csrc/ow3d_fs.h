@@ -1,0 +1,51 @@
+// Free-surface kernels' argument blocks and launchers (fs.cu).
+#pragma once
+#include "ow3d_internal.h"
+
+namespace ow3d {
+
+struct FsArgs {
+    int Nxg, Nyg, Nzg;
+    int three, nonlinear;
+    double g;
+    const double* SX;   // [2][Nxg][7]
+    const double* SY;   // [2][Nyg][7]
+    const double* SZ;   // [2][Nzg][7]
+    const double* h;
+};
+
+// One relaxation zone on the device (PreprocessRelaxationZones.f90).
+struct RelaxZoneDev {
+    int i0, i1, j0, j1;      // 1-based, ghost-inclusive box
+    int xdir;                // gamma varies along x (XorY == 'X') or y
+    int wavegen, phion;
+    const double* gam;       // gamma along the relaxation direction
+    int tmode, nt;           // target table (see ow3d_set_relax_target)
+    double tdt;
+    const double* eta;       // [nt][box]
+    const double* phis;
+};
+
+// Savitzky-Golay filter coefficients (FilterInit.f90) as FILTERING.f90 reads them.
+struct FilterDev {
+    int alpha;
+    const double* fc;        // 2*alpha+1 centred weights (offset -alpha..alpha)
+    const double* F2;        // (2*alpha+1) x alpha boundary weights, column-major
+};
+
+void fs_stage(const FsArgs& a, const double* E, const double* P, const double* W, const double* Ex, const double* Px,
+              const double* Ey, const double* Py, const double* E0, const double* P0, double c, double* kE,
+              double* kP, double* tE, double* tP, cudaStream_t st);
+void fs_rk_final(const FsArgs& a, double* E, double* P, double* const* kE, double* const* kP, double dt,
+                 cudaStream_t st);
+void fs_relax(const FsArgs& a, const RelaxZoneDev* zones, int nz, double* E, double* P, double RKtime, double time,
+              double transient, cudaStream_t st);
+void fs_derivs(const FsArgs& a, double* E, double* P, double* Ex, double* Exx, double* Px, double* Ey, double* Eyy,
+               double* Py, cudaStream_t st);
+void fs_wvel(const FsArgs& a, const double* phi, const double* E, double* W, cudaStream_t st);
+void fs_set_rhs(const FsArgs& a, const double* P, double* rhs, cudaStream_t st);
+void fs_extrap(double* phi, const double* lnew, const double* llast, int64_t n, int stage3, cudaStream_t st);
+void fs_filter(const FsArgs& a, const FilterDev& f, double* U, double* tmp, cudaStream_t st);
+void fs_unstable(const FsArgs& a, const double* E, double hmax10, int* flag, cudaStream_t st);
+
+}  // namespace ow3d

@@ -1,0 +1,504 @@
+// Host-side set-up: deck parsing, grid, finite-difference stencils, the
+// multigrid hierarchy metadata, relaxation zones and Savitzky-Golay filter
+// coefficients. Everything here runs once per simulation; the per-step work
+// is on the device.
+#include "setup.h"
+
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+
+namespace ow3d {
+
+// ------------------------------------------------------------- stencils
+// Finite-difference weights on arbitrary nodes by Fornberg's recurrence
+// (B. Fornberg, Math. Comp. 51 (1988) 699-706), the algorithm of the
+// reference's `weights` routine (src/utilities/stream_func_wave_finite.f:128-168).
+// Returns the weights of derivative `order` at z on nodes x[0..n].
+void fd_weights(double z, const double* x, int n, int order, double* w) {
+    const int M = order;
+    std::vector<double> c((size_t)(n + 1) * (M + 1), 0.0);
+    auto C = [&](int j, int k) -> double& { return c[(size_t)j * (M + 1) + k]; };
+    double c1 = 1.0, c4 = x[0] - z;
+    C(0, 0) = 1.0;
+    for (int i = 1; i <= n; ++i) {
+        const int mn = std::min(i, M);
+        double c2 = 1.0;
+        const double c5 = c4;
+        c4 = x[i] - z;
+        for (int j = 0; j < i; ++j) {
+            const double c3 = x[i] - x[j];
+            c2 *= c3;
+            if (j == i - 1) {
+                for (int k = mn; k >= 1; --k) C(i, k) = c1 * (k * C(i - 1, k - 1) - c5 * C(i - 1, k)) / c2;
+                C(i, 0) = -c1 * c5 * C(i - 1, 0) / c2;
+            }
+            for (int k = mn; k >= 1; --k) C(j, k) = (c4 * C(j, k) - k * C(j, k - 1)) / c3;
+            C(j, 0) = c4 * C(j, 0) / c3;
+        }
+        c1 = c2;
+    }
+    for (int j = 0; j <= n; ++j) w[j] = C(j, M);
+}
+
+// x / y stencils: window of 2a+1 nodes centred on the point, shifted inwards at
+// the first and last a points (BuildStencilsGridX.f90:162-196).
+Stencil stencils_xy(const std::vector<double>& x, int a) {
+    Stencil s;
+    s.n = (int)x.size();
+    s.rank = 2 * a + 1;
+    s.w.assign((size_t)2 * s.n * s.rank, 0.0);
+    if (s.n == 1 || a == 0) return s;
+    std::vector<double> nodes(s.rank), w(s.rank);
+    for (int order = 1; order <= 2; ++order)
+        for (int i = 1; i <= s.n; ++i) {
+            const int shift = (i - 1 < a) ? a - i + 1 : (i >= s.n - a + 1 ? (s.n - a) - i : 0);
+            for (int m = 0; m < s.rank; ++m) nodes[m] = x[(size_t)(i + m - a + shift - 1)];
+            fd_weights(x[i - 1], nodes.data(), s.rank - 1, order, w.data());
+            std::copy(w.begin(), w.end(), s.w.begin() + ((size_t)(order - 1) * s.n + (i - 1)) * s.rank);
+        }
+    return s;
+}
+
+// sigma stencils, one-sided near the free surface and the bottom ghost
+// (PreProcessDiffStencils.f90:108-132).
+Stencil stencils_z(const std::vector<double>& z, int Nz, int gz, int g) {
+    Stencil s;
+    const int Nzp = Nz + gz;
+    s.n = Nzp;
+    s.rank = 2 * g + 1;
+    s.w.assign((size_t)2 * s.n * s.rank, 0.0);
+    std::vector<double> nodes(s.rank), w(s.rank);
+    for (int order = 1; order <= 2; ++order)
+        for (int i = 1; i <= Nzp; ++i) {
+            int left, off;  // expansion node index within the window, window offset
+            if (i - 1 < g) { const int d = g - i + 1; left = g - d; off = d; }
+            else if (i >= Nz - g + 1) { const int d = i - (Nzp - g); left = g + d; off = -d; }
+            else { left = g; off = 0; }
+            for (int m = 0; m < s.rank; ++m) nodes[m] = z[(size_t)(i + m - g + off - 1)];
+            fd_weights(nodes[left], nodes.data(), s.rank - 1, order, w.data());
+            std::copy(w.begin(), w.end(), s.w.begin() + ((size_t)(order - 1) * s.n + (i - 1)) * s.rank);
+        }
+    return s;
+}
+
+// ------------------------------------------------------------- hierarchy
+// Level count: NINT(log2(max(Nx,Ny,Nz)-1)) in single precision (MGPreProcess.f90:449-458).
+static int level_count(int nx, int ny, int nz) {
+    const float nmax = (float)std::max(nx, std::max(ny, nz));
+    return (int)std::lround(std::log10(nmax - 1.0f) / std::log10(2.0f));
+}
+
+static void coarsen_flags(int strategy, int nx, int ny, int nz, int& xc, int& yc, int& zc) {
+    xc = yc = zc = 0;
+    if (strategy == 1) {
+        if (nx == ny && nx == nz) xc = yc = zc = 1;
+        else if (nx > ny && nx > nz) xc = 1;
+        else if (ny > nx && ny > nz) yc = 1;
+        else if (nz > nx && nz > ny) zc = 1;
+        else if (nx == ny && nx > nz) xc = yc = 1;
+        else if (nx == nz && nx > ny) xc = zc = 1;
+        else if (ny == nz && ny > nx) yc = zc = 1;
+    } else if (strategy == 2) {
+        xc = nx > 3; yc = ny > 3; zc = nz > 3;
+    } else {  // MGPreProcess.f90:140-178
+        if (nx == 1) { yc = 1; zc = (ny == nz); }
+        else if (ny == 1) { xc = 1; zc = (nx == nz); }
+        else if (nx == ny && nx == nz) xc = yc = zc = 1;
+        else { xc = nx > nz; yc = ny > nz; zc = (nx < nz && ny < nz); }
+    }
+}
+
+static void level_sigma(LevelHost& L) {
+    L.zs = L.z;
+    L.zs[0] = 0.0;  // DetermineTransformationConstantsArray.f90:59 (sigma = 0 below the bottom)
+}
+
+static void level_colours(LevelHost& L) {
+    double m = 0;
+    for (size_t c = 0; c < L.hx.size(); ++c) m = std::max(m, std::max(std::fabs(L.hx[c]), std::fabs(L.hy[c])));
+    // Mixed-derivative terms couple diagonal neighbour columns; without them a
+    // red-black colouring of the columns is a proper colouring.
+    L.ncolor = (L.Nxg > 1 && L.Nyg > 1 && m > 0) ? 4 : 2;
+}
+
+int build_grid(const ow3d_params& p, const double* h, const double* hx, const double* hxx, const double* hy,
+               const double* hyy, GridHost& G, std::string* err) {
+    auto fail = [&](const char* m) { if (err) *err = m; return OW3D_ERR_BAD_INPUT; };
+    if (p.Nx < 1 || p.Ny < 1 || p.Nz < 3) return fail("Nx, Ny >= 1 and Nz >= 3 required");
+    if (p.Nx == 1) return fail("Nx == 1 (2-D in y) is not supported; orient the flume along x");
+    if (p.GhostGridZ != 1) return fail("GhostGridZ must be 1 (ReadInputFileParameters.f90:283-285)");
+    if (p.Nx > 1 && p.GhostGridX != 1) return fail("GhostGridX must be 1");
+    if (p.Ny > 1 && p.GhostGridY != 1) return fail("GhostGridY must be 1");
+    if (p.alpha != 3 || (p.Ny > 1 && p.beta != 3) || p.gamma != 3) return fail("alpha = beta = gamma = 3 required");
+    if (p.alphaprecond != 1 || (p.Ny > 1 && p.betaprecond != 1) || p.gammaprecond != 1)
+        return fail("alphaprecond = betaprecond = gammaprecond = 1 required");
+    if (p.Nz + 1 > kMaxNzgHost) return fail("Nz too large");
+    G.Nx = p.Nx; G.Ny = p.Ny; G.Nz = p.Nz;
+    G.gx = 1; G.gy = (p.Ny > 1) ? 1 : 0; G.gz = 1;
+    G.Nxg = p.Nx + 2 * G.gx; G.Nyg = p.Ny + 2 * G.gy; G.Nzg = p.Nz + G.gz;
+    G.C = (int64_t)G.Nxg * G.Nyg; G.N = G.C * G.Nzg;
+    G.three = (p.Ny > 1) ? 1 : 0;
+    if (G.Nxg < 8 || (G.three && G.Nyg < 8) || G.Nzg < 8) return fail("at least 7 points per direction (6th-order stencils)");
+    // SetupCompDomain.f90:35-79
+    if (p.filteringONOFF > 0) {
+        const int NP = 2 * p.filterALPHA + 1;
+        if (p.filterALPHA < 1 || p.filterALPHA > 6) return fail("filterALPHA must be 1..6 (FilterInit.f90 boundary filters)");
+        if (G.Nxg < NP + 2 || (G.three && G.Nyg < NP + 2)) return fail("grid too small for the filter width");
+    }
+    G.x.assign(G.Nxg, 0.0); G.y.assign(G.Nyg, p.Ly); G.z.assign(G.Nzg, 0.0);
+    for (int i = -G.gx; i <= p.Nx - 1 + G.gx; ++i) G.x[i + G.gx] = (double)i / (double)(p.Nx - 1) * p.Lx;
+    if (p.Ny > 1)
+        for (int j = -G.gy; j <= p.Ny - 1 + G.gy; ++j) G.y[j + G.gy] = (double)j / (double)(p.Ny - 1) * p.Ly;
+    const double pi = 3.14159265358979323846;
+    for (int k = 0; k <= p.Nz - 1; ++k)
+        G.z[k + 1] = (p.GridZ == 0) ? (double)k / (double)(p.Nz - 1) * p.Lz
+                                    : std::sin(pi * (double)k / (double)(2 * (p.Nz - 1)));
+    G.z[0] = -G.z[2];
+    G.zs = G.z; G.zs[0] = 0.0;
+    const size_t C = (size_t)G.C;
+    auto cp = [&](const double* s, std::vector<double>& d) { d.assign(C, 0.0); if (s) std::copy(s, s + C, d.begin()); };
+    cp(h, G.h); cp(hx, G.hx); cp(hxx, G.hxx); cp(hy, G.hy); cp(hyy, G.hyy);
+    if (!h) return fail("bathymetry h is required");
+    for (size_t c = 0; c < C; ++c) if (!(G.h[c] > 0)) return fail("depth h must be positive everywhere (ghosts included)");
+    G.SX = stencils_xy(G.x, 3);
+    G.SY = stencils_xy(G.y, G.three ? 3 : 0);
+    G.SZ = stencils_z(G.z, p.Nz, 1, 3);
+    // multigrid hierarchy (MGPreProcess.f90:31-318)
+    G.levels.clear();
+    if (p.Precond != 3) return 0;
+    int L = level_count(p.Nx, p.Ny, p.Nz);
+    if (L > p.MGmaxgrids && p.MGmaxgrids > 0) L = p.MGmaxgrids;
+    if (L < 1) L = 1;
+    if (L > kMaxLevelsHost) return fail("too many multigrid levels");
+    G.levels.assign(L, LevelHost());
+    LevelHost& F = G.levels[L - 1];
+    F.Nx = p.Nx; F.Ny = p.Ny; F.Nz = p.Nz; F.Nxg = G.Nxg; F.Nyg = G.Nyg; F.Nzg = G.Nzg;
+    F.x = G.x; F.y = G.y; F.z = G.z;
+    F.h = G.h; F.hx = G.hx; F.hxx = G.hxx; F.hy = G.hy; F.hyy = G.hyy;
+    for (int l = L - 2; l >= 0; --l) {
+        const LevelHost& f = G.levels[l + 1];
+        LevelHost& c = G.levels[l];
+        int xc, yc, zc;
+        coarsen_flags(p.MGCoarseningStrategy, f.Nx, f.Ny, f.Nz, xc, yc, zc);
+        if (xc && f.Nx % 2 == 0) return fail("cannot coarsen in x: Nx must be odd (MGPreProcess.f90:184)");
+        if (yc && f.Ny % 2 == 0) return fail("cannot coarsen in y: Ny must be odd");
+        c.Nx = xc ? (f.Nx - 1) / 2 + 1 : f.Nx;
+        c.Ny = yc ? (f.Ny - 1) / 2 + 1 : f.Ny;
+        c.Nz = zc ? (f.Nz - 1) / 2 + 1 : f.Nz;
+        if (zc && c.Nz % 2 == 0) return fail("cannot coarsen in z: Nz must be odd");
+        c.xc = xc; c.yc = yc; c.zc = zc;
+        const int XF = xc ? 2 : 1, YF = yc ? 2 : 1, ZF = zc ? 2 : 1;
+        c.Nxg = c.Nx + 2 * G.gx; c.Nyg = c.Ny + 2 * G.gy; c.Nzg = c.Nz + 1;
+        c.x.assign(c.Nxg, 0.0);
+        for (int i = 2; i <= c.Nxg - 1; ++i) c.x[i - 1] = f.x[(size_t)(2 + (i - 2) * XF - 1)];
+        c.x[0] = c.x[1] - (c.x[2] - c.x[1]);
+        c.x[c.Nxg - 1] = c.x[c.Nxg - 2] + (c.x[c.Nxg - 2] - c.x[c.Nxg - 3]);
+        c.y.assign(c.Nyg, p.Ly);
+        if (G.three) {
+            for (int j = 2; j <= c.Nyg - 1; ++j) c.y[j - 1] = f.y[(size_t)(2 + (j - 2) * YF - 1)];
+            c.y[0] = c.y[1] - (c.y[2] - c.y[1]);
+            c.y[c.Nyg - 1] = c.y[c.Nyg - 2] + (c.y[c.Nyg - 2] - c.y[c.Nyg - 3]);
+        }
+        c.z.assign(c.Nzg, 0.0);
+        c.z[0] = -f.z[(size_t)(2 + ZF - 1)];
+        for (int k = 2; k <= c.Nzg; ++k) c.z[k - 1] = f.z[(size_t)(2 + (k - 2) * ZF - 1)];
+        const size_t Cc = (size_t)c.Nxg * c.Nyg;
+        c.h.assign(Cc, 0.0); c.hx.assign(Cc, 0.0); c.hxx.assign(Cc, 0.0); c.hy.assign(Cc, 0.0); c.hyy.assign(Cc, 0.0);
+        for (int j = 1 + G.gy; j <= c.Nyg - G.gy; ++j)
+            for (int i = 2; i <= c.Nxg - 1; ++i) {
+                const int fi = 2 + (i - 2) * XF, fj = G.gy ? 2 + (j - 2) * YF : 1;
+                const size_t cc = (size_t)(i - 1) + (size_t)c.Nxg * (j - 1);
+                const size_t ff = (size_t)(fi - 1) + (size_t)f.Nxg * (fj - 1);
+                c.h[cc] = f.h[ff]; c.hx[cc] = f.hx[ff]; c.hxx[cc] = f.hxx[ff]; c.hy[cc] = f.hy[ff]; c.hyy[cc] = f.hyy[ff];
+            }
+        // depth on the ghost points copied from the adjacent interior (MGPreProcess.f90:311-314)
+        for (int j = 1; j <= c.Nyg; ++j) {
+            c.h[(size_t)c.Nxg * (j - 1)] = c.h[1 + (size_t)c.Nxg * (j - 1)];
+            c.h[(size_t)(c.Nxg - 1) + (size_t)c.Nxg * (j - 1)] = c.h[(size_t)(c.Nxg - 2) + (size_t)c.Nxg * (j - 1)];
+        }
+        for (int i = 1; i <= c.Nxg; ++i) {
+            c.h[(size_t)(i - 1)] = c.h[(size_t)(i - 1) + (size_t)c.Nxg * (1 + G.gy - 1)];
+            c.h[(size_t)(i - 1) + (size_t)c.Nxg * (c.Nyg - 1)] = c.h[(size_t)(i - 1) + (size_t)c.Nxg * (c.Nyg - G.gy - 1)];
+        }
+    }
+    for (auto& Lv : G.levels) {
+        level_sigma(Lv);
+        level_colours(Lv);
+        Lv.SX = stencils_xy(Lv.x, 1);
+        Lv.SY = stencils_xy(Lv.y, G.three ? 1 : 0);
+        Lv.SZ = stencils_z(Lv.z, Lv.Nz, 1, 1);
+        if (Lv.Nxg < 4 || (G.three && Lv.Nyg < 4) || Lv.Nzg < 4) return fail("multigrid level too small");
+    }
+    return 0;
+}
+
+// ------------------------------------------------------- relaxation zones
+// PreprocessRelaxationZones.f90 (TracePosition) + GammaFunctions.f90:20-35.
+static int trace_position(const std::vector<double>& x, double x0) {
+    for (size_t i = 0; i < x.size(); ++i) if (x0 <= x[i]) return (int)i + 1;
+    return (int)x.size();
+}
+static std::vector<double> gamma_fn(const double* x, int n, int dir, int ftype, double param) {
+    std::vector<double> g(n), t(n);
+    for (int i = 0; i < n; ++i) t[i] = (n > 1) ? (x[i] - x[0]) / (x[n - 1] - x[0]) : x[i];
+    const double e1 = std::exp(1.0) - 1.0;
+    for (int i = 0; i < n; ++i) {
+        const double q = (n > 1) ? (x[i] - x[n - 1]) / (x[n - 1] - x[0]) : 0.0;
+        switch (std::abs(ftype)) {
+            case 9: g[i] = 1.0 - std::pow(t[i], param); break;
+            case 10: g[i] = 3.0 * t[i] * t[i] - 2.0 * t[i] * t[i] * t[i]; break;
+            case 11: g[i] = (std::exp(std::pow(t[i], param)) - 1.0) / e1; break;
+            case 12: g[i] = std::exp(-q * q / (2.0 * param * param)); break;
+            case 13: g[i] = 1.0 - std::exp(-q * q / (2.0 * param * param)); break;
+            case 14: g[i] = 1.0 - (std::exp(std::pow(t[i], param)) - 1.0) / e1; break;
+            default: g[i] = 1.0;
+        }
+    }
+    if (dir == -1) std::reverse(g.begin(), g.end());
+    return g;
+}
+std::vector<ZoneHost> build_zones(const ow3d_params& p, const GridHost& G) {
+    std::vector<ZoneHost> out;
+    if (p.relaxONOFF != 1) return out;
+    for (int z = 0; z < p.relaxNo && z < OW3D_MAX_ZONES; ++z) {
+        const ow3d_zone& d = p.zones[z];
+        ZoneHost Z;
+        Z.i0 = Z.i1 = Z.j0 = Z.j1 = 1;
+        if (p.Nx > 1) { Z.i0 = trace_position(G.x, d.x1); Z.i1 = trace_position(G.x, d.x2); }
+        if (p.Ny > 1) { Z.j0 = trace_position(G.y, d.y1); Z.j1 = trace_position(G.y, d.y2); }
+        Z.xdir = (d.XorY == 'X' || d.XorY == 'x');
+        Z.wavegen = d.WavegenONOFF;
+        Z.phion = d.PhiOnOff;
+        const int dir = d.ftype >= 0 ? 1 : -1;
+        if (Z.xdir) Z.gam = gamma_fn(&G.x[(size_t)Z.i0 - 1], Z.i1 - Z.i0 + 1, dir, d.ftype, d.param);
+        else Z.gam = gamma_fn(&G.y[(size_t)Z.j0 - 1], Z.j1 - Z.j0 + 1, dir, d.ftype, d.param);
+        out.push_back(Z);
+    }
+    return out;
+}
+
+// -------------------------------------------------------------- filtering
+// Savitzky-Golay smoothing weights: value at offset 0 of the least-squares
+// polynomial of degree m through offsets -nl..nr (savgol.f90 with ld = 0).
+static std::vector<double> savgol(int nl, int nr, int m) {
+    const int M = m + 1;
+    std::vector<double> A((size_t)M * M, 0.0), b(M, 0.0);
+    // normal equations: A(a,b) = sum_k k^(a+b)
+    for (int a = 0; a < M; ++a)
+        for (int c = 0; c < M; ++c) {
+            double s = 0;
+            for (int k = -nl; k <= nr; ++k) s += (a + c == 0) ? 1.0 : std::pow((double)k, a + c);
+            A[(size_t)a * M + c] = s;
+        }
+    b[0] = 1.0;
+    for (int k = 0; k < M; ++k) {  // Gaussian elimination, partial pivoting
+        int pr = k;
+        for (int r = k + 1; r < M; ++r) if (std::fabs(A[(size_t)r * M + k]) > std::fabs(A[(size_t)pr * M + k])) pr = r;
+        if (pr != k) { for (int c = 0; c < M; ++c) std::swap(A[(size_t)k * M + c], A[(size_t)pr * M + c]); std::swap(b[k], b[pr]); }
+        for (int r = k + 1; r < M; ++r) {
+            const double f = A[(size_t)r * M + k] / A[(size_t)k * M + k];
+            for (int c = k; c < M; ++c) A[(size_t)r * M + c] -= f * A[(size_t)k * M + c];
+            b[r] -= f * b[k];
+        }
+    }
+    for (int r = M - 1; r >= 0; --r) {
+        double t = b[r];
+        for (int c = r + 1; c < M; ++c) t -= A[(size_t)r * M + c] * b[c];
+        b[r] = t / A[(size_t)r * M + r];
+    }
+    std::vector<double> w(nl + nr + 1);
+    for (int k = -nl; k <= nr; ++k) {
+        double s = b[0], f = 1.0;
+        for (int q = 1; q <= m; ++q) { f *= k; s += b[q] * f; }
+        w[k + nl] = s;
+    }
+    return w;
+}
+
+// FilterInit.f90:29-231. fc: 2a+1 centred weights. F2: the boundary weights in
+// the (2a+1) x a column-major view FILTERING.f90 uses on the reference's
+// max(2a+1,13) x max(a,6) storage.
+void filter_coeffs(const ow3d_params& p, std::vector<double>& fc, std::vector<double>& F2) {
+    const int a = p.filterALPHA, NP = 2 * a + 1;
+    fc = savgol(a, a, p.filterORDER);
+    const int ld = std::max(NP, 13), nc = std::max(a, 6);
+    std::vector<double> S((size_t)ld * nc, 0.0);
+    auto at = [&](int r, int c) -> double& { return S[(size_t)(c - 1) * ld + (r - 1)]; };
+    // Off-centred boundary filters of Berland et al. (J. Comput. Phys. 224,
+    // 2007), the table FilterInit.f90:149-186 applies with weights sigma_filt.
+    static const double b1[4] = {0.320882352941, -0.465, 0.179117647059, -0.035};
+    static const double b2[7] = {-0.085777408970, 0.277628171524, -0.356848072173, 0.223119093072,
+                                 -0.057347064865, -0.000747264596, -0.000027453993};
+    static const double b3[11] = {0.052523901012, -0.206299133811, 0.353527998250, -0.348142394842,
+                                  0.181481803619, 0.009440804370, -0.077675100452, 0.044887364863,
+                                  -0.009971961849, 0.000113359420, 0.000113359420};
+    at(1, 1) = 1.0; for (int r = 0; r < 4; ++r) at(r + 1, 1) -= p.sigma_filt[0] * b1[r];
+    at(2, 2) = 1.0; for (int r = 0; r < 7; ++r) at(r + 1, 2) -= p.sigma_filt[1] * b2[r];
+    at(3, 3) = 1.0; for (int r = 0; r < 11; ++r) at(r + 1, 3) -= p.sigma_filt[2] * b3[r];
+    const int degree[3] = {5, 6, 8};
+    for (int c = 4; c <= 6; ++c) {
+        const int hw = c - 1;
+        const std::vector<double> w = savgol(hw, hw, degree[c - 4]);
+        for (int r = 1; r <= 2 * hw + 1; ++r) at(r, c) = w[(size_t)r - 1];
+    }
+    if (std::fabs(p.sigma_filt[0]) < 1e-12) {
+        std::fill(S.begin(), S.end(), 0.0);
+        for (int i = 1; i <= nc; ++i) at(i, i) = 1.0;
+    }
+    F2.assign(S.begin(), S.begin() + (size_t)NP * a);
+}
+
+// ------------------------------------------------------------- the deck
+int default_params(ow3d_params* p) {
+    if (!p) return OW3D_ERR_BAD_INPUT;
+    std::memset(p, 0, sizeof(*p));
+    p->IC = 0; p->IncWaveType = 0;
+    p->Lx = p->Ly = p->Lz = 1.0;
+    p->Nx = 17; p->Ny = 1; p->Nz = 9;
+    p->GridZ = 1; p->GhostGridX = p->GhostGridY = p->GhostGridZ = 1;
+    p->alpha = p->beta = p->gamma = 3;
+    p->alphaprecond = p->betaprecond = p->gammaprecond = 1;
+    p->Nsteps = 1; p->dt = 0.01; p->timemethod = 1; p->CFL = 0; p->extrapolationONOFF = 1;
+    p->g = 9.81;
+    p->solver = 1; p->Precond = 3; p->MGCoarseningStrategy = 0; p->GMRESmaxiterations = 23;
+    p->reltol = 1e-8; p->abstol = 1e-6; p->maxit = 1; p->cyclet = 'V'; p->nu1 = 1; p->nu2 = 1; p->MGmaxgrids = 0;
+    p->LinearONOFF = 1; p->PressureTermOnOff = 0;
+    p->filteringONOFF = 0; p->filterALPHA = 6; p->filterORDER = 10;
+    p->sigma_filt[0] = 0.08; p->sigma_filt[1] = 0.08; p->sigma_filt[2] = 0.4;
+    p->relaxONOFF = 0; p->relaxXorY = 'X';
+    for (auto& z : p->zones) { z.XorY = 'X'; z.XorYgen = 'X'; z.PhiOnOff = 1; }
+    p->precision = OW3D_PREC_FP64; p->krylov = OW3D_KRYLOV_FGMRES; p->device = 0;
+    return OW3D_OK;
+}
+
+namespace {
+// Fortran list-directed records: whitespace/comma separated items, D exponents.
+struct Record {
+    std::vector<std::string> t;
+    bool num(size_t i) const {
+        if (i >= t.size()) return false;
+        std::string s = t[i];
+        for (auto& ch : s) if (ch == 'd' || ch == 'D') ch = 'e';
+        char* end = nullptr;
+        std::strtod(s.c_str(), &end);
+        return end && *end == 0 && !s.empty();
+    }
+    double d(size_t i) const {
+        std::string s = t[i];
+        for (auto& ch : s) if (ch == 'd' || ch == 'D') ch = 'e';
+        return std::strtod(s.c_str(), nullptr);
+    }
+    int n(size_t i) const { return (int)std::lround(d(i)); }
+    char c(size_t i) const {
+        std::string s = t[i];
+        for (char ch : s) if (ch != '\'' && ch != '"') return ch;
+        return ' ';
+    }
+    size_t nnum() const { size_t k = 0; while (num(k)) ++k; return k; }
+};
+Record split(const std::string& line) {
+    Record r;
+    std::string cur;
+    for (char ch : line) {
+        if (std::isspace((unsigned char)ch) || ch == ',') { if (!cur.empty()) { r.t.push_back(cur); cur.clear(); } }
+        else cur += ch;
+    }
+    if (!cur.empty()) r.t.push_back(cur);
+    return r;
+}
+}  // namespace
+
+// ReadInputFileParameters.f90:18-517 (lines 1-13 of the deck).
+int read_deck(const char* path, ow3d_params* p, std::string* err) {
+    auto fail = [&](const std::string& m) { if (err) *err = m; return OW3D_ERR_BAD_INPUT; };
+    std::ifstream f(path);
+    if (!f) { if (err) *err = std::string("cannot open ") + path; return OW3D_ERR_IO; }
+    default_params(p);
+    std::vector<std::string> lines;
+    std::string s;
+    while (std::getline(f, s)) lines.push_back(s);
+    size_t li = 1;  // line 0 is the header
+    auto next = [&]() -> Record { return li < lines.size() ? split(lines[li++]) : Record(); };
+    Record r = next();  // IC [IncWaveType [accel_tol_fact]]
+    if (!r.num(0)) return fail("line 2: IC expected");
+    p->IC = r.n(0);
+    p->IncWaveType = r.num(1) ? r.n(1) : 0;
+    if (p->IncWaveType == 4) p->IncWaveType = 1;
+    r = next();  // Lx Ly Lz Nx Ny Nz GridX GridY GridZ GhostGridX GhostGridY GhostGridZ
+    if (r.nnum() < 12) return fail("line 3: 12 grid values expected");
+    p->Lx = r.d(0); p->Ly = r.d(1); p->Lz = r.d(2);
+    p->Nx = r.n(3); p->Ny = r.n(4); p->Nz = r.n(5);
+    p->GridX = r.n(6); p->GridY = r.n(7); p->GridZ = r.n(8);
+    p->GhostGridX = r.n(9); p->GhostGridY = r.n(10); p->GhostGridZ = r.n(11);
+    if (p->Nx == 1) p->GhostGridX = 0;
+    if (p->Ny == 1) p->GhostGridY = 0;
+    r = next();  // alpha beta gamma alphaprecond betaprecond gammaprecond
+    if (r.nnum() < 6) return fail("line 4: 6 stencil values expected");
+    p->alpha = r.n(0); p->beta = r.n(1); p->gamma = r.n(2);
+    p->alphaprecond = r.n(3); p->betaprecond = r.n(4); p->gammaprecond = r.n(5);
+    if (p->Nx == 1) { p->alpha = 0; p->alphaprecond = 0; }
+    if (p->Ny == 1) { p->beta = 0; p->betaprecond = 0; }
+    r = next();  // Nsteps dt timemethod CFL extrapolationONOFF [time0]
+    if (r.nnum() < 5) return fail("line 5: Nsteps dt timemethod CFL extrapolationONOFF expected");
+    p->Nsteps = r.n(0); p->dt = r.d(1); p->timemethod = r.n(2); p->CFL = r.d(3); p->extrapolationONOFF = r.n(4);
+    p->time0 = r.num(5) ? r.d(5) : 0.0;
+    if (p->CFL != 0.0) {
+        const double dx = p->Lx / (p->Nx - 1.0), dy = p->Ny > 1 ? p->Ly / (p->Ny - 1.0) : dx;
+        p->dt = p->CFL * (p->Nx == 1 ? dy : dx);
+    }
+    r = next();  // g [rho]
+    if (!r.num(0)) return fail("line 6: g expected");
+    p->g = r.d(0);
+    r = next();  // [solver] Precond MGCoarseningStrategy GMRESmaxiterations reltol abstol maxit cyclet nu1 nu2 MGmaxgrids
+    {
+        const size_t k = r.nnum();
+        size_t o;
+        if (k >= 7 && r.t.size() >= 11 && !r.num(7)) { p->solver = r.n(0); o = 1; }
+        else if (k >= 6 && r.t.size() >= 10 && !r.num(6)) { p->solver = 1; o = 0; }
+        else return fail("line 7: solver line not recognised");
+        p->Precond = r.n(o); p->MGCoarseningStrategy = r.n(o + 1); p->GMRESmaxiterations = r.n(o + 2);
+        p->reltol = r.d(o + 3); p->abstol = r.d(o + 4); p->maxit = r.n(o + 5); p->cyclet = r.c(o + 6);
+        p->nu1 = r.n(o + 7); p->nu2 = r.n(o + 8); p->MGmaxgrids = r.n(o + 9);
+    }
+    r = next();  // stream-function line (always present)
+    r = next();  // StoreDataONOFF formattype [iKinematics nOutFiles]
+    if (r.nnum() >= 2) {
+        const int ft = r.n(1);
+        if (ft == 20 || ft == 21 || ft == 22) {
+            const int nout = r.num(3) ? r.n(3) : 0;
+            for (int i = 0; i < nout; ++i) next();
+        }
+    }
+    r = next();  // LinearONOFF PressureTermONOFF
+    if (r.nnum() < 1) return fail("line 10: LinearONOFF expected");
+    p->LinearONOFF = r.n(0); p->PressureTermOnOff = r.num(1) ? r.n(1) : 0;
+    r = next();  // filteringONOFF filterALPHA filterORDER sigma_filt(1:3)
+    if (r.nnum() < 3) return fail("line 11: filter line expected");
+    p->filteringONOFF = r.n(0); p->filterALPHA = r.n(1); p->filterORDER = r.n(2);
+    for (int q = 0; q < 3; ++q) p->sigma_filt[q] = r.num(3 + q) ? r.d(3 + q) : 0.0;
+    r = next();  // optional breaking line (7 numbers), else the relaxation line
+    if (r.nnum() >= 7) r = next();
+    // relaxONOFF relaxTransientTime relaxNo relaxXorY relaxDegrees
+    if (r.nnum() < 3) return fail("line 13: relaxation line expected");
+    p->relaxONOFF = r.n(0); p->relaxTransientTime = r.d(1); p->relaxNo = r.n(2);
+    p->relaxXorY = r.t.size() > 3 ? r.c(3) : 'X';
+    p->relaxDegrees = (r.t.size() > 4 && r.num(4)) ? r.d(4) : 0.0;
+    if (p->relaxONOFF == 1) {
+        if (p->relaxNo > OW3D_MAX_ZONES) return fail("too many relaxation zones");
+        for (int z = 0; z < p->relaxNo; ++z) {
+            Record q = next();
+            if (q.t.size() < 10) return fail("relaxation zone line: 10 items expected");
+            ow3d_zone& Z = p->zones[z];
+            Z.x1 = q.d(0); Z.x2 = q.d(1); Z.y1 = q.d(2); Z.y2 = q.d(3); Z.ftype = q.n(4); Z.param = q.d(5);
+            Z.XorY = q.c(6); Z.WavegenONOFF = q.n(7); Z.XorYgen = q.c(8); Z.degrees = q.d(9); Z.PhiOnOff = 1;
+        }
+    }
+    return OW3D_OK;
+}
+
+}  // namespace ow3d

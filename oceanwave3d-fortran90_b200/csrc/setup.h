@@ -1,0 +1,59 @@
+// Host-side set-up of one simulation: grid, stencils, multigrid hierarchy,
+// relaxation zones and filter coefficients (the device-relevant half of
+// OceanWave3DT0Setup, src/main/OceanWave3DT0Setup.f90:35-444).
+#pragma once
+#include <string>
+#include <vector>
+#include "../../include/ow3d.h"
+
+namespace ow3d {
+
+constexpr int kMaxNzgHost = 64;      // sigma levels incl. the ghost level
+constexpr int kMaxLevelsHost = 16;   // multigrid levels
+
+// Per-position stencils of half width a: w[((order-1)*n + pos)*rank + m].
+struct Stencil {
+    int n = 0, rank = 0;
+    std::vector<double> w;
+    double at(int order, int pos, int m) const { return w[((size_t)(order - 1) * n + pos) * rank + m]; }
+};
+
+struct LevelHost {
+    int Nx = 1, Ny = 1, Nz = 1, Nxg = 1, Nyg = 1, Nzg = 1;
+    int xc = 0, yc = 0, zc = 0;     // coarsened w.r.t. the next finer level
+    int ncolor = 2;
+    std::vector<double> x, y, z, zs;
+    std::vector<double> h, hx, hxx, hy, hyy;
+    Stencil SX, SY, SZ;             // half width 1
+};
+
+struct GridHost {
+    int Nx, Ny, Nz, gx, gy, gz, Nxg, Nyg, Nzg;
+    int64_t N, C;
+    int three;
+    std::vector<double> x, y, z, zs;
+    std::vector<double> h, hx, hxx, hy, hyy;
+    Stencil SX, SY, SZ;             // half width 3
+    std::vector<LevelHost> levels;  // levels[0] coarsest
+};
+
+struct ZoneHost {
+    int i0, i1, j0, j1;
+    int xdir, wavegen, phion;
+    std::vector<double> gam;
+};
+
+void fd_weights(double z, const double* x, int n, int order, double* w);
+Stencil stencils_xy(const std::vector<double>& x, int a);
+Stencil stencils_z(const std::vector<double>& z, int Nz, int gz, int g);
+
+// Returns 0 or an OW3D_ERR_* code with a message in *err.
+int build_grid(const ow3d_params& p, const double* h, const double* hx, const double* hxx, const double* hy,
+               const double* hyy, GridHost& G, std::string* err);
+std::vector<ZoneHost> build_zones(const ow3d_params& p, const GridHost& G);
+void filter_coeffs(const ow3d_params& p, std::vector<double>& fc, std::vector<double>& F2);
+
+int default_params(ow3d_params* p);
+int read_deck(const char* path, ow3d_params* p, std::string* err);
+
+}  // namespace ow3d
