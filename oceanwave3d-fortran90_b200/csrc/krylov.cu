@@ -62,7 +62,16 @@ __device__ bool last_block_reduce(double* partial, int nv, int nblocks, unsigned
     for (int v = wid; v < nv; v += nw) {
         const double* pv = partial + (int64_t)v * nblocks;
         double s = 0;
-        for (int b = lane; b < nblocks; b += 32) s += __ldcg(pv + b);
+        int b = lane;
+        // eight independent L2 loads in flight per lane, then added in order
+        for (; b + 7 * 32 < nblocks; b += 8 * 32) {
+            double q[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) q[u] = __ldcg(pv + b + u * 32);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) s += q[u];
+        }
+        for (; b < nblocks; b += 32) s += __ldcg(pv + b);
         s = warp_sum(s);
         if (lane == 0) out[v] = s;
     }
@@ -71,75 +80,150 @@ __device__ bool last_block_reduce(double* partial, int nv, int nblocks, unsigned
     return true;
 }
 
-// Basis vectors are contiguous: V_i = V + i * ldv.
+// One thread: finish Arnoldi step k (1-based after increment).
+__device__ void arnoldi_finish_dev(KrylovState* ks, int maxmv, int m) {
+    if (ks->done) return;
+    const int k = ks->k + 1;           // this step's column index is ks->k (0-based)
+    double* hc = ks->H[ks->k];
+    const double nrm = sqrt(ks->w1);
+    hc[k] = nrm;
+    ks->scale[k] = nrm > 0 ? 1.0 / nrm : 0.0;
+    for (int i = 0; i < k - 1; ++i) {
+        const double a0 = hc[i];
+        hc[i] = ks->cs[i] * a0 + ks->sn[i] * hc[i + 1];
+        hc[i + 1] = ks->cs[i] * hc[i + 1] - ks->sn[i] * a0;
+    }
+    double x = hc[k - 1], yv = hc[k];
+    const double r = sqrt(x * x + yv * yv);
+    double c = 1.0, s = 0.0;
+    if (r != 0.0) { c = x / r; s = yv / r; }
+    hc[k - 1] = r; hc[k] = 0.0;
+    ks->cs[k - 1] = c; ks->sn[k - 1] = s;
+    const double al = -s * ks->g[k - 1];
+    ks->g[k - 1] = c * ks->g[k - 1];
+    ks->g[k] = al;
+    ks->resid = fabs(al);
+    ks->k = k;
+    ks->iters += 1;
+    ks->reorth = 0;
+    const bool conv = ks->resid <= ks->tol;
+    if (conv) ks->converged = 1;
+    if (conv || k >= m || ks->iters >= maxmv || nrm == 0.0) ks->done = 1;
+}
+
+__global__ void k_arnoldi_finish(KrylovState* ks, int maxmv, int m) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    arnoldi_finish_dev(ks, maxmv, m);
+}
+
+// Basis vectors are contiguous: V_i = V + i * ldv, ldv even and the padding
+// past n zero, so element pairs (16-byte loads) can run to n rounded up.
+// Grid (nbx, k+1): block (bx, v) forms a partial of <V_v, w> (v < k) or of
+// |w|^2 (v == k) over a slice of the elements; w is re-read per v from L2.
 // cond: 0 always run; 1 run only when ks->reorth is set (second CGS pass).
 __global__ void __launch_bounds__(kThreads) k_multidot(const double* __restrict__ V, int64_t ldv, int k,
                                                        const double* __restrict__ w, int64_t n, double* partial,
-                                                       unsigned int* counter, int nblocks, KrylovState* ks, int cond) {
+                                                       unsigned int* counter, int nbx, KrylovState* ks, int cond) {
     if (cond && !ks->reorth) return;
     if (ks->done) return;
-    const int nv = k + 1;   // k dot products and |w|^2
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    __shared__ double red[kThreads / 32][8];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int v0 = 0; v0 < nv; v0 += 8) {
-        double acc[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) acc[u] = 0.0;
-        for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += stride) {
-            const double wt = w[t];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int v = v0 + u;
-                if (v < k) acc[u] += V[(int64_t)v * ldv + t] * wt;
-                else if (v == k) acc[u] += wt * wt;
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            double sm = warp_sum(acc[u]);
-            if (lane == 0) red[wid][u] = sm;
-        }
-        __syncthreads();
-        if (threadIdx.x < 8 && v0 + (int)threadIdx.x < nv) {
-            double sm = 0;
-            for (int q = 0; q < (int)(blockDim.x / 32); ++q) sm += red[q][threadIdx.x];
-            partial[(int64_t)(v0 + threadIdx.x) * nblocks + blockIdx.x] = sm;
-        }
-        __syncthreads();
+    const int v = blockIdx.y;
+    const int64_t n2 = (n + 1) / 2;
+    const double2* w2 = reinterpret_cast<const double2*>(w);
+    const double2* a2 = reinterpret_cast<const double2*>(v < k ? V + (int64_t)v * ldv : w);
+    const int64_t stride = (int64_t)nbx * blockDim.x;
+    double acc0 = 0, acc1 = 0, acc2 = 0, acc3 = 0;
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (; t + 3 * stride < n2; t += 4 * stride) {
+        const double2 x0 = a2[t], x1 = a2[t + stride], x2 = a2[t + 2 * stride], x3 = a2[t + 3 * stride];
+        const double2 y0 = w2[t], y1 = w2[t + stride], y2 = w2[t + 2 * stride], y3 = w2[t + 3 * stride];
+        acc0 += x0.x * y0.x + x0.y * y0.y;
+        acc1 += x1.x * y1.x + x1.y * y1.y;
+        acc2 += x2.x * y2.x + x2.y * y2.y;
+        acc3 += x3.x * y3.x + x3.y * y3.y;
     }
+    for (; t < n2; t += stride) { const double2 x0 = a2[t], y0 = w2[t]; acc0 += x0.x * y0.x + x0.y * y0.y; }
+    double acc[1] = {(acc0 + acc1) + (acc2 + acc3)};
+    // block partial -> partial[v * nbx + bx]
+    __shared__ double red[kThreads / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double sm = warp_sum(acc[0]);
+    if (lane == 0) red[wid] = sm;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tt = 0;
+        for (int q = 0; q < (int)(blockDim.x / 32); ++q) tt += red[q];
+        partial[(int64_t)v * nbx + blockIdx.x] = tt;
+    }
+    // last block over the whole grid reduces every vector's partials
+    __shared__ bool amlast;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned int total = gridDim.x * gridDim.y;
+        amlast = (atomicAdd(counter, 1u) == total - 1);
+    }
+    __syncthreads();
+    if (!amlast) return;
+    __threadfence();
     __shared__ double res[kMaxDots];
-    if (last_block_reduce(partial, nv, nblocks, counter, res)) {
-        if (threadIdx.x == 0) {
-            for (int v = 0; v < k; ++v) ks->dots[v] = ks->scale[v] * res[v];
-            if (cond) {
-                for (int v = 0; v < k; ++v) ks->H[ks->k][v] += ks->dots[v];
-            } else {
-                for (int v = 0; v < k; ++v) ks->H[ks->k][v] = ks->dots[v];
-                ks->w0 = res[k];
-            }
+    const int nv = k + 1, nw = blockDim.x >> 5;
+    for (int u = wid; u < nv; u += nw) {
+        const double* pv = partial + (int64_t)u * nbx;
+        double s = 0;
+        int b = lane;
+        for (; b + 7 * 32 < nbx; b += 8 * 32) {
+            double q[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) q[e] = __ldcg(pv + b + e * 32);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) s += q[e];
+        }
+        for (; b < nbx; b += 32) s += __ldcg(pv + b);
+        s = warp_sum(s);
+        if (lane == 0) res[u] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *counter = 0u;
+        for (int u = 0; u < k; ++u) ks->dots[u] = ks->scale[u] * res[u];
+        if (cond) {
+            for (int u = 0; u < k; ++u) ks->H[ks->k][u] += ks->dots[u];
+        } else {
+            for (int u = 0; u < k; ++u) ks->H[ks->k][u] = ks->dots[u];
+            ks->w0 = res[k];
         }
     }
 }
 
 // w -= sum_v dots[v] * scale[v] * V_v ; |w|^2 -> ks->w1, and decide re-orthogonalisation.
+// The last block also finishes the Arnoldi step (Hessenberg column, Givens
+// rotation, stopping test) once no second Gram-Schmidt pass follows.
 __global__ void __launch_bounds__(kThreads) k_project(const double* __restrict__ V, int64_t ldv, int k,
                                                       double* __restrict__ w, int64_t n,
                                                       double* partial, unsigned int* counter, int nblocks,
-                                                      KrylovState* ks, int cond) {
+                                                      KrylovState* ks, int cond, int maxmv, int m) {
     if (cond && !ks->reorth) return;
     if (ks->done) return;
     __shared__ double coef[kMaxDots];
     for (int v = threadIdx.x; v < k; v += blockDim.x) coef[v] = ks->dots[v] * ks->scale[v];
     __syncthreads();
     double acc[1] = {0.0};
+    const int64_t n2 = (n + 1) / 2;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += stride) {
-        double a = w[t];
-#pragma unroll 4
-        for (int v = 0; v < k; ++v) a -= coef[v] * V[(int64_t)v * ldv + t];
-        w[t] = a;
-        acc[0] += a * a;
+    double2* w2 = reinterpret_cast<double2*>(w);
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n2; t += stride) {
+        double2 a = w2[t];
+        for (int v0 = 0; v0 < k; v0 += 8) {
+            double2 vv[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (v0 + u < k) vv[u] = __ldcs(reinterpret_cast<const double2*>(V + (int64_t)(v0 + u) * ldv) + t);
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (v0 + u < k) { a.x -= coef[v0 + u] * vv[u].x; a.y -= coef[v0 + u] * vv[u].y; }
+        }
+        w2[t] = a;
+        acc[0] += a.x * a.x + a.y * a.y;
     }
     block_store_partials(acc, 1, partial, nblocks);
     __shared__ double res[1];
@@ -149,6 +233,7 @@ __global__ void __launch_bounds__(kThreads) k_project(const double* __restrict__
             // Daniel-Gragg-Kaufman-Stewart test: re-orthogonalise once when the
             // projection removed more than half of |w|^2.
             ks->reorth = (!cond && res[0] < 0.5 * ks->w0) ? 1 : 0;
+            if (!ks->reorth) arnoldi_finish_dev(ks, maxmv, m);
         }
     }
 }
@@ -177,38 +262,6 @@ __global__ void __launch_bounds__(kThreads) k_norm_init(const double* __restrict
             if (beta <= ks->tol) { ks->done = 1; ks->converged = 1; }
         }
     }
-}
-
-// One thread: finish Arnoldi step k (1-based after increment).
-__global__ void k_arnoldi_finish(KrylovState* ks, int maxmv, int m) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    if (ks->done) return;
-    const int k = ks->k + 1;           // this step's column index is ks->k (0-based)
-    double* hc = ks->H[ks->k];
-    const double nrm = sqrt(ks->w1);
-    hc[k] = nrm;
-    ks->scale[k] = nrm > 0 ? 1.0 / nrm : 0.0;
-    for (int i = 0; i < k - 1; ++i) {
-        const double a0 = hc[i];
-        hc[i] = ks->cs[i] * a0 + ks->sn[i] * hc[i + 1];
-        hc[i + 1] = ks->cs[i] * hc[i + 1] - ks->sn[i] * a0;
-    }
-    double x = hc[k - 1], yv = hc[k];
-    const double r = sqrt(x * x + yv * yv);
-    double c = 1.0, s = 0.0;
-    if (r != 0.0) { c = x / r; s = yv / r; }
-    hc[k - 1] = r; hc[k] = 0.0;
-    ks->cs[k - 1] = c; ks->sn[k - 1] = s;
-    const double al = -s * ks->g[k - 1];
-    ks->g[k - 1] = c * ks->g[k - 1];
-    ks->g[k] = al;
-    ks->resid = fabs(al);
-    ks->k = k;
-    ks->iters += 1;
-    ks->reorth = 0;
-    const bool conv = ks->resid <= ks->tol;
-    if (conv) ks->converged = 1;
-    if (conv || k >= m || ks->iters >= maxmv || nrm == 0.0) ks->done = 1;
 }
 
 // Upper-triangular solve H y = g for the current k (1 thread).
@@ -252,12 +305,18 @@ __global__ void k_krylov_reset(KrylovState* ks) {
 
 void launch_multidot(const double* V, int64_t ldv, int k, const double* w, int64_t n, const DotScratch& sc,
                      KrylovState* ks, int cond, cudaStream_t st) {
-    k_multidot<<<sc.nblocks, kThreads, 0, st>>>(V, ldv, k, w, n, sc.partial, sc.counter, sc.nblocks, ks, cond);
+    // about 8 blocks per SM in total, split over the k+1 products
+    int nbx = (148 * 8 + k) / (k + 1);
+    const int64_t need = ((n + 1) / 2 + kThreads - 1) / kThreads;
+    if (nbx > need) nbx = (int)need;
+    if (nbx < 1) nbx = 1;
+    if (nbx > sc.nblocks) nbx = sc.nblocks;
+    k_multidot<<<dim3(nbx, k + 1), kThreads, 0, st>>>(V, ldv, k, w, n, sc.partial, sc.counter, nbx, ks, cond);
 }
 
 void launch_project(const double* V, int64_t ldv, int k, double* w, int64_t n, const DotScratch& sc, KrylovState* ks,
-                    int cond, cudaStream_t st) {
-    k_project<<<sc.nblocks, kThreads, 0, st>>>(V, ldv, k, w, n, sc.partial, sc.counter, sc.nblocks, ks, cond);
+                    int cond, int maxmv, int m, cudaStream_t st) {
+    k_project<<<sc.nblocks, kThreads, 0, st>>>(V, ldv, k, w, n, sc.partial, sc.counter, sc.nblocks, ks, cond, maxmv, m);
 }
 
 void launch_arnoldi_finish(KrylovState* ks, int maxmv, int m, cudaStream_t st) {

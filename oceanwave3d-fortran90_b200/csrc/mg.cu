@@ -16,160 +16,30 @@
 //                   column (k = 2..Nzg, free surface row last)
 // sequence per smoothing step as MultiGridSolver.f90:118-126,174-181:
 //   special; [colours; special] x nu
+//
+// Levels with few points run inside one cooperative kernel (k_mg_coarse_cycle)
+// that executes the phases of every coarse level back to back with grid-wide
+// barriers, instead of one launch per phase.
 #include "ow3d_internal.h"
+#include "mg_device.cuh"
+#include <cooperative_groups.h>
 #include <vector>
 
 namespace ow3d {
 
 namespace {
+using namespace mgdev;
+namespace cg = cooperative_groups;
 
-template <typename T>
-__device__ __forceinline__ int64_t IX(const LevelDev<T>& L, int k, int i, int j) {
-    return (int64_t)(k - 1) + (int64_t)L.Nzg * ((int64_t)(i - 1) + (int64_t)L.Nxg * (j - 1));
-}
-template <typename T>
-__device__ __forceinline__ T sx(const LevelDev<T>& L, int o, int i, int m) { return L.SX[((o - 1) * L.Nxg + (i - 1)) * 3 + m]; }
-template <typename T>
-__device__ __forceinline__ T sy(const LevelDev<T>& L, int o, int j, int m) { return L.SY[((o - 1) * L.Nyg + (j - 1)) * 3 + m]; }
-template <typename T>
-__device__ __forceinline__ T sz(const LevelDev<T>& L, int o, int k, int m) { return L.SZ[((o - 1) * L.Nzg + (k - 1)) * 3 + m]; }
+#define OW3D_GRID_STRIDE(var, n) \
+    for (int64_t var = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; var < (n); var += (int64_t)gridDim.x * blockDim.x)
 
-// Interior row (2 <= k <= Nzg-1, interior column). Returns A x at the row and
-// the diagonal coefficient.
-template <typename T, bool THREE>
-__device__ T lo_interior(const LevelDev<T>& L, const T* x, int k, int i, int j, T& diag) {
-    const int64_t c = (int64_t)(i - 1) + (int64_t)L.Nxg * (j - 1);
-    const T h = L.h[c], hx = L.hx[c], hxx = L.hxx[c];
-    const T hy = THREE ? L.hy[c] : T(0), hyy = THREE ? L.hyy[c] : T(0);
-    const T sg = L.zs[k - 1], om = T(1) - sg;
-    const T d = h;
-    // DetermineTransformationConstantsArray with eta = 0
-    const T s2 = (om * hx) / d;
-    const T s4 = (om * hy) / d;
-    const T s5 = T(1) / d;
-    const T s3 = -T(2) * om * (hx * hx + hy * hy) / (d * d) + om * (hxx + hyy) / d;
-    const T cz = s2 * s2 + s4 * s4 + s5 * s5;
-    T acc = 0;
-    // d2/dx2, d2/dy2 (centred 3-point, PrepareFullOperatorStencils.f90:213-231)
-#pragma unroll
-    for (int m = 0; m < 3; ++m) acc += sx(L, 2, i, m) * x[IX(L, k, i - 1 + m, j)];
-    if (THREE) {
-#pragma unroll
-        for (int m = 0; m < 3; ++m) acc += sy(L, 2, j, m) * x[IX(L, k, i, j - 1 + m)];
-    }
-    T dz = 0, dzz = 0;
-#pragma unroll
-    for (int m = 0; m < 3; ++m) {
-        const T v = x[IX(L, k - 1 + m, i, j)];
-        dz += sz(L, 1, k, m) * v;
-        dzz += sz(L, 2, k, m) * v;
-    }
-    acc += s3 * dz + cz * dzz;
-    diag = sx(L, 2, i, 1) + (THREE ? sy(L, 2, j, 1) : T(0)) + s3 * sz(L, 1, k, 1) + cz * sz(L, 2, k, 1);
-    // mixed d2/dxds: sum over y-planes J of Dz(Dx x), the x stencil at level 1
-    // shifted away from the ghost corner columns.
-    if (s2 != T(0)) {
-        T xz = 0;
-        const int jlo = THREE ? j - 1 : j, jhi = THREE ? j + 1 : j;
-        for (int jj = jlo; jj <= jhi; ++jj) {
-#pragma unroll
-            for (int kk = 0; kk < 3; ++kk) {
-                const int kz = k - 1 + kk;
-                int sh = 0;
-                if (kz == 1) { if (i - 1 == 1) sh = 1; if (i + 1 == L.Nxg) sh = -1; }
-                T dx = 0;
-#pragma unroll
-                for (int m = 0; m < 3; ++m) dx += sx(L, 1, i - sh, m) * x[IX(L, kz, i - 1 + sh + m, jj)];
-                xz += sz(L, 1, k, kk) * dx;
-            }
-        }
-        acc += T(2) * s2 * xz;
-        diag += T(2) * s2 * (sz(L, 1, k, 1) * sx(L, 1, i, 1));
-    }
-    if (THREE && s4 != T(0)) {
-        T yz = 0;
-        for (int ii = i - 1; ii <= i + 1; ++ii) {
-#pragma unroll
-            for (int kk = 0; kk < 3; ++kk) {
-                const int kz = k - 1 + kk;
-                int sh = 0;
-                if (kz == 1) { if (j - 1 == 1) sh = 1; if (j + 1 == L.Nyg) sh = -1; }
-                T dy = 0;
-#pragma unroll
-                for (int m = 0; m < 3; ++m) dy += sy(L, 1, j - sh, m) * x[IX(L, kz, ii, j - 1 + sh + m)];
-                yz += sz(L, 1, k, kk) * dy;
-            }
-        }
-        acc += T(2) * s4 * yz;
-        diag += T(2) * s4 * (sz(L, 1, k, 1) * sy(L, 1, j, 1));
-    }
-    return acc;
-}
+// Points per level below which the level runs in the fused coarse kernel.
+constexpr int64_t kCoopMaxPoints = 160000;
 
-// Bottom row (k = 1, interior column), BuildLinearSystemMatrix.f90:50-70.
-template <typename T, bool THREE>
-__device__ T lo_bottom(const LevelDev<T>& L, const T* x, int i, int j, T& diag) {
-    const int64_t c = (int64_t)(i - 1) + (int64_t)L.Nxg * (j - 1);
-    const T h = L.h[c], hx = L.hx[c];
-    const T hy = THREE ? L.hy[c] : T(0);
-    const T om = T(1) - L.zs[1];
-    const T s2 = (om * hx) / h, s4 = (om * hy) / h, s5 = T(1) / h;
-    const T f = THREE ? (s5 + hx * s2 + hy * s4) : (s5 + hx * s2);
-    T dz = 0;
-#pragma unroll
-    for (int m = 0; m < 3; ++m) dz += sz(L, 1, 2, m) * x[IX(L, 1 + m, i, j)];
-    T dx = 0;
-#pragma unroll
-    for (int m = 0; m < 3; ++m) dx += sx(L, 1, i, m) * x[IX(L, 2, i - 1 + m, j)];
-    T acc = f * dz + hx * dx;
-    if (THREE) {
-        T dy = 0;
-#pragma unroll
-        for (int m = 0; m < 3; ++m) dy += sy(L, 1, j, m) * x[IX(L, 2, i, j - 1 + m)];
-        acc += hy * dy;
-    }
-    diag = f * sz(L, 1, 2, 0);
-    return acc;
-}
-
-// Ghost-column row (lateral Neumann or identity).
-template <typename T, bool THREE>
-__device__ T lo_ghost(const LevelDev<T>& L, const T* x, int k, int i, int j, T& diag) {
-    const bool gxx = (i == 1 || i == L.Nxg), gyy = THREE && (j == 1 || j == L.Nyg);
-    if ((gxx && gyy) || k == 1) { diag = T(1); return x[IX(L, k, i, j)]; }
-    T acc = 0;
-    if (gxx) {
-        const int ia = (i == 1) ? 2 : L.Nxg - 1;
-#pragma unroll
-        for (int m = 0; m < 3; ++m) acc += sx(L, 1, ia, m) * x[IX(L, k, ia - 1 + m, j)];
-        diag = sx(L, 1, ia, (i == 1) ? 0 : 2);
-    } else {
-        const int ja = (j == 1) ? 2 : L.Nyg - 1;
-#pragma unroll
-        for (int m = 0; m < 3; ++m) acc += sy(L, 1, ja, m) * x[IX(L, k, i, ja - 1 + m)];
-        diag = sy(L, 1, ja, (j == 1) ? 0 : 2);
-    }
-    return acc;
-}
-
-template <typename T, bool THREE>
-__device__ __forceinline__ bool is_ghost_col(const LevelDev<T>& L, int i, int j) {
-    return i == 1 || i == L.Nxg || (THREE && (j == 1 || j == L.Nyg));
-}
-
-template <typename T, bool THREE>
-__device__ T lo_row(const LevelDev<T>& L, const T* x, int k, int i, int j, T& diag) {
-    if (is_ghost_col<T, THREE>(L, i, j)) return lo_ghost<T, THREE>(L, x, k, i, j, diag);
-    if (k == L.Nzg) { diag = T(1); return x[IX(L, k, i, j)]; }
-    if (k == 1) return lo_bottom<T, THREE>(L, x, i, j, diag);
-    return lo_interior<T, THREE>(L, x, k, i, j, diag);
-}
-
-// ------------------------------------------------------------- kernels
 template <typename T, bool THREE>
 __global__ void k_lo_matvec(LevelDev<T> L, const T* __restrict__ x, T* __restrict__ y) {
-    const int64_t n = L.N;
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+    OW3D_GRID_STRIDE(p, L.N) {
         const int k = (int)(p % L.Nzg) + 1;
         const int64_t c = p / L.Nzg;
         const int i = (int)(c % L.Nxg) + 1, j = (int)(c / L.Nxg) + 1;
@@ -178,287 +48,124 @@ __global__ void k_lo_matvec(LevelDev<T> L, const T* __restrict__ x, T* __restric
     }
 }
 
-// r = b - A x
 template <typename T, bool THREE>
 __global__ void k_lo_residual(LevelDev<T> L) {
-    const int64_t n = L.N;
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
-        const int k = (int)(p % L.Nzg) + 1;
-        const int64_t c = p / L.Nzg;
-        const int i = (int)(c % L.Nxg) + 1, j = (int)(c / L.Nxg) + 1;
-        T dg;
-        L.rv[p] = L.bv[p] - lo_row<T, THREE>(L, L.xv, k, i, j, dg);
-    }
+    OW3D_GRID_STRIDE(p, L.N) residual_item<T, THREE>(L, p);
 }
 
-// Special pass, part 1: every row of the ghost columns (lateral Neumann rows
-// and identity rows). These rows only read interior-column values, so the
-// columns update independently.
 template <typename T, bool THREE>
-__global__ void k_lo_special_ghost(LevelDev<T> L) {
-    // ghost columns enumerated along the perimeter: west/east (all j), then
-    // south/north (interior i) in 3-D
-    const int Nxg = L.Nxg, Nyg = L.Nyg;
-    const int64_t nper = THREE ? (int64_t)2 * Nyg + 2 * (Nxg - 2) : 2;
-    const int64_t total = nper * L.Nzg;
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
-        const int k = (int)(q % L.Nzg) + 1;
-        const int64_t e = q / L.Nzg;
-        int i, j;
-        if (!THREE) { i = (e == 0) ? 1 : Nxg; j = 1; }
-        else if (e < 2 * Nyg) { i = (e % 2 == 0) ? 1 : Nxg; j = (int)(e / 2) + 1; }
-        else { const int64_t f = e - 2 * Nyg; j = (f % 2 == 0) ? 1 : Nyg; i = (int)(f / 2) + 2; }
-        T dg;
-        const T a = lo_ghost<T, THREE>(L, L.xv, k, i, j, dg);
-        const int64_t p = IX(L, k, i, j);
-        L.xv[p] = L.xv[p] + (L.bv[p] - a) / dg;
-    }
+__global__ void k_lo_special(LevelDev<T> L) {
+    OW3D_GRID_STRIDE(q, (special_count<T, THREE>(L))) special_item<T, THREE>(L, q);
 }
 
-// Special pass, part 2: bottom rows of the interior columns (they read the
-// ghost-column values part 1 produced, and no other bottom row).
-template <typename T, bool THREE>
-__global__ void k_lo_special_bottom(LevelDev<T> L) {
-    const int64_t C = (int64_t)L.Nxg * L.Nyg;
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < C; c += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(c % L.Nxg) + 1, j = (int)(c / L.Nxg) + 1;
-        if (is_ghost_col<T, THREE>(L, i, j)) continue;
-        T dg;
-        const T a = lo_bottom<T, THREE>(L, L.xv, i, j, dg);
-        const int64_t p = IX(L, 1, i, j);
-        L.xv[p] = L.xv[p] + (L.bv[p] - a) / dg;
-    }
-}
-
-// Read-only load: the neighbour columns a colour phase reads belong to other
-// colours and are not written during the phase.
-template <typename T>
-__device__ __forceinline__ T ro(const T* p) { return __ldg(p); }
-
-// Colour phase: Gauss-Seidel up the interior rows k = 2..Nzg-1 of every
-// interior column of this colour, then the free-surface row. The column's own
-// unknowns stay in registers (NZ > 0: compile-time Nzg); rows 1 and Nzg of the
-// column are constant during the sweep.
-template <typename T, bool THREE, int NZ>
+template <typename T, bool THREE, int S, bool CROSS>
 __global__ void __launch_bounds__(128) k_lo_colour(LevelDev<T> L, int colour) {
-    constexpr int ZM = NZ > 0 ? NZ : kMaxNzg;
-    const int Nzg = NZ > 0 ? NZ : L.Nzg;
-    const int Nxg = L.Nxg, Nyg = L.Nyg;
-    const int nxi = Nxg - 2, nyi = THREE ? Nyg - 2 : 1;
-    const int64_t total = (int64_t)nxi * nyi;
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(q % nxi) + 2, j = THREE ? (int)(q / nxi) + 2 : 1;
-        const int col = (L.ncolor == 4) ? ((i & 1) + 2 * (j & 1)) : ((i + j) & 1);
-        if (col != colour) continue;
-        const int64_t c = (int64_t)(i - 1) + (int64_t)Nxg * (j - 1);
-        T* xc = L.xv + c * Nzg;
-        const T* bc = L.bv + c * Nzg;
-        const T h = L.h[c], hx = L.hx[c], hxx = L.hxx[c];
-        const T hy = THREE ? L.hy[c] : T(0), hyy = THREE ? L.hyy[c] : T(0);
-        const bool cross = (hx != T(0)) || (hy != T(0));
-        T xo[ZM];
-#pragma unroll
-        for (int k = 0; k < ZM; ++k) if (NZ > 0 || k < Nzg) xo[k] = xc[k];
-        const T* xw = L.xv + (c - 1) * Nzg;           // west column
-        const T* xe = L.xv + (c + 1) * Nzg;           // east column
-        const T* xs = THREE ? L.xv + (c - Nxg) * Nzg : xc;  // south
-        const T* xn = THREE ? L.xv + (c + Nxg) * Nzg : xc;  // north
-        const T sxx0 = sx(L, 2, i, 0), sxx1 = sx(L, 2, i, 1), sxx2 = sx(L, 2, i, 2);
-        const T syy0 = THREE ? sy(L, 2, j, 0) : T(0), syy1 = THREE ? sy(L, 2, j, 1) : T(0), syy2 = THREE ? sy(L, 2, j, 2) : T(0);
-        const T sx1c = sx(L, 1, i, 1), sy1c = THREE ? sy(L, 1, j, 1) : T(0);
-#pragma unroll
-        for (int k = 2; k < ZM; ++k) {
-            if (k >= Nzg) break;
-            const T sg = L.zs[k - 1], om = T(1) - sg;
-            const T s2 = (om * hx) / h, s4 = (om * hy) / h, s5 = T(1) / h;
-            const T s3 = -T(2) * om * (hx * hx + hy * hy) / (h * h) + om * (hxx + hyy) / h;
-            const T cz = s2 * s2 + s4 * s4 + s5 * s5;
-            const T z0 = sz(L, 1, k, 0), z1 = sz(L, 1, k, 1), z2 = sz(L, 1, k, 2);
-            const T zz0 = sz(L, 2, k, 0), zz1 = sz(L, 2, k, 1), zz2 = sz(L, 2, k, 2);
-            // off-column part of the row (constant during this phase)
-            T off = sxx0 * ro(xw + k - 1) + sxx2 * ro(xe + k - 1);
-            if (THREE) off += syy0 * ro(xs + k - 1) + syy2 * ro(xn + k - 1);
-            T diag = sxx1 + syy1 + s3 * z1 + cz * zz1;
-            T lo = s3 * z0 + cz * zz0, up = s3 * z2 + cz * zz2;
-            if (cross && s2 != T(0)) {
-                const int jlo = THREE ? j - 1 : j, jhi = THREE ? j + 1 : j;
-                T xz = 0;
-                for (int jj = jlo; jj <= jhi; ++jj) {
-#pragma unroll
-                    for (int kk = 0; kk < 3; ++kk) {
-                        const int kz = k - 1 + kk;
-                        int sh = 0;
-                        if (kz == 1) { if (i - 1 == 1) sh = 1; if (i + 1 == Nxg) sh = -1; }
-                        T dx = 0;
-#pragma unroll
-                        for (int m = 0; m < 3; ++m) {
-                            const int ii = i - 1 + sh + m;
-                            const T w = sx(L, 1, i - sh, m);
-                            if (ii == i && jj == j && kz >= 2 && kz <= Nzg - 1) {
-                                // own-column unknown: goes into the tridiagonal part
-                                const T cf = T(2) * s2 * sz(L, 1, k, kk) * w;
-                                if (kk == 0) lo += cf; else if (kk == 1) diag += cf; else up += cf;
-                            } else {
-                                const T* src = L.xv + ((int64_t)(ii - 1) + (int64_t)Nxg * (jj - 1)) * Nzg + (kz - 1);
-                                dx += w * ((ii == i && jj == j) ? *src : ro(src));
-                            }
-                        }
-                        xz += sz(L, 1, k, kk) * dx;
-                    }
-                }
-                off += T(2) * s2 * xz;
-            }
-            if (THREE && cross && s4 != T(0)) {
-                T yz = 0;
-                for (int ii = i - 1; ii <= i + 1; ++ii) {
-#pragma unroll
-                    for (int kk = 0; kk < 3; ++kk) {
-                        const int kz = k - 1 + kk;
-                        int sh = 0;
-                        if (kz == 1) { if (j - 1 == 1) sh = 1; if (j + 1 == Nyg) sh = -1; }
-                        T dy = 0;
-#pragma unroll
-                        for (int m = 0; m < 3; ++m) {
-                            const int jj = j - 1 + sh + m;
-                            const T w = sy(L, 1, j - sh, m);
-                            if (ii == i && jj == j && kz >= 2 && kz <= Nzg - 1) {
-                                const T cf = T(2) * s4 * sz(L, 1, k, kk) * w;
-                                if (kk == 0) lo += cf; else if (kk == 1) diag += cf; else up += cf;
-                            } else {
-                                const T* src = L.xv + ((int64_t)(ii - 1) + (int64_t)Nxg * (jj - 1)) * Nzg + (kz - 1);
-                                dy += w * ((ii == i && jj == j) ? *src : ro(src));
-                            }
-                        }
-                        yz += sz(L, 1, k, kk) * dy;
-                    }
-                }
-                off += T(2) * s4 * yz;
-            }
-            (void)sx1c; (void)sy1c;
-            // row residual with the current iterate: lower neighbour already updated
-            const T xm = xo[k - 2], x0 = xo[k - 1], xp = xo[k];
-            const T a = lo * xm + diag * x0 + up * xp + off;
-            xo[k - 1] = x0 + (bc[k - 1] - a) / diag;
-        }
-        xo[Nzg - 1] = bc[Nzg - 1];
-#pragma unroll
-        for (int k = 1; k < ZM; ++k) if (k < Nzg) xc[k] = xo[k];
-    }
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t total = colour_count<T, THREE>(L);
+    for (int64_t base = warp * (32 / S); base < total; base += nwarps * (32 / S))
+        colour_warp<T, THREE, S, CROSS>(L, colour, base);
 }
 
-// MGRestriction3DExplicit.f90:19-128 as a gather per coarse point.
 template <typename T>
 __global__ void k_restrict(LevelDev<T> F, LevelDev<T> Cc, const T* __restrict__ rf, T* __restrict__ rc, T* __restrict__ xc) {
-    const int64_t n = Cc.N;
-    const int gy = (F.Nyg > 1) ? 1 : 0;
-    const int Nzf = F.Nzg - 1, Nyf = F.Nyg - 2 * gy;
-    const int xcz = Cc.xc, ycz = Cc.yc, zcz = Cc.zc;
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
-        const int kc = (int)(p % Cc.Nzg) + 1;
-        const int64_t cc = p / Cc.Nzg;
-        const int ic = (int)(cc % Cc.Nxg) + 1, jc = (int)(cc / Cc.Nxg) + 1;
-        xc[p] = T(0);
-        const bool ghost = kc == 1 || ic == 1 || ic == Cc.Nxg || (gy && (jc == 1 || jc == Cc.Nyg));
-        if (ghost) { rc[p] = T(0); continue; }
-        const int kf = 2 + (kc - 2) * (1 + zcz), ifn = 2 + (ic - 2) * (1 + xcz), jf = gy ? 2 + (jc - 2) * (1 + ycz) : 1;
-        auto R = [&](int k, int i, int j) -> T { return rf[IX(F, k, i, j)]; };
-        if (kf == F.Nzg) { rc[p] = R(kf, ifn, jf); continue; }
-        // x-weighted value at (k, ifn, j) (raw on ghost rows and outside 2..Nzf)
-        auto Sx = [&](int k, int j) -> T {
-            if (!xcz || k < 2 || k > Nzf || (gy && (j < 2 || j > Nyf + 1))) return R(k, ifn, j);
-            const double dW = F.x[ifn - 1] - F.x[ifn - 2], dE = F.x[ifn] - F.x[ifn - 1];
-            const T dxc = T(1.0 / (dW + dE));
-            return (T(0.5) * dxc) * (T(dW) * R(k, ifn - 1, j) + T(dW + dE) * R(k, ifn, j) + T(dE) * R(k, ifn + 1, j));
-        };
-        auto Sxy = [&](int k) -> T {
-            if (!ycz || k < 2 || k > Nzf) return Sx(k, jf);
-            const double dS = F.y[jf - 1] - F.y[jf - 2], dN = F.y[jf] - F.y[jf - 1];
-            const T dyc = T(1.0 / (dS + dN));
-            return (T(0.5) * dyc) * (T(dS) * Sx(k, jf - 1) + T(dN + dS) * Sx(k, jf) + T(dN) * Sx(k, jf + 1));
-        };
-        T v;
-        if (zcz) {
-            const double dU = F.z[kf] - F.z[kf - 1], dD = F.z[kf - 1] - F.z[kf - 2];
-            const T dzc = T(1.0 / (dD + dU));
-            v = (T(0.5) * dzc) * (T(dD) * Sxy(kf - 1) + T(dU) * Sxy(kf + 1)) + T(0.5) * Sxy(kf);
-        } else {
-            v = Sxy(kf);
-        }
-        rc[p] = v;
-    }
+    OW3D_GRID_STRIDE(p, Cc.N) restrict_item<T>(F, Cc, rf, rc, xc, p);
 }
 
-// MGProlongation3DExplicit.f90:19-110 as a gather per fine point, added to xf.
 template <typename T>
 __global__ void k_prolong_add(LevelDev<T> F, LevelDev<T> Cc, const T* __restrict__ xc, T* __restrict__ xf) {
-    const int64_t n = F.N;
-    const int gy = (F.Nyg > 1) ? 1 : 0;
-    const int XF = Cc.xc ? 2 : 1, YF = Cc.yc ? 2 : 1, ZF = Cc.zc ? 2 : 1;
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
-        const int kf = (int)(p % F.Nzg) + 1;
-        const int64_t cf = p / F.Nzg;
-        const int ifn = (int)(cf % F.Nxg) + 1, jf = (int)(cf / F.Nxg) + 1;
-        if (kf == 1 || kf == F.Nzg || ifn == 1 || ifn == F.Nxg || (gy && (jf == 1 || jf == F.Nyg))) continue;
-        // coarse value at coincident fine indices
-        auto Cv = [&](int k, int i, int j) -> T {
-            if (k == F.Nzg) return T(0);  // free-surface layer is not injected
-            const int kc = 2 + (k - 2) / ZF, ic = 2 + (i - 2) / XF, jc = gy ? 2 + (j - 2) / YF : 1;
-            return xc[IX(Cc, kc, ic, jc)];
-        };
-        auto Px = [&](int k, int j) -> T {
-            if (k == F.Nzg) return T(0);
-            if (XF == 1 || ((ifn - 2) % 2) == 0) return Cv(k, ifn, j);
-            const double dW = F.x[ifn - 1] - F.x[ifn - 2], dE = F.x[ifn] - F.x[ifn - 1];
-            const T dxf = T(1.0 / (dW + dE));
-            return (T(dE) * Cv(k, ifn - 1, j) + T(dW) * Cv(k, ifn + 1, j)) * dxf;
-        };
-        auto Py = [&](int k) -> T {
-            if (k == F.Nzg) return T(0);
-            if (!gy || YF == 1 || ((jf - 2) % 2) == 0) return Px(k, jf);
-            const double dS = F.y[jf - 1] - F.y[jf - 2], dN = F.y[jf] - F.y[jf - 1];
-            const T dyf = T(1.0 / (dS + dN));
-            return (T(dN) * Px(k, jf - 1) + T(dS) * Px(k, jf + 1)) * dyf;
-        };
-        T v;
-        if (ZF == 1 || ((kf - 2) % 2) == 0) v = Py(kf);
-        else {
-            const double dD = F.z[kf - 1] - F.z[kf - 2], dU = F.z[kf] - F.z[kf - 1];
-            const T dzf = T(1.0 / (dD + dU));
-            v = (T(dU) * Py(kf - 1) + T(dD) * Py(kf + 1)) * dzf;
-        }
-        xf[p] += v;
-    }
+    OW3D_GRID_STRIDE(p, F.N) prolong_item<T>(F, Cc, xc, xf, p);
 }
 
 // Coarsest level: x = A^{-1} b with the explicit inverse (the reference factors
 // this matrix with HSL MA41 once, LUfactor.f90:20-66, and solves with it).
 template <typename T>
 __global__ void k_coarse(int n, const T* __restrict__ inv, const T* __restrict__ b, T* __restrict__ x) {
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-        T acc = 0;
-        for (int c = 0; c < n; ++c) acc += inv[(int64_t)r * n + c] * b[c];
-        x[r] = acc;
-    }
+    OW3D_GRID_STRIDE(r, n) coarse_item<T>(n, inv, b, x, (int)r);
 }
 
 template <typename T>
 __global__ void k_scale_copy(const double* __restrict__ src, double s, T* __restrict__ dst, int64_t n) {
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
-        dst[p] = T(s * src[p]);
+    OW3D_GRID_STRIDE(p, n) dst[p] = T(s * src[p]);
 }
 template <typename T>
 __global__ void k_scale_copy_dev(const double* __restrict__ src, const double* __restrict__ ds, T* __restrict__ dst, int64_t n) {
     const double s = ds ? *ds : 1.0;
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
-        dst[p] = T(s * src[p]);
+    OW3D_GRID_STRIDE(p, n) dst[p] = T(s * src[p]);
 }
 __global__ void k_convert(const float* __restrict__ src, double* __restrict__ dst, int64_t n) {
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
-        dst[p] = (double)src[p];
+    OW3D_GRID_STRIDE(p, n) dst[p] = (double)src[p];
 }
 template <typename T>
 __global__ void k_fill(T* __restrict__ dst, T v, int64_t n) {
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) dst[p] = v;
+    OW3D_GRID_STRIDE(p, n) dst[p] = v;
+}
+
+// ------------------------------------------------- fused coarse levels
+template <typename T>
+struct LevelPack { LevelDev<T> l[kMaxLevels]; };
+
+inline int seg_width(int Nzg) {
+    const int R = Nzg - 2;
+    return R <= 2 ? 2 : (R <= 4 ? 4 : (R <= 8 ? 8 : (R <= 16 ? 16 : 32)));
+}
+
+template <typename T, bool THREE, int S, bool CROSS>
+__device__ void coop_colour_loop(const LevelDev<T>& L, int colour) {
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t total = colour_count<T, THREE>(L);
+    for (int64_t base = warp * (32 / S); base < total; base += nwarps * (32 / S))
+        colour_warp<T, THREE, S, CROSS>(L, colour, base);
+}
+
+template <typename T, bool THREE>
+__device__ void coop_colour(const LevelDev<T>& L, int colour) {
+    const int R = L.Nzg - 2;
+    const bool cr = L.cross != 0;
+#define OW3D_CC(SW) { if (cr) coop_colour_loop<T, THREE, SW, true>(L, colour); else coop_colour_loop<T, THREE, SW, false>(L, colour); }
+    if (R <= 2) OW3D_CC(2) else if (R <= 4) OW3D_CC(4) else if (R <= 8) OW3D_CC(8) else if (R <= 16) OW3D_CC(16) else OW3D_CC(32)
+#undef OW3D_CC
+}
+
+template <typename T, bool THREE>
+__device__ void coop_smooth(const LevelDev<T>& L, int nu, cg::grid_group& grid) {
+    OW3D_GRID_STRIDE(q, (special_count<T, THREE>(L))) special_item<T, THREE>(L, q);
+    grid.sync();
+    for (int s = 0; s < nu; ++s) {
+        for (int c = 0; c < L.ncolor; ++c) { coop_colour<T, THREE>(L, c); grid.sync(); }
+        OW3D_GRID_STRIDE(q, (special_count<T, THREE>(L))) special_item<T, THREE>(L, q);
+        grid.sync();
+    }
+}
+
+// V cycle over levels lc..0 (MultiGridSolver.f90:5-192) in one cooperative
+// launch. Level lc's right-hand side is set and its iterate zeroed on entry.
+template <typename T, bool THREE>
+__global__ void __launch_bounds__(256) k_mg_coarse_cycle(LevelPack<T> P, int lc, const T* __restrict__ inv, int nu1,
+                                                         int nu2) {
+    cg::grid_group grid = cg::this_grid();
+    for (int l = lc; l >= 1; --l) {
+        const LevelDev<T>& L = P.l[l];
+        const LevelDev<T>& Cc = P.l[l - 1];
+        coop_smooth<T, THREE>(L, nu1, grid);
+        OW3D_GRID_STRIDE(p, L.N) residual_item<T, THREE>(L, p);
+        grid.sync();
+        OW3D_GRID_STRIDE(p, Cc.N) restrict_item<T>(L, Cc, L.rv, Cc.bv, Cc.xv, p);
+        grid.sync();
+    }
+    {
+        const LevelDev<T>& L0 = P.l[0];
+        OW3D_GRID_STRIDE(r, L0.N) coarse_item<T>((int)L0.N, inv, L0.bv, L0.xv, (int)r);
+        grid.sync();
+    }
+    for (int l = 1; l <= lc; ++l) {
+        const LevelDev<T>& L = P.l[l];
+        const LevelDev<T>& Cc = P.l[l - 1];
+        OW3D_GRID_STRIDE(p, L.N) prolong_item<T>(L, Cc, Cc.xv, L.xv, p);
+        grid.sync();
+        coop_smooth<T, THREE>(L, nu2, grid);
+    }
 }
 
 inline int nblk(int64_t n, int t = 256) {
@@ -476,31 +183,29 @@ void launch_lo_matvec(const LevelDev<T>& L, const T* x, T* y, cudaStream_t st) {
 
 template <typename T>
 static void special(const LevelDev<T>& L, cudaStream_t st) {
-    const int64_t C = (int64_t)L.Nxg * L.Nyg;
-    const int64_t G = (L.Nyg > 1) ? ((int64_t)2 * L.Nyg + 2 * (L.Nxg - 2)) * L.Nzg : 2 * L.Nzg;
-    if (L.Nyg > 1) {
-        k_lo_special_ghost<T, true><<<nblk(G, 128), 128, 0, st>>>(L);
-        k_lo_special_bottom<T, true><<<nblk(C, 128), 128, 0, st>>>(L);
-    } else {
-        k_lo_special_ghost<T, false><<<nblk(G, 128), 128, 0, st>>>(L);
-        k_lo_special_bottom<T, false><<<nblk(C, 128), 128, 0, st>>>(L);
-    }
+    const int64_t n = (int64_t)L.Nxg * L.Nyg + ((L.Nyg > 1) ? ((int64_t)2 * L.Nyg + 2 * (L.Nxg - 2)) : 2) * L.Nzg;
+    if (L.Nyg > 1) k_lo_special<T, true><<<nblk(n, 128), 128, 0, st>>>(L);
+    else k_lo_special<T, false><<<nblk(n, 128), 128, 0, st>>>(L);
 }
-template <typename T, bool THREE, int NZ>
+
+template <typename T, bool THREE, int S>
 static void colour_launch(const LevelDev<T>& L, int c, cudaStream_t st) {
-    const int64_t C = (int64_t)(L.Nxg - 2) * (THREE ? L.Nyg - 2 : 1);
-    k_lo_colour<T, THREE, NZ><<<nblk(C, 128), 128, 0, st>>>(L, c);
+    const int64_t cols = (int64_t)((L.Nxg - 1) / 2) * (THREE ? L.Nyg - 2 : 1);
+    const int64_t warps = (cols + (32 / S) - 1) / (32 / S);
+    int64_t blocks = (warps * 32 + 127) / 128;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    if (blocks < 1) blocks = 1;
+    if (L.cross) k_lo_colour<T, THREE, S, true><<<(int)blocks, 128, 0, st>>>(L, c);
+    else k_lo_colour<T, THREE, S, false><<<(int)blocks, 128, 0, st>>>(L, c);
 }
 template <typename T, bool THREE>
 static void colour_dispatch(const LevelDev<T>& L, int c, cudaStream_t st) {
-    switch (L.Nzg) {
+    switch (seg_width(L.Nzg)) {
+        case 2: colour_launch<T, THREE, 2>(L, c, st); break;
         case 4: colour_launch<T, THREE, 4>(L, c, st); break;
-        case 6: colour_launch<T, THREE, 6>(L, c, st); break;
         case 8: colour_launch<T, THREE, 8>(L, c, st); break;
-        case 10: colour_launch<T, THREE, 10>(L, c, st); break;
-        case 14: colour_launch<T, THREE, 14>(L, c, st); break;
-        case 18: colour_launch<T, THREE, 18>(L, c, st); break;
-        default: colour_launch<T, THREE, 0>(L, c, st); break;
+        case 16: colour_launch<T, THREE, 16>(L, c, st); break;
+        default: colour_launch<T, THREE, 32>(L, c, st); break;
     }
 }
 template <typename T>
@@ -546,9 +251,38 @@ void launch_convert(const float* src, double* dst, int64_t n, cudaStream_t st) {
     k_convert<<<nblk(n), 256, 0, st>>>(src, dst, n);
 }
 
+// Launch the fused coarse cycle over levels lc..0 with a fully co-resident grid.
+template <typename T, bool THREE>
+static void coarse_cycle(const LevelDev<T>* lev, int lc, const T* inv, int nu1, int nu2, cudaStream_t st) {
+    static int grid = 0;
+    if (grid == 0) {
+        int dev = 0, nsm = 148, per = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_mg_coarse_cycle<T, THREE>, 256, 0);
+        grid = nsm * (per < 2 ? (per < 1 ? 1 : per) : 2);
+    }
+    LevelPack<T> P;
+    for (int l = 0; l <= lc; ++l) P.l[l] = lev[l];
+    void* args[] = {(void*)&P, (void*)&lc, (void*)&inv, (void*)&nu1, (void*)&nu2};
+    cudaLaunchCooperativeKernel((const void*)k_mg_coarse_cycle<T, THREE>, dim3(grid), dim3(256), args, 0, st);
+}
+
+template <typename T>
+static int coop_level(const LevelDev<T>* lev, int nlev) {
+    int lc = -1;
+    for (int l = 0; l < nlev; ++l) if (lev[l].N <= kCoopMaxPoints) lc = l;
+    return lc;
+}
+
 // MultiGridSolver.f90:5-192 (V cycle, gam = 1), levels lev[0] coarsest.
 template <typename T>
-static void vcycle(LevelDev<T>* lev, int l, const T* inv, int nu1, int nu2, cudaStream_t st) {
+static void vcycle(LevelDev<T>* lev, int l, int lc, const T* inv, int nu1, int nu2, cudaStream_t st) {
+    if (l <= lc) {
+        if (lev[0].Nyg > 1) coarse_cycle<T, true>(lev, l, inv, nu1, nu2, st);
+        else coarse_cycle<T, false>(lev, l, inv, nu1, nu2, st);
+        return;
+    }
     if (l == 0) { launch_coarse_solve(lev[0], inv, st); return; }
     const LevelDev<T>& F = lev[l];
     LevelDev<T>& Cc = lev[l - 1];
@@ -556,7 +290,7 @@ static void vcycle(LevelDev<T>* lev, int l, const T* inv, int nu1, int nu2, cuda
     if (F.Nyg > 1) k_lo_residual<T, true><<<nblk(F.N), 256, 0, st>>>(F);
     else k_lo_residual<T, false><<<nblk(F.N), 256, 0, st>>>(F);
     launch_restrict(F, Cc, (const T*)F.rv, Cc.bv, st);   // also zeroes Cc.xv
-    vcycle(lev, l - 1, inv, nu1, nu2, st);
+    vcycle(lev, l - 1, lc, inv, nu1, nu2, st);
     launch_prolong_add(F, Cc, (const T*)Cc.xv, F.xv, st);
     launch_lo_smooth(F, nu2, st);
 }
@@ -566,9 +300,10 @@ template <typename T>
 void launch_mg_vcycle(LevelDev<T>* lev, int nlev, const T* coarse_inv, int nu1, int nu2, int maxit, cudaStream_t st) {
     LevelDev<T>& F = lev[nlev - 1];
     launch_fill<T>(F.xv, T(0), F.N, st);
+    const int lc = (nlev > 1) ? coop_level(lev, nlev) : -1;
     for (int it = 1; it <= maxit; ++it) {
         if (nlev == 1 && it > 1) break;
-        vcycle(lev, nlev - 1, coarse_inv, nu1, nu2, st);
+        vcycle(lev, nlev - 1, lc, coarse_inv, nu1, nu2, st);
     }
 }
 

@@ -130,15 +130,26 @@ int build_levels(ow3d_handle* H, MgSet<T>& S, bool alloc_fine_x) {
         d.Nx = h.Nx; d.Ny = h.Ny; d.Nz = h.Nz; d.Nxg = h.Nxg; d.Nyg = h.Nyg; d.Nzg = h.Nzg;
         d.N = (int64_t)h.Nxg * h.Nyg * h.Nzg;
         d.ncolor = h.ncolor; d.xc = h.xc; d.yc = h.yc; d.zc = h.zc;
+        d.cross = 0;
+        for (size_t q = 0; q < h.hx.size(); ++q) if (h.hx[q] != 0.0 || h.hy[q] != 0.0) { d.cross = 1; break; }
         T *sx, *sy, *sz, *zs, *hh, *hx, *hxx, *hy, *hyy;
         TRY(upload(H, &sx, h.SX.w)); TRY(upload(H, &sy, h.SY.w.empty() ? std::vector<double>(1, 0.0) : h.SY.w));
         TRY(upload(H, &sz, h.SZ.w)); TRY(upload(H, &zs, h.zs));
         TRY(upload(H, &hh, h.h)); TRY(upload(H, &hx, h.hx)); TRY(upload(H, &hxx, h.hxx));
         TRY(upload(H, &hy, h.hy)); TRY(upload(H, &hyy, h.hyy));
         d.SX = sx; d.SY = sy; d.SZ = sz; d.zs = zs; d.h = hh; d.hx = hx; d.hxx = hxx; d.hy = hy; d.hyy = hyy;
-        double *x, *y, *z;
+        double *x, *y, *z, *ix, *iy, *iz;
         TRY(upload(H, &x, h.x)); TRY(upload(H, &y, h.y)); TRY(upload(H, &z, h.z));
         d.x = x; d.y = y; d.z = z;
+        // reciprocal of the two-sided spacing, 1/((c[i]-c[i-1]) + (c[i+1]-c[i])), the
+        // weight normaliser of MGRestriction3DExplicit.f90:55 / MGProlongation3DExplicit.f90:69
+        auto recip = [](const std::vector<double>& c) {
+            std::vector<double> r(c.size(), 0.0);
+            for (size_t q = 1; q + 1 < c.size(); ++q) r[q] = 1.0 / ((c[q] - c[q - 1]) + (c[q + 1] - c[q]));
+            return r;
+        };
+        TRY(upload(H, &ix, recip(h.x))); TRY(upload(H, &iy, recip(h.y))); TRY(upload(H, &iz, recip(h.z)));
+        d.ix = ix; d.iy = iy; d.iz = iz;
         T* r;
         TRY(dalloc(H, &r, d.N)); d.rv = r;
         if (l < L - 1) {
@@ -298,10 +309,9 @@ int solve_device(ow3d_handle* H, const double* rhs, double* phi, const Surface& 
                 precond_into(H, H->w, nullptr, Vn);
             }
             launch_multidot(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 0, H->st);
-            launch_project(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 0, H->st);
+            launch_project(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 0, maxmv, m, H->st);
             launch_multidot(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 1, H->st);
-            launch_project(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 1, H->st);
-            launch_arnoldi_finish(H->ks, maxmv, m, H->st);
+            launch_project(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 1, maxmv, m, H->st);
             TRY(sync_ks_small(H));
             ++j;
         }
@@ -387,6 +397,10 @@ int create_impl(const ow3d_params* p, const double* h, const double* hx, const d
         else { double* z; TRY(dalloc(H.get(), &z, (size_t)H->m * H->ldv)); H->Z = z; }
     }
     TRY(dalloc(H.get(), &H->w, (size_t)H->ldv));
+    // the Krylov kernels read element pairs up to n rounded up: padding stays zero
+    CK(cudaMemset(H->V, 0, sizeof(double) * (size_t)(H->m + 1) * H->ldv));
+    CK(cudaMemset(H->w, 0, sizeof(double) * (size_t)H->ldv));
+    if (H->Z) CK(cudaMemset(H->Z, 0, (H->mixed ? sizeof(float) : sizeof(double)) * (size_t)H->m * H->ldv));
     TRY(dalloc(H.get(), &H->ks, 1));
     CK(cudaMallocHost(&H->ks_host, sizeof(KrylovState)));
     std::memset(H->ks_host, 0, sizeof(KrylovState));

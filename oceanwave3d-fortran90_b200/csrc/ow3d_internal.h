@@ -46,6 +46,7 @@ struct LevelDev {
     int Nxg, Nyg, Nzg;
     int64_t N;
     int ncolor;             // 2 or 4 (multicolour column Gauss-Seidel)
+    int cross;              // mixed-derivative terms present (h_x or h_y nonzero on the level)
     int xc, yc, zc;         // this level is coarsened w.r.t. the next finer one
     const T* SX;            // [2][Nxg][3]
     const T* SY;            // [2][Nyg][3]
@@ -53,6 +54,7 @@ struct LevelDev {
     const T* zs;            // sigma with zs[0] = 0
     const T *h, *hx, *hxx, *hy, *hyy;  // Nxg*Nyg (ghost values as MGPreProcess sets them)
     const double *x, *y, *z;           // coordinates for transfer weights (FP64)
+    const double *ix, *iy, *iz;        // 1/(x[i+1]-x[i-1]) etc. (computed as (dW+dE)) per index
     T* xv;                  // iterate
     T* bv;                  // right-hand side
     T* rv;                  // residual
@@ -113,8 +115,10 @@ struct DotScratch {
 };
 void launch_multidot(const double* V, int64_t ldv, int k, const double* w, int64_t n, const DotScratch& sc,
                      KrylovState* ks, int cond, cudaStream_t st);
+// Projection pass; the last block finishes the Arnoldi step (Givens rotation,
+// stopping test) when no re-orthogonalisation pass follows.
 void launch_project(const double* V, int64_t ldv, int k, double* w, int64_t n, const DotScratch& sc, KrylovState* ks,
-                    int cond, cudaStream_t st);
+                    int cond, int maxmv, int m, cudaStream_t st);
 void launch_arnoldi_finish(KrylovState* ks, int maxmv, int m, cudaStream_t st);
 void launch_norm_init(const double* v, int64_t n, const DotScratch& sc, KrylovState* ks, double rtol, double atol,
                       cudaStream_t st);

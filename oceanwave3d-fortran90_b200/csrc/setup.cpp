@@ -137,7 +137,7 @@ int build_grid(const ow3d_params& p, const double* h, const double* hx, const do
     if (p.alpha != 3 || (p.Ny > 1 && p.beta != 3) || p.gamma != 3) return fail("alpha = beta = gamma = 3 required");
     if (p.alphaprecond != 1 || (p.Ny > 1 && p.betaprecond != 1) || p.gammaprecond != 1)
         return fail("alphaprecond = betaprecond = gammaprecond = 1 required");
-    if (p.Nz + 1 > kMaxNzgHost) return fail("Nz too large");
+    if (p.Nz + 1 > 34) return fail("Nz must be at most 33 (32 interior sigma rows per multigrid column)");
     G.Nx = p.Nx; G.Ny = p.Ny; G.Nz = p.Nz;
     G.gx = 1; G.gy = (p.Ny > 1) ? 1 : 0; G.gz = 1;
     G.Nxg = p.Nx + 2 * G.gx; G.Nyg = p.Ny + 2 * G.gy; G.Nzg = p.Nz + G.gz;
