@@ -98,6 +98,27 @@ def dof(p):
     return p.Nx * p.Ny * p.Nz
 
 
+def replica_seed(rank):
+    """Each rank runs an independent replica (its own seeded sea); nothing is
+    exchanged between ranks on the data path."""
+    return 1234 + rank
+
+
+def max_over_ranks(value, world, device):
+    """Slowest rank's time: the job is done when the last replica is."""
+    if world <= 1:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(dof_per_replica, steps, world, ms):
+    """Whole-job DOF-timesteps/s: every rank advanced its replica `steps` steps."""
+    return dof_per_replica * steps * world / (ms / 1e3)
+
+
 def run_gpu(args, rank, world):
     import torch
     pkg = package()
@@ -108,7 +129,7 @@ def run_gpu(args, rank, world):
     res = {}
     states = {}
     for prec in ("fp64", "mixed"):
-        p, geo, E0, P0 = W.irregular_sea(**WORKLOAD, precision=(1 if prec == "mixed" else 0), seed=1234 + rank)
+        p, geo, E0, P0 = W.irregular_sea(**WORKLOAD, precision=(1 if prec == "mixed" else 0), seed=replica_seed(rank))
         p.device = dev
         sim = pkg.Simulation(p, **geo)
         sim.set_state(E0, P0)
@@ -117,16 +138,15 @@ def run_gpu(args, rank, world):
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
+        n0 = lib.ow3d_launch_count()
         with ClockSampler(dev) as clk:
             st, ms = sim.step_timed(args.steps)
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        if world > 1:
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+        launches = lib.ow3d_launch_count() - n0
+        ms = max_over_ranks(ms, world, "cuda")
         s = sim.stats()
         E, P, Wv, phi, tt = sim.get_state()
         states[prec] = (E, phi)
-        res[prec] = dict(ms=ms, stats=s, clocks=clk.summary(), params=p, bytes=sim.device_bytes())
+        res[prec] = dict(ms=ms, stats=s, clocks=clk.summary(), params=p, bytes=sim.device_bytes(), launches=launches)
         if prec == "mixed":
             res["sim"] = sim
         else:
@@ -151,10 +171,7 @@ def run_gpu(args, rank, world):
         lib.ow3d_get_state(sim.h, pkg._d(hostE), pkg._d(hostP), pkg._d(outW), None, None)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, world, "cuda")
     sim.close()
     # eta / phi error of the mixed path against the FP64 path after the same steps
     Ef, phif = states["fp64"]; Em, phim = states["mixed"]
@@ -238,8 +255,8 @@ def main():
     pkg = package()
     D = dof(pm)
     ms_mixed, ms_fp64 = res["mixed"]["ms"], res["fp64"]["ms"]
-    v_mixed = D * args.steps * world / (ms_mixed / 1e3)
-    v_fp64 = D * args.steps * world / (ms_fp64 / 1e3)
+    v_mixed = job_throughput(D, args.steps, world, ms_mixed)
+    v_fp64 = job_throughput(D, args.steps, world, ms_fp64)
     peak, peak_kind = peaks()
     roof = None
     kr = kernel_roofline(pkg, pm, int(os.environ.get("LOCAL_RANK", "0")))
@@ -271,10 +288,10 @@ def main():
                   "eta_rel_err_vs_fp64": err_eta, "phi_rel_err_vs_fp64": err_phi},
         "speedup_mixed_vs_fp64": v_mixed / v_fp64,
         "laplace_solves_per_s": sm["solves"] * world / (ms_mixed / 1e3),
-        "e2e": {"value": D * args.steps * world / e2e_s, "unit": UNIT,
+        "e2e": {"value": job_throughput(D, args.steps, world, e2e_s * 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": 2 * 8 * C, "d2h_bytes_per_step": 3 * 8 * C},
         "roofline": roof, "cpu_baseline": cpu, "clocks": res["mixed"]["clocks"],
-        "gpu_launches": None,
+        "gpu_launches": res["mixed"]["launches"],
     }
     print(json.dumps(out))
     if world > 1:

@@ -27,6 +27,10 @@ int ow3d_test_level_op(ow3d_handle* h, int level, int op, int nu, const double* 
 /* Time `reps` back-to-back launches of one kernel group with CUDA events on
  * the handle's stream: which 0 = high-order operator, 1 = one preconditioner
  * application (V-cycle). Returns the total milliseconds. */
+/* Number of kernels this library has launched since it was loaded, over all
+ * handles and threads (the cooperative coarse-grid kernel counts as one). */
+unsigned long long ow3d_launch_count(void);
+
 int ow3d_bench_kernel(ow3d_handle* h, int which, int reps, double* ms_total);
 /* sizeof the C structs: 0 ow3d_params, 1 ow3d_zone, 2 ow3d_stats. */
 int ow3d_test_sizeof(int which);

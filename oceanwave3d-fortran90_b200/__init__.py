@@ -53,6 +53,8 @@ def lib():
         L.ow3d_test_level_op.argtypes = [_C.c_void_p, _C.c_int, _C.c_int, _C.c_int, D, D, D]
         L.ow3d_test_sizeof.argtypes = [_C.c_int]
         L.ow3d_bench_kernel.argtypes = [_C.c_void_p, _C.c_int, _C.c_int, D]
+        L.ow3d_launch_count.argtypes = []
+        L.ow3d_launch_count.restype = _C.c_ulonglong
         _lib = L
     return _lib
 

@@ -279,51 +279,51 @@ void fs_stage(const FsArgs& a, const double* E, const double* P, const double* W
               const double* Ey, const double* Py, const double* E0, const double* P0, double c, double* kE,
               double* kP, double* tE, double* tP, cudaStream_t st) {
     int64_t C = (int64_t)a.Nxg * a.Nyg;
-    k_fs_stage<<<nb(C), 256, 0, st>>>(a, E, P, W, Ex, Px, Ey, Py, E0, P0, c, kE, kP, tE, tP);
+    note_launch(), k_fs_stage<<<nb(C), 256, 0, st>>>(a, E, P, W, Ex, Px, Ey, Py, E0, P0, c, kE, kP, tE, tP);
 }
 void fs_rk_final(const FsArgs& a, double* E, double* P, double* const* kE, double* const* kP, double dt,
                  cudaStream_t st) {
     int64_t C = (int64_t)a.Nxg * a.Nyg;
-    k_rk_final<<<nb(C), 256, 0, st>>>(a, E, P, kE[0], kE[1], kE[2], kE[3], kP[0], kP[1], kP[2], kP[3], dt);
+    note_launch(), k_rk_final<<<nb(C), 256, 0, st>>>(a, E, P, kE[0], kE[1], kE[2], kE[3], kP[0], kP[1], kP[2], kP[3], dt);
 }
 void fs_relax(const FsArgs& a, const RelaxZoneDev* zones, int nz, double* E, double* P, double RKtime, double time,
               double transient, cudaStream_t st) {
     const double FAC = (RKtime < transient) ? RKtime / transient : 1.0;
     for (int z = 0; z < nz; ++z) {
         int64_t box = (int64_t)(zones[z].i1 - zones[z].i0 + 1) * (zones[z].j1 - zones[z].j0 + 1);
-        k_relax<<<nb(box), 256, 0, st>>>(a, zones[z], E, P, FAC, RKtime, time);
+        note_launch(), k_relax<<<nb(box), 256, 0, st>>>(a, zones[z], E, P, FAC, RKtime, time);
     }
 }
 void fs_derivs(const FsArgs& a, double* E, double* P, double* Ex, double* Exx, double* Px, double* Ey, double* Eyy,
                double* Py, cudaStream_t st) {
     int64_t C = (int64_t)a.Nxg * a.Nyg;
-    k_ghost_x<<<nb(a.Nyg, 128), 128, 0, st>>>(a, E, P);
-    k_diff_x<<<nb(C), 256, 0, st>>>(a, E, P, Ex, Exx, Px);
+    note_launch(), k_ghost_x<<<nb(a.Nyg, 128), 128, 0, st>>>(a, E, P);
+    note_launch(), k_diff_x<<<nb(C), 256, 0, st>>>(a, E, P, Ex, Exx, Px);
     if (a.three) {
-        k_ghost_y<<<nb(a.Nxg, 128), 128, 0, st>>>(a, E, P);
-        k_diff_y<<<nb(C), 256, 0, st>>>(a, E, P, Ey, Eyy, Py);
+        note_launch(), k_ghost_y<<<nb(a.Nxg, 128), 128, 0, st>>>(a, E, P);
+        note_launch(), k_diff_y<<<nb(C), 256, 0, st>>>(a, E, P, Ey, Eyy, Py);
     }
 }
 void fs_wvel(const FsArgs& a, const double* phi, const double* E, double* W, cudaStream_t st) {
     int64_t C = (int64_t)a.Nxg * a.Nyg;
-    k_wvel<<<nb(C), 256, 0, st>>>(a, phi, E, W);
+    note_launch(), k_wvel<<<nb(C), 256, 0, st>>>(a, phi, E, W);
 }
 void fs_set_rhs(const FsArgs& a, const double* P, double* rhs, cudaStream_t st) {
     int64_t C = (int64_t)a.Nxg * a.Nyg;
-    k_set_rhs<<<nb(C), 256, 0, st>>>(a, P, rhs);
+    note_launch(), k_set_rhs<<<nb(C), 256, 0, st>>>(a, P, rhs);
 }
 void fs_extrap(double* phi, const double* lnew, const double* llast, int64_t n, int stage3, cudaStream_t st) {
-    k_extrap<<<nb(n), 256, 0, st>>>(phi, lnew, llast, n, stage3);
+    note_launch(), k_extrap<<<nb(n), 256, 0, st>>>(phi, lnew, llast, n, stage3);
 }
 void fs_filter(const FsArgs& a, const FilterDev& f, double* U, double* tmp, cudaStream_t st) {
     int64_t C = (int64_t)a.Nxg * a.Nyg;
-    k_filter_x<<<nb(C), 256, 0, st>>>(a, f, U, tmp);
-    if (a.three) k_filter_y<<<nb(C), 256, 0, st>>>(a, f, tmp, U);
+    note_launch(), k_filter_x<<<nb(C), 256, 0, st>>>(a, f, U, tmp);
+    if (a.three) note_launch(), k_filter_y<<<nb(C), 256, 0, st>>>(a, f, tmp, U);
     else cudaMemcpyAsync(U, tmp, sizeof(double) * C, cudaMemcpyDeviceToDevice, st);
 }
 void fs_unstable(const FsArgs& a, const double* E, double hmax10, int* flag, cudaStream_t st) {
     int64_t C = (int64_t)a.Nxg * a.Nyg;
-    k_unstable<<<nb(C), 256, 0, st>>>(a, E, hmax10, flag);
+    note_launch(), k_unstable<<<nb(C), 256, 0, st>>>(a, E, hmax10, flag);
 }
 
 }  // namespace ow3d

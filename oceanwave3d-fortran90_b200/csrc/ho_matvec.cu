@@ -218,7 +218,7 @@ void launch_impl(const HoGrid& g, const Surface& s, const TIN* phi, const double
         cudaFuncSetAttribute(k_ho_matvec<NZG, THREE, TIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         attr = true;
     }
-    k_ho_matvec<NZG, THREE, TIN><<<grd, blk, smem, st>>>(g, s, phi, scale, b, y, mode, BX, BY);
+    note_launch(), k_ho_matvec<NZG, THREE, TIN><<<grd, blk, smem, st>>>(g, s, phi, scale, b, y, mode, BX, BY);
 }
 
 template <bool THREE, typename TIN>

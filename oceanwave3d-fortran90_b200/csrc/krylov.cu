@@ -311,24 +311,24 @@ void launch_multidot(const double* V, int64_t ldv, int k, const double* w, int64
     if (nbx > need) nbx = (int)need;
     if (nbx < 1) nbx = 1;
     if (nbx > sc.nblocks) nbx = sc.nblocks;
-    k_multidot<<<dim3(nbx, k + 1), kThreads, 0, st>>>(V, ldv, k, w, n, sc.partial, sc.counter, nbx, ks, cond);
+    note_launch(), k_multidot<<<dim3(nbx, k + 1), kThreads, 0, st>>>(V, ldv, k, w, n, sc.partial, sc.counter, nbx, ks, cond);
 }
 
 void launch_project(const double* V, int64_t ldv, int k, double* w, int64_t n, const DotScratch& sc, KrylovState* ks,
                     int cond, int maxmv, int m, cudaStream_t st) {
-    k_project<<<sc.nblocks, kThreads, 0, st>>>(V, ldv, k, w, n, sc.partial, sc.counter, sc.nblocks, ks, cond, maxmv, m);
+    note_launch(), k_project<<<sc.nblocks, kThreads, 0, st>>>(V, ldv, k, w, n, sc.partial, sc.counter, sc.nblocks, ks, cond, maxmv, m);
 }
 
 void launch_arnoldi_finish(KrylovState* ks, int maxmv, int m, cudaStream_t st) {
-    k_arnoldi_finish<<<1, 32, 0, st>>>(ks, maxmv, m);
+    note_launch(), k_arnoldi_finish<<<1, 32, 0, st>>>(ks, maxmv, m);
 }
 
 void launch_norm_init(const double* v, int64_t n, const DotScratch& sc, KrylovState* ks, double rtol, double atol,
                       cudaStream_t st) {
-    k_norm_init<<<sc.nblocks, kThreads, 0, st>>>(v, n, sc.partial, sc.counter, sc.nblocks, ks, rtol, atol);
+    note_launch(), k_norm_init<<<sc.nblocks, kThreads, 0, st>>>(v, n, sc.partial, sc.counter, sc.nblocks, ks, rtol, atol);
 }
 
-void launch_backsolve(KrylovState* ks, cudaStream_t st) { k_backsolve<<<1, 32, 0, st>>>(ks); }
+void launch_backsolve(KrylovState* ks, cudaStream_t st) { note_launch(), k_backsolve<<<1, 32, 0, st>>>(ks); }
 
 template <typename TZ>
 void launch_solution_update(double* x, const TZ* Z, int64_t ldz, int64_t n, const KrylovState* ks, int use_scale,
@@ -336,20 +336,20 @@ void launch_solution_update(double* x, const TZ* Z, int64_t ldz, int64_t n, cons
     int nb = (int)((n + kThreads - 1) / kThreads);
     if (nb > 148 * 8) nb = 148 * 8;
     if (nb < 1) nb = 1;
-    k_solution_update<TZ><<<nb, kThreads, 0, st>>>(x, Z, ldz, n, ks, use_scale);
+    note_launch(), k_solution_update<TZ><<<nb, kThreads, 0, st>>>(x, Z, ldz, n, ks, use_scale);
 }
 template void launch_solution_update<double>(double*, const double*, int64_t, int64_t, const KrylovState*, int,
                                              cudaStream_t);
 template void launch_solution_update<float>(double*, const float*, int64_t, int64_t, const KrylovState*, int,
                                             cudaStream_t);
 
-void launch_krylov_reset(KrylovState* ks, cudaStream_t st) { k_krylov_reset<<<1, 32, 0, st>>>(ks); }
+void launch_krylov_reset(KrylovState* ks, cudaStream_t st) { note_launch(), k_krylov_reset<<<1, 32, 0, st>>>(ks); }
 
 // Restart after a full subspace: keep the matvec count and the tolerance.
 __global__ void k_krylov_restart(KrylovState* ks) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     ks->k = 0; ks->done = 0; ks->converged = 0; ks->reorth = 0;
 }
-void launch_krylov_restart(KrylovState* ks, cudaStream_t st) { k_krylov_restart<<<1, 32, 0, st>>>(ks); }
+void launch_krylov_restart(KrylovState* ks, cudaStream_t st) { note_launch(), k_krylov_restart<<<1, 32, 0, st>>>(ks); }
 
 }  // namespace ow3d

@@ -177,15 +177,15 @@ inline int nblk(int64_t n, int t = 256) {
 
 template <typename T>
 void launch_lo_matvec(const LevelDev<T>& L, const T* x, T* y, cudaStream_t st) {
-    if (L.Nyg > 1) k_lo_matvec<T, true><<<nblk(L.N), 256, 0, st>>>(L, x, y);
-    else k_lo_matvec<T, false><<<nblk(L.N), 256, 0, st>>>(L, x, y);
+    if (L.Nyg > 1) note_launch(), k_lo_matvec<T, true><<<nblk(L.N), 256, 0, st>>>(L, x, y);
+    else note_launch(), k_lo_matvec<T, false><<<nblk(L.N), 256, 0, st>>>(L, x, y);
 }
 
 template <typename T>
 static void special(const LevelDev<T>& L, cudaStream_t st) {
     const int64_t n = (int64_t)L.Nxg * L.Nyg + ((L.Nyg > 1) ? ((int64_t)2 * L.Nyg + 2 * (L.Nxg - 2)) : 2) * L.Nzg;
-    if (L.Nyg > 1) k_lo_special<T, true><<<nblk(n, 128), 128, 0, st>>>(L);
-    else k_lo_special<T, false><<<nblk(n, 128), 128, 0, st>>>(L);
+    if (L.Nyg > 1) note_launch(), k_lo_special<T, true><<<nblk(n, 128), 128, 0, st>>>(L);
+    else note_launch(), k_lo_special<T, false><<<nblk(n, 128), 128, 0, st>>>(L);
 }
 
 template <typename T, bool THREE, int S>
@@ -195,8 +195,8 @@ static void colour_launch(const LevelDev<T>& L, int c, cudaStream_t st) {
     int64_t blocks = (warps * 32 + 127) / 128;
     if (blocks > 148 * 32) blocks = 148 * 32;
     if (blocks < 1) blocks = 1;
-    if (L.cross) k_lo_colour<T, THREE, S, true><<<(int)blocks, 128, 0, st>>>(L, c);
-    else k_lo_colour<T, THREE, S, false><<<(int)blocks, 128, 0, st>>>(L, c);
+    if (L.cross) note_launch(), k_lo_colour<T, THREE, S, true><<<(int)blocks, 128, 0, st>>>(L, c);
+    else note_launch(), k_lo_colour<T, THREE, S, false><<<(int)blocks, 128, 0, st>>>(L, c);
 }
 template <typename T, bool THREE>
 static void colour_dispatch(const LevelDev<T>& L, int c, cudaStream_t st) {
@@ -224,31 +224,31 @@ void launch_lo_smooth(const LevelDev<T>& L, int nu, cudaStream_t st) {
 
 template <typename T>
 void launch_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* rf, T* rc, cudaStream_t st) {
-    k_restrict<T><<<nblk(Cc.N), 256, 0, st>>>(F, Cc, rf, rc, Cc.xv);
+    note_launch(), k_restrict<T><<<nblk(Cc.N), 256, 0, st>>>(F, Cc, rf, rc, Cc.xv);
 }
 template <typename T>
 void launch_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* xc, T* xf, cudaStream_t st) {
-    k_prolong_add<T><<<nblk(F.N), 256, 0, st>>>(F, Cc, xc, xf);
+    note_launch(), k_prolong_add<T><<<nblk(F.N), 256, 0, st>>>(F, Cc, xc, xf);
 }
 template <typename T>
 void launch_coarse_solve(const LevelDev<T>& Lc, const T* inv, cudaStream_t st) {
     int n = (int)Lc.N;
-    k_coarse<T><<<(n + 127) / 128, 128, 0, st>>>(n, inv, Lc.bv, Lc.xv);
+    note_launch(), k_coarse<T><<<(n + 127) / 128, 128, 0, st>>>(n, inv, Lc.bv, Lc.xv);
 }
 template <typename T>
 void launch_scale_copy(const double* src, double s, T* dst, int64_t n, cudaStream_t st) {
-    k_scale_copy<T><<<nblk(n), 256, 0, st>>>(src, s, dst, n);
+    note_launch(), k_scale_copy<T><<<nblk(n), 256, 0, st>>>(src, s, dst, n);
 }
 template <typename T>
 void launch_fill(T* dst, T v, int64_t n, cudaStream_t st) {
-    k_fill<T><<<nblk(n), 256, 0, st>>>(dst, v, n);
+    note_launch(), k_fill<T><<<nblk(n), 256, 0, st>>>(dst, v, n);
 }
 template <typename T>
 void launch_scale_copy_dev(const double* src, const double* ds, T* dst, int64_t n, cudaStream_t st) {
-    k_scale_copy_dev<T><<<nblk(n), 256, 0, st>>>(src, ds, dst, n);
+    note_launch(), k_scale_copy_dev<T><<<nblk(n), 256, 0, st>>>(src, ds, dst, n);
 }
 void launch_convert(const float* src, double* dst, int64_t n, cudaStream_t st) {
-    k_convert<<<nblk(n), 256, 0, st>>>(src, dst, n);
+    note_launch(), k_convert<<<nblk(n), 256, 0, st>>>(src, dst, n);
 }
 
 // Launch the fused coarse cycle over levels lc..0 with a fully co-resident grid.
@@ -265,6 +265,7 @@ static void coarse_cycle(const LevelDev<T>* lev, int lc, const T* inv, int nu1, 
     LevelPack<T> P;
     for (int l = 0; l <= lc; ++l) P.l[l] = lev[l];
     void* args[] = {(void*)&P, (void*)&lc, (void*)&inv, (void*)&nu1, (void*)&nu2};
+    note_launch();
     cudaLaunchCooperativeKernel((const void*)k_mg_coarse_cycle<T, THREE>, dim3(grid), dim3(256), args, 0, st);
 }
 
@@ -287,8 +288,8 @@ static void vcycle(LevelDev<T>* lev, int l, int lc, const T* inv, int nu1, int n
     const LevelDev<T>& F = lev[l];
     LevelDev<T>& Cc = lev[l - 1];
     launch_lo_smooth(F, nu1, st);
-    if (F.Nyg > 1) k_lo_residual<T, true><<<nblk(F.N), 256, 0, st>>>(F);
-    else k_lo_residual<T, false><<<nblk(F.N), 256, 0, st>>>(F);
+    if (F.Nyg > 1) note_launch(), k_lo_residual<T, true><<<nblk(F.N), 256, 0, st>>>(F);
+    else note_launch(), k_lo_residual<T, false><<<nblk(F.N), 256, 0, st>>>(F);
     launch_restrict(F, Cc, (const T*)F.rv, Cc.bv, st);   // also zeroes Cc.xv
     vcycle(lev, l - 1, lc, inv, nu1, nu2, st);
     launch_prolong_add(F, Cc, (const T*)Cc.xv, F.xv, st);

@@ -21,6 +21,8 @@
 
 using namespace ow3d;
 
+std::atomic<unsigned long long> ow3d::g_kernel_launches{0ull};
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -592,6 +594,8 @@ int level_op_t(ow3d_handle* H, MgSet<T>& S, int l, int op, int nu, const double*
 // ====================================================================== C ABI
 extern "C" {
 
+unsigned long long ow3d_launch_count(void) { return g_kernel_launches.load(std::memory_order_relaxed); }
+
 int ow3d_default_params(ow3d_params* p) { return default_params(p); }
 
 int ow3d_read_deck(const char* path, ow3d_params* p) {
@@ -634,6 +638,11 @@ int ow3d_dims(const ow3d_handle* H, int* Nxg, int* Nyg, int* Nzg, size_t* bytes)
 
 int ow3d_estimate_bytes(const ow3d_params* p, size_t* bytes) {
     if (!p || !bytes) return OW3D_ERR_BAD_INPUT;
+    {
+        std::string err;
+        if (check_params(*p, &err) != 0) { g_last_error = err; return OW3D_ERR_BAD_INPUT; }
+        if (p->GMRESmaxiterations < 2 || p->GMRESmaxiterations > kMaxKrylov) { g_last_error = "GMRESmaxiterations out of range"; return OW3D_ERR_BAD_INPUT; }
+    }
     const int gx = p->Nx > 1 ? 1 : 0, gy = p->Ny > 1 ? 1 : 0;
     const double C = (double)(p->Nx + 2 * gx) * (p->Ny + 2 * gy);
     const double N = C * (p->Nz + 1);

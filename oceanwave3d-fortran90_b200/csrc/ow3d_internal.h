@@ -7,12 +7,17 @@
 //   2-D fields  E(i,j):     i fastest, index (i-1) + Nxg*(j-1)
 // Ghost points are included (one layer in x, y and below the bottom).
 #pragma once
+#include <atomic>
 #include <cstdint>
 #include <cstddef>
 #include <cuda_runtime.h>
 #include "../../include/ow3d.h"
 
 namespace ow3d {
+
+// Kernels launched by this library since load (all handles, all threads).
+extern std::atomic<unsigned long long> g_kernel_launches;
+inline void note_launch() { g_kernel_launches.fetch_add(1ull, std::memory_order_relaxed); }
 
 constexpr int kMaxLevels = 16;
 constexpr int kMaxKrylov = 64;     // maximum GMRESmaxiterations

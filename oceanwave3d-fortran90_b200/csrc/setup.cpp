@@ -126,8 +126,7 @@ static void level_colours(LevelHost& L) {
     L.ncolor = (L.Nxg > 1 && L.Nyg > 1 && m > 0) ? 4 : 2;
 }
 
-int build_grid(const ow3d_params& p, const double* h, const double* hx, const double* hxx, const double* hy,
-               const double* hyy, GridHost& G, std::string* err) {
+int check_params(const ow3d_params& p, std::string* err) {
     auto fail = [&](const char* m) { if (err) *err = m; return OW3D_ERR_BAD_INPUT; };
     if (p.Nx < 1 || p.Ny < 1 || p.Nz < 3) return fail("Nx, Ny >= 1 and Nz >= 3 required");
     if (p.Nx == 1) return fail("Nx == 1 (2-D in y) is not supported; orient the flume along x");
@@ -138,6 +137,23 @@ int build_grid(const ow3d_params& p, const double* h, const double* hx, const do
     if (p.alphaprecond != 1 || (p.Ny > 1 && p.betaprecond != 1) || p.gammaprecond != 1)
         return fail("alphaprecond = betaprecond = gammaprecond = 1 required");
     if (p.Nz + 1 > 34) return fail("Nz must be at most 33 (32 interior sigma rows per multigrid column)");
+    const int Nxg = p.Nx + 2, Nyg = p.Ny + (p.Ny > 1 ? 2 : 0), Nzg = p.Nz + 1;
+    if (Nxg < 8 || (p.Ny > 1 && Nyg < 8) || Nzg < 8) return fail("at least 7 points per direction (6th-order stencils)");
+    if (p.filteringONOFF > 0) {
+        const int NP = 2 * p.filterALPHA + 1;
+        if (p.filterALPHA < 1 || p.filterALPHA > 6) return fail("filterALPHA must be 1..6 (FilterInit.f90 boundary filters)");
+        if (Nxg < NP + 2 || (p.Ny > 1 && Nyg < NP + 2)) return fail("grid too small for the filter width");
+    }
+    if (p.precision != OW3D_PREC_FP64 && p.precision != OW3D_PREC_MIXED) return fail("precision must be 0 or 1");
+    if (p.krylov != OW3D_KRYLOV_FGMRES && p.krylov != OW3D_KRYLOV_LGMRES) return fail("krylov must be 0 or 1");
+    if (p.GMRESmaxiterations < 1) return fail("GMRESmaxiterations must be >= 1");
+    return 0;
+}
+
+int build_grid(const ow3d_params& p, const double* h, const double* hx, const double* hxx, const double* hy,
+               const double* hyy, GridHost& G, std::string* err) {
+    auto fail = [&](const char* m) { if (err) *err = m; return OW3D_ERR_BAD_INPUT; };
+    if (int r = check_params(p, err)) return r;
     G.Nx = p.Nx; G.Ny = p.Ny; G.Nz = p.Nz;
     G.gx = 1; G.gy = (p.Ny > 1) ? 1 : 0; G.gz = 1;
     G.Nxg = p.Nx + 2 * G.gx; G.Nyg = p.Ny + 2 * G.gy; G.Nzg = p.Nz + G.gz;

@@ -1,0 +1,85 @@
+"""Golden vectors (tests/golden, made by make_golden.py from the oracle).
+
+CPU: the files are intact (MANIFEST.txt SHA-256) and the oracle still
+reproduces them. GPU: the CUDA path matches the device-ordered vectors
+(1e-10 relative on solves and time steps, 1e-12 on the operator).
+"""
+import hashlib
+import pathlib
+import sys
+
+import numpy as np
+import pytest
+
+HERE = pathlib.Path(__file__).resolve().parent
+GOLDEN = HERE / "golden"
+sys.path.insert(0, str(GOLDEN))
+
+
+def rel(a, b):
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+def load(name):
+    with np.load(GOLDEN / f"{name}.npz") as z:
+        return {k: z[k] for k in z.files}
+
+
+def names():
+    return sorted(f.stem for f in GOLDEN.glob("*.npz"))
+
+
+def test_manifest_hashes():
+    lines = (GOLDEN / "MANIFEST.txt").read_text().split("\n")
+    listed = {}
+    for ln in lines:
+        if ln.strip():
+            h, f = ln.split()
+            listed[f] = h
+    assert sorted(listed) == sorted(f"{n}.npz" for n in names())
+    for f, h in listed.items():
+        assert hashlib.sha256((GOLDEN / f).read_bytes()).hexdigest() == h, f
+
+
+def test_oracle_reproduces_golden(ow3d, oracle):
+    import make_golden
+    fresh = make_golden.generate()
+    assert sorted(fresh) == names()
+    for name in names():
+        g = load(name)
+        for k, v in fresh[name].items():
+            if k in ("iterations", "status"):
+                assert np.array_equal(v, g[k]), (name, k)
+            else:
+                # same code, same inputs; only the host compiler's contraction choices may differ
+                assert rel(v, g[k]) < 1e-11, (name, k, rel(v, g[k]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["bump3d_17x9x9", "bump3d_33x17x9", "slope2d_33x9"])
+def test_device_matches_golden_operators(ow3d, name):
+    import make_golden
+    case, kw = make_golden.cases_table()[name]
+    g = load(f"op_{name}_dev")
+    p, geo = case(**kw)
+    sim = ow3d.Simulation(p, **geo)
+    surf = list(g["surface"])
+    assert rel(sim.matvec(g["phi"], *surf), g["matvec"]) < 1e-12
+    assert rel(sim.precondition(g["r"]), g["precond"]) < 1e-10
+    phi, it, st = sim.solve(g["rhs"], np.zeros(sim.N), *surf)
+    assert abs(it - int(g["iterations"][0])) <= 1
+    assert rel(phi, g["solve"]) < 1e-10
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nl", ["lin", "nl"])
+def test_device_matches_golden_standing_wave(ow3d, nl):
+    import cases
+    g = load(f"rk4_standing2d_{nl}_dev")
+    p, geo = cases.flat_2d(Nx=33, Nz=9, L=2.0, LinearONOFF=(1 if nl == "nl" else 0), dt=0.02)
+    sim = ow3d.Simulation(p, **geo)
+    sim.set_state(g["E0"], np.zeros_like(g["E0"]))
+    sim.step(10)
+    E, P, W, phi, t = sim.get_state()
+    assert abs(t - float(g["t"][0])) < 1e-14
+    assert rel(E, g["E"]) < 1e-10 and rel(P, g["P"]) < 1e-10 and rel(phi, g["phi"]) < 1e-10
