@@ -213,6 +213,24 @@ def cpu_baseline(threads, steps=1):
     return dof(p) * steps / dt, dt, p
 
 
+def profile_step(args):
+    """One warm-up step and one step of the workload, for ncu launch lists and
+    captures (prints the step time; the numbers are not bench values)."""
+    pkg = package()
+    kw = dict(WORKLOAD)
+    if args.grid:
+        kw = dict(zip(("Nx", "Ny", "Nz"), (int(v) for v in args.grid.lower().split("x"))))
+    p, geo, E0, P0 = pkg.workloads.irregular_sea(**kw, precision=(1 if args.profile == "mixed" else 0))
+    sim = pkg.Simulation(p, **geo)
+    sim.set_state(E0, P0)
+    sim.step(1)
+    st, ms = sim.step_timed(1)
+    s = sim.stats()
+    print(f"profile {args.profile} {p.Nx}x{p.Ny}x{p.Nz}: step {ms:.2f} ms, solves {s['solves']}, "
+          f"iterations {s['total_iterations']}")
+    sim.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -220,7 +238,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile", choices=["fp64", "mixed"], default=None,
+                    help="profiling driver: one warm-up step then one step of the workload, no JSON line")
+    ap.add_argument("--grid", default=None, help="NXxNYxNZ override for --profile (e.g. 257x65x17)")
     args = ap.parse_args()
+    if args.profile:
+        profile_step(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
