@@ -22,7 +22,9 @@ int ow3d_test_filter_coeffs(const ow3d_handle* h, double* centre, double* bounda
  * op 0: out = A_l in1;  op 1: out = smoothed in1 with rhs in2 (nu steps);
  * op 2: out = restriction of the fine residual in1 to level-1;
  * op 3: out = prolongation of the level-1 vector in1 (added to zero);
- * op 4: out = coarsest-level solve of in1 (level 0 only). */
+ * op 4: out = coarsest-level solve of in1 (level 0 only);
+ * op 5: out = in1 after one smoother phase with rhs in2: colour pass `nu`, or
+ *       the bottom-row pass when nu < 0 (levels with mixed-derivative terms). */
 int ow3d_test_level_op(ow3d_handle* h, int level, int op, int nu, const double* in1, const double* in2, double* out);
 /* Time `reps` back-to-back launches of one kernel group with CUDA events on
  * the handle's stream: which 0 = high-order operator, 1 = one preconditioner

@@ -201,7 +201,7 @@ class Simulation:
 
     def level_op(self, l, op, in1, in2=None, nu=1):
         n_out = {0: self.level_size(l), 1: self.level_size(l), 2: self.level_size(l - 1) if l > 0 else 0,
-                 3: self.level_size(l), 4: self.level_size(l)}[op]
+                 3: self.level_size(l), 4: self.level_size(l), 5: self.level_size(l)}[op]
         out = _np.zeros(n_out)
         a = _f64(in1).ravel(); b = None if in2 is None else _f64(in2).ravel()
         _check(lib().ow3d_test_level_op(self.h, l, op, nu, _d(a), _d(b), _d(out)), "level_op")

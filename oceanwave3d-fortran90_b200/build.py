@@ -35,7 +35,7 @@ def sources():
 
 
 def headers():
-    return sorted(list(CSRC.glob("*.h")) + list((HERE.parent / "include").glob("*.h")))
+    return sorted(list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list((HERE.parent / "include").glob("*.h")))
 
 
 def _needs(obj, src, deps):

@@ -8,14 +8,14 @@
 // y-planes for d2/dxds and x-planes for d2/dyds). Coefficients are evaluated in
 // the kernels from the level's depth fields instead of being stored as CSR.
 //
-// Smoother (device-matched ordering, deterministic):
-//   special pass  : rows of the ghost columns (lateral Neumann / identity) and
-//                   the bottom rows of the interior columns (the reference's
-//                   iGhost list, MGPreProcess.f90:376-439)
-//   colour sweeps : interior columns in 2 or 4 colours, Gauss-Seidel up each
-//                   column (k = 2..Nzg, free surface row last)
-// sequence per smoothing step as MultiGridSolver.f90:118-126,174-181:
-//   special; [colours; special] x nu
+// Smoother (device-matched ordering, deterministic): one smoothing step is one
+// pass per colour of the interior columns (2 colours, or 4 when the level has
+// mixed-derivative terms). A column's task relaxes its bottom row, then its
+// rows k = 2..Nzg bottom to top, then the rows of the lateral ghost columns it
+// borders -- so the reference's special rows (iGhost, MGPreProcess.f90:376-439,
+// relaxed by GaussSeidelSpecialPoints around each sweep in
+// MultiGridSolver.f90:118-126,174-181) are relaxed inside the colour passes
+// instead of in separate strided passes.
 //
 // Levels with few points run inside one cooperative kernel (k_mg_coarse_cycle)
 // that executes the phases of every coarse level back to back with grid-wide
@@ -23,6 +23,7 @@
 #include "ow3d_internal.h"
 #include "mg_device.cuh"
 #include <cooperative_groups.h>
+#include <cstring>
 #include <vector>
 
 namespace ow3d {
@@ -36,35 +37,39 @@ namespace cg = cooperative_groups;
 
 // Points per level below which the level runs in the fused coarse kernel.
 constexpr int64_t kCoopMaxPoints = 160000;
+// Threads per block of the fused coarse kernel (one block per SM: fewer
+// blocks make the grid-wide barrier cheaper).
+constexpr int kCoopThreads = 512;
 
 template <typename T, bool THREE>
 __global__ void k_lo_matvec(LevelDev<T> L, const T* __restrict__ x, T* __restrict__ y) {
     OW3D_GRID_STRIDE(p, L.N) {
-        const int k = (int)(p % L.Nzg) + 1;
-        const int64_t c = p / L.Nzg;
-        const int i = (int)(c % L.Nxg) + 1, j = (int)(c / L.Nxg) + 1;
+        int k, i, j;
+        int64_t c;
+        decomp(L, p, k, c, i, j);
         T dg;
         y[p] = lo_row<T, THREE>(L, x, k, i, j, dg);
     }
 }
 
-template <typename T, bool THREE>
+template <typename T, bool THREE, bool CROSS>
 __global__ void k_lo_residual(LevelDev<T> L) {
-    OW3D_GRID_STRIDE(p, L.N) residual_item<T, THREE>(L, p);
+    OW3D_GRID_STRIDE(p, L.N) residual_item<T, THREE, CROSS>(L, p);
 }
 
 template <typename T, bool THREE>
-__global__ void k_lo_special(LevelDev<T> L) {
-    OW3D_GRID_STRIDE(q, (special_count<T, THREE>(L))) special_item<T, THREE>(L, q);
+__global__ void k_lo_bottom(LevelDev<T> L) {
+    OW3D_GRID_STRIDE(q, (bottom_count<T, THREE>(L))) bottom_item<T, THREE>(L, q);
 }
 
 template <typename T, bool THREE, int S, bool CROSS>
-__global__ void __launch_bounds__(128) k_lo_colour(LevelDev<T> L, int colour) {
+__global__ void __launch_bounds__(128, 8) k_lo_colour(LevelDev<T> L, int colour) {
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t total = colour_count<T, THREE>(L);
+    const RowConst<T> rk = row_const<T, S>(L);
     for (int64_t base = warp * (32 / S); base < total; base += nwarps * (32 / S))
-        colour_warp<T, THREE, S, CROSS>(L, colour, base);
+        colour_warp<T, THREE, S, CROSS>(L, colour, base, rk);
 }
 
 template <typename T>
@@ -82,6 +87,28 @@ __global__ void k_prolong_add(LevelDev<T> F, LevelDev<T> Cc, const T* __restrict
 template <typename T>
 __global__ void k_coarse(int n, const T* __restrict__ inv, const T* __restrict__ b, T* __restrict__ x) {
     OW3D_GRID_STRIDE(r, n) coarse_item<T>(n, inv, b, x, (int)r);
+}
+
+// x = M b for a dense row-major n x n operator: one warp per row, lanes
+// stride along the row (coalesced), shuffle reduction.
+template <typename T>
+__device__ __forceinline__ void dense_rows(int n, const T* __restrict__ M, const T* __restrict__ b, T* __restrict__ x) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = warp; r < n; r += nwarps) {
+        const T* row = M + r * n;
+        T acc = 0;
+        for (int c = lane; c < n; c += 32) acc += row[c] * b[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) x[r] = acc;
+    }
+}
+
+template <typename T>
+__global__ void k_dense_apply(int n, const T* __restrict__ M, const T* __restrict__ b, T* __restrict__ x) {
+    dense_rows<T>(n, M, b, x);
 }
 
 template <typename T>
@@ -102,8 +129,6 @@ __global__ void k_fill(T* __restrict__ dst, T v, int64_t n) {
 }
 
 // ------------------------------------------------- fused coarse levels
-template <typename T>
-struct LevelPack { LevelDev<T> l[kMaxLevels]; };
 
 inline int seg_width(int Nzg) {
     const int R = Nzg - 2;
@@ -115,8 +140,9 @@ __device__ void coop_colour_loop(const LevelDev<T>& L, int colour) {
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t total = colour_count<T, THREE>(L);
+    const RowConst<T> rk = row_const<T, S>(L);
     for (int64_t base = warp * (32 / S); base < total; base += nwarps * (32 / S))
-        colour_warp<T, THREE, S, CROSS>(L, colour, base);
+        colour_warp<T, THREE, S, CROSS>(L, colour, base, rk);
 }
 
 template <typename T, bool THREE>
@@ -129,39 +155,46 @@ __device__ void coop_colour(const LevelDev<T>& L, int colour) {
 }
 
 template <typename T, bool THREE>
-__device__ void coop_smooth(const LevelDev<T>& L, int nu, cg::grid_group& grid) {
-    OW3D_GRID_STRIDE(q, (special_count<T, THREE>(L))) special_item<T, THREE>(L, q);
+__device__ void coop_bottoms(const LevelDev<T>& L, cg::grid_group& grid) {
+    OW3D_GRID_STRIDE(q, (bottom_count<T, THREE>(L))) bottom_item<T, THREE>(L, q);
     grid.sync();
+}
+
+template <typename T, bool THREE>
+__device__ void coop_smooth(const LevelDev<T>& L, int nu, cg::grid_group& grid) {
+    if (L.cross) coop_bottoms<T, THREE>(L, grid);
     for (int s = 0; s < nu; ++s) {
         for (int c = 0; c < L.ncolor; ++c) { coop_colour<T, THREE>(L, c); grid.sync(); }
-        OW3D_GRID_STRIDE(q, (special_count<T, THREE>(L))) special_item<T, THREE>(L, q);
-        grid.sync();
+        if (L.cross) coop_bottoms<T, THREE>(L, grid);
     }
 }
 
-// V cycle over levels lc..0 (MultiGridSolver.f90:5-192) in one cooperative
-// launch. Level lc's right-hand side is set and its iterate zeroed on entry.
+// V cycle over levels lc..ld (MultiGridSolver.f90:5-192) in one cooperative
+// launch; level ld is solved with the dense operator M (the coarsest level's
+// inverse when ld = 0, otherwise the V cycle below ld as one precomputed map).
+// Level lc's right-hand side is set and its iterate zeroed on entry.
 template <typename T, bool THREE>
-__global__ void __launch_bounds__(256) k_mg_coarse_cycle(LevelPack<T> P, int lc, const T* __restrict__ inv, int nu1,
-                                                         int nu2) {
+__global__ void __launch_bounds__(kCoopThreads) k_mg_coarse_cycle(const LevelDev<T>* __restrict__ P, int lc, int ld,
+                                                                  const T* __restrict__ M, int nu1, int nu2) {
     cg::grid_group grid = cg::this_grid();
-    for (int l = lc; l >= 1; --l) {
-        const LevelDev<T>& L = P.l[l];
-        const LevelDev<T>& Cc = P.l[l - 1];
+    for (int l = lc; l > ld; --l) {
+        const LevelDev<T>& L = P[l];
+        const LevelDev<T>& Cc = P[l - 1];
         coop_smooth<T, THREE>(L, nu1, grid);
-        OW3D_GRID_STRIDE(p, L.N) residual_item<T, THREE>(L, p);
+        if (L.cross) { OW3D_GRID_STRIDE(p, L.N) residual_item<T, THREE, true>(L, p); }
+        else { OW3D_GRID_STRIDE(p, L.N) residual_item<T, THREE, false>(L, p); }
         grid.sync();
         OW3D_GRID_STRIDE(p, Cc.N) restrict_item<T>(L, Cc, L.rv, Cc.bv, Cc.xv, p);
         grid.sync();
     }
     {
-        const LevelDev<T>& L0 = P.l[0];
-        OW3D_GRID_STRIDE(r, L0.N) coarse_item<T>((int)L0.N, inv, L0.bv, L0.xv, (int)r);
+        const LevelDev<T>& Ld = P[ld];
+        dense_rows<T>((int)Ld.N, M, Ld.bv, Ld.xv);
         grid.sync();
     }
-    for (int l = 1; l <= lc; ++l) {
-        const LevelDev<T>& L = P.l[l];
-        const LevelDev<T>& Cc = P.l[l - 1];
+    for (int l = ld + 1; l <= lc; ++l) {
+        const LevelDev<T>& L = P[l];
+        const LevelDev<T>& Cc = P[l - 1];
         OW3D_GRID_STRIDE(p, L.N) prolong_item<T>(L, Cc, Cc.xv, L.xv, p);
         grid.sync();
         coop_smooth<T, THREE>(L, nu2, grid);
@@ -179,13 +212,6 @@ template <typename T>
 void launch_lo_matvec(const LevelDev<T>& L, const T* x, T* y, cudaStream_t st) {
     if (L.Nyg > 1) note_launch(), k_lo_matvec<T, true><<<nblk(L.N), 256, 0, st>>>(L, x, y);
     else note_launch(), k_lo_matvec<T, false><<<nblk(L.N), 256, 0, st>>>(L, x, y);
-}
-
-template <typename T>
-static void special(const LevelDev<T>& L, cudaStream_t st) {
-    const int64_t n = (int64_t)L.Nxg * L.Nyg + ((L.Nyg > 1) ? ((int64_t)2 * L.Nyg + 2 * (L.Nxg - 2)) : 2) * L.Nzg;
-    if (L.Nyg > 1) note_launch(), k_lo_special<T, true><<<nblk(n, 128), 128, 0, st>>>(L);
-    else note_launch(), k_lo_special<T, false><<<nblk(n, 128), 128, 0, st>>>(L);
 }
 
 template <typename T, bool THREE, int S>
@@ -217,9 +243,27 @@ static void colours(const LevelDev<T>& L, cudaStream_t st) {
 }
 
 template <typename T>
+static void bottoms(const LevelDev<T>& L, cudaStream_t st) {
+    const int64_t nyi = L.Nyg > 1 ? L.Nyg - 2 : 1;
+    const int64_t n = (int64_t)(L.Nxg - 2) * nyi + 2 * nyi + (L.Nyg > 1 ? 2 * (int64_t)(L.Nxg - 2) : 0);
+    if (L.Nyg > 1) note_launch(), k_lo_bottom<T, true><<<nblk(n), 256, 0, st>>>(L);
+    else note_launch(), k_lo_bottom<T, false><<<nblk(n), 256, 0, st>>>(L);
+}
+
+template <typename T>
+void launch_lo_pass(const LevelDev<T>& L, int colour, cudaStream_t st) {
+    if (colour < 0) { bottoms(L, st); return; }
+    if (L.Nyg > 1) colour_dispatch<T, true>(L, colour, st);
+    else colour_dispatch<T, false>(L, colour, st);
+}
+
+template <typename T>
 void launch_lo_smooth(const LevelDev<T>& L, int nu, cudaStream_t st) {
-    special(L, st);
-    for (int s = 0; s < nu; ++s) { colours(L, st); special(L, st); }
+    if (L.cross) bottoms(L, st);
+    for (int s = 0; s < nu; ++s) {
+        colours(L, st);
+        if (L.cross) bottoms(L, st);
+    }
 }
 
 template <typename T>
@@ -251,22 +295,40 @@ void launch_convert(const float* src, double* dst, int64_t n, cudaStream_t st) {
     note_launch(), k_convert<<<nblk(n), 256, 0, st>>>(src, dst, n);
 }
 
-// Launch the fused coarse cycle over levels lc..0 with a fully co-resident grid.
+template <typename T>
+void launch_dense_apply(const LevelDev<T>& L, const T* M, cudaStream_t st) {
+    const int n = (int)L.N;
+    const int warps_per_block = 8;
+    int blocks = (n + warps_per_block - 1) / warps_per_block;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    note_launch(), k_dense_apply<T><<<blocks, 32 * warps_per_block, 0, st>>>(n, M, L.bv, L.xv);
+}
+
+// Launch the fused coarse cycle over levels lc..ld with a fully co-resident grid.
 template <typename T, bool THREE>
-static void coarse_cycle(const LevelDev<T>* lev, int lc, const T* inv, int nu1, int nu2, cudaStream_t st) {
+static void coarse_cycle(const LevelDev<T>* lev, int lc, int ld, const T* M, int nu1, int nu2, LevelTable<T>& pack,
+                         cudaStream_t st) {
+    // one block per SM; a grid that cannot be co-resident makes the launch
+    // fail (cudaErrorCooperativeLaunchTooLarge), which the caller's error
+    // check reports
     static int grid = 0;
     if (grid == 0) {
-        int dev = 0, nsm = 148, per = 1;
+        int dev = 0, nsm = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_mg_coarse_cycle<T, THREE>, 256, 0);
-        grid = nsm * (per < 2 ? (per < 1 ? 1 : per) : 2);
+        grid = nsm;
     }
-    LevelPack<T> P;
-    for (int l = 0; l <= lc; ++l) P.l[l] = lev[l];
-    void* args[] = {(void*)&P, (void*)&lc, (void*)&inv, (void*)&nu1, (void*)&nu2};
+    // the level table lives in device memory (a by-value parameter indexed
+    // by a run-time level would be copied to every thread's stack); upload it
+    // only when a level's pointers or sizes changed since the last launch
+    if (std::memcmp(pack.host, lev, sizeof(LevelDev<T>) * (size_t)(lc + 1)) != 0) {
+        std::memcpy(pack.host, lev, sizeof(LevelDev<T>) * (size_t)(lc + 1));
+        cudaMemcpyAsync(pack.dev, pack.host, sizeof(LevelDev<T>) * (size_t)(lc + 1), cudaMemcpyHostToDevice, st);
+    }
+    const LevelDev<T>* P = pack.dev;
+    void* args[] = {(void*)&P, (void*)&lc, (void*)&ld, (void*)&M, (void*)&nu1, (void*)&nu2};
     note_launch();
-    cudaLaunchCooperativeKernel((const void*)k_mg_coarse_cycle<T, THREE>, dim3(grid), dim3(256), args, 0, st);
+    cudaLaunchCooperativeKernel((const void*)k_mg_coarse_cycle<T, THREE>, dim3(grid), dim3(kCoopThreads), args, 0, st);
 }
 
 template <typename T>
@@ -276,42 +338,62 @@ static int coop_level(const LevelDev<T>* lev, int nlev) {
     return lc;
 }
 
-// MultiGridSolver.f90:5-192 (V cycle, gam = 1), levels lev[0] coarsest.
+// MultiGridSolver.f90:5-192 (V cycle, gam = 1), levels lev[0] coarsest;
+// level ld is solved by the dense operator M.
 template <typename T>
-static void vcycle(LevelDev<T>* lev, int l, int lc, const T* inv, int nu1, int nu2, cudaStream_t st) {
+static void vcycle(LevelDev<T>* lev, int l, int lc, int ld, const T* M, int nu1, int nu2, LevelTable<T>& pack,
+                   cudaStream_t st) {
+    if (l == ld) { launch_dense_apply(lev[l], M, st); return; }
     if (l <= lc) {
-        if (lev[0].Nyg > 1) coarse_cycle<T, true>(lev, l, inv, nu1, nu2, st);
-        else coarse_cycle<T, false>(lev, l, inv, nu1, nu2, st);
+        if (lev[0].Nyg > 1) coarse_cycle<T, true>(lev, l, ld, M, nu1, nu2, pack, st);
+        else coarse_cycle<T, false>(lev, l, ld, M, nu1, nu2, pack, st);
         return;
     }
-    if (l == 0) { launch_coarse_solve(lev[0], inv, st); return; }
     const LevelDev<T>& F = lev[l];
     LevelDev<T>& Cc = lev[l - 1];
     launch_lo_smooth(F, nu1, st);
-    if (F.Nyg > 1) note_launch(), k_lo_residual<T, true><<<nblk(F.N), 256, 0, st>>>(F);
-    else note_launch(), k_lo_residual<T, false><<<nblk(F.N), 256, 0, st>>>(F);
+    if (F.Nyg > 1) {
+        if (F.cross) note_launch(), k_lo_residual<T, true, true><<<nblk(F.N), 256, 0, st>>>(F);
+        else note_launch(), k_lo_residual<T, true, false><<<nblk(F.N), 256, 0, st>>>(F);
+    } else {
+        if (F.cross) note_launch(), k_lo_residual<T, false, true><<<nblk(F.N), 256, 0, st>>>(F);
+        else note_launch(), k_lo_residual<T, false, false><<<nblk(F.N), 256, 0, st>>>(F);
+    }
     launch_restrict(F, Cc, (const T*)F.rv, Cc.bv, st);   // also zeroes Cc.xv
-    vcycle(lev, l - 1, lc, inv, nu1, nu2, st);
+    vcycle(lev, l - 1, lc, ld, M, nu1, nu2, pack, st);
     launch_prolong_add(F, Cc, (const T*)Cc.xv, F.xv, st);
     launch_lo_smooth(F, nu2, st);
 }
 
+// One V cycle from level l (its b set, its x zeroed by the caller) down to the
+// dense level ld; used to build the dense operator of a coarse level.
+template <typename T>
+void launch_mg_subcycle(LevelDev<T>* lev, int nlev, int l, int ld, const T* M, int nu1, int nu2, LevelTable<T>& pack,
+                        cudaStream_t st) {
+    const int lc = (nlev > 1) ? coop_level(lev, nlev) : -1;
+    vcycle(lev, l, lc, ld, M, nu1, nu2, pack, st);
+}
+
 // MultiGridSolveLinearSystem.f90:26-91: u = 0, then maxit cycles.
 template <typename T>
-void launch_mg_vcycle(LevelDev<T>* lev, int nlev, const T* coarse_inv, int nu1, int nu2, int maxit, cudaStream_t st) {
+void launch_mg_vcycle(LevelDev<T>* lev, int nlev, const T* M, int ld, int nu1, int nu2, int maxit, LevelTable<T>& pack,
+                      cudaStream_t st) {
     LevelDev<T>& F = lev[nlev - 1];
     launch_fill<T>(F.xv, T(0), F.N, st);
     const int lc = (nlev > 1) ? coop_level(lev, nlev) : -1;
     for (int it = 1; it <= maxit; ++it) {
         if (nlev == 1 && it > 1) break;
-        vcycle(lev, nlev - 1, lc, coarse_inv, nu1, nu2, st);
+        vcycle(lev, nlev - 1, lc, ld, M, nu1, nu2, pack, st);
     }
 }
 
 #define OW3D_INST(T)                                                                                         \
-    template void launch_mg_vcycle<T>(LevelDev<T>*, int, const T*, int, int, int, cudaStream_t);           \
+    template void launch_mg_vcycle<T>(LevelDev<T>*, int, const T*, int, int, int, int, LevelTable<T>&, cudaStream_t); \
+    template void launch_mg_subcycle<T>(LevelDev<T>*, int, int, int, const T*, int, int, LevelTable<T>&, cudaStream_t); \
+    template void launch_dense_apply<T>(const LevelDev<T>&, const T*, cudaStream_t);                        \
     template void launch_lo_matvec<T>(const LevelDev<T>&, const T*, T*, cudaStream_t);                      \
     template void launch_lo_smooth<T>(const LevelDev<T>&, int, cudaStream_t);                               \
+    template void launch_lo_pass<T>(const LevelDev<T>&, int, cudaStream_t);                                 \
     template void launch_restrict<T>(const LevelDev<T>&, const LevelDev<T>&, const T*, T*, cudaStream_t);   \
     template void launch_prolong_add<T>(const LevelDev<T>&, const LevelDev<T>&, const T*, T*, cudaStream_t); \
     template void launch_coarse_solve<T>(const LevelDev<T>&, const T*, cudaStream_t);                       \

@@ -1,12 +1,34 @@
 // Device-side pieces of the multigrid preconditioner shared by the per-phase
-// kernels (mg.cu) and the fused coarse-level kernel (mg_coarse.cu): row
-// evaluation of the low-order operator, the Gauss-Seidel phases and the grid
-// transfers, each as a function of one work item.
+// kernels and the fused coarse-level kernel (mg.cu): row evaluation of the
+// low-order operator, the Gauss-Seidel colour pass and the grid transfers,
+// each as a function of one work item.
 #pragma once
 #include "ow3d_internal.h"
 
 namespace ow3d {
 namespace mgdev {
+
+// Linear point index p (k fastest) -> 1-based (k, i, j) and column c.
+template <typename T>
+__device__ __forceinline__ void decomp(const LevelDev<T>& L, int64_t p, int& k, int64_t& c, int& i, int& j) {
+    const uint64_t cc = qdiv((uint64_t)p, L.mz);
+    k = (int)((uint64_t)p - cc * (uint64_t)L.Nzg) + 1;
+    const uint64_t jj = qdiv(cc, L.mx);
+    i = (int)(cc - jj * (uint64_t)L.Nxg) + 1;
+    j = (int)jj + 1;
+    c = (int64_t)cc;
+}
+
+// Column coefficients (1/h, h_x/h, h_y/h, c3), one 32- or 16-byte read.
+__device__ __forceinline__ void load_cf(const double* cf, int64_t c, double& ih, double& a, double& b, double& c3) {
+    const double2 u = __ldg(reinterpret_cast<const double2*>(cf) + 2 * c);
+    const double2 v = __ldg(reinterpret_cast<const double2*>(cf) + 2 * c + 1);
+    ih = u.x; a = u.y; b = v.x; c3 = v.y;
+}
+__device__ __forceinline__ void load_cf(const float* cf, int64_t c, float& ih, float& a, float& b, float& c3) {
+    const float4 u = __ldg(reinterpret_cast<const float4*>(cf) + c);
+    ih = u.x; a = u.y; b = u.z; c3 = u.w;
+}
 
 template <typename T>
 __device__ __forceinline__ int64_t IX(const LevelDev<T>& L, int k, int i, int j) {
@@ -22,17 +44,16 @@ __device__ __forceinline__ T sz(const LevelDev<T>& L, int o, int k, int m) { ret
 
 // Interior row (2 <= k <= Nzg-1, interior column). Returns A x at the row and
 // the diagonal coefficient.
-template <typename T, bool THREE>
+template <typename T, bool THREE, bool CROSS = true>
 __device__ T lo_interior(const LevelDev<T>& L, const T* x, int k, int i, int j, T& diag) {
     const int64_t c = (int64_t)(i - 1) + (int64_t)L.Nxg * (j - 1);
-    const T h = L.h[c], hx = L.hx[c], hxx = L.hxx[c];
-    const T hy = THREE ? L.hy[c] : T(0), hyy = THREE ? L.hyy[c] : T(0);
+    T s5, ca, cb, c3;
+    load_cf(L.cf, c, s5, ca, cb, c3);
     const T sg = __ldg(L.zs + k - 1), om = T(1) - sg;
     // DetermineTransformationConstantsArray with eta = 0
-    const T s5 = T(1) / h;
-    const T s2 = om * hx * s5;
-    const T s4 = om * hy * s5;
-    const T s3 = om * ((hxx + hyy) * s5 - T(2) * (hx * hx + hy * hy) * s5 * s5);
+    const T s2 = om * ca;
+    const T s4 = THREE ? om * cb : T(0);
+    const T s3 = om * c3;
     const T cz = s2 * s2 + s4 * s4 + s5 * s5;
     T acc = 0;
     // d2/dx2, d2/dy2 (centred 3-point, PrepareFullOperatorStencils.f90:213-231)
@@ -53,7 +74,7 @@ __device__ T lo_interior(const LevelDev<T>& L, const T* x, int k, int i, int j, 
     diag = sx(L, 2, i, 1) + (THREE ? sy(L, 2, j, 1) : T(0)) + s3 * sz(L, 1, k, 1) + cz * sz(L, 2, k, 1);
     // mixed d2/dxds: sum over y-planes J of Dz(Dx x), the x stencil at level 1
     // shifted away from the ghost corner columns.
-    if (s2 != T(0)) {
+    if (CROSS && s2 != T(0)) {
         T xz = 0;
         const int jlo = THREE ? j - 1 : j, jhi = THREE ? j + 1 : j;
         for (int jj = jlo; jj <= jhi; ++jj) {
@@ -71,7 +92,7 @@ __device__ T lo_interior(const LevelDev<T>& L, const T* x, int k, int i, int j, 
         acc += T(2) * s2 * xz;
         diag += T(2) * s2 * (sz(L, 1, k, 1) * sx(L, 1, i, 1));
     }
-    if (THREE && s4 != T(0)) {
+    if (THREE && CROSS && s4 != T(0)) {
         T yz = 0;
         for (int ii = i - 1; ii <= i + 1; ++ii) {
 #pragma unroll
@@ -95,10 +116,12 @@ __device__ T lo_interior(const LevelDev<T>& L, const T* x, int k, int i, int j, 
 template <typename T, bool THREE>
 __device__ T lo_bottom(const LevelDev<T>& L, const T* x, int i, int j, T& diag) {
     const int64_t c = (int64_t)(i - 1) + (int64_t)L.Nxg * (j - 1);
-    const T h = L.h[c], hx = L.hx[c];
+    const T hx = L.hx[c];
     const T hy = THREE ? L.hy[c] : T(0);
     const T om = T(1) - L.zs[1];
-    const T s5 = T(1) / h, s2 = om * hx * s5, s4 = om * hy * s5;
+    T s5, ca, cb, c3;
+    load_cf(L.cf, c, s5, ca, cb, c3);
+    const T s2 = om * ca, s4 = THREE ? om * cb : T(0);
     const T f = THREE ? (s5 + hx * s2 + hy * s4) : (s5 + hx * s2);
     T dz = 0;
 #pragma unroll
@@ -142,125 +165,131 @@ __device__ __forceinline__ bool is_ghost_col(const LevelDev<T>& L, int i, int j)
     return i == 1 || i == L.Nxg || (THREE && (j == 1 || j == L.Nyg));
 }
 
-// Gauss-Seidel value of a ghost-column row, (b - off-diagonal part) / diagonal.
-// It does not read the row's own current value, so a thread that needs the
-// updated ghost value can recompute it while another thread writes it.
-template <typename T, bool THREE>
-__device__ T ghost_gs(const LevelDev<T>& L, int k, int i, int j) {
-    const int64_t p = IX(L, k, i, j);
-    const bool gxx = (i == 1 || i == L.Nxg), gyy = THREE && (j == 1 || j == L.Nyg);
-    if ((gxx && gyy) || k == 1) return L.bv[p];
-    T off = 0, dg;
-    if (gxx) {
-        const int ia = (i == 1) ? 2 : L.Nxg - 1;
-        const int self = (i == 1) ? 0 : 2;
-#pragma unroll
-        for (int m = 0; m < 3; ++m) if (m != self) off += sx(L, 1, ia, m) * L.xv[IX(L, k, ia - 1 + m, j)];
-        dg = sx(L, 1, ia, self);
-    } else {
-        const int ja = (j == 1) ? 2 : L.Nyg - 1;
-        const int self = (j == 1) ? 0 : 2;
-#pragma unroll
-        for (int m = 0; m < 3; ++m) if (m != self) off += sy(L, 1, ja, m) * L.xv[IX(L, k, i, ja - 1 + m)];
-        dg = sy(L, 1, ja, self);
-    }
-    return (L.bv[p] - off) / dg;
-}
-
-template <typename T, bool THREE>
+template <typename T, bool THREE, bool CROSS = true>
 __device__ T lo_row(const LevelDev<T>& L, const T* x, int k, int i, int j, T& diag) {
     if (is_ghost_col<T, THREE>(L, i, j)) return lo_ghost<T, THREE>(L, x, k, i, j, diag);
     if (k == L.Nzg) { diag = T(1); return x[IX(L, k, i, j)]; }
     if (k == 1) return lo_bottom<T, THREE>(L, x, i, j, diag);
-    return lo_interior<T, THREE>(L, x, k, i, j, diag);
+    return lo_interior<T, THREE, CROSS>(L, x, k, i, j, diag);
 }
 
 
+// Iterates, right-hand sides and residuals are written by earlier phases of
+// the same fused coarse-level kernel, so they are read with ordinary
+// (coherent) loads, never through the read-only data path; only the stencil
+// and coefficient tables, constant for the whole solve, use __ldg.
 template <typename T>
-__device__ __forceinline__ T ro(const T* p) { return __ldg(p); }
+__device__ __forceinline__ T ro(const T* p) { return *p; }
 
-template <typename T, bool THREE>
+template <typename T, bool THREE, bool CROSS>
 __device__ __forceinline__ void residual_item(const LevelDev<T>& L, int64_t p) {
-    const int k = (int)(p % L.Nzg) + 1;
-    const int64_t c = p / L.Nzg;
-    const int i = (int)(c % L.Nxg) + 1, j = (int)(c / L.Nxg) + 1;
+    int k, i, j;
+    int64_t c;
+    decomp(L, p, k, c, i, j);
     T dg;
-    L.rv[p] = L.bv[p] - lo_row<T, THREE>(L, L.xv, k, i, j, dg);
+    L.rv[p] = L.bv[p] - lo_row<T, THREE, CROSS>(L, L.xv, k, i, j, dg);
 }
 
-// Special pass item q in [0, special_count): ghost-column rows first, then
-// the bottom rows of the interior columns (the reference's iGhost rows,
-// MGPreProcess.f90:376-439). A bottom row next to a ghost column uses the ghost
-// value of this pass, recomputed with ghost_gs (the ghost thread's arithmetic).
+// Gauss-Seidel value of the bottom row (k = 1) of interior column c = (i, j)
+// (BuildLinearSystemMatrix.f90:50-70), given rows 2 and 3 of the column; the
+// neighbours' row-2 values are read from X.
 template <typename T, bool THREE>
-__device__ __forceinline__ int64_t special_count(const LevelDev<T>& L) {
-    const int64_t nper = THREE ? (int64_t)2 * L.Nyg + 2 * (L.Nxg - 2) : 2;
-    return nper * L.Nzg + (int64_t)L.Nxg * L.Nyg;
-}
-template <typename T, bool THREE>
-__device__ void special_item(const LevelDev<T>& L, int64_t q) {
-    const int Nxg = L.Nxg, Nyg = L.Nyg, Nzg = L.Nzg;
-    const int64_t nper = THREE ? (int64_t)2 * Nyg + 2 * (Nxg - 2) : 2;
-    const int64_t nghost = nper * Nzg;
-
-        if (q < nghost) {
-            const int k = (int)(q % Nzg) + 1;
-            const int64_t e = q / Nzg;
-            int i, j;
-            if (!THREE) { i = (e == 0) ? 1 : Nxg; j = 1; }
-            else if (e < 2 * Nyg) { i = (e % 2 == 0) ? 1 : Nxg; j = (int)(e / 2) + 1; }
-            else { const int64_t f = e - 2 * Nyg; j = (f % 2 == 0) ? 1 : Nyg; i = (int)(f / 2) + 2; }
-            L.xv[IX(L, k, i, j)] = ghost_gs<T, THREE>(L, k, i, j);
-            return;
-        }
-        const int64_t c = q - nghost;
-        const int i = (int)(c % Nxg) + 1, j = (int)(c / Nxg) + 1;
-        if (is_ghost_col<T, THREE>(L, i, j)) return;
-        const T h = L.h[c], hx = L.hx[c];
-        const T hy = THREE ? L.hy[c] : T(0);
-        const T om = T(1) - L.zs[1], ih = T(1) / h;
-        const T s2 = om * hx * ih, s4 = om * hy * ih;
-        const T f = THREE ? (ih + hx * s2 + hy * s4) : (ih + hx * s2);
-        const T* xc = L.xv + c * Nzg;
-        const T dz = sz(L, 1, 2, 1) * xc[1] + sz(L, 1, 2, 2) * xc[2];
-        T dx = 0;
-#pragma unroll
-        for (int m = 0; m < 3; ++m) {
-            const int ii = i - 1 + m;
-            dx += sx(L, 1, i, m) * (is_ghost_col<T, THREE>(L, ii, j) ? ghost_gs<T, THREE>(L, 2, ii, j) : L.xv[IX(L, 2, ii, j)]);
-        }
-        T off = f * dz + hx * dx;
-        if (THREE) {
-            T dy = 0;
-#pragma unroll
-            for (int m = 0; m < 3; ++m) {
-                const int jj = j - 1 + m;
-                dy += sy(L, 1, j, m) * (is_ghost_col<T, THREE>(L, i, jj) ? ghost_gs<T, THREE>(L, 2, i, jj) : L.xv[IX(L, 2, i, jj)]);
-            }
-            off += hy * dy;
-        }
-        L.xv[c * Nzg] = (L.bv[c * Nzg] - off) / (f * sz(L, 1, 2, 0));
+__device__ __forceinline__ T bottom_value(const LevelDev<T>& L, const T* X, const T* B, int64_t c, int i, int j, T x2,
+                                          T x3) {
+    const int Nzg = L.Nzg, Nxg = L.Nxg;
+    const T hx = L.hx[c];
+    const T hy = THREE ? L.hy[c] : T(0);
+    T ih, ca, cb, c3;
+    load_cf(L.cf, c, ih, ca, cb, c3);
+    const T omb = T(1) - __ldg(L.zs + 1);
+    const T s2 = omb * ca, s4 = THREE ? omb * cb : T(0);
+    const T f = THREE ? (ih + hx * s2 + hy * s4) : (ih + hx * s2);
+    const T dz = sz(L, 1, 2, 1) * x2 + sz(L, 1, 2, 2) * x3;
+    T dx = sx(L, 1, i, 0) * X[(c - 1) * Nzg + 1] + sx(L, 1, i, 1) * x2;
+    dx += sx(L, 1, i, 2) * X[(c + 1) * Nzg + 1];
+    T off = f * dz + hx * dx;
+    if (THREE) {
+        T dy = sy(L, 1, j, 0) * X[(c - Nxg) * Nzg + 1] + sy(L, 1, j, 1) * x2;
+        dy += sy(L, 1, j, 2) * X[(c + Nxg) * Nzg + 1];
+        off += hy * dy;
     }
+    return (B[c * Nzg] - off) / (f * sz(L, 1, 2, 0));
+}
 
-// Colour phase, warp-cooperative form. A segment of S lanes (S a power of two
-// >= Nzg-2) owns one interior column of the colour; lane r holds row k = r+2.
-// Each lane forms its row's Gauss-Seidel update as an affine map of the new
-// value below it, x_k = q_k - g_k x_{k-1}; the chain over the column (the
-// bottom-to-top Gauss-Seidel order) is evaluated with a shuffle scan of the
-// composed maps. Loads are coalesced along the column. CROSS: the level has
-// mixed-derivative terms (sloping bottom). All 32 lanes of the warp call this
-// with the same `base` (the first column index of the warp).
+// Level-1 pass item q (levels with mixed-derivative terms relax their level-1
+// rows in a pass of their own): the bottom rows of the interior columns, then
+// the identity level-1 rows of the lateral ghost columns (corners excluded).
+template <typename T, bool THREE>
+__device__ __forceinline__ int64_t bottom_count(const LevelDev<T>& L) {
+    const int64_t nyi = THREE ? L.Nyg - 2 : 1;
+    return (int64_t)(L.Nxg - 2) * nyi + 2 * nyi + (THREE ? 2 * (int64_t)(L.Nxg - 2) : 0);
+}
+template <typename T, bool THREE>
+__device__ __forceinline__ void bottom_item(const LevelDev<T>& L, int64_t q) {
+    const int nxi = L.Nxg - 2, nyi = THREE ? L.Nyg - 2 : 1;
+    const int64_t nint = (int64_t)nxi * nyi;
+    T* X = L.xv;
+    if (q < nint) {
+        const int64_t tj = q / nxi;
+        const int i = 2 + (int)(q - tj * nxi), j = THREE ? 2 + (int)tj : 1;
+        const int64_t c = (int64_t)(i - 1) + (int64_t)L.Nxg * (j - 1);
+        X[c * L.Nzg] = bottom_value<T, THREE>(L, X, L.bv, c, i, j, X[c * L.Nzg + 1], X[c * L.Nzg + 2]);
+        return;
+    }
+    q -= nint;
+    int i, j;
+    if (q < 2 * nyi) { j = THREE ? 2 + (int)(q >> 1) : 1; i = (q & 1) ? L.Nxg : 1; }
+    else { q -= 2 * nyi; i = 2 + (int)(q >> 1); j = (q & 1) ? L.Nyg : 1; }
+    const int64_t c = (int64_t)(i - 1) + (int64_t)L.Nxg * (j - 1);
+    X[c * L.Nzg] = L.bv[c * L.Nzg];
+}
+
+// Colour pass, warp-cooperative form. A segment of S lanes (S a power of two
+// >= Nzg-2) owns one interior column (i, j) of the colour; lane r holds row
+// k = r+2. The column's task, in the order the oracle's device mode uses:
+//   1. identity corner columns diagonal to it (3-D): x = b,
+//   2. the lateral ghost columns it reads (i = 2 / Nxg-1, j = 2 / Nyg-1),
+//      relaxed from the current values,
+//   3. its bottom row (k = 1, kinematic bottom condition), lane 0,
+//   4. rows k = 2..Nzg-1 bottom to top: each lane forms its row's
+//      Gauss-Seidel update as an affine map of the new value below it,
+//      x_k = q_k - g_k x_{k-1}, and the chain is evaluated with a shuffle scan
+//      of the composed maps; the free-surface row (identity) last,
+//   5. its bottom row again, from the new column,
+//   6. the lateral ghost columns whose Neumann stencil contains the column
+//      (i = 2 or 3 / Nxg-1 or Nxg-2, likewise in j), from the new values.
+// A ghost column so ends every smoothing step consistent with both interior
+// columns of its stencil. Columns of one colour never read what another
+// column of that colour writes, so all tasks of a pass run concurrently.
+// Loads are coalesced along the column. CROSS: the level has mixed-derivative
+// terms (sloping bottom). All 32 lanes of the warp call this with the same
+// `base` (the first column index of the warp).
 template <typename T, bool THREE>
 __device__ __forceinline__ int64_t colour_count(const LevelDev<T>& L) {
     const int nxi = L.Nxg - 2, nyi = THREE ? L.Nyg - 2 : 1;
     const int ni = (nxi + 1) / 2, nj = (L.ncolor == 4) ? (nyi + 1) / 2 : nyi;
     return (int64_t)ni * nj;
 }
+
+// Per-lane constants of row k = r+2 (the same for every column of a level).
+template <typename T>
+struct RowConst { T om, z0, z1, z2, zz0, zz1, zz2; };
+
+template <typename T, int S>
+__device__ __forceinline__ RowConst<T> row_const(const LevelDev<T>& L) {
+    const int r = (threadIdx.x & 31) & (S - 1);
+    const int k = min(r + 2, L.Nzg - 1);
+    RowConst<T> c;
+    c.om = T(1) - __ldg(L.zs + k - 1);
+    c.z0 = sz(L, 1, k, 0); c.z1 = sz(L, 1, k, 1); c.z2 = sz(L, 1, k, 2);
+    c.zz0 = sz(L, 2, k, 0); c.zz1 = sz(L, 2, k, 1); c.zz2 = sz(L, 2, k, 2);
+    return c;
+}
+
 template <typename T, bool THREE, int S, bool CROSS>
-__device__ void colour_warp(const LevelDev<T>& L, int colour, int64_t base) {
+__device__ void colour_warp(const LevelDev<T>& L, int colour, int64_t base, const RowConst<T>& rk) {
     const int Nxg = L.Nxg, Nyg = L.Nyg, Nzg = L.Nzg, R = Nzg - 2;
     const int lane = threadIdx.x & 31, r = lane & (S - 1);
-    const int seg_per_warp = 32 / S;
     const int nxi = Nxg - 2, nyi = THREE ? Nyg - 2 : 1;
     // columns of this colour: every other i (and every other j with 4 colours)
     const bool four = (L.ncolor == 4);
@@ -268,120 +297,224 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int64_t base) {
     const int nj = four ? (nyi + 1) / 2 : nyi;
     const int64_t total = (int64_t)ni * nj;
     const unsigned segmask = 0xffffffffu;   // the whole warp runs the scan together
+    T* const X = L.xv;
+    const T* const B = L.bv;
 
-        const int64_t q = base + (lane / S);
-        bool act = q < total;
-        int i = 0, j = 1;
-        if (act) {
-            const int ti = (int)(q % ni), tj = (int)(q / ni);
-            if (four) {
-                j = THREE ? 2 + 2 * tj + (((colour >> 1) - 2) & 1) : 1;
-                i = 2 + 2 * ti + (((colour & 1) - 2) & 1);
-            } else {
-                j = THREE ? 2 + tj : 1;
-                i = 2 + 2 * ti + ((colour + j) & 1);    // (i + j) & 1 == colour
-            }
-            act = (i <= Nxg - 1) && (!THREE || j <= Nyg - 1);
+    const int64_t q = base + (lane / S);
+    bool act = q < total;
+    int i = 0, j = 1;
+    if (act) {
+        const int tj = (int)(q / ni), ti = (int)(q - (int64_t)tj * ni);
+        if (four) {
+            j = THREE ? 2 + 2 * tj + (((colour >> 1) - 2) & 1) : 1;
+            i = 2 + 2 * ti + (((colour & 1) - 2) & 1);
+        } else {
+            j = THREE ? 2 + tj : 1;
+            i = 2 + 2 * ti + ((colour + j) & 1);    // (i + j) & 1 == colour
         }
-        const bool rowact = act && (r < R);
-        const int k = r + 2;
-        T qv = 0, gv = 0, x1 = 0;
-        const int64_t c = (int64_t)(i - 1) + (int64_t)Nxg * (j - 1);
-        if (rowact) {
-            const T* xc = L.xv + c * Nzg;
-            const T h = L.h[c], hx = L.hx[c], hxx = L.hxx[c];
-            const T hy = THREE ? L.hy[c] : T(0), hyy = THREE ? L.hyy[c] : T(0);
-                const T ih = T(1) / h;
-            const T sg = __ldg(L.zs + k - 1), om = T(1) - sg;
-            const T s2 = om * hx * ih, s4 = om * hy * ih;
-            const T s3 = om * ((hxx + hyy) * ih - T(2) * (hx * hx + hy * hy) * ih * ih);
-            const T cz = s2 * s2 + s4 * s4 + ih * ih;
-            const T z0 = sz(L, 1, k, 0), z1 = sz(L, 1, k, 1), z2 = sz(L, 1, k, 2);
-            const T zz0 = sz(L, 2, k, 0), zz1 = sz(L, 2, k, 1), zz2 = sz(L, 2, k, 2);
-            T off = sx(L, 2, i, 0) * ro(L.xv + (c - 1) * Nzg + k - 1) + sx(L, 2, i, 2) * ro(L.xv + (c + 1) * Nzg + k - 1);
-            T diag = sx(L, 2, i, 1) + s3 * z1 + cz * zz1;
-            if (THREE) {
-                off += sy(L, 2, j, 0) * ro(L.xv + (c - Nxg) * Nzg + k - 1) + sy(L, 2, j, 2) * ro(L.xv + (c + Nxg) * Nzg + k - 1);
-                diag += sy(L, 2, j, 1);
-            }
-            T lo = s3 * z0 + cz * zz0, up = s3 * z2 + cz * zz2;
-            if (CROSS && s2 != T(0)) {
-                const int jlo = THREE ? j - 1 : j, jhi = THREE ? j + 1 : j;
-                T xz = 0;
-                for (int jj = jlo; jj <= jhi; ++jj) {
+        act = (i <= Nxg - 1) && (!THREE || j <= Nyg - 1);
+    }
+    const bool rowact = act && (r < R);
+    const int k = r + 2;
+    const int64_t c = (int64_t)(i - 1) + (int64_t)Nxg * (j - 1);
+    const T* xc = X + c * Nzg;
+
+    auto colidx = [&](int ii, int jj) -> int64_t { return (int64_t)(ii - 1) + (int64_t)Nxg * (jj - 1); };
+    // Relax ghost column cg: Neumann rows k = 2..Nzg with the 3-point stencil
+    // wa x(ca) + wb x(cb) + wg x(cg) = b, identity row k = 1. With post set,
+    // the value of this column (ca if own == 1, cb if own == 2) is the lane's
+    // new one (xnew for rows 2..Nzg-1, xfsn for the free-surface row).
+    auto relax_ghost = [&](int64_t cg, int64_t ca, T wa, int64_t cb, T wb, T wg, int own, bool post, T xnew, T xfsn) {
+        auto row = [&](int kk, T xo) {
+            const T va = (post && own == 1) ? xo : X[ca * Nzg + kk - 1];
+            const T vb = (post && own == 2) ? xo : X[cb * Nzg + kk - 1];
+            X[cg * Nzg + kk - 1] = (B[cg * Nzg + kk - 1] - (wa * va + wb * vb)) / wg;
+        };
+        if (act && r < R) row(k, xnew);
+        if (act && r == R - 1) row(Nzg, xfsn);
+        if (!CROSS && act && r == 0) X[cg * Nzg] = B[cg * Nzg];   // identity level-1 row
+    };
+    // the four ghost columns that can touch column (i, j); `pre` selects the
+    // ones this column reads, otherwise the ones whose stencil contains it
+    auto ghosts = [&](bool post, T xnew, T xfsn) {
+        if (!act) return;
+        if (i == 2 || (post && i == 3))
+            relax_ghost(colidx(1, j), colidx(2, j), sx(L, 1, 2, 1), colidx(3, j), sx(L, 1, 2, 2), sx(L, 1, 2, 0),
+                        i == 2 ? 1 : 2, post, xnew, xfsn);
+        if (i == Nxg - 1 || (post && i == Nxg - 2))
+            relax_ghost(colidx(Nxg, j), colidx(Nxg - 2, j), sx(L, 1, Nxg - 1, 0), colidx(Nxg - 1, j),
+                        sx(L, 1, Nxg - 1, 1), sx(L, 1, Nxg - 1, 2), i == Nxg - 1 ? 2 : 1, post, xnew, xfsn);
+        if (THREE) {
+            if (j == 2 || (post && j == 3))
+                relax_ghost(colidx(i, 1), colidx(i, 2), sy(L, 1, 2, 1), colidx(i, 3), sy(L, 1, 2, 2), sy(L, 1, 2, 0),
+                            j == 2 ? 1 : 2, post, xnew, xfsn);
+            if (j == Nyg - 1 || (post && j == Nyg - 2))
+                relax_ghost(colidx(i, Nyg), colidx(i, Nyg - 2), sy(L, 1, Nyg - 1, 0), colidx(i, Nyg - 1),
+                            sy(L, 1, Nyg - 1, 1), sy(L, 1, Nyg - 1, 2), j == Nyg - 1 ? 2 : 1, post, xnew, xfsn);
+        }
+    };
+    // 1. identity corner columns
+    if (THREE && act) {
+        const int cis[2] = {(i == 2) ? 1 : 0, (i == Nxg - 1) ? Nxg : 0};
+        const int cjs[2] = {(j == 2) ? 1 : 0, (j == Nyg - 1) ? Nyg : 0};
 #pragma unroll
-                    for (int kk = 0; kk < 3; ++kk) {
-                        const int kz = k - 1 + kk;
-                        int sh = 0;
-                        if (kz == 1) { if (i - 1 == 1) sh = 1; if (i + 1 == Nxg) sh = -1; }
-                        T dx = 0;
+        for (int a = 0; a < 2; ++a)
 #pragma unroll
-                        for (int m = 0; m < 3; ++m) {
-                            const int ii = i - 1 + sh + m;
-                            const T w = sx(L, 1, i - sh, m);
-                            if (ii == i && jj == j && kz >= 2 && kz <= Nzg - 1) {
-                                const T cf = T(2) * s2 * sz(L, 1, k, kk) * w;
-                                if (kk == 0) lo += cf; else if (kk == 1) diag += cf; else up += cf;
-                            } else {
-                                const T* src = L.xv + ((int64_t)(ii - 1) + (int64_t)Nxg * (jj - 1)) * Nzg + (kz - 1);
-                                dx += w * ((ii == i && jj == j) ? *src : ro(src));
-                            }
-                        }
-                        xz += sz(L, 1, k, kk) * dx;
-                    }
+            for (int bq = 0; bq < 2; ++bq)
+                if (cis[a] && cjs[bq]) {
+                    const int64_t cc = colidx(cis[a], cjs[bq]);
+                    for (int kk = r; kk < Nzg; kk += S) X[cc * Nzg + kk] = B[cc * Nzg + kk];
                 }
-                off += T(2) * s2 * xz;
-            }
-            if (THREE && CROSS && s4 != T(0)) {
-                T yz = 0;
-                for (int ii = i - 1; ii <= i + 1; ++ii) {
+    }
+    // 2. ghost columns this column reads, from the current values
+    ghosts(false, T(0), T(0));
+    __syncwarp();
+
+    // 3.-5. the column. Every lane of an active segment evaluates its row
+    // (lanes past the last interior row evaluate row Nzg-1 and discard it)
+    // and the pieces of the bottom row, loads first and without lane-dependent
+    // branches, so that one round trip to memory serves the whole task.
+    const int kr = (r < R) ? k : R + 1;
+    T qv = 0, gv = 0, x1 = 0;
+    T bf = 0, bhx = 0, bhy = 0, bb1 = 0, bl = 0, br = 0, bd = 0, bu = 0;
+    if (act) {
+        T ih, ca, cb, c3;
+        load_cf(L.cf, c, ih, ca, cb, c3);
+        const T xl = X[(c - 1) * Nzg + kr - 1], xr = X[(c + 1) * Nzg + kr - 1];
+        const T xd = THREE ? X[(c - Nxg) * Nzg + kr - 1] : T(0), xu = THREE ? X[(c + Nxg) * Nzg + kr - 1] : T(0);
+        const T x0 = xc[kr - 1];
+        const T xp = xc[kr];                   // old value of the row above (row Nzg: free surface)
+        const T bk = B[c * Nzg + kr - 1];
+        T x2o = 0, x3o = 0;
+        if (!CROSS) {
+            bhx = L.hx[c]; bhy = THREE ? L.hy[c] : T(0);
+            x2o = xc[1]; x3o = xc[2]; bb1 = B[c * Nzg];
+            bl = X[(c - 1) * Nzg + 1]; br = X[(c + 1) * Nzg + 1];
+            if (THREE) { bd = X[(c - Nxg) * Nzg + 1]; bu = X[(c + Nxg) * Nzg + 1]; }
+        } else {
+            x1 = xc[0];                        // bottom rows are fixed during this pass
+        }
+        const T om = rk.om;
+        const T s2 = om * ca, s4 = THREE ? om * cb : T(0);
+        const T s3 = om * c3;
+        const T cz = s2 * s2 + s4 * s4 + ih * ih;
+        T off = sx(L, 2, i, 0) * xl + sx(L, 2, i, 2) * xr;
+        T diag = sx(L, 2, i, 1) + s3 * rk.z1 + cz * rk.zz1;
+        if (THREE) {
+            off += sy(L, 2, j, 0) * xd + sy(L, 2, j, 2) * xu;
+            diag += sy(L, 2, j, 1);
+        }
+        T lo = s3 * rk.z0 + cz * rk.zz0, up = s3 * rk.z2 + cz * rk.zz2;
+        if (CROSS && s2 != T(0)) {
+            const int jlo = THREE ? j - 1 : j, jhi = THREE ? j + 1 : j;
+            T xz = 0;
+            for (int jj = jlo; jj <= jhi; ++jj) {
 #pragma unroll
-                    for (int kk = 0; kk < 3; ++kk) {
-                        const int kz = k - 1 + kk;
-                        int sh = 0;
-                        if (kz == 1) { if (j - 1 == 1) sh = 1; if (j + 1 == Nyg) sh = -1; }
-                        T dy = 0;
+                for (int kk = 0; kk < 3; ++kk) {
+                    const int kz = kr - 1 + kk;
+                    int sh = 0;
+                    if (kz == 1) { if (i - 1 == 1) sh = 1; if (i + 1 == Nxg) sh = -1; }
+                    T dx = 0;
 #pragma unroll
-                        for (int m = 0; m < 3; ++m) {
-                            const int jj = j - 1 + sh + m;
-                            const T w = sy(L, 1, j - sh, m);
-                            if (ii == i && jj == j && kz >= 2 && kz <= Nzg - 1) {
-                                const T cf = T(2) * s4 * sz(L, 1, k, kk) * w;
-                                if (kk == 0) lo += cf; else if (kk == 1) diag += cf; else up += cf;
-                            } else {
-                                const T* src = L.xv + ((int64_t)(ii - 1) + (int64_t)Nxg * (jj - 1)) * Nzg + (kz - 1);
-                                dy += w * ((ii == i && jj == j) ? *src : ro(src));
-                            }
+                    for (int m = 0; m < 3; ++m) {
+                        const int ii = i - 1 + sh + m;
+                        const T w = sx(L, 1, i - sh, m);
+                        if (ii == i && jj == j && kz <= Nzg - 1) {
+                            // own column: the term joins the scan (below / diagonal / above)
+                            const T cf2 = T(2) * s2 * sz(L, 1, kr, kk) * w;
+                            if (kk == 0) lo += cf2; else if (kk == 1) diag += cf2; else up += cf2;
+                        } else {
+                            const T* src = X + ((int64_t)(ii - 1) + (int64_t)Nxg * (jj - 1)) * Nzg + (kz - 1);
+                            dx += w * ((ii == i && jj == j) ? *src : ro(src));
                         }
-                        yz += sz(L, 1, k, kk) * dy;
                     }
+                    xz += sz(L, 1, kr, kk) * dx;
                 }
-                off += T(2) * s4 * yz;
             }
-            const T x0 = xc[k - 1];
-            const T xp = xc[k];                    // old value of the row above (row Nzg: free surface)
-            const T bk = L.bv[c * Nzg + k - 1];
-            // row update x0 + (b - (lo x_{k-1} + diag x0 + up xp + off)) / diag
-            const T id = T(1) / diag;
+            off += T(2) * s2 * xz;
+        }
+        if (THREE && CROSS && s4 != T(0)) {
+            T yz = 0;
+            for (int ii = i - 1; ii <= i + 1; ++ii) {
+#pragma unroll
+                for (int kk = 0; kk < 3; ++kk) {
+                    const int kz = kr - 1 + kk;
+                    int sh = 0;
+                    if (kz == 1) { if (j - 1 == 1) sh = 1; if (j + 1 == Nyg) sh = -1; }
+                    T dy = 0;
+#pragma unroll
+                    for (int m = 0; m < 3; ++m) {
+                        const int jj = j - 1 + sh + m;
+                        const T w = sy(L, 1, j - sh, m);
+                        if (ii == i && jj == j && kz <= Nzg - 1) {
+                            const T cf2 = T(2) * s4 * sz(L, 1, kr, kk) * w;
+                            if (kk == 0) lo += cf2; else if (kk == 1) diag += cf2; else up += cf2;
+                        } else {
+                            const T* src = X + ((int64_t)(ii - 1) + (int64_t)Nxg * (jj - 1)) * Nzg + (kz - 1);
+                            dy += w * ((ii == i && jj == j) ? *src : ro(src));
+                        }
+                    }
+                    yz += sz(L, 1, kr, kk) * dy;
+                }
+            }
+            off += T(2) * s4 * yz;
+        }
+        // row update x0 + (b - (lo x_{k-1} + diag x0 + up xp + off)) / diag
+        const T id = T(1) / diag;
+        if (r < R) {
             qv = x0 + (bk - diag * x0 - up * xp - off) * id;
             gv = lo * id;
-            if (r == 0) x1 = xc[0];                // bottom row: constant during the phase
         }
-        // inclusive scan of the affine maps x -> a x + b, a = -g, b = q (in row order)
-        T a = -gv, bb = qv;
-#pragma unroll
-        for (int d = 1; d < S; d <<= 1) {
-            const T ap = __shfl_up_sync(segmask, a, d, S);
-            const T bp = __shfl_up_sync(segmask, bb, d, S);
-            if (r >= d) { bb = a * bp + bb; a = a * ap; }
+        if (!CROSS) {
+            const T omb = T(1) - __ldg(L.zs + 1);
+            const T s2b = omb * ca, s4b = THREE ? omb * cb : T(0);
+            bf = THREE ? (ih + bhx * s2b + bhy * s4b) : (ih + bhx * s2b);
         }
-        x1 = __shfl_sync(segmask, x1, 0, S);
-        if (rowact) {
-            T* xc = L.xv + c * Nzg;
-            xc[k - 1] = a * x1 + bb;
-            if (r == R - 1) xc[Nzg - 1] = L.bv[c * Nzg + Nzg - 1];   // free-surface row
+        // bottom row from the current column
+        if (!CROSS) {
+            const T dz = sz(L, 1, 2, 1) * x2o + sz(L, 1, 2, 2) * x3o;
+            T dx = sx(L, 1, i, 0) * bl + sx(L, 1, i, 1) * x2o;
+            dx += sx(L, 1, i, 2) * br;
+            T boff = bf * dz + bhx * dx;
+            if (THREE) {
+                T dy = sy(L, 1, j, 0) * bd + sy(L, 1, j, 1) * x2o;
+                dy += sy(L, 1, j, 2) * bu;
+                boff += bhy * dy;
+            }
+            x1 = (bb1 - boff) / (bf * sz(L, 1, 2, 0));
         }
     }
+    // inclusive scan of the affine maps x -> a x + b, a = -g, b = q (in row order)
+    T a = -gv, bb = qv;
+#pragma unroll
+    for (int d = 1; d < S; d <<= 1) {
+        const T ap = __shfl_up_sync(segmask, a, d, S);
+        const T bp = __shfl_up_sync(segmask, bb, d, S);
+        if (r >= d) { bb = a * bp + bb; a = a * ap; }
+    }
+    const T xn = a * x1 + bb;                  // new value of row k
+    const T x2n = __shfl_sync(segmask, xn, 0, S);
+    const T x3n = __shfl_sync(segmask, xn, 1, S);
+    T* xw = X + c * Nzg;
+    if (rowact) xw[k - 1] = xn;
+    const T xfs = act ? B[c * Nzg + Nzg - 1] : T(0);
+    if (act && r == R - 1) xw[Nzg - 1] = xfs;  // free-surface row
+    // 5. bottom row again, from the new column (the neighbours are unchanged)
+    if (!CROSS && act && r == 0) {
+        const T dz = sz(L, 1, 2, 1) * x2n + sz(L, 1, 2, 2) * x3n;
+        T dx = sx(L, 1, i, 0) * bl + sx(L, 1, i, 1) * x2n;
+        dx += sx(L, 1, i, 2) * br;
+        T boff = bf * dz + bhx * dx;
+        if (THREE) {
+            T dy = sy(L, 1, j, 0) * bd + sy(L, 1, j, 1) * x2n;
+            dy += sy(L, 1, j, 2) * bu;
+            boff += bhy * dy;
+        }
+        xw[0] = (bb1 - boff) / (bf * sz(L, 1, 2, 0));
+    }
+    // 6. ghost columns whose stencil contains this column, from the new values
+    ghosts(true, xn, xfs);
+}
 
 // MGRestriction3DExplicit.f90:19-128 as a gather for coarse point p (also zeroes the coarse iterate).
 template <typename T>
@@ -391,9 +524,9 @@ __device__ void restrict_item(const LevelDev<T>& F, const LevelDev<T>& Cc, const
     const int Nzf = F.Nzg - 1, Nyf = F.Nyg - 2 * gy;
     const int xcz = Cc.xc, ycz = Cc.yc, zcz = Cc.zc;
 
-        const int kc = (int)(p % Cc.Nzg) + 1;
-        const int64_t cc = p / Cc.Nzg;
-        const int ic = (int)(cc % Cc.Nxg) + 1, jc = (int)(cc / Cc.Nxg) + 1;
+        int kc, ic, jc;
+        int64_t cc;
+        decomp(Cc, p, kc, cc, ic, jc);
         xc[p] = T(0);
         const bool ghost = kc == 1 || ic == 1 || ic == Cc.Nxg || (gy && (jc == 1 || jc == Cc.Nyg));
         if (ghost) { rc[p] = T(0); return; }
@@ -424,46 +557,42 @@ __device__ void restrict_item(const LevelDev<T>& F, const LevelDev<T>& Cc, const
         rc[p] = v;
     }
 
-// MGProlongation3DExplicit.f90:19-110 as a gather for fine point p, added to xf.
+// MGProlongation3DExplicit.f90:19-110 as a gather for fine point p, added to
+// xf: the sequential x, y, z interpolation sweeps are a tensor product, so the
+// value is the weighted sum over (at most) 2 x 2 x 2 coarse points with the
+// fine level's per-direction tables. The free-surface row, the bottom ghost
+// row and the ghost columns are not touched.
 template <typename T>
 __device__ void prolong_item(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* __restrict__ xc, T* __restrict__ xf, int64_t p) {
-
     const int gy = (F.Nyg > 1) ? 1 : 0;
-    const int XF = Cc.xc ? 2 : 1, YF = Cc.yc ? 2 : 1, ZF = Cc.zc ? 2 : 1;
-
-        const int kf = (int)(p % F.Nzg) + 1;
-        const int64_t cf = p / F.Nzg;
-        const int ifn = (int)(cf % F.Nxg) + 1, jf = (int)(cf / F.Nxg) + 1;
-        if (kf == 1 || kf == F.Nzg || ifn == 1 || ifn == F.Nxg || (gy && (jf == 1 || jf == F.Nyg))) return;
-        // coarse value at coincident fine indices
-        auto Cv = [&](int k, int i, int j) -> T {
-            if (k == F.Nzg) return T(0);  // free-surface layer is not injected
-            const int kc = 2 + (k - 2) / ZF, ic = 2 + (i - 2) / XF, jc = gy ? 2 + (j - 2) / YF : 1;
-            return xc[IX(Cc, kc, ic, jc)];
-        };
-        auto Px = [&](int k, int j) -> T {
-            if (k == F.Nzg) return T(0);
-            if (XF == 1 || ((ifn - 2) % 2) == 0) return Cv(k, ifn, j);
-            const double dW = F.x[ifn - 1] - F.x[ifn - 2], dE = F.x[ifn] - F.x[ifn - 1];
-            const T dxf = T(F.ix[ifn - 1]);
-            return (T(dE) * Cv(k, ifn - 1, j) + T(dW) * Cv(k, ifn + 1, j)) * dxf;
-        };
-        auto Py = [&](int k) -> T {
-            if (k == F.Nzg) return T(0);
-            if (!gy || YF == 1 || ((jf - 2) % 2) == 0) return Px(k, jf);
-            const double dS = F.y[jf - 1] - F.y[jf - 2], dN = F.y[jf] - F.y[jf - 1];
-            const T dyf = T(F.iy[jf - 1]);
-            return (T(dN) * Px(k, jf - 1) + T(dS) * Px(k, jf + 1)) * dyf;
-        };
-        T v;
-        if (ZF == 1 || ((kf - 2) % 2) == 0) v = Py(kf);
-        else {
-            const double dD = F.z[kf - 1] - F.z[kf - 2], dU = F.z[kf] - F.z[kf - 1];
-            const T dzf = T(F.iz[kf - 1]);
-            v = (T(dU) * Py(kf - 1) + T(dD) * Py(kf + 1)) * dzf;
-        }
-        xf[p] += v;
-    }
+    int kf, ifn, jf;
+    int64_t cfl;
+    decomp(F, p, kf, cfl, ifn, jf);
+    if (kf == 1 || kf == F.Nzg || ifn == 1 || ifn == F.Nxg || (gy && (jf == 1 || jf == F.Nyg))) return;
+    const int2 zi = __ldg(reinterpret_cast<const int2*>(F.piz) + (kf - 1));
+    const int2 xi = __ldg(reinterpret_cast<const int2*>(F.pix) + (ifn - 1));
+    const int2 yi = __ldg(reinterpret_cast<const int2*>(F.piy) + (gy ? jf - 1 : 0));
+    const T wz0 = __ldg(F.pwz + 2 * (kf - 1)), wz1 = __ldg(F.pwz + 2 * (kf - 1) + 1);
+    const T wx0 = __ldg(F.pwx + 2 * (ifn - 1)), wx1 = __ldg(F.pwx + 2 * (ifn - 1) + 1);
+    const T wy0 = __ldg(F.pwy + 2 * (gy ? jf - 1 : 0)), wy1 = __ldg(F.pwy + 2 * (gy ? jf - 1 : 0) + 1);
+    const int Ncz = Cc.Nzg, Ncx = Cc.Nxg;
+    auto C = [&](int kc, int ic, int jc) -> T {
+        return xc[(int64_t)(kc - 1) + (int64_t)Ncz * ((int64_t)(ic - 1) + (int64_t)Ncx * (jc - 1))];
+    };
+    auto Px = [&](int kc, int jc) -> T {
+        T v = wx0 * C(kc, xi.x, jc);
+        if (wx1 != T(0)) v += wx1 * C(kc, xi.y, jc);
+        return v;
+    };
+    auto Py = [&](int kc) -> T {
+        T v = wy0 * Px(kc, yi.x);
+        if (wy1 != T(0)) v += wy1 * Px(kc, yi.y);
+        return v;
+    };
+    T v = wz0 * Py(zi.x);
+    if (wz1 != T(0)) v += wz1 * Py(zi.y);
+    xf[p] += v;
+}
 
 // Coarsest level, row r of x = A^{-1} b.
 template <typename T>

@@ -40,6 +40,9 @@ template <typename T>
 struct MgSet {
     std::vector<LevelDev<T>> lev;
     T* coarse_inv = nullptr;
+    T* dense_op = nullptr;  // dense operator of level dense_level (coarse_inv when 0)
+    int dense_level = 0;
+    LevelTable<T> table;    // level table of the fused coarse-level kernel
     T* fine_b = nullptr;    // right-hand side of the finest level
     T* fine_x = nullptr;    // iterate of the finest level when not written in place
 };
@@ -152,6 +155,68 @@ int build_levels(ow3d_handle* H, MgSet<T>& S, bool alloc_fine_x) {
         };
         TRY(upload(H, &ix, recip(h.x))); TRY(upload(H, &iy, recip(h.y))); TRY(upload(H, &iz, recip(h.z)));
         d.ix = ix; d.iy = iy; d.iz = iz;
+        {
+            std::vector<double> cf(4 * h.h.size());
+            for (size_t q = 0; q < h.h.size(); ++q) {
+                const double ih = 1.0 / h.h[q];
+                const bool three = h.Nyg > 1;   // 2-D levels ignore any y-derivatives of h
+                const double hyq = three ? h.hy[q] : 0.0, hyyq = three ? h.hyy[q] : 0.0;
+                cf[4 * q + 0] = ih;
+                cf[4 * q + 1] = h.hx[q] * ih;
+                cf[4 * q + 2] = hyq * ih;
+                cf[4 * q + 3] = (h.hxx[q] + hyyq) * ih - 2.0 * (h.hx[q] * h.hx[q] + hyq * hyq) * ih * ih;
+            }
+            T* c;
+            TRY(upload(H, &c, cf));
+            d.cf = c;
+        }
+        d.mz = div_magic((uint64_t)d.Nzg);
+        d.mx = div_magic((uint64_t)d.Nxg);
+        d.pix = d.piy = d.piz = nullptr;
+        d.pwx = d.pwy = d.pwz = nullptr;
+        if (l > 0) {
+            // interpolation along one direction of MGProlongation3DExplicit.f90:62-110:
+            // coincident fine index n -> coarse 2 + (n-2)/F; in between ->
+            // (dE c(n-1) + dW c(n+1)) / (dW + dE). The free-surface row of the
+            // coarse grid is not injected (its contribution is zero).
+            const LevelHost& hc = H->G.levels[l - 1];
+            auto table = [&](const std::vector<double>& cf, int ng, int coarsened, bool zdir,
+                             std::vector<int>& idx, std::vector<double>& w) {
+                idx.assign(2 * (size_t)ng, 1); w.assign(2 * (size_t)ng, 0.0);
+                const int ff = coarsened ? 2 : 1;
+                for (int n = 2; n <= ng - 1; ++n) {
+                    auto cidx = [&](int m) { return 2 + (m - 2) / ff; };
+                    if (!coarsened || ((n - 2) % 2) == 0) {
+                        idx[2 * (n - 1)] = cidx(n); w[2 * (n - 1)] = 1.0;
+                        idx[2 * (n - 1) + 1] = cidx(n); w[2 * (n - 1) + 1] = 0.0;
+                    } else {
+                        const double dW = cf[n - 1] - cf[n - 2], dE = cf[n] - cf[n - 1];
+                        const double inv = 1.0 / (dW + dE);
+                        idx[2 * (n - 1)] = cidx(n - 1); w[2 * (n - 1)] = dE * inv;
+                        idx[2 * (n - 1) + 1] = cidx(n + 1); w[2 * (n - 1) + 1] = dW * inv;
+                        if (zdir && n + 1 == ng) w[2 * (n - 1) + 1] = 0.0;
+                    }
+                }
+            };
+            std::vector<int> ix_, iy_, iz_;
+            std::vector<double> wx_, wy_, wz_;
+            table(h.x, h.Nxg, hc.xc, false, ix_, wx_);
+            if (h.Nyg > 1) table(h.y, h.Nyg, hc.yc, false, iy_, wy_);
+            else { iy_.assign(2, 1); wy_.assign(2, 0.0); wy_[0] = 1.0; }
+            table(h.z, h.Nzg, hc.zc, true, iz_, wz_);
+            auto upi = [&](const int** dst, const std::vector<int>& v) -> int {
+                int* q;
+                int rr = dalloc(H, &q, v.size());
+                if (rr) return rr;
+                CK(cudaMemcpy(q, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice));
+                *dst = q;
+                return OW3D_OK;
+            };
+            TRY(upi(&d.pix, ix_)); TRY(upi(&d.piy, iy_)); TRY(upi(&d.piz, iz_));
+            T *a1, *a2, *a3;
+            TRY(upload(H, &a1, wx_)); TRY(upload(H, &a2, wy_)); TRY(upload(H, &a3, wz_));
+            d.pwx = a1; d.pwy = a2; d.pwz = a3;
+        }
         T* r;
         TRY(dalloc(H, &r, d.N)); d.rv = r;
         if (l < L - 1) {
@@ -160,6 +225,8 @@ int build_levels(ow3d_handle* H, MgSet<T>& S, bool alloc_fine_x) {
             d.xv = xv; d.bv = bv;
         }
     }
+    TRY(dalloc(H, &S.table.dev, (size_t)kMaxLevels));
+    std::memset((void*)S.table.host, 0, sizeof(S.table.host));
     LevelDev<T>& F = S.lev[L - 1];
     TRY(dalloc(H, &S.fine_b, F.N));
     F.bv = S.fine_b;
@@ -215,6 +282,50 @@ int coarse_inverse(ow3d_handle* H, MgSet<T>& S) {
     return OW3D_OK;
 }
 
+// Levels with at most this many points, below the finest, may be replaced by
+// one dense operator (row-major, n^2 values).
+constexpr int64_t kDenseMaxPoints = 2500;
+
+// The preconditioner is independent of the free surface (the low-order
+// operator linearises about eta = 0), so the V cycle from a coarse level ld
+// down to the coarsest level -- pre-smoothing, residual, restriction, the
+// recursion, prolongation and post-smoothing, started from x = 0 -- is a fixed
+// linear map b_ld -> x_ld. Build it once by applying that sub-cycle to every
+// unit vector, and apply it as one dense product: this replaces ~10 dependent
+// phases per level below ld with one.
+template <typename T>
+int dense_subcycle(ow3d_handle* H, MgSet<T>& S) {
+    S.dense_op = S.coarse_inv;
+    S.dense_level = 0;
+    const int L = (int)S.lev.size();
+    int ld = 0;
+    for (int l = 1; l <= L - 2; ++l) if (S.lev[l].N <= kDenseMaxPoints) ld = l;
+    if (ld == 0) return OW3D_OK;
+    LevelDev<T>* lev = S.lev.data();
+    const int64_t n = lev[ld].N;
+    T* Mcol;
+    TRY(dalloc(H, &Mcol, (size_t)(n * n)));
+    const T one = T(1);
+    for (int64_t c = 0; c < n; ++c) {
+        launch_fill<T>(lev[ld].bv, T(0), n, H->st);
+        launch_fill<T>(lev[ld].xv, T(0), n, H->st);
+        CK(cudaMemcpyAsync(lev[ld].bv + c, &one, sizeof(T), cudaMemcpyHostToDevice, H->st));
+        launch_mg_subcycle<T>(lev, L, ld, 0, S.coarse_inv, H->p.nu1, H->p.nu2, S.table, H->st);
+        CK(cudaMemcpyAsync(Mcol + c * n, lev[ld].xv, n * sizeof(T), cudaMemcpyDeviceToDevice, H->st));
+    }
+    CK(cudaStreamSynchronize(H->st));
+    CK(cudaGetLastError());
+    std::vector<T> col((size_t)(n * n));
+    CK(cudaMemcpy(col.data(), Mcol, col.size() * sizeof(T), cudaMemcpyDeviceToHost));
+    std::vector<T> row((size_t)(n * n));
+    for (int64_t c = 0; c < n; ++c)
+        for (int64_t r = 0; r < n; ++r) row[(size_t)(r * n + c)] = col[(size_t)(c * n + r)];
+    CK(cudaMemcpy(Mcol, row.data(), row.size() * sizeof(T), cudaMemcpyHostToDevice));
+    S.dense_op = Mcol;
+    S.dense_level = ld;
+    return OW3D_OK;
+}
+
 int alloc_state(ow3d_handle* H) {
     const size_t C = (size_t)H->G.C, N = (size_t)H->G.N;
     double** cs[] = {&H->E, &H->P, &H->W, &H->Ex, &H->Exx, &H->Ey, &H->Eyy, &H->Px, &H->Py,
@@ -240,7 +351,7 @@ void run_precond(ow3d_handle* H, MgSet<T>& S, const double* src, const double* d
     LevelDev<T>& F = lev[L - 1];
     launch_scale_copy_dev<T>(src, dscale, S.fine_b, F.N, H->st);
     F.xv = out;
-    launch_mg_vcycle<T>(lev, L, S.coarse_inv, H->p.nu1, H->p.nu2, H->p.maxit, H->st);
+    launch_mg_vcycle<T>(lev, L, S.dense_op, S.dense_level, H->p.nu1, H->p.nu2, H->p.maxit, S.table, H->st);
 }
 
 // Apply M^{-1} to src (times *dscale) into the FP64 vector dst.
@@ -387,8 +498,15 @@ int create_impl(const ow3d_params* p, const double* h, const double* hx, const d
     // multigrid
     H->nlev = (int)G.levels.size();
     if (H->nlev > 0) {
-        if (!H->mixed) { TRY(build_levels<double>(H.get(), H->mg64, true)); TRY(coarse_inverse<double>(H.get(), H->mg64)); }
-        else { TRY(build_levels<float>(H.get(), H->mg32, true)); TRY(coarse_inverse<float>(H.get(), H->mg32)); }
+        if (!H->mixed) {
+            TRY(build_levels<double>(H.get(), H->mg64, true));
+            TRY(coarse_inverse<double>(H.get(), H->mg64));
+            TRY(dense_subcycle<double>(H.get(), H->mg64));
+        } else {
+            TRY(build_levels<float>(H.get(), H->mg32, true));
+            TRY(coarse_inverse<float>(H.get(), H->mg32));
+            TRY(dense_subcycle<float>(H.get(), H->mg32));
+        }
     }
     // Krylov workspace
     H->m = p->GMRESmaxiterations;
@@ -579,6 +697,9 @@ int level_op_t(ow3d_handle* H, MgSet<T>& S, int l, int op, int nu, const double*
             cudaMemsetAsync(b, 0, n * sizeof(T), H->st);
             launch_prolong_add<T>(Lv, Cc, a, b, H->st); cudaStreamSynchronize(H->st); r = get(out, b, n);
         }
+    } else if (op == 5) {  // one smoother phase: colour pass nu, or the bottom-row pass (nu < 0)
+        r = put(a, in1, n); if (!r) r = put(b, in2, n);
+        if (!r) { Lv.xv = a; Lv.bv = b; launch_lo_pass<T>(Lv, nu, H->st); cudaStreamSynchronize(H->st); r = get(out, a, n); }
     } else if (op == 4 && l == 0) {  // coarse solve
         r = put(b, in1, n);
         if (!r) { Lv.bv = b; Lv.xv = a; launch_coarse_solve<T>(Lv, S.coarse_inv, H->st); cudaStreamSynchronize(H->st); r = get(out, a, n); }
@@ -648,7 +769,8 @@ int ow3d_estimate_bytes(const ow3d_params* p, size_t* bytes) {
     const double N = C * (p->Nz + 1);
     const double s = (p->precision == OW3D_PREC_MIXED) ? 4.0 : 8.0;
     const int m = p->GMRESmaxiterations;
-    double b = 8.0 * N * (m + 1) + s * N * m + 8.0 * N * 5 + 3.0 * s * N * 1.6 + 8.0 * C * 60;
+    double b = 8.0 * N * (m + 1) + s * N * m + 8.0 * N * 5 + 3.0 * s * N * 1.6 + 8.0 * C * 60 +
+               s * (double)kDenseMaxPoints * (double)kDenseMaxPoints * 2.0;
     *bytes = (size_t)(b * 1.05) + ((size_t)64 << 20);
     return OW3D_OK;
 }

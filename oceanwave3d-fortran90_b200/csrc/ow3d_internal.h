@@ -60,10 +60,28 @@ struct LevelDev {
     const T *h, *hx, *hxx, *hy, *hyy;  // Nxg*Nyg (ghost values as MGPreProcess sets them)
     const double *x, *y, *z;           // coordinates for transfer weights (FP64)
     const double *ix, *iy, *iz;        // 1/(x[i+1]-x[i-1]) etc. (computed as (dW+dE)) per index
+    // per column: 1/h, h_x/h, h_y/h, (h_xx+h_yy)/h - 2(h_x^2+h_y^2)/h^2 -- the
+    // eta = 0 sigma coefficients divided by (1 - sigma)
+    const T* cf;            // [Nxg*Nyg][4]
+    uint64_t mz, mx;        // division magics for Nzg and Nxg (see qdiv)
+    // prolongation from the next coarser level onto this one
+    // (MGProlongation3DExplicit.f90:19-110) as per-direction tables over this
+    // level's indices: coarse indices (1-based) and weights of the two coarse
+    // points that interpolate fine index n; weight 0 marks an unused point
+    const int *pix, *piy, *piz;        // [2*Nxg], [2*Nyg], [2*Nzg]
+    const T *pwx, *pwy, *pwz;          // same layout
     T* xv;                  // iterate
     T* bv;                  // right-hand side
     T* rv;                  // residual
 };
+
+// n / d as a 64-bit multiply-high with m = floor((2^64-1)/d) + 1: exact for
+// every n < 2^48 and 2 <= d < 2^16 (the error term n*(m*d - 2^64) / 2^64 stays
+// below 1/d), and a few instructions instead of a 64-bit division.
+inline uint64_t div_magic(uint64_t d) { return ~0ull / d + 1ull; }
+#ifdef __CUDACC__
+__device__ __forceinline__ uint64_t qdiv(uint64_t n, uint64_t m) { return __umul64hi(n, m); }
+#endif
 
 // ------------------------------------------------ Krylov device scalars
 struct KrylovState {
@@ -90,13 +108,30 @@ void launch_ho_matvec(const HoGrid& g, const Surface& s, const TIN* phi, const d
                       double* y, int mode, cudaStream_t st);
 
 // Multigrid (T = double or float)
+// Device copy of the level table for the fused coarse-level kernel, with the
+// host image of what was last uploaded.
 template <typename T>
-void launch_mg_vcycle(LevelDev<T>* lev, int nlev, const T* coarse_inv, int nu1, int nu2, int maxit,
-                      cudaStream_t st);
+struct LevelTable {
+    LevelDev<T>* dev = nullptr;
+    LevelDev<T> host[kMaxLevels];
+};
+
+// M: dense operator of level ld (the coarsest level's inverse when ld = 0).
+template <typename T>
+void launch_mg_vcycle(LevelDev<T>* lev, int nlev, const T* M, int ld, int nu1, int nu2, int maxit,
+                      LevelTable<T>& pack, cudaStream_t st);
+template <typename T>
+void launch_mg_subcycle(LevelDev<T>* lev, int nlev, int l, int ld, const T* M, int nu1, int nu2,
+                        LevelTable<T>& pack, cudaStream_t st);
+template <typename T>
+void launch_dense_apply(const LevelDev<T>& L, const T* M, cudaStream_t st);
 template <typename T>
 void launch_lo_matvec(const LevelDev<T>& L, const T* x, T* y, cudaStream_t st);
 template <typename T>
 void launch_lo_smooth(const LevelDev<T>& L, int nu, cudaStream_t st);
+// One smoother phase: colour pass `colour`, or the bottom-row pass (colour < 0).
+template <typename T>
+void launch_lo_pass(const LevelDev<T>& L, int colour, cudaStream_t st);
 template <typename T>
 void launch_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* rf, T* rc, cudaStream_t st);
 template <typename T>

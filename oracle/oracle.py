@@ -64,6 +64,7 @@ def lib():
         L.orc_level_csr.argtypes = [V, C.c_int, I, I, D]
         L.orc_level_matvec.argtypes = [V, C.c_int, D, D]
         L.orc_level_smooth.argtypes = [V, C.c_int, D, D, C.c_int]
+        L.orc_level_pass.argtypes = [V, C.c_int, C.c_int, D, D]
         L.orc_restrict.argtypes = [V, C.c_int, D, D]
         L.orc_prolong.argtypes = [V, C.c_int, D, D]
         L.orc_coarse_solve.argtypes = [V, D]
@@ -167,6 +168,10 @@ class Oracle:
 
     def level_smooth(self, l, x, b, nu=1):
         x = _c(x).copy(); b = _c(b); lib().orc_level_smooth(self.h, l, _p(x), _p(b), nu); return x
+
+    def level_pass(self, l, colour, x, b):
+        """One device-ordering smoother phase: colour pass, or the bottom-row pass (colour < 0)."""
+        x = _c(x).copy(); b = _c(b); lib().orc_level_pass(self.h, l, colour, _p(x), _p(b)); return x
 
     def restrict(self, lf, rf):
         rc = np.zeros(self.level_size(lf - 1)); lib().orc_restrict(self.h, lf, _p(_c(rf)), _p(rc)); return rc

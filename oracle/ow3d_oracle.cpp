@@ -36,6 +36,7 @@ struct Level {
     vector<int> ighost;       // 1-based global row indices (MGPreProcess.f90:376-439)
     vector<double> LU; vector<int> piv;  // coarsest level dense LU
     int ncolor = 0;
+    int cross = 0;            // mixed-derivative terms present (h_x or h_y nonzero)
     // work vectors for the V-cycle
     vector<double> x, b, r;
 };
@@ -338,6 +339,7 @@ static void assemble_level(const Sim& s, Level& Lv) {
     // diagonal neighbour columns only through the cross terms.
     double hmax = 0; for (size_t c = 0; c < G.hx.size(); ++c) hmax = std::max(hmax, std::max(std::fabs(G.hx[c]), std::fabs(G.hy[c])));
     Lv.ncolor = (Nyg > 1 && Nxg > 1) ? (hmax > 0 ? 4 : 2) : 2;
+    Lv.cross = hmax > 0 ? 1 : 0;
 }
 
 static void dense_lu(Level& Lv) {
@@ -391,29 +393,79 @@ static void gs_lex(const CSR& A, double* x, const double* b) { for (int r = 0; r
 static void gs_special(const Level& Lv, double* x, const double* b) {
     for (int g1 : Lv.ighost) gs_row(Lv.A, g1 - 1, x, b);
 }
-// Device-matched smoother phases. S1: all rows of ghost columns; S2: bottom
-// rows of interior columns; colour c: interior rows (k = 2..Nzg) of interior
-// columns of colour c, bottom-to-top.
-static void dm_special(const Level& Lv, double* x, const double* b) {
+// Device-matched smoother (mode 1). One smoothing step is one pass per colour
+// over the interior columns of that colour (2 colours by (i+j) parity, or 4 by
+// (i, j) parities when mixed-derivative terms couple diagonal columns). The
+// task of one interior column (i, j), in this order:
+//   1. identity corner columns diagonal to it (3-D; (2,2) owns (1,1), ...),
+//   2. the lateral ghost columns it reads (i = 2 -> (1, j), i = Nxg-1 ->
+//      (Nxg, j), likewise in j), relaxed from the current values,
+//   3. its bottom row (k = 1, the kinematic bottom condition),
+//   4. its rows k = 2..Nzg, bottom to top,
+//   5. its bottom row again (consistent with the new column),
+//   6. the lateral ghost columns whose Neumann stencil contains the column
+//      (i = 2 or 3 -> (1, j); i = Nxg-1 or Nxg-2 -> (Nxg, j); likewise in j).
+// Each ghost column is thus relaxed after each of its two interior neighbours
+// and ends every smoothing step consistent with both, as the reference's
+// trailing GaussSeidelSpecialPoints pass leaves it.
+// On levels with mixed-derivative terms the row k = 2 of a column next to a
+// ghost column reads level-1 values of the columns two to the side (the
+// shifted stencil of ConstructTableCrossDerivatives at the ghost level): the
+// bottom rows of same-colour interior columns and the (identity) level-1 rows
+// of ghost columns other same-colour tasks relax. There all level-1 rows --
+// interior bottoms and ghost identities -- are relaxed in a separate pass
+// before the first and after every colour sweep instead (steps 3 and 5 and the
+// ghosts' level-1 rows dropped from the colour passes), so that no task reads
+// what another task of its pass writes.
+static void dm_pass(const Level& Lv, int colour, double* x, const double* b) {
     const LevelGrid& G = Lv.G; const int Nzg = G.Nzg, Nxg = G.Nxg, Nyg = G.Nyg;
-    bool three = Nxg > 1 && Nyg > 1;
-    auto ghostcol = [&](int i, int j) { return (Nxg > 1 && (i == 1 || i == Nxg)) || (three && (j == 1 || j == Nyg)); };
-    for (int j = 1; j <= Nyg; ++j) for (int i = 1; i <= Nxg; ++i)
-        if (ghostcol(i, j)) for (int k = 1; k <= Nzg; ++k) gs_row(Lv.A, (k - 1) + Nzg * ((i - 1) + Nxg * (j - 1)), x, b);
-    for (int j = 1; j <= Nyg; ++j) for (int i = 1; i <= Nxg; ++i)
-        if (!ghostcol(i, j)) gs_row(Lv.A, Nzg * ((i - 1) + Nxg * (j - 1)), x, b);
-}
-static void dm_sweep(const Level& Lv, double* x, const double* b) {
-    const LevelGrid& G = Lv.G; const int Nzg = G.Nzg, Nxg = G.Nxg, Nyg = G.Nyg;
-    bool three = Nxg > 1 && Nyg > 1;
-    for (int c = 0; c < Lv.ncolor; ++c)
-        for (int j = 1; j <= Nyg; ++j) for (int i = 1; i <= Nxg; ++i) {
-            bool ghost = (Nxg > 1 && (i == 1 || i == Nxg)) || (three && (j == 1 || j == Nyg));
-            if (ghost) continue;
-            int col = (Lv.ncolor == 4) ? ((i & 1) + 2 * (j & 1)) : ((i + j) & 1);
-            if (col != c) continue;
-            for (int k = 2; k <= Nzg; ++k) gs_row(Lv.A, (k - 1) + Nzg * ((i - 1) + Nxg * (j - 1)), x, b);
+    const bool three = Nxg > 1 && Nyg > 1;
+    const bool fuse_bottom = !Lv.cross;
+    auto col_rows = [&](int i, int j, int k0, int k1) {
+        for (int k = k0; k <= k1; ++k) gs_row(Lv.A, (k - 1) + Nzg * ((i - 1) + Nxg * (j - 1)), x, b);
+    };
+    const int j0 = three ? 2 : 1, j1 = three ? Nyg - 1 : 1;
+    for (int j = j0; j <= j1; ++j)
+        for (int i = 2; i <= Nxg - 1; ++i) {
+            const int col = (Lv.ncolor == 4) ? ((i & 1) + 2 * (j & 1)) : ((i + j) & 1);
+            if (col != colour) continue;
+            if (three) {
+                const int cis[2] = {i == 2 ? 1 : 0, i == Nxg - 1 ? Nxg : 0};
+                const int cjs[2] = {j == 2 ? 1 : 0, j == Nyg - 1 ? Nyg : 0};
+                for (int ci : cis) for (int cj : cjs) if (ci && cj) col_rows(ci, cj, 1, Nzg);
+            }
+            const int g0 = fuse_bottom ? 1 : 2;   // first ghost row this pass relaxes
+            if (i == 2) col_rows(1, j, g0, Nzg);
+            if (i == Nxg - 1) col_rows(Nxg, j, g0, Nzg);
+            if (three && j == 2) col_rows(i, 1, g0, Nzg);
+            if (three && j == Nyg - 1) col_rows(i, Nyg, g0, Nzg);
+            col_rows(i, j, fuse_bottom ? 1 : 2, Nzg);
+            if (fuse_bottom) col_rows(i, j, 1, 1);
+            if (i == 2 || i == 3) col_rows(1, j, g0, Nzg);
+            if (i == Nxg - 1 || i == Nxg - 2) col_rows(Nxg, j, g0, Nzg);
+            if (three && (j == 2 || j == 3)) col_rows(i, 1, g0, Nzg);
+            if (three && (j == Nyg - 1 || j == Nyg - 2)) col_rows(i, Nyg, g0, Nzg);
         }
+}
+// Level-1 rows: bottom rows of all interior columns (each reads only rows >= 2)
+// and the identity rows of the lateral ghost columns (corners excluded).
+static void dm_bottoms(const Level& Lv, double* x, const double* b) {
+    const LevelGrid& G = Lv.G; const int Nzg = G.Nzg, Nxg = G.Nxg, Nyg = G.Nyg;
+    const bool three = Nxg > 1 && Nyg > 1;
+    const int j0 = three ? 2 : 1, j1 = three ? Nyg - 1 : 1;
+    auto row1 = [&](int i, int j) { gs_row(Lv.A, Nzg * ((i - 1) + Nxg * (j - 1)), x, b); };
+    for (int j = j0; j <= j1; ++j)
+        for (int i = 2; i <= Nxg - 1; ++i) row1(i, j);
+    for (int j = j0; j <= j1; ++j) { row1(1, j); row1(Nxg, j); }
+    if (three)
+        for (int i = 2; i <= Nxg - 1; ++i) { row1(i, 1); row1(i, Nyg); }
+}
+static void dm_smooth(const Level& Lv, double* x, const double* b, int nu) {
+    if (Lv.cross) dm_bottoms(Lv, x, b);
+    for (int s = 0; s < nu; ++s) {
+        for (int c = 0; c < Lv.ncolor; ++c) dm_pass(Lv, c, x, b);
+        if (Lv.cross) dm_bottoms(Lv, x, b);
+    }
 }
 static void csr_mv(const CSR& A, const double* x, double* y) {
 #pragma omp parallel for schedule(static)
@@ -516,7 +568,7 @@ static void mg_solver(Sim& s, int k, double* x, const double* b) {
     }
     auto smooth = [&](int nu) {
         if (s.mode == 0) { gs_special(Lv, x, b); for (int i = 0; i < nu; ++i) { gs_lex(Lv.A, x, b); gs_special(Lv, x, b); } }
-        else { dm_special(Lv, x, b); for (int i = 0; i < nu; ++i) { dm_sweep(Lv, x, b); dm_special(Lv, x, b); } }
+        else dm_smooth(Lv, x, b, nu);
     };
     smooth(s.p.nu1);
     size_t n = Lv.A.n;
@@ -1243,10 +1295,14 @@ void orc_level_csr(void* sv, int l, int* rp, int* ci, double* v) {
     std::copy(A.rp.begin(), A.rp.end(), rp); std::copy(A.ci.begin(), A.ci.end(), ci); std::copy(A.v.begin(), A.v.end(), v);
 }
 void orc_level_matvec(void* sv, int l, const double* x, double* y) { csr_mv(((Sim*)sv)->lev[l].A, x, y); }
+void orc_level_pass(void* sv, int l, int colour, double* x, const double* b) {
+    Sim* s = (Sim*)sv; Level& Lv = s->lev[l];
+    if (colour < 0) dm_bottoms(Lv, x, b); else dm_pass(Lv, colour, x, b);
+}
 void orc_level_smooth(void* sv, int l, double* x, const double* b, int nu) {
     Sim* s = (Sim*)sv; Level& Lv = s->lev[l];
     if (s->mode == 0) { gs_special(Lv, x, b); for (int i = 0; i < nu; ++i) { gs_lex(Lv.A, x, b); gs_special(Lv, x, b); } }
-    else { dm_special(Lv, x, b); for (int i = 0; i < nu; ++i) { dm_sweep(Lv, x, b); dm_special(Lv, x, b); } }
+    else dm_smooth(Lv, x, b, nu);
 }
 void orc_restrict(void* sv, int lf, const double* rf, double* rc) { Sim* s = (Sim*)sv; restrict_(*s, s->lev[lf], s->lev[lf - 1], rf, rc); }
 void orc_prolong(void* sv, int lf, double* pf, const double* pc) { Sim* s = (Sim*)sv; prolong_(*s, s->lev[lf], s->lev[lf - 1], pf, pc); }

@@ -78,6 +78,15 @@ def main():
     lines = []
     for name, arrs in sorted(sets.items()):
         f = HERE / f"{name}.npz"
+        if f.exists():
+            # keep a fixture whose content is unchanged up to reduction-order rounding
+            with np.load(f) as old:
+                same = sorted(old.files) == sorted(arrs) and all(
+                    old[k].shape == np.shape(v) and np.allclose(old[k], v, rtol=1e-12, atol=1e-14 * max(1.0, np.max(np.abs(v))))
+                    for k, v in arrs.items())
+            if same:
+                lines.append(f"{hashlib.sha256(f.read_bytes()).hexdigest()}  {f.name}")
+                continue
         np.savez_compressed(f, **arrs)
         lines.append(f"{hashlib.sha256(f.read_bytes()).hexdigest()}  {f.name}")
     (HERE / "MANIFEST.txt").write_text("\n".join(lines) + "\n")
