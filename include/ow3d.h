@@ -206,6 +206,22 @@ int ow3d_matvec(ow3d_handle* h, const double* phi, double* y,
                 const double* E, const double* Ex, const double* Exx,
                 const double* Ey, const double* Eyy);
 
+/* Allocation-free residual check -- no counterpart in the reference, which
+ * has no device. d_res = d_rhs - A(eta) d_phi with the high-order operator
+ * and *norm2 = ||d_res||_2 (host scalar). Every array is caller-owned DEVICE
+ * memory of the handle's device (d_Ey, d_Eyy may be NULL in 2-D; the surface
+ * is ignored for a linear run). The call allocates nothing: its only scratch
+ * is a fixed file-scope device array (1024 partial sums) whose address is
+ * looked up once per device on the first call -- make one call before
+ * capturing the handle's stream into a graph. Vectors longer than 2^31-1
+ * elements are rejected with OW3D_ERR_UNSUPPORTED. Calls that overlap in time
+ * on one device share that scratch and must be serialised by the caller.
+ * Runs on the handle's stream and returns after the norm is on the host. */
+int ow3d_residual_device_noalloc(ow3d_handle* h, const double* d_rhs, const double* d_phi,
+                                 const double* d_E, const double* d_Ex, const double* d_Exx,
+                                 const double* d_Ey, const double* d_Eyy,
+                                 double* d_res, double* norm2);
+
 /* u = M^{-1} r: maxit V-cycles of the low-order multigrid preconditioner from
  * u = 0 (MultiGridSolveLinearSystem.f90:1-95). Host pointers. */
 int ow3d_precondition(ow3d_handle* h, const double* r, double* u);

@@ -137,6 +137,7 @@ def declare(lib):
                                         C.c_void_p, C.c_void_p, C.c_void_p, _I]),
         "ow3d_matvec": (C.c_int, [H, _D, _D, _D, _D, _D, _D, _D]),
         "ow3d_precondition": (C.c_int, [H, _D, _D]),
+        "ow3d_residual_device_noalloc": (C.c_int, [H] + [C.c_void_p] * 8 + [_D]),
         "ow3d_set_state": (C.c_int, [H, _D, _D, _D, _D, C.c_double]),
         "ow3d_get_state": (C.c_int, [H, _D, _D, _D, _D, _D]),
         "ow3d_put_surface": (C.c_int, [H, _D, _D]),

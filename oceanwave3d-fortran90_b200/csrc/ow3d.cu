@@ -819,6 +819,25 @@ int ow3d_matvec(ow3d_handle* H, const double* phi, double* y, const double* E, c
     return OW3D_OK;
 }
 
+int ow3d_residual_device_noalloc(ow3d_handle* H, const double* d_rhs, const double* d_phi, const double* d_E,
+                                 const double* d_Ex, const double* d_Exx, const double* d_Ey, const double* d_Eyy,
+                                 double* d_res, double* norm2) {
+    if (!H || !d_rhs || !d_phi || !d_res || !norm2) return OW3D_ERR_BAD_INPUT;
+    CK(cudaSetDevice(H->dev));
+    const bool nl = H->p.LinearONOFF == 1;
+    if (nl && (!d_E || !d_Ex || !d_Exx || (H->G.three && (!d_Ey || !d_Eyy)))) {
+        g_last_error = "ow3d_residual_device_noalloc: the nonlinear operator needs E, Ex, Exx (and Ey, Eyy in 3-D)";
+        return OW3D_ERR_BAD_INPUT;
+    }
+    const Surface s = nl ? Surface{d_E, d_Ex, d_Exx, d_Ey, d_Eyy} : Surface{nullptr, nullptr, nullptr, nullptr, nullptr};
+    launch_ho_matvec<double>(H->hg, s, d_phi, nullptr, d_rhs, d_res, 1, H->st);
+    CK(cudaGetLastError());
+    std::string err;
+    const int r = noalloc_norm2(H->dev, d_res, H->G.N, norm2, H->st, err);
+    if (r) g_last_error = err;
+    return r;
+}
+
 int ow3d_precondition(ow3d_handle* H, const double* r, double* u) {
     if (!H || !r || !u) return OW3D_ERR_BAD_INPUT;
     CK(cudaSetDevice(H->dev));

@@ -10,6 +10,7 @@
 #include <atomic>
 #include <cstdint>
 #include <cstddef>
+#include <string>
 #include <cuda_runtime.h>
 #include "../../include/ow3d.h"
 
@@ -82,6 +83,10 @@ inline uint64_t div_magic(uint64_t d) { return ~0ull / d + 1ull; }
 #ifdef __CUDACC__
 __device__ __forceinline__ uint64_t qdiv(uint64_t n, uint64_t m) { return __umul64hi(n, m); }
 #endif
+
+// sqrt(sum y^2) of a device vector using only fixed file-scope device scratch
+// (noalloc.cu); result written to host memory, stream synchronised.
+int noalloc_norm2(int dev, const double* d_y, int64_t n, double* host_norm2, cudaStream_t st, std::string& err);
 
 // ------------------------------------------------ Krylov device scalars
 struct KrylovState {
