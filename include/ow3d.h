@@ -264,6 +264,15 @@ int ow3d_step(ow3d_handle* h, int nsteps);
  * the handle's stream (milliseconds). */
 int ow3d_step_timed(ow3d_handle* h, int nsteps, double* device_ms);
 
+/* Advance n independent simulations together -- no counterpart in the
+ * reference, which runs one simulation per process. Handle i takes nsteps[i]
+ * RK4 steps; one host thread drives each handle's stream, so their kernels
+ * overlap on the device. status[i] and wall_ms[i] (either may be NULL)
+ * receive each handle's ow3d_step status and host wall time in milliseconds.
+ * The handles must be distinct. Returns the most severe status. Each result
+ * is the same as ow3d_step on that handle alone (handles share no state). */
+int ow3d_step_batch(ow3d_handle* const* hs, int n, const int* nsteps, int* status, double* wall_ms);
+
 int ow3d_get_stats(const ow3d_handle* h, ow3d_stats* s);
 int ow3d_reset_stats(ow3d_handle* h);
 

@@ -216,3 +216,6 @@ class Simulation:
 
 def version():
     return lib().ow3d_version().decode()
+
+
+from . import serving  # noqa: E402,F401  (needs Simulation and OW3DError above)

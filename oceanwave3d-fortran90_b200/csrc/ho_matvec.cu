@@ -213,10 +213,15 @@ void launch_impl(const HoGrid& g, const Surface& s, const TIN* phi, const double
     dim3 blk(BX, BY), grd((g.Nxg + BX - 1) / BX, (g.Nyg + BY - 1) / BY);
     const int NZP = g.Nzg | 1;
     size_t smem = (size_t)(THREE ? BY + 9 : 1) * (BX + 9) * NZP * sizeof(double);
-    static bool attr = false;
-    if (!attr) {
+    // the shared-memory opt-in is per device; setting it twice is harmless,
+    // so concurrent first launches from several host threads need no lock
+    static std::atomic<unsigned long long> attr_set{0ull};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(attr_set.load(std::memory_order_relaxed) & bit)) {
         cudaFuncSetAttribute(k_ho_matvec<NZG, THREE, TIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        attr = true;
+        attr_set.fetch_or(bit, std::memory_order_relaxed);
     }
     note_launch(), k_ho_matvec<NZG, THREE, TIN><<<grd, blk, smem, st>>>(g, s, phi, scale, b, y, mode, BX, BY);
 }

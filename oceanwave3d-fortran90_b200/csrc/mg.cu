@@ -311,12 +311,13 @@ static void coarse_cycle(const LevelDev<T>* lev, int lc, int ld, const T* M, int
     // one block per SM; a grid that cannot be co-resident makes the launch
     // fail (cudaErrorCooperativeLaunchTooLarge), which the caller's error
     // check reports
-    static int grid = 0;
+    static std::atomic<int> sm_count[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int grid = sm_count[dev & 63].load(std::memory_order_relaxed);
     if (grid == 0) {
-        int dev = 0, nsm = 148;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        grid = nsm;
+        cudaDeviceGetAttribute(&grid, cudaDevAttrMultiProcessorCount, dev);
+        sm_count[dev & 63].store(grid, std::memory_order_relaxed);
     }
     // the level table lives in device memory (a by-value parameter indexed
     // by a run-time level would be copied to every thread's stack); upload it

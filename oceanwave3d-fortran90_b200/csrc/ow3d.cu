@@ -7,6 +7,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -926,6 +928,43 @@ int ow3d_step(ow3d_handle* H, int nsteps) {
         if (r > 0) st = r;
     }
     return st;
+}
+
+int ow3d_step_batch(ow3d_handle* const* hs, int n, const int* nsteps, int* status, double* wall_ms) {
+    if (!hs || n < 0 || !nsteps) return OW3D_ERR_BAD_INPUT;
+    for (int i = 0; i < n; ++i) {
+        if (!hs[i] || nsteps[i] < 0) return OW3D_ERR_BAD_INPUT;
+        for (int q = 0; q < i; ++q)
+            if (hs[q] == hs[i]) { g_last_error = "ow3d_step_batch: a handle appears twice"; return OW3D_ERR_BAD_INPUT; }
+    }
+    // One host thread per handle: each drives its handle's stream (the GMRES
+    // control loop synchronises with its own stream only), so the device runs
+    // the simulations' kernels concurrently.
+    std::vector<int> st(n, OW3D_OK);
+    std::vector<double> ms(n, 0.0);
+    std::vector<std::string> errs(n);
+    auto work = [&](int i) {
+        const auto t0 = std::chrono::steady_clock::now();
+        st[i] = ow3d_step(hs[i], nsteps[i]);
+        const auto t1 = std::chrono::steady_clock::now();
+        ms[i] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        if (st[i] < 0) errs[i] = g_last_error;
+    };
+    if (n == 1) work(0);
+    else {
+        std::vector<std::thread> th;
+        th.reserve(n);
+        for (int i = 0; i < n; ++i) th.emplace_back(work, i);
+        for (auto& t : th) t.join();
+    }
+    int worst = OW3D_OK;
+    for (int i = 0; i < n; ++i) {
+        if (status) status[i] = st[i];
+        if (wall_ms) wall_ms[i] = ms[i];
+        if (st[i] < 0 && (worst >= 0 || st[i] < worst)) { worst = st[i]; g_last_error = errs[i]; }
+        else if (st[i] > 0 && worst == OW3D_OK) worst = st[i];
+    }
+    return worst;
 }
 
 int ow3d_step_timed(ow3d_handle* H, int nsteps, double* device_ms) {
