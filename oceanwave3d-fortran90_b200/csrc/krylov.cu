@@ -264,15 +264,17 @@ __global__ void __launch_bounds__(kThreads) k_norm_init(const double* __restrict
     }
 }
 
-// Upper-triangular solve H y = g for the current k (1 thread).
-__global__ void k_backsolve(KrylovState* ks) {
+// Upper-triangular solve R y = g for the current k (1 thread); R is the
+// in-place rotated H (left GMRES) or the separate rotated copy (FGMRES).
+__global__ void k_backsolve(KrylovState* ks, int rotated_R) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    auto Rv = [&](int col, int row) -> double { return rotated_R ? ks->R[col][row] : ks->H[col][row]; };
     int kk = ks->k;
-    while (kk > 0 && ks->H[kk - 1][kk - 1] == 0.0) --kk;
+    while (kk > 0 && Rv(kk - 1, kk - 1) == 0.0) --kk;
     for (int i = kk - 1; i >= 0; --i) {
         double t = ks->g[i];
-        for (int j = i + 1; j < kk; ++j) t -= ks->H[j][i] * ks->y[j];
-        ks->y[i] = t / ks->H[i][i];
+        for (int j = i + 1; j < kk; ++j) t -= Rv(j, i) * ks->y[j];
+        ks->y[i] = t / Rv(i, i);
     }
     for (int i = kk; i <= kMaxKrylov; ++i) ks->y[i] = 0.0;
     ks->k = kk;
@@ -301,7 +303,197 @@ __global__ void k_krylov_reset(KrylovState* ks) {
     ks->tol = 0; ks->resid = 0; ks->beta = 0;
 }
 
+// ---------------------------------------------------------------- DCGS2
+// Flexible GMRES orthogonalisation by delayed classical Gram-Schmidt with
+// reorthogonalisation (Swirydowicz, Langou, Ananthan, Yang, Thomas, "Low
+// synchronization Gram-Schmidt and generalized minimal residual algorithms",
+// NLAA 2021): the second Gram-Schmidt pass of V_j rides on step j's single
+// reduction, so each Arnoldi step reads the basis twice (reduce, update)
+// instead of four times. V_0..V_{j-1} are final, V_j has had one pass.
+
+// rotate unrotated column col of H with rotations 0..col-1 into R, form
+// rotation col, rotate g from its value before rotation col; returns |g[col+1]|
+__device__ double dcgs_rotate(KrylovState* ks, int col) {
+    for (int r = 0; r <= col + 1; ++r) ks->R[col][r] = ks->H[col][r];
+    for (int i = 0; i < col; ++i) {
+        const double a0 = ks->R[col][i];
+        ks->R[col][i] = ks->cs[i] * a0 + ks->sn[i] * ks->R[col][i + 1];
+        ks->R[col][i + 1] = ks->cs[i] * ks->R[col][i + 1] - ks->sn[i] * a0;
+    }
+    const double x = ks->R[col][col], yv = ks->R[col][col + 1];
+    const double r = sqrt(x * x + yv * yv);
+    double c = 1.0, sg = 0.0;
+    if (r != 0.0) { c = x / r; sg = yv / r; ks->R[col][col] = r; ks->R[col][col + 1] = 0.0; }
+    ks->cs[col] = c; ks->sn[col] = sg;
+    const double g0 = ks->gsave[col];
+    const double al = -sg * g0;
+    ks->g[col] = c * g0;
+    ks->g[col + 1] = al;
+    return fabs(al);
+}
+
+// One thread, after step j's reduction: res[2i] = <V_i, V_j>, res[2i+1] = <V_i, W>, i <= j.
+__device__ void dcgs_column(KrylovState* ks, int j, const double* res) {
+    double ss = 0.0, corr = 0.0;
+    if (j >= 1) {
+        for (int i = 0; i < j; ++i) {
+            const double sig = ks->scale[i] * res[2 * i];
+            ks->coefA[i] = sig;          // sigma_i, scaled below
+            ss += sig * sig;
+        }
+        const double nu = sqrt(fmax(res[2 * j] - ss, 0.0));
+        // complete column j-1: W_{j-1} = sum (h + sigma) q_i + nu q_j
+        for (int i = 0; i < j; ++i) ks->H[j - 1][i] += ks->coefA[i];
+        ks->H[j - 1][j] = nu;
+        ks->scale[j] = nu > 0 ? 1.0 / nu : 0.0;
+        ks->resid = dcgs_rotate(ks, j - 1);
+    }
+    for (int i = 0; i < j; ++i) {
+        const double hq = ks->scale[i] * res[2 * i + 1];
+        ks->H[j][i] = hq;
+        corr += ks->coefA[i] * hq;
+        ks->coefB[i] = hq * ks->scale[i];
+        ks->coefA[i] *= ks->scale[i];
+    }
+    const double hj = (j >= 1) ? (res[2 * j + 1] - corr) * ks->scale[j] : ks->scale[j] * res[2 * j + 1];
+    ks->H[j][j] = hj;
+    ks->coefB[j] = hj * ks->scale[j];
+}
+
+// Reduction, grid (nbx, j+1): block (bx, v) forms partials of <V_v, V_j> and
+// <V_v, W> over a slice (V_j and W are re-read per v from L2). The last block
+// reduces everything and runs dcgs_column.
+__global__ void __launch_bounds__(kThreads) k_dcgs_reduce(const double* __restrict__ V, int64_t ldv, int j,
+                                                          const double* __restrict__ W, int64_t n, double* partial,
+                                                          unsigned int* counter, int nbx, KrylovState* ks) {
+    if (ks->done) return;
+    const int v = blockIdx.y;
+    const int64_t n2 = (n + 1) / 2;
+    const double2* a2 = reinterpret_cast<const double2*>(V + (int64_t)v * ldv);
+    const double2* q2 = reinterpret_cast<const double2*>(V + (int64_t)j * ldv);
+    const double2* w2 = reinterpret_cast<const double2*>(W);
+    const int64_t stride = (int64_t)nbx * blockDim.x;
+    double s0 = 0, s1 = 0, t0 = 0, t1 = 0;
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (; t + stride < n2; t += 2 * stride) {
+        const double2 x0 = a2[t], x1 = a2[t + stride];
+        const double2 q0 = q2[t], q1 = q2[t + stride];
+        const double2 y0 = w2[t], y1 = w2[t + stride];
+        s0 += x0.x * q0.x + x0.y * q0.y; s1 += x1.x * q1.x + x1.y * q1.y;
+        t0 += x0.x * y0.x + x0.y * y0.y; t1 += x1.x * y1.x + x1.y * y1.y;
+    }
+    for (; t < n2; t += stride) {
+        const double2 x0 = a2[t], q0 = q2[t], y0 = w2[t];
+        s0 += x0.x * q0.x + x0.y * q0.y;
+        t0 += x0.x * y0.x + x0.y * y0.y;
+    }
+    __shared__ double red[2][kThreads / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const double sa = warp_sum(s0 + s1), sb = warp_sum(t0 + t1);
+    if (lane == 0) { red[0][wid] = sa; red[1][wid] = sb; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double pa = 0, pb = 0;
+        for (int q = 0; q < (int)(blockDim.x / 32); ++q) { pa += red[0][q]; pb += red[1][q]; }
+        partial[(int64_t)(2 * v) * nbx + blockIdx.x] = pa;
+        partial[(int64_t)(2 * v + 1) * nbx + blockIdx.x] = pb;
+    }
+    __shared__ bool amlast;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) amlast = (atomicAdd(counter, 1u) == gridDim.x * gridDim.y - 1);
+    __syncthreads();
+    if (!amlast) return;
+    __threadfence();
+    __shared__ double res[2 * kMaxDots];
+    const int nv = 2 * (j + 1), nw = blockDim.x >> 5;
+    for (int u = wid; u < nv; u += nw) {
+        const double* pv = partial + (int64_t)u * nbx;
+        double sacc = 0;
+        for (int b = lane; b < nbx; b += 32) sacc += __ldcg(pv + b);
+        sacc = warp_sum(sacc);
+        if (lane == 0) res[u] = sacc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *counter = 0u;
+        dcgs_column(ks, j, res);
+    }
+}
+
+// Update: V_j <- V_j - sum_{i<j} coefA_i V_i,  W <- W - sum_{i<j} coefB_i V_i - coefB_j V_j(new),
+// |W|^2; the last block completes column j's provisional norm, its rotation,
+// the residual estimate and the stopping test.
+__global__ void __launch_bounds__(kThreads) k_dcgs_update(double* __restrict__ V, int64_t ldv, int j,
+                                                          double* __restrict__ W, int64_t n, double* partial,
+                                                          unsigned int* counter, int nblocks, KrylovState* ks,
+                                                          int maxmv, int m) {
+    if (ks->done) return;
+    __shared__ double cA[kMaxDots], cB[kMaxDots + 1];
+    for (int v = threadIdx.x; v <= j; v += blockDim.x) { cB[v] = ks->coefB[v]; if (v < j) cA[v] = ks->coefA[v]; }
+    __syncthreads();
+    const double cBj = cB[j];
+    double acc[1] = {0.0};
+    const int64_t n2 = (n + 1) / 2;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    double2* vj2 = reinterpret_cast<double2*>(V + (int64_t)j * ldv);
+    double2* w2 = reinterpret_cast<double2*>(W);
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n2; t += stride) {
+        double2 q = vj2[t], a = w2[t];
+        for (int v0 = 0; v0 < j; v0 += 8) {
+            double2 vv[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (v0 + u < j) vv[u] = __ldcs(reinterpret_cast<const double2*>(V + (int64_t)(v0 + u) * ldv) + t);
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (v0 + u < j) {
+                    q.x -= cA[v0 + u] * vv[u].x; q.y -= cA[v0 + u] * vv[u].y;
+                    a.x -= cB[v0 + u] * vv[u].x; a.y -= cB[v0 + u] * vv[u].y;
+                }
+        }
+        a.x -= cBj * q.x; a.y -= cBj * q.y;
+        if (j > 0) vj2[t] = q;
+        w2[t] = a;
+        acc[0] += a.x * a.x + a.y * a.y;
+    }
+    block_store_partials(acc, 1, partial, nblocks);
+    __shared__ double res[1];
+    if (last_block_reduce(partial, 1, nblocks, counter, res)) {
+        if (threadIdx.x == 0) {
+            const double nrm = sqrt(res[0]);
+            ks->H[j][j + 1] = nrm;
+            ks->scale[j + 1] = nrm > 0 ? 1.0 / nrm : 0.0;
+            ks->gsave[j] = ks->g[j];
+            ks->resid = dcgs_rotate(ks, j);
+            ks->k = j + 1;
+            ks->iters += 1;
+            const bool conv = ks->resid <= ks->tol;
+            if (conv) ks->converged = 1;
+            if (conv || j + 1 >= m || ks->iters >= maxmv || nrm == 0.0) ks->done = 1;
+        }
+    }
+}
+
 }  // namespace
+
+void launch_dcgs_reduce(const double* V, int64_t ldv, int j, const double* W, int64_t n, const DotScratch& sc,
+                        KrylovState* ks, cudaStream_t st) {
+    // about 8 blocks per SM in total over the j+1 basis vectors; 2(j+1) partial rows
+    int nbx = (148 * 8 + j) / (j + 1);
+    const int64_t need = ((n + 1) / 2 + kThreads - 1) / kThreads;
+    if (nbx > need) nbx = (int)need;
+    const int cap = (int)(((int64_t)(kMaxKrylov + 2) * sc.nblocks) / (2 * (j + 1)));
+    if (nbx > cap) nbx = cap;
+    if (nbx < 1) nbx = 1;
+    note_launch(), k_dcgs_reduce<<<dim3(nbx, j + 1), kThreads, 0, st>>>(V, ldv, j, W, n, sc.partial, sc.counter, nbx, ks);
+}
+
+void launch_dcgs_update(double* V, int64_t ldv, int j, double* W, int64_t n, const DotScratch& sc, KrylovState* ks,
+                        int maxmv, int m, cudaStream_t st) {
+    note_launch(), k_dcgs_update<<<sc.nblocks, kThreads, 0, st>>>(V, ldv, j, W, n, sc.partial, sc.counter, sc.nblocks,
+                                                                  ks, maxmv, m);
+}
 
 void launch_multidot(const double* V, int64_t ldv, int k, const double* w, int64_t n, const DotScratch& sc,
                      KrylovState* ks, int cond, cudaStream_t st) {
@@ -328,7 +520,9 @@ void launch_norm_init(const double* v, int64_t n, const DotScratch& sc, KrylovSt
     note_launch(), k_norm_init<<<sc.nblocks, kThreads, 0, st>>>(v, n, sc.partial, sc.counter, sc.nblocks, ks, rtol, atol);
 }
 
-void launch_backsolve(KrylovState* ks, cudaStream_t st) { note_launch(), k_backsolve<<<1, 32, 0, st>>>(ks); }
+void launch_backsolve(KrylovState* ks, cudaStream_t st, int rotated_R) {
+    note_launch(), k_backsolve<<<1, 32, 0, st>>>(ks, rotated_R);
+}
 
 template <typename TZ>
 void launch_solution_update(double* x, const TZ* Z, int64_t ldz, int64_t n, const KrylovState* ks, int use_scale,

@@ -423,15 +423,20 @@ int solve_device(ow3d_handle* H, const double* rhs, double* phi, const Surface& 
                 launch_ho_matvec<double>(H->hg, s, Vj, sj, nullptr, H->w, 0, H->st);
                 precond_into(H, H->w, nullptr, Vn);
             }
-            launch_multidot(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 0, H->st);
-            launch_project(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 0, maxmv, m, H->st);
-            launch_multidot(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 1, H->st);
-            launch_project(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 1, maxmv, m, H->st);
+            if (!left) {
+                launch_dcgs_reduce(H->V, H->ldv, j, Vn, N, H->dsc, H->ks, H->st);
+                launch_dcgs_update(H->V, H->ldv, j, Vn, N, H->dsc, H->ks, maxmv, m, H->st);
+            } else {
+                launch_multidot(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 0, H->st);
+                launch_project(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 0, maxmv, m, H->st);
+                launch_multidot(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 1, H->st);
+                launch_project(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 1, maxmv, m, H->st);
+            }
             TRY(sync_ks_small(H));
             ++j;
         }
         if (H->ks_host->k > 0) {
-            launch_backsolve(H->ks, H->st);
+            launch_backsolve(H->ks, H->st, left ? 0 : 1);
             if (!left) {
                 if (!H->mixed) launch_solution_update<double>(phi, (const double*)H->Z, H->ldv, N, H->ks, 0, H->st);
                 else launch_solution_update<float>(phi, (const float*)H->Z, H->ldv, N, H->ks, 0, H->st);

@@ -90,7 +90,11 @@ int noalloc_norm2(int dev, const double* d_y, int64_t n, double* host_norm2, cud
 
 // ------------------------------------------------ Krylov device scalars
 struct KrylovState {
-    double H[kMaxKrylov + 1][kMaxKrylov + 1];   // H[col][row]
+    double H[kMaxKrylov + 1][kMaxKrylov + 1];   // H[col][row] (FGMRES: unrotated columns)
+    double R[kMaxKrylov + 1][kMaxKrylov + 2];   // FGMRES: rotated columns (upper triangle)
+    double gsave[kMaxKrylov + 2];               // FGMRES: g[col] before rotation col
+    double coefA[kMaxKrylov + 2];               // FGMRES update: V_j -= coefA_i V_i
+    double coefB[kMaxKrylov + 2];               // FGMRES update: W -= coefB_i V_i (i <= j)
     double cs[kMaxKrylov + 1], sn[kMaxKrylov + 1], g[kMaxKrylov + 2];
     double scale[kMaxKrylov + 2];               // v_i = scale[i] * V_i (stored unnormalised)
     double y[kMaxKrylov + 1];
@@ -160,6 +164,12 @@ struct DotScratch {
 };
 void launch_multidot(const double* V, int64_t ldv, int k, const double* w, int64_t n, const DotScratch& sc,
                      KrylovState* ks, int cond, cudaStream_t st);
+// FGMRES Arnoldi step j with delayed classical Gram-Schmidt (DCGS2): the one
+// reduction pass and the one update pass; W = A z_j sits in V_{j+1}.
+void launch_dcgs_reduce(const double* V, int64_t ldv, int j, const double* W, int64_t n, const DotScratch& sc,
+                        KrylovState* ks, cudaStream_t st);
+void launch_dcgs_update(double* V, int64_t ldv, int j, double* W, int64_t n, const DotScratch& sc, KrylovState* ks,
+                        int maxmv, int m, cudaStream_t st);
 // Projection pass; the last block finishes the Arnoldi step (Givens rotation,
 // stopping test) when no re-orthogonalisation pass follows.
 void launch_project(const double* V, int64_t ldv, int k, double* w, int64_t n, const DotScratch& sc, KrylovState* ks,
@@ -167,7 +177,7 @@ void launch_project(const double* V, int64_t ldv, int k, double* w, int64_t n, c
 void launch_arnoldi_finish(KrylovState* ks, int maxmv, int m, cudaStream_t st);
 void launch_norm_init(const double* v, int64_t n, const DotScratch& sc, KrylovState* ks, double rtol, double atol,
                       cudaStream_t st);
-void launch_backsolve(KrylovState* ks, cudaStream_t st);
+void launch_backsolve(KrylovState* ks, cudaStream_t st, int rotated_R = 0);
 template <typename TZ>
 void launch_solution_update(double* x, const TZ* Z, int64_t ldz, int64_t n, const KrylovState* ks, int use_scale,
                             cudaStream_t st);

@@ -827,61 +827,107 @@ static int solve_lgmres(Sim& s, const double* rhs, double* sol, int& iters, doub
 // Right-preconditioned flexible GMRES as the device path runs it: classical
 // Gram-Schmidt, one re-orthogonalisation pass when the norm drops below
 // 1/sqrt(2) of its value before projection (Daniel-Gragg-Kaufman-Stewart).
+// Right-preconditioned flexible GMRES (device mode, krylov = FGMRES) with
+// delayed classical Gram-Schmidt with reorthogonalisation (DCGS2: Swirydowicz,
+// Langou, Ananthan, Yang, Thomas, "Low synchronization Gram-Schmidt and
+// generalized minimal residual algorithms", NLAA 2021). Step j:
+//   z_j = M^{-1} (s_j V_j), W = A z_j;
+//   one reduction: a_i = <V_i, V_j> (i < j), alpha = <V_j, V_j>, b_i = <V_i, W> (i <= j);
+//   the second Gram-Schmidt pass of V_j, lagged by one step: sigma_i = s_i a_i,
+//   nu = sqrt(alpha - sum sigma_i^2), q_j = (V_j - sum sigma_i s_i V_i) / nu, which
+//   completes Hessenberg column j-1 (H[j-1][i] += sigma_i, H[j-1][j] = nu) and
+//   its Givens rotation;
+//   column j: h_i = s_i b_i (i < j), h_j = (b_j - sum sigma_i s_i b_i) / nu;
+//   one update: V_j <- nu q_j, W <- W - sum_i h_i q_i, |W| gives H[j][j+1];
+//   the Givens rotation of column j and the stopping test use that norm (the
+//   next step's reorthogonalisation of W refines the column and its rotation).
+// Vectors are stored unnormalised with s_i = 1/|V_i| as on the device.
 static int solve_fgmres(Sim& s, const double* rhs, double* sol, int& iters, double& resid) {
     const size_t n = s.N; const int m = std::max(2, s.p.GMRESmaxiterations);
     const int maxmv = m;
     vector<vector<double>> V(m + 1, vector<double>(n)), Z(m, vector<double>(n));
-    vector<double> w(n), sc(m + 1), H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), hh(m + 1);
+    vector<double> W(n), vin(n), sc(m + 2), Hr((size_t)(m + 1) * (m + 1), 0.0), R((size_t)(m + 1) * (m + 1), 0.0);
+    vector<double> cs(m + 1), sn(m + 1), g(m + 2), gsave(m + 1), a(m + 1), bb(m + 1), sig(m + 1), hq(m + 1);
+    auto HR = [&](int col, int row) -> double& { return Hr[(size_t)col * (m + 1) + row]; };
+    auto RR = [&](int col, int row) -> double& { return R[(size_t)col * (m + 1) + row]; };
+    // rotate raw column col with the rotations 0..col-1, form rotation col and update g
+    auto rotate = [&](int col) {
+        for (int r = 0; r <= col + 1; ++r) RR(col, r) = HR(col, r);
+        for (int i = 0; i < col; ++i) {
+            const double a0 = RR(col, i);
+            RR(col, i) = cs[i] * a0 + sn[i] * RR(col, i + 1);
+            RR(col, i + 1) = cs[i] * RR(col, i + 1) - sn[i] * a0;
+        }
+        double c, sg;
+        givens(RR(col, col), RR(col, col + 1), c, sg);
+        cs[col] = c; sn[col] = sg;
+        g[col] = gsave[col];
+        const double al = -sg * g[col];
+        g[col] = c * g[col];
+        g[col + 1] = al;
+        return std::fabs(al);
+    };
     int mv = 0; double tol = 0; bool first = true;
     for (;;) {
-        matvec_ho(s, sol, w.data()); ++mv;
-        for (size_t t = 0; t < n; ++t) V[0][t] = rhs[t] - w[t];
+        matvec_ho(s, sol, W.data()); ++mv;
+        for (size_t t = 0; t < n; ++t) V[0][t] = rhs[t] - W[t];
         double beta = std::sqrt(dot(V[0].data(), V[0].data(), n));
         if (first) { tol = s.p.reltol * beta + s.p.abstol; first = false; }
         resid = beta;
         if (beta <= tol) { iters = mv; return OW3D_OK; }
         sc[0] = 1.0 / beta;
         std::fill(g.begin(), g.end(), 0.0); g[0] = beta;
+        std::fill(Hr.begin(), Hr.end(), 0.0);
         int k = 0;
-        vector<double> vin(n);
-        for (;;) {
-            ++k;
-            for (size_t t = 0; t < n; ++t) vin[t] = V[k - 1][t] * sc[k - 1];
-            precond(s, vin.data(), Z[k - 1].data());
-            matvec_ho(s, Z[k - 1].data(), w.data()); ++mv;
-            double* hc = &H[(size_t)(k - 1) * (m + 1)];
-            double w0 = dot(w.data(), w.data(), n);
-            for (int i = 0; i < k; ++i) hc[i] = sc[i] * dot(V[i].data(), w.data(), n);
-            for (size_t t = 0; t < n; ++t) { double a = w[t]; for (int i = 0; i < k; ++i) a -= hc[i] * sc[i] * V[i][t]; w[t] = a; }
-            double w1 = dot(w.data(), w.data(), n);
-            if (w1 < 0.5 * w0) {
-                for (int i = 0; i < k; ++i) hh[i] = sc[i] * dot(V[i].data(), w.data(), n);
-                for (size_t t = 0; t < n; ++t) { double a = w[t]; for (int i = 0; i < k; ++i) a -= hh[i] * sc[i] * V[i][t]; w[t] = a; }
-                for (int i = 0; i < k; ++i) hc[i] += hh[i];
-                w1 = dot(w.data(), w.data(), n);
+        for (int j = 0;; ++j) {
+            for (size_t t = 0; t < n; ++t) vin[t] = V[j][t] * sc[j];
+            precond(s, vin.data(), Z[j].data());
+            matvec_ho(s, Z[j].data(), W.data()); ++mv;
+            for (int i = 0; i < j; ++i) a[i] = dot(V[i].data(), V[j].data(), n);
+            const double alpha = dot(V[j].data(), V[j].data(), n);
+            for (int i = 0; i <= j; ++i) bb[i] = dot(V[i].data(), W.data(), n);
+            if (j >= 1) {
+                double ss = 0;
+                for (int i = 0; i < j; ++i) { sig[i] = sc[i] * a[i]; ss += sig[i] * sig[i]; }
+                const double nu = std::sqrt(std::max(alpha - ss, 0.0));
+                for (int i = 0; i < j; ++i) HR(j - 1, i) += sig[i];
+                HR(j - 1, j) = nu;
+                sc[j] = nu > 0 ? 1.0 / nu : 0.0;
+                resid = rotate(j - 1);
             }
-            double nrm = std::sqrt(w1);
-            hc[k] = nrm; V[k] = w; sc[k] = nrm > 0 ? 1.0 / nrm : 0.0;
-            for (int i = 0; i < k - 1; ++i) {
-                double a0 = hc[i];
-                hc[i] = cs[i] * a0 + sn[i] * hc[i + 1];
-                hc[i + 1] = cs[i] * hc[i + 1] - sn[i] * a0;
+            double corr = 0;
+            for (int i = 0; i < j; ++i) { hq[i] = sc[i] * bb[i]; corr += sig[i] * hq[i]; }
+            const double hj = (j >= 1) ? (bb[j] - corr) * sc[j] : sc[j] * bb[j];
+            for (int i = 0; i < j; ++i) HR(j, i) = hq[i];
+            HR(j, j) = hj;
+            // update: V_j <- V_j - sum sigma_i s_i V_i ; W <- W - sum h_i s_i V_i - h_j s_j V_j(new)
+            double ww = 0;
+            for (size_t t = 0; t < n; ++t) {
+                double vj = V[j][t], w = W[t];
+                for (int i = 0; i < j; ++i) { vj -= sig[i] * sc[i] * V[i][t]; w -= hq[i] * sc[i] * V[i][t]; }
+                w -= hj * sc[j] * vj;
+                V[j][t] = vj; W[t] = w;
+                ww += w * w;
             }
-            double c, sg; givens(hc[k - 1], hc[k], c, sg); cs[k - 1] = c; sn[k - 1] = sg;
-            double al = -sg * g[k - 1]; g[k - 1] = c * g[k - 1]; g[k] = al;
-            resid = std::fabs(al);
+            const double nrm = std::sqrt(ww);
+            V[j + 1] = W;
+            HR(j, j + 1) = nrm;
+            sc[j + 1] = nrm > 0 ? 1.0 / nrm : 0.0;
+            gsave[j] = g[j];
+            resid = rotate(j);
+            k = j + 1;
             if (k < m && !(resid <= tol) && mv < maxmv && nrm > 0) continue;
             break;
         }
         int kk = k;
-        while (kk > 0 && H[(size_t)(kk - 1) * (m + 1) + kk - 1] == 0.0) --kk;
+        while (kk > 0 && RR(kk - 1, kk - 1) == 0.0) --kk;
         vector<double> y(kk);
         for (int i = kk - 1; i >= 0; --i) {
             double t = g[i];
-            for (int j = i + 1; j < kk; ++j) t -= H[(size_t)j * (m + 1) + i] * y[j];
-            y[i] = t / H[(size_t)i * (m + 1) + i];
+            for (int j = i + 1; j < kk; ++j) t -= RR(j, i) * y[j];
+            y[i] = t / RR(i, i);
         }
-        for (size_t t = 0; t < n; ++t) { double a = sol[t]; for (int i = 0; i < kk; ++i) a += y[i] * Z[i][t]; sol[t] = a; }
+        for (size_t t = 0; t < n; ++t) { double acc = sol[t]; for (int i = 0; i < kk; ++i) acc += y[i] * Z[i][t]; sol[t] = acc; }
         if (resid <= tol) { iters = mv; return OW3D_OK; }
         if (mv >= maxmv) { iters = mv; return OW3D_NOT_CONVERGED; }
     }
