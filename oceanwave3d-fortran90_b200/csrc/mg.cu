@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(128, 8) k_lo_colour(LevelDev<T> L, int colour)
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t total = colour_count<T, THREE>(L);
     const RowConst<T> rk = row_const<T, S>(L);
-    for (int64_t base = warp * (32 / S); base < total; base += nwarps * (32 / S))
+    for (int base = (int)warp * (32 / S); base < (int)total; base += (int)nwarps * (32 / S))
         colour_warp<T, THREE, S, CROSS>(L, colour, base, rk);
 }
 
@@ -141,7 +141,7 @@ __device__ void coop_colour_loop(const LevelDev<T>& L, int colour) {
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t total = colour_count<T, THREE>(L);
     const RowConst<T> rk = row_const<T, S>(L);
-    for (int64_t base = warp * (32 / S); base < total; base += nwarps * (32 / S))
+    for (int base = (int)warp * (32 / S); base < (int)total; base += (int)nwarps * (32 / S))
         colour_warp<T, THREE, S, CROSS>(L, colour, base, rk);
 }
 

@@ -30,6 +30,18 @@ __device__ __forceinline__ void load_cf(const float* cf, int64_t c, float& ih, f
     ih = u.x; a = u.y; b = u.z; c3 = u.w;
 }
 
+// Bottom-row coefficients of a column (see LevelDev::bt).
+__device__ __forceinline__ void load_bt(const double* bt, int64_t c, double* o) {
+    const double2* p = reinterpret_cast<const double2*>(bt) + 4 * c;
+    const double2 a = __ldg(p), b = __ldg(p + 1), d = __ldg(p + 2), e = __ldg(p + 3);
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y; o[4] = d.x; o[5] = d.y; o[6] = e.x;
+}
+__device__ __forceinline__ void load_bt(const float* bt, int64_t c, float* o) {
+    const float4* p = reinterpret_cast<const float4*>(bt) + 2 * c;
+    const float4 a = __ldg(p), b = __ldg(p + 1);
+    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w; o[4] = b.x; o[5] = b.y; o[6] = b.z;
+}
+
 template <typename T>
 __device__ __forceinline__ int64_t IX(const LevelDev<T>& L, int k, int i, int j) {
     return (int64_t)(k - 1) + (int64_t)L.Nzg * ((int64_t)(i - 1) + (int64_t)L.Nxg * (j - 1));
@@ -287,7 +299,7 @@ __device__ __forceinline__ RowConst<T> row_const(const LevelDev<T>& L) {
 }
 
 template <typename T, bool THREE, int S, bool CROSS>
-__device__ void colour_warp(const LevelDev<T>& L, int colour, int64_t base, const RowConst<T>& rk) {
+__device__ void colour_warp(const LevelDev<T>& L, int colour, int base, const RowConst<T>& rk) {
     const int Nxg = L.Nxg, Nyg = L.Nyg, Nzg = L.Nzg, R = Nzg - 2;
     const int lane = threadIdx.x & 31, r = lane & (S - 1);
     const int nxi = Nxg - 2, nyi = THREE ? Nyg - 2 : 1;
@@ -295,16 +307,16 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int64_t base, cons
     const bool four = (L.ncolor == 4);
     const int ni = (nxi + 1) / 2;
     const int nj = four ? (nyi + 1) / 2 : nyi;
-    const int64_t total = (int64_t)ni * nj;
+    const int total = ni * nj;                // columns of one colour (< 2^31)
     const unsigned segmask = 0xffffffffu;   // the whole warp runs the scan together
     T* const X = L.xv;
     const T* const B = L.bv;
 
-    const int64_t q = base + (lane / S);
+    const int q = base + (lane / S);
     bool act = q < total;
     int i = 0, j = 1;
     if (act) {
-        const int tj = (int)(q / ni), ti = (int)(q - (int64_t)tj * ni);
+        const int tj = q / ni, ti = q - tj * ni;   // 32-bit division
         if (four) {
             j = THREE ? 2 + 2 * tj + (((colour >> 1) - 2) & 1) : 1;
             i = 2 + 2 * ti + (((colour & 1) - 2) & 1);
@@ -376,7 +388,8 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int64_t base, cons
     // branches, so that one round trip to memory serves the whole task.
     const int kr = (r < R) ? k : R + 1;
     T qv = 0, gv = 0, x1 = 0;
-    T bf = 0, bhx = 0, bhy = 0, bb1 = 0, bl = 0, br = 0, bd = 0, bu = 0;
+    T bb1 = 0, bl = 0, br = 0, bd = 0, bu = 0;
+    T bt[7] = {0, 0, 0, 0, 0, 0, 0};
     if (act) {
         T ih, ca, cb, c3;
         load_cf(L.cf, c, ih, ca, cb, c3);
@@ -387,7 +400,7 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int64_t base, cons
         const T bk = B[c * Nzg + kr - 1];
         T x2o = 0, x3o = 0;
         if (!CROSS) {
-            bhx = L.hx[c]; bhy = THREE ? L.hy[c] : T(0);
+            load_bt(L.bt, c, bt);
             x2o = xc[1]; x3o = xc[2]; bb1 = B[c * Nzg];
             bl = X[(c - 1) * Nzg + 1]; br = X[(c + 1) * Nzg + 1];
             if (THREE) { bd = X[(c - Nxg) * Nzg + 1]; bu = X[(c + Nxg) * Nzg + 1]; }
@@ -465,23 +478,11 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int64_t base, cons
             qv = x0 + (bk - diag * x0 - up * xp - off) * id;
             gv = lo * id;
         }
-        if (!CROSS) {
-            const T omb = T(1) - __ldg(L.zs + 1);
-            const T s2b = omb * ca, s4b = THREE ? omb * cb : T(0);
-            bf = THREE ? (ih + bhx * s2b + bhy * s4b) : (ih + bhx * s2b);
-        }
         // bottom row from the current column
         if (!CROSS) {
-            const T dz = sz(L, 1, 2, 1) * x2o + sz(L, 1, 2, 2) * x3o;
-            T dx = sx(L, 1, i, 0) * bl + sx(L, 1, i, 1) * x2o;
-            dx += sx(L, 1, i, 2) * br;
-            T boff = bf * dz + bhx * dx;
-            if (THREE) {
-                T dy = sy(L, 1, j, 0) * bd + sy(L, 1, j, 1) * x2o;
-                dy += sy(L, 1, j, 2) * bu;
-                boff += bhy * dy;
-            }
-            x1 = (bb1 - boff) / (bf * sz(L, 1, 2, 0));
+            T boff = bt[0] * x2o + bt[1] * x3o + bt[2] * bl + bt[3] * br;
+            if (THREE) boff += bt[4] * bd + bt[5] * bu;
+            x1 = (bb1 - boff) * bt[6];
         }
     }
     // inclusive scan of the affine maps x -> a x + b, a = -g, b = q (in row order)
@@ -501,16 +502,9 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int64_t base, cons
     if (act && r == R - 1) xw[Nzg - 1] = xfs;  // free-surface row
     // 5. bottom row again, from the new column (the neighbours are unchanged)
     if (!CROSS && act && r == 0) {
-        const T dz = sz(L, 1, 2, 1) * x2n + sz(L, 1, 2, 2) * x3n;
-        T dx = sx(L, 1, i, 0) * bl + sx(L, 1, i, 1) * x2n;
-        dx += sx(L, 1, i, 2) * br;
-        T boff = bf * dz + bhx * dx;
-        if (THREE) {
-            T dy = sy(L, 1, j, 0) * bd + sy(L, 1, j, 1) * x2n;
-            dy += sy(L, 1, j, 2) * bu;
-            boff += bhy * dy;
-        }
-        xw[0] = (bb1 - boff) / (bf * sz(L, 1, 2, 0));
+        T boff = bt[0] * x2n + bt[1] * x3n + bt[2] * bl + bt[3] * br;
+        if (THREE) boff += bt[4] * bd + bt[5] * bu;
+        xw[0] = (bb1 - boff) * bt[6];
     }
     // 6. ghost columns whose stencil contains this column, from the new values
     ghosts(true, xn, xfs);

@@ -172,6 +172,38 @@ int build_levels(ow3d_handle* H, MgSet<T>& S, bool alloc_fine_x) {
             TRY(upload(H, &c, cf));
             d.cf = c;
         }
+        {
+            // bottom row (k = 1) of column (i, j): f Dz(x)|_2 + h_x Dx(x)|_2 + h_y Dy(x)|_2
+            // with f = 1/h + h_x s2 + h_y s4 at sigma_2 (BuildLinearSystemMatrix.f90:50-70)
+            const bool three = h.Nyg > 1;
+            const double omb = 1.0 - h.zs[1];
+            const double z0 = h.SZ.w[3 + 0], z1 = h.SZ.w[3 + 1], z2 = h.SZ.w[3 + 2];   // order 1, row 2
+            std::vector<double> bt(8 * h.h.size(), 0.0);
+            for (int jj = 1; jj <= h.Nyg; ++jj)
+                for (int ii = 1; ii <= h.Nxg; ++ii) {
+                    const size_t q = (size_t)(ii - 1) + (size_t)h.Nxg * (jj - 1);
+                    const double ih = 1.0 / h.h[q];
+                    const double hxq = h.hx[q], hyq = three ? h.hy[q] : 0.0;
+                    const double s2 = omb * (hxq * ih), s4 = omb * (hyq * ih);
+                    const double f = three ? (ih + hxq * s2 + hyq * s4) : (ih + hxq * s2);
+                    const double* wx = &h.SX.w[(size_t)(ii - 1) * 3];
+                    double* o = &bt[8 * q];
+                    o[0] = f * z1 + hxq * wx[1];
+                    o[1] = f * z2;
+                    o[2] = hxq * wx[0];
+                    o[3] = hxq * wx[2];
+                    if (three) {
+                        const double* wy = &h.SY.w[(size_t)(jj - 1) * 3];
+                        o[0] += hyq * wy[1];
+                        o[4] = hyq * wy[0];
+                        o[5] = hyq * wy[2];
+                    }
+                    o[6] = 1.0 / (f * z0);
+                }
+            T* btd;
+            TRY(upload(H, &btd, bt));
+            d.bt = btd;
+        }
         d.mz = div_magic((uint64_t)d.Nzg);
         d.mx = div_magic((uint64_t)d.Nxg);
         d.pix = d.piy = d.piz = nullptr;

@@ -64,6 +64,10 @@ struct LevelDev {
     // per column: 1/h, h_x/h, h_y/h, (h_xx+h_yy)/h - 2(h_x^2+h_y^2)/h^2 -- the
     // eta = 0 sigma coefficients divided by (1 - sigma)
     const T* cf;            // [Nxg*Nyg][4]
+    // per column, the bottom row's Gauss-Seidel coefficients (levels without
+    // mixed-derivative terms): x2, x3 of the column, row 2 of the left, right,
+    // lower and upper neighbours, and 1/diagonal
+    const T* bt;            // [Nxg*Nyg][8]
     uint64_t mz, mx;        // division magics for Nzg and Nxg (see qdiv)
     // prolongation from the next coarser level onto this one
     // (MGProlongation3DExplicit.f90:19-110) as per-direction tables over this

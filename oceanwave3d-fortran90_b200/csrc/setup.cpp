@@ -144,6 +144,8 @@ int check_params(const ow3d_params& p, std::string* err) {
         if (p.filterALPHA < 1 || p.filterALPHA > 6) return fail("filterALPHA must be 1..6 (FilterInit.f90 boundary filters)");
         if (Nxg < NP + 2 || (p.Ny > 1 && Nyg < NP + 2)) return fail("grid too small for the filter width");
     }
+    if ((double)Nxg * (double)Nyg * (double)Nzg >= 2147483647.0)
+        return fail("grid too large: at most 2^31-1 unknowns per simulation (32-bit point indices)");
     if (p.precision != OW3D_PREC_FP64 && p.precision != OW3D_PREC_MIXED) return fail("precision must be 0 or 1");
     if (p.krylov != OW3D_KRYLOV_FGMRES && p.krylov != OW3D_KRYLOV_LGMRES) return fail("krylov must be 0 or 1");
     if (p.GMRESmaxiterations < 1) return fail("GMRESmaxiterations must be >= 1");
