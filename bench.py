@@ -13,6 +13,7 @@ host cores, on a bounded sub-basin of the same workload.
 import argparse
 import importlib.util
 import json
+import re
 import os
 import pathlib
 import subprocess
@@ -198,6 +199,16 @@ def kernel_roofline(pkg, p, dev):
     return ms.value / reps, alg
 
 
+def profiled_traffic(kernel):
+    """DRAM bytes (read + write) per launch of `kernel` from its committed ncu
+    summary (the `traffic_bytes_per_launch:` line), or None."""
+    for f in sorted((ROOT / "profiles").glob(f"{kernel}_*.md")):
+        m = re.search(r"^traffic_bytes_per_launch:\s*(\d+)", f.read_text(), re.M)
+        if m:
+            return int(m.group(1))
+    return None
+
+
 def serving_sample(n=16, seed=2024):
     """Bounded sample of the serving stream: n seeded requests (Poisson
     arrivals at 50/s; Nx in {65,129,257}, Ny in {1,33,65}, Nz in {9,13,17};
@@ -320,7 +331,7 @@ def main():
         kms, alg = kr
         ach = alg / (kms / 1e3) / 1e9
         roof = {"bound": "hbm", "kernel": "k_ho_matvec (6th-order sigma operator, FP64)", "achieved": ach,
-                "peak": peak, "unit": "GB/s", "frac": ach / peak, "traffic": None,
+                "peak": peak, "unit": "GB/s", "frac": ach / peak, "traffic": profiled_traffic("k_ho_matvec"),
                 "peak_kind": peak_kind, "alg_bytes_per_launch": alg, "ms_per_launch": kms}
     cpu = None
     if not args.no_cpu:
