@@ -54,7 +54,7 @@ __global__ void k_lo_matvec(LevelDev<T> L, const T* __restrict__ x, T* __restric
 
 template <typename T, bool THREE, bool CROSS>
 __global__ void k_lo_residual(LevelDev<T> L) {
-    OW3D_GRID_STRIDE(p, L.N) residual_item<T, THREE, CROSS>(L, p);
+    OW3D_GRID_STRIDE(p, L.N) residual_point<T, THREE, CROSS>(L, p);
 }
 
 template <typename T, bool THREE>
@@ -63,7 +63,7 @@ __global__ void k_lo_bottom(LevelDev<T> L) {
 }
 
 template <typename T, bool THREE, int S, bool CROSS>
-__global__ void __launch_bounds__(128, 8) k_lo_colour(LevelDev<T> L, int colour) {
+__global__ void __launch_bounds__(128, 6) k_lo_colour(LevelDev<T> L, int colour) {
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t total = colour_count<T, THREE>(L);
@@ -181,8 +181,8 @@ __global__ void __launch_bounds__(kCoopThreads) k_mg_coarse_cycle(const LevelDev
         const LevelDev<T>& L = P[l];
         const LevelDev<T>& Cc = P[l - 1];
         coop_smooth<T, THREE>(L, nu1, grid);
-        if (L.cross) { OW3D_GRID_STRIDE(p, L.N) residual_item<T, THREE, true>(L, p); }
-        else { OW3D_GRID_STRIDE(p, L.N) residual_item<T, THREE, false>(L, p); }
+        if (L.cross) { OW3D_GRID_STRIDE(p, L.N) residual_point<T, THREE, true>(L, p); }
+        else { OW3D_GRID_STRIDE(p, L.N) residual_point<T, THREE, false>(L, p); }
         grid.sync();
         OW3D_GRID_STRIDE(p, Cc.N) restrict_item<T>(L, Cc, L.rv, Cc.bv, Cc.xv, p);
         grid.sync();

@@ -202,6 +202,53 @@ __device__ __forceinline__ void residual_item(const LevelDev<T>& L, int64_t p) {
     L.rv[p] = L.bv[p] - lo_row<T, THREE, CROSS>(L, L.xv, k, i, j, dg);
 }
 
+// Residual r = b - A x at point p (k fastest, so a warp covers about two
+// columns and the column constants are the same for most of its lanes).
+// Interior rows address the neighbours by offsets from the point; ghost
+// columns, the bottom and free-surface rows and levels with mixed-derivative
+// terms take lo_row.
+template <typename T, bool THREE, bool CROSS>
+__device__ __forceinline__ void residual_point(const LevelDev<T>& L, int64_t p) {
+    int k, i, j;
+    int64_t c;
+    decomp(L, p, k, c, i, j);
+    const int Nzg = L.Nzg, Nxg = L.Nxg;
+    T v;
+    if (CROSS || k == 1 || k == Nzg || is_ghost_col<T, THREE>(L, i, j)) {
+        T dg;
+        v = lo_row<T, THREE, CROSS>(L, L.xv, k, i, j, dg);
+    } else {
+        const T* __restrict__ xp = L.xv + p;
+        const int ox = Nzg, oy = Nzg * Nxg;
+        T ih, ca, cb, c3;
+        load_cf(L.cf, c, ih, ca, cb, c3);
+        const T* sxp = L.SX + (Nxg + i - 1) * 3;       // order 2, position i
+        const T* zp1 = L.SZ + (k - 1) * 3;             // order 1, row k
+        const T* zp2 = L.SZ + (Nzg + k - 1) * 3;       // order 2, row k
+        const T om = T(1) - __ldg(L.zs + k - 1);
+        const T s2 = om * ca, s4 = THREE ? om * cb : T(0);
+        const T s3 = om * c3;
+        const T cz = s2 * s2 + s4 * s4 + ih * ih;
+        const T x0 = xp[0];
+        T acc = __ldg(sxp) * xp[-ox];
+        acc += __ldg(sxp + 1) * x0;
+        acc += __ldg(sxp + 2) * xp[ox];
+        if (THREE) {
+            const T* syp = L.SY + (L.Nyg + j - 1) * 3;
+            acc += __ldg(syp) * xp[-oy];
+            acc += __ldg(syp + 1) * x0;
+            acc += __ldg(syp + 2) * xp[oy];
+        }
+        const T xd = xp[-1], xu = xp[1];
+        T dz = __ldg(zp1) * xd, dzz = __ldg(zp2) * xd;
+        dz += __ldg(zp1 + 1) * x0; dzz += __ldg(zp2 + 1) * x0;
+        dz += __ldg(zp1 + 2) * xu; dzz += __ldg(zp2 + 2) * xu;
+        acc += s3 * dz + cz * dzz;
+        v = acc;
+    }
+    L.rv[p] = L.bv[p] - v;
+}
+
 // Gauss-Seidel value of the bottom row (k = 1) of interior column c = (i, j)
 // (BuildLinearSystemMatrix.f90:50-70), given rows 2 and 3 of the column; the
 // neighbours' row-2 values are read from X.
@@ -314,12 +361,12 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int base, const Ro
 
     const int q = base + (lane / S);
     bool act = q < total;
-    int i = 0, j = 1;
+    int i = 2, j = THREE ? 2 : 1;
     if (act) {
         const int tj = q / ni, ti = q - tj * ni;   // 32-bit division
         if (four) {
-            j = THREE ? 2 + 2 * tj + (((colour >> 1) - 2) & 1) : 1;
-            i = 2 + 2 * ti + (((colour & 1) - 2) & 1);
+            j = THREE ? 2 + 2 * tj + (colour >> 1) : 1;
+            i = 2 + 2 * ti + (colour & 1);
         } else {
             j = THREE ? 2 + tj : 1;
             i = 2 + 2 * ti + ((colour + j) & 1);    // (i + j) & 1 == colour
@@ -328,8 +375,15 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int base, const Ro
     }
     const bool rowact = act && (r < R);
     const int k = r + 2;
-    const int64_t c = (int64_t)(i - 1) + (int64_t)Nxg * (j - 1);
-    const T* xc = X + c * Nzg;
+    // the column's base; neighbours and rows are 32-bit offsets from it
+    // (every level has fewer than 2^31 points)
+    const int c = (i - 1) + Nxg * (j - 1);
+    T* const xc = X + (int64_t)c * Nzg;
+    const T* const bc = B + (int64_t)c * Nzg;
+    const int ox = Nzg, oy = Nzg * Nxg;
+    // the column borders a ghost column (ghost relaxation before or after it,
+    // and the corner columns)
+    const bool edge = act && (i <= 3 || i >= Nxg - 2 || (THREE && (j <= 3 || j >= Nyg - 2)));
 
     auto colidx = [&](int ii, int jj) -> int64_t { return (int64_t)(ii - 1) + (int64_t)Nxg * (jj - 1); };
     // Relax ghost column cg: Neumann rows k = 2..Nzg with the 3-point stencil
@@ -342,14 +396,13 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int base, const Ro
             const T vb = (post && own == 2) ? xo : X[cb * Nzg + kk - 1];
             X[cg * Nzg + kk - 1] = (B[cg * Nzg + kk - 1] - (wa * va + wb * vb)) / wg;
         };
-        if (act && r < R) row(k, xnew);
-        if (act && r == R - 1) row(Nzg, xfsn);
-        if (!CROSS && act && r == 0) X[cg * Nzg] = B[cg * Nzg];   // identity level-1 row
+        if (r < R) row(k, xnew);
+        if (r == R - 1) row(Nzg, xfsn);
+        if (!CROSS && r == 0) X[cg * Nzg] = B[cg * Nzg];   // identity level-1 row
     };
     // the four ghost columns that can touch column (i, j); `pre` selects the
     // ones this column reads, otherwise the ones whose stencil contains it
     auto ghosts = [&](bool post, T xnew, T xfsn) {
-        if (!act) return;
         if (i == 2 || (post && i == 3))
             relax_ghost(colidx(1, j), colidx(2, j), sx(L, 1, 2, 1), colidx(3, j), sx(L, 1, 2, 2), sx(L, 1, 2, 0),
                         i == 2 ? 1 : 2, post, xnew, xfsn);
@@ -365,21 +418,15 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int base, const Ro
                             sy(L, 1, Nyg - 1, 1), sy(L, 1, Nyg - 1, 2), j == Nyg - 1 ? 2 : 1, post, xnew, xfsn);
         }
     };
-    // 1. identity corner columns
-    if (THREE && act) {
-        const int cis[2] = {(i == 2) ? 1 : 0, (i == Nxg - 1) ? Nxg : 0};
-        const int cjs[2] = {(j == 2) ? 1 : 0, (j == Nyg - 1) ? Nyg : 0};
-#pragma unroll
-        for (int a = 0; a < 2; ++a)
-#pragma unroll
-            for (int bq = 0; bq < 2; ++bq)
-                if (cis[a] && cjs[bq]) {
-                    const int64_t cc = colidx(cis[a], cjs[bq]);
-                    for (int kk = r; kk < Nzg; kk += S) X[cc * Nzg + kk] = B[cc * Nzg + kk];
-                }
+    if (edge) {
+        // 1. identity corner column diagonal to (i, j) (3-D; at most one)
+        if (THREE && (i == 2 || i == Nxg - 1) && (j == 2 || j == Nyg - 1)) {
+            const int64_t cc = colidx(i == 2 ? 1 : Nxg, j == 2 ? 1 : Nyg);
+            for (int kk = r; kk < Nzg; kk += S) X[cc * Nzg + kk] = B[cc * Nzg + kk];
+        }
+        // 2. ghost columns this column reads, from the current values
+        ghosts(false, T(0), T(0));
     }
-    // 2. ghost columns this column reads, from the current values
-    ghosts(false, T(0), T(0));
     __syncwarp();
 
     // 3.-5. the column. Every lane of an active segment evaluates its row
@@ -387,35 +434,40 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int base, const Ro
     // and the pieces of the bottom row, loads first and without lane-dependent
     // branches, so that one round trip to memory serves the whole task.
     const int kr = (r < R) ? k : R + 1;
+    const int o = kr - 1;
     T qv = 0, gv = 0, x1 = 0;
     T bb1 = 0, bl = 0, br = 0, bd = 0, bu = 0;
-    T bt[7] = {0, 0, 0, 0, 0, 0, 0};
+    T t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0, t6 = 0;   // bottom-row coefficients
     if (act) {
         T ih, ca, cb, c3;
-        load_cf(L.cf, c, ih, ca, cb, c3);
-        const T xl = X[(c - 1) * Nzg + kr - 1], xr = X[(c + 1) * Nzg + kr - 1];
-        const T xd = THREE ? X[(c - Nxg) * Nzg + kr - 1] : T(0), xu = THREE ? X[(c + Nxg) * Nzg + kr - 1] : T(0);
-        const T x0 = xc[kr - 1];
-        const T xp = xc[kr];                   // old value of the row above (row Nzg: free surface)
-        const T bk = B[c * Nzg + kr - 1];
+        load_cf(L.cf, (int64_t)c, ih, ca, cb, c3);
+        const T xl = xc[o - ox], xr = xc[o + ox];
+        const T xd = THREE ? xc[o - oy] : T(0), xu = THREE ? xc[o + oy] : T(0);
+        const T x0 = xc[o];
+        const T xp = xc[o + 1];                // old value of the row above (row Nzg: free surface)
+        const T bk = bc[o];
         T x2o = 0, x3o = 0;
         if (!CROSS) {
-            load_bt(L.bt, c, bt);
-            x2o = xc[1]; x3o = xc[2]; bb1 = B[c * Nzg];
-            bl = X[(c - 1) * Nzg + 1]; br = X[(c + 1) * Nzg + 1];
-            if (THREE) { bd = X[(c - Nxg) * Nzg + 1]; bu = X[(c + Nxg) * Nzg + 1]; }
+            T btv[7];
+            load_bt(L.bt, (int64_t)c, btv);
+            t0 = btv[0]; t1 = btv[1]; t2 = btv[2]; t3 = btv[3]; t4 = btv[4]; t5 = btv[5]; t6 = btv[6];
+            x2o = xc[1]; x3o = xc[2]; bb1 = bc[0];
+            bl = xc[1 - ox]; br = xc[1 + ox];
+            if (THREE) { bd = xc[1 - oy]; bu = xc[1 + oy]; }
         } else {
             x1 = xc[0];                        // bottom rows are fixed during this pass
         }
+        const T* sxp = L.SX + (Nxg + i - 1) * 3;          // order 2, position i
         const T om = rk.om;
         const T s2 = om * ca, s4 = THREE ? om * cb : T(0);
         const T s3 = om * c3;
         const T cz = s2 * s2 + s4 * s4 + ih * ih;
-        T off = sx(L, 2, i, 0) * xl + sx(L, 2, i, 2) * xr;
-        T diag = sx(L, 2, i, 1) + s3 * rk.z1 + cz * rk.zz1;
+        T off = __ldg(sxp) * xl + __ldg(sxp + 2) * xr;
+        T diag = __ldg(sxp + 1) + s3 * rk.z1 + cz * rk.zz1;
         if (THREE) {
-            off += sy(L, 2, j, 0) * xd + sy(L, 2, j, 2) * xu;
-            diag += sy(L, 2, j, 1);
+            const T* syp = L.SY + (Nyg + j - 1) * 3;
+            off += __ldg(syp) * xd + __ldg(syp + 2) * xu;
+            diag += __ldg(syp + 1);
         }
         T lo = s3 * rk.z0 + cz * rk.zz0, up = s3 * rk.z2 + cz * rk.zz2;
         if (CROSS && s2 != T(0)) {
@@ -437,8 +489,7 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int base, const Ro
                             const T cf2 = T(2) * s2 * sz(L, 1, kr, kk) * w;
                             if (kk == 0) lo += cf2; else if (kk == 1) diag += cf2; else up += cf2;
                         } else {
-                            const T* src = X + ((int64_t)(ii - 1) + (int64_t)Nxg * (jj - 1)) * Nzg + (kz - 1);
-                            dx += w * ((ii == i && jj == j) ? *src : ro(src));
+                            dx += w * xc[(ii - i) * ox + (jj - j) * oy + (kz - 1)];
                         }
                     }
                     xz += sz(L, 1, kr, kk) * dx;
@@ -463,8 +514,7 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int base, const Ro
                             const T cf2 = T(2) * s4 * sz(L, 1, kr, kk) * w;
                             if (kk == 0) lo += cf2; else if (kk == 1) diag += cf2; else up += cf2;
                         } else {
-                            const T* src = X + ((int64_t)(ii - 1) + (int64_t)Nxg * (jj - 1)) * Nzg + (kz - 1);
-                            dy += w * ((ii == i && jj == j) ? *src : ro(src));
+                            dy += w * xc[(ii - i) * ox + (jj - j) * oy + (kz - 1)];
                         }
                     }
                     yz += sz(L, 1, kr, kk) * dy;
@@ -480,9 +530,9 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int base, const Ro
         }
         // bottom row from the current column
         if (!CROSS) {
-            T boff = bt[0] * x2o + bt[1] * x3o + bt[2] * bl + bt[3] * br;
-            if (THREE) boff += bt[4] * bd + bt[5] * bu;
-            x1 = (bb1 - boff) * bt[6];
+            T boff = t0 * x2o + t1 * x3o + t2 * bl + t3 * br;
+            if (THREE) boff += t4 * bd + t5 * bu;
+            x1 = (bb1 - boff) * t6;
         }
     }
     // inclusive scan of the affine maps x -> a x + b, a = -g, b = q (in row order)
@@ -496,18 +546,17 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int base, const Ro
     const T xn = a * x1 + bb;                  // new value of row k
     const T x2n = __shfl_sync(segmask, xn, 0, S);
     const T x3n = __shfl_sync(segmask, xn, 1, S);
-    T* xw = X + c * Nzg;
-    if (rowact) xw[k - 1] = xn;
-    const T xfs = act ? B[c * Nzg + Nzg - 1] : T(0);
-    if (act && r == R - 1) xw[Nzg - 1] = xfs;  // free-surface row
+    if (rowact) xc[k - 1] = xn;
+    const T xfs = act ? bc[Nzg - 1] : T(0);
+    if (act && r == R - 1) xc[Nzg - 1] = xfs;  // free-surface row
     // 5. bottom row again, from the new column (the neighbours are unchanged)
     if (!CROSS && act && r == 0) {
-        T boff = bt[0] * x2n + bt[1] * x3n + bt[2] * bl + bt[3] * br;
-        if (THREE) boff += bt[4] * bd + bt[5] * bu;
-        xw[0] = (bb1 - boff) * bt[6];
+        T boff = t0 * x2n + t1 * x3n + t2 * bl + t3 * br;
+        if (THREE) boff += t4 * bd + t5 * bu;
+        xc[0] = (bb1 - boff) * t6;
     }
     // 6. ghost columns whose stencil contains this column, from the new values
-    ghosts(true, xn, xfs);
+    if (edge) ghosts(true, xn, xfs);
 }
 
 // MGRestriction3DExplicit.f90:19-128 as a gather for coarse point p (also zeroes the coarse iterate).
@@ -525,7 +574,10 @@ __device__ void restrict_item(const LevelDev<T>& F, const LevelDev<T>& Cc, const
         const bool ghost = kc == 1 || ic == 1 || ic == Cc.Nxg || (gy && (jc == 1 || jc == Cc.Nyg));
         if (ghost) { rc[p] = T(0); return; }
         const int kf = 2 + (kc - 2) * (1 + zcz), ifn = 2 + (ic - 2) * (1 + xcz), jf = gy ? 2 + (jc - 2) * (1 + ycz) : 1;
-        auto R = [&](int k, int i, int j) -> T { return rf[IX(F, k, i, j)]; };
+        // fine values by 32-bit offsets from (kf, ifn, jf) (levels have < 2^31 points)
+        const T* __restrict__ rb = rf + IX(F, kf, ifn, jf);
+        const int fox = F.Nzg, foy = F.Nzg * F.Nxg;
+        auto R = [&](int k, int i, int j) -> T { return rb[(k - kf) + (i - ifn) * fox + (j - jf) * foy]; };
         if (kf == F.Nzg) { rc[p] = R(kf, ifn, jf); return; }
         // x-weighted value at (k, ifn, j) (raw on ghost rows and outside 2..Nzf)
         auto Sx = [&](int k, int j) -> T {
@@ -570,8 +622,8 @@ __device__ void prolong_item(const LevelDev<T>& F, const LevelDev<T>& Cc, const 
     const T wx0 = __ldg(F.pwx + 2 * (ifn - 1)), wx1 = __ldg(F.pwx + 2 * (ifn - 1) + 1);
     const T wy0 = __ldg(F.pwy + 2 * (gy ? jf - 1 : 0)), wy1 = __ldg(F.pwy + 2 * (gy ? jf - 1 : 0) + 1);
     const int Ncz = Cc.Nzg, Ncx = Cc.Nxg;
-    auto C = [&](int kc, int ic, int jc) -> T {
-        return xc[(int64_t)(kc - 1) + (int64_t)Ncz * ((int64_t)(ic - 1) + (int64_t)Ncx * (jc - 1))];
+    auto C = [&](int kc, int ic, int jc) -> T {   // 32-bit: levels have < 2^31 points
+        return xc[(kc - 1) + Ncz * ((ic - 1) + Ncx * (jc - 1))];
     };
     auto Px = [&](int kc, int jc) -> T {
         T v = wx0 * C(kc, xi.x, jc);
