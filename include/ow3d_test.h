@@ -33,6 +33,11 @@ int ow3d_test_level_op(ow3d_handle* h, int level, int op, int nu, const double* 
  * handles and threads (the cooperative coarse-grid kernel counts as one). */
 unsigned long long ow3d_launch_count(void);
 
+/* Tuning knob for measurements: cap on the number of blocks of the fused
+ * coarse-level multigrid kernel (0 = one block per SM, the default). Returns
+ * the previous value. Process-wide. */
+int ow3d_test_set_coarse_blocks(int blocks);
+
 int ow3d_bench_kernel(ow3d_handle* h, int which, int reps, double* ms_total);
 /* sizeof the C structs: 0 ow3d_params, 1 ow3d_zone, 2 ow3d_stats. */
 int ow3d_test_sizeof(int which);

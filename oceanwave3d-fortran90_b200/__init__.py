@@ -55,6 +55,7 @@ def lib():
         L.ow3d_bench_kernel.argtypes = [_C.c_void_p, _C.c_int, _C.c_int, D]
         L.ow3d_launch_count.argtypes = []
         L.ow3d_launch_count.restype = _C.c_ulonglong
+        L.ow3d_test_set_coarse_blocks.argtypes = [_C.c_int]
         _lib = L
     return _lib
 

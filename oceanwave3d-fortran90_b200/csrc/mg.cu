@@ -304,6 +304,10 @@ void launch_dense_apply(const LevelDev<T>& L, const T* M, cudaStream_t st) {
     note_launch(), k_dense_apply<T><<<blocks, 32 * warps_per_block, 0, st>>>(n, M, L.bv, L.xv);
 }
 
+// Block count of the fused coarse kernel: 0 = one block per SM, else at most
+// this many (a tuning knob for measurements, set through the test API).
+std::atomic<int> g_coarse_blocks{0};
+
 // Launch the fused coarse cycle over levels lc..ld with a fully co-resident grid.
 template <typename T, bool THREE>
 static void coarse_cycle(const LevelDev<T>* lev, int lc, int ld, const T* M, int nu1, int nu2, LevelTable<T>& pack,
@@ -319,6 +323,8 @@ static void coarse_cycle(const LevelDev<T>* lev, int lc, int ld, const T* M, int
         cudaDeviceGetAttribute(&grid, cudaDevAttrMultiProcessorCount, dev);
         sm_count[dev & 63].store(grid, std::memory_order_relaxed);
     }
+    const int cap = g_coarse_blocks.load(std::memory_order_relaxed);
+    if (cap > 0 && cap < grid) grid = cap;
     // the level table lives in device memory (a by-value parameter indexed
     // by a run-time level would be copied to every thread's stack); upload it
     // only when a level's pointers or sizes changed since the last launch

@@ -9,12 +9,15 @@ namespace ow3d {
 namespace mgdev {
 
 // Linear point index p (k fastest) -> 1-based (k, i, j) and column c.
+// Every level has fewer than 2^31 points (the set-up rejects larger grids),
+// so the decomposition runs in 32 bits.
 template <typename T>
 __device__ __forceinline__ void decomp(const LevelDev<T>& L, int64_t p, int& k, int64_t& c, int& i, int& j) {
-    const uint64_t cc = qdiv((uint64_t)p, L.mz);
-    k = (int)((uint64_t)p - cc * (uint64_t)L.Nzg) + 1;
-    const uint64_t jj = qdiv(cc, L.mx);
-    i = (int)(cc - jj * (uint64_t)L.Nxg) + 1;
+    const uint32_t pp = (uint32_t)p;
+    const uint32_t cc = div32(pp, L.mz32, L.sz32);
+    k = (int)(pp - cc * (uint32_t)L.Nzg) + 1;
+    const uint32_t jj = div32(cc, L.mx32, L.sx32);
+    i = (int)(cc - jj * (uint32_t)L.Nxg) + 1;
     j = (int)jj + 1;
     c = (int64_t)cc;
 }

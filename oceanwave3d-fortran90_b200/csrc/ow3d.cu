@@ -206,6 +206,8 @@ int build_levels(ow3d_handle* H, MgSet<T>& S, bool alloc_fine_x) {
         }
         d.mz = div_magic((uint64_t)d.Nzg);
         d.mx = div_magic((uint64_t)d.Nxg);
+        div_magic32((uint32_t)d.Nzg, d.mz32, d.sz32);
+        div_magic32((uint32_t)d.Nxg, d.mx32, d.sx32);
         d.pix = d.piy = d.piz = nullptr;
         d.pwx = d.pwy = d.pwz = nullptr;
         if (l > 0) {
@@ -530,6 +532,7 @@ int create_impl(const ow3d_params* p, const double* h, const double* hx, const d
     hg.Nxg = G.Nxg; hg.Nyg = G.Nyg; hg.Nzg = G.Nzg; hg.gx = G.gx; hg.gy = G.gy; hg.three = G.three;
     hg.nonlinear = (p->LinearONOFF == 1); hg.SX = H->SX; hg.SY = H->SY; hg.SZ = H->SZ; hg.zs = H->zs;
     hg.h = H->h; hg.hx = H->hx; hg.hxx = H->hxx; hg.hy = H->hy; hg.hyy = H->hyy;
+    hg.hSX = G.SX.w.data(); hg.hSY = G.SY.w.data(); hg.hSZ = G.SZ.w.data(); hg.hzs = G.zs.data();
     FsArgs& fa = H->fa;
     fa.Nxg = G.Nxg; fa.Nyg = G.Nyg; fa.Nzg = G.Nzg; fa.three = G.three; fa.nonlinear = hg.nonlinear; fa.g = p->g;
     fa.SX = H->SX; fa.SY = H->SY; fa.SZ = H->SZ; fa.h = H->h;
@@ -755,6 +758,8 @@ int level_op_t(ow3d_handle* H, MgSet<T>& S, int l, int op, int nu, const double*
 extern "C" {
 
 unsigned long long ow3d_launch_count(void) { return g_kernel_launches.load(std::memory_order_relaxed); }
+
+int ow3d_test_set_coarse_blocks(int blocks) { return g_coarse_blocks.exchange(blocks < 0 ? 0 : blocks); }
 
 int ow3d_default_params(ow3d_params* p) { return default_params(p); }
 

@@ -18,6 +18,8 @@ namespace ow3d {
 
 // Kernels launched by this library since load (all handles, all threads).
 extern std::atomic<unsigned long long> g_kernel_launches;
+// Block count cap of the fused coarse-level kernel (0: one block per SM).
+extern std::atomic<int> g_coarse_blocks;
 inline void note_launch() { g_kernel_launches.fetch_add(1ull, std::memory_order_relaxed); }
 
 constexpr int kMaxLevels = 16;
@@ -38,6 +40,9 @@ struct HoGrid {
     const double* SZ;       // 2*Nzg*7 (PreProcessDiffStencils.f90:108-132)
     const double* zs;       // sigma levels with zs[0] = 0 (DetermineTransformationConstantsArray.f90:59)
     const double *h, *hx, *hxx, *hy, *hyy;   // bathymetry, Nxg*Nyg
+    // host copies of the stencil tables and levels (owned by the handle), for
+    // kernel parameters
+    const double *hSX, *hSY, *hSZ, *hzs;
 };
 
 // Surface state that defines the sigma coefficients of one solve.
@@ -69,6 +74,8 @@ struct LevelDev {
     // lower and upper neighbours, and 1/diagonal
     const T* bt;            // [Nxg*Nyg][8]
     uint64_t mz, mx;        // division magics for Nzg and Nxg (see qdiv)
+    uint32_t mz32, mx32;    // 32-bit magics for Nzg and Nxg (see div32) and their shifts
+    int sz32, sx32;
     // prolongation from the next coarser level onto this one
     // (MGProlongation3DExplicit.f90:19-110) as per-direction tables over this
     // level's indices: coarse indices (1-based) and weights of the two coarse
@@ -86,6 +93,18 @@ struct LevelDev {
 inline uint64_t div_magic(uint64_t d) { return ~0ull / d + 1ull; }
 #ifdef __CUDACC__
 __device__ __forceinline__ uint64_t qdiv(uint64_t n, uint64_t m) { return __umul64hi(n, m); }
+#endif
+// n / d for every n < 2^31 and d >= 2 as umulhi(n, m) >> sh with
+// m = ceil(2^(31+l) / d), l = ceil(log2 d), sh = l - 1 (Granlund and
+// Montgomery's round-up method; m < 2^32).
+inline void div_magic32(uint32_t d, uint32_t& m, int& sh) {
+    int l = 0;
+    while ((1ull << l) < d) ++l;
+    m = (uint32_t)(((1ull << (31 + l)) + d - 1) / d);
+    sh = l - 1;
+}
+#ifdef __CUDACC__
+__device__ __forceinline__ uint32_t div32(uint32_t n, uint32_t m, int sh) { return __umulhi(n, m) >> sh; }
 #endif
 
 // sqrt(sum y^2) of a device vector using only fixed file-scope device scratch

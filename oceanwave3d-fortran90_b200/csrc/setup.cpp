@@ -46,19 +46,31 @@ void fd_weights(double z, const double* x, int n, int order, double* w) {
 }
 
 // x / y stencils: window of 2a+1 nodes centred on the point, shifted inwards at
-// the first and last a points (BuildStencilsGridX.f90:162-196).
+// the first and last a points (BuildStencilsGridX.f90:162-196). The grids are
+// uniform, so the nodes are taken at their exact offsets q*dx from the point
+// (q an integer): every row with the same window shift gets bitwise the same
+// weights, which lets the device keep one centred stencil for all interior
+// points. The reference forms the offsets from absolute coordinates, which
+// perturbs the weights row by row at the level of rounding only (about 1e-13
+// relative at x ~ 50 m). A grid that is not uniform to 1e-12 takes the
+// absolute coordinates.
 Stencil stencils_xy(const std::vector<double>& x, int a) {
     Stencil s;
     s.n = (int)x.size();
     s.rank = 2 * a + 1;
     s.w.assign((size_t)2 * s.n * s.rank, 0.0);
     if (s.n == 1 || a == 0) return s;
+    const double dx = (x[(size_t)s.n - 1] - x[0]) / (double)(s.n - 1);
+    bool uniform = dx > 0.0;
+    for (int i = 0; i < s.n && uniform; ++i)
+        uniform = std::fabs(x[(size_t)i] - (x[0] + dx * i)) <= 1e-12 * std::fabs(dx) * s.n;
     std::vector<double> nodes(s.rank), w(s.rank);
     for (int order = 1; order <= 2; ++order)
         for (int i = 1; i <= s.n; ++i) {
             const int shift = (i - 1 < a) ? a - i + 1 : (i >= s.n - a + 1 ? (s.n - a) - i : 0);
-            for (int m = 0; m < s.rank; ++m) nodes[m] = x[(size_t)(i + m - a + shift - 1)];
-            fd_weights(x[i - 1], nodes.data(), s.rank - 1, order, w.data());
+            for (int m = 0; m < s.rank; ++m)
+                nodes[m] = uniform ? (double)(m - a + shift) * dx : x[(size_t)(i + m - a + shift - 1)];
+            fd_weights(uniform ? 0.0 : x[i - 1], nodes.data(), s.rank - 1, order, w.data());
             std::copy(w.begin(), w.end(), s.w.begin() + ((size_t)(order - 1) * s.n + (i - 1)) * s.rank);
         }
     return s;
