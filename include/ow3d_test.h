@@ -26,9 +26,6 @@ int ow3d_test_filter_coeffs(const ow3d_handle* h, double* centre, double* bounda
  * op 5: out = in1 after one smoother phase with rhs in2: colour pass `nu`, or
  *       the bottom-row pass when nu < 0 (levels with mixed-derivative terms). */
 int ow3d_test_level_op(ow3d_handle* h, int level, int op, int nu, const double* in1, const double* in2, double* out);
-/* Time `reps` back-to-back launches of one kernel group with CUDA events on
- * the handle's stream: which 0 = high-order operator, 1 = one preconditioner
- * application (V-cycle). Returns the total milliseconds. */
 /* Number of kernels this library has launched since it was loaded, over all
  * handles and threads (the cooperative coarse-grid kernel counts as one). */
 unsigned long long ow3d_launch_count(void);
@@ -38,6 +35,12 @@ unsigned long long ow3d_launch_count(void);
  * the previous value. Process-wide. */
 int ow3d_test_set_coarse_blocks(int blocks);
 
+/* Device time of `reps` launches of one kernel on this handle's stream,
+ * measured with CUDA events around each launch; before each launch a write of
+ * the Krylov basis (larger than L2) evicts the inputs from L2, outside the
+ * timed interval. which 0 = high-order operator, 1 = one preconditioner
+ * application (V-cycle), 2 = one colour pass of the finest multigrid level
+ * (FP64 handles). Returns the total milliseconds of the launches. */
 int ow3d_bench_kernel(ow3d_handle* h, int which, int reps, double* ms_total);
 /* sizeof the C structs: 0 ow3d_params, 1 ow3d_zone, 2 ow3d_stats. */
 int ow3d_test_sizeof(int which);

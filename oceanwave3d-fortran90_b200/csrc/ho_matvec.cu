@@ -345,6 +345,7 @@ __global__ void __launch_bounds__(THREE ? 256 : 256, 2)
         const int64_t gbase = ((int64_t)(jj - 1) * Nxg + (ilo - 1)) * Nzg;
         const int cnt = ncolx * Nzg;
         double* dst = sm + (int64_t)r * HX * NZP;
+#pragma unroll 8
         for (int e = tid; e < cnt; e += blockDim.x) {
             const int cc = e / Nzg, k = e - cc * Nzg;
             dst[cc * NZP + k] = (double)phi[gbase + e];
