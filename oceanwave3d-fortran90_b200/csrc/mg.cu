@@ -92,7 +92,7 @@ __global__ void k_coarse(int n, const T* __restrict__ inv, const T* __restrict__
 // x = M b for a dense row-major n x n operator: one warp per row, lanes
 // stride along the row (coalesced), shuffle reduction.
 template <typename T>
-__device__ __forceinline__ void dense_rows(int n, const T* __restrict__ M, const T* __restrict__ b, T* __restrict__ x) {
+__device__ __forceinline__ void dense_rows(int n, const T* __restrict__ M, const T* b, T* x) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -154,51 +154,64 @@ __device__ void coop_colour(const LevelDev<T>& L, int colour) {
 #undef OW3D_CC
 }
 
-template <typename T, bool THREE>
-__device__ void coop_bottoms(const LevelDev<T>& L, cg::grid_group& grid) {
+// Barrier of the fused coarse kernel: the whole cooperative grid.
+struct GridSync {
+    cg::grid_group g;
+    __device__ void sync() { g.sync(); }
+};
+
+template <typename T, bool THREE, typename SY>
+__device__ void coop_bottoms(const LevelDev<T>& L, SY& sy) {
     OW3D_GRID_STRIDE(q, (bottom_count<T, THREE>(L))) bottom_item<T, THREE>(L, q);
-    grid.sync();
+    sy.sync();
 }
 
-template <typename T, bool THREE>
-__device__ void coop_smooth(const LevelDev<T>& L, int nu, cg::grid_group& grid) {
-    if (L.cross) coop_bottoms<T, THREE>(L, grid);
+template <typename T, bool THREE, typename SY>
+__device__ void coop_smooth(const LevelDev<T>& L, int nu, SY& sy) {
+    if (L.cross) coop_bottoms<T, THREE>(L, sy);
     for (int s = 0; s < nu; ++s) {
-        for (int c = 0; c < L.ncolor; ++c) { coop_colour<T, THREE>(L, c); grid.sync(); }
-        if (L.cross) coop_bottoms<T, THREE>(L, grid);
+        for (int c = 0; c < L.ncolor; ++c) { coop_colour<T, THREE>(L, c); sy.sync(); }
+        if (L.cross) coop_bottoms<T, THREE>(L, sy);
     }
 }
 
-// V cycle over levels lc..ld (MultiGridSolver.f90:5-192) in one cooperative
-// launch; level ld is solved with the dense operator M (the coarsest level's
-// inverse when ld = 0, otherwise the V cycle below ld as one precomputed map).
-// Level lc's right-hand side is set and its iterate zeroed on entry.
-template <typename T, bool THREE>
-__global__ void __launch_bounds__(kCoopThreads) k_mg_coarse_cycle(const LevelDev<T>* __restrict__ P, int lc, int ld,
-                                                                  const T* __restrict__ M, int nu1, int nu2) {
-    cg::grid_group grid = cg::this_grid();
+// V cycle over levels lc..ld (MultiGridSolver.f90:5-192) in one launch whose
+// phases are separated by the barrier SY; level ld is solved with the dense
+// operator M (the coarsest level's inverse when ld = 0, otherwise the V cycle
+// below ld as one precomputed map). Level lc's right-hand side is set and its
+// iterate zeroed on entry.
+template <typename T, bool THREE, typename SY>
+__device__ void coarse_body(const LevelDev<T>* __restrict__ P, int lc, int ld, const T* __restrict__ M, int nu1,
+                            int nu2, SY& sy) {
     for (int l = lc; l > ld; --l) {
         const LevelDev<T>& L = P[l];
         const LevelDev<T>& Cc = P[l - 1];
-        coop_smooth<T, THREE>(L, nu1, grid);
+        coop_smooth<T, THREE>(L, nu1, sy);
         if (L.cross) { OW3D_GRID_STRIDE(p, L.N) residual_point<T, THREE, true>(L, p); }
         else { OW3D_GRID_STRIDE(p, L.N) residual_point<T, THREE, false>(L, p); }
-        grid.sync();
+        sy.sync();
         OW3D_GRID_STRIDE(p, Cc.N) restrict_item<T>(L, Cc, L.rv, Cc.bv, Cc.xv, p);
-        grid.sync();
+        sy.sync();
     }
     {
         const LevelDev<T>& Ld = P[ld];
         dense_rows<T>((int)Ld.N, M, Ld.bv, Ld.xv);
-        grid.sync();
+        sy.sync();
     }
     for (int l = ld + 1; l <= lc; ++l) {
         const LevelDev<T>& L = P[l];
         const LevelDev<T>& Cc = P[l - 1];
         OW3D_GRID_STRIDE(p, L.N) prolong_item<T>(L, Cc, Cc.xv, L.xv, p);
-        grid.sync();
-        coop_smooth<T, THREE>(L, nu2, grid);
+        sy.sync();
+        coop_smooth<T, THREE>(L, nu2, sy);
     }
+}
+
+template <typename T, bool THREE>
+__global__ void __launch_bounds__(kCoopThreads) k_mg_coarse_cycle(const LevelDev<T>* __restrict__ P, int lc, int ld,
+                                                                  const T* __restrict__ M, int nu1, int nu2) {
+    GridSync sy{cg::this_grid()};
+    coarse_body<T, THREE>(P, lc, ld, M, nu1, nu2, sy);
 }
 
 inline int nblk(int64_t n, int t = 256) {
@@ -307,7 +320,6 @@ void launch_dense_apply(const LevelDev<T>& L, const T* M, cudaStream_t st) {
 // Block count of the fused coarse kernel: 0 = one block per SM, else at most
 // this many (a tuning knob for measurements, set through the test API).
 std::atomic<int> g_coarse_blocks{0};
-
 // Launch the fused coarse cycle over levels lc..ld with a fully co-resident grid.
 template <typename T, bool THREE>
 static void coarse_cycle(const LevelDev<T>* lev, int lc, int ld, const T* M, int nu1, int nu2, LevelTable<T>& pack,

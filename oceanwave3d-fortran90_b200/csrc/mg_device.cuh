@@ -191,8 +191,11 @@ __device__ T lo_row(const LevelDev<T>& L, const T* x, int k, int i, int j, T& di
 
 // Iterates, right-hand sides and residuals are written by earlier phases of
 // the same fused coarse-level kernel, so they are read with ordinary
-// (coherent) loads, never through the read-only data path; only the stencil
-// and coefficient tables, constant for the whole solve, use __ldg.
+// (coherent) loads, never through the read-only data path: the item functions
+// below take them through pointers without __restrict__ (the per-level
+// kernels, where they are read-only, put the qualifier on their own
+// parameters). Only the stencil and coefficient tables, constant for the
+// whole solve, use __ldg.
 template <typename T>
 __device__ __forceinline__ T ro(const T* p) { return *p; }
 
@@ -221,7 +224,7 @@ __device__ __forceinline__ void residual_point(const LevelDev<T>& L, int64_t p) 
         T dg;
         v = lo_row<T, THREE, CROSS>(L, L.xv, k, i, j, dg);
     } else {
-        const T* __restrict__ xp = L.xv + p;
+        const T* xp = L.xv + p;
         const int ox = Nzg, oy = Nzg * Nxg;
         T ih, ca, cb, c3;
         load_cf(L.cf, c, ih, ca, cb, c3);
@@ -564,7 +567,7 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int base, const Ro
 
 // MGRestriction3DExplicit.f90:19-128 as a gather for coarse point p (also zeroes the coarse iterate).
 template <typename T>
-__device__ void restrict_item(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* __restrict__ rf, T* __restrict__ rc, T* __restrict__ xc, int64_t p) {
+__device__ void restrict_item(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* rf, T* rc, T* xc, int64_t p) {
 
     const int gy = (F.Nyg > 1) ? 1 : 0;
     const int Nzf = F.Nzg - 1, Nyf = F.Nyg - 2 * gy;
@@ -578,7 +581,7 @@ __device__ void restrict_item(const LevelDev<T>& F, const LevelDev<T>& Cc, const
         if (ghost) { rc[p] = T(0); return; }
         const int kf = 2 + (kc - 2) * (1 + zcz), ifn = 2 + (ic - 2) * (1 + xcz), jf = gy ? 2 + (jc - 2) * (1 + ycz) : 1;
         // fine values by 32-bit offsets from (kf, ifn, jf) (levels have < 2^31 points)
-        const T* __restrict__ rb = rf + IX(F, kf, ifn, jf);
+        const T* rb = rf + IX(F, kf, ifn, jf);
         const int fox = F.Nzg, foy = F.Nzg * F.Nxg;
         auto R = [&](int k, int i, int j) -> T { return rb[(k - kf) + (i - ifn) * fox + (j - jf) * foy]; };
         if (kf == F.Nzg) { rc[p] = R(kf, ifn, jf); return; }
@@ -612,7 +615,7 @@ __device__ void restrict_item(const LevelDev<T>& F, const LevelDev<T>& Cc, const
 // fine level's per-direction tables. The free-surface row, the bottom ghost
 // row and the ghost columns are not touched.
 template <typename T>
-__device__ void prolong_item(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* __restrict__ xc, T* __restrict__ xf, int64_t p) {
+__device__ void prolong_item(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* xc, T* xf, int64_t p) {
     const int gy = (F.Nyg > 1) ? 1 : 0;
     int kf, ifn, jf;
     int64_t cfl;
