@@ -126,6 +126,9 @@ typedef struct ow3d_params {
     int    precision;             /* OW3D_PREC_*   */
     int    krylov;                /* OW3D_KRYLOV_* */
     int    device;                /* CUDA device ordinal */
+    /* line 9 (after the build-only knobs, so the layout above is unchanged) */
+    int    StoreDataONOFF;        /* >0: EP_#####.bin every n steps, <0: fort.NNN every -n steps, 0: none */
+    int    formattype;            /* EP file form (1 and the default both write unformatted records) */
 } ow3d_params;
 
 typedef struct ow3d_handle ow3d_handle;
@@ -281,6 +284,41 @@ int ow3d_set_graphs(ow3d_handle* h, int on);
 
 /* Zone-box of relaxation zone `zone` in 1-based ghost-inclusive indices. */
 int ow3d_zone_box(const ow3d_handle* h, int zone, int* i0, int* i1, int* j0, int* j1);
+
+/* ------------------------------------------------------------- files
+ * The reference's result and hot-start files (io.cpp). The *_file functions
+ * work on host arrays only (no device, no handle); the handle forms copy the
+ * state off the device first. Messages of the *_file functions are in
+ * ow3d_io_last_error(). */
+
+/* EP_#####.bin as StoreData writes it (src/IO/StoreData.f90:11-29): three
+ * Fortran unformatted records (32-bit length markers, little-endian):
+ * nx ny | x(nx*ny) y(nx*ny) | E(nx*ny) P(nx*ny), x fastest, ghosts included. */
+int ow3d_write_ep_file(const char* path, int nx, int ny, const double* x, const double* y,
+                       const double* E, const double* P);
+/* fort.NNN as StoreDataAscii writes it (src/IO/StoreDataAscii.f90:21-31):
+ * "x y E P" per point in 4e16.6e3, an empty line after each row. */
+int ow3d_write_ascii_file(const char* path, int nx, int ny, const double* x, const double* y,
+                          const double* E, const double* P);
+/* OceanWave3D.end (OceanWave3DTakeATimeStep.f90:146-162): header line,
+ * "Lx Ly Nx Ny time", then "E P" at the Nx*Ny interior points, x fastest. */
+int ow3d_write_end_file(const char* path, double xtank, double ytank, int Nx, int Ny, double time,
+                        const double* E, const double* P);
+/* Read a hot-start file OceanWave3D.init in that format
+ * (ReadInputFileParameters.f90:113-125, SetupInitialConditions.f90:18-27);
+ * its Nx, Ny must equal the given ones. E, P: Nx*Ny interior values. */
+int ow3d_read_init_file(const char* path, int Nx, int Ny, double* E, double* P, double* time);
+const char* ow3d_io_last_error(void);
+
+/* Handle forms: the current state into dir ("" = working directory).
+ * fields 0 = E, P; 1 = h, hx (the reference's bathymetry file, nr 99999 /
+ * 899). ow3d_store_data applies the deck's StoreDataONOFF schedule at the
+ * handle's current step, as OceanWave3DT0Setup.f90:531-548 (step 0) and
+ * OceanWave3DTakeATimeStep.f90:131-187 do; *files = number written. */
+int ow3d_write_ep(ow3d_handle* h, const char* dir, int nr, int fields);
+int ow3d_write_ascii(ow3d_handle* h, const char* dir, int nr, int fields);
+int ow3d_write_end(ow3d_handle* h, const char* path);
+int ow3d_store_data(ow3d_handle* h, const char* dir, int* files);
 
 const char* ow3d_strerror(int status);
 /* Message of the last failing call on this host thread (empty if none). */

@@ -81,6 +81,39 @@ def read_deck(path):
     return p
 
 
+def _b(path):
+    return str(path).encode()
+
+
+def read_init_file(path, Nx, Ny):
+    """Read a hot-start file (OceanWave3D.init format): interior E, P (Nx*Ny
+    each, x fastest) and the start time."""
+    E = _np.zeros(Nx * Ny); P = _np.zeros(Nx * Ny); t = _C.c_double()
+    st = lib().ow3d_read_init_file(_b(path), Nx, Ny, _d(E), _d(P), _C.byref(t))
+    if st:
+        raise OW3DError(st, "ow3d_read_init_file: " + lib().ow3d_io_last_error().decode())
+    return E, P, t.value
+
+
+def load_ep(path):
+    """Read an EP_#####.bin file (Fortran unformatted records with 32-bit
+    length markers, as StoreData writes it): nx, ny and x, y, E, P as
+    (ny, nx) arrays."""
+    raw = _pathlib.Path(path).read_bytes()
+    recs, pos = [], 0
+    while pos < len(raw):
+        n = int(_np.frombuffer(raw, "<i4", 1, pos)[0])
+        body = raw[pos + 4:pos + 4 + n]
+        if int(_np.frombuffer(raw, "<i4", 1, pos + 4 + n)[0]) != n:
+            raise ValueError(f"{path}: record markers disagree")
+        recs.append(body)
+        pos += n + 8
+    nx, ny = (int(v) for v in _np.frombuffer(recs[0], "<i4"))
+    xy = _np.frombuffer(recs[1], "<f8").reshape(2, ny, nx)
+    ep = _np.frombuffer(recs[2], "<f8").reshape(2, ny, nx)
+    return nx, ny, xy[0], xy[1], ep[0], ep[1]
+
+
 class Simulation:
     """One simulation resident on one GPU (an ow3d_handle)."""
 
@@ -177,6 +210,20 @@ class Simulation:
         a, b, c, d = (_C.c_int() for _ in range(4))
         _check(lib().ow3d_zone_box(self.h, zone, _C.byref(a), _C.byref(b), _C.byref(c), _C.byref(d)), "ow3d_zone_box")
         return a.value, b.value, c.value, d.value
+
+    def write_ep(self, directory, nr, fields=0):
+        _check(lib().ow3d_write_ep(self.h, _b(directory), nr, fields), "ow3d_write_ep")
+
+    def write_ascii(self, directory, nr, fields=0):
+        _check(lib().ow3d_write_ascii(self.h, _b(directory), nr, fields), "ow3d_write_ascii")
+
+    def write_end(self, path):
+        _check(lib().ow3d_write_end(self.h, _b(path)), "ow3d_write_end")
+
+    def store_data(self, directory):
+        n = _C.c_int()
+        _check(lib().ow3d_store_data(self.h, _b(directory), _C.byref(n)), "ow3d_store_data")
+        return n.value
 
     def stats(self):
         s = Stats()

@@ -56,6 +56,7 @@ class Params(C.Structure):
         ("relaxXorY", C.c_char), ("relaxDegrees", C.c_double),
         ("zones", Zone * MAX_ZONES),
         ("precision", C.c_int), ("krylov", C.c_int), ("device", C.c_int),
+        ("StoreDataONOFF", C.c_int), ("formattype", C.c_int),
     ]
 
 
@@ -91,6 +92,7 @@ def default_params(**kw):
     p.relaxONOFF = 0; p.relaxTransientTime = 0.0; p.relaxNo = 0
     p.relaxXorY = b"X"; p.relaxDegrees = 0.0
     p.precision = PREC_FP64; p.krylov = KRYLOV_FGMRES; p.device = 0
+    p.StoreDataONOFF = 0; p.formattype = 0
     for k, v in kw.items():
         if k == "zones":
             for i, z in enumerate(v):
@@ -152,6 +154,15 @@ def declare(lib):
         "ow3d_zone_box": (C.c_int, [H, C.c_int, _I, _I, _I, _I]),
         "ow3d_strerror": (C.c_char_p, [C.c_int]),
         "ow3d_version": (C.c_char_p, []),
+        "ow3d_write_ep_file": (C.c_int, [C.c_char_p, C.c_int, C.c_int, _D, _D, _D, _D]),
+        "ow3d_write_ascii_file": (C.c_int, [C.c_char_p, C.c_int, C.c_int, _D, _D, _D, _D]),
+        "ow3d_write_end_file": (C.c_int, [C.c_char_p, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, _D, _D]),
+        "ow3d_read_init_file": (C.c_int, [C.c_char_p, C.c_int, C.c_int, _D, _D, _D]),
+        "ow3d_io_last_error": (C.c_char_p, []),
+        "ow3d_write_ep": (C.c_int, [H, C.c_char_p, C.c_int, C.c_int]),
+        "ow3d_write_ascii": (C.c_int, [H, C.c_char_p, C.c_int, C.c_int]),
+        "ow3d_write_end": (C.c_int, [H, C.c_char_p]),
+        "ow3d_store_data": (C.c_int, [H, C.c_char_p, _I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -960,6 +960,102 @@ int ow3d_zone_box(const ow3d_handle* H, int zone, int* i0, int* i1, int* j0, int
     return OW3D_OK;
 }
 
+// ------------------------------------------------------------ result files
+namespace {
+// E and P (fields 0) or h and hx (fields 1) on the host, ghosts included, and
+// the grid as the reference's 2-D arrays x(i,j), y(i,j).
+int host_fields(ow3d_handle* H, int fields, std::vector<double>& a, std::vector<double>& b, std::vector<double>& x,
+                std::vector<double>& y) {
+    const GridHost& G = H->G;
+    const size_t C = (size_t)G.C;
+    a.resize(C); b.resize(C); x.resize(C); y.resize(C);
+    if (fields == 0) {
+        CK(cudaMemcpyAsync(a.data(), H->E, C * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+        CK(cudaMemcpyAsync(b.data(), H->P, C * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+        CK(cudaStreamSynchronize(H->st));
+    } else {
+        a = G.h; b = G.hx;
+    }
+    for (int j = 0; j < G.Nyg; ++j)
+        for (int i = 0; i < G.Nxg; ++i) { x[(size_t)j * G.Nxg + i] = G.x[i]; y[(size_t)j * G.Nxg + i] = G.y[j]; }
+    return OW3D_OK;
+}
+}  // namespace
+
+int ow3d_write_ep(ow3d_handle* H, const char* dir, int nr, int fields) {
+    if (!H || nr < 0 || nr > 99999 || fields < 0 || fields > 1) return OW3D_ERR_BAD_INPUT;
+    CK(cudaSetDevice(H->dev));
+    std::vector<double> a, b, x, y;
+    TRY(host_fields(H, fields, a, b, x, y));
+    char name[32];
+    std::snprintf(name, sizeof name, "EP_%05d.bin", nr);
+    std::string path = (dir && *dir) ? std::string(dir) + "/" + name : std::string(name);
+    const int r = ow3d_write_ep_file(path.c_str(), H->G.Nxg, H->G.Nyg, x.data(), y.data(), a.data(), b.data());
+    if (r) g_last_error = ow3d_io_last_error();
+    return r;
+}
+
+int ow3d_write_ascii(ow3d_handle* H, const char* dir, int nr, int fields) {
+    // the unit number 100 + nr names the file with three digits (CHOUT3)
+    if (!H || nr < 0 || 100 + nr > 999 || fields < 0 || fields > 1) return OW3D_ERR_BAD_INPUT;
+    CK(cudaSetDevice(H->dev));
+    std::vector<double> a, b, x, y;
+    TRY(host_fields(H, fields, a, b, x, y));
+    char name[32];
+    std::snprintf(name, sizeof name, "fort.%03d", 100 + nr);
+    std::string path = (dir && *dir) ? std::string(dir) + "/" + name : std::string(name);
+    const int r = ow3d_write_ascii_file(path.c_str(), H->G.Nxg, H->G.Nyg, x.data(), y.data(), a.data(), b.data());
+    if (r) g_last_error = ow3d_io_last_error();
+    return r;
+}
+
+int ow3d_write_end(ow3d_handle* H, const char* path) {
+    if (!H || !path) return OW3D_ERR_BAD_INPUT;
+    CK(cudaSetDevice(H->dev));
+    std::vector<double> a, b, x, y;
+    TRY(host_fields(H, 0, a, b, x, y));
+    const GridHost& G = H->G;
+    std::vector<double> E, P;
+    for (int j = G.gy; j < G.Ny + G.gy; ++j)
+        for (int i = G.gx; i < G.Nx + G.gx; ++i) {
+            E.push_back(a[(size_t)j * G.Nxg + i]);
+            P.push_back(b[(size_t)j * G.Nxg + i]);
+        }
+    // domain size as the reference forms it, x(Nx,1) - x(1,1) and
+    // y(Nx,1) - y(1,1) of its ghost-including arrays (the second is 0)
+    const double xtank = G.x[(size_t)G.Nx - 1] - G.x[0];
+    const double ytank = 0.0;
+    const int r = ow3d_write_end_file(path, xtank, ytank, G.Nx, G.Ny, H->time, E.data(), P.data());
+    if (r) g_last_error = ow3d_io_last_error();
+    return r;
+}
+
+int ow3d_store_data(ow3d_handle* H, const char* dir, int* files) {
+    if (!H) return OW3D_ERR_BAD_INPUT;
+    const int S = H->p.StoreDataONOFF;
+    const int64_t t = H->tstep;
+    int n = 0;
+    auto end_path = [&]() { return (dir && *dir) ? std::string(dir) + "/OceanWave3D.end" : std::string("OceanWave3D.end"); };
+    if (S > 0) {
+        if (t == 0) {
+            TRY(ow3d_write_ep(H, dir, 0, 0)); TRY(ow3d_write_ep(H, dir, 99999, 1)); n = 2;
+        } else if (t % S == 0) {
+            if (t > 99999) { g_last_error = "ow3d_store_data: EP file numbers have five digits"; return OW3D_ERR_BAD_INPUT; }
+            TRY(ow3d_write_ep(H, dir, (int)t, 0)); TRY(ow3d_write_end(H, end_path().c_str())); n = 2;
+        }
+    } else if (S < 0) {
+        if (t == 0) {
+            TRY(ow3d_write_ascii(H, dir, 0, 0)); TRY(ow3d_write_ascii(H, dir, 899, 1)); n = 2;
+        } else if (t % (-S) == 0) {
+            const int64_t nr = t / (-S);
+            if (100 + nr > 999) { g_last_error = "ow3d_store_data: ASCII file numbers have three digits"; return OW3D_ERR_BAD_INPUT; }
+            TRY(ow3d_write_ascii(H, dir, (int)nr, 0)); TRY(ow3d_write_end(H, end_path().c_str())); n = 2;
+        }
+    }
+    if (files) *files = n;
+    return OW3D_OK;
+}
+
 int ow3d_step(ow3d_handle* H, int nsteps) {
     if (!H || nsteps < 0) return OW3D_ERR_BAD_INPUT;
     CK(cudaSetDevice(H->dev));

@@ -403,6 +403,7 @@ int default_params(ow3d_params* p) {
     p->relaxONOFF = 0; p->relaxXorY = 'X';
     for (auto& z : p->zones) { z.XorY = 'X'; z.XorYgen = 'X'; z.PhiOnOff = 1; }
     p->precision = OW3D_PREC_FP64; p->krylov = OW3D_KRYLOV_FGMRES; p->device = 0;
+    p->StoreDataONOFF = 0; p->formattype = 0;
     return OW3D_OK;
 }
 
@@ -497,8 +498,10 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
     }
     r = next();  // stream-function line (always present)
     r = next();  // StoreDataONOFF formattype [iKinematics nOutFiles]
+    if (r.nnum() >= 1) p->StoreDataONOFF = r.n(0);
     if (r.nnum() >= 2) {
         const int ft = r.n(1);
+        p->formattype = ft;
         if (ft == 20 || ft == 21 || ft == 22) {
             const int nout = r.num(3) ? r.n(3) : 0;
             for (int i = 0; i < nout; ++i) next();
