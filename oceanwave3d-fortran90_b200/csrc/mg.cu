@@ -62,14 +62,16 @@ __global__ void k_lo_bottom(LevelDev<T> L) {
     OW3D_GRID_STRIDE(q, (bottom_count<T, THREE>(L))) bottom_item<T, THREE>(L, q);
 }
 
+// Per-level colour pass: two rows per lane (colour_warp2), S lanes per column.
 template <typename T, bool THREE, int S, bool CROSS>
-__global__ void __launch_bounds__(128, 6) k_lo_colour(LevelDev<T> L, int colour) {
+__global__ void __launch_bounds__(128, 4) k_lo_colour(LevelDev<T> L, int colour) {
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t total = colour_count<T, THREE>(L);
-    const RowConst<T> rk = row_const<T, S>(L);
+    const int r = (threadIdx.x & 31) & (S - 1);
+    const RowConst<T> rka = row_const_k<T>(L, 2 + 2 * r), rkb = row_const_k<T>(L, 3 + 2 * r);
     for (int base = (int)warp * (32 / S); base < (int)total; base += (int)nwarps * (32 / S))
-        colour_warp<T, THREE, S, CROSS>(L, colour, base, rk);
+        colour_warp2<T, THREE, S, CROSS>(L, colour, base, rka, rkb);
 }
 
 template <typename T>
@@ -237,9 +239,14 @@ static void colour_launch(const LevelDev<T>& L, int c, cudaStream_t st) {
     if (L.cross) note_launch(), k_lo_colour<T, THREE, S, true><<<(int)blocks, 128, 0, st>>>(L, c);
     else note_launch(), k_lo_colour<T, THREE, S, false><<<(int)blocks, 128, 0, st>>>(L, c);
 }
+// Lanes per column of the two-rows-per-lane pass.
+inline int seg_width2(int Nzg) {
+    const int R2 = (Nzg - 2 + 1) / 2;
+    return R2 <= 2 ? 2 : (R2 <= 4 ? 4 : (R2 <= 8 ? 8 : (R2 <= 16 ? 16 : 32)));
+}
 template <typename T, bool THREE>
 static void colour_dispatch(const LevelDev<T>& L, int c, cudaStream_t st) {
-    switch (seg_width(L.Nzg)) {
+    switch (seg_width2(L.Nzg)) {
         case 2: colour_launch<T, THREE, 2>(L, c, st); break;
         case 4: colour_launch<T, THREE, 4>(L, c, st); break;
         case 8: colour_launch<T, THREE, 8>(L, c, st); break;

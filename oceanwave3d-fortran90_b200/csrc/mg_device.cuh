@@ -565,6 +565,232 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int base, const Ro
     if (edge) ghosts(true, xn, xfs);
 }
 
+// Row constants of row k (clamped to the interior rows 2..Nzg-1).
+template <typename T>
+__device__ __forceinline__ RowConst<T> row_const_k(const LevelDev<T>& L, int k) {
+    k = min(max(k, 2), L.Nzg - 1);
+    RowConst<T> c;
+    c.om = T(1) - __ldg(L.zs + k - 1);
+    c.z0 = sz(L, 1, k, 0); c.z1 = sz(L, 1, k, 1); c.z2 = sz(L, 1, k, 2);
+    c.zz0 = sz(L, 2, k, 0); c.zz1 = sz(L, 2, k, 1); c.zz2 = sz(L, 2, k, 2);
+    return c;
+}
+
+// Colour pass with two rows per lane: a segment of S lanes (S a power of two
+// >= (Nzg-2)/2) owns one column, lane r its rows ka = 2+2r and kb = ka+1. The
+// column's task and its order are colour_warp's; a lane composes its two
+// rows' affine maps before the segment's shuffle scan, so a warp solves 32/S
+// columns and the per-column work (column decode, coefficient and bottom-row
+// loads, the bottom row itself) is shared by twice as many rows.
+template <typename T, bool THREE, int S, bool CROSS>
+__device__ void colour_warp2(const LevelDev<T>& L, int colour, int base, const RowConst<T>& rka,
+                             const RowConst<T>& rkb) {
+    const int Nxg = L.Nxg, Nyg = L.Nyg, Nzg = L.Nzg, R = Nzg - 2;
+    const int lane = threadIdx.x & 31, r = lane & (S - 1);
+    const int nxi = Nxg - 2, nyi = THREE ? Nyg - 2 : 1;
+    const bool four = (L.ncolor == 4);
+    const int ni = (nxi + 1) / 2;
+    const int nj = four ? (nyi + 1) / 2 : nyi;
+    const int total = ni * nj;
+    const unsigned segmask = 0xffffffffu;   // the whole warp runs the scan together
+    T* const X = L.xv;
+    const T* const B = L.bv;
+
+    const int q = base + (lane / S);
+    bool act = q < total;
+    int i = 2, j = THREE ? 2 : 1;
+    if (act) {
+        const int tj = q / ni, ti = q - tj * ni;
+        if (four) {
+            j = THREE ? 2 + 2 * tj + (colour >> 1) : 1;
+            i = 2 + 2 * ti + (colour & 1);
+        } else {
+            j = THREE ? 2 + tj : 1;
+            i = 2 + 2 * ti + ((colour + j) & 1);
+        }
+        act = (i <= Nxg - 1) && (!THREE || j <= Nyg - 1);
+    }
+    const int ka = 2 + 2 * r, kb = ka + 1;
+    const bool va = act && ka <= Nzg - 1, vb = act && kb <= Nzg - 1;
+    const int last = (R - 1) / 2;           // lane holding row Nzg-1 (the free surface follows it)
+    const int c = (i - 1) + Nxg * (j - 1);
+    T* const xc = X + (int64_t)c * Nzg;
+    const T* const bc = B + (int64_t)c * Nzg;
+    const int ox = Nzg, oy = Nzg * Nxg;
+    const bool edge = act && (i <= 3 || i >= Nxg - 2 || (THREE && (j <= 3 || j >= Nyg - 2)));
+
+    auto colidx = [&](int ii, int jj) -> int64_t { return (int64_t)(ii - 1) + (int64_t)Nxg * (jj - 1); };
+    // ghost column cg: Neumann rows of this lane's levels, wa x(ca) + wb x(cb) + wg x(cg) = b;
+    // with post set, the value of this column (ca if own == 1, cb if own == 2)
+    // is the lane's new one
+    auto relax_ghost = [&](int64_t cg, int64_t ca, T wa, int64_t cb, T wb, T wg, int own, bool post, T xna, T xnb,
+                           T xfsn) {
+        auto row = [&](int kk, T xo) {
+            const T v1 = (post && own == 1) ? xo : X[ca * Nzg + kk - 1];
+            const T v2 = (post && own == 2) ? xo : X[cb * Nzg + kk - 1];
+            X[cg * Nzg + kk - 1] = (B[cg * Nzg + kk - 1] - (wa * v1 + wb * v2)) / wg;
+        };
+        if (ka <= Nzg - 1) row(ka, xna);
+        if (kb <= Nzg - 1) row(kb, xnb);
+        if (r == last) row(Nzg, xfsn);
+        if (!CROSS && r == 0) X[cg * Nzg] = B[cg * Nzg];   // identity level-1 row
+    };
+    auto ghosts = [&](bool post, T xna, T xnb, T xfsn) {
+        if (i == 2 || (post && i == 3))
+            relax_ghost(colidx(1, j), colidx(2, j), sx(L, 1, 2, 1), colidx(3, j), sx(L, 1, 2, 2), sx(L, 1, 2, 0),
+                        i == 2 ? 1 : 2, post, xna, xnb, xfsn);
+        if (i == Nxg - 1 || (post && i == Nxg - 2))
+            relax_ghost(colidx(Nxg, j), colidx(Nxg - 2, j), sx(L, 1, Nxg - 1, 0), colidx(Nxg - 1, j),
+                        sx(L, 1, Nxg - 1, 1), sx(L, 1, Nxg - 1, 2), i == Nxg - 1 ? 2 : 1, post, xna, xnb, xfsn);
+        if (THREE) {
+            if (j == 2 || (post && j == 3))
+                relax_ghost(colidx(i, 1), colidx(i, 2), sy(L, 1, 2, 1), colidx(i, 3), sy(L, 1, 2, 2), sy(L, 1, 2, 0),
+                            j == 2 ? 1 : 2, post, xna, xnb, xfsn);
+            if (j == Nyg - 1 || (post && j == Nyg - 2))
+                relax_ghost(colidx(i, Nyg), colidx(i, Nyg - 2), sy(L, 1, Nyg - 1, 0), colidx(i, Nyg - 1),
+                            sy(L, 1, Nyg - 1, 1), sy(L, 1, Nyg - 1, 2), j == Nyg - 1 ? 2 : 1, post, xna, xnb, xfsn);
+        }
+    };
+    if (edge) {
+        if (THREE && (i == 2 || i == Nxg - 1) && (j == 2 || j == Nyg - 1)) {
+            const int64_t cc = colidx(i == 2 ? 1 : Nxg, j == 2 ? 1 : Nyg);
+            for (int kk = r; kk < Nzg; kk += S) X[cc * Nzg + kk] = B[cc * Nzg + kk];
+        }
+        ghosts(false, T(0), T(0), T(0));
+    }
+    __syncwarp();
+
+    // rows ka and kb (clamped for loads; lanes past the last row discard theirs)
+    const int kra = min(ka, Nzg - 1), krb = min(kb, Nzg - 1);
+    T qa = 0, ga = 0, qb = 0, gb = 0, x1 = 0;
+    T bb1 = 0, bl = 0, br = 0, bd = 0, bu = 0;
+    T t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0, t6 = 0;
+    if (act) {
+        T ih, ca, cb, c3;
+        load_cf(L.cf, (int64_t)c, ih, ca, cb, c3);
+        const T* sxp = L.SX + (Nxg + i - 1) * 3;
+        const T wxl = __ldg(sxp), wxc = __ldg(sxp + 1), wxr = __ldg(sxp + 2);
+        T wyd = 0, wyc = 0, wyu = 0;
+        if (THREE) {
+            const T* syp = L.SY + (Nyg + j - 1) * 3;
+            wyd = __ldg(syp); wyc = __ldg(syp + 1); wyu = __ldg(syp + 2);
+        }
+        // q, g of row kr (x_kr = q - g x_{kr-1})
+        auto rowq = [&](int kr, const RowConst<T>& rk, T x0, T xp, T& qo, T& go) {
+            const int o = kr - 1;
+            const T xl = xc[o - ox], xr = xc[o + ox];
+            const T xd = THREE ? xc[o - oy] : T(0), xu = THREE ? xc[o + oy] : T(0);
+            const T bk = bc[o];
+            const T om = rk.om;
+            const T s2 = om * ca, s4 = THREE ? om * cb : T(0);
+            const T s3 = om * c3;
+            const T cz = s2 * s2 + s4 * s4 + ih * ih;
+            T off = wxl * xl + wxr * xr;
+            T diag = wxc + s3 * rk.z1 + cz * rk.zz1;
+            if (THREE) { off += wyd * xd + wyu * xu; diag += wyc; }
+            T lo = s3 * rk.z0 + cz * rk.zz0, up = s3 * rk.z2 + cz * rk.zz2;
+            if (CROSS && s2 != T(0)) {
+                const int jlo = THREE ? j - 1 : j, jhi = THREE ? j + 1 : j;
+                T xz = 0;
+                for (int jj = jlo; jj <= jhi; ++jj) {
+#pragma unroll
+                    for (int kk = 0; kk < 3; ++kk) {
+                        const int kz = kr - 1 + kk;
+                        int sh = 0;
+                        if (kz == 1) { if (i - 1 == 1) sh = 1; if (i + 1 == Nxg) sh = -1; }
+                        T dx = 0;
+#pragma unroll
+                        for (int m = 0; m < 3; ++m) {
+                            const int ii = i - 1 + sh + m;
+                            const T w = sx(L, 1, i - sh, m);
+                            if (ii == i && jj == j && kz <= Nzg - 1) {
+                                const T cf2 = T(2) * s2 * sz(L, 1, kr, kk) * w;
+                                if (kk == 0) lo += cf2; else if (kk == 1) diag += cf2; else up += cf2;
+                            } else {
+                                dx += w * xc[(ii - i) * ox + (jj - j) * oy + (kz - 1)];
+                            }
+                        }
+                        xz += sz(L, 1, kr, kk) * dx;
+                    }
+                }
+                off += T(2) * s2 * xz;
+            }
+            if (THREE && CROSS && s4 != T(0)) {
+                T yz = 0;
+                for (int ii = i - 1; ii <= i + 1; ++ii) {
+#pragma unroll
+                    for (int kk = 0; kk < 3; ++kk) {
+                        const int kz = kr - 1 + kk;
+                        int sh = 0;
+                        if (kz == 1) { if (j - 1 == 1) sh = 1; if (j + 1 == Nyg) sh = -1; }
+                        T dy = 0;
+#pragma unroll
+                        for (int m = 0; m < 3; ++m) {
+                            const int jj = j - 1 + sh + m;
+                            const T w = sy(L, 1, j - sh, m);
+                            if (ii == i && jj == j && kz <= Nzg - 1) {
+                                const T cf2 = T(2) * s4 * sz(L, 1, kr, kk) * w;
+                                if (kk == 0) lo += cf2; else if (kk == 1) diag += cf2; else up += cf2;
+                            } else {
+                                dy += w * xc[(ii - i) * ox + (jj - j) * oy + (kz - 1)];
+                            }
+                        }
+                        yz += sz(L, 1, kr, kk) * dy;
+                    }
+                }
+                off += T(2) * s4 * yz;
+            }
+            const T id = T(1) / diag;
+            qo = x0 + (bk - diag * x0 - up * xp - off) * id;
+            go = lo * id;
+        };
+        const T x0a = xc[kra - 1], xpa = xc[kra], xpb = xc[krb];
+        rowq(kra, rka, x0a, xpa, qa, ga);
+        rowq(krb, rkb, xpa, xpb, qb, gb);            // row kb's old value is row ka's "above"
+        if (!va) { qa = 0; ga = 0; }
+        if (!vb) { qb = 0; gb = 0; }
+        if (!CROSS) {
+            T btv[7];
+            load_bt(L.bt, (int64_t)c, btv);
+            t0 = btv[0]; t1 = btv[1]; t2 = btv[2]; t3 = btv[3]; t4 = btv[4]; t5 = btv[5]; t6 = btv[6];
+            bb1 = bc[0];
+            bl = xc[1 - ox]; br = xc[1 + ox];
+            if (THREE) { bd = xc[1 - oy]; bu = xc[1 + oy]; }
+            T boff = t0 * xc[1] + t1 * xc[2] + t2 * bl + t3 * br;
+            if (THREE) boff += t4 * bd + t5 * bu;
+            x1 = (bb1 - boff) * t6;
+        } else {
+            x1 = xc[0];
+        }
+    }
+    // this lane's two rows as one map x_{ka-1} -> x_kb, then the segment scan
+    T a = 1, bb = 0;
+    if (va) { bb = qa; a = -ga; }
+    if (vb) { bb = qb - gb * bb; a = -gb * a; }
+#pragma unroll
+    for (int d = 1; d < S; d <<= 1) {
+        const T ap = __shfl_up_sync(segmask, a, d, S);
+        const T bp = __shfl_up_sync(segmask, bb, d, S);
+        if (r >= d) { bb = a * bp + bb; a = a * ap; }
+    }
+    const T ae = __shfl_up_sync(segmask, a, 1, S), be = __shfl_up_sync(segmask, bb, 1, S);
+    const T xin = (r == 0) ? x1 : ae * x1 + be;   // new value of row ka-1
+    const T xna = qa - ga * xin;
+    const T xnb = qb - gb * xna;
+    const T x2n = __shfl_sync(segmask, xna, 0, S);
+    const T x3n = __shfl_sync(segmask, xnb, 0, S);
+    if (va) xc[ka - 1] = xna;
+    if (vb) xc[kb - 1] = xnb;
+    const T xfs = act ? bc[Nzg - 1] : T(0);
+    if (act && r == last) xc[Nzg - 1] = xfs;  // free-surface row
+    if (!CROSS && act && r == 0) {
+        T boff = t0 * x2n + t1 * x3n + t2 * bl + t3 * br;
+        if (THREE) boff += t4 * bd + t5 * bu;
+        xc[0] = (bb1 - boff) * t6;
+    }
+    if (edge) ghosts(true, xna, xnb, xfs);
+}
+
 // MGRestriction3DExplicit.f90:19-128 as a gather for coarse point p (also zeroes the coarse iterate).
 template <typename T>
 __device__ void restrict_item(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* rf, T* rc, T* xc, int64_t p) {
