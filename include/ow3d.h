@@ -279,7 +279,12 @@ int ow3d_step_batch(ow3d_handle* const* hs, int n, const int* nsteps, int* statu
 int ow3d_get_stats(const ow3d_handle* h, ow3d_stats* s);
 int ow3d_reset_stats(ow3d_handle* h);
 
-/* Capture each RK stage as a CUDA graph (1) or launch kernels directly (0). */
+/* 1 (the default): from the handle's second solve on, each Arnoldi step of
+ * the FGMRES solve with the multigrid preconditioner (V-cycle, operator,
+ * orthogonalisation) is one CUDA graph launch, captured on first use per
+ * step index and surface arrays; 0: kernels are launched one by one. The
+ * left-preconditioned variant always launches directly. Results are the
+ * same either way. */
 int ow3d_set_graphs(ow3d_handle* h, int on);
 
 /* Zone-box of relaxation zone `zone` in 1-based ghost-inclusive indices. */

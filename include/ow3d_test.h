@@ -35,6 +35,10 @@ unsigned long long ow3d_launch_count(void);
  * the previous value. Process-wide. */
 int ow3d_test_set_coarse_blocks(int blocks);
 
+/* Number of captured Arnoldi-step graphs the handle holds, or -1 when a
+ * capture failed and the handle launches kernels directly. */
+int ow3d_test_graph_count(const ow3d_handle* h);
+
 /* Device time of `reps` launches of one kernel on this handle's stream,
  * measured with CUDA events around each launch; before each launch a write of
  * the Krylov basis (larger than L2) evicts the inputs from L2, outside the

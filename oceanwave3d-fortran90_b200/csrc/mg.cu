@@ -327,6 +327,8 @@ void launch_dense_apply(const LevelDev<T>& L, const T* M, cudaStream_t st) {
 // Block count of the fused coarse kernel: 0 = one block per SM, else at most
 // this many (a tuning knob for measurements, set through the test API).
 std::atomic<int> g_coarse_blocks{0};
+thread_local bool g_capture_unsafe = false;
+
 // Launch the fused coarse cycle over levels lc..ld with a fully co-resident grid.
 template <typename T, bool THREE>
 static void coarse_cycle(const LevelDev<T>* lev, int lc, int ld, const T* M, int nu1, int nu2, LevelTable<T>& pack,
@@ -348,8 +350,18 @@ static void coarse_cycle(const LevelDev<T>* lev, int lc, int ld, const T* M, int
     // by a run-time level would be copied to every thread's stack); upload it
     // only when a level's pointers or sizes changed since the last launch
     if (std::memcmp(pack.host, lev, sizeof(LevelDev<T>) * (size_t)(lc + 1)) != 0) {
-        std::memcpy(pack.host, lev, sizeof(LevelDev<T>) * (size_t)(lc + 1));
-        cudaMemcpyAsync(pack.dev, pack.host, sizeof(LevelDev<T>) * (size_t)(lc + 1), cudaMemcpyHostToDevice, st);
+        // Inside a stream capture this copy would replay from a host buffer
+        // that later calls overwrite: mark the capture unusable and leave the
+        // host image as it was, so that the direct launches that replace the
+        // capture upload the table themselves.
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(st, &cs);
+        if (cs != cudaStreamCaptureStatusNone) {
+            g_capture_unsafe = true;
+        } else {
+            std::memcpy(pack.host, lev, sizeof(LevelDev<T>) * (size_t)(lc + 1));
+            cudaMemcpyAsync(pack.dev, pack.host, sizeof(LevelDev<T>) * (size_t)(lc + 1), cudaMemcpyHostToDevice, st);
+        }
     }
     const LevelDev<T>* P = pack.dev;
     void* args[] = {(void*)&P, (void*)&lc, (void*)&ld, (void*)&M, (void*)&nu1, (void*)&nu2};

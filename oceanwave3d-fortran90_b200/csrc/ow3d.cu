@@ -96,7 +96,17 @@ struct ow3d_handle {
     double time = 0;
     int64_t tstep = 0;
     ow3d_stats stats{};
-    int graphs = 0;
+    // CUDA graphs of the FGMRES Arnoldi step (preconditioner, operator,
+    // DCGS2 passes), one per step index j and sigma-surface arrays
+    struct IterGraph {
+        const double* surf[5];
+        int j;
+        cudaGraphExec_t exec;
+        unsigned long long kernels;   // kernel nodes, counted per replay
+    };
+    std::vector<IterGraph> iter_graphs;
+    int graphs = 1;
+    bool graphs_failed = false;
 };
 
 namespace {
@@ -418,6 +428,71 @@ int sync_ks_small(ow3d_handle* H) {
     return OW3D_OK;
 }
 
+// The kernels of FGMRES Arnoldi step j with the multigrid preconditioner:
+// z_j = M^{-1} v_j, w = A z_j into V_{j+1}, DCGS2 reduction and update.
+void fgmres_step_launches(ow3d_handle* H, const Surface& s, int j, int maxmv, int m) {
+    const int64_t N = H->G.N;
+    double* Vj = H->V + (int64_t)j * H->ldv;
+    double* Vn = H->V + (int64_t)(j + 1) * H->ldv;
+    const double* sj = &H->ks->scale[j];
+    if (!H->mixed) {
+        double* Zj = (double*)H->Z + (int64_t)j * H->ldv;
+        run_precond<double>(H, H->mg64, Vj, sj, Zj);
+        launch_ho_matvec<double>(H->hg, s, Zj, nullptr, nullptr, Vn, 0, H->st);
+    } else {
+        float* Zj = (float*)H->Z + (int64_t)j * H->ldv;
+        run_precond<float>(H, H->mg32, Vj, sj, Zj);
+        launch_ho_matvec<float>(H->hg, s, Zj, nullptr, nullptr, Vn, 0, H->st);
+    }
+    launch_dcgs_reduce(H->V, H->ldv, j, Vn, N, H->dsc, H->ks, H->st);
+    launch_dcgs_update(H->V, H->ldv, j, Vn, N, H->dsc, H->ks, maxmv, m, H->st);
+}
+
+// Step j as a CUDA graph: captured on its first use (the handle has finished
+// a solve by then, so every one-time set-up of the launches is done),
+// replayed afterwards. The launch sequence depends on j and on the surface
+// arrays only; everything else it touches is fixed for the handle's
+// lifetime. A capture that fails switches the handle to direct launches.
+int fgmres_step_graph(ow3d_handle* H, const Surface& s, int j, int maxmv, int m) {
+    const double* key[5] = {s.E, s.Ex, s.Exx, s.Ey, s.Eyy};
+    ow3d_handle::IterGraph* g = nullptr;
+    for (auto& q : H->iter_graphs)
+        if (q.j == j && std::memcmp(q.surf, key, sizeof key) == 0) { g = &q; break; }
+    if (!g) {
+        const unsigned long long k0 = g_kernel_launches.load(std::memory_order_relaxed);
+        cudaGraph_t graph = nullptr;
+        g_capture_unsafe = false;
+        cudaError_t e = cudaStreamBeginCapture(H->st, cudaStreamCaptureModeThreadLocal);
+        unsigned long long nk = 0;
+        if (e == cudaSuccess) {
+            fgmres_step_launches(H, s, j, maxmv, m);
+            e = cudaStreamEndCapture(H->st, &graph);
+            if (e == cudaSuccess && g_capture_unsafe) e = cudaErrorStreamCaptureUnsupported;
+        }
+        // the captured launches did not run: count them per replay instead
+        nk = g_kernel_launches.load(std::memory_order_relaxed) - k0;
+        g_kernel_launches.fetch_sub(nk, std::memory_order_relaxed);
+        cudaGraphExec_t ex = nullptr;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&ex, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            H->graphs_failed = true;
+            fgmres_step_launches(H, s, j, maxmv, m);
+            CK(cudaGetLastError());
+            return OW3D_OK;
+        }
+        ow3d_handle::IterGraph ng;
+        std::memcpy(ng.surf, key, sizeof key);
+        ng.j = j; ng.exec = ex; ng.kernels = nk;
+        H->iter_graphs.push_back(ng);
+        g = &H->iter_graphs.back();
+    }
+    CK(cudaGraphLaunch(g->exec, H->st));
+    g_kernel_launches.fetch_add(g->kernels, std::memory_order_relaxed);
+    return OW3D_OK;
+}
+
 // One Laplace solve on the device: phi <- A^{-1} rhs, initial guess in phi.
 int solve_device(ow3d_handle* H, const double* rhs, double* phi, const Surface& s, int* iters_out) {
     const int64_t N = H->G.N;
@@ -437,6 +512,13 @@ int solve_device(ow3d_handle* H, const double* rhs, double* phi, const Surface& 
         TRY(sync_ks_small(H));
         int j = 0;
         while (!H->ks_host->done) {
+            if (!left && H->nlev > 0 && H->graphs && !H->graphs_failed && H->stats.solves > 0) {
+                // FGMRES step j as one graph launch
+                TRY(fgmres_step_graph(H, s, j, maxmv, m));
+                TRY(sync_ks_small(H));
+                ++j;
+                continue;
+            }
             double* Vj = H->V + (int64_t)j * H->ldv;
             double* Vn = H->V + (int64_t)(j + 1) * H->ldv;
             const double* sj = &H->ks->scale[j];
@@ -761,6 +843,11 @@ unsigned long long ow3d_launch_count(void) { return g_kernel_launches.load(std::
 
 int ow3d_test_set_coarse_blocks(int blocks) { return g_coarse_blocks.exchange(blocks < 0 ? 0 : blocks); }
 
+int ow3d_test_graph_count(const ow3d_handle* H) {
+    if (!H) return OW3D_ERR_BAD_INPUT;
+    return H->graphs_failed ? -1 : (int)H->iter_graphs.size();
+}
+
 int ow3d_default_params(ow3d_params* p) { return default_params(p); }
 
 int ow3d_read_deck(const char* path, ow3d_params* p) {
@@ -784,6 +871,7 @@ int ow3d_destroy(ow3d_handle* H) {
     if (!H) return OW3D_OK;
     cudaSetDevice(H->dev);
     if (H->st) cudaStreamSynchronize(H->st);
+    for (auto& g : H->iter_graphs) cudaGraphExecDestroy(g.exec);
     for (void* q : H->allocs) cudaFree(q);
     if (H->ks_host) cudaFreeHost(H->ks_host);
     if (H->flag_host) cudaFreeHost(H->flag_host);
@@ -1144,7 +1232,7 @@ int ow3d_reset_stats(ow3d_handle* H) {
 
 int ow3d_set_graphs(ow3d_handle* H, int on) {
     if (!H) return OW3D_ERR_BAD_INPUT;
-    H->graphs = on;
+    H->graphs = on ? 1 : 0;
     return OW3D_OK;
 }
 

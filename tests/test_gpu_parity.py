@@ -204,3 +204,32 @@ def test_mixed_precision_error(ow3d, oracle):
     Eo, Po, Wo, phio, to = orc.get_state()
     assert rel(E, Eo) < 1e-6
     assert rel(phi, phio) < 1e-6
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "mixed"])
+def test_graph_launched_steps_match_direct_launches(ow3d, precision):
+    """FGMRES steps replayed as CUDA graphs (the default from the second solve
+    on) give bitwise the same state and launch count as direct launches."""
+    # large enough that the finest multigrid level runs outside the fused
+    # coarse kernel (the graph path's case; on smaller grids it falls back)
+    p, geo = cases.bump_3d(Nx=257, Ny=33, Nz=17, Lx=16.0, Ly=2.0, dt=0.02)
+    p.precision = precision
+    Nxg, Nyg = p.Nx + 2, p.Ny + 2
+    x = (np.arange(Nxg) - 1) / (p.Nx - 1) * p.Lx
+    E0 = np.tile(0.01 * np.cos(np.pi * x / p.Lx), Nyg)
+    L = ow3d.lib()
+    out = []
+    for graphs in (1, 0):
+        sim = ow3d.Simulation(p, **geo)
+        assert L.ow3d_set_graphs(sim.h, graphs) == 0
+        sim.set_state(E0, np.zeros_like(E0))
+        n0 = L.ow3d_launch_count()
+        assert sim.step(3) >= 0
+        out.append((sim.get_state(), L.ow3d_launch_count() - n0, sim.stats()["total_iterations"]))
+        ng_cached = L.ow3d_test_graph_count(sim.h)
+        assert (ng_cached > 0) if graphs else (ng_cached == 0), ng_cached
+        sim.close()
+    (sg, ng, ig), (sd, nd, idd) = out
+    for a, b in zip(sg[:4], sd[:4]):
+        assert np.array_equal(a, b)
+    assert ng == nd and ig == idd
