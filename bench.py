@@ -208,7 +208,7 @@ def kernel_roofline(pkg, p, dev):
 def profiled_traffic(kernel):
     """DRAM bytes (read + write) per launch of `kernel` from its committed ncu
     summary (the `traffic_bytes_per_launch:` line), or None."""
-    for f in sorted((ROOT / "profiles").glob(f"{kernel}_*.md")):
+    for f in sorted((ROOT / "profiles").glob(f"{kernel}_irregular_sea_*.md")):
         m = re.search(r"^traffic_bytes_per_launch:\s*(\d+)", f.read_text(), re.M)
         if m:
             return int(m.group(1))
