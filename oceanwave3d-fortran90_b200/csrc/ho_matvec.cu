@@ -34,6 +34,18 @@ namespace {
 constexpr int kZMax = 34;   // largest Nzg the library accepts (Nz <= 33)
 constexpr int kBand = 5;    // columns from each wall handled by the band path
 
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(smem_u32(dst)), "l"(src), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+// Levels of a tile's first staging group: the rows these complete are
+// computed while the remaining levels are still arriving.
+__host__ __device__ constexpr int stage_split(int nzg) { return nzg > 0 ? (nzg + 2) / 2 : 0; }
+
 __device__ __forceinline__ int win_start(int i, int n) {  // 1-based DiffXEven window start, half width 3
     return i <= 3 ? 1 : (i <= n - 3 ? i - 3 : n - 6);
 }
@@ -238,12 +250,13 @@ __device__ void ho_column_general(const HoGrid& g, const Surface& s, const TIN* 
 template <int NZG, bool THREE, typename ZT, typename PF>
 __device__ __forceinline__ void ho_column_tile(const HoGrid& g, const Surface& s, double scale,
                                                const double* __restrict__ b, double* __restrict__ y, int mode,
-                                               const ZT& zt, int i, int j, const PF& P) {
+                                               const ZT& zt, int i, int j, bool active, const PF& P) {
     constexpr int ZA = NZG > 0 ? NZG : kZMax;
     const int Nzg = NZG > 0 ? NZG : g.Nzg;
     const int64_t col = (int64_t)(i - 1) + (int64_t)g.Nxg * (j - 1);
     const int64_t gb = col * Nzg;
     auto emit = [&](int k, double v) {
+        if (!active) return;
         if (mode == 0) y[gb + k - 1] = scale * v;
         else y[gb + k - 1] = b[gb + k - 1] - v;
     };
@@ -300,6 +313,10 @@ __device__ __forceinline__ void ho_column_tile(const HoGrid& g, const Surface& s
     if constexpr (NZG > 0) {
 #pragma unroll
         for (int kk = 1; kk <= NZG; ++kk) {
+            if (kk == stage_split(NZG) + 1) {   // the upper levels of the tile
+                cp_wait<0>();
+                __syncthreads();
+            }
             level(kk);
 #pragma unroll
             for (int k = 1; k <= NZG; ++k)
@@ -330,34 +347,50 @@ __global__ void __launch_bounds__(THREE ? 256 : 256, 2)
         return;
     }
     // interior tile: columns i0..i0+BX-1 (x), j0..j0+BY-1 (y) inside [kBand+1, N-kBand]
-    extern __shared__ double sm[];
+    extern __shared__ __align__(16) unsigned char smraw[];
+    TIN* const sm = reinterpret_cast<TIN*>(smraw);
     const int NZP = Nzg | 1;   // odd column pitch
     const int t = (int)blockIdx.x - band_blocks;
     const int ty_ = t / tiles_x, tx_ = t - ty_ * tiles_x;
     const int i0 = kBand + 1 + tx_ * BX;
     const int j0 = THREE ? kBand + 1 + ty_ * BY : 1;
     const int ilo = i0 - 3, jlo = THREE ? j0 - 3 : 1;
-    // stage: each staged y row's column range is contiguous in global memory
+    // stage with cp.async in two groups, levels [0, KA) then [KA, Nzg); each
+    // staged y row's column range is contiguous in global memory
+    constexpr int KA0 = stage_split(NZG);
+    const int KA = NZG > 0 ? KA0 : Nzg;
     const int ncolx = min(HX, Nxg - ilo + 1);
-    for (int r = 0; r < HY; ++r) {
-        const int jj = jlo + r;
-        if (jj > Nyg) break;
-        const int64_t gbase = ((int64_t)(jj - 1) * Nxg + (ilo - 1)) * Nzg;
-        const int cnt = ncolx * Nzg;
-        double* dst = sm + (int64_t)r * HX * NZP;
-#pragma unroll 8
-        for (int e = tid; e < cnt; e += blockDim.x) {
-            const int cc = e / Nzg, k = e - cc * Nzg;
-            dst[cc * NZP + k] = (double)phi[gbase + e];
+    auto stage = [&](int k0, int k1) {
+        const int nk = k1 - k0;
+        if (nk <= 0) return;
+        for (int r = 0; r < HY; ++r) {
+            const int jj = jlo + r;
+            if (jj > Nyg) break;
+            const TIN* src = phi + ((int64_t)(jj - 1) * Nxg + (ilo - 1)) * Nzg;
+            TIN* dst = sm + (int64_t)r * HX * NZP;
+            const int cnt = ncolx * nk;
+            for (int e = tid; e < cnt; e += blockDim.x) {
+                const int cc = e / nk, k = k0 + (e - cc * nk);
+                cp_async<sizeof(TIN)>(dst + cc * NZP + k, src + (int64_t)cc * Nzg + k);
+            }
         }
-    }
+    };
+    stage(0, KA);
+    cp_commit();
+    stage(KA, Nzg);
+    cp_commit();
+    if (NZG > 0) cp_wait<1>();
+    else cp_wait<0>();
     __syncthreads();
+    // every thread stays to the end (the tile's second barrier); threads past
+    // the interior work on the nearest interior column and store nothing
     const int lx = tid % BX, ly = tid / BX;
     const int i = i0 + lx, j = j0 + ly;
-    if (i > Nxg - kBand || (THREE && j > Nyg - kBand)) return;
-    const double* base = sm + ((int64_t)(ly + (THREE ? 3 : 0)) * HX + (lx + 3)) * NZP;
-    auto P = [&](int k, int di, int dj) -> double { return base[((int64_t)dj * HX + di) * NZP + (k - 1)]; };
-    ho_column_tile<NZG, THREE>(g, s, scale, b, y, mode, zt, i, j, P);
+    const bool active = i <= Nxg - kBand && (!THREE || j <= Nyg - kBand);
+    const int ic = min(i, Nxg - kBand), jc = THREE ? min(j, Nyg - kBand) : 1;
+    const TIN* base = sm + ((int64_t)(jc - j0 + (THREE ? 3 : 0)) * HX + (ic - i0 + 3)) * NZP;
+    auto P = [&](int k, int di, int dj) -> double { return (double)base[((int64_t)dj * HX + di) * NZP + (k - 1)]; };
+    ho_column_tile<NZG, THREE>(g, s, scale, b, y, mode, zt, ic, jc, active, P);
 }
 
 template <int NZG, bool THREE, typename TIN>
@@ -402,7 +435,7 @@ void launch_impl(const HoGrid& g, const Surface& s, const TIN* phi, const double
     const int threads = BX * BY;
     const int band_blocks = (int)((nband + threads - 1) / threads);
     const int NZP = g.Nzg | 1;
-    const size_t smem = (size_t)HX * HY * NZP * sizeof(double);
+    const size_t smem = (size_t)HX * HY * NZP * sizeof(TIN);
     // the shared-memory opt-in is per device; setting it twice is harmless,
     // so concurrent first launches from several host threads need no lock
     static std::atomic<unsigned long long> attr_set{0ull};
