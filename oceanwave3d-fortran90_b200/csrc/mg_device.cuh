@@ -45,6 +45,18 @@ __device__ __forceinline__ void load_bt(const float* bt, int64_t c, float* o) {
     o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w; o[4] = b.x; o[5] = b.y; o[6] = b.z;
 }
 
+// All eight bottom-row coefficients of a column.
+__device__ __forceinline__ void load_bt8(const double* bt, int64_t c, double* o) {
+    const double2* p = reinterpret_cast<const double2*>(bt) + 4 * c;
+    const double2 a = __ldg(p), b = __ldg(p + 1), d = __ldg(p + 2), e = __ldg(p + 3);
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y; o[4] = d.x; o[5] = d.y; o[6] = e.x; o[7] = e.y;
+}
+__device__ __forceinline__ void load_bt8(const float* bt, int64_t c, float* o) {
+    const float4* p = reinterpret_cast<const float4*>(bt) + 2 * c;
+    const float4 a = __ldg(p), b = __ldg(p + 1);
+    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w; o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
+}
+
 template <typename T>
 __device__ __forceinline__ int64_t IX(const LevelDev<T>& L, int k, int i, int j) {
     return (int64_t)(k - 1) + (int64_t)L.Nzg * ((int64_t)(i - 1) + (int64_t)L.Nxg * (j - 1));
@@ -209,10 +221,14 @@ __device__ __forceinline__ void residual_item(const LevelDev<T>& L, int64_t p) {
 }
 
 // Residual r = b - A x at point p (k fastest, so a warp covers about two
-// columns and the column constants are the same for most of its lanes).
-// Interior rows address the neighbours by offsets from the point; ghost
-// columns, the bottom and free-surface rows and levels with mixed-derivative
-// terms take lo_row.
+// columns). On levels without mixed-derivative terms the rows of an interior
+// column -- interior rows, the bottom row (BuildLinearSystemMatrix.f90:50-70)
+// and the free-surface row -- are all a 7-term combination of the same seven
+// values: the column at levels kk-1, kk, kk+1 and the four neighbour columns
+// at level kk (kk = 2 for the bottom row, the row itself otherwise), so the
+// lanes of a warp share one branch-free form and only select their
+// coefficients. Ghost columns and levels with mixed-derivative terms take
+// lo_row.
 template <typename T, bool THREE, bool CROSS>
 __device__ __forceinline__ void residual_point(const LevelDev<T>& L, int64_t p) {
     int k, i, j;
@@ -220,37 +236,40 @@ __device__ __forceinline__ void residual_point(const LevelDev<T>& L, int64_t p) 
     decomp(L, p, k, c, i, j);
     const int Nzg = L.Nzg, Nxg = L.Nxg;
     T v;
-    if (CROSS || k == 1 || k == Nzg || is_ghost_col<T, THREE>(L, i, j)) {
+    if (CROSS || is_ghost_col<T, THREE>(L, i, j)) {
         T dg;
         v = lo_row<T, THREE, CROSS>(L, L.xv, k, i, j, dg);
     } else {
-        const T* xp = L.xv + p;
+        const bool bot = (k == 1), top = (k == Nzg);
+        const int kk = bot ? 2 : (top ? Nzg - 1 : k);
+        const T* xp = L.xv + c * Nzg + (kk - 1);
         const int ox = Nzg, oy = Nzg * Nxg;
+        // interior-row coefficients of row kk
         T ih, ca, cb, c3;
         load_cf(L.cf, c, ih, ca, cb, c3);
         const T* sxp = L.SX + (Nxg + i - 1) * 3;       // order 2, position i
-        const T* zp1 = L.SZ + (k - 1) * 3;             // order 1, row k
-        const T* zp2 = L.SZ + (Nzg + k - 1) * 3;       // order 2, row k
-        const T om = T(1) - __ldg(L.zs + k - 1);
+        const T* zp1 = L.SZ + (kk - 1) * 3;            // order 1, row kk
+        const T* zp2 = L.SZ + (Nzg + kk - 1) * 3;      // order 2, row kk
+        const T om = T(1) - __ldg(L.zs + kk - 1);
         const T s2 = om * ca, s4 = THREE ? om * cb : T(0);
         const T s3 = om * c3;
         const T cz = s2 * s2 + s4 * s4 + ih * ih;
-        const T x0 = xp[0];
-        T acc = __ldg(sxp) * xp[-ox];
-        acc += __ldg(sxp + 1) * x0;
-        acc += __ldg(sxp + 2) * xp[ox];
+        const T wx0 = __ldg(sxp), wx1 = __ldg(sxp + 1), wx2 = __ldg(sxp + 2);
+        T wy0 = 0, wy1 = 0, wy2 = 0;
         if (THREE) {
             const T* syp = L.SY + (L.Nyg + j - 1) * 3;
-            acc += __ldg(syp) * xp[-oy];
-            acc += __ldg(syp + 1) * x0;
-            acc += __ldg(syp + 2) * xp[oy];
+            wy0 = __ldg(syp); wy1 = __ldg(syp + 1); wy2 = __ldg(syp + 2);
         }
-        const T xd = xp[-1], xu = xp[1];
-        T dz = __ldg(zp1) * xd, dzz = __ldg(zp2) * xd;
-        dz += __ldg(zp1 + 1) * x0; dzz += __ldg(zp2 + 1) * x0;
-        dz += __ldg(zp1 + 2) * xu; dzz += __ldg(zp2 + 2) * xu;
-        acc += s3 * dz + cz * dzz;
-        v = acc;
+        T cm = s3 * __ldg(zp1) + cz * __ldg(zp2);
+        T c0 = wx1 + wy1 + s3 * __ldg(zp1 + 1) + cz * __ldg(zp2 + 1);
+        T cq = s3 * __ldg(zp1 + 2) + cz * __ldg(zp2 + 2);
+        T cl = wx0, cr = wx2, cd = wy0, cu = wy2;
+        T bt[8];
+        load_bt8(L.bt, c, bt);
+        if (bot) { cm = bt[7]; c0 = bt[0]; cq = bt[1]; cl = bt[2]; cr = bt[3]; cd = bt[4]; cu = bt[5]; }
+        if (top) { cm = 0; c0 = 0; cq = 1; cl = 0; cr = 0; cd = 0; cu = 0; }
+        v = cm * xp[-1] + c0 * xp[0] + cq * xp[1] + cl * xp[-ox] + cr * xp[ox];
+        if (THREE) v += cd * xp[-oy] + cu * xp[oy];
     }
     L.rv[p] = L.bv[p] - v;
 }

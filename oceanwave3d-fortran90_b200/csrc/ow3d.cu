@@ -209,6 +209,7 @@ int build_levels(ow3d_handle* H, MgSet<T>& S, bool alloc_fine_x) {
                         o[5] = hyq * wy[2];
                     }
                     o[6] = 1.0 / (f * z0);
+                    o[7] = f * z0;
                 }
             T* btd;
             TRY(upload(H, &btd, bt));

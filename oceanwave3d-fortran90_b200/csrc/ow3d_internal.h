@@ -74,7 +74,8 @@ struct LevelDev {
     const T* cf;            // [Nxg*Nyg][4]
     // per column, the bottom row's Gauss-Seidel coefficients (levels without
     // mixed-derivative terms): x2, x3 of the column, row 2 of the left, right,
-    // lower and upper neighbours, and 1/diagonal
+    // lower and upper neighbours, 1/diagonal, and the diagonal (coefficient
+    // of x1)
     const T* bt;            // [Nxg*Nyg][8]
     uint64_t mz, mx;        // division magics for Nzg and Nxg (see qdiv)
     uint32_t mz32, mx32;    // 32-bit magics for Nzg and Nxg (see div32) and their shifts
