@@ -360,57 +360,88 @@ __device__ void dcgs_column(KrylovState* ks, int j, const double* res) {
     ks->coefB[j] = hj * ks->scale[j];
 }
 
-// Reduction, grid (nbx, j+1): block (bx, v) forms partials of <V_v, V_j> and
-// <V_v, W> over a slice (V_j and W are re-read per v from L2). The last block
-// reduces everything and runs dcgs_column.
+// Reduction: res[2v] = <V_v, V_j>, res[2v+1] = <V_v, W> for v <= j. The
+// vectors are cut into chunks of kDotE * blockDim.x element pairs; a block
+// takes chunks in turn, keeps its thread's kDotE pairs of V_j and W in
+// registers, and streams every V_v of the chunk once (so each vector is read
+// from memory once per step). Per vector, each warp adds its sum to its own
+// shared-memory slot; the block's slots become partial[u * gridDim.x + b];
+// the last block reduces the partials in a fixed order and runs dcgs_column.
+constexpr int kDotE = 4;
+constexpr int kDotG = 4;   // vectors whose loads are issued together
+
 __global__ void __launch_bounds__(kThreads) k_dcgs_reduce(const double* __restrict__ V, int64_t ldv, int j,
                                                           const double* __restrict__ W, int64_t n, double* partial,
                                                           unsigned int* counter, int nbx, KrylovState* ks) {
     if (ks->done) return;
-    const int v = blockIdx.y;
+    __shared__ double acc[2 * kMaxDots][kThreads / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int nv = 2 * (j + 1);
+    for (int u = threadIdx.x; u < nv * nw; u += blockDim.x) acc[u / nw][u % nw] = 0.0;
+    __syncthreads();
     const int64_t n2 = (n + 1) / 2;
-    const double2* a2 = reinterpret_cast<const double2*>(V + (int64_t)v * ldv);
+    const int64_t chunk = (int64_t)kDotE * blockDim.x;
+    const int64_t nchunks = (n2 + chunk - 1) / chunk;
     const double2* q2 = reinterpret_cast<const double2*>(V + (int64_t)j * ldv);
     const double2* w2 = reinterpret_cast<const double2*>(W);
-    const int64_t stride = (int64_t)nbx * blockDim.x;
-    double s0 = 0, s1 = 0, t0 = 0, t1 = 0;
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    for (; t + stride < n2; t += 2 * stride) {
-        const double2 x0 = a2[t], x1 = a2[t + stride];
-        const double2 q0 = q2[t], q1 = q2[t + stride];
-        const double2 y0 = w2[t], y1 = w2[t + stride];
-        s0 += x0.x * q0.x + x0.y * q0.y; s1 += x1.x * q1.x + x1.y * q1.y;
-        t0 += x0.x * y0.x + x0.y * y0.y; t1 += x1.x * y1.x + x1.y * y1.y;
+    for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+        const int64_t t0 = ch * chunk + threadIdx.x;
+        double2 q[kDotE], w[kDotE];
+#pragma unroll
+        for (int e = 0; e < kDotE; ++e) {
+            const int64_t t = t0 + (int64_t)e * blockDim.x;
+            if (t < n2) { q[e] = q2[t]; w[e] = w2[t]; }
+            else { q[e] = make_double2(0.0, 0.0); w[e] = make_double2(0.0, 0.0); }
+        }
+        // vectors in groups of kDotG, all their loads in flight together
+        for (int v0 = 0; v0 <= j; v0 += kDotG) {
+            double2 x[kDotG][kDotE];
+#pragma unroll
+            for (int g = 0; g < kDotG; ++g) {
+                const int v = v0 + g;
+                const double2* a2 = reinterpret_cast<const double2*>(V + (int64_t)min(v, j) * ldv);
+#pragma unroll
+                for (int e = 0; e < kDotE; ++e) {
+                    const int64_t t = t0 + (int64_t)e * blockDim.x;
+                    x[g][e] = (v < j && t < n2) ? a2[t] : make_double2(0.0, 0.0);
+                }
+            }
+#pragma unroll
+            for (int g = 0; g < kDotG; ++g) {
+                const int v = v0 + g;
+                if (v > j) break;
+                double sa = 0, sb = 0;
+#pragma unroll
+                for (int e = 0; e < kDotE; ++e) {
+                    const double2 xe = (v == j) ? q[e] : x[g][e];
+                    sa += xe.x * q[e].x + xe.y * q[e].y;
+                    sb += xe.x * w[e].x + xe.y * w[e].y;
+                }
+                sa = warp_sum(sa);
+                sb = warp_sum(sb);
+                if (lane == 0) { acc[2 * v][wid] += sa; acc[2 * v + 1][wid] += sb; }
+            }
+        }
     }
-    for (; t < n2; t += stride) {
-        const double2 x0 = a2[t], q0 = q2[t], y0 = w2[t];
-        s0 += x0.x * q0.x + x0.y * q0.y;
-        t0 += x0.x * y0.x + x0.y * y0.y;
-    }
-    __shared__ double red[2][kThreads / 32];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const double sa = warp_sum(s0 + s1), sb = warp_sum(t0 + t1);
-    if (lane == 0) { red[0][wid] = sa; red[1][wid] = sb; }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double pa = 0, pb = 0;
-        for (int q = 0; q < (int)(blockDim.x / 32); ++q) { pa += red[0][q]; pb += red[1][q]; }
-        partial[(int64_t)(2 * v) * nbx + blockIdx.x] = pa;
-        partial[(int64_t)(2 * v + 1) * nbx + blockIdx.x] = pb;
+    for (int u = threadIdx.x; u < nv; u += blockDim.x) {
+        double t = 0;
+        for (int w = 0; w < nw; ++w) t += acc[u][w];
+        partial[(int64_t)u * gridDim.x + blockIdx.x] = t;
     }
     __shared__ bool amlast;
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) amlast = (atomicAdd(counter, 1u) == gridDim.x * gridDim.y - 1);
+    if (threadIdx.x == 0) amlast = (atomicAdd(counter, 1u) == gridDim.x - 1);
     __syncthreads();
     if (!amlast) return;
     __threadfence();
     __shared__ double res[2 * kMaxDots];
-    const int nv = 2 * (j + 1), nw = blockDim.x >> 5;
+    const int nb = gridDim.x;
     for (int u = wid; u < nv; u += nw) {
-        const double* pv = partial + (int64_t)u * nbx;
+        const double* pv = partial + (int64_t)u * nb;
         double sacc = 0;
-        for (int b = lane; b < nbx; b += 32) sacc += __ldcg(pv + b);
+        for (int bb = lane; bb < nb; bb += 32) sacc += __ldcg(pv + bb);
         sacc = warp_sum(sacc);
         if (lane == 0) res[u] = sacc;
     }
@@ -419,6 +450,7 @@ __global__ void __launch_bounds__(kThreads) k_dcgs_reduce(const double* __restri
         *counter = 0u;
         dcgs_column(ks, j, res);
     }
+    (void)nbx;
 }
 
 // Update: V_j <- V_j - sum_{i<j} coefA_i V_i,  W <- W - sum_{i<j} coefB_i V_i - coefB_j V_j(new),
@@ -479,14 +511,14 @@ __global__ void __launch_bounds__(kThreads) k_dcgs_update(double* __restrict__ V
 
 void launch_dcgs_reduce(const double* V, int64_t ldv, int j, const double* W, int64_t n, const DotScratch& sc,
                         KrylovState* ks, cudaStream_t st) {
-    // about 8 blocks per SM in total over the j+1 basis vectors; 2(j+1) partial rows
-    int nbx = (148 * 8 + j) / (j + 1);
-    const int64_t need = ((n + 1) / 2 + kThreads - 1) / kThreads;
-    if (nbx > need) nbx = (int)need;
-    const int cap = (int)(((int64_t)(kMaxKrylov + 2) * sc.nblocks) / (2 * (j + 1)));
-    if (nbx > cap) nbx = cap;
-    if (nbx < 1) nbx = 1;
-    note_launch(), k_dcgs_reduce<<<dim3(nbx, j + 1), kThreads, 0, st>>>(V, ldv, j, W, n, sc.partial, sc.counter, nbx, ks);
+    // one block per chunk up to the scratch's blocks; 2(j+1) partial rows
+    const int64_t chunks = ((n + 1) / 2 + (int64_t)kDotE * kThreads - 1) / ((int64_t)kDotE * kThreads);
+    int nb = sc.nblocks;
+    if (nb > chunks) nb = (int)chunks;
+    const int cap = (int)(((int64_t)(kMaxKrylov + 2) * sc.nblocks) / (2 * (j + 1)));   // scratch rows
+    if (nb > cap) nb = cap;
+    if (nb < 1) nb = 1;
+    note_launch(), k_dcgs_reduce<<<nb, kThreads, 0, st>>>(V, ldv, j, W, n, sc.partial, sc.counter, nb, ks);
 }
 
 void launch_dcgs_update(double* V, int64_t ldv, int j, double* W, int64_t n, const DotScratch& sc, KrylovState* ks,
