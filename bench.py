@@ -55,6 +55,7 @@ class ClockSampler:
 
     def __init__(self, gpu=0):
         self.gpu, self.rows, self.proc = gpu, [], None
+        self.first = threading.Event()
 
     def __enter__(self):
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
@@ -75,6 +76,13 @@ class ClockSampler:
             parts = [s.strip() for s in line.split(",")]
             if len(parts) >= 7:
                 self.rows.append(parts)
+                self.first.set()
+
+    def wait_first(self, timeout=3.0):
+        """Block (at most `timeout` s) until nvidia-smi has produced a sample,
+        so that a short timed region still falls inside the sampling."""
+        if self.proc:
+            self.first.wait(timeout)
 
     def __exit__(self, *a):
         if self.proc:
@@ -141,6 +149,7 @@ def run_gpu(args, rank, world):
         torch.cuda.synchronize()
         n0 = lib.ow3d_launch_count()
         with ClockSampler(dev) as clk:
+            clk.wait_first()
             st, ms = sim.step_timed(args.steps)
         launches = lib.ow3d_launch_count() - n0
         ms = max_over_ranks(ms, world, "cuda")
