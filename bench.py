@@ -156,7 +156,9 @@ def run_gpu(args, rank, world):
         s = sim.stats()
         E, P, Wv, phi, tt = sim.get_state()
         states[prec] = (E, phi)
-        res[prec] = dict(ms=ms, stats=s, clocks=clk.summary(), params=p, bytes=sim.device_bytes(), launches=launches)
+        pb, pinfo = path_bytes_per_step(sim, s, args.steps, 8 if prec == "fp64" else 4)
+        res[prec] = dict(ms=ms, stats=s, clocks=clk.summary(), params=p, bytes=sim.device_bytes(), launches=launches,
+                         path_bytes=pb, path_info=pinfo)
         if prec == "mixed":
             res["sim"] = sim
         else:
@@ -188,6 +190,40 @@ def run_gpu(args, rank, world):
     err_eta = float(np.max(np.abs(Em - Ef)) / np.max(np.abs(Ef)))
     err_phi = float(np.max(np.abs(phim - phif)) / np.max(np.abs(phif)))
     return res, e2e_s, err_eta, err_phi, pm
+
+
+def path_bytes_per_step(sim, stats, steps, s):
+    """Algorithmic HBM bytes of one RK4 step of the whole path (4 Laplace
+    solves and the free-surface terms), from the per-unit figures: the
+    high-order operator 2*8*N + 10*8*C (the FP32 basis vector read at 4 bytes
+    in mixed mode); one Gauss-Seidel sweep on level l 3*s*N_l + 5*s*C_l;
+    residual + restriction 2*s*N_l + s*N_(l-1); prolongation + correction
+    s*N_(l-1) + 2*s*N_l; Arnoldi step j (2j+3)*8*N plus s*N to store z_j;
+    solution update (k*s + 16)*N; free surface 30*8*C. s = 8 (FP64) or 4
+    (FP32 multigrid and basis). The iteration count per solve is the run's
+    mean (exact when every solve took the same count)."""
+    p = sim.params
+    gy = 1 if p.Ny > 1 else 0
+    nl = sim.level_count()
+    dims = [sim.level_dims(l) for l in range(nl)]
+    Cl = [(nx + 2) * (ny + 2 * gy) for nx, ny, nz, _ in dims]
+    Nl = [c * (nz + 1) for c, (nx, ny, nz, _) in zip(Cl, dims)]
+    N, C = Nl[-1], Cl[-1]
+    vcycle = 0
+    for l in range(1, nl):
+        vcycle += (p.nu1 + p.nu2) * (3 * s * Nl[l] + 5 * s * Cl[l])
+        vcycle += 2 * s * Nl[l] + s * Nl[l - 1] + s * Nl[l - 1] + 2 * s * Nl[l]
+    solves = max(stats["solves"], 1)
+    it = stats["total_iterations"] / solves            # matvecs per solve, the initial residual's included
+    k = max(it - 1.0, 0.0)                              # Arnoldi steps = preconditioner applications
+    per_solve = (3 * 8 * N + 10 * 8 * C + 8 * N                       # initial residual (phi, rhs -> r), its norm
+                 + k * ((s + 8) * N + 10 * 8 * C)                     # operator on z_j
+                 + k * vcycle                                         # V-cycles
+                 + (k * k + 4 * k) * 8 * N + k * s * N                # Arnoldi steps j = 1..k, z_j stored
+                 + (k * s + 16) * N)                                  # solution update
+    return (stats["solves"] / steps) * per_solve + 30 * 8 * C, {
+        "levels": nl, "N": N, "C": C, "sum_N_levels": int(sum(Nl)), "iterations_per_solve": it,
+        "iterations_min_max": [stats["min_iterations"], stats["max_iterations"]]}
 
 
 def kernel_roofline(pkg, p, dev):
@@ -356,6 +392,15 @@ def main():
         roof_op = {"bound": "hbm", "kernel": "k_ho_matvec (6th-order sigma operator, FP64)", "achieved": ach,
                    "peak": peak, "unit": "GB/s", "frac": ach / peak, "traffic": profiled_traffic("k_ho_matvec"),
                    "peak_kind": peak_kind, "alg_bytes_per_launch": alg, "ms_per_launch": kms}
+    path_roof = {"peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                 "per_unit": "operator 2*8*N+10*8*C; GS sweep 3sN_l+5sC_l; residual+restriction 2sN_l+sN_(l-1); "
+                             "prolongation sN_(l-1)+2sN_l; Arnoldi step j (2j+3)*8N+sN; update (ks+16)N; "
+                             "free surface 30*8*C",
+                 **res["fp64"]["path_info"]}
+    for prec in ("fp64", "mixed"):
+        b = res[prec]["path_bytes"]
+        ach = b / (res[prec]["ms"] / args.steps / 1e3) / 1e9
+        path_roof[prec] = {"alg_bytes_per_step": b, "achieved": ach, "frac": ach / peak}
     cpu = None
     if not args.no_cpu:
         nthreads = os.cpu_count() or 1
@@ -384,7 +429,7 @@ def main():
         "laplace_solves_per_s": sm["solves"] * world / (ms_mixed / 1e3),
         "e2e": {"value": job_throughput(D, args.steps, world, e2e_s * 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": 2 * 8 * C, "d2h_bytes_per_step": 3 * 8 * C},
-        "roofline": roof, "roofline_operator": roof_op, "cpu_baseline": cpu, "clocks": res["mixed"]["clocks"], "serving": serve,
+        "roofline": roof, "roofline_operator": roof_op, "roofline_path": path_roof, "cpu_baseline": cpu, "clocks": res["mixed"]["clocks"], "serving": serve,
         "gpu_launches": res["mixed"]["launches"],
     }
     print(json.dumps(out))

@@ -35,6 +35,20 @@ unsigned long long ow3d_launch_count(void);
  * the previous value. Process-wide. */
 int ow3d_test_set_coarse_blocks(int blocks);
 
+/* Tuning knob for measurements: levels with at most this many points run in
+ * the fused coarse-level kernel (default 160000; 0 = none, every level above
+ * the dense one as separate launches). Read when a V-cycle is launched, so it
+ * applies to handles created after the change (and to captures made after
+ * it). Returns the previous value. Process-wide. */
+long long ow3d_test_set_coop_max_points(long long points);
+
+/* Levels without mixed-derivative terms that cover at least `min_tiles`
+ * tiles of 32 x 8 columns take the tiled colour pass (columns away from the
+ * walls solved from shared-memory tiles); 0: the per-column colour pass on
+ * every level, the default. Both give bitwise-identical results. Returns the
+ * previous value. Process-wide. */
+int ow3d_test_set_colour_tiles(int min_tiles);
+
 /* Number of captured Arnoldi-step graphs the handle holds, or -1 when a
  * capture failed and the handle launches kernels directly. */
 int ow3d_test_graph_count(const ow3d_handle* h);

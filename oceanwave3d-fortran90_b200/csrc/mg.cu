@@ -36,7 +36,6 @@ namespace cg = cooperative_groups;
     for (int64_t var = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; var < (n); var += (int64_t)gridDim.x * blockDim.x)
 
 // Points per level below which the level runs in the fused coarse kernel.
-constexpr int64_t kCoopMaxPoints = 160000;
 // Threads per block of the fused coarse kernel (one block per SM: fewer
 // blocks make the grid-wide barrier cheaper).
 constexpr int kCoopThreads = 512;
@@ -72,6 +71,146 @@ __global__ void __launch_bounds__(128, 4) k_lo_colour(LevelDev<T> L, int colour)
     const RowConst<T> rka = row_const_k<T>(L, 2 + 2 * r), rkb = row_const_k<T>(L, 3 + 2 * r);
     for (int base = (int)warp * (32 / S); base < (int)total; base += (int)nwarps * (32 / S))
         colour_warp2<T, THREE, S, CROSS>(L, colour, base, rka, rkb);
+}
+
+// ------------------------------------------------- tiled colour pass
+//
+// Levels without mixed-derivative terms (two colours, 3-D): every column of
+// the inner part (i in 4..Nxg-3, j in 4..Nyg-3) is solved from a tile staged
+// in shared memory by cp.async: kCTX x kCTY columns of x with one ring of
+// neighbour columns, and the colour's b, coefficients and bottom-row tables.
+// The tile arrives in two groups (tile rows 0-3 with their neighbour rows,
+// then the rest), and the first half is solved while the second arrives. The
+// columns within two columns of a wall (their ghost and corner work included)
+// run in the leading blocks of the same launch from global memory. Within one
+// colour no column reads another column that the pass writes, so both parts
+// read the values the per-column pass reads, and the arithmetic per column is
+// the same code (colour_col2).
+constexpr int kCTX = 32, kCTY = 8, kCTThreads = 256;
+constexpr int kCTSlots = kCTX * kCTY / 2;      // columns of one colour in a tile
+
+// Shared-memory layout of a tile, in elements: x rows RS apart (row rj holds
+// the columns i0-1.. of row j0-1+rj), b in slots BS apart, then 4 coefficients
+// and 8 bottom-row values per slot. Rows are copied in 16-byte chunks from the
+// 16-byte boundary at or below their first element; RS has the residue of a
+// global row (Nxg*Nzg) modulo a chunk, so the chunks of every row land on
+// 16-byte boundaries and neighbouring rows stay RS apart.
+template <typename T>
+struct TileShape {
+    int RS, BS, oB, oCF, oBT, bytes;
+};
+template <typename T>
+inline TileShape<T> tile_shape(int Nxg, int Nzg) {
+    constexpr int V = 16 / (int)sizeof(T);
+    TileShape<T> sh;
+    const int rmin = (kCTX + 2) * Nzg + 2 * V;
+    const int want = (int)(((int64_t)Nxg * Nzg) % V);
+    sh.RS = rmin + ((want - rmin % V) % V + V) % V;
+    sh.BS = (Nzg + 3 * V - 1) / V * V;
+    sh.oB = ((kCTY + 2) * sh.RS + V - 1) / V * V;
+    sh.oCF = sh.oB + kCTSlots * sh.BS;
+    sh.oBT = sh.oCF + kCTSlots * 4;
+    sh.bytes = (sh.oBT + kCTSlots * 8) * (int)sizeof(T);
+    return sh;
+}
+
+__device__ __forceinline__ void cp16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <typename T>
+__device__ __forceinline__ int chunk_pad(const T* p) {
+    return (int)(((uintptr_t)p & 15u) / sizeof(T));
+}
+
+template <typename T, int S>
+__global__ void __launch_bounds__(kCTThreads, 2) k_lo_colour_tile(LevelDev<T> L, int colour, int nband, int ntx,
+                                                                  TileShape<T> sh) {
+    extern __shared__ __align__(16) unsigned char ct_smem[];
+    constexpr int V = 16 / (int)sizeof(T);
+    constexpr int CPW = 32 / S;                       // columns per warp
+    constexpr int NW = kCTThreads / 32;
+    const int warp = threadIdx.x >> 5, r = (threadIdx.x & 31) & (S - 1);
+    const RowConst<T> rka = row_const_k<T>(L, 2 + 2 * r), rkb = row_const_k<T>(L, 3 + 2 * r);
+    if ((int)blockIdx.x < nband) {
+        colour_band2<T, S>(L, colour, ((int)blockIdx.x * NW + warp) * CPW, rka, rkb);
+        return;
+    }
+    const int t = (int)blockIdx.x - nband;
+    const int ty = t / ntx, tx = t - ty * ntx;
+    const int i0 = 4 + tx * kCTX, j0 = 4 + ty * kCTY;
+    const int Nxg = L.Nxg, Nyg = L.Nyg, Nzg = L.Nzg;
+    T* const xs = reinterpret_cast<T*>(ct_smem);
+    T* const bs = xs + sh.oB;
+    T* const cfs = xs + sh.oCF;
+    T* const bts = xs + sh.oBT;
+    const T* const X = L.xv;
+    const T* const B = L.bv;
+    const int tid = threadIdx.x;
+    const int ncols = min(kCTX + 2, Nxg - i0);       // x columns i0-1 .. at most Nxg-2
+    const int P = chunk_pad(X + ((int64_t)(i0 - 2) + (int64_t)Nxg * (j0 - 2)) * Nzg);
+    // x rows rj in [rlo, rhi) (level rows j0-1+rj up to Nyg-2)
+    auto stage_rows = [&](int rlo, int rhi) {
+        for (int rj = rlo; rj < rhi; ++rj) {
+            const int jj = j0 - 1 + rj;
+            if (jj > Nyg - 2) break;
+            const T* g = X + ((int64_t)(i0 - 2) + (int64_t)Nxg * (jj - 1)) * Nzg;
+            const int pad = chunk_pad(g);
+            const int n16 = (pad + ncols * Nzg + V - 1) / V;
+            T* d = xs + rj * sh.RS + P - pad;
+            const T* ga = g - pad;
+            for (int e = tid; e < n16; e += kCTThreads) cp16(d + e * V, ga + e * V);
+        }
+    };
+    // b, coefficients and bottom-row table of the colour's columns in slots [slo, shi)
+    auto stage_slots = [&](int slo, int shi) {
+        constexpr int CFC = 4 / V, BTC = 8 / V;
+        const int nb = sh.BS / V, per = nb + CFC + BTC;
+        for (int e = tid; e < (shi - slo) * per; e += kCTThreads) {
+            const int q = e / per, w = e - q * per, s = slo + q;
+            const int rr = s / (kCTX / 2), m = s - rr * (kCTX / 2);
+            const int j = j0 + rr, i = i0 + 2 * m + ((colour + j - i0) & 1);
+            if (i > Nxg - 3 || j > Nyg - 3) continue;
+            const int64_t c = (int64_t)(i - 1) + (int64_t)Nxg * (j - 1);
+            if (w < nb) {
+                const T* gb = B + c * Nzg;
+                cp16(bs + s * sh.BS + w * V, gb - chunk_pad(gb) + w * V);
+            } else if (w < nb + CFC) {
+                cp16(cfs + s * 4 + (w - nb) * V, L.cf + c * 4 + (w - nb) * V);
+            } else {
+                cp16(bts + s * 8 + (w - nb - CFC) * V, L.bt + c * 8 + (w - nb - CFC) * V);
+            }
+        }
+    };
+    stage_rows(0, kCTY / 2 + 2);
+    stage_slots(0, kCTSlots / 2);
+    cp_commit();
+    stage_rows(kCTY / 2 + 2, kCTY + 2);
+    stage_slots(kCTSlots / 2, kCTSlots);
+    cp_commit();
+    constexpr int GPR = (kCTX / 2) / CPW;            // warp groups per tile row
+    constexpr int G = kCTSlots / CPW;                // warp groups per tile
+    auto group = [&](int g) {
+        const int rr = g / GPR, m = (g - rr * GPR) * CPW + ((threadIdx.x & 31) / S);
+        const int s = rr * (kCTX / 2) + m;
+        const int j = j0 + rr, i = i0 + 2 * m + ((colour + j - i0) & 1);
+        const bool act = i <= Nxg - 3 && j <= Nyg - 3;
+        const int64_t c = (int64_t)(i - 1) + (int64_t)Nxg * (j - 1);
+        const T* xr = xs + (rr + 1) * sh.RS + P + (i - i0 + 1) * Nzg;
+        const T* br = bs + s * sh.BS + chunk_pad(B + c * Nzg);
+        colour_col2<T, true, S, false, true>(L, i, j, act, rka, rkb, xr, sh.RS, br, cfs + s * 4, bts + s * 8);
+    };
+    cp_wait<1>();
+    __syncthreads();
+    for (int g = warp; g < G / 2; g += NW) group(g);
+    cp_wait<0>();
+    __syncthreads();
+    for (int g = G / 2 + warp; g < G; g += NW) group(g);
 }
 
 template <typename T>
@@ -229,8 +368,39 @@ void launch_lo_matvec(const LevelDev<T>& L, const T* x, T* y, cudaStream_t st) {
     else note_launch(), k_lo_matvec<T, false><<<nblk(L.N), 256, 0, st>>>(L, x, y);
 }
 
+// Tiled colour pass for the levels it covers (see k_lo_colour_tile); false
+// when the level takes the per-column pass. Measured on one B200 (1025 x 257
+// x 17): alone after an L2 flush the tiled pass is faster on the two finest
+// levels (49 against 55 us, 19 against 24 us, FP64), but inside the solve,
+// where the previous kernel leaves x and b in L2, the per-column pass is as
+// fast in FP64 and 2-3 ms per step faster in mixed precision; on 2049 x 513
+// x 9 (4 lanes per column) the tiled pass is slower alone too (111 against
+// 94 us). It is therefore off by default (g_colour_tiles).
+template <typename T, int S>
+static bool colour_tile_launch(const LevelDev<T>& L, int c, cudaStream_t st) {
+    const int min_tiles = g_colour_tiles.load(std::memory_order_relaxed);
+    if (S < 4 || L.cross || L.ncolor != 2 || L.Nxg < 12 || L.Nyg < 12 || min_tiles <= 0) return false;
+    const int ntx = (L.Nxg - 6 + kCTX - 1) / kCTX, nty = (L.Nyg - 6 + kCTY - 1) / kCTY;
+    if (ntx * nty < min_tiles) return false;
+    const TileShape<T> sh = tile_shape<T>(L.Nxg, L.Nzg);
+    if (sh.bytes > 200 * 1024) return false;
+    static std::atomic<unsigned long long> attr_set{0ull};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(attr_set.load(std::memory_order_relaxed) & bit)) {
+        cudaFuncSetAttribute(k_lo_colour_tile<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        attr_set.fetch_or(bit, std::memory_order_relaxed);
+    }
+    const int per_block = (kCTThreads / 32) * (32 / S);
+    const int nband = (mgdev::wall_band_count(L) + per_block - 1) / per_block;
+    note_launch(), k_lo_colour_tile<T, S><<<nband + ntx * nty, kCTThreads, sh.bytes, st>>>(L, c, nband, ntx, sh);
+    return true;
+}
+
 template <typename T, bool THREE, int S>
 static void colour_launch(const LevelDev<T>& L, int c, cudaStream_t st) {
+    if (THREE && colour_tile_launch<T, S>(L, c, st)) return;
     const int64_t cols = (int64_t)((L.Nxg - 1) / 2) * (THREE ? L.Nyg - 2 : 1);
     const int64_t warps = (cols + (32 / S) - 1) / (32 / S);
     int64_t blocks = (warps * 32 + 127) / 128;
@@ -327,6 +497,13 @@ void launch_dense_apply(const LevelDev<T>& L, const T* M, cudaStream_t st) {
 // Block count of the fused coarse kernel: 0 = one block per SM, else at most
 // this many (a tuning knob for measurements, set through the test API).
 std::atomic<int> g_coarse_blocks{0};
+// Levels with at most this many points run in the fused coarse kernel.
+std::atomic<int64_t> g_coop_max_points{160000};
+// Levels of at least this many tiles take the tiled colour pass (0: none, the
+// default: inside the solve the per-column pass measured faster, see the
+// launcher).
+std::atomic<int> g_colour_tiles{0};
+
 thread_local bool g_capture_unsafe = false;
 
 // Launch the fused coarse cycle over levels lc..ld with a fully co-resident grid.
@@ -372,7 +549,8 @@ static void coarse_cycle(const LevelDev<T>* lev, int lc, int ld, const T* M, int
 template <typename T>
 static int coop_level(const LevelDev<T>* lev, int nlev) {
     int lc = -1;
-    for (int l = 0; l < nlev; ++l) if (lev[l].N <= kCoopMaxPoints) lc = l;
+    const int64_t cap = g_coop_max_points.load(std::memory_order_relaxed);
+    for (int l = 0; l < nlev; ++l) if (lev[l].N <= cap) lc = l;
     return lc;
 }
 

@@ -601,42 +601,33 @@ __device__ __forceinline__ RowConst<T> row_const_k(const LevelDev<T>& L, int k) 
 // rows' affine maps before the segment's shuffle scan, so a warp solves 32/S
 // columns and the per-column work (column decode, coefficient and bottom-row
 // loads, the bottom row itself) is shared by twice as many rows.
-template <typename T, bool THREE, int S, bool CROSS>
-__device__ void colour_warp2(const LevelDev<T>& L, int colour, int base, const RowConst<T>& rka,
-                             const RowConst<T>& rkb) {
+//
+// colour_col2 is the task of column (i, j) for its segment (act false: the
+// segment joins the warp's shuffles and touches no memory). x is read through
+// xr, the column's first row, with neighbour columns at +-Nzg (x) and +-oy (y);
+// b through br; x is written in global memory. With TILE the reads come from
+// a shared-memory tile (cfs, bts: the column's coefficients and bottom-row
+// table there) and the column is not next to a wall; otherwise they come from
+// global memory and the ghost-column and corner work of the wall columns runs
+// here.
+template <typename T, bool THREE, int S, bool CROSS, bool TILE>
+__device__ __forceinline__ void colour_col2(const LevelDev<T>& L, int i, int j, bool act, const RowConst<T>& rka,
+                                            const RowConst<T>& rkb, const T* xr, int oy, const T* br, const T* cfs,
+                                            const T* bts) {
     const int Nxg = L.Nxg, Nyg = L.Nyg, Nzg = L.Nzg, R = Nzg - 2;
     const int lane = threadIdx.x & 31, r = lane & (S - 1);
-    const int nxi = Nxg - 2, nyi = THREE ? Nyg - 2 : 1;
-    const bool four = (L.ncolor == 4);
-    const int ni = (nxi + 1) / 2;
-    const int nj = four ? (nyi + 1) / 2 : nyi;
-    const int total = ni * nj;
     const unsigned segmask = 0xffffffffu;   // the whole warp runs the scan together
     T* const X = L.xv;
     const T* const B = L.bv;
 
-    const int q = base + (lane / S);
-    bool act = q < total;
-    int i = 2, j = THREE ? 2 : 1;
-    if (act) {
-        const int tj = q / ni, ti = q - tj * ni;
-        if (four) {
-            j = THREE ? 2 + 2 * tj + (colour >> 1) : 1;
-            i = 2 + 2 * ti + (colour & 1);
-        } else {
-            j = THREE ? 2 + tj : 1;
-            i = 2 + 2 * ti + ((colour + j) & 1);
-        }
-        act = (i <= Nxg - 1) && (!THREE || j <= Nyg - 1);
-    }
     const int ka = 2 + 2 * r, kb = ka + 1;
     const bool va = act && ka <= Nzg - 1, vb = act && kb <= Nzg - 1;
     const int last = (R - 1) / 2;           // lane holding row Nzg-1 (the free surface follows it)
     const int c = (i - 1) + Nxg * (j - 1);
     T* const xc = X + (int64_t)c * Nzg;
-    const T* const bc = B + (int64_t)c * Nzg;
-    const int ox = Nzg, oy = Nzg * Nxg;
-    const bool edge = act && (i <= 3 || i >= Nxg - 2 || (THREE && (j <= 3 || j >= Nyg - 2)));
+    const T* const bc = br;
+    const int ox = Nzg;
+    const bool edge = !TILE && act && (i <= 3 || i >= Nxg - 2 || (THREE && (j <= 3 || j >= Nyg - 2)));
 
     auto colidx = [&](int ii, int jj) -> int64_t { return (int64_t)(ii - 1) + (int64_t)Nxg * (jj - 1); };
     // ghost column cg: Neumann rows of this lane's levels, wa x(ca) + wb x(cb) + wg x(cg) = b;
@@ -670,23 +661,26 @@ __device__ void colour_warp2(const LevelDev<T>& L, int colour, int base, const R
                             sy(L, 1, Nyg - 1, 1), sy(L, 1, Nyg - 1, 2), j == Nyg - 1 ? 2 : 1, post, xna, xnb, xfsn);
         }
     };
-    if (edge) {
-        if (THREE && (i == 2 || i == Nxg - 1) && (j == 2 || j == Nyg - 1)) {
-            const int64_t cc = colidx(i == 2 ? 1 : Nxg, j == 2 ? 1 : Nyg);
-            for (int kk = r; kk < Nzg; kk += S) X[cc * Nzg + kk] = B[cc * Nzg + kk];
+    if (!TILE) {
+        if (edge) {
+            if (THREE && (i == 2 || i == Nxg - 1) && (j == 2 || j == Nyg - 1)) {
+                const int64_t cc = colidx(i == 2 ? 1 : Nxg, j == 2 ? 1 : Nyg);
+                for (int kk = r; kk < Nzg; kk += S) X[cc * Nzg + kk] = B[cc * Nzg + kk];
+            }
+            ghosts(false, T(0), T(0), T(0));
         }
-        ghosts(false, T(0), T(0), T(0));
+        __syncwarp();
     }
-    __syncwarp();
 
     // rows ka and kb (clamped for loads; lanes past the last row discard theirs)
     const int kra = min(ka, Nzg - 1), krb = min(kb, Nzg - 1);
     T qa = 0, ga = 0, qb = 0, gb = 0, x1 = 0;
-    T bb1 = 0, bl = 0, br = 0, bd = 0, bu = 0;
+    T bb1 = 0, bl = 0, br1 = 0, bd = 0, bu = 0;
     T t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0, t6 = 0;
     if (act) {
         T ih, ca, cb, c3;
-        load_cf(L.cf, (int64_t)c, ih, ca, cb, c3);
+        if (TILE) { ih = cfs[0]; ca = cfs[1]; cb = cfs[2]; c3 = cfs[3]; }
+        else load_cf(L.cf, (int64_t)c, ih, ca, cb, c3);
         const T* sxp = L.SX + (Nxg + i - 1) * 3;
         const T wxl = __ldg(sxp), wxc = __ldg(sxp + 1), wxr = __ldg(sxp + 2);
         T wyd = 0, wyc = 0, wyu = 0;
@@ -697,14 +691,14 @@ __device__ void colour_warp2(const LevelDev<T>& L, int colour, int base, const R
         // q, g of row kr (x_kr = q - g x_{kr-1})
         auto rowq = [&](int kr, const RowConst<T>& rk, T x0, T xp, T& qo, T& go) {
             const int o = kr - 1;
-            const T xl = xc[o - ox], xr = xc[o + ox];
-            const T xd = THREE ? xc[o - oy] : T(0), xu = THREE ? xc[o + oy] : T(0);
+            const T xl = xr[o - ox], xrr = xr[o + ox];
+            const T xd = THREE ? xr[o - oy] : T(0), xu = THREE ? xr[o + oy] : T(0);
             const T bk = bc[o];
             const T om = rk.om;
             const T s2 = om * ca, s4 = THREE ? om * cb : T(0);
             const T s3 = om * c3;
             const T cz = s2 * s2 + s4 * s4 + ih * ih;
-            T off = wxl * xl + wxr * xr;
+            T off = wxl * xl + wxr * xrr;
             T diag = wxc + s3 * rk.z1 + cz * rk.zz1;
             if (THREE) { off += wyd * xd + wyu * xu; diag += wyc; }
             T lo = s3 * rk.z0 + cz * rk.zz0, up = s3 * rk.z2 + cz * rk.zz2;
@@ -726,7 +720,7 @@ __device__ void colour_warp2(const LevelDev<T>& L, int colour, int base, const R
                                 const T cf2 = T(2) * s2 * sz(L, 1, kr, kk) * w;
                                 if (kk == 0) lo += cf2; else if (kk == 1) diag += cf2; else up += cf2;
                             } else {
-                                dx += w * xc[(ii - i) * ox + (jj - j) * oy + (kz - 1)];
+                                dx += w * xr[(ii - i) * ox + (jj - j) * oy + (kz - 1)];
                             }
                         }
                         xz += sz(L, 1, kr, kk) * dx;
@@ -751,7 +745,7 @@ __device__ void colour_warp2(const LevelDev<T>& L, int colour, int base, const R
                                 const T cf2 = T(2) * s4 * sz(L, 1, kr, kk) * w;
                                 if (kk == 0) lo += cf2; else if (kk == 1) diag += cf2; else up += cf2;
                             } else {
-                                dy += w * xc[(ii - i) * ox + (jj - j) * oy + (kz - 1)];
+                                dy += w * xr[(ii - i) * ox + (jj - j) * oy + (kz - 1)];
                             }
                         }
                         yz += sz(L, 1, kr, kk) * dy;
@@ -763,23 +757,27 @@ __device__ void colour_warp2(const LevelDev<T>& L, int colour, int base, const R
             qo = x0 + (bk - diag * x0 - up * xp - off) * id;
             go = lo * id;
         };
-        const T x0a = xc[kra - 1], xpa = xc[kra], xpb = xc[krb];
+        const T x0a = xr[kra - 1], xpa = xr[kra], xpb = xr[krb];
         rowq(kra, rka, x0a, xpa, qa, ga);
         rowq(krb, rkb, xpa, xpb, qb, gb);            // row kb's old value is row ka's "above"
         if (!va) { qa = 0; ga = 0; }
         if (!vb) { qb = 0; gb = 0; }
         if (!CROSS) {
-            T btv[7];
-            load_bt(L.bt, (int64_t)c, btv);
-            t0 = btv[0]; t1 = btv[1]; t2 = btv[2]; t3 = btv[3]; t4 = btv[4]; t5 = btv[5]; t6 = btv[6];
+            if (TILE) {
+                t0 = bts[0]; t1 = bts[1]; t2 = bts[2]; t3 = bts[3]; t4 = bts[4]; t5 = bts[5]; t6 = bts[6];
+            } else {
+                T btv[7];
+                load_bt(L.bt, (int64_t)c, btv);
+                t0 = btv[0]; t1 = btv[1]; t2 = btv[2]; t3 = btv[3]; t4 = btv[4]; t5 = btv[5]; t6 = btv[6];
+            }
             bb1 = bc[0];
-            bl = xc[1 - ox]; br = xc[1 + ox];
-            if (THREE) { bd = xc[1 - oy]; bu = xc[1 + oy]; }
-            T boff = t0 * xc[1] + t1 * xc[2] + t2 * bl + t3 * br;
+            bl = xr[1 - ox]; br1 = xr[1 + ox];
+            if (THREE) { bd = xr[1 - oy]; bu = xr[1 + oy]; }
+            T boff = t0 * xr[1] + t1 * xr[2] + t2 * bl + t3 * br1;
             if (THREE) boff += t4 * bd + t5 * bu;
             x1 = (bb1 - boff) * t6;
         } else {
-            x1 = xc[0];
+            x1 = xr[0];
         }
     }
     // this lane's two rows as one map x_{ka-1} -> x_kb, then the segment scan
@@ -803,11 +801,78 @@ __device__ void colour_warp2(const LevelDev<T>& L, int colour, int base, const R
     const T xfs = act ? bc[Nzg - 1] : T(0);
     if (act && r == last) xc[Nzg - 1] = xfs;  // free-surface row
     if (!CROSS && act && r == 0) {
-        T boff = t0 * x2n + t1 * x3n + t2 * bl + t3 * br;
+        T boff = t0 * x2n + t1 * x3n + t2 * bl + t3 * br1;
         if (THREE) boff += t4 * bd + t5 * bu;
         xc[0] = (bb1 - boff) * t6;
     }
-    if (edge) ghosts(true, xna, xnb, xfs);
+    if (!TILE && edge) ghosts(true, xna, xnb, xfs);
+}
+
+// The colour's columns in order (rows of constant j, i fastest), 32/S per
+// warp from column `base` on.
+template <typename T, bool THREE, int S, bool CROSS>
+__device__ void colour_warp2(const LevelDev<T>& L, int colour, int base, const RowConst<T>& rka,
+                             const RowConst<T>& rkb) {
+    const int Nxg = L.Nxg, Nyg = L.Nyg, Nzg = L.Nzg;
+    const int lane = threadIdx.x & 31;
+    const int nxi = Nxg - 2, nyi = THREE ? Nyg - 2 : 1;
+    const bool four = (L.ncolor == 4);
+    const int ni = (nxi + 1) / 2;
+    const int nj = four ? (nyi + 1) / 2 : nyi;
+    const int total = ni * nj;
+    const int q = base + (lane / S);
+    bool act = q < total;
+    int i = 2, j = THREE ? 2 : 1;
+    if (act) {
+        const int tj = q / ni, ti = q - tj * ni;
+        if (four) {
+            j = THREE ? 2 + 2 * tj + (colour >> 1) : 1;
+            i = 2 + 2 * ti + (colour & 1);
+        } else {
+            j = THREE ? 2 + tj : 1;
+            i = 2 + 2 * ti + ((colour + j) & 1);
+        }
+        act = (i <= Nxg - 1) && (!THREE || j <= Nyg - 1);
+    }
+    const int64_t c = (int64_t)(i - 1) + (int64_t)Nxg * (j - 1);
+    colour_col2<T, THREE, S, CROSS, false>(L, i, j, act, rka, rkb, L.xv + c * Nzg, Nzg * Nxg, L.bv + c * Nzg,
+                                           nullptr, nullptr);
+}
+
+// Number of columns of one colour (two colours, 3-D) within two columns of a
+// wall: rows j = 2, 3, Nyg-2, Nyg-1 whole, and on the rows between them the
+// columns i = 2, 3, Nxg-2, Nxg-1. The tiled pass covers the rest.
+template <typename T>
+__device__ __host__ __forceinline__ int wall_band_count(const LevelDev<T>& L) {
+    const int ni = (L.Nxg - 1) / 2;
+    return 4 * ni + 2 * (L.Nyg - 6);
+}
+
+// The wall-band columns of `colour` (wall_band_count of them), 32/S per warp
+// from band column `base` on.
+template <typename T, int S>
+__device__ void colour_band2(const LevelDev<T>& L, int colour, int base, const RowConst<T>& rka,
+                             const RowConst<T>& rkb) {
+    const int Nxg = L.Nxg, Nyg = L.Nyg, Nzg = L.Nzg;
+    const int ni = (Nxg - 1) / 2;
+    const int q = base + ((threadIdx.x & 31) / S);
+    bool act = q < wall_band_count(L);
+    int i = 2, j = 2;
+    if (act) {
+        if (q < 4 * ni) {
+            const int rr = q / ni, ti = q - rr * ni;
+            j = rr < 2 ? 2 + rr : Nyg - 4 + rr;
+            i = 2 + 2 * ti + ((colour + j) & 1);
+            act = i <= Nxg - 1;
+        } else {
+            const int q2 = q - 4 * ni;
+            j = 4 + (q2 >> 1);
+            i = (q2 & 1) ? Nxg - 2 + ((colour + j - (Nxg - 2)) & 1) : 2 + ((colour + j) & 1);
+        }
+    }
+    const int64_t c = (int64_t)(i - 1) + (int64_t)Nxg * (j - 1);
+    colour_col2<T, true, S, false, false>(L, i, j, act, rka, rkb, L.xv + c * Nzg, Nzg * Nxg, L.bv + c * Nzg,
+                                          nullptr, nullptr);
 }
 
 // MGRestriction3DExplicit.f90:19-128 as a gather for coarse point p (also zeroes the coarse iterate).

@@ -843,6 +843,10 @@ extern "C" {
 unsigned long long ow3d_launch_count(void) { return g_kernel_launches.load(std::memory_order_relaxed); }
 
 int ow3d_test_set_coarse_blocks(int blocks) { return g_coarse_blocks.exchange(blocks < 0 ? 0 : blocks); }
+int ow3d_test_set_colour_tiles(int min_tiles) { return g_colour_tiles.exchange(min_tiles < 0 ? 0 : min_tiles); }
+long long ow3d_test_set_coop_max_points(long long points) {
+    return g_coop_max_points.exchange(points < 0 ? 0 : (int64_t)points);
+}
 
 int ow3d_test_graph_count(const ow3d_handle* H) {
     if (!H) return OW3D_ERR_BAD_INPUT;

@@ -20,6 +20,8 @@ namespace ow3d {
 extern std::atomic<unsigned long long> g_kernel_launches;
 // Block count cap of the fused coarse-level kernel (0: one block per SM).
 extern std::atomic<int> g_coarse_blocks;
+extern std::atomic<int64_t> g_coop_max_points;
+extern std::atomic<int> g_colour_tiles;
 // Set (on the capturing thread) when a launch sequence under stream capture
 // issued a host-to-device copy whose source the host later overwrites.
 extern thread_local bool g_capture_unsafe;
