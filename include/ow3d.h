@@ -61,6 +61,7 @@ extern "C" {
                                        used by iterative_solution.f90:23-24)            */
 
 #define OW3D_MAX_ZONES          8
+#define OW3D_MAX_KIN_FILES     20   /* kinematics output slices (ReadInputFileParameters.f90:305) */
 
 /* One relaxation zone: deck line 13 continuation
  * "x1 x2 y1 y2 ftype param XorY WavegenONOFF XorYgen degrees"
@@ -128,7 +129,16 @@ typedef struct ow3d_params {
     int    device;                /* CUDA device ordinal */
     /* line 9 (after the build-only knobs, so the layout above is unchanged) */
     int    StoreDataONOFF;        /* >0: EP_#####.bin every n steps, <0: fort.NNN every -n steps, 0: none */
-    int    formattype;            /* EP file form (1 and the default both write unformatted records) */
+    int    formattype;            /* EP file form (1 and the default both write unformatted records);
+                                     20 / 21: kinematics output to Kinematics<nn>.bin / one
+                                     Kinematics_<nn>_<it>.bin per output time (22: point
+                                     output, parsed but not supported) */
+    /* line 9, formattype 20-22 (ReadInputFileParameters.f90:300-405) */
+    int    iKinematics;           /* nonzero: kinematics output */
+    int    nOutFiles;             /* output slices, at most OW3D_MAX_KIN_FILES (10 for 21, 22) */
+    int    kinematics[OW3D_MAX_KIN_FILES][9];  /* per slice: xbeg xend xstride ybeg yend ystride
+                                     tbeg tend tstride (interior indices and time levels, 1-based;
+                                     formattype 22 keeps tbeg tend tstride only) */
 } ow3d_params;
 
 typedef struct ow3d_handle ow3d_handle;
@@ -324,6 +334,34 @@ int ow3d_write_ep(ow3d_handle* h, const char* dir, int nr, int fields);
 int ow3d_write_ascii(ow3d_handle* h, const char* dir, int nr, int fields);
 int ow3d_write_end(ow3d_handle* h, const char* path);
 int ow3d_store_data(ow3d_handle* h, const char* dir, int* files);
+
+/* Fluid kinematics of the current state on the whole grid, ghost points
+ * included (Nzg*Nxg*Nyg values each, k fastest), as StoreKinematicData
+ * computes them (src/IO/StoreKinematicData.f90:256-460):
+ *   u = phi_x + s_x phi_s, v = phi_y + s_y phi_s, w = phi_s / d,
+ * with phi_s the sigma derivative, d = h + eta and s_x = ((1 - z) h_x -
+ * z eta_x) / d (the s_x, s_y terms only when LinearONOFF is nonzero);
+ * grads (9 consecutive fields, may be NULL), in the reference's order and
+ * meaning: D_s(phi_s)/d, D_x(phi_s)+s_x D_s(phi_s), D_y(phi_s)+s_y D_s(phi_s),
+ * D_s(u)/d, D_x(u)+s_x D_s(u), D_y(u)+s_y D_s(u), and the same three for v.
+ * Any of u, v, w may be NULL. Computed on the device from the handle's phi,
+ * eta and eta derivatives after the last step (or ow3d_set_state). */
+int ow3d_kinematics(ow3d_handle* h, double* u, double* v, double* w, double* grads);
+
+/* Kinematics output of the deck's line 9 (formattype 20 or 21, iKinematics
+ * nonzero) at the handle's current step, as OceanWave3DT0Setup.f90:551-590
+ * and OceanWave3DTakeATimeStep.f90:193-204 call StoreKinematicData: at step
+ * 0 the header records of every slice, then, for each slice whose time range
+ * holds level L = step + 1 and with step a multiple of tstride, the 16
+ * records of level L. formattype 20 appends to dir/Kinematics<nn>.bin (the
+ * header truncates it); 21 writes dir/Kinematics_<nn>_<L>.bin per call (the
+ * header into ..._00000.bin). Records are Fortran unformatted (32-bit length
+ * markers): header (xbeg, xend, xstride, ybeg, yend, ystride, tbeg, tend,
+ * tstride as int32, dt as double, Nzg as int32), (x, y, h, hx, hy) per point
+ * of the slice, z(1:Nzg); per level: eta, eta_x, eta_y on the slice, then
+ * phi, u, v, w and the 9 gradient fields on the slice's columns (k fastest).
+ * *files = number of files written or appended to. */
+int ow3d_store_kinematics(ow3d_handle* h, const char* dir, int* files);
 
 const char* ow3d_strerror(int status);
 /* Message of the last failing call on this host thread (empty if none). */

@@ -13,6 +13,10 @@ extern "C" {
 
 int ow3d_test_level_count(const ow3d_handle* h);
 int ow3d_test_level_dims(const ow3d_handle* h, int level, int* Nx, int* Ny, int* Nz, int* ncolor);
+/* eta_x and eta_y of the current state as the device holds them (Nxg*Nyg
+ * each; on the ghost rows they are the derivatives taken before that
+ * direction's ghost update, as DifferentiationsFreeSurfacePlane leaves them). */
+int ow3d_test_surface_derivs(ow3d_handle* h, double* Ex, double* Ey);
 /* High-order stencil tables [order-1][pos][7] for x (2*Nxg*7), y (2*Nyg*7), sigma (2*Nzg*7). */
 int ow3d_test_stencils(const ow3d_handle* h, double* SX, double* SY, double* SZ);
 int ow3d_test_level_z(const ow3d_handle* h, int level, double* z);

@@ -47,6 +47,7 @@ def lib():
         L.ow3d_test_level_count.argtypes = [_C.c_void_p]
         L.ow3d_test_level_dims.argtypes = [_C.c_void_p, _C.c_int] + [_C.POINTER(_C.c_int)] * 4
         L.ow3d_test_stencils.argtypes = [_C.c_void_p, D, D, D]
+        L.ow3d_test_surface_derivs.argtypes = [_C.c_void_p, D, D]
         L.ow3d_test_level_z.argtypes = [_C.c_void_p, _C.c_int, D]
         L.ow3d_test_zone_gamma.argtypes = [_C.c_void_p, _C.c_int, D]
         L.ow3d_test_filter_coeffs.argtypes = [_C.c_void_p, D, D]
@@ -116,6 +117,50 @@ def load_ep(path):
     xy = _np.frombuffer(recs[1], "<f8").reshape(2, ny, nx)
     ep = _np.frombuffer(recs[2], "<f8").reshape(2, ny, nx)
     return nx, ny, xy[0], xy[1], ep[0], ep[1]
+
+
+def load_records(path):
+    """The records of a Fortran unformatted sequential file (32-bit length
+    markers) as a list of byte strings."""
+    raw = _pathlib.Path(path).read_bytes()
+    recs, pos = [], 0
+    while pos < len(raw):
+        n = int(_np.frombuffer(raw, "<i4", 1, pos)[0])
+        if int(_np.frombuffer(raw, "<i4", 1, pos + 4 + n)[0]) != n:
+            raise ValueError(f"{path}: record markers disagree")
+        recs.append(raw[pos + 4:pos + 4 + n])
+        pos += n + 8
+    return recs
+
+
+KINEMATICS_FIELDS = ("eta", "eta_x", "eta_y", "phi", "u", "v", "w", "w_z", "w_x", "w_y",
+                     "u_z", "u_x", "u_y", "v_z", "v_x", "v_y")
+
+
+def load_kinematics(path):
+    """Read a Kinematics file as ow3d_store_kinematics (and the reference's
+    StoreKinematicData) writes it: a dict with the header ('range', 'dt',
+    'nz', 'geometry' as (points, 5) x y h hx hy, 'z') when present, and
+    'levels', a list of dicts of the 16 fields (surface fields per slice
+    point, column fields as (points, nz))."""
+    recs = load_records(path)
+    out, pos = {"levels": []}, 0
+    if recs and len(recs[0]) == 48:
+        h = recs[0]
+        out["range"] = [int(v) for v in _np.frombuffer(h, "<i4", 9, 0)]
+        out["dt"] = float(_np.frombuffer(h, "<f8", 1, 36)[0])
+        out["nz"] = int(_np.frombuffer(h, "<i4", 1, 44)[0])
+        out["geometry"] = _np.frombuffer(recs[1], "<f8").reshape(-1, 5)
+        out["z"] = _np.frombuffer(recs[2], "<f8")
+        pos = 3
+    while pos + 16 <= len(recs):
+        lv = {}
+        for q, name in enumerate(KINEMATICS_FIELDS):
+            a = _np.frombuffer(recs[pos + q], "<f8")
+            lv[name] = a if q < 3 else a.reshape(len(_np.frombuffer(recs[pos], "<f8")), -1)
+        out["levels"].append(lv)
+        pos += 16
+    return out
 
 
 class Simulation:
@@ -229,6 +274,18 @@ class Simulation:
         _check(lib().ow3d_store_data(self.h, _b(directory), _C.byref(n)), "ow3d_store_data")
         return n.value
 
+    def kinematics(self):
+        """u, v, w and the 9 gradient fields (9, N) of the current state."""
+        u, v, w = (_np.zeros(self.N) for _ in range(3))
+        g = _np.zeros(9 * self.N)
+        _check(lib().ow3d_kinematics(self.h, _d(u), _d(v), _d(w), _d(g)), "ow3d_kinematics")
+        return u, v, w, g.reshape(9, self.N)
+
+    def store_kinematics(self, directory):
+        n = _C.c_int()
+        _check(lib().ow3d_store_kinematics(self.h, _b(directory), _C.byref(n)), "ow3d_store_kinematics")
+        return n.value
+
     def stats(self):
         s = Stats()
         _check(lib().ow3d_get_stats(self.h, _C.byref(s)), "ow3d_get_stats")
@@ -258,6 +315,12 @@ class Simulation:
         a = _f64(in1).ravel(); b = None if in2 is None else _f64(in2).ravel()
         _check(lib().ow3d_test_level_op(self.h, l, op, nu, _d(a), _d(b), _d(out)), "level_op")
         return out
+
+    def surface_derivs(self):
+        """eta_x, eta_y as the device holds them (include/ow3d_test.h)."""
+        Ex, Ey = _np.zeros(self.C), _np.zeros(self.C)
+        _check(lib().ow3d_test_surface_derivs(self.h, _d(Ex), _d(Ey)), "surface_derivs")
+        return Ex, Ey
 
     def stencils(self):
         SX = _np.zeros((2, self.Nxg, 7)); SY = _np.zeros((2, self.Nyg, 7 if self.params.Ny > 1 else 1))

@@ -22,6 +22,7 @@ PREC_MIXED = 1
 KRYLOV_FGMRES = 0
 KRYLOV_LGMRES = 1
 MAX_ZONES = 8
+MAX_KIN_FILES = 20
 
 
 class Zone(C.Structure):
@@ -57,6 +58,7 @@ class Params(C.Structure):
         ("zones", Zone * MAX_ZONES),
         ("precision", C.c_int), ("krylov", C.c_int), ("device", C.c_int),
         ("StoreDataONOFF", C.c_int), ("formattype", C.c_int),
+        ("iKinematics", C.c_int), ("nOutFiles", C.c_int), ("kinematics", (C.c_int * 9) * MAX_KIN_FILES),
     ]
 
 
@@ -163,6 +165,8 @@ def declare(lib):
         "ow3d_write_ascii": (C.c_int, [H, C.c_char_p, C.c_int, C.c_int]),
         "ow3d_write_end": (C.c_int, [H, C.c_char_p]),
         "ow3d_store_data": (C.c_int, [H, C.c_char_p, _I]),
+        "ow3d_kinematics": (C.c_int, [H, _D, _D, _D, _D]),
+        "ow3d_store_kinematics": (C.c_int, [H, C.c_char_p, _I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "../../include/ow3d.h"
+#include "ow3d_internal.h"
 
 namespace {
 
@@ -76,6 +77,21 @@ void fortran_e16_6e3(double v, char* out) {
 }
 
 }  // namespace
+
+namespace ow3d {
+// One Fortran unformatted sequential record made of `n` parts written back
+// to back, framed by its total length as a 32-bit integer (below 2 GiB).
+bool write_record(std::FILE* f, const void* const* parts, const size_t* bytes, int n) {
+    uint64_t len = 0;
+    for (int q = 0; q < n; ++q) len += bytes[q];
+    if (len > 0x7fffffffull) return false;
+    const int32_t m = (int32_t)len;
+    if (std::fwrite(&m, 4, 1, f) != 1) return false;
+    for (int q = 0; q < n; ++q)
+        if (bytes[q] && std::fwrite(parts[q], 1, bytes[q], f) != bytes[q]) return false;
+    return std::fwrite(&m, 4, 1, f) == 1;
+}
+}  // namespace ow3d
 
 extern "C" {
 

@@ -1149,6 +1149,183 @@ int ow3d_store_data(ow3d_handle* H, const char* dir, int* files) {
     return OW3D_OK;
 }
 
+namespace {
+// The 13 kinematics fields of the current state in a device buffer the
+// caller frees (cudaFree).
+int kinematics_fields(ow3d_handle* H, double** out) {
+    const GridHost& G = H->G;
+    const size_t N = (size_t)G.N;
+    double* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, (13 * N + (size_t)G.Nzg) * sizeof(double));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        g_last_error = std::string("ow3d_kinematics: cudaMalloc: ") + cudaGetErrorString(e);
+        return OW3D_ERR_OOM;
+    }
+    double* dz = d + 13 * N;
+    e = cudaMemcpyAsync(dz, G.z.data(), (size_t)G.Nzg * sizeof(double), cudaMemcpyHostToDevice, H->st);
+    KinArgs a;
+    a.Nxg = G.Nxg; a.Nyg = G.Nyg; a.Nzg = G.Nzg;
+    a.dox = G.Nx > 1; a.doy = G.three && G.Ny > 1;
+    a.chain = H->p.LinearONOFF != 0;
+    a.N = G.N;
+    a.SX = H->SX; a.SY = H->SY; a.SZ = H->SZ; a.z = dz;
+    a.h = H->h; a.hx = H->hx; a.hy = H->hy; a.E = H->E; a.Ex = H->Ex; a.Ey = H->Ey;
+    if (e == cudaSuccess) {
+        launch_kinematics(a, H->PHI, d, H->st);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(H->st);
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        g_last_error = std::string("ow3d_kinematics: ") + cudaGetErrorString(e);
+        return OW3D_ERR_CUDA;
+    }
+    *out = d;
+    return OW3D_OK;
+}
+}  // namespace
+
+int ow3d_kinematics(ow3d_handle* H, double* u, double* v, double* w, double* grads) {
+    if (!H) return OW3D_ERR_BAD_INPUT;
+    CK(cudaSetDevice(H->dev));
+    double* d = nullptr;
+    TRY(kinematics_fields(H, &d));
+    const size_t N = (size_t)H->G.N, b = N * sizeof(double);
+    cudaError_t e = cudaSuccess;
+    if (u && e == cudaSuccess) e = cudaMemcpy(u, d, b, cudaMemcpyDeviceToHost);
+    if (v && e == cudaSuccess) e = cudaMemcpy(v, d + N, b, cudaMemcpyDeviceToHost);
+    if (w && e == cudaSuccess) e = cudaMemcpy(w, d + 3 * N, b, cudaMemcpyDeviceToHost);
+    if (grads && e == cudaSuccess) e = cudaMemcpy(grads, d + 4 * N, 9 * b, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) { g_last_error = std::string("ow3d_kinematics: ") + cudaGetErrorString(e); return OW3D_ERR_CUDA; }
+    return OW3D_OK;
+}
+
+// StoreKinematicData.f90:98-155 (header, it = 0) and :232-460 (a level).
+int ow3d_store_kinematics(ow3d_handle* H, const char* dir, int* files) {
+    if (!H) return OW3D_ERR_BAD_INPUT;
+    if (files) *files = 0;
+    const ow3d_params& p = H->p;
+    if (!p.iKinematics || p.nOutFiles <= 0) return OW3D_OK;
+    if (p.formattype != 20 && p.formattype != 21) {
+        g_last_error = "ow3d_store_kinematics: formattype " + std::to_string(p.formattype) +
+                       " kinematics output is not supported (20 and 21 are)";
+        return OW3D_ERR_UNSUPPORTED;
+    }
+    if (p.nOutFiles > OW3D_MAX_KIN_FILES) { g_last_error = "ow3d_store_kinematics: too many slices"; return OW3D_ERR_BAD_INPUT; }
+    for (int io = 1; io <= p.nOutFiles; ++io) {
+        const int* r = p.kinematics[io - 1];
+        if (r[0] < 1 || r[1] > p.Nx || r[0] > r[1] || r[3] < 1 || r[4] > p.Ny || r[3] > r[4] || r[2] < 1 ||
+            r[5] < 1 || r[8] < 1 || r[6] > r[7]) {
+            g_last_error = "ow3d_store_kinematics: slice " + std::to_string(io) + " is outside the grid or empty";
+            return OW3D_ERR_BAD_INPUT;
+        }
+    }
+    CK(cudaSetDevice(H->dev));
+    const GridHost& G = H->G;
+    const int64_t t = H->tstep;
+    const int64_t L = t + 1;   // time level of the current state (level 1 = initial)
+    const size_t N = (size_t)G.N, Cn = (size_t)G.C;
+    const int nz = G.Nzg;
+    auto path_of = [&](int io, int64_t it) {
+        char name[48];
+        if (p.formattype == 20) std::snprintf(name, sizeof name, "Kinematics%02d.bin", io);
+        else std::snprintf(name, sizeof name, "Kinematics_%02d_%05lld.bin", io, (long long)it);
+        return (dir && *dir) ? std::string(dir) + "/" + name : std::string(name);
+    };
+    bool any = false;
+    for (int io = 1; io <= p.nOutFiles; ++io) {
+        const int* r = p.kinematics[io - 1];
+        if (L >= r[6] && L <= r[7] && t % r[8] == 0) any = true;
+    }
+    // host copies of the fields a level writes
+    std::vector<double> E(Cn), Ex(Cn), Ey(Cn, 0.0), phi, kin;
+    if (any) {
+        if (L > 99999) { g_last_error = "ow3d_store_kinematics: time levels have five digits"; return OW3D_ERR_BAD_INPUT; }
+        double* d = nullptr;
+        TRY(kinematics_fields(H, &d));
+        phi.resize(N); kin.resize(13 * N);
+        cudaError_t e = cudaMemcpy(kin.data(), d, 13 * N * sizeof(double), cudaMemcpyDeviceToHost);
+        cudaFree(d);
+        if (e == cudaSuccess) e = cudaMemcpy(phi.data(), H->PHI, N * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(E.data(), H->E, Cn * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(Ex.data(), H->Ex, Cn * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && G.Nyg > 1) e = cudaMemcpy(Ey.data(), H->Ey, Cn * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) { g_last_error = std::string("ow3d_store_kinematics: ") + cudaGetErrorString(e); return OW3D_ERR_CUDA; }
+    }
+    int written = 0;
+    for (int io = 1; io <= p.nOutFiles; ++io) {
+        const int* r = p.kinematics[io - 1];
+        // slice in ghost-inclusive 0-based indices
+        std::vector<size_t> cols;
+        for (int j = r[3] + G.gy; j <= r[4] + G.gy; j += r[5])
+            for (int i = r[0] + G.gx; i <= r[1] + G.gx; i += r[2]) cols.push_back((size_t)(i - 1) + (size_t)G.Nxg * (j - 1));
+        auto put = [&](std::FILE* f, const void* a, size_t nb) {
+            const void* parts[1] = {a};
+            const size_t sz[1] = {nb};
+            return write_record(f, parts, sz, 1);
+        };
+        auto column_field = [&](const double* F) {
+            std::vector<double> s;
+            s.reserve(cols.size() * nz);
+            for (size_t c : cols) s.insert(s.end(), F + c * nz, F + c * nz + nz);
+            return s;
+        };
+        auto surface_field = [&](const double* F) {
+            std::vector<double> s;
+            s.reserve(cols.size());
+            for (size_t c : cols) s.push_back(F[c]);
+            return s;
+        };
+        if (t == 0) {
+            const std::string path = path_of(io, 0);
+            std::FILE* f = std::fopen(path.c_str(), "wb");
+            if (!f) { g_last_error = "ow3d_store_kinematics: cannot open " + path; return OW3D_ERR_IO; }
+            int32_t ints[9];
+            for (int m = 0; m < 9; ++m) ints[m] = r[m];
+            const double dt = p.dt;
+            const int32_t nzi = nz;
+            const void* parts[3] = {ints, &dt, &nzi};
+            const size_t sz[3] = {sizeof ints, sizeof dt, sizeof nzi};
+            bool ok = write_record(f, parts, sz, 3);
+            std::vector<double> geo;
+            geo.reserve(cols.size() * 5);
+            for (size_t c : cols) {
+                const size_t i = c % (size_t)G.Nxg, j = c / (size_t)G.Nxg;
+                geo.push_back(G.x[i]); geo.push_back(G.y[j]); geo.push_back(G.h[c]);
+                geo.push_back(G.hx[c]); geo.push_back(G.three ? G.hy[c] : 0.0);
+            }
+            ok = ok && put(f, geo.data(), geo.size() * sizeof(double));
+            ok = ok && put(f, G.z.data(), (size_t)nz * sizeof(double));
+            ok = (std::fclose(f) == 0) && ok;
+            if (!ok) { g_last_error = "ow3d_store_kinematics: write failed: " + path; return OW3D_ERR_IO; }
+            ++written;
+        }
+        if (!(L >= r[6] && L <= r[7] && t % r[8] == 0)) continue;
+        const std::string path = path_of(io, L);
+        std::FILE* f = std::fopen(path.c_str(), p.formattype == 20 ? "ab" : "wb");
+        if (!f) { g_last_error = "ow3d_store_kinematics: cannot open " + path; return OW3D_ERR_IO; }
+        bool ok = true;
+        for (const double* F : {E.data(), Ex.data(), Ey.data()}) {
+            const std::vector<double> s = surface_field(F);
+            ok = ok && put(f, s.data(), s.size() * sizeof(double));
+        }
+        // phi, u, v, w, then the 9 gradient fields
+        const double* fields[13] = {phi.data(), &kin[0], &kin[N], &kin[3 * N]};
+        for (int q = 0; q < 9; ++q) fields[4 + q] = &kin[(4 + q) * N];
+        for (const double* F : fields) {
+            const std::vector<double> s = column_field(F);
+            ok = ok && put(f, s.data(), s.size() * sizeof(double));
+        }
+        ok = (std::fclose(f) == 0) && ok;
+        if (!ok) { g_last_error = "ow3d_store_kinematics: write failed: " + path; return OW3D_ERR_IO; }
+        ++written;
+    }
+    if (files) *files = written;
+    return OW3D_OK;
+}
+
 int ow3d_step(ow3d_handle* H, int nsteps) {
     if (!H || nsteps < 0) return OW3D_ERR_BAD_INPUT;
     CK(cudaSetDevice(H->dev));
@@ -1276,6 +1453,16 @@ int ow3d_test_stencils(const ow3d_handle* H, double* SX, double* SY, double* SZ)
     if (SX) std::copy(H->G.SX.w.begin(), H->G.SX.w.end(), SX);
     if (SY) std::copy(H->G.SY.w.begin(), H->G.SY.w.end(), SY);
     if (SZ) std::copy(H->G.SZ.w.begin(), H->G.SZ.w.end(), SZ);
+    return OW3D_OK;
+}
+
+int ow3d_test_surface_derivs(ow3d_handle* H, double* Ex, double* Ey) {
+    if (!H) return OW3D_ERR_BAD_INPUT;
+    CK(cudaSetDevice(H->dev));
+    const size_t cb = sizeof(double) * (size_t)H->G.C;
+    if (Ex) CK(cudaMemcpyAsync(Ex, H->Ex, cb, cudaMemcpyDeviceToHost, H->st));
+    if (Ey) CK(cudaMemcpyAsync(Ey, H->Ey, cb, cudaMemcpyDeviceToHost, H->st));
+    CK(cudaStreamSynchronize(H->st));
     return OW3D_OK;
 }
 

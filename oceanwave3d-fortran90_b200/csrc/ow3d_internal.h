@@ -10,6 +10,7 @@
 #include <atomic>
 #include <cstdint>
 #include <cstddef>
+#include <cstdio>
 #include <string>
 #include <cuda_runtime.h>
 #include "../../include/ow3d.h"
@@ -49,6 +50,22 @@ struct HoGrid {
     // kernel parameters
     const double *hSX, *hSY, *hSZ, *hzs;
 };
+
+// Inputs of the kinematics passes (kinematics.cu, StoreKinematicData.f90).
+struct KinArgs {
+    int Nxg, Nyg, Nzg;
+    int dox, doy;          // x / y derivatives present (Nx > 1, Ny > 1)
+    int chain;             // LinearONOFF != 0: the s_x, s_y terms
+    int64_t N;
+    const double *SX, *SY, *SZ;   // order-1 blocks of the per-position stencils, [pos][7]
+    const double* z;              // sigma levels, ghost level included
+    const double *h, *hx, *hy, *E, *Ex, *Ey;
+};
+// One Fortran unformatted record of n parts (io.cpp).
+bool write_record(std::FILE* f, const void* const* parts, const size_t* bytes, int n);
+
+// out: 13 fields of N doubles: u, v, phi_s, w, then the 9 gradient fields.
+void launch_kinematics(const KinArgs& a, const double* phi, double* out, cudaStream_t st);
 
 // Surface state that defines the sigma coefficients of one solve.
 struct Surface {

@@ -404,6 +404,8 @@ int default_params(ow3d_params* p) {
     for (auto& z : p->zones) { z.XorY = 'X'; z.XorYgen = 'X'; z.PhiOnOff = 1; }
     p->precision = OW3D_PREC_FP64; p->krylov = OW3D_KRYLOV_FGMRES; p->device = 0;
     p->StoreDataONOFF = 0; p->formattype = 0;
+    p->iKinematics = 0; p->nOutFiles = 0;
+    std::memset(p->kinematics, 0, sizeof(p->kinematics));
     return OW3D_OK;
 }
 
@@ -497,14 +499,34 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
         p->nu1 = r.n(o + 7); p->nu2 = r.n(o + 8); p->MGmaxgrids = r.n(o + 9);
     }
     r = next();  // stream-function line (always present)
-    r = next();  // StoreDataONOFF formattype [iKinematics nOutFiles]
+    r = next();  // StoreDataONOFF formattype [iKinematics nOutFiles] (ReadInputFileParameters.f90:300-405)
     if (r.nnum() >= 1) p->StoreDataONOFF = r.n(0);
     if (r.nnum() >= 2) {
         const int ft = r.n(1);
         p->formattype = ft;
         if (ft == 20 || ft == 21 || ft == 22) {
-            const int nout = r.num(3) ? r.n(3) : 0;
-            for (int i = 0; i < nout; ++i) next();
+            if (!r.num(2) || !r.num(3)) return fail("line 9: formattype 20-22 needs iKinematics and nOutFiles");
+            p->iKinematics = r.n(2);
+            const int nout = r.n(3);
+            if (nout < 0 || nout > (ft == 20 ? OW3D_MAX_KIN_FILES : 10))
+                return fail("line 9: too many kinematics output files");
+            p->nOutFiles = nout;
+            for (int i = 0; i < nout; ++i) {
+                Record q = next();
+                int* o = p->kinematics[i];
+                if (ft == 22) {
+                    // x y tbeg tend tstride: point output (kept: the time range only)
+                    if (q.nnum() < 5) return fail("line 9: kinematics output line " + std::to_string(i + 1) + " unreadable");
+                    o[6] = q.n(2); o[7] = q.n(3); o[8] = q.n(4);
+                } else {
+                    if (q.nnum() < 9) return fail("line 9: kinematics output line " + std::to_string(i + 1) + " unreadable");
+                    for (int m = 0; m < 9; ++m) o[m] = q.n(m);
+                    if (o[0] < 1 || o[1] > p->Nx || o[0] > o[1]) return fail("kinematics x coordinate range is invalid");
+                    if (o[3] < 1 || o[4] > p->Ny || o[3] > o[4]) return fail("kinematics y coordinate range is invalid");
+                    if (o[2] < 1 || o[5] < 1 || o[8] < 1) return fail("kinematics strides must be positive");
+                }
+                if (o[6] < 1 || o[7] > p->Nsteps || o[6] > o[7]) return fail("kinematics time range is invalid");
+            }
         }
     }
     r = next();  // LinearONOFF PressureTermONOFF

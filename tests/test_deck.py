@@ -77,7 +77,10 @@ def test_deck_2d_optional_fields(ow3d, tmp_path):
     # solver field omitted: GMRES is implied, the line starts at Precond
     assert (p.solver, p.Precond, p.MGCoarseningStrategy, p.GMRESmaxiterations) == (1, 3, 0, 30)
     assert (p.reltol, p.abstol, p.maxit, p.cyclet, p.nu1, p.nu2, p.MGmaxgrids) == (1e-9, 1e-7, 2, b"W", 2, 3, 0)
-    # output-file lines and the breaking line are skipped
+    # kinematics output lines (ReadInputFileParameters.f90:300-336), then the breaking line is skipped
+    assert (p.StoreDataONOFF, p.formattype, p.iKinematics, p.nOutFiles) == (-5, 20, 1, 2)
+    assert list(p.kinematics[0]) == [1, 65, 1, 1, 1, 1, 1, 100, 1]
+    assert list(p.kinematics[1]) == [1, 65, 2, 1, 1, 1, 1, 100, 2]
     assert p.LinearONOFF == 0 and p.PressureTermOnOff == 1
     assert p.filteringONOFF == 0 and p.relaxONOFF == 0
 
@@ -93,6 +96,13 @@ def test_deck_errors(ow3d, tmp_path):
     many = DECK_3D.replace("1 2.0 2 X 0", "1 2.0 9 X 0")
     with pytest.raises(ow3d.OW3DError):
         ow3d.read_deck(write(tmp_path, "many.inp", many))
+    # kinematics ranges outside the grid or the run (ReadInputFileParameters.f90:318-330)
+    for old, new, what in (("1 65 2 1 1 1 1 100 2", "1 66 2 1 1 1 1 100 2", "x coordinate range"),
+                           ("1 65 2 1 1 1 1 100 2", "1 65 2 1 2 1 1 100 2", "y coordinate range"),
+                           ("1 65 2 1 1 1 1 100 2", "1 65 2 1 1 1 5 101 2", "time range"),
+                           ("-5 20 1 2 ", "-5 20 1 21 ", "too many")):
+        with pytest.raises(ow3d.OW3DError, match=what):
+            ow3d.read_deck(write(tmp_path, "kin.inp", DECK_2D_CFL.replace(old, new)))
 
 
 def test_parsed_deck_builds_a_valid_estimate(ow3d, tmp_path):
@@ -119,4 +129,12 @@ def test_reference_example_decks_parse(ow3d):
         assert p.Nx >= 1 and p.Ny >= 1 and p.Nz >= 2
         assert p.GMRESmaxiterations >= 1 and p.reltol > 0
         assert p.cyclet in (b"V", b"W", b"F")
+        if p.formattype in (20, 21):
+            # the kinematics lines follow line 9 (counted without blank lines)
+            lines = [ln for ln in f.read_text(errors="replace").splitlines()]
+            i9 = next(i for i, ln in enumerate(lines[1:], 1)
+                      if ln.split()[:2] == [str(p.StoreDataONOFF), str(p.formattype)])
+            for q in range(p.nOutFiles):
+                want = [int(float(v)) for v in lines[i9 + 1 + q].replace(",", " ").split()[:9]]
+                assert list(p.kinematics[q]) == want, (f.name, q)
     assert parsed >= 0.8 * len(decks), (parsed, len(decks))
