@@ -139,6 +139,14 @@ typedef struct ow3d_params {
     int    kinematics[OW3D_MAX_KIN_FILES][9];  /* per slice: xbeg xend xstride ybeg yend ystride
                                      tbeg tend tstride (interior indices and time levels, 1-based;
                                      formattype 22 keeps tbeg tend tstride only) */
+    /* the incident linear wave of IncWaveType 2, the deck line after the
+     * curvilinear line (ReadInputFileParameters.f90:591-647) */
+    int    ispec;                 /* -1 mono-chromatic, 0 PM, 1 and 3 JONSWAP, 2 from a file,
+                                     |ispec| >= 30 directional */
+    int    seed, seed2;           /* random-wave seeds, made negative as the reference does */
+    double Tp, Hs, h0;            /* period (peak period), height (significant height), depth */
+    double kh_max, x0, y0;        /* spectrum cut-off; origin of the wave's phase */
+    double gamma_jonswap, beta0, s0;  /* JONSWAP gamma (3.3 unless ispec 3 / >= 30), heading, spreading */
 } ow3d_params;
 
 typedef struct ow3d_handle ow3d_handle;
@@ -256,6 +264,18 @@ int ow3d_put_surface(ow3d_handle* h, const double* E, const double* P);
 /* Read back E, P, W (Nxg*Nyg) and phi (Nzg*Nxg*Nyg); any pointer may be NULL. */
 int ow3d_get_state(ow3d_handle* h, double* E, double* P, double* W,
                    double* phi, double* t);
+
+/* The incident wave of IncWaveType 2 on generation zone `zone` (0-based), as
+ * OceanWave3DT0Setup.f90:197-255 builds RandomWave(zone)%eta and %Phis
+ * before the time loop: nt samples from t = time0 every dt, on the zone's box
+ * (i fastest, then j; the x-directed wave repeated on every row), ready for
+ * ow3d_set_relax_target(h, zone, 0, nt, dt, eta, phis). box (may be NULL)
+ * receives the ghost-inclusive 1-based bounds i0 i1 j0 j1; eta and phis may
+ * be NULL to query the box only. Host-only (no handle, no device). The
+ * mono-chromatic wave (ispec -1, random_wave_signal.f90:151-172, wavenumber
+ * as fdwvnum.f90) is supported; random and directional spectra return
+ * OW3D_ERR_UNSUPPORTED. The reference computes nt = Nsteps samples. */
+int ow3d_incident_wave(const ow3d_params* p, int zone, int nt, double* eta, double* phis, int* box);
 
 /* Relaxation-zone target signal for generation zone `zone` (0-based):
  * nt samples of eta and surface phi on the zone rectangle (i fastest, then j,

@@ -90,6 +90,23 @@ def _b(path):
     return str(path).encode()
 
 
+def incident_wave(params, zone, nt=None):
+    """The incident wave of IncWaveType 2 on generation zone `zone` (0-based):
+    eta and surface phi as (nt, rows, columns) arrays from t = time0 every dt
+    (nt defaults to Nsteps, as the reference), and the zone's ghost-inclusive
+    1-based box (i0, i1, j0, j1). Pass them to Simulation.set_relax_target
+    with mode 0 and dt_sample = dt."""
+    L = lib()
+    box = (_C.c_int * 4)()
+    _check(L.ow3d_incident_wave(_C.byref(params), zone, 1, None, None, box), "ow3d_incident_wave")
+    i0, i1, j0, j1 = list(box)
+    nt = int(params.Nsteps if nt is None else nt)
+    eta = _np.zeros((nt, j1 - j0 + 1, i1 - i0 + 1))
+    phis = _np.zeros_like(eta)
+    _check(L.ow3d_incident_wave(_C.byref(params), zone, nt, _d(eta), _d(phis), box), "ow3d_incident_wave")
+    return eta, phis, (i0, i1, j0, j1)
+
+
 def read_init_file(path, Nx, Ny):
     """Read a hot-start file (OceanWave3D.init format): interior E, P (Nx*Ny
     each, x fastest) and the start time."""

@@ -59,6 +59,10 @@ class Params(C.Structure):
         ("precision", C.c_int), ("krylov", C.c_int), ("device", C.c_int),
         ("StoreDataONOFF", C.c_int), ("formattype", C.c_int),
         ("iKinematics", C.c_int), ("nOutFiles", C.c_int), ("kinematics", (C.c_int * 9) * MAX_KIN_FILES),
+        ("ispec", C.c_int), ("seed", C.c_int), ("seed2", C.c_int),
+        ("Tp", C.c_double), ("Hs", C.c_double), ("h0", C.c_double),
+        ("kh_max", C.c_double), ("x0", C.c_double), ("y0", C.c_double),
+        ("gamma_jonswap", C.c_double), ("beta0", C.c_double), ("s0", C.c_double),
     ]
 
 
@@ -95,6 +99,7 @@ def default_params(**kw):
     p.relaxXorY = b"X"; p.relaxDegrees = 0.0
     p.precision = PREC_FP64; p.krylov = KRYLOV_FGMRES; p.device = 0
     p.StoreDataONOFF = 0; p.formattype = 0
+    p.ispec = -1; p.gamma_jonswap = 3.3; p.s0 = 1.0
     for k, v in kw.items():
         if k == "zones":
             for i, z in enumerate(v):
@@ -166,6 +171,7 @@ def declare(lib):
         "ow3d_write_end": (C.c_int, [H, C.c_char_p]),
         "ow3d_store_data": (C.c_int, [H, C.c_char_p, _I]),
         "ow3d_kinematics": (C.c_int, [H, _D, _D, _D, _D]),
+        "ow3d_incident_wave": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _D, _D, _I]),
         "ow3d_store_kinematics": (C.c_int, [H, C.c_char_p, _I]),
     }
     for name, (res, args) in sig.items():

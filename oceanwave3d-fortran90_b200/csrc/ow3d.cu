@@ -863,6 +863,14 @@ int ow3d_read_deck(const char* path, ow3d_params* p) {
     return r;
 }
 
+int ow3d_incident_wave(const ow3d_params* p, int zone, int nt, double* eta, double* phis, int* box) {
+    if (!p) return OW3D_ERR_BAD_INPUT;
+    std::string err;
+    const int r = incident_wave(*p, zone, nt, eta, phis, box, &err);
+    if (r) g_last_error = err;
+    return r;
+}
+
 int ow3d_create(const ow3d_params* p, const double* h, const double* hx, const double* hxx, const double* hy,
                 const double* hyy, ow3d_handle** out) {
     if (!out) return OW3D_ERR_BAD_INPUT;

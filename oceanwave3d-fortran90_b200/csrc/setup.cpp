@@ -312,6 +312,81 @@ std::vector<ZoneHost> build_zones(const ow3d_params& p, const GridHost& G) {
     return out;
 }
 
+// ------------------------------------------------------ incident linear wave
+// Finite-depth wavenumber of angular frequency omega in depth hb, with the
+// steps of the reference's fdwvnum (src/utilities/fdwvnum.f90:14-45): an
+// explicit first guess for the root of r tanh r = h (h = hb omega^2/g) and,
+// for h <= 4.8, one correction; the shallow and deep limits outside
+// 1e-5 < h < 1e5. Kept step for step so that the incident wave has the
+// reference's wavenumber to the last bit.
+double fd_wavenumber(double hb, double omega, double grav) {
+    const double kinf = omega * omega / grav;
+    const double h = hb * kinf;
+    if (h < 1e-5) return omega / std::sqrt(grav * hb);
+    if (h > 1e5) return kinf;
+    const double hi = 1.0 / h, twoh = h + h, hh = h * h;
+    const double e2h = std::exp(-std::min(twoh, 30.0));
+    double r0h = (h <= 2.0) ? std::sqrt(h) * ((0.031 * h + 0.169) * h + 1.0) : h + h * e2h * (2.0 - 12.0 * e2h);
+    if (h <= 4.8) {
+        const double rh = hh - r0h * r0h;
+        const double sh = 1.0 / (h - rh);
+        const double fh = sh * (0.5 * std::log((r0h + h) / (r0h - h)) - r0h);
+        r0h = r0h - fh * rh * (1.0 + fh * r0h * h * sh);
+    }
+    return r0h * hi * kinf;
+}
+
+// The mono-chromatic incident wave of IncWaveType 2 (ispec = -1) on the box of
+// generation zone `zone` (random_wave_signal.f90:151-172, with the x-directed
+// line replicated over the zone's rows as RelaxationModule_new.f90:104-112
+// applies it): eta = H/2 cos(nu (x - x0) - omega t), phiS = g/omega H/2
+// sin(nu (x - x0) - omega t), t = time0 + n dt for n = 0..nt-1.
+int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* phis, int* box, std::string* err) {
+    auto fail = [&](const std::string& m, int code) { if (err) *err = m; return code; };
+    if (p.IncWaveType != 2) return fail("incident_wave: the deck's IncWaveType is not 2", OW3D_ERR_BAD_INPUT);
+    if (p.ispec != -1)
+        return fail("incident_wave: ispec " + std::to_string(p.ispec) +
+                        " (random or directional waves) is not supported; the mono-chromatic wave (ispec -1) is",
+                    OW3D_ERR_UNSUPPORTED);
+    if (p.relaxONOFF != 1 || zone < 0 || zone >= p.relaxNo || zone >= OW3D_MAX_ZONES)
+        return fail("incident_wave: no such relaxation zone", OW3D_ERR_BAD_INPUT);
+    const ow3d_zone& d = p.zones[zone];
+    if (!(d.XorYgen == 'X' || d.XorYgen == 'x') || d.WavegenONOFF != 1)
+        return fail("incident_wave: zone " + std::to_string(zone) + " is not an x-directed generation zone",
+                    OW3D_ERR_BAD_INPUT);
+    if (nt < 1 || !(p.Tp > 0) || !(p.h0 > 0) || !(p.dt > 0)) return fail("incident_wave: bad arguments", OW3D_ERR_BAD_INPUT);
+    int r = check_params(p, err);
+    if (r) return r;
+    GridHost G;
+    const int Nxg = p.Nx + (p.Nx > 1 ? 2 : 0), Nyg = p.Ny + (p.Ny > 1 ? 2 : 0);
+    std::vector<double> ones((size_t)Nxg * Nyg, 1.0), zeros(ones.size(), 0.0);
+    r = build_grid(p, ones.data(), zeros.data(), zeros.data(), zeros.data(), zeros.data(), G, err);
+    if (r) return r;
+    const std::vector<ZoneHost> Z = build_zones(p, G);
+    const ZoneHost& z = Z[(size_t)zone];
+    if (box) { box[0] = z.i0; box[1] = z.i1; box[2] = z.j0; box[3] = z.j1; }
+    if (!eta && !phis) return OW3D_OK;
+    const double pi = std::acos(-1.0), two = 2.0;
+    const double omega = two * pi / p.Tp;
+    const double nu = fd_wavenumber(p.h0, omega, p.g);
+    const double amp = p.Hs / two, phifact = p.g / omega;
+    const int bx = z.i1 - z.i0 + 1, by = z.j1 - z.j0 + 1;
+    for (int n = 0; n < nt; ++n) {
+        const double t = p.time0 + n * p.dt;
+        for (int i = 0; i < bx; ++i) {
+            const double dist = G.x[(size_t)(z.i0 - 1 + i)] - p.x0;
+            const double e = amp * std::cos(nu * dist - omega * t);
+            const double f = phifact * amp * std::sin(nu * dist - omega * t);
+            for (int j = 0; j < by; ++j) {
+                const size_t q = (size_t)n * bx * by + (size_t)j * bx + i;
+                if (eta) eta[q] = e;
+                if (phis) phis[q] = f;
+            }
+        }
+    }
+    return OW3D_OK;
+}
+
 // -------------------------------------------------------------- filtering
 // Savitzky-Golay smoothing weights: value at offset 0 of the least-squares
 // polynomial of degree m through offsets -nl..nr (savgol.f90 with ld = 0).
@@ -406,6 +481,9 @@ int default_params(ow3d_params* p) {
     p->StoreDataONOFF = 0; p->formattype = 0;
     p->iKinematics = 0; p->nOutFiles = 0;
     std::memset(p->kinematics, 0, sizeof(p->kinematics));
+    p->ispec = -1; p->seed = 0; p->seed2 = 0;
+    p->Tp = 0; p->Hs = 0; p->h0 = 0; p->kh_max = 0; p->x0 = 0; p->y0 = 0;
+    p->gamma_jonswap = 3.3; p->beta0 = 0; p->s0 = 1.0;
     return OW3D_OK;
 }
 
@@ -456,7 +534,12 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
     std::string s;
     while (std::getline(f, s)) lines.push_back(s);
     size_t li = 1;  // line 0 is the header
-    auto next = [&]() -> Record { return li < lines.size() ? split(lines[li++]) : Record(); };
+    // list-directed reads pass over blank records
+    auto blank = [&](size_t i) { return lines[i].find_first_not_of(" \t\r") == std::string::npos; };
+    auto next = [&]() -> Record {
+        while (li < lines.size() && blank(li)) ++li;
+        return li < lines.size() ? split(lines[li++]) : Record();
+    };
     Record r = next();  // IC [IncWaveType [accel_tol_fact]]
     if (!r.num(0)) return fail("line 2: IC expected");
     p->IC = r.n(0);
@@ -552,6 +635,51 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
             Z.x1 = q.d(0); Z.x2 = q.d(1); Z.y1 = q.d(2); Z.y2 = q.d(3); Z.ftype = q.n(4); Z.param = q.d(5);
             Z.XorY = q.c(6); Z.WavegenONOFF = q.n(7); Z.XorYgen = q.c(8); Z.degrees = q.d(9); Z.PhiOnOff = 1;
         }
+    }
+    // ReadInputFileParameters.f90:534-653: an optional pressure-damping line
+    // (two integers, then its zone lines when on), the SWENSE line, the
+    // curvilinear line, then the incident-wave line of IncWaveType 2. Decks
+    // that end earlier keep the defaults (the hot path does not need them).
+    while (li < lines.size() && blank(li)) ++li;
+    if (li >= lines.size()) return OW3D_OK;
+    {
+        Record q = next();
+        auto integer = [&](size_t i) {
+            if (!q.num(i)) return false;
+            for (char ch : q.t[i]) if (!(std::isdigit((unsigned char)ch) || ch == '-' || ch == '+')) return false;
+            return true;
+        };
+        if (integer(0) && integer(1)) {
+            if (q.n(0) != 0) for (int z = 0; z < q.n(1); ++z) next();   // pressure-damping zone lines
+        } else {
+            --li;   // not a pressure-damping line (the reference backspaces, :555-562)
+        }
+    }
+    while (li < lines.size() && blank(li)) ++li;
+    if (li >= lines.size()) return OW3D_OK;
+    next();  // SWENSE line
+    while (li < lines.size() && blank(li)) ++li;
+    if (li >= lines.size()) return OW3D_OK;
+    next();  // curvilinearONOFF
+    if (p->IncWaveType == 2) {
+        Record q = next();
+        if (q.nnum() < 1) return fail("incident-wave line expected for IncWaveType 2");
+        p->ispec = q.n(0);
+        if (q.nnum() < 9) return fail("incident-wave line: ispec Tp Hs h0 kh_max seed seed2 x0 y0 expected");
+        p->Tp = q.d(1); p->Hs = q.d(2); p->h0 = q.d(3); p->kh_max = q.d(4);
+        p->seed = q.n(5); p->seed2 = q.n(6); p->x0 = q.d(7); p->y0 = q.d(8);
+        p->gamma_jonswap = 3.3; p->beta0 = 0.0; p->s0 = 1.0;
+        if (p->ispec == 3) {
+            if (q.nnum() < 10) return fail("incident-wave line: ispec 3 needs gamma");
+            p->gamma_jonswap = q.d(9);
+        } else if (std::abs(p->ispec) >= 30) {
+            // ... x0 y0 inc_wave_file beta0 s0 gamma (the file name is the 10th item)
+            if (q.t.size() < 13 || !q.num(10) || !q.num(11) || !q.num(12))
+                return fail("incident-wave line: |ispec| >= 30 needs a file name, beta0, s0 and gamma");
+            p->beta0 = q.d(10); p->s0 = q.d(11); p->gamma_jonswap = q.d(12);
+        }
+        if (p->seed >= 0) p->seed = -p->seed;     // :632-647
+        if (p->seed2 >= 0) p->seed2 = -p->seed2;
     }
     return OW3D_OK;
 }

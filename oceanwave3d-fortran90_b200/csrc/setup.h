@@ -57,6 +57,8 @@ std::vector<ZoneHost> build_zones(const ow3d_params& p, const GridHost& G);
 void filter_coeffs(const ow3d_params& p, std::vector<double>& fc, std::vector<double>& F2);
 
 int default_params(ow3d_params* p);
+double fd_wavenumber(double hb, double omega, double grav);
+int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* phis, int* box, std::string* err);
 int read_deck(const char* path, ow3d_params* p, std::string* err);
 
 }  // namespace ow3d
