@@ -266,15 +266,20 @@ int ow3d_get_state(ow3d_handle* h, double* E, double* P, double* W,
                    double* phi, double* t);
 
 /* The incident wave of IncWaveType 2 on generation zone `zone` (0-based), as
- * OceanWave3DT0Setup.f90:197-255 builds RandomWave(zone)%eta and %Phis
- * before the time loop: nt samples from t = time0 every dt, on the zone's box
- * (i fastest, then j; the x-directed wave repeated on every row), ready for
- * ow3d_set_relax_target(h, zone, 0, nt, dt, eta, phis). box (may be NULL)
- * receives the ghost-inclusive 1-based bounds i0 i1 j0 j1; eta and phis may
- * be NULL to query the box only. Host-only (no handle, no device). The
- * mono-chromatic wave (ispec -1, random_wave_signal.f90:151-172, wavenumber
- * as fdwvnum.f90) is supported; random and directional spectra return
- * OW3D_ERR_UNSUPPORTED. The reference computes nt = Nsteps samples. */
+ * OceanWave3DT0Setup.f90:176-255 builds RandomWave(zone)%eta and %Phis
+ * before the time loop: nt samples every dt, on the zone's box (i fastest,
+ * then j; the x-directed wave repeated on every row), ready for
+ * ow3d_set_relax_target(h, zone, 0, nt, dt, eta, phis). box (5 ints, may be
+ * NULL) receives the ghost-inclusive 1-based bounds i0 i1 j0 j1 and the
+ * number of samples the reference builds (Nsteps for ispec -1, else the
+ * power of two at or above Nsteps); eta and phis may be NULL to query box
+ * only. Host-only (no handle, no device). Supported: ispec -1 (mono-chromatic
+ * from t = time0, random_wave_signal.f90:151-172), 0 (Pierson-Moskowitz), 1
+ * and 3 (JONSWAP) long-crested random waves from t = 0 with the reference's
+ * random phases (RAN1_b seeded with seed2), spectra, kh_max truncation and
+ * wavenumbers (fdwvnum.f90); for random waves nt is at most the reference's
+ * sample count. Waves from a file (ispec 2) and directional waves return
+ * OW3D_ERR_UNSUPPORTED. */
 int ow3d_incident_wave(const ow3d_params* p, int zone, int nt, double* eta, double* phis, int* box);
 
 /* Relaxation-zone target signal for generation zone `zone` (0-based):

@@ -13,6 +13,9 @@ extern "C" {
 
 int ow3d_test_level_count(const ow3d_handle* h);
 int ow3d_test_level_dims(const ow3d_handle* h, int level, int* Nx, int* Ny, int* Nz, int* ncolor);
+/* n deviates of the incident-wave generator (Park-Miller with the
+ * Bays-Durham shuffle, RAN1_b.f90) started from idum, and the final idum. */
+int ow3d_test_ran1(int idum, int n, float* out, int* idum_out);
 /* eta_x and eta_y of the current state as the device holds them (Nxg*Nyg
  * each; on the ghost rows they are the derivatives taken before that
  * direction's ghost update, as DifferentiationsFreeSurfacePlane leaves them). */

@@ -48,6 +48,7 @@ def lib():
         L.ow3d_test_level_dims.argtypes = [_C.c_void_p, _C.c_int] + [_C.POINTER(_C.c_int)] * 4
         L.ow3d_test_stencils.argtypes = [_C.c_void_p, D, D, D]
         L.ow3d_test_surface_derivs.argtypes = [_C.c_void_p, D, D]
+        L.ow3d_test_ran1.argtypes = [_C.c_int, _C.c_int, _C.POINTER(_C.c_float), _C.POINTER(_C.c_int)]
         L.ow3d_test_level_z.argtypes = [_C.c_void_p, _C.c_int, D]
         L.ow3d_test_zone_gamma.argtypes = [_C.c_void_p, _C.c_int, D]
         L.ow3d_test_filter_coeffs.argtypes = [_C.c_void_p, D, D]
@@ -92,15 +93,15 @@ def _b(path):
 
 def incident_wave(params, zone, nt=None):
     """The incident wave of IncWaveType 2 on generation zone `zone` (0-based):
-    eta and surface phi as (nt, rows, columns) arrays from t = time0 every dt
-    (nt defaults to Nsteps, as the reference), and the zone's ghost-inclusive
-    1-based box (i0, i1, j0, j1). Pass them to Simulation.set_relax_target
-    with mode 0 and dt_sample = dt."""
+    eta and surface phi as (nt, rows, columns) arrays every dt (nt defaults
+    to the reference's sample count), and the zone's ghost-inclusive 1-based
+    box (i0, i1, j0, j1). Pass them to Simulation.set_relax_target with mode
+    0 and dt_sample = dt."""
     L = lib()
-    box = (_C.c_int * 4)()
+    box = (_C.c_int * 5)()
     _check(L.ow3d_incident_wave(_C.byref(params), zone, 1, None, None, box), "ow3d_incident_wave")
-    i0, i1, j0, j1 = list(box)
-    nt = int(params.Nsteps if nt is None else nt)
+    i0, i1, j0, j1, nref = list(box)
+    nt = int(nref if nt is None else nt)
     eta = _np.zeros((nt, j1 - j0 + 1, i1 - i0 + 1))
     phis = _np.zeros_like(eta)
     _check(L.ow3d_incident_wave(_C.byref(params), zone, nt, _d(eta), _d(phis), box), "ow3d_incident_wave")

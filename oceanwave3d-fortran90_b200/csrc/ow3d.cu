@@ -1474,6 +1474,14 @@ int ow3d_test_surface_derivs(ow3d_handle* H, double* Ex, double* Ey) {
     return OW3D_OK;
 }
 
+int ow3d_test_ran1(int idum, int n, float* out, int* idum_out) {
+    if (n < 0 || (n > 0 && !out)) return OW3D_ERR_BAD_INPUT;
+    Ran1 r;
+    for (int i = 0; i < n; ++i) out[i] = r.next(idum);
+    if (idum_out) *idum_out = idum;
+    return OW3D_OK;
+}
+
 int ow3d_test_level_z(const ow3d_handle* H, int l, double* z) {
     if (!H || l < 0 || l >= H->nlev) return OW3D_ERR_BAD_INPUT;
     std::copy(H->G.levels[l].z.begin(), H->G.levels[l].z.end(), z);

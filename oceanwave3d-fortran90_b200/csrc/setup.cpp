@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cctype>
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -336,17 +337,104 @@ double fd_wavenumber(double hb, double omega, double grav) {
     return r0h * hi * kinf;
 }
 
-// The mono-chromatic incident wave of IncWaveType 2 (ispec = -1) on the box of
-// generation zone `zone` (random_wave_signal.f90:151-172, with the x-directed
-// line replicated over the zone's rows as RelaxationModule_new.f90:104-112
-// applies it): eta = H/2 cos(nu (x - x0) - omega t), phiS = g/omega H/2
-// sin(nu (x - x0) - omega t), t = time0 + n dt for n = 0..nt-1.
+// Park and Miller's minimal standard generator (x <- 16807 x mod 2^31-1, by
+// Schrage's factorisation) with the Bays-Durham shuffle over 32 entries, in
+// the form of the reference's RAN1_b (src/utilities/RAN1_b.f90:1-36): a
+// non-positive idum (re)starts the sequence, the deviate is single precision
+// and kept below 1. The state persists between calls like the routine's SAVE.
+float Ran1::next(int& idum) {
+    const int ia = 16807, im = 2147483647, iq = 127773, ir = 2836, ntab = 32, ndiv = 1 + (im - 1) / ntab;
+    const float am = 1.0f / (float)im, rnmx = 1.0f - 1.2e-7f;
+    if (idum <= 0 || iy == 0) {
+        idum = std::max(-idum, 1);
+        for (int j = ntab + 8; j >= 1; --j) {
+            const int k = idum / iq;
+            idum = ia * (idum - k * iq) - ir * k;
+            if (idum < 0) idum += im;
+            if (j <= ntab) iv[j - 1] = idum;
+        }
+        iy = iv[0];
+    }
+    const int k = idum / iq;
+    idum = ia * (idum - k * iq) - ir * k;
+    if (idum < 0) idum += im;
+    const int j = 1 + iy / ndiv;
+    iy = iv[j - 1];
+    iv[j - 1] = idum;
+    return std::min(am * (float)iy, rnmx);
+}
+
+namespace {
+// PM_spectrum.f90:9-21 (T02 = 0.71 Tp with 0.71 a single-precision constant)
+double pm_spectrum(double f, double Hs, double Tp) {
+    const double pi = std::acos(-1.0);
+    const double T02 = (double)0.71f * Tp;
+    const double A = Hs * Hs / (4.0 * pi * std::pow(T02, 4)), B = 1.0 / (pi * std::pow(T02, 4));
+    return f <= 0.0 ? 0.0 : A / std::pow(f, 5) * std::exp(-B / std::pow(f, 4));
+}
+// JONSWAP_spectrum.f90:8-29 (g = 9.82 there)
+double jonswap_spectrum(double f, double Hs, double Tp, double gamma) {
+    const double pi = std::acos(-1.0), grav = 9.82;
+    const double fp = 1.0 / Tp;
+    const double alpha = 3.32285 * Hs * Hs * std::pow(fp, 4);
+    const double A = alpha * grav * grav / std::pow(2.0 * pi, 4), B = 5.0 / 4.0 * std::pow(fp, 4);
+    if (f <= 0.0) return 0.0;
+    const double sigma = f <= fp ? 0.07 : 0.09;
+    const double a = std::exp(-0.5 * std::pow((f - fp) / (sigma * fp), 2));
+    return A / std::pow(f, 5) * std::exp(-B / std::pow(f, 4)) * std::pow(gamma, a);
+}
+// In-place radix-2 transform X_j = sum_k Z_k exp(-2 pi i j k / n), n a power of two.
+void fft_minus(std::vector<std::complex<double>>& Z) {
+    const size_t n = Z.size();
+    for (size_t i = 1, j = 0; i < n; ++i) {
+        size_t bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) std::swap(Z[i], Z[j]);
+    }
+    const double pi = std::acos(-1.0);
+    for (size_t len = 2; len <= n; len <<= 1) {
+        for (size_t i = 0; i < n; i += len)
+            for (size_t q = 0; q < len / 2; ++q) {
+                const double a = -2.0 * pi * (double)q / (double)len;
+                const std::complex<double> w(std::cos(a), std::sin(a));
+                const std::complex<double> u = Z[i + q], v = Z[i + q + len / 2] * w;
+                Z[i + q] = u + v;
+                Z[i + q + len / 2] = u - v;
+            }
+    }
+}
+}  // namespace
+
+// Samples of the incident wave the reference builds: nt_ref = Nsteps for the
+// mono-chromatic wave, else the power of two at or above Nsteps
+// (OceanWave3DT0Setup.f90:178-191).
+int incident_wave_samples(const ow3d_params& p) {
+    if (p.ispec < 0) return p.Nsteps;
+    int i = (int)std::lround(std::log((double)p.Nsteps) / std::log(2.0));
+    if (std::pow(2.0, i) < p.Nsteps) ++i;
+    return 1 << std::max(i, 1);
+}
+
+// The incident wave of IncWaveType 2 on the box of generation zone `zone`,
+// the x-directed line replicated over the zone's rows as
+// RelaxationModule_new.f90:104-112 applies it:
+//  * ispec -1 (random_wave_signal.f90:151-172): eta = H/2 cos(nu (x - x0) -
+//    omega t), phiS = g/omega H/2 sin(...), t = time0 + n dt;
+//  * ispec 0 (P-M), 1 and 3 (JONSWAP) (build_coeff.f90:19-63,
+//    random_wave_coefficients.f90:53-100, random_wave_signal.f90:48-150):
+//    coefficients c_k = sqrt(2 S(f_k) df) e^(2 pi i psi_k), psi_k from the
+//    generator above seeded with seed2 (the phase rounded to single precision
+//    as CMPLX does), truncated at kh_max, moved to x by e^(i nu_k (x - x0)),
+//    and summed over the N = nt_ref samples t = n dt as the inverse real
+//    transform does: eta_n = sum_k Re(c_k e^(i nu_k d) e^(-2 pi i k n / N)),
+//    phiS likewise with g/omega_k (-i) c_k.
 int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* phis, int* box, std::string* err) {
     auto fail = [&](const std::string& m, int code) { if (err) *err = m; return code; };
     if (p.IncWaveType != 2) return fail("incident_wave: the deck's IncWaveType is not 2", OW3D_ERR_BAD_INPUT);
-    if (p.ispec != -1)
+    if (!(p.ispec == -1 || p.ispec == 0 || p.ispec == 1 || p.ispec == 3))
         return fail("incident_wave: ispec " + std::to_string(p.ispec) +
-                        " (random or directional waves) is not supported; the mono-chromatic wave (ispec -1) is",
+                        " (waves from a file or directional waves) is not supported; -1, 0, 1 and 3 are",
                     OW3D_ERR_UNSUPPORTED);
     if (p.relaxONOFF != 1 || zone < 0 || zone >= p.relaxNo || zone >= OW3D_MAX_ZONES)
         return fail("incident_wave: no such relaxation zone", OW3D_ERR_BAD_INPUT);
@@ -354,7 +442,11 @@ int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* p
     if (!(d.XorYgen == 'X' || d.XorYgen == 'x') || d.WavegenONOFF != 1)
         return fail("incident_wave: zone " + std::to_string(zone) + " is not an x-directed generation zone",
                     OW3D_ERR_BAD_INPUT);
-    if (nt < 1 || !(p.Tp > 0) || !(p.h0 > 0) || !(p.dt > 0)) return fail("incident_wave: bad arguments", OW3D_ERR_BAD_INPUT);
+    const int nref = incident_wave_samples(p);
+    if (nt < 1 || !(p.Tp > 0) || !(p.h0 > 0) || !(p.dt > 0) || p.Nsteps < 1)
+        return fail("incident_wave: bad arguments", OW3D_ERR_BAD_INPUT);
+    if (p.ispec >= 0 && nt > nref)
+        return fail("incident_wave: a random wave has " + std::to_string(nref) + " samples", OW3D_ERR_BAD_INPUT);
     int r = check_params(p, err);
     if (r) return r;
     GridHost G;
@@ -364,26 +456,69 @@ int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* p
     if (r) return r;
     const std::vector<ZoneHost> Z = build_zones(p, G);
     const ZoneHost& z = Z[(size_t)zone];
-    if (box) { box[0] = z.i0; box[1] = z.i1; box[2] = z.j0; box[3] = z.j1; }
+    if (box) { box[0] = z.i0; box[1] = z.i1; box[2] = z.j0; box[3] = z.j1; box[4] = nref; }
     if (!eta && !phis) return OW3D_OK;
-    const double pi = std::acos(-1.0), two = 2.0;
-    const double omega = two * pi / p.Tp;
-    const double nu = fd_wavenumber(p.h0, omega, p.g);
-    const double amp = p.Hs / two, phifact = p.g / omega;
+    const double pi = std::acos(-1.0), two = 2.0, twopi = two * pi;
     const int bx = z.i1 - z.i0 + 1, by = z.j1 - z.j0 + 1;
-    for (int n = 0; n < nt; ++n) {
-        const double t = p.time0 + n * p.dt;
+    std::vector<double> le((size_t)nt * bx), lp((size_t)nt * bx);   // the x line, [n][i]
+    if (p.ispec == -1) {
+        const double omega = twopi / p.Tp;
+        const double nu = fd_wavenumber(p.h0, omega, p.g);
+        const double amp = p.Hs / two, phifact = p.g / omega;
+        for (int n = 0; n < nt; ++n) {
+            const double t = p.time0 + n * p.dt;
+            for (int i = 0; i < bx; ++i) {
+                const double dist = G.x[(size_t)(z.i0 - 1 + i)] - p.x0;
+                le[(size_t)n * bx + i] = amp * std::cos(nu * dist - omega * t);
+                lp[(size_t)n * bx + i] = phifact * amp * std::sin(nu * dist - omega * t);
+            }
+        }
+    } else {
+        const int N = nref;
+        const double df = 1.0 / (N * p.dt), cst = std::sqrt(df), domega = twopi / (N * p.dt);
+        std::vector<std::complex<double>> c((size_t)N / 2, 0.0);
+        Ran1 rng;
+        int seed2 = p.seed2;
+        for (int i = 2; i <= N / 2; ++i) {
+            const double freq = (i - 1) * df;
+            const double psi = (double)rng.next(seed2);
+            const float cr = (float)std::cos(twopi * psi), ci = (float)std::sin(twopi * psi);
+            const double spec = p.ispec == 0 ? pm_spectrum(freq, p.Hs, p.Tp) : jonswap_spectrum(freq, p.Hs, p.Tp, p.gamma_jonswap);
+            const double a = std::sqrt(two * spec) * cst;
+            c[(size_t)(i - 1)] = std::complex<double>(a * (double)cr, a * (double)ci);
+        }
+        // truncation at kh_max (random_wave_coefficients.f90:92-100): the
+        // coefficients from index n_cut - 1 on are zero
+        const int n_cut = (int)std::lround(std::sqrt(p.g * p.kh_max / p.h0 * std::tanh(p.kh_max)) / domega) + 1;
+        for (int k = std::max(n_cut - 1, 1); k < N / 2; ++k) c[(size_t)k] = 0.0;
+        std::vector<std::complex<double>> ZE((size_t)N), ZP((size_t)N);
         for (int i = 0; i < bx; ++i) {
             const double dist = G.x[(size_t)(z.i0 - 1 + i)] - p.x0;
-            const double e = amp * std::cos(nu * dist - omega * t);
-            const double f = phifact * amp * std::sin(nu * dist - omega * t);
-            for (int j = 0; j < by; ++j) {
-                const size_t q = (size_t)n * bx * by + (size_t)j * bx + i;
-                if (eta) eta[q] = e;
-                if (phis) phis[q] = f;
+            std::fill(ZE.begin(), ZE.end(), 0.0);
+            std::fill(ZP.begin(), ZP.end(), 0.0);
+            for (int k = 1; k < std::min(n_cut, N / 2); ++k) {
+                const double omega = k * domega;
+                const double nu = fd_wavenumber(p.h0, omega, p.g);
+                const std::complex<double> e = c[(size_t)k] * std::complex<double>(std::cos(nu * dist), std::sin(nu * dist));
+                const std::complex<double> v = (p.g / omega) * std::complex<double>(e.imag(), -e.real());
+                ZE[(size_t)k] = e; ZE[(size_t)(N - k)] = std::conj(e);
+                ZP[(size_t)k] = v; ZP[(size_t)(N - k)] = std::conj(v);
+            }
+            fft_minus(ZE);
+            fft_minus(ZP);
+            for (int n = 0; n < nt; ++n) {
+                le[(size_t)n * bx + i] = 0.5 * ZE[(size_t)n].real();
+                lp[(size_t)n * bx + i] = 0.5 * ZP[(size_t)n].real();
             }
         }
     }
+    for (int n = 0; n < nt; ++n)
+        for (int j = 0; j < by; ++j)
+            for (int i = 0; i < bx; ++i) {
+                const size_t q = (size_t)n * bx * by + (size_t)j * bx + i;
+                if (eta) eta[q] = le[(size_t)n * bx + i];
+                if (phis) phis[q] = lp[(size_t)n * bx + i];
+            }
     return OW3D_OK;
 }
 

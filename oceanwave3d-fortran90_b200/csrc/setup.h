@@ -58,6 +58,12 @@ void filter_coeffs(const ow3d_params& p, std::vector<double>& fc, std::vector<do
 
 int default_params(ow3d_params* p);
 double fd_wavenumber(double hb, double omega, double grav);
+struct Ran1 {
+    int iv[32] = {0};
+    int iy = 0;
+    float next(int& idum);
+};
+int incident_wave_samples(const ow3d_params& p);
 int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* phis, int* box, std::string* err);
 int read_deck(const char* path, ow3d_params* p, std::string* err);
 

@@ -64,7 +64,8 @@ def _newton_k(omega, h, g):
     k = omega ** 2 / g
     for _ in range(60):
         f = g * k * np.tanh(k * h) - omega ** 2
-        k -= f / (g * np.tanh(k * h) + g * k * h / np.cosh(k * h) ** 2)
+        t = np.tanh(k * h)
+        k -= f / (g * t + g * k * h * (1 - t * t))
     return k
 
 
@@ -111,7 +112,7 @@ def test_incident_wave_errors(ow3d, tmp_path):
         ow3d.incident_wave(p, 1)
     with pytest.raises(ow3d.OW3DError, match="no such relaxation zone"):
         ow3d.incident_wave(p, 5)
-    p.ispec = 1
+    p.ispec = 33                                   # directional: not built
     with pytest.raises(ow3d.OW3DError) as e:
         ow3d.incident_wave(p, 0)
     assert e.value.status == ow3d.capi.ERR_UNSUPPORTED
@@ -146,3 +147,93 @@ def test_reference_wave_lines(ow3d):
         assert -abs(int(float(ln[5]))) == p.seed and float(ln[7]) == p.x0, f.name
         seen += 1
     assert seen >= 5
+
+
+def test_generator_park_miller_check(ow3d):
+    """The generator's underlying sequence is Park and Miller's minimal
+    standard: from x0 = 1, x10000 = 1043618065 (their published check). A
+    restart (idum <= 0) takes 40 steps to fill the shuffle table, so 9960
+    deviates later idum is x10000."""
+    import ctypes as C
+    L = ow3d.lib()
+    out = (C.c_float * 9960)()
+    idum = C.c_int()
+    assert L.ow3d_test_ran1(-1, 9960, out, C.byref(idum)) == 0
+    assert idum.value == 1043618065
+    v = np.frombuffer(out, dtype=np.float32)
+    assert v.min() > 0 and v.max() < 1 and abs(v.mean() - 0.5) < 0.02
+
+
+def _random_deck(tmp_path, ispec):
+    text = DECK.replace("400 0.02 1 0 1 0.3", "4000 0.02 1 0 1 0.")
+    text = text.replace("-1 1.25 0.04 0.8 35. 4 -34 1.5 0. run06.el 0.0", f"{ispec} 1.25 0.04 0.8 20. 4 -34 0. 0. run06.el")
+    return ow3d_read(tmp_path, text)
+
+
+def ow3d_read(tmp_path, text):
+    from conftest import load_package
+    return load_package().read_deck(_deck(tmp_path, text))
+
+
+def _jonswap(f, Hs, Tp, gamma):
+    fp = 1 / Tp
+    A = 3.32285 * Hs ** 2 * fp ** 4 * 9.82 ** 2 / (2 * np.pi) ** 4
+    B = 1.25 * fp ** 4
+    sigma = np.where(f <= fp, 0.07, 0.09)
+    return A / f ** 5 * np.exp(-B / f ** 4) * gamma ** np.exp(-0.5 * ((f - fp) / (sigma * fp)) ** 2)
+
+
+def _pm(f, Hs, Tp):
+    T02 = float(np.float32(0.71)) * Tp
+    return Hs ** 2 / (4 * np.pi * T02 ** 4) / f ** 5 * np.exp(-1 / (np.pi * T02 ** 4) / f ** 4)
+
+
+@pytest.mark.parametrize("ispec", [1, 0])
+def test_random_wave_spectrum_phases_and_dispersion(ow3d, tmp_path, ispec):
+    """JONSWAP (1) and P-M (0): at x = x0 the Fourier coefficients of the
+    generated series are sqrt(2 S(f_k) df) e^(2 pi i psi_k) with psi_k the
+    generator's deviates from seed2 (phases rounded to single precision),
+    zero from the kh_max cut-off on; downstream they carry e^(i nu_k d) with
+    nu_k the dispersion root; phiS has the coefficients g/omega (-i) c_k; and
+    the variance is sum S(f_k) df (Parseval)."""
+    import ctypes as C
+    p = _random_deck(tmp_path, ispec)
+    eta, phis, (i0, i1, j0, j1) = ow3d.incident_wave(p, 0)
+    N = eta.shape[0]
+    assert N == 4096
+    dt = p.dt
+    df = 1 / (N * dt)
+    k = np.arange(1, N // 2)
+    f = k * df
+    S = _jonswap(f, p.Hs, p.Tp, 3.3) if ispec == 1 else _pm(f, p.Hs, p.Tp)
+    n_cut = int(np.floor(np.sqrt(p.g * p.kh_max / p.h0 * np.tanh(p.kh_max)) / (2 * np.pi * df) + 0.5)) + 1
+    keep = k < n_cut - 1
+    psi = (C.c_float * (N // 2 - 1))()
+    assert ow3d.lib().ow3d_test_ran1(-34, N // 2 - 1, psi, None) == 0
+    ph = 2 * np.pi * np.frombuffer(psi, dtype=np.float32).astype(np.float64)
+    want = np.sqrt(2 * S * df) * (np.cos(ph).astype(np.float32) + 1j * np.sin(ph).astype(np.float32))
+    want = np.where(keep, want, 0)
+    x = (np.arange(p.Nx + 2) - 1) * p.Lx / (p.Nx - 1)
+    omega = 2 * np.pi * f
+    nu = _newton_k(omega, p.h0, p.g)
+    for col in (0, 7):                         # x = x0 = 0, and 7 columns downstream
+        d = x[i0 - 1 + col] - p.x0
+        ce = np.conj(np.fft.fft(eta[:, 0, col])[1:N // 2]) * 2 / N
+        cp = np.conj(np.fft.fft(phis[:, 0, col])[1:N // 2]) * 2 / N
+        w = want * np.exp(1j * nu * d)
+        scale = np.abs(want).max()
+        assert np.max(np.abs(ce - w)) < 1e-6 * scale, col
+        assert np.max(np.abs(cp - p.g / omega * (-1j) * w)) < 1e-6 * scale * p.g / omega.min(), col
+    var = np.sum(np.where(keep, S, 0) * df)
+    assert abs(np.var(eta[:, 0, 0]) / var - 1) < 1e-6     # |phase| = 1 to single precision
+    assert abs(4 * np.sqrt(var) / p.Hs - 1) < 0.1       # the spectrum's H_s, before truncation effects
+
+
+def test_random_wave_limits(ow3d, tmp_path):
+    p = _random_deck(tmp_path, 1)
+    with pytest.raises(ow3d.OW3DError, match="samples"):
+        ow3d.incident_wave(p, 0, nt=5000)
+    p.ispec = 2
+    with pytest.raises(ow3d.OW3DError) as e:
+        ow3d.incident_wave(p, 0)
+    assert e.value.status == ow3d.capi.ERR_UNSUPPORTED
