@@ -277,9 +277,11 @@ int ow3d_get_state(ow3d_handle* h, double* E, double* P, double* W,
  * from t = time0, random_wave_signal.f90:151-172), 0 (Pierson-Moskowitz), 1
  * and 3 (JONSWAP) long-crested random waves from t = 0 with the reference's
  * random phases (RAN1_b seeded with seed2), spectra, kh_max truncation and
- * wavenumbers (fdwvnum.f90); for random waves nt is at most the reference's
- * sample count. Waves from a file (ispec 2) and directional waves return
- * OW3D_ERR_UNSUPPORTED. */
+ * wavenumbers (fdwvnum.f90); -30, 30 and 31, the same waves at heading beta0
+ * on every point of the zone (random_wave_signal_3D.f90, zones with
+ * degrees = 0); for random waves nt is at most the reference's sample
+ * count. Waves from a file (ispec 2) and spread directional waves (33, 34)
+ * return OW3D_ERR_UNSUPPORTED. */
 int ow3d_incident_wave(const ow3d_params* p, int zone, int nt, double* eta, double* phis, int* box);
 
 /* Relaxation-zone target signal for generation zone `zone` (0-based):

@@ -432,9 +432,10 @@ int incident_wave_samples(const ow3d_params& p) {
 int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* phis, int* box, std::string* err) {
     auto fail = [&](const std::string& m, int code) { if (err) *err = m; return code; };
     if (p.IncWaveType != 2) return fail("incident_wave: the deck's IncWaveType is not 2", OW3D_ERR_BAD_INPUT);
-    if (!(p.ispec == -1 || p.ispec == 0 || p.ispec == 1 || p.ispec == 3))
+    if (!(p.ispec == -1 || p.ispec == 0 || p.ispec == 1 || p.ispec == 3 || p.ispec == -30 || p.ispec == 30 ||
+          p.ispec == 31))
         return fail("incident_wave: ispec " + std::to_string(p.ispec) +
-                        " (waves from a file or directional waves) is not supported; -1, 0, 1 and 3 are",
+                        " (waves from a file or spread directional waves) is not supported; -1, 0, 1, 3, -30, 30 and 31 are",
                     OW3D_ERR_UNSUPPORTED);
     if (p.relaxONOFF != 1 || zone < 0 || zone >= p.relaxNo || zone >= OW3D_MAX_ZONES)
         return fail("incident_wave: no such relaxation zone", OW3D_ERR_BAD_INPUT);
@@ -442,6 +443,8 @@ int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* p
     if (!(d.XorYgen == 'X' || d.XorYgen == 'x') || d.WavegenONOFF != 1)
         return fail("incident_wave: zone " + std::to_string(zone) + " is not an x-directed generation zone",
                     OW3D_ERR_BAD_INPUT);
+    if (std::abs(p.ispec) >= 30 && d.degrees != 0.0)   // ReadInputFileParameters.f90:710-714
+        return fail("incident_wave: waves at a heading need a zone with degrees = 0", OW3D_ERR_BAD_INPUT);
     const int nref = incident_wave_samples(p);
     if (nt < 1 || !(p.Tp > 0) || !(p.h0 > 0) || !(p.dt > 0) || p.Nsteps < 1)
         return fail("incident_wave: bad arguments", OW3D_ERR_BAD_INPUT);
@@ -460,22 +463,36 @@ int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* p
     if (!eta && !phis) return OW3D_OK;
     const double pi = std::acos(-1.0), two = 2.0, twopi = two * pi;
     const int bx = z.i1 - z.i0 + 1, by = z.j1 - z.j0 + 1;
-    std::vector<double> le((size_t)nt * bx), lp((size_t)nt * bx);   // the x line, [n][i]
-    if (p.ispec == -1) {
+    // long-crested along x (|ispec| < 30): one x line, repeated on the rows;
+    // at heading beta0 (random_wave_signal_3D.f90): every point of the box
+    const bool heading = std::abs(p.ispec) >= 30;
+    const int ny_eval = heading ? by : 1;
+    const double cosb = heading ? std::cos(pi / 180.0 * p.beta0) : 1.0;
+    const double sinb = heading ? std::sin(pi / 180.0 * p.beta0) : 0.0;
+    auto dist_of = [&](int i, int j) {
+        const double dx = G.x[(size_t)(z.i0 - 1 + i)] - p.x0;
+        const double dy = heading ? G.y[(size_t)(z.j0 - 1 + j)] - p.y0 : 0.0;
+        return cosb * dx + sinb * dy;
+    };
+    std::vector<double> le((size_t)nt * bx * ny_eval), lp(le.size());   // [n][j][i]
+    auto at = [&](int n, int j, int i) { return ((size_t)n * ny_eval + j) * bx + i; };
+    if (p.ispec < 0) {
         const double omega = twopi / p.Tp;
         const double nu = fd_wavenumber(p.h0, omega, p.g);
         const double amp = p.Hs / two, phifact = p.g / omega;
         for (int n = 0; n < nt; ++n) {
             const double t = p.time0 + n * p.dt;
-            for (int i = 0; i < bx; ++i) {
-                const double dist = G.x[(size_t)(z.i0 - 1 + i)] - p.x0;
-                le[(size_t)n * bx + i] = amp * std::cos(nu * dist - omega * t);
-                lp[(size_t)n * bx + i] = phifact * amp * std::sin(nu * dist - omega * t);
-            }
+            for (int j = 0; j < ny_eval; ++j)
+                for (int i = 0; i < bx; ++i) {
+                    const double dist = dist_of(i, j);
+                    le[at(n, j, i)] = amp * std::cos(nu * dist - omega * t);
+                    lp[at(n, j, i)] = phifact * amp * std::sin(nu * dist - omega * t);
+                }
         }
     } else {
         const int N = nref;
         const double df = 1.0 / (N * p.dt), cst = std::sqrt(df), domega = twopi / (N * p.dt);
+        const bool pm = (p.ispec == 0 || p.ispec == 30);
         std::vector<std::complex<double>> c((size_t)N / 2, 0.0);
         Ran1 rng;
         int seed2 = p.seed2;
@@ -483,7 +500,7 @@ int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* p
             const double freq = (i - 1) * df;
             const double psi = (double)rng.next(seed2);
             const float cr = (float)std::cos(twopi * psi), ci = (float)std::sin(twopi * psi);
-            const double spec = p.ispec == 0 ? pm_spectrum(freq, p.Hs, p.Tp) : jonswap_spectrum(freq, p.Hs, p.Tp, p.gamma_jonswap);
+            const double spec = pm ? pm_spectrum(freq, p.Hs, p.Tp) : jonswap_spectrum(freq, p.Hs, p.Tp, p.gamma_jonswap);
             const double a = std::sqrt(two * spec) * cst;
             c[(size_t)(i - 1)] = std::complex<double>(a * (double)cr, a * (double)ci);
         }
@@ -491,33 +508,38 @@ int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* p
         // coefficients from index n_cut - 1 on are zero
         const int n_cut = (int)std::lround(std::sqrt(p.g * p.kh_max / p.h0 * std::tanh(p.kh_max)) / domega) + 1;
         for (int k = std::max(n_cut - 1, 1); k < N / 2; ++k) c[(size_t)k] = 0.0;
+        const int kmax = std::min(n_cut, N / 2);
+        std::vector<double> nus((size_t)std::max(kmax, 1), 0.0);
+        for (int k = 1; k < kmax; ++k) nus[(size_t)k] = fd_wavenumber(p.h0, k * domega, p.g);
         std::vector<std::complex<double>> ZE((size_t)N), ZP((size_t)N);
-        for (int i = 0; i < bx; ++i) {
-            const double dist = G.x[(size_t)(z.i0 - 1 + i)] - p.x0;
-            std::fill(ZE.begin(), ZE.end(), 0.0);
-            std::fill(ZP.begin(), ZP.end(), 0.0);
-            for (int k = 1; k < std::min(n_cut, N / 2); ++k) {
-                const double omega = k * domega;
-                const double nu = fd_wavenumber(p.h0, omega, p.g);
-                const std::complex<double> e = c[(size_t)k] * std::complex<double>(std::cos(nu * dist), std::sin(nu * dist));
-                const std::complex<double> v = (p.g / omega) * std::complex<double>(e.imag(), -e.real());
-                ZE[(size_t)k] = e; ZE[(size_t)(N - k)] = std::conj(e);
-                ZP[(size_t)k] = v; ZP[(size_t)(N - k)] = std::conj(v);
+        for (int j = 0; j < ny_eval; ++j)
+            for (int i = 0; i < bx; ++i) {
+                const double dist = dist_of(i, j);
+                std::fill(ZE.begin(), ZE.end(), 0.0);
+                std::fill(ZP.begin(), ZP.end(), 0.0);
+                for (int k = 1; k < kmax; ++k) {
+                    const double omega = k * domega, nu = nus[(size_t)k];
+                    const std::complex<double> e =
+                        c[(size_t)k] * std::complex<double>(std::cos(nu * dist), std::sin(nu * dist));
+                    const std::complex<double> v = (p.g / omega) * std::complex<double>(e.imag(), -e.real());
+                    ZE[(size_t)k] = e; ZE[(size_t)(N - k)] = std::conj(e);
+                    ZP[(size_t)k] = v; ZP[(size_t)(N - k)] = std::conj(v);
+                }
+                fft_minus(ZE);
+                fft_minus(ZP);
+                for (int n = 0; n < nt; ++n) {
+                    le[at(n, j, i)] = 0.5 * ZE[(size_t)n].real();
+                    lp[at(n, j, i)] = 0.5 * ZP[(size_t)n].real();
+                }
             }
-            fft_minus(ZE);
-            fft_minus(ZP);
-            for (int n = 0; n < nt; ++n) {
-                le[(size_t)n * bx + i] = 0.5 * ZE[(size_t)n].real();
-                lp[(size_t)n * bx + i] = 0.5 * ZP[(size_t)n].real();
-            }
-        }
     }
     for (int n = 0; n < nt; ++n)
         for (int j = 0; j < by; ++j)
             for (int i = 0; i < bx; ++i) {
                 const size_t q = (size_t)n * bx * by + (size_t)j * bx + i;
-                if (eta) eta[q] = le[(size_t)n * bx + i];
-                if (phis) phis[q] = lp[(size_t)n * bx + i];
+                const size_t src = at(n, heading ? j : 0, i);
+                if (eta) eta[q] = le[src];
+                if (phis) phis[q] = lp[src];
             }
     return OW3D_OK;
 }

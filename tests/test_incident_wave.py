@@ -237,3 +237,65 @@ def test_random_wave_limits(ow3d, tmp_path):
     with pytest.raises(ow3d.OW3DError) as e:
         ow3d.incident_wave(p, 0)
     assert e.value.status == ow3d.capi.ERR_UNSUPPORTED
+
+
+def _heading_deck(tmp_path, line, nsteps="400"):
+    text = DECK.replace("400 0.02 1 0 1 0.3", f"{nsteps} 0.02 1 0 1 0.3")
+    return ow3d_read(tmp_path, text.replace("-1 1.25 0.04 0.8 35. 4 -34 1.5 0. run06.el 0.0", line))
+
+
+def _xy(p):
+    x = (np.arange(p.Nx + 2) - 1) * p.Lx / (p.Nx - 1)
+    y = (np.arange(p.Ny + 2) - 1) * p.Ly / (p.Ny - 1)
+    return x, y
+
+
+def test_monochromatic_wave_at_heading(ow3d, tmp_path):
+    """ispec -30 (random_wave_signal_3D.f90:150-171): the wave at beta0 to
+    the x-axis on every point of the zone, phase nu ((x-x0) cos b + (y-y0) sin b)."""
+    p = _heading_deck(tmp_path, "-30 1.25 0.04 0.8 35. 4 -34 1.5 0.5 run06.el 22.5 1.0 3.3")
+    assert (p.ispec, p.beta0) == (-30, 22.5)
+    eta, phis, (i0, i1, j0, j1) = ow3d.incident_wave(p, 0)
+    x, y = _xy(p)
+    b = np.deg2rad(p.beta0)
+    omega = 2 * np.pi / p.Tp
+    nu = _newton_k(omega, p.h0, p.g)
+    X, Y = np.meshgrid(x[i0 - 1:i1], y[j0 - 1:j1])
+    d = np.cos(b) * (X - p.x0) + np.sin(b) * (Y - p.y0)
+    t = p.time0 + np.arange(eta.shape[0]) * p.dt
+    arg = nu * d[None] - omega * t[:, None, None]
+    assert np.max(np.abs(eta - 0.5 * p.Hs * np.cos(arg))) < 1e-7 * p.Hs
+    assert np.max(np.abs(phis - p.g / omega * 0.5 * p.Hs * np.sin(arg))) < 1e-7 * p.Hs * p.g / omega
+    assert not np.array_equal(eta[:, 0, :], eta[:, -1, :])      # rows differ at a heading
+
+
+def test_random_wave_at_heading(ow3d, tmp_path):
+    """ispec 31: the JONSWAP coefficients of the long-crested case, moved to
+    each point along the heading."""
+    import ctypes as C
+    p = _heading_deck(tmp_path, "31 1.25 0.04 0.8 20. 4 -34 0. 0. run06.el 30.0 1.0 3.3", nsteps="1000")
+    eta, phis, (i0, i1, j0, j1) = ow3d.incident_wave(p, 0)
+    N = eta.shape[0]
+    assert N == 1024
+    df = 1 / (N * p.dt)
+    k = np.arange(1, N // 2)
+    S = _jonswap(k * df, p.Hs, p.Tp, p.gamma_jonswap)
+    n_cut = int(np.floor(np.sqrt(p.g * p.kh_max / p.h0 * np.tanh(p.kh_max)) / (2 * np.pi * df) + 0.5)) + 1
+    psi = (C.c_float * (N // 2 - 1))()
+    ow3d.lib().ow3d_test_ran1(-34, N // 2 - 1, psi, None)
+    ph = 2 * np.pi * np.frombuffer(psi, dtype=np.float32).astype(np.float64)
+    want = np.where(k < n_cut - 1, np.sqrt(2 * S * df) * (np.cos(ph).astype(np.float32) + 1j * np.sin(ph).astype(np.float32)), 0)
+    nu = _newton_k(2 * np.pi * k * df, p.h0, p.g)
+    x, y = _xy(p)
+    b = np.deg2rad(p.beta0)
+    for (ci, cj) in ((0, 0), (5, 3)):
+        d = np.cos(b) * (x[i0 - 1 + ci] - p.x0) + np.sin(b) * (y[j0 - 1 + cj] - p.y0)
+        ce = np.conj(np.fft.fft(eta[:, cj, ci])[1:N // 2]) * 2 / N
+        assert np.max(np.abs(ce - want * np.exp(1j * nu * d))) < 1e-6 * np.abs(want).max(), (ci, cj)
+
+
+def test_heading_needs_zone_without_rotation(ow3d, tmp_path):
+    p = _heading_deck(tmp_path, "-30 1.25 0.04 0.8 35. 4 -34 1.5 0.5 run06.el 22.5 1.0 3.3")
+    p.zones[0].degrees = 10.0
+    with pytest.raises(ow3d.OW3DError, match="degrees"):
+        ow3d.incident_wave(p, 0)
