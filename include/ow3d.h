@@ -147,6 +147,13 @@ typedef struct ow3d_params {
     double Tp, Hs, h0;            /* period (peak period), height (significant height), depth */
     double kh_max, x0, y0;        /* spectrum cut-off; origin of the wave's phase */
     double gamma_jonswap, beta0, s0;  /* JONSWAP gamma (3.3 unless ispec 3 / >= 30), heading, spreading */
+    /* line 8, the stream-function wave of IncWaveType 1 (ReadInputFileParameters.f90:291-293) */
+    double sf_H, sf_h, sf_L, sf_T;    /* height, depth, wavelength, period */
+    double sf_uEorS;                  /* mean current (Eulerian or Stokes) */
+    int    sf_wavel_or_per;           /* 0: the wavelength is given, 1: the period */
+    int    sf_euler_or_stokes;        /* 0: Eulerian current, 1: Stokes drift */
+    int    sf_nsteps;                 /* height steps of the solver */
+    int    sf_nmodes;                 /* Fourier modes */
 } ow3d_params;
 
 typedef struct ow3d_handle ow3d_handle;
@@ -264,6 +271,19 @@ int ow3d_put_surface(ow3d_handle* h, const double* E, const double* P);
 /* Read back E, P, W (Nxg*Nyg) and phi (Nzg*Nxg*Nyg); any pointer may be NULL. */
 int ow3d_get_state(ow3d_handle* h, double* E, double* P, double* W,
                    double* phi, double* t);
+
+/* The stream-function wave of the deck's line 8 (IncWaveType 1): Fenton's
+ * Fourier solution as stream_func_set_up / stream_func_coeffs compute it
+ * (src/utilities/stream_func_set_up.f90:1-59, stream_func_coeffs.f:1-153),
+ * evaluated as stream_func_wave_finite (stream_func_wave_finite.f:3-71):
+ * eta and the surface potential phiS at the n positions x (m, in the frame
+ * where the crest is at x = 0 at t = 0) at time t (s); eta / phis may be
+ * NULL. info (4 doubles, may be NULL): wavenumber, wavelength, period and
+ * phase speed. Host-only. For relaxation targets sample every RK stage time
+ * and pass the series with ow3d_set_relax_target mode 1; for an initial
+ * condition evaluate at t = 0. */
+int ow3d_stream_function_wave(const ow3d_params* p, int n, const double* x, double t, double* eta,
+                              double* phis, double* info);
 
 /* The incident wave of IncWaveType 2 on generation zone `zone` (0-based), as
  * OceanWave3DT0Setup.f90:176-255 builds RandomWave(zone)%eta and %Phis

@@ -91,6 +91,16 @@ def _b(path):
     return str(path).encode()
 
 
+def stream_function_wave(params, x, t=0.0):
+    """The stream-function wave of the deck's line 8 at positions x and time t:
+    eta, surface phi and (k, L, T, c)."""
+    x = _np.ascontiguousarray(x, dtype=_np.float64)
+    eta, phis, info = _np.zeros_like(x), _np.zeros_like(x), _np.zeros(4)
+    _check(lib().ow3d_stream_function_wave(_C.byref(params), x.size, _d(x), float(t), _d(eta), _d(phis), _d(info)),
+           "ow3d_stream_function_wave")
+    return eta, phis, tuple(info)
+
+
 def incident_wave(params, zone, nt=None):
     """The incident wave of IncWaveType 2 on generation zone `zone` (0-based):
     eta and surface phi as (nt, rows, columns) arrays every dt (nt defaults

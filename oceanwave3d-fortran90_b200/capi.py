@@ -63,6 +63,9 @@ class Params(C.Structure):
         ("Tp", C.c_double), ("Hs", C.c_double), ("h0", C.c_double),
         ("kh_max", C.c_double), ("x0", C.c_double), ("y0", C.c_double),
         ("gamma_jonswap", C.c_double), ("beta0", C.c_double), ("s0", C.c_double),
+        ("sf_H", C.c_double), ("sf_h", C.c_double), ("sf_L", C.c_double), ("sf_T", C.c_double),
+        ("sf_uEorS", C.c_double), ("sf_wavel_or_per", C.c_int), ("sf_euler_or_stokes", C.c_int),
+        ("sf_nsteps", C.c_int), ("sf_nmodes", C.c_int),
     ]
 
 
@@ -100,6 +103,7 @@ def default_params(**kw):
     p.precision = PREC_FP64; p.krylov = KRYLOV_FGMRES; p.device = 0
     p.StoreDataONOFF = 0; p.formattype = 0
     p.ispec = -1; p.gamma_jonswap = 3.3; p.s0 = 1.0
+    p.sf_nsteps = 1
     for k, v in kw.items():
         if k == "zones":
             for i, z in enumerate(v):
@@ -172,6 +176,7 @@ def declare(lib):
         "ow3d_store_data": (C.c_int, [H, C.c_char_p, _I]),
         "ow3d_kinematics": (C.c_int, [H, _D, _D, _D, _D]),
         "ow3d_incident_wave": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _D, _D, _I]),
+        "ow3d_stream_function_wave": (C.c_int, [C.c_void_p, C.c_int, _D, C.c_double, _D, _D, _D]),
         "ow3d_store_kinematics": (C.c_int, [H, C.c_char_p, _I]),
     }
     for name, (res, args) in sig.items():

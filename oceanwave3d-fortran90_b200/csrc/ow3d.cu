@@ -863,6 +863,18 @@ int ow3d_read_deck(const char* path, ow3d_params* p) {
     return r;
 }
 
+int ow3d_stream_function_wave(const ow3d_params* p, int n, const double* x, double t, double* eta, double* phis,
+                              double* info) {
+    if (!p || n < 0 || (n > 0 && !x)) return OW3D_ERR_BAD_INPUT;
+    SFWave w;
+    std::string err;
+    const int r = stream_function_solve(*p, w, &err);
+    if (r) { g_last_error = err; return r; }
+    stream_function_eval(w, n, x, t, eta, phis);
+    if (info) { info[0] = w.k; info[1] = w.L; info[2] = w.T; info[3] = w.c; }
+    return OW3D_OK;
+}
+
 int ow3d_incident_wave(const ow3d_params* p, int zone, int nt, double* eta, double* phis, int* box) {
     if (!p) return OW3D_ERR_BAD_INPUT;
     std::string err;

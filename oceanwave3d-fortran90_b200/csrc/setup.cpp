@@ -641,6 +641,8 @@ int default_params(ow3d_params* p) {
     p->ispec = -1; p->seed = 0; p->seed2 = 0;
     p->Tp = 0; p->Hs = 0; p->h0 = 0; p->kh_max = 0; p->x0 = 0; p->y0 = 0;
     p->gamma_jonswap = 3.3; p->beta0 = 0; p->s0 = 1.0;
+    p->sf_H = p->sf_h = p->sf_L = p->sf_T = p->sf_uEorS = 0;
+    p->sf_wavel_or_per = p->sf_euler_or_stokes = 0; p->sf_nsteps = 1; p->sf_nmodes = 0;
     return OW3D_OK;
 }
 
@@ -738,7 +740,11 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
         p->reltol = r.d(o + 3); p->abstol = r.d(o + 4); p->maxit = r.n(o + 5); p->cyclet = r.c(o + 6);
         p->nu1 = r.n(o + 7); p->nu2 = r.n(o + 8); p->MGmaxgrids = r.n(o + 9);
     }
-    r = next();  // stream-function line (always present)
+    r = next();  // stream-function line H h L T WAVELorPER uEorS EorS nsteps nmodes (always present, :291-293)
+    if (r.nnum() >= 9) {
+        p->sf_H = r.d(0); p->sf_h = r.d(1); p->sf_L = r.d(2); p->sf_T = r.d(3); p->sf_wavel_or_per = r.n(4);
+        p->sf_uEorS = r.d(5); p->sf_euler_or_stokes = r.n(6); p->sf_nsteps = r.n(7); p->sf_nmodes = r.n(8);
+    }
     r = next();  // StoreDataONOFF formattype [iKinematics nOutFiles] (ReadInputFileParameters.f90:300-405)
     if (r.nnum() >= 1) p->StoreDataONOFF = r.n(0);
     if (r.nnum() >= 2) {

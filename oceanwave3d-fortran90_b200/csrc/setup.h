@@ -64,6 +64,17 @@ struct Ran1 {
     float next(int& idum);
 };
 int incident_wave_samples(const ow3d_params& p);
+
+// Stream-function wave of the deck's line 8 (sfwave.cpp): the solution
+// vector z (1-based, 2N+10 unknowns), the elevation coefficients y (1..N),
+// wavenumber, wavelength, period, phase speed and gravity.
+struct SFWave {
+    int n = 0;
+    double k = 0, L = 0, T = 0, c = 0, g = 0;
+    std::vector<double> z, y;
+};
+int stream_function_solve(const ow3d_params& p, SFWave& w, std::string* err);
+void stream_function_eval(const SFWave& w, int nx, const double* x, double t, double* eta, double* phis);
 int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* phis, int* box, std::string* err);
 int read_deck(const char* path, ow3d_params* p, std::string* err);
 

@@ -1,0 +1,248 @@
+// The stream-function (Fourier) solution of a steady periodic wave on
+// constant depth, the incident wave of IncWaveType 1. It is Fenton's method
+// in the form the reference uses (src/utilities/stream_func_set_up.f90:1-59,
+// stream_func_coeffs.f:1-153, init.f:1-72, eqns.f:1-74): 2N+10 unknowns
+// (kd, kH, T sqrt(gk), c sqrt(k/g), the two mean currents, the mean fluid
+// speed, the volume flux, the Bernoulli constant, k eta at the N+1
+// collocation points over half a wavelength and the N stream-function
+// coefficients), Newton's method with a forward-difference Jacobian
+// (step 1% of the unknown, 1e-5 near zero), the height reached in nsteps
+// steps with the solution extrapolated from the last two, convergence when
+// the summed correction is below 1e-6 (1e-8 on the last step). The surface
+// elevation and potential at (x, t) follow stream_func_wave_finite
+// (stream_func_wave_finite.f:3-71).
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "setup.h"
+
+namespace ow3d {
+namespace {
+
+struct SFProblem {
+    int n = 0, num = 0;
+    bool finite = true, period = false, euler = true;
+    double hoverd = 0, height = 0, value = 0, pi = 0;
+    std::vector<double> cosa, sina, coeff;   // cosa, sina: 0..2N; coeff: 1..N
+};
+
+// init.f: the linear solution as the first guess; z is 1-based (z[0] unused)
+void sf_init(SFProblem& P, std::vector<double>& z, std::vector<double>& s1, std::vector<double>& s2) {
+    const int n = P.n, num = P.num;
+    const double pi = P.pi;
+    if (P.finite) {
+        if (P.period) {
+            const double A = 4.0 * pi * pi * P.height / P.hoverd;
+            const double B = A / std::sqrt(std::tanh(A));
+            const double T = std::tanh(B);
+            z[1] = B + (A - B * T) / (T + B * (1.0 - T * T));
+        } else {
+            z[1] = 2.0 * pi * P.height / P.hoverd;
+        }
+        z[2] = z[1] * P.hoverd;
+        z[4] = std::sqrt(std::tanh(z[1]));
+    } else {
+        z[1] = -1.0;
+        z[4] = 1.0;
+        z[2] = P.period ? 4.0 * pi * pi * P.height : 2.0 * pi * P.height;
+    }
+    z[3] = 2.0 * pi / z[4];
+    if (P.euler) { z[5] = P.value * std::sqrt(z[2]); z[6] = 0.0; }
+    else { z[5] = 0.0; z[6] = P.value * std::sqrt(z[2]); }
+    z[7] = z[4];
+    z[8] = 0.0;
+    z[9] = 0.5 * z[7] * z[7];
+    z[10] = 0.5 * z[2];
+    P.cosa[0] = 1.0;
+    P.sina[0] = 0.0;
+    for (int i = 1; i <= n; ++i) {
+        P.cosa[i] = std::cos(i * pi / n);
+        P.cosa[i + n] = std::cos((i + n) * pi / n);
+        P.sina[i] = std::sin(i * pi / n);
+        P.sina[i + n] = std::sin((i + n) * pi / n);
+        z[n + i + 10] = 0.0;
+        z[i + 10] = 0.5 * z[2] * P.cosa[i];
+    }
+    z[n + 11] = 0.5 * z[2] / z[7];
+    for (int i = 1; i <= 9; ++i) s1[i] = z[i];
+    for (int i = 10; i <= num; ++i) s1[i] = 0.0;
+    for (int i = 1; i <= num; ++i) s2[i] = 0.0;
+}
+
+// eqns.f: the residuals of the 2N+10 equations
+void sf_eqns(SFProblem& P, const std::vector<double>& z, std::vector<double>& rhs) {
+    const int n = P.n;
+    rhs[1] = P.finite ? z[2] - z[1] * P.hoverd : z[1] + 1.0;
+    rhs[2] = P.period ? z[2] - P.height * z[3] * z[3] : z[2] - 2.0 * P.pi * P.height;
+    rhs[3] = z[4] * z[3] - P.pi - P.pi;
+    rhs[4] = z[5] + z[7] - z[4];
+    rhs[5] = z[6] + z[7] - z[4];
+    if (P.finite) {
+        rhs[5] = rhs[5] - z[8] / z[1];
+        for (int i = 1; i <= n; ++i) P.coeff[i] = z[n + i + 10] / std::cosh(i * z[1]);
+    }
+    const int it = P.euler ? 5 : 6;
+    rhs[6] = z[it] - P.value * std::sqrt(z[2]);
+    rhs[7] = z[10] + z[n + 10];
+    for (int i = 1; i <= n - 1; ++i) rhs[7] = rhs[7] + z[10 + i] + z[10 + i];
+    rhs[8] = z[10] - z[n + 10] - z[2];
+    for (int m = 0; m <= n; ++m) {
+        double psi = 0.0, u = 0.0, v = 0.0;
+        if (P.finite) {
+            for (int j = 1; j <= n; ++j) {
+                const int nm = (m * j) % (n + n);
+                const double e = std::exp(j * (z[1] + z[10 + m]));
+                const double s = 0.5 * (e - 1.0 / e), c = 0.5 * (e + 1.0 / e);
+                psi = psi + P.coeff[j] * s * P.cosa[nm];
+                u = u + j * P.coeff[j] * c * P.cosa[nm];
+                v = v + j * P.coeff[j] * s * P.sina[nm];
+            }
+        } else {
+            for (int j = 1; j <= n; ++j) {
+                const int nm = (m * j) % (n + n);
+                const double e = std::exp(j * z[10 + m]);
+                psi = psi + z[n + j + 10] * e * P.cosa[nm];
+                u = u + j * z[n + j + 10] * e * P.cosa[nm];
+                v = v + j * z[n + j + 10] * e * P.sina[nm];
+            }
+        }
+        rhs[m + 9] = psi - z[8] - z[7] * z[m + 10];
+        rhs[n + m + 10] = 0.5 * ((-z[7] + u) * (-z[7] + u) + v * v) + z[m + 10] - z[9];
+    }
+}
+
+// A x = b for a dense column-major matrix (Gaussian elimination with partial
+// pivoting); 1-based b, 0-based A(i, j) = A[(j-1)*n + (i-1)]. false when singular.
+bool dense_solve(int n, std::vector<double>& A, std::vector<double>& b) {
+    auto a = [&](int i, int j) -> double& { return A[(size_t)(j - 1) * n + (i - 1)]; };
+    for (int k = 1; k <= n; ++k) {
+        int piv = k;
+        for (int i = k + 1; i <= n; ++i) if (std::fabs(a(i, k)) > std::fabs(a(piv, k))) piv = i;
+        if (a(piv, k) == 0.0) return false;
+        if (piv != k) {
+            for (int j = 1; j <= n; ++j) std::swap(a(k, j), a(piv, j));
+            std::swap(b[k], b[piv]);
+        }
+        for (int i = k + 1; i <= n; ++i) {
+            const double f = a(i, k) / a(k, k);
+            if (f == 0.0) continue;
+            for (int j = k + 1; j <= n; ++j) a(i, j) -= f * a(k, j);
+            b[i] -= f * b[k];
+        }
+    }
+    for (int k = n; k >= 1; --k) {
+        double s = b[k];
+        for (int j = k + 1; j <= n; ++j) s -= a(k, j) * b[j];
+        b[k] = s / a(k, k);
+    }
+    return true;
+}
+
+}  // namespace
+
+// stream_func_set_up.f90:21-57 and stream_func_coeffs.f:15-80.
+int stream_function_solve(const ow3d_params& p, SFWave& w, std::string* err) {
+    auto fail = [&](const std::string& m) { if (err) *err = m; return OW3D_ERR_BAD_INPUT; };
+    const int n = p.sf_nmodes;
+    if (n < 2 || n > 1000 || p.sf_nsteps < 1 || !(p.sf_H > 0) || !(p.sf_h > 0) || !(p.sf_L > 0) || !(p.g > 0))
+        return fail("stream_function_wave: line 8 needs H, h, L > 0, nsteps >= 1 and at least 2 Fourier modes");
+    if (p.sf_wavel_or_per != 0 && !(p.sf_T > 0)) return fail("stream_function_wave: the period must be positive");
+    const double grav = p.g, depth = p.sf_h;
+    double wavenum = 2.0 * std::acos(-1.0) / p.sf_L;   // ReadInputFileParameters.f90:293
+    SFProblem P;
+    P.n = n;
+    P.num = 2 * n + 10;
+    P.pi = 4.0 * std::atan(1.0);
+    P.finite = !(wavenum * depth > 9.0);
+    P.period = p.sf_wavel_or_per != 0;
+    P.euler = p.sf_euler_or_stokes == 0;
+    const double hoverd0 = P.finite ? p.sf_H / depth : 0.0;
+    const double height0 = P.period ? p.sf_H / (grav * p.sf_T * p.sf_T) : p.sf_H / p.sf_L;
+    P.value = p.sf_uEorS / std::sqrt(grav * p.sf_H);
+    const int num = P.num;
+    P.cosa.assign((size_t)num + 1, 0.0);
+    P.sina.assign((size_t)num + 1, 0.0);
+    P.coeff.assign((size_t)num + 1, 0.0);
+    std::vector<double> z((size_t)num + 1, 0.0), s1(z), s2(z), rhs1(z), rhs2(z), b(z);
+    std::vector<double> A((size_t)num * num);
+    const double crit = 1e-6;
+    const int nstep = p.sf_nsteps, number = 256;
+    const double dhe = height0 / nstep, dho = hoverd0 / nstep;
+    for (int ns = 1; ns <= nstep; ++ns) {
+        P.height = ns * dhe;
+        P.hoverd = ns * dho;
+        if (ns <= 1) sf_init(P, z, s1, s2);
+        else for (int i = 1; i <= num; ++i) z[i] = 2.0 * s2[i] - s1[i];
+        bool done = false;
+        for (int iter = 1; iter <= number && !done; ++iter) {
+            sf_eqns(P, z, rhs1);
+            for (int i = 1; i <= num; ++i) {
+                double h = 0.01 * z[i];
+                if (std::fabs(z[i]) < 1e-4) h = 1e-5;
+                z[i] = z[i] + h;
+                sf_eqns(P, z, rhs2);
+                z[i] = z[i] - h;
+                b[i] = -rhs1[i];
+                for (int j = 1; j <= num; ++j) A[(size_t)(i - 1) * num + (j - 1)] = (rhs2[j] - rhs1[j]) / h;
+            }
+            if (!dense_solve(num, A, b)) return fail("stream_function_wave: singular Newton matrix");
+            double sum = 0.0;
+            for (int i = 1; i <= num; ++i) { sum += std::fabs(b[i]); z[i] = z[i] + b[i]; }
+            const double criter = (ns == nstep) ? 0.01 * crit : crit;
+            if (sum < criter) done = true;
+        }
+        if (!done) return fail("stream_function_wave: the solution did not converge in 256 iterations");
+        if (ns == 1) { for (int i = 1; i <= num; ++i) s2[i] = z[i]; }
+        else { for (int i = 1; i <= num; ++i) { s1[i] = s2[i]; s2[i] = z[i]; } }
+    }
+    // Fourier coefficients of the elevation (stream_func_coeffs.f:72-78)
+    std::vector<double> y((size_t)num + 1, 0.0);
+    for (int j = 1; j <= n; ++j) {
+        double sum = 0.5 * (z[10] + z[n + 10] * ((j % 2) ? -1.0 : 1.0));
+        for (int m = 1; m <= n - 1; ++m) sum = sum + z[10 + m] * P.cosa[(m * j) % (n + n)];
+        y[j] = 2.0 * sum / n;
+    }
+    double period = p.sf_T;
+    if (!P.period) period = z[3] / std::sqrt(grav * wavenum);
+    else wavenum = z[1] / depth;
+    w.n = n;
+    w.k = wavenum;
+    w.T = period;
+    w.L = 2.0 * std::acos(-1.0) / wavenum;
+    w.c = w.L / w.T;
+    w.g = grav;
+    w.z = z;
+    w.y = y;
+    return OW3D_OK;
+}
+
+// stream_func_wave_finite.f:10-66: elevation and surface potential at x, t.
+void stream_function_eval(const SFWave& w, int nx, const double* x, double t, double* eta, double* phis) {
+    const int n = w.n;
+    const std::vector<double>& zz = w.z;
+    const std::vector<double>& yy = w.y;
+    const double kinv = 1.0 / w.k;
+    const double ufactor = std::sqrt(w.g * kinv), pfactor = ufactor * kinv;
+    const double omega_t = w.k * ufactor * zz[4] * t;
+    for (int j = 0; j < nx; ++j) {
+        const double kx = w.k * x[j] - omega_t;
+        double km = (double)n;
+        double e_j = 0.5 * yy[n] * std::cos(km * kx);
+        for (int m = 1; m <= n - 1; ++m) {
+            km = (double)m;
+            e_j = e_j + yy[m] * std::cos(km * kx);
+        }
+        double ph = (zz[4] - zz[7]) * x[j] * w.k;
+        for (int m = 1; m <= n; ++m) {
+            km = (double)m;
+            const double e = std::exp(km * (zz[1] + e_j));
+            const double b = zz[n + m + 10] * 0.5 * (e + 1.0 / e) / std::cosh(km * zz[1]);
+            ph = ph + b * std::sin(km * kx);
+        }
+        if (eta) eta[j] = kinv * e_j;
+        if (phis) phis[j] = ph * pfactor;
+    }
+}
+
+}  // namespace ow3d

@@ -1,0 +1,112 @@
+"""Stream-function wave of IncWaveType 1 (ow3d_stream_function_wave): the
+reference's Fenton solution, host-only.
+
+Pinned by theory: the linear limit (Airy dispersion and profile), the
+third-order Stokes phase speed c^2 = g/k tanh(kd) (1 + (ka)^2 (9 - 10 s^2 +
+9 s^4) / (8 s^4)), s = tanh(kd), which the solution must follow up to
+(ka)^4 terms; and exact properties of a steady wave: crest-to-trough height,
+zero mean elevation, translation at the phase speed. The reference's
+example decks with IncWaveType 1 all solve.
+"""
+import os
+import pathlib
+
+import numpy as np
+import pytest
+
+
+def _params(ow3d, kd, kH, nmodes=20, nsteps=4, period=None):
+    p = ow3d.default_params(Nx=65, Nz=9, Lx=2 * np.pi, Ly=1.0, Lz=kd)
+    p.g = 9.81
+    p.sf_h, p.sf_L, p.sf_H = kd, 2 * np.pi, kH
+    p.sf_wavel_or_per, p.sf_nsteps, p.sf_nmodes = 0, nsteps, nmodes
+    if period is not None:
+        p.sf_wavel_or_per, p.sf_T = 1, period
+    return p
+
+
+def test_line_8_parsed(ow3d, tmp_path):
+    from test_deck import DECK_3D
+    f = tmp_path / "a.inp"
+    f.write_text(DECK_3D)
+    p = ow3d.read_deck(f)
+    assert (p.sf_H, p.sf_h, p.sf_L, p.sf_T) == (0.1, 1.0, 3.0, 2.0)
+    assert (p.sf_wavel_or_per, p.sf_uEorS, p.sf_euler_or_stokes, p.sf_nsteps, p.sf_nmodes) == (0, 0.0, 1, 6, 24)
+
+
+def test_linear_limit(ow3d):
+    p = _params(ow3d, 1.0, 1e-5)
+    x = np.linspace(0, 2 * np.pi, 41)
+    t = 0.37
+    eta, phis, (k, L, T, c) = ow3d.stream_function_wave(p, x, t)
+    om = np.sqrt(p.g * np.tanh(1.0))
+    assert abs(T - 2 * np.pi / om) < 1e-9 * T and abs(c - L / T) < 1e-12 * c and k == 1.0
+    a = 0.5e-5
+    assert np.max(np.abs(eta - a * np.cos(x - om * t))) < 1e-3 * a
+    # the surface potential of the linear wave, g/omega a sin(kx - omega t)
+    assert np.max(np.abs(phis - p.g / om * a * np.sin(x - om * t))) < 1e-3 * p.g / om * a
+
+
+@pytest.mark.parametrize("kd,ka", [(3.0, 0.1), (1.0, 0.05), (3.0, 0.05)])
+def test_stokes_third_order_phase_speed(ow3d, kd, ka):
+    _, _, (k, L, T, c) = ow3d.stream_function_wave(_params(ow3d, kd, 2 * ka), np.zeros(1))
+    s = np.tanh(kd)
+    c0 = np.sqrt(9.81 * s)
+    pred = 1 + 0.5 * ka ** 2 * (9 - 10 * s ** 2 + 9 * s ** 4) / (8 * s ** 4)
+    assert abs(c / c0 - pred) < 3 * ka ** 4
+
+
+def test_steep_wave_exact_properties(ow3d):
+    """kd = 1 and H/L at half the breaking limit (about 0.054 at kd = 1):
+    height, mean level and steady translation."""
+    p = _params(ow3d, 1.0, 0.054 * 2 * np.pi, nmodes=24, nsteps=6)
+    H = p.sf_H
+    x = np.linspace(0, 2 * np.pi, 257)[:-1]
+    eta, phis, (k, L, T, c) = ow3d.stream_function_wave(p, x, 0.0)
+    crest, trough = ow3d.stream_function_wave(p, np.array([0.0, np.pi]), 0.0)[0]
+    assert abs((crest - trough) - H) < 1e-10 * H
+    assert abs(eta.mean()) < 1e-12 * H
+    assert crest > 0.55 * H and -trough < 0.45 * H          # crests sharper than troughs
+    t = 0.3
+    eta_t, _, _ = ow3d.stream_function_wave(p, x + c * t, t)
+    assert np.max(np.abs(eta_t - eta)) < 1e-10 * H
+
+
+def test_period_given(ow3d):
+    """With the period given (WAVELorPER = 1) the wavelength follows from the
+    solution; in the linear limit it is the Airy wavelength."""
+    om = 2 * np.pi / 2.0
+    p = _params(ow3d, 1.0, 1e-5, period=2.0)
+    _, _, (k, L, T, c) = ow3d.stream_function_wave(p, np.zeros(1))
+    assert T == 2.0 and abs(om ** 2 - p.g * k * np.tanh(k * p.sf_h)) < 1e-6 * om ** 2
+    assert abs(c - L / T) < 1e-12 * c
+
+
+def test_errors(ow3d):
+    p = _params(ow3d, 1.0, 0.1, nmodes=1)
+    with pytest.raises(ow3d.OW3DError, match="Fourier modes"):
+        ow3d.stream_function_wave(p, np.zeros(3))
+
+
+REF_DECKS = pathlib.Path(os.environ.get("OW3D_REFERENCE_DECKS", "/root/reference/examples/inputfiles"))
+
+
+@pytest.mark.skipif(not REF_DECKS.is_dir(), reason="reference example decks not on this machine")
+def test_reference_stream_function_decks_solve(ow3d):
+    solved = 0
+    for f in sorted(REF_DECKS.iterdir()):
+        if not f.name.startswith("OceanWave3D.inp"):
+            continue
+        try:
+            p = ow3d.read_deck(f)
+        except ow3d.OW3DError:
+            continue
+        if p.IncWaveType != 1:
+            continue
+        L = ow3d.stream_function_wave(p, np.zeros(1))[2][1]     # the solution's wavelength
+        x = np.linspace(0, L, 257)
+        eta, phis, (k, L, T, c) = ow3d.stream_function_wave(p, x)
+        assert abs((eta.max() - eta.min()) - p.sf_H) < 1e-3 * p.sf_H, f.name
+        assert np.all(np.isfinite(phis)) and abs(c - L / T) < 1e-12 * c, f.name
+        solved += 1
+    assert solved >= 3
