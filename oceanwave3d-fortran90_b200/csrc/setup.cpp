@@ -383,6 +383,41 @@ double jonswap_spectrum(double f, double Hs, double Tp, double gamma) {
     const double a = std::exp(-0.5 * std::pow((f - fp) / (sigma * fp), 2));
     return A / std::pow(f, 5) * std::exp(-B / std::pow(f, 4)) * std::pow(gamma, a);
 }
+// Headings (radians) of the ncta frequency components of a cos^(2 s0)
+// spread sea, drawn from the generator by the inverse of the tabulated
+// cumulative distribution (spreading.f90:1-89). beta0 enters as the
+// reference passes it (in degrees, used as radians there). A deviate above
+// the table's last value takes the last heading (the reference reads past
+// its table there).
+std::vector<double> spread_headings(Ran1& rng, int& seed2, double s0, double beta0, int ncta) {
+    const double pi = std::acos(-1.0);
+    const double ipow = 2.0 * s0;
+    const double ctamax = beta0 + 0.5 * pi, ctamin = beta0 - 0.5 * pi;
+    const double dcta1 = (ctamax - ctamin) / (double)(float)(ncta - 1);
+    double sum1 = 0.0;
+    for (int i = 1; i <= ncta; ++i) {
+        const double aaa = ctamin + (i - 1) * dcta1;
+        sum1 = sum1 + std::pow(std::cos((aaa - beta0) / 2.0), ipow) * dcta1;
+    }
+    const double spm = 1.0 / sum1;
+    std::vector<double> cta((size_t)ncta + 1), cosint((size_t)ncta + 1);
+    double ds = 0.0;
+    const double dcta = pi / (double)(float)ncta;
+    for (int i = 1; i <= ncta; ++i) {
+        cta[(size_t)i] = ctamin + (i - 1) * dcta;
+        ds = ds + std::pow(std::cos((cta[(size_t)i] - beta0) / 2.0), ipow) * dcta;
+        cosint[(size_t)i] = ds * spm;
+    }
+    std::vector<double> beta((size_t)ncta + 1, 0.0);
+    for (int j = 1; j <= ncta; ++j) {
+        const double ps = (double)rng.next(seed2);
+        int i = 1;
+        while (i <= ncta && !(cosint[(size_t)i] >= ps)) ++i;
+        beta[(size_t)j] = cta[(size_t)std::min(i, ncta)];
+    }
+    return beta;   // 1-based
+}
+
 // In-place radix-2 transform X_j = sum_k Z_k exp(-2 pi i j k / n), n a power of two.
 void fft_minus(std::vector<std::complex<double>>& Z) {
     const size_t n = Z.size();
@@ -433,9 +468,9 @@ int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* p
     auto fail = [&](const std::string& m, int code) { if (err) *err = m; return code; };
     if (p.IncWaveType != 2) return fail("incident_wave: the deck's IncWaveType is not 2", OW3D_ERR_BAD_INPUT);
     if (!(p.ispec == -1 || p.ispec == 0 || p.ispec == 1 || p.ispec == 3 || p.ispec == -30 || p.ispec == 30 ||
-          p.ispec == 31))
+          p.ispec == 31 || p.ispec == 34))
         return fail("incident_wave: ispec " + std::to_string(p.ispec) +
-                        " (waves from a file or spread directional waves) is not supported; -1, 0, 1, 3, -30, 30 and 31 are",
+                        " (waves from a file, normal spreading) is not supported; -1, 0, 1, 3, -30, 30, 31 and 34 are",
                     OW3D_ERR_UNSUPPORTED);
     if (p.relaxONOFF != 1 || zone < 0 || zone >= p.relaxNo || zone >= OW3D_MAX_ZONES)
         return fail("incident_wave: no such relaxation zone", OW3D_ERR_BAD_INPUT);
@@ -474,6 +509,8 @@ int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* p
         const double dy = heading ? G.y[(size_t)(z.j0 - 1 + j)] - p.y0 : 0.0;
         return cosb * dx + sinb * dy;
     };
+    // per-frequency headings of a spread sea (ispec 34), cos and sin, index k
+    std::vector<double> kcos, ksin;
     std::vector<double> le((size_t)nt * bx * ny_eval), lp(le.size());   // [n][j][i]
     auto at = [&](int n, int j, int i) { return ((size_t)n * ny_eval + j) * bx + i; };
     if (p.ispec < 0) {
@@ -492,10 +529,22 @@ int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* p
     } else {
         const int N = nref;
         const double df = 1.0 / (N * p.dt), cst = std::sqrt(df), domega = twopi / (N * p.dt);
-        const bool pm = (p.ispec == 0 || p.ispec == 30);
+        const bool pm = (p.ispec == 0 || p.ispec == 30);   // the others: JONSWAP
         std::vector<std::complex<double>> c((size_t)N / 2, 0.0);
         Ran1 rng;
         int seed2 = p.seed2;
+        if (p.ispec == 34) {
+            // build_coeff_3D_Cos.f90:38-52: the headings take the first N/2
+            // deviates; converted to degrees and back for the phase
+            const std::vector<double> b = spread_headings(rng, seed2, p.s0, p.beta0, N / 2);
+            kcos.assign((size_t)N / 2, 0.0); ksin.assign((size_t)N / 2, 0.0);
+            const double rad2deg = 1.0 / (pi / 180.0), deg2rad = pi / 180.0;
+            for (int k = 1; k < N / 2; ++k) {
+                const double deg = b[(size_t)(k + 1)] * rad2deg;   // beta(i) with i = k + 1
+                kcos[(size_t)k] = std::cos(deg2rad * deg);
+                ksin[(size_t)k] = std::sin(deg2rad * deg);
+            }
+        }
         for (int i = 2; i <= N / 2; ++i) {
             const double freq = (i - 1) * df;
             const double psi = (double)rng.next(seed2);
@@ -514,11 +563,13 @@ int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* p
         std::vector<std::complex<double>> ZE((size_t)N), ZP((size_t)N);
         for (int j = 0; j < ny_eval; ++j)
             for (int i = 0; i < bx; ++i) {
-                const double dist = dist_of(i, j);
+                const double dx = G.x[(size_t)(z.i0 - 1 + i)] - p.x0;
+                const double dy = heading ? G.y[(size_t)(z.j0 - 1 + j)] - p.y0 : 0.0;
                 std::fill(ZE.begin(), ZE.end(), 0.0);
                 std::fill(ZP.begin(), ZP.end(), 0.0);
                 for (int k = 1; k < kmax; ++k) {
                     const double omega = k * domega, nu = nus[(size_t)k];
+                    const double dist = kcos.empty() ? dist_of(i, j) : kcos[(size_t)k] * dx + ksin[(size_t)k] * dy;
                     const std::complex<double> e =
                         c[(size_t)k] * std::complex<double>(std::cos(nu * dist), std::sin(nu * dist));
                     const std::complex<double> v = (p.g / omega) * std::complex<double>(e.imag(), -e.real());

@@ -299,3 +299,49 @@ def test_heading_needs_zone_without_rotation(ow3d, tmp_path):
     p.zones[0].degrees = 10.0
     with pytest.raises(ow3d.OW3DError, match="degrees"):
         ow3d.incident_wave(p, 0)
+
+
+def _spread_headings(draws, s0, beta0, ncta):
+    """Headings drawn by the inverse of the tabulated cos^(2 s0) distribution
+    (spreading.f90): the first grid heading whose cumulative value reaches the
+    deviate."""
+    ipow = 2 * s0
+    cmin, cmax = beta0 - np.pi / 2, beta0 + np.pi / 2
+    d1 = (cmax - cmin) / float(np.float32(ncta - 1))
+    cc1 = cmin + np.arange(ncta) * d1
+    spm = 1.0 / np.sum(np.cos((cc1 - beta0) / 2) ** ipow * d1)
+    dc = np.pi / float(np.float32(ncta))
+    cta = cmin + np.arange(ncta) * dc
+    cosint = np.cumsum(np.cos((cta - beta0) / 2) ** ipow * dc) * spm
+    idx = np.minimum(np.searchsorted(cosint, draws, side="left"), ncta - 1)
+    return cta[idx]
+
+
+def test_spread_sea_cos2s(ow3d, tmp_path):
+    """ispec 34 (build_coeff_3D_Cos.f90, spreading.f90): N/2 headings drawn
+    first from the generator, then the phases; every component travels along
+    its own heading."""
+    import ctypes as C
+    p = _heading_deck(tmp_path, "34 1.25 0.04 0.8 20. 4 -34 0. 0.5 run06.el 0 8.0 3.3", nsteps="1000")
+    assert (p.ispec, p.beta0, p.s0) == (34, 0.0, 8.0)
+    eta, phis, (i0, i1, j0, j1) = ow3d.incident_wave(p, 0)
+    N = eta.shape[0]
+    draws = (C.c_float * (N - 1))()
+    ow3d.lib().ow3d_test_ran1(-34, N - 1, draws, None)
+    d = np.frombuffer(draws, dtype=np.float32).astype(np.float64)
+    beta = _spread_headings(d[:N // 2], p.s0, p.beta0, N // 2)      # beta0 enters as the deck gives it
+    assert np.all(np.abs(beta) <= np.pi / 2) and abs(np.mean(beta)) < 0.1
+    ph = 2 * np.pi * d[N // 2:]
+    df = 1 / (N * p.dt)
+    k = np.arange(1, N // 2)
+    S = _jonswap(k * df, p.Hs, p.Tp, p.gamma_jonswap)
+    n_cut = int(np.floor(np.sqrt(p.g * p.kh_max / p.h0 * np.tanh(p.kh_max)) / (2 * np.pi * df) + 0.5)) + 1
+    want = np.where(k < n_cut - 1, np.sqrt(2 * S * df) * (np.cos(ph).astype(np.float32) + 1j * np.sin(ph).astype(np.float32)), 0)
+    nu = _newton_k(2 * np.pi * k * df, p.h0, p.g)
+    bk = beta[1:N // 2]                                   # heading of component k is beta(k + 1)
+    x, y = _xy(p)
+    for (ci, cj) in ((0, 0), (6, 4)):
+        dx, dy = x[i0 - 1 + ci] - p.x0, y[j0 - 1 + cj] - p.y0
+        ce = np.conj(np.fft.fft(eta[:, cj, ci])[1:N // 2]) * 2 / N
+        w = want * np.exp(1j * nu * (np.cos(bk) * dx + np.sin(bk) * dy))
+        assert np.max(np.abs(ce - w)) < 1e-6 * np.abs(want).max(), (ci, cj)
