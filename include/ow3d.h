@@ -299,10 +299,11 @@ int ow3d_stream_function_wave(const ow3d_params* p, int n, const double* x, doub
  * random phases (RAN1_b seeded with seed2), spectra, kh_max truncation and
  * wavenumbers (fdwvnum.f90); -30, 30 and 31, the same waves at heading beta0
  * on every point of the zone (random_wave_signal_3D.f90, zones with
- * degrees = 0); 34, a JONSWAP sea with cos^(2 s0) spreading, each component
- * on its own heading drawn as spreading.f90 draws it; for random waves nt is
- * at most the reference's sample count. Waves from a file (ispec 2) and the
- * normal spreading of ispec 33 return OW3D_ERR_UNSUPPORTED. */
+ * degrees = 0); 33 and 34, JONSWAP seas with normal (build_coeff_3D.f90)
+ * and cos^(2 s0) (spreading.f90) spreading, each component on its own
+ * heading drawn as the reference draws it; for random waves nt is at most
+ * the reference's sample count. Waves from a file (ispec 2) return
+ * OW3D_ERR_UNSUPPORTED. */
 int ow3d_incident_wave(const ow3d_params* p, int zone, int nt, double* eta, double* phis, int* box);
 
 /* Relaxation-zone target signal for generation zone `zone` (0-based):

@@ -418,6 +418,25 @@ std::vector<double> spread_headings(Ran1& rng, int& seed2, double s0, double bet
     return beta;   // 1-based
 }
 
+// erf^-1(p) for 0 <= p < 1: a first guess from the asymptotic form
+// sqrt(-log(1-p)) blended with the series p sqrt(pi)/2, refined by Newton
+// steps on erf(x) - p (the reference's InvErf, a rational approximation of
+// Blair, Edwards and Johnson 1976, returns the same root to rounding).
+double inverse_erf(double p) {
+    if (p <= 0.0) return 0.0;
+    const double spi = std::sqrt(std::acos(-1.0));
+    double x = p < 0.7 ? 0.5 * spi * p * (1.0 + std::acos(-1.0) / 12.0 * p * p)
+                       : std::sqrt(-std::log((1.0 - p) * spi)) ;
+    for (int it = 0; it < 60; ++it) {
+        const double f = std::erf(x) - p;
+        const double d = 2.0 / spi * std::exp(-x * x);
+        const double step = f / d;
+        x -= step;
+        if (std::fabs(step) <= 1e-16 * std::max(1.0, std::fabs(x))) break;
+    }
+    return x;
+}
+
 // In-place radix-2 transform X_j = sum_k Z_k exp(-2 pi i j k / n), n a power of two.
 void fft_minus(std::vector<std::complex<double>>& Z) {
     const size_t n = Z.size();
@@ -468,9 +487,9 @@ int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* p
     auto fail = [&](const std::string& m, int code) { if (err) *err = m; return code; };
     if (p.IncWaveType != 2) return fail("incident_wave: the deck's IncWaveType is not 2", OW3D_ERR_BAD_INPUT);
     if (!(p.ispec == -1 || p.ispec == 0 || p.ispec == 1 || p.ispec == 3 || p.ispec == -30 || p.ispec == 30 ||
-          p.ispec == 31 || p.ispec == 34))
+          p.ispec == 31 || p.ispec == 33 || p.ispec == 34))
         return fail("incident_wave: ispec " + std::to_string(p.ispec) +
-                        " (waves from a file, normal spreading) is not supported; -1, 0, 1, 3, -30, 30, 31 and 34 are",
+                        " (waves from a file) is not supported; -1, 0, 1, 3, -30, 30, 31, 33 and 34 are",
                     OW3D_ERR_UNSUPPORTED);
     if (p.relaxONOFF != 1 || zone < 0 || zone >= p.relaxNo || zone >= OW3D_MAX_ZONES)
         return fail("incident_wave: no such relaxation zone", OW3D_ERR_BAD_INPUT);
@@ -552,6 +571,20 @@ int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* p
             const double spec = pm ? pm_spectrum(freq, p.Hs, p.Tp) : jonswap_spectrum(freq, p.Hs, p.Tp, p.gamma_jonswap);
             const double a = std::sqrt(two * spec) * cst;
             c[(size_t)(i - 1)] = std::complex<double>(a * (double)cr, a * (double)ci);
+            if (p.ispec == 33) {
+                // build_coeff_3D.f90:44-58: a normally spread heading from the
+                // same deviate; the reference's InvErf returns -1 for a
+                // negative argument (ErfReal.f90:406-409), kept as it is
+                const double rad2deg = 180.0 / pi, fp = 1.0 / p.Tp;
+                const double sigma = 0.2 * std::pow(freq / fp, 2.5);
+                const double erf1 = std::erf(pi / (two * std::sqrt(two * sigma)));
+                const double arg = (two * psi - 1.0) * erf1;
+                const double erf2 = arg >= 0.0 ? inverse_erf(arg) : -1.0;
+                const double deg = p.beta0 + rad2deg * std::sqrt(2.0 * sigma) * erf2;
+                if (kcos.empty()) { kcos.assign((size_t)N / 2, 0.0); ksin.assign((size_t)N / 2, 0.0); }
+                kcos[(size_t)(i - 1)] = std::cos(pi / 180.0 * deg);
+                ksin[(size_t)(i - 1)] = std::sin(pi / 180.0 * deg);
+            }
         }
         // truncation at kh_max (random_wave_coefficients.f90:92-100): the
         // coefficients from index n_cut - 1 on are zero

@@ -112,7 +112,7 @@ def test_incident_wave_errors(ow3d, tmp_path):
         ow3d.incident_wave(p, 1)
     with pytest.raises(ow3d.OW3DError, match="no such relaxation zone"):
         ow3d.incident_wave(p, 5)
-    p.ispec = 33                                   # directional: not built
+    p.ispec = 2                                    # waves from a file: not built
     with pytest.raises(ow3d.OW3DError) as e:
         ow3d.incident_wave(p, 0)
     assert e.value.status == ow3d.capi.ERR_UNSUPPORTED
@@ -344,4 +344,38 @@ def test_spread_sea_cos2s(ow3d, tmp_path):
         dx, dy = x[i0 - 1 + ci] - p.x0, y[j0 - 1 + cj] - p.y0
         ce = np.conj(np.fft.fft(eta[:, cj, ci])[1:N // 2]) * 2 / N
         w = want * np.exp(1j * nu * (np.cos(bk) * dx + np.sin(bk) * dy))
+        assert np.max(np.abs(ce - w)) < 1e-6 * np.abs(want).max(), (ci, cj)
+
+
+def test_normally_spread_sea(ow3d, tmp_path):
+    """ispec 33 (build_coeff_3D.f90): each component's heading from its phase
+    deviate psi, beta = beta0 + sqrt(2 sigma) erf^-1((2 psi - 1) erf(pi /
+    (2 sqrt(2 sigma)))) with sigma = 0.2 (f / fp)^2.5, and -1 in place of the
+    inverse for psi < 1/2, which is what the reference's inverse returns
+    for a negative argument."""
+    import ctypes as C
+    from scipy.special import erf, erfinv
+    p = _heading_deck(tmp_path, "33 1.25 0.04 0.8 20. 4 -34 0. 0.5 run06.el 0 1.0 3.3", nsteps="1000")
+    eta, phis, (i0, i1, j0, j1) = ow3d.incident_wave(p, 0)
+    N = eta.shape[0]
+    draws = (C.c_float * (N // 2 - 1))()
+    ow3d.lib().ow3d_test_ran1(-34, N // 2 - 1, draws, None)
+    psi = np.frombuffer(draws, dtype=np.float32).astype(np.float64)
+    df = 1 / (N * p.dt)
+    k = np.arange(1, N // 2)
+    f = k * df
+    sigma = 0.2 * (f * p.Tp) ** 2.5
+    arg = (2 * psi - 1) * erf(np.pi / (2 * np.sqrt(2 * sigma)))
+    e2 = np.where(arg >= 0, erfinv(np.maximum(arg, 0)), -1.0)
+    beta = np.deg2rad(p.beta0 + np.rad2deg(np.sqrt(2 * sigma) * e2))
+    S = _jonswap(f, p.Hs, p.Tp, p.gamma_jonswap)
+    n_cut = int(np.floor(np.sqrt(p.g * p.kh_max / p.h0 * np.tanh(p.kh_max)) / (2 * np.pi * df) + 0.5)) + 1
+    ph = 2 * np.pi * psi
+    want = np.where(k < n_cut - 1, np.sqrt(2 * S * df) * (np.cos(ph).astype(np.float32) + 1j * np.sin(ph).astype(np.float32)), 0)
+    nu = _newton_k(2 * np.pi * f, p.h0, p.g)
+    x, y = _xy(p)
+    for (ci, cj) in ((0, 0), (6, 4)):
+        dx, dy = x[i0 - 1 + ci] - p.x0, y[j0 - 1 + cj] - p.y0
+        ce = np.conj(np.fft.fft(eta[:, cj, ci])[1:N // 2]) * 2 / N
+        w = want * np.exp(1j * nu * (np.cos(beta) * dx + np.sin(beta) * dy))
         assert np.max(np.abs(ce - w)) < 1e-6 * np.abs(want).max(), (ci, cj)
