@@ -8,6 +8,11 @@ No external dataset is involved: every input is generated here from a seed.
   shoal           3-D 35 m x 6 m basin, 0.45 m depth rising to 0.15 m over a
                   semi-elliptic shoal with a cos^2 taper, 257 x 33 x 9
   standing_2d     2-D flume with a cosine free surface (2-D x-sigma cases)
+  stream_function_2d
+                  2-D stream-function wave, kh = 1, H/L half the breaking
+                  limit, 64 points per wavelength, 9 sigma levels: the wave
+                  over the whole flume at t = 0 (the reference's IC 7),
+                  generated in the first wavelength, absorbed in the last
 """
 import numpy as np
 
@@ -123,3 +128,45 @@ def standing_2d(Nx=65, Nz=9, L=2 * np.pi, h0=1.0, amp=0.05, courant=0.5, **kw):
     x, _ = grid_xy(p)
     E0 = amp * np.cos(2 * np.pi * x / L)
     return p, dict(h=np.full(x.size, h0)), E0, np.zeros_like(E0)
+
+
+def breaking_steepness(kh):
+    """Limiting steepness H/L of a periodic wave at relative depth kh
+    (Miche's criterion, 0.142 tanh(kh))."""
+    return 0.142 * np.tanh(kh)
+
+
+def stream_function_2d(n_waves=8, ppw=64, Nz=9, kh=1.0, h0=1.0, steepness=0.5, courant=0.5, sponge_waves=3, **kw):
+    """The 2-D stream-function wave case: a flume of n_waves wavelengths
+    (L = 2 pi h0 / kh) with ppw points per wavelength, the wave of height
+    steepness x the breaking limit everywhere at t = 0 (IC 7 of the
+    reference), a generation zone over the first wavelength fed with the
+    exact wave at every RK stage time (relaxation target mode 1) and a sponge
+    over the last. Returns params, geometry, E0, P0 and the targets
+    {zone: (mode, nt, dt_sample, eta, phis)} for `steps` time steps."""
+    from . import stream_function_wave
+    L = 2 * np.pi * h0 / kh
+    Nx = n_waves * ppw + 1
+    steps = kw.pop("steps", 200)
+    p = default_params(Nx=Nx, Ny=1, Nz=Nz, Lx=n_waves * L, Ly=1.0, Lz=h0, GridZ=1,
+                       relaxONOFF=1, relaxNo=2, relaxTransientTime=0.0,
+                       zones=[dict(x1=0.0, x2=L, ftype=10, param=3.5, wavegen=1),
+                              dict(x1=(n_waves - sponge_waves) * L, x2=n_waves * L, ftype=9, param=3.5)], **kw)
+    p.IncWaveType = 1
+    p.g = G
+    p.sf_H, p.sf_h, p.sf_L = steepness * breaking_steepness(kh) * L, h0, L
+    p.sf_T, p.sf_wavel_or_per, p.sf_uEorS, p.sf_euler_or_stokes = 0.0, 0, 0.0, 0
+    p.sf_nsteps, p.sf_nmodes = 6, 24
+    _, _, (k, Lw, T, c) = stream_function_wave(p, np.zeros(1))
+    p.dt = courant * (L / ppw) / c
+    Nxg, Nyg, _ = dims(p)
+    x = (np.arange(Nxg) - 1) * (p.Lx / (Nx - 1))
+    E0, P0, _ = stream_function_wave(p, x, 0.0)
+    geo = dict(h=np.full(Nxg * Nyg, h0))
+    # zone 0 box: the first wavelength (1-based ghost-inclusive indices)
+    i0, i1 = 2, 2 + ppw
+    nt = 2 * steps + 2
+    tt = np.arange(nt) * (0.5 * p.dt)
+    eta = np.array([stream_function_wave(p, x[i0 - 1:i1], t)[0] for t in tt])
+    phis = np.array([stream_function_wave(p, x[i0 - 1:i1], t)[1] for t in tt])
+    return p, geo, E0, P0, {0: (1, nt, 0.5 * p.dt, eta, phis)}

@@ -5,7 +5,9 @@ benchmark configurations' own grids, a few time steps each:
   generation zone (0-3 m) and the sponge (30-35 m), FP64;
 * the 2-D x-sigma wave at 65 x 9 (one wavelength, kh = 1, steep), FP64;
 * a 129 x 33 x 17 sub-basin of the irregular sea (same dx, Nz and spectrum),
-  FP64 and mixed precision.
+  FP64 and mixed precision;
+* the 2-D stream-function wave (kh = 1, half the breaking steepness) in a
+  flume with stream-function generation and a sponge, 257 x 9, FP64.
 
 Tolerances as in test_gpu_parity: 1e-10 relative L-infinity on eta, P and phi
 for FP64 (reduction order and fused multiply-adds only), iteration totals
@@ -101,3 +103,21 @@ def test_irregular_sea_129x33x17(ow3d, oracle, precision):
     else:
         # FP32 preconditioner inside FP64 FGMRES: eta within 1e-6 of the FP64 oracle
         _compare(sim, orc, tol=1e-6)
+
+
+def test_stream_function_flume_2d(ow3d, oracle):
+    """The 2-D stream-function case (kh = 1, H/L half the breaking limit, 32
+    points per wavelength, 9 sigma levels) as the reference can run it: the
+    wave over the flume at t = 0, generated in the first wavelength from
+    targets at every RK stage time (mode 1), absorbed in the last three."""
+    W = ow3d.workloads
+    p, geo, E0, P0, targets = W.stream_function_2d(ppw=32, steps=12)
+    sim = ow3d.Simulation(p, **geo)
+    orc = oracle.Oracle(p, **geo, mode=oracle.MODE_DEVICE)
+    for s in (sim, orc):
+        s.set_state(E0, P0)
+        s.set_relax_target(0, *targets[0])
+    assert sim.step(12) >= 0
+    assert orc.step(12) >= 0
+    _compare(sim, orc)
+    _iterations_match(sim, orc)

@@ -110,3 +110,30 @@ def test_reference_stream_function_decks_solve(ow3d):
         assert np.all(np.isfinite(phis)) and abs(c - L / T) < 1e-12 * c, f.name
         solved += 1
     assert solved >= 3
+
+
+def test_flume_propagation_oracle(ow3d, oracle):
+    """The 2-D stream-function case (workloads.stream_function_2d: the wave
+    over the flume at t = 0, generated in the first wavelength with
+    relaxation targets of mode 1, absorbed in the last three) stepped one
+    period by the oracle: over the second to fourth wavelengths the
+    elevation stays within 3% of H of the exact translating wave, and inside
+    the generation zone within 0.5% (the exact wave is steady in its own
+    frame, so any other change is the flume's error)."""
+    W = ow3d.workloads
+    ppw = 32
+    steps = 2 * ppw                                    # Courant 0.5: one period
+    p, geo, E0, P0, targets = W.stream_function_2d(ppw=ppw, steps=steps)
+    orc = oracle.Oracle(p, **geo, mode=oracle.MODE_DEVICE)
+    assert orc.zone_box(0) == (2, 2 + ppw, 1, 1)
+    orc.set_state(E0, P0)
+    orc.set_relax_target(0, *targets[0])
+    assert orc.step(steps) >= 0
+    E, P, W_, phi, t = orc.get_state()
+    x = (np.arange(p.Nx + 2) - 1) * p.Lx / (p.Nx - 1)
+    Ee, Pe, (k, L, T, c) = ow3d.stream_function_wave(p, x, t)
+    assert abs(t - T) < 0.02 * T
+    mid = (x >= L) & (x <= 4 * L)
+    gen = (x >= 0) & (x <= 0.5 * L)
+    assert np.max(np.abs(E[mid] - Ee[mid])) < 0.03 * p.sf_H
+    assert np.max(np.abs(E[gen] - Ee[gen])) < 0.005 * p.sf_H
