@@ -154,6 +154,8 @@ typedef struct ow3d_params {
     int    sf_euler_or_stokes;        /* 0: Eulerian current, 1: Stokes drift */
     int    sf_nsteps;                 /* height steps of the solver */
     int    sf_nmodes;                 /* Fourier modes */
+    /* line 3 with Lz <= 0: the bathymetry file named after the ghost flags */
+    char   bathymetry_file[256];
 } ow3d_params;
 
 typedef struct ow3d_handle ow3d_handle;
@@ -271,6 +273,17 @@ int ow3d_put_surface(ow3d_handle* h, const double* E, const double* P);
 /* Read back E, P, W (Nxg*Nyg) and phi (Nzg*Nxg*Nyg); any pointer may be NULL. */
 int ow3d_get_state(ow3d_handle* h, double* E, double* P, double* W,
                    double* phi, double* t);
+
+/* The bathymetry file of a deck with Lz <= 0 (its name is p->bathymetry_file,
+ * relative to where the deck's run starts), as SetupInitialConditions.f90:51-111
+ * reads it: a header line, the gradient flag (0: each record holds h, h_x,
+ * h_xx, h_y, h_yy; 1: h only, the derivatives then taken with the 7-point x
+ * and y stencils as OceanWave3DT0Setup.f90:346-364 does), one record per
+ * interior point, x fastest. Outputs are Nxg*Nyg (ghosts take the values of
+ * the adjacent interior points), ready for ow3d_create; hx..hyy and flag may
+ * be NULL. The reference then sets Lz to h at the first point. Host-only. */
+int ow3d_read_bathymetry(const ow3d_params* p, const char* path, double* h, double* hx, double* hxx,
+                         double* hy, double* hyy, int* flag);
 
 /* The stream-function wave of the deck's line 8 (IncWaveType 1): Fenton's
  * Fourier solution as stream_func_set_up / stream_func_coeffs compute it

@@ -91,6 +91,21 @@ def _b(path):
     return str(path).encode()
 
 
+def read_bathymetry(params, path=None, deck_dir=None):
+    """The bathymetry file of a deck with Lz <= 0: a dict of h, hx, hxx, hy,
+    hyy (Nxg*Nyg, ghosts included) for Simulation, and the file's gradient
+    flag. path defaults to the deck's file name, taken relative to deck_dir."""
+    if path is None:
+        name = params.bathymetry_file.decode()
+        path = _pathlib.Path(deck_dir or ".") / name
+    Nxg, Nyg, _ = dims(params)
+    out = {k: _np.zeros(Nxg * Nyg) for k in ("h", "hx", "hxx", "hy", "hyy")}
+    flag = _C.c_int()
+    _check(lib().ow3d_read_bathymetry(_C.byref(params), str(path).encode(), *[_d(out[k]) for k in out],
+                                      _C.byref(flag)), "ow3d_read_bathymetry")
+    return out, flag.value
+
+
 def stream_function_wave(params, x, t=0.0):
     """The stream-function wave of the deck's line 8 at positions x and time t:
     eta, surface phi and (k, L, T, c)."""

@@ -66,6 +66,7 @@ class Params(C.Structure):
         ("sf_H", C.c_double), ("sf_h", C.c_double), ("sf_L", C.c_double), ("sf_T", C.c_double),
         ("sf_uEorS", C.c_double), ("sf_wavel_or_per", C.c_int), ("sf_euler_or_stokes", C.c_int),
         ("sf_nsteps", C.c_int), ("sf_nmodes", C.c_int),
+        ("bathymetry_file", C.c_char * 256),
     ]
 
 
@@ -177,6 +178,7 @@ def declare(lib):
         "ow3d_kinematics": (C.c_int, [H, _D, _D, _D, _D]),
         "ow3d_incident_wave": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _D, _D, _I]),
         "ow3d_stream_function_wave": (C.c_int, [C.c_void_p, C.c_int, _D, C.c_double, _D, _D, _D]),
+        "ow3d_read_bathymetry": (C.c_int, [C.c_void_p, C.c_char_p, _D, _D, _D, _D, _D, _I]),
         "ow3d_store_kinematics": (C.c_int, [H, C.c_char_p, _I]),
     }
     for name, (res, args) in sig.items():

@@ -863,6 +863,15 @@ int ow3d_read_deck(const char* path, ow3d_params* p) {
     return r;
 }
 
+int ow3d_read_bathymetry(const ow3d_params* p, const char* path, double* h, double* hx, double* hxx, double* hy,
+                         double* hyy, int* flag) {
+    if (!p) return OW3D_ERR_BAD_INPUT;
+    std::string err;
+    const int r = read_bathymetry(*p, path, h, hx, hxx, hy, hyy, flag, &err);
+    if (r) g_last_error = err;
+    return r;
+}
+
 int ow3d_stream_function_wave(const ow3d_params* p, int n, const double* x, double t, double* eta, double* phis,
                               double* info) {
     if (!p || n < 0 || (n > 0 && !x)) return OW3D_ERR_BAD_INPUT;

@@ -727,6 +727,7 @@ int default_params(ow3d_params* p) {
     p->gamma_jonswap = 3.3; p->beta0 = 0; p->s0 = 1.0;
     p->sf_H = p->sf_h = p->sf_L = p->sf_T = p->sf_uEorS = 0;
     p->sf_wavel_or_per = p->sf_euler_or_stokes = 0; p->sf_nsteps = 1; p->sf_nmodes = 0;
+    std::memset(p->bathymetry_file, 0, sizeof p->bathymetry_file);
     return OW3D_OK;
 }
 
@@ -796,6 +797,10 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
     p->GhostGridX = r.n(9); p->GhostGridY = r.n(10); p->GhostGridZ = r.n(11);
     if (p->Nx == 1) p->GhostGridX = 0;
     if (p->Ny == 1) p->GhostGridY = 0;
+    if (p->Lz <= 0.0) {   // the bathymetry comes from a file (ReadInputFileParameters.f90:61-69)
+        if (r.t.size() < 13) return fail("line 3: Lz <= 0 needs a bathymetry file name");
+        std::snprintf(p->bathymetry_file, sizeof p->bathymetry_file, "%s", r.t[12].c_str());
+    }
     r = next();  // alpha beta gamma alphaprecond betaprecond gammaprecond
     if (r.nnum() < 6) return fail("line 4: 6 stencil values expected");
     p->alpha = r.n(0); p->beta = r.n(1); p->gamma = r.n(2);
@@ -928,6 +933,78 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
         if (p->seed >= 0) p->seed = -p->seed;     // :632-647
         if (p->seed2 >= 0) p->seed2 = -p->seed2;
     }
+    return OW3D_OK;
+}
+
+// ------------------------------------------------------------- bathymetry
+// The bathymetry file of a deck with Lz <= 0 (SetupInitialConditions.f90:51-111,
+// OceanWave3DT0Setup.f90:346-364): a header line, the gradient flag, then one
+// record per interior point (x fastest) holding h (flag 1) or h, h_x, h_xx,
+// h_y, h_yy (flag 0). The ghost points take the values of the adjacent
+// interior points; with flag 1 the derivatives are the 7-point DiffXEven /
+// DiffYEven ones of the ghost-extended h. Outputs are Nxg*Nyg, ghosts included.
+int read_bathymetry(const ow3d_params& p, const char* path, double* h, double* hx, double* hxx, double* hy,
+                    double* hyy, int* flag_out, std::string* err) {
+    auto fail = [&](const std::string& m, int code) { if (err) *err = m; return code; };
+    if (!path || !h) return fail("read_bathymetry: bad arguments", OW3D_ERR_BAD_INPUT);
+    std::ifstream f(path);
+    if (!f) return fail(std::string("read_bathymetry: cannot open ") + path, OW3D_ERR_IO);
+    std::vector<std::string> lines;
+    std::string s;
+    while (std::getline(f, s)) lines.push_back(s);
+    size_t li = 1;   // line 0 is the header
+    auto next = [&]() -> Record {
+        while (li < lines.size() && lines[li].find_first_not_of(" \t\r") == std::string::npos) ++li;
+        return li < lines.size() ? split(lines[li++]) : Record();
+    };
+    Record r = next();
+    if (!r.num(0)) return fail("read_bathymetry: the gradient flag is missing", OW3D_ERR_BAD_INPUT);
+    const int flag = r.n(0);
+    if (flag != 0 && flag != 1) return fail("read_bathymetry: the gradient flag must be 0 or 1", OW3D_ERR_BAD_INPUT);
+    const int gx = p.Nx > 1 ? 1 : 0, gy = p.Ny > 1 ? 1 : 0;
+    const int Nxg = p.Nx + 2 * gx, Nyg = p.Ny + 2 * gy;
+    std::vector<double> F[5];
+    for (auto& v : F) v.assign((size_t)Nxg * Nyg, 0.0);
+    for (int j = 1 + gy; j <= p.Ny + gy; ++j)
+        for (int i = 1 + gx; i <= p.Nx + gx; ++i) {
+            Record q = next();
+            const size_t c = (size_t)(i - 1) + (size_t)Nxg * (j - 1);
+            const int need = flag == 1 ? 1 : 5;
+            if ((int)q.nnum() < need)
+                return fail("read_bathymetry: record for point (" + std::to_string(i - gx) + ", " + std::to_string(j - gy) +
+                                ") needs " + std::to_string(need) + " values",
+                            OW3D_ERR_BAD_INPUT);
+            for (int m = 0; m < need; ++m) F[m][c] = q.d(m);
+        }
+    auto at = [&](std::vector<double>& v, int i, int j) -> double& { return v[(size_t)(i - 1) + (size_t)Nxg * (j - 1)]; };
+    for (auto& v : F) {   // ghost extension (SetupInitialConditions.f90:89-108)
+        for (int j = 1; j <= Nyg; ++j) { at(v, 1, j) = at(v, 1 + gx, j); at(v, Nxg, j) = at(v, p.Nx + gx, j); }
+        for (int i = 1; i <= Nxg; ++i) { at(v, i, 1) = at(v, i, 1 + gy); at(v, i, Nyg) = at(v, i, p.Ny + gy); }
+    }
+    if (flag == 1) {
+        GridHost G;
+        std::vector<double> ones((size_t)Nxg * Nyg, 1.0), zeros(ones.size(), 0.0);
+        int rc = build_grid(p, ones.data(), zeros.data(), zeros.data(), zeros.data(), zeros.data(), G, err);
+        if (rc) return rc;
+        auto diff = [&](const Stencil& S, bool alongx, int order, std::vector<double>& out) {
+            const int n = alongx ? Nxg : Nyg;
+            for (int j = 1; j <= Nyg; ++j)
+                for (int i = 1; i <= Nxg; ++i) {
+                    const int pos = alongx ? i : j;
+                    const int ws = pos <= 3 ? 1 : (pos <= n - 3 ? pos - 3 : n - 6);
+                    double acc = 0.0;
+                    for (int m = 0; m < 7; ++m)
+                        acc += S.at(order, pos - 1, m) * (alongx ? at(F[0], ws + m, j) : at(F[0], i, ws + m));
+                    at(out, i, j) = acc;
+                }
+        };
+        if (p.Nx > 1) { diff(G.SX, true, 1, F[1]); diff(G.SX, true, 2, F[2]); }
+        if (p.Ny > 1) { diff(G.SY, false, 1, F[3]); diff(G.SY, false, 2, F[4]); }
+    }
+    double* out[5] = {h, hx, hxx, hy, hyy};
+    for (int m = 0; m < 5; ++m)
+        if (out[m]) std::copy(F[m].begin(), F[m].end(), out[m]);
+    if (flag_out) *flag_out = flag;
     return OW3D_OK;
 }
 

@@ -64,6 +64,8 @@ struct Ran1 {
     float next(int& idum);
 };
 int incident_wave_samples(const ow3d_params& p);
+int read_bathymetry(const ow3d_params& p, const char* path, double* h, double* hx, double* hxx, double* hy,
+                    double* hyy, int* flag_out, std::string* err);
 
 // Stream-function wave of the deck's line 8 (sfwave.cpp): the solution
 // vector z (1-based, 2N+10 unknowns), the elevation coefficients y (1..N),
