@@ -274,6 +274,18 @@ int ow3d_put_surface(ow3d_handle* h, const double* E, const double* P);
 int ow3d_get_state(ow3d_handle* h, double* E, double* P, double* W,
                    double* phi, double* t);
 
+/* Geometry and initial surface of the deck's IC where the reference builds
+ * them from formulas (SetupInitialConditions.f90): 0 (Lz > 0: flat, still
+ * water), 4 and 5 (flat deep / shallow water, a cosine surface), 7 (flat,
+ * the stream-function wave over the basin at time0 when relaxation is on,
+ * the non-generating zones' weights then applied three times as the
+ * reference does). h..hyy, E, P: Nxg*Nyg, ghosts included, for ow3d_create
+ * and ow3d_set_state (which takes the surface derivatives itself). Other ICs
+ * return OW3D_ERR_UNSUPPORTED (IC -1: ow3d_read_init_file; Lz <= 0:
+ * ow3d_read_bathymetry). hx..hyy may be NULL. Host-only. */
+int ow3d_initial_condition(const ow3d_params* p, double* h, double* hx, double* hxx, double* hy, double* hyy,
+                           double* E, double* P);
+
 /* The bathymetry file of a deck with Lz <= 0 (its name is p->bathymetry_file,
  * relative to where the deck's run starts), as SetupInitialConditions.f90:51-111
  * reads it: a header line, the gradient flag (0: each record holds h, h_x,

@@ -91,6 +91,17 @@ def _b(path):
     return str(path).encode()
 
 
+def initial_condition(params):
+    """Geometry dict (h, hx, hxx, hy, hyy) and initial E, P of the deck's IC
+    (0, 4, 5, 7; include/ow3d.h ow3d_initial_condition)."""
+    Nxg, Nyg, _ = dims(params)
+    geo = {k: _np.zeros(Nxg * Nyg) for k in ("h", "hx", "hxx", "hy", "hyy")}
+    E, P = _np.zeros(Nxg * Nyg), _np.zeros(Nxg * Nyg)
+    _check(lib().ow3d_initial_condition(_C.byref(params), *[_d(geo[k]) for k in geo], _d(E), _d(P)),
+           "ow3d_initial_condition")
+    return geo, E, P
+
+
 def read_bathymetry(params, path=None, deck_dir=None):
     """The bathymetry file of a deck with Lz <= 0: a dict of h, hx, hxx, hy,
     hyy (Nxg*Nyg, ghosts included) for Simulation, and the file's gradient

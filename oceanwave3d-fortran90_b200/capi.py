@@ -179,6 +179,7 @@ def declare(lib):
         "ow3d_incident_wave": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _D, _D, _I]),
         "ow3d_stream_function_wave": (C.c_int, [C.c_void_p, C.c_int, _D, C.c_double, _D, _D, _D]),
         "ow3d_read_bathymetry": (C.c_int, [C.c_void_p, C.c_char_p, _D, _D, _D, _D, _D, _I]),
+        "ow3d_initial_condition": (C.c_int, [C.c_void_p, _D, _D, _D, _D, _D, _D, _D]),
         "ow3d_store_kinematics": (C.c_int, [H, C.c_char_p, _I]),
     }
     for name, (res, args) in sig.items():

@@ -863,6 +863,15 @@ int ow3d_read_deck(const char* path, ow3d_params* p) {
     return r;
 }
 
+int ow3d_initial_condition(const ow3d_params* p, double* h, double* hx, double* hxx, double* hy, double* hyy,
+                           double* E, double* P) {
+    if (!p) return OW3D_ERR_BAD_INPUT;
+    std::string err;
+    const int r = initial_condition(*p, h, hx, hxx, hy, hyy, E, P, &err);
+    if (r) g_last_error = err;
+    return r;
+}
+
 int ow3d_read_bathymetry(const ow3d_params* p, const char* path, double* h, double* hx, double* hxx, double* hy,
                          double* hyy, int* flag) {
     if (!p) return OW3D_ERR_BAD_INPUT;

@@ -77,6 +77,8 @@ struct SFWave {
 };
 int stream_function_solve(const ow3d_params& p, SFWave& w, std::string* err);
 void stream_function_eval(const SFWave& w, int nx, const double* x, double t, double* eta, double* phis);
+int initial_condition(const ow3d_params& p, double* h, double* hx, double* hxx, double* hy, double* hyy, double* E,
+                      double* P, std::string* err);
 int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* phis, int* box, std::string* err);
 int read_deck(const char* path, ow3d_params* p, std::string* err);
 

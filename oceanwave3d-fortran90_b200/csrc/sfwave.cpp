@@ -245,4 +245,94 @@ void stream_function_eval(const SFWave& w, int nx, const double* x, double t, do
     }
 }
 
+// Initial geometry and surface of the deck's IC for the cases built from
+// formulas (SetupInitialConditions.f90): 0 (flat, depth Lz > 0, still water),
+// 4 and 5 (flat deep / shallow water with a cosine surface along x, or y in
+// a y-only basin), 7 (flat, depth of the stream-function wave, that wave over
+// the whole basin at t = time0 when relaxation is on, then the relaxation
+// weights of the non-generating zones applied three times). Outputs are
+// Nxg*Nyg, ghosts included.
+int initial_condition(const ow3d_params& p, double* h, double* hx, double* hxx, double* hy, double* hyy, double* E,
+                      double* P, std::string* err) {
+    auto fail = [&](const std::string& m, int code) { if (err) *err = m; return code; };
+    if (!h || !E || !P) return fail("initial_condition: h, E and P are required", OW3D_ERR_BAD_INPUT);
+    GridHost G;
+    const int Nxg = p.Nx + (p.Nx > 1 ? 2 : 0), Nyg = p.Ny + (p.Ny > 1 ? 2 : 0);
+    const size_t C = (size_t)Nxg * Nyg;
+    std::vector<double> ones(C, 1.0), zeros(C, 0.0);
+    int r = build_grid(p, ones.data(), zeros.data(), zeros.data(), zeros.data(), zeros.data(), G, err);
+    if (r) return r;
+    for (double* a : {hx, hxx, hy, hyy}) if (a) std::fill(a, a + C, 0.0);
+    std::fill(E, E + C, 0.0);
+    std::fill(P, P + C, 0.0);
+    const double pi = std::acos(-1.0), two = 2.0;
+    const bool alongx = p.Nx > 1;
+    auto coord = [&](size_t c) { return alongx ? G.x[c % (size_t)Nxg] : G.y[c / (size_t)Nxg]; };
+    switch (p.IC) {
+        case 0:   // :18-114 with Lz > 0 and no pressure forcing: still water
+            if (!(p.Lz > 0)) return fail("initial_condition: IC 0 with Lz <= 0 reads a bathymetry file", OW3D_ERR_UNSUPPORTED);
+            std::fill(h, h + C, p.Lz);
+            return OW3D_OK;
+        case 4:
+        case 5: {   // :183-234
+            const double L = alongx ? p.Lx : p.Ly;
+            const double kw = two * pi / L;
+            const double kh = p.IC == 4 ? two * pi : 0.5;
+            const double depth = kh / kw;
+            const double HH = p.IC == 4 ? L / 10.0 : depth * 0.75;
+            std::fill(h, h + C, depth);
+            for (size_t c = 0; c < C; ++c) E[c] = HH / two * std::cos(kw * coord(c));
+            return OW3D_OK;
+        }
+        case 7: {   // :303-385 (Cartesian grids)
+            std::fill(h, h + C, p.sf_h);
+            if (p.relaxONOFF != 1) return OW3D_OK;
+            SFWave w;
+            r = stream_function_solve(p, w, err);
+            if (r) return r;
+            const bool xdir = (p.relaxXorY == 'X' || p.relaxXorY == 'x');
+            const double rd = p.relaxDegrees / 180.0 * pi;
+            const int n1 = xdir ? Nxg : Nyg, n2 = xdir ? Nyg : Nxg;
+            std::vector<double> pos((size_t)n1), e((size_t)n1), f((size_t)n1);
+            for (int b = 0; b < n2; ++b) {
+                for (int a = 0; a < n1; ++a) {
+                    const double xa = xdir ? G.x[(size_t)a] : G.y[(size_t)a];
+                    const double yb = xdir ? G.y[(size_t)b] : G.x[(size_t)b];
+                    pos[(size_t)a] = rd == 0.0 ? xa : (xdir ? xa * std::cos(rd) + yb * std::sin(rd)
+                                                            : -xa * std::sin(rd) + yb * std::cos(rd));
+                }
+                if (rd == 0.0 && b > 0) {
+                    // the line is the same for every row
+                } else {
+                    stream_function_eval(w, n1, pos.data(), p.time0, e.data(), f.data());
+                }
+                for (int a = 0; a < n1; ++a) {
+                    const size_t c = xdir ? (size_t)a + (size_t)Nxg * b : (size_t)b + (size_t)Nxg * a;
+                    E[c] = e[(size_t)a];
+                    P[c] = f[(size_t)a];
+                }
+            }
+            // the relaxation three times (:364-366): generation zones relax
+            // towards the same wave (no change), the others damp
+            const std::vector<ZoneHost> Z = build_zones(p, G);
+            for (int pass = 0; pass < 3; ++pass)
+                for (const ZoneHost& z : Z) {
+                    if (z.wavegen) continue;
+                    for (int j = z.j0; j <= z.j1; ++j)
+                        for (int i = z.i0; i <= z.i1; ++i) {
+                            const double gm = z.xdir ? z.gam[(size_t)(i - z.i0)] : z.gam[(size_t)(j - z.j0)];
+                            const size_t c = (size_t)(i - 1) + (size_t)Nxg * (j - 1);
+                            E[c] *= gm;
+                            if (z.phion) P[c] *= gm;
+                        }
+                }
+            return OW3D_OK;
+        }
+        default:
+            return fail("initial_condition: IC " + std::to_string(p.IC) +
+                            " is not built (0, 4, 5 and 7 are; -1 reads OceanWave3D.init)",
+                        OW3D_ERR_UNSUPPORTED);
+    }
+}
+
 }  // namespace ow3d

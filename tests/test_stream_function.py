@@ -137,3 +137,43 @@ def test_flume_propagation_oracle(ow3d, oracle):
     gen = (x >= 0) & (x <= 0.5 * L)
     assert np.max(np.abs(E[mid] - Ee[mid])) < 0.03 * p.sf_H
     assert np.max(np.abs(E[gen] - Ee[gen])) < 0.005 * p.sf_H
+
+
+def test_initial_conditions(ow3d):
+    """ow3d_initial_condition for the ICs built from formulas
+    (SetupInitialConditions.f90): 4 and 5 (cosine surface on flat deep and
+    shallow water), 7 (the stream-function wave over the basin, the sponge's
+    weights applied three times), 0 (still water) and an unsupported one."""
+    W = ow3d.workloads
+    p = ow3d.default_params(Nx=33, Nz=9, Lx=4.0, Ly=1.0, Lz=1.0)
+    x = (np.arange(p.Nx + 2) - 1) * p.Lx / (p.Nx - 1)
+    for ic, kh, hh in ((4, 2 * np.pi, p.Lx / 10), (5, 0.5, None)):
+        p.IC = ic
+        geo, E, P = ow3d.initial_condition(p)
+        kw = 2 * np.pi / p.Lx
+        depth = kh / kw
+        H = hh if hh is not None else 0.75 * depth
+        assert np.allclose(geo["h"], depth, rtol=1e-15) and not geo["hx"].any()
+        assert np.allclose(E, H / 2 * np.cos(kw * x), rtol=0, atol=1e-15 * H) and not P.any()
+    p.IC = 0
+    geo, E, P = ow3d.initial_condition(p)
+    assert np.all(geo["h"] == 1.0) and not E.any() and not P.any()
+    p.IC = 2
+    with pytest.raises(ow3d.OW3DError) as e:
+        ow3d.initial_condition(p)
+    assert e.value.status == ow3d.capi.ERR_UNSUPPORTED
+    # IC 7 on the stream-function flume: the wave everywhere, damped in the sponge
+    q, geo_w, E0, P0, _ = W.stream_function_2d(ppw=32, steps=2)
+    q.IC = 7
+    geo, E, P = ow3d.initial_condition(q)
+    assert np.all(geo["h"] == q.sf_h)
+    xq = (np.arange(q.Nx + 2) - 1) * q.Lx / (q.Nx - 1)
+    Ee, Pe, _ = ow3d.stream_function_wave(q, xq, q.time0)
+    L = q.sf_L
+    free = xq < (8 - 3) * L
+    assert np.array_equal(E[free], Ee[free]) and np.array_equal(P[free], Pe[free])
+    sponge = xq > 5.5 * L
+    assert np.max(np.abs(E[sponge])) < np.max(np.abs(Ee[sponge]))
+    q.relaxONOFF = 0
+    geo, E, P = ow3d.initial_condition(q)
+    assert not E.any() and not P.any()                  # the reference sets the wave only with relaxation on
