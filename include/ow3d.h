@@ -276,7 +276,9 @@ int ow3d_get_state(ow3d_handle* h, double* E, double* P, double* W,
 
 /* Geometry and initial surface of the deck's IC where the reference builds
  * them from formulas (SetupInitialConditions.f90): 0 (Lz > 0: flat, still
- * water), 4 and 5 (flat deep / shallow water, a cosine surface), 7 (flat,
+ * water), 1 (deep-water nonlinear standing wave, nonlinearstandingwave1D.f90),
+ * 3 (the Whalin shoal, bottomWhalin.f90), 4 and 5 (flat deep / shallow water,
+ * a cosine surface), 7 (flat,
  * the stream-function wave over the basin at time0 when relaxation is on,
  * the non-generating zones' weights then applied three times as the
  * reference does). h..hyy, E, P: Nxg*Nyg, ghosts included, for ow3d_create

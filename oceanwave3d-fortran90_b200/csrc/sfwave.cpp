@@ -247,7 +247,8 @@ void stream_function_eval(const SFWave& w, int nx, const double* x, double t, do
 
 // Initial geometry and surface of the deck's IC for the cases built from
 // formulas (SetupInitialConditions.f90): 0 (flat, depth Lz > 0, still water),
-// 4 and 5 (flat deep / shallow water with a cosine surface along x, or y in
+// 1 (the deep-water standing wave of nonlinearstandingwave1D.f90), 3 (the
+// Whalin shoal of bottomWhalin.f90), 4 and 5 (flat deep / shallow water with a cosine surface along x, or y in
 // a y-only basin), 7 (flat, depth of the stream-function wave, that wave over
 // the whole basin at t = time0 when relaxation is on, then the relaxation
 // weights of the non-generating zones applied three times). Outputs are
@@ -273,6 +274,56 @@ int initial_condition(const ow3d_params& p, double* h, double* hx, double* hxx, 
             if (!(p.Lz > 0)) return fail("initial_condition: IC 0 with Lz <= 0 reads a bathymetry file", OW3D_ERR_UNSUPPORTED);
             std::fill(h, h + C, p.Lz);
             return OW3D_OK;
+        case 1: {   // :116-129, nonlinearstandingwave1D.f90: deep-water standing wave (Agnon and Glozman)
+            // the series' coefficients carry the reference's single-precision
+            // literals (0.5243 and 10.0**(-2) are REAL there)
+            std::fill(h, h + C, two);   // wavenumber pi, wavelength 2: L/h = 1, deep water
+            const float a[8] = {0.0f, 0.5243f, 0.4978f, 0.6542f, 0.1007f, 0.1653f, 0.2753f, 0.4522f};
+            const int e10[8] = {-1, -2, -3, -4, -4, -5, -6, -7};
+            double coef[8];
+            for (int n = 0; n < 8; ++n) {
+                float pw = 1.0f;
+                for (int q = 0; q < -e10[n]; ++q) pw *= 10.0f;
+                const float tenpow = 1.0f / pw;
+                coef[n] = n == 0 ? 0.8867 * (double)tenpow
+                                 : std::sqrt(std::sqrt((double)(n + 1))) * (double)a[n] * (double)tenpow;
+            }
+            for (size_t c = 0; c < C; ++c) {
+                const double X = coord(c);
+                double s = 0.0;
+                for (int n = 0; n < 8; ++n) s += coef[n] * std::cos((n + 1) * pi * X);
+                E[c] = 0.5 * s;
+            }
+            return OW3D_OK;
+        }
+        case 3: {   // :155-161, bottomWhalin.f90: the Whalin shoal (flat surface)
+            const bool xlong = p.Nx > p.Ny;
+            const double y0 = xlong ? (G.y.size() > 1 ? (G.y[1] - G.y[0]) / two : 0.0)
+                                    : (G.x.size() > 1 ? (G.x[1] - G.x[0]) / two : 0.0);
+            // the single-precision 10.67 and 18.29 of the x-long branch are kept
+            const double lo = xlong ? (double)10.67f : 10.67, hi = xlong ? (double)18.29f : 18.29;
+            for (int j = 1; j <= Nyg; ++j)
+                for (int i = 1; i <= Nxg; ++i) {
+                    const size_t c = (size_t)(i - 1) + (size_t)Nxg * (j - 1);
+                    double across = xlong ? G.y[(size_t)(j - 1)] : G.x[(size_t)(i - 1)];
+                    const double along = xlong ? G.x[(size_t)(i - 1)] : G.y[(size_t)(j - 1)];
+                    if (across < y0) across = y0;
+                    const double sg = std::sqrt(6.096 * across - across * across);
+                    const double sgd = -0.04 * (6.096 - two * across) * 0.5 / sg;
+                    const double sgdd = 0.04 * 6.096 * 6.096 / (4.0 * sg * sg * sg);
+                    double vh, valong = 0, vacross = 0, vaa = 0, vcc = 0;
+                    if (along <= lo - sg) vh = 0.4572;
+                    else if (along >= hi - sg) vh = 0.1524;
+                    else { vh = 0.4572 + 0.04 * (10.67 - sg - along); valong = -0.04; vacross = sgd; vcc = sgdd; }
+                    h[c] = vh;
+                    if (xlong) {
+                        if (hx) hx[c] = valong; if (hxx) hxx[c] = vaa; if (hy) hy[c] = vacross; if (hyy) hyy[c] = vcc;
+                    } else {
+                        if (hy) hy[c] = valong; if (hyy) hyy[c] = vaa; if (hx) hx[c] = vacross; if (hxx) hxx[c] = vcc;
+                    }
+                }
+            return OW3D_OK;
+        }
         case 4:
         case 5: {   // :183-234
             const double L = alongx ? p.Lx : p.Ly;
@@ -330,7 +381,7 @@ int initial_condition(const ow3d_params& p, double* h, double* hx, double* hxx, 
         }
         default:
             return fail("initial_condition: IC " + std::to_string(p.IC) +
-                            " is not built (0, 4, 5 and 7 are; -1 reads OceanWave3D.init)",
+                            " is not built (0, 1, 3, 4, 5 and 7 are; -1 reads OceanWave3D.init)",
                         OW3D_ERR_UNSUPPORTED);
     }
 }

@@ -177,3 +177,39 @@ def test_initial_conditions(ow3d):
     q.relaxONOFF = 0
     geo, E, P = ow3d.initial_condition(q)
     assert not E.any() and not P.any()                  # the reference sets the wave only with relaxation on
+
+
+def test_initial_conditions_standing_wave_and_whalin(ow3d):
+    """IC 1 (nonlinearstandingwave1D.f90: h = 2 and the eight-term series with
+    the reference's single-precision coefficients) and IC 3 (bottomWhalin.f90:
+    the shoal's depth and slopes; the x-long basin compares with the
+    single-precision 10.67 and 18.29)."""
+    p = ow3d.default_params(Nx=65, Nz=9, Lx=2.0, Ly=1.0, Lz=2.0)
+    p.IC = 1
+    geo, E, P = ow3d.initial_condition(p)
+    x = (np.arange(p.Nx + 2) - 1) * p.Lx / (p.Nx - 1)
+    a = [0.8867 * float(np.float32(0.1))] + [
+        np.sqrt(np.sqrt(n + 1)) * float(np.float32(c)) * float(np.float32(1) / np.float32(10.0 ** e))
+        for n, (c, e) in enumerate(zip([0.5243, 0.4978, 0.6542, 0.1007, 0.1653, 0.2753, 0.4522],
+                                       [2, 3, 4, 4, 5, 6, 7]), start=1)]
+    want = 0.5 * sum(a[n] * np.cos((n + 1) * np.pi * x) for n in range(8))
+    assert np.all(geo["h"] == 2.0) and np.max(np.abs(E - want)) < 1e-15 and not P.any()
+    q = ow3d.default_params(Nx=129, Ny=17, Nz=9, Lx=35.0, Ly=3.048, Lz=0.4572)   # the reference's Whalin basin (Nz 9)
+    q.IC = 3
+    geo, E, P = ow3d.initial_condition(q)
+    xg = (np.arange(q.Nx + 2) - 1) * q.Lx / (q.Nx - 1)
+    yg = (np.arange(q.Ny + 2) - 1) * q.Ly / (q.Ny - 1)
+    h = geo["h"].reshape(q.Ny + 2, q.Nx + 2)
+    hx = geo["hx"].reshape(q.Ny + 2, q.Nx + 2)
+    y0 = (yg[1] - yg[0]) / 2
+    for j in (1, 9, 18):
+        y = max(yg[j], y0)
+        s = np.sqrt(6.096 * y - y * y)
+        for i in range(q.Nx + 2):
+            if xg[i] <= float(np.float32(10.67)) - s:
+                assert h[j, i] == 0.4572 and hx[j, i] == 0.0
+            elif xg[i] >= float(np.float32(18.29)) - s:
+                assert h[j, i] == 0.1524
+            else:
+                assert abs(h[j, i] - (0.4572 + 0.04 * (10.67 - s - xg[i]))) < 1e-15 and hx[j, i] == -0.04
+    assert not E.any() and h.min() == 0.1524 and h.max() == 0.4572
