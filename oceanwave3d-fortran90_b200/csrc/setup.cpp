@@ -485,25 +485,12 @@ int incident_wave_samples(const ow3d_params& p) {
 //    phiS likewise with g/omega_k (-i) c_k.
 int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* phis, int* box, std::string* err) {
     auto fail = [&](const std::string& m, int code) { if (err) *err = m; return code; };
-    if (p.IncWaveType != 2) return fail("incident_wave: the deck's IncWaveType is not 2", OW3D_ERR_BAD_INPUT);
-    if (!(p.ispec == -1 || p.ispec == 0 || p.ispec == 1 || p.ispec == 3 || p.ispec == -30 || p.ispec == 30 ||
-          p.ispec == 31 || p.ispec == 33 || p.ispec == 34))
-        return fail("incident_wave: ispec " + std::to_string(p.ispec) +
-                        " (waves from a file) is not supported; -1, 0, 1, 3, -30, 30, 31, 33 and 34 are",
-                    OW3D_ERR_UNSUPPORTED);
     if (p.relaxONOFF != 1 || zone < 0 || zone >= p.relaxNo || zone >= OW3D_MAX_ZONES)
         return fail("incident_wave: no such relaxation zone", OW3D_ERR_BAD_INPUT);
     const ow3d_zone& d = p.zones[zone];
     if (!(d.XorYgen == 'X' || d.XorYgen == 'x') || d.WavegenONOFF != 1)
         return fail("incident_wave: zone " + std::to_string(zone) + " is not an x-directed generation zone",
                     OW3D_ERR_BAD_INPUT);
-    if (std::abs(p.ispec) >= 30 && d.degrees != 0.0)   // ReadInputFileParameters.f90:710-714
-        return fail("incident_wave: waves at a heading need a zone with degrees = 0", OW3D_ERR_BAD_INPUT);
-    const int nref = incident_wave_samples(p);
-    if (nt < 1 || !(p.Tp > 0) || !(p.h0 > 0) || !(p.dt > 0) || p.Nsteps < 1)
-        return fail("incident_wave: bad arguments", OW3D_ERR_BAD_INPUT);
-    if (p.ispec >= 0 && nt > nref)
-        return fail("incident_wave: a random wave has " + std::to_string(nref) + " samples", OW3D_ERR_BAD_INPUT);
     int r = check_params(p, err);
     if (r) return r;
     GridHost G;
@@ -513,8 +500,21 @@ int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* p
     if (r) return r;
     const std::vector<ZoneHost> Z = build_zones(p, G);
     const ZoneHost& z = Z[(size_t)zone];
+    const int nref = incident_wave_samples(p);
     if (box) { box[0] = z.i0; box[1] = z.i1; box[2] = z.j0; box[3] = z.j1; box[4] = nref; }
-    if (!eta && !phis) return OW3D_OK;
+    if (!eta && !phis) return OW3D_OK;   // the box query works for every deck
+    if (p.IncWaveType != 2) return fail("incident_wave: the deck's IncWaveType is not 2", OW3D_ERR_BAD_INPUT);
+    if (!(p.ispec == -1 || p.ispec == 0 || p.ispec == 1 || p.ispec == 3 || p.ispec == -30 || p.ispec == 30 ||
+          p.ispec == 31 || p.ispec == 33 || p.ispec == 34))
+        return fail("incident_wave: ispec " + std::to_string(p.ispec) +
+                        " (waves from a file) is not supported; -1, 0, 1, 3, -30, 30, 31, 33 and 34 are",
+                    OW3D_ERR_UNSUPPORTED);
+    if (std::abs(p.ispec) >= 30 && d.degrees != 0.0)   // ReadInputFileParameters.f90:710-714
+        return fail("incident_wave: waves at a heading need a zone with degrees = 0", OW3D_ERR_BAD_INPUT);
+    if (nt < 1 || !(p.Tp > 0) || !(p.h0 > 0) || !(p.dt > 0) || p.Nsteps < 1)
+        return fail("incident_wave: bad arguments", OW3D_ERR_BAD_INPUT);
+    if (p.ispec >= 0 && nt > nref)
+        return fail("incident_wave: a random wave has " + std::to_string(nref) + " samples", OW3D_ERR_BAD_INPUT);
     const double pi = std::acos(-1.0), two = 2.0, twopi = two * pi;
     const int bx = z.i1 - z.i0 + 1, by = z.j1 - z.j0 + 1;
     // long-crested along x (|ispec| < 30): one x line, repeated on the rows;
