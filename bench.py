@@ -323,6 +323,41 @@ def profile_step(args):
     sim.close()
 
 
+def largest_instance(args):
+    """The largest single instance, 2049 x 513 x 9 (flat 1 m, seeded JONSWAP
+    sea): FP64 and mixed precision at GMRES rtol 1e-6, 1e-8 and 1e-10, one
+    JSON line per tolerance with both precisions' DOF-timesteps/s, iterations
+    per solve and the mixed path's eta error against FP64. Timed like the
+    main line (device events around the steps, after warm-up steps)."""
+    import torch
+    pkg = package()
+    W = pkg.workloads
+    torch.cuda.set_device(0)
+    for rtol in (1e-6, 1e-8, 1e-10):
+        res, states = {}, {}
+        for prec in ("fp64", "mixed"):
+            p, geo, E0, P0 = W.irregular_sea(Nx=2049, Ny=513, Nz=9, precision=(1 if prec == "mixed" else 0),
+                                             reltol=rtol, seed=1234)
+            sim = pkg.Simulation(p, **geo)
+            sim.set_state(E0, P0)
+            sim.step(args.warmup)
+            sim.reset_stats()
+            torch.cuda.synchronize()
+            st, ms = sim.step_timed(args.steps)
+            s = sim.stats()
+            E, P, Wv, phi, t = sim.get_state()
+            states[prec] = E
+            res[prec] = dict(value=dof(p) * args.steps / (ms / 1e3), ms_per_step=ms / args.steps,
+                             iterations_per_solve=s["total_iterations"] / max(s["solves"], 1),
+                             not_converged=s["not_converged"])
+            sim.close()
+        err = float(np.max(np.abs(states["mixed"] - states["fp64"])) / np.max(np.abs(states["fp64"])))
+        print(json.dumps({"config": "largest instance 2049x513x9, flat 1 m, JONSWAP", "rtol": rtol,
+                          "unit": UNIT, "steps": args.steps, "warmup": args.warmup, "fp64": res["fp64"],
+                          "mixed": res["mixed"], "speedup_mixed_vs_fp64": res["mixed"]["value"] / res["fp64"]["value"],
+                          "eta_rel_err_mixed_vs_fp64": err}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -334,9 +369,14 @@ def main():
     ap.add_argument("--profile", choices=["fp64", "mixed"], default=None,
                     help="profiling driver: one warm-up step then one step of the workload, no JSON line")
     ap.add_argument("--grid", default=None, help="NXxNYxNZ override for --profile (e.g. 257x65x17)")
+    ap.add_argument("--config", choices=["sea", "largest"], default="sea",
+                    help="largest: the 2049x513x9 instance at three GMRES tolerances (one JSON line each)")
     args = ap.parse_args()
     if args.profile:
         profile_step(args)
+        return
+    if args.config == "largest":
+        largest_instance(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
