@@ -156,6 +156,13 @@ typedef struct ow3d_params {
     int    sf_nmodes;                 /* Fourier modes */
     /* line 3 with Lz <= 0: the bathymetry file named after the ghost flags */
     char   bathymetry_file[256];
+    /* deck features outside this library's path, kept so that ow3d_create
+     * can refuse a deck that needs them instead of running without them */
+    double accel_tol_fact;            /* line 2: local filtering by acceleration (1e30 when absent) */
+    int    i_breaking;                /* line 12: breaking model on */
+    int    PDampingONOFF;             /* pressure-damping zones on */
+    int    swenseONOFF;               /* SWENSE on */
+    int    curvilinearONOFF;          /* curvilinear grid on */
 } ow3d_params;
 
 typedef struct ow3d_handle ow3d_handle;

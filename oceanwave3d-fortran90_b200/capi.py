@@ -67,6 +67,8 @@ class Params(C.Structure):
         ("sf_uEorS", C.c_double), ("sf_wavel_or_per", C.c_int), ("sf_euler_or_stokes", C.c_int),
         ("sf_nsteps", C.c_int), ("sf_nmodes", C.c_int),
         ("bathymetry_file", C.c_char * 256),
+        ("accel_tol_fact", C.c_double), ("i_breaking", C.c_int), ("PDampingONOFF", C.c_int),
+        ("swenseONOFF", C.c_int), ("curvilinearONOFF", C.c_int),
     ]
 
 
@@ -105,6 +107,7 @@ def default_params(**kw):
     p.StoreDataONOFF = 0; p.formattype = 0
     p.ispec = -1; p.gamma_jonswap = 3.3; p.s0 = 1.0
     p.sf_nsteps = 1
+    p.accel_tol_fact = 1e30
     for k, v in kw.items():
         if k == "zones":
             for i, z in enumerate(v):

@@ -595,10 +595,11 @@ int check_dims(const ow3d_params* p) {
 int create_impl(const ow3d_params* p, const double* h, const double* hx, const double* hxx, const double* hy,
                 const double* hyy, ow3d_handle** out) {
     TRY(check_dims(p));
+    std::string err;
+    if (check_supported(*p, &err) != 0) { g_last_error = err; return OW3D_ERR_UNSUPPORTED; }
     std::unique_ptr<ow3d_handle> H(new ow3d_handle());
     H->p = *p;
     H->mixed = (p->precision == OW3D_PREC_MIXED);
-    std::string err;
     int r = build_grid(*p, h, hx, hxx, hy, hyy, H->G, &err);
     if (r) { g_last_error = err; return r; }
     H->dev = p->device;
@@ -937,6 +938,7 @@ int ow3d_estimate_bytes(const ow3d_params* p, size_t* bytes) {
     {
         std::string err;
         if (check_params(*p, &err) != 0) { g_last_error = err; return OW3D_ERR_BAD_INPUT; }
+        if (check_supported(*p, &err) != 0) { g_last_error = err; return OW3D_ERR_UNSUPPORTED; }
         if (p->GMRESmaxiterations < 2 || p->GMRESmaxiterations > kMaxKrylov) { g_last_error = "GMRESmaxiterations out of range"; return OW3D_ERR_BAD_INPUT; }
     }
     const int gx = p->Nx > 1 ? 1 : 0, gy = p->Ny > 1 ? 1 : 0;

@@ -139,6 +139,23 @@ static void level_colours(LevelHost& L) {
     L.ncolor = (L.Nxg > 1 && L.Nyg > 1 && m > 0) ? 4 : 2;
 }
 
+// Deck features that change the physics but lie outside this library's path:
+// a deck that turns one on is refused (OW3D_ERR_UNSUPPORTED) rather than run
+// without it. The acceleration limit of line 2 counts as on between 0 and
+// 10 g (accelerations of these flows stay far below 10 g; decks write 1000
+// to turn it off, and 0 is no limit).
+int check_supported(const ow3d_params& p, std::string* err) {
+    auto no = [&](const char* m) { if (err) *err = m; return OW3D_ERR_UNSUPPORTED; };
+    if (p.IncWaveType == 3) return no("IncWaveType 3 (flux wave generation at the boundary) is not built");
+    if (p.i_breaking != 0) return no("the breaking model (deck line 12) is not built");
+    if (p.accel_tol_fact > 0.0 && p.accel_tol_fact < 10.0)
+        return no("local filtering by the vertical acceleration (deck line 2) is not built");
+    if (p.PDampingONOFF != 0) return no("pressure-damping zones are not built");
+    if (p.swenseONOFF != 0) return no("SWENSE is not built");
+    if (p.curvilinearONOFF != 0 && p.Nx > 1 && p.Ny > 1) return no("curvilinear grids are not built");
+    return 0;
+}
+
 int check_params(const ow3d_params& p, std::string* err) {
     auto fail = [&](const char* m) { if (err) *err = m; return OW3D_ERR_BAD_INPUT; };
     if (p.Nx < 1 || p.Ny < 1 || p.Nz < 3) return fail("Nx, Ny >= 1 and Nz >= 3 required");
@@ -728,6 +745,7 @@ int default_params(ow3d_params* p) {
     p->sf_H = p->sf_h = p->sf_L = p->sf_T = p->sf_uEorS = 0;
     p->sf_wavel_or_per = p->sf_euler_or_stokes = 0; p->sf_nsteps = 1; p->sf_nmodes = 0;
     std::memset(p->bathymetry_file, 0, sizeof p->bathymetry_file);
+    p->accel_tol_fact = 1e30; p->i_breaking = 0; p->PDampingONOFF = 0; p->swenseONOFF = 0; p->curvilinearONOFF = 0;
     return OW3D_OK;
 }
 
@@ -789,6 +807,7 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
     p->IC = r.n(0);
     p->IncWaveType = r.num(1) ? r.n(1) : 0;
     if (p->IncWaveType == 4) p->IncWaveType = 1;
+    if (r.num(2)) p->accel_tol_fact = r.d(2);
     r = next();  // Lx Ly Lz Nx Ny Nz GridX GridY GridZ GhostGridX GhostGridY GhostGridZ
     if (r.nnum() < 12) return fail("line 3: 12 grid values expected");
     p->Lx = r.d(0); p->Ly = r.d(1); p->Lz = r.d(2);
@@ -872,7 +891,7 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
     p->filteringONOFF = r.n(0); p->filterALPHA = r.n(1); p->filterORDER = r.n(2);
     for (int q = 0; q < 3; ++q) p->sigma_filt[q] = r.num(3 + q) ? r.d(3 + q) : 0.0;
     r = next();  // optional breaking line (7 numbers), else the relaxation line
-    if (r.nnum() >= 7) r = next();
+    if (r.nnum() >= 7) { p->i_breaking = r.n(0); r = next(); }
     // relaxONOFF relaxTransientTime relaxNo relaxXorY relaxDegrees
     if (r.nnum() < 3) return fail("line 13: relaxation line expected");
     p->relaxONOFF = r.n(0); p->relaxTransientTime = r.d(1); p->relaxNo = r.n(2);
@@ -902,6 +921,7 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
             return true;
         };
         if (integer(0) && integer(1)) {
+            p->PDampingONOFF = q.n(0);
             if (q.n(0) != 0) for (int z = 0; z < q.n(1); ++z) next();   // pressure-damping zone lines
         } else {
             --li;   // not a pressure-damping line (the reference backspaces, :555-562)
@@ -909,10 +929,16 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
     }
     while (li < lines.size() && blank(li)) ++li;
     if (li >= lines.size()) return OW3D_OK;
-    next();  // SWENSE line
+    {
+        Record q = next();  // SWENSE line
+        if (q.num(0)) p->swenseONOFF = q.n(0);
+    }
     while (li < lines.size() && blank(li)) ++li;
     if (li >= lines.size()) return OW3D_OK;
-    next();  // curvilinearONOFF
+    {
+        Record q = next();  // curvilinearONOFF
+        if (q.num(0)) p->curvilinearONOFF = q.n(0);
+    }
     if (p->IncWaveType == 2) {
         Record q = next();
         if (q.nnum() < 1) return fail("incident-wave line expected for IncWaveType 2");

@@ -50,6 +50,9 @@ Stencil stencils_z(const std::vector<double>& z, int Nz, int gz, int g);
 // Returns 0 or an OW3D_ERR_* code with a message in *err.
 // Parameter checks that need no geometry (grid sizes, stencil widths, knobs).
 int check_params(const ow3d_params& p, std::string* err);
+// Deck features outside the path (breaking, pressure damping, SWENSE, ...):
+// 0, or OW3D_ERR_UNSUPPORTED with a message.
+int check_supported(const ow3d_params& p, std::string* err);
 
 int build_grid(const ow3d_params& p, const double* h, const double* hx, const double* hxx, const double* hy,
                const double* hyy, GridHost& G, std::string* err);

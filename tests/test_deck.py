@@ -138,3 +138,32 @@ def test_reference_example_decks_parse(ow3d):
                 want = [int(float(v)) for v in lines[i9 + 1 + q].replace(",", " ").split()[:9]]
                 assert list(p.kinematics[q]) == want, (f.name, q)
     assert parsed >= 0.8 * len(decks), (parsed, len(decks))
+
+
+def test_decks_needing_unbuilt_features_are_refused(ow3d, tmp_path):
+    """A deck that turns on a feature outside this library's path (breaking
+    model, pressure damping, SWENSE, flux wave generation, local filtering by
+    acceleration) is refused with OW3D_ERR_UNSUPPORTED by ow3d_create and
+    ow3d_estimate_bytes instead of running without it."""
+    import ctypes as C
+    L = ow3d.lib()
+    base = DECK_3D + "0 0\n0 2.0 2 0 0 1 0\n0\n"
+
+    def status(text):
+        p = ow3d.read_deck(write(tmp_path, "f.inp", text))
+        return L.ow3d_estimate_bytes(C.byref(p), C.byref(C.c_size_t())), p
+
+    st, p = status(base)
+    assert st == 0 and (p.PDampingONOFF, p.swenseONOFF, p.curvilinearONOFF, p.i_breaking) == (0, 0, 0, 0)
+    cases_ = {
+        "pressure": base.replace("0 0\n0 2.0 2", "1 1\n0. 5. 0. 10. 0.1 0.1 0\n0 2.0 2"),
+        "SWENSE": base.replace("0 2.0 2 0 0 1 0", "1 2.0 2 0 0 1 0"),
+        "breaking": base.replace("1 6 10 0.08 0.08 0.4", "1 6 10 0.08 0.08 0.4\n1 1.0 0.6 0.2 0.1 0.8 0.5"),
+        "IncWaveType 3": base.replace("-1 0  ", "-1 3  "),
+        "acceleration": base.replace("-1 0  ", "-1 0 0.5 "),
+    }
+    for what, text in cases_.items():
+        st, p = status(text)
+        assert st == ow3d.capi.ERR_UNSUPPORTED, (what, st)
+    msg = L.ow3d_last_error().decode()
+    assert "acceleration" in msg
