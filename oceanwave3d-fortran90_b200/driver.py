@@ -3,7 +3,7 @@
 for the parts this library builds.
 
     from ow3d_b200 import driver
-    result = driver.run("OceanWave3D.inp", outdir="out")
+    sim, setup, status = driver.run("OceanWave3D.inp", outdir="out")
 
 prepare() does the host set-up (no device): the deck, the geometry and
 initial state (a bathymetry file when Lz <= 0, the formula initial conditions,
@@ -122,7 +122,9 @@ def prepare(deck, deck_dir=None):
 def run(deck, outdir=None, steps=None, backend=Simulation, deck_dir=None):
     """prepare() then the time loop (OceanWave3D.f90:18-28): the deck's
     output schedule at step 0 and after each of the steps (Nsteps - 1 by
-    default). Returns the simulation and the setup."""
+    default). Returns the simulation (still open: close it when done), the
+    setup and the worst step status (1: some solve reached the matvec limit,
+    which the reference accepts silently)."""
     s = prepare(deck, deck_dir)
     p = s.params
     sim = backend(p, **s.geometry)
