@@ -4,7 +4,8 @@
 
 The reference has no Fortran compiler or SPARSKIT2/HSL libraries here and no
 stored outputs of its own, so these vectors come from the oracle (the CPU
-restatement of the reference algorithm). They pin the oracle and the CUDA path
+restatement of the reference algorithm), except host_*, which the library's
+own host set-up computes (incident waves), to keep those fixed across builds. They pin the oracle and the CUDA path
 against drift: test_golden.py re-runs the oracle on the same seeded inputs and
 the GPU parity tests compare the device against the same files.
 Each case is stored as <name>.npz; MANIFEST.txt lists their SHA-256.
@@ -59,9 +60,33 @@ def standing_case(oracle, mode, nonlinear):
     return dict(E0=E0, E=E, P=P, W=W, phi=phi, t=np.array([t]), iterations=np.array([s["total_iterations"]]))
 
 
+def host_setup_cases():
+    """Host set-up computed by the library itself (no device, no oracle): the
+    stream-function wave of the first configuration (kh = 1, half the
+    breaking steepness) and the first samples of a JONSWAP incident wave with
+    the reference's random phases, so that these stay fixed across builds."""
+    from conftest import load_package
+    ow3d = load_package()
+    out = {}
+    p = ow3d.default_params(Nx=65, Nz=9, Lx=2 * np.pi, Ly=1.0, Lz=1.0)
+    p.g = 9.81
+    p.sf_H, p.sf_h, p.sf_L = 0.5 * 0.142 * np.tanh(1.0) * 2 * np.pi, 1.0, 2 * np.pi
+    p.sf_wavel_or_per, p.sf_nsteps, p.sf_nmodes = 0, 6, 24
+    x = np.linspace(0.0, 2 * np.pi, 33)
+    eta, phis, info = ow3d.stream_function_wave(p, x, 0.25)
+    out["host_stream_function_kh1"] = dict(x=x, eta=eta, phis=phis, info=np.array(info))
+    q = ow3d.default_params(Nx=129, Ny=1, Nz=9, Lx=20.0, Ly=1.0, Lz=1.0, relaxONOFF=1, relaxNo=1,
+                            zones=[dict(x1=0.0, x2=4.0, ftype=10, param=3.5, wavegen=1)])
+    q.IncWaveType, q.ispec, q.Tp, q.Hs, q.h0, q.kh_max, q.seed, q.seed2 = 2, 1, 1.25, 0.04, 0.8, 20.0, -4, -34
+    q.Nsteps, q.dt, q.g = 256, 0.02, 9.81
+    e, f, box = ow3d.incident_wave(q, 0)
+    out["host_jonswap_zone"] = dict(eta=e[:64, 0, ::8], phis=f[:64, 0, ::8], box=np.array(box))
+    return out
+
+
 def generate():
     import oracle
-    out = {}
+    out = host_setup_cases()
     for name, (case, kw) in cases_table().items():
         for mode, tag in ((oracle.MODE_REFERENCE, "ref"), (oracle.MODE_DEVICE, "dev")):
             out[f"op_{name}_{tag}"] = operator_case(oracle, case, kw, mode)

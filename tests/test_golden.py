@@ -1,7 +1,8 @@
 """Golden vectors (tests/golden, made by make_golden.py from the oracle).
 
 CPU: the files are intact (MANIFEST.txt SHA-256) and the oracle still
-reproduces them. GPU: the CUDA path matches the device-ordered vectors
+reproduces them; the host set-up fixtures (host_*: the stream-function wave and
+a JONSWAP incident wave, computed by the library on the host) likewise. GPU: the CUDA path matches the device-ordered vectors
 (1e-10 relative on solves and time steps, 1e-12 on the operator).
 """
 import hashlib
