@@ -163,6 +163,12 @@ typedef struct ow3d_params {
     int    PDampingONOFF;             /* pressure-damping zones on */
     int    swenseONOFF;               /* SWENSE on */
     int    curvilinearONOFF;          /* curvilinear grid on */
+    /* the pressure-damping line and its zone (ReadInputFileParameters.f90:534-545;
+     * the reference runs one zone, PreprocessPDampingZones.f90) */
+    int    NDampZones;
+    int    pd_type;                   /* 0: damp the velocity through p_d (a 1-D solve over the zone), else phi */
+    double pd_x0, pd_x1, pd_y0, pd_y1;/* zone box BBox(1:4) */
+    double pd_g0Phi, pd_g0Eta;        /* strengths: gamma = 2 pi g0 exp(-((x - x1)/(x1 - x0))^2 / 0.125) */
 } ow3d_params;
 
 typedef struct ow3d_handle ow3d_handle;

@@ -16,6 +16,13 @@ int ow3d_test_level_dims(const ow3d_handle* h, int level, int* Nx, int* Ny, int*
 /* n deviates of the incident-wave generator (Park-Miller with the
  * Bays-Durham shuffle, RAN1_b.f90) started from idum, and the final idum. */
 int ow3d_test_ran1(int idum, int n, float* out, int* idum_out);
+/* The pressure-damping zone a 2-D deck sets up (host only, flat bottom):
+ * its first point i1 (1-based, ghosts included) and its nd points, gamma_phi
+ * and gamma_eta over the row (Nxg each), and for type 0 the zone matrix L
+ * (Dirichlet row, Laplacian rows, Neumann row; nd x nd, row-major) and the
+ * inverse the device applies. Arrays may be null. */
+int ow3d_test_pdamp_setup(const ow3d_params* p, int* i1, int* nd, double* gamPhi, double* gamEta, double* L,
+                          double* Linv);
 /* eta_x and eta_y of the current state as the device holds them (Nxg*Nyg
  * each; on the ghost rows they are the derivatives taken before that
  * direction's ghost update, as DifferentiationsFreeSurfacePlane leaves them). */

@@ -69,6 +69,9 @@ class Params(C.Structure):
         ("bathymetry_file", C.c_char * 256),
         ("accel_tol_fact", C.c_double), ("i_breaking", C.c_int), ("PDampingONOFF", C.c_int),
         ("swenseONOFF", C.c_int), ("curvilinearONOFF", C.c_int),
+        ("NDampZones", C.c_int), ("pd_type", C.c_int),
+        ("pd_x0", C.c_double), ("pd_x1", C.c_double), ("pd_y0", C.c_double), ("pd_y1", C.c_double),
+        ("pd_g0Phi", C.c_double), ("pd_g0Eta", C.c_double),
     ]
 
 

@@ -11,6 +11,7 @@
 //   k_rk_final     Runge_Kutta_4.f90:347-351
 //   k_filter_x/_y  FILTERING.f90:17-57
 //   k_extrap       Runge_Kutta_4.f90:118-121, 294-303
+//   k_pd_*         funPressureTerm.f90:218-311, the pressure-damping terms
 #include "ow3d_fs.h"
 
 namespace ow3d {
@@ -24,7 +25,8 @@ inline int nb(int64_t n, int t = 256) {
 
 __global__ void k_fs_stage(FsArgs a, const double* E, const double* P, const double* W, const double* Ex,
                            const double* Px, const double* Ey, const double* Py, const double* E0,
-                           const double* P0, double c, double* kE, double* kP, double* tE, double* tP) {
+                           const double* P0, double c, double* kE, double* kP, double* tE, double* tP,
+                           const double* NuD, const double* Pd) {
     const int64_t C = (int64_t)a.Nxg * a.Nyg;
     const double g = a.g, one = 1.0, half = 0.5;
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < C; p += (int64_t)gridDim.x * blockDim.x) {
@@ -39,12 +41,72 @@ __global__ void k_fs_stage(FsArgs a, const double* E, const double* P, const dou
             ke = -Ex[p] * Px[p] - Ey[p] * Py[p] + W[p] * (one + Ex[p] * Ex[p] + Ey[p] * Ey[p]);
             kp = -g * E[p] - half * (Px[p] * Px[p] + Py[p] * Py[p] - W[p] * W[p] * (one + Ex[p] * Ex[p] + Ey[p] * Ey[p]));
         }
+        if (NuD) { ke += NuD[p]; kp += Pd[p]; }   // rhsFreeSurface3D.f90:27-28
         if (a.three) {
             const int i = (int)(p % a.Nxg), j = (int)(p / a.Nxg);
             if ((i == 0 || i == a.Nxg - 1) && (j == 0 || j == a.Nyg - 1)) { ke = 0.0; kp = 0.0; }
         }
         kE[p] = ke; kP[p] = kp;
         if (tE) { tE[p] = E0[p] + c * ke; tP[p] = P0[p] + c * kp; }
+    }
+}
+
+// Type 0 (funPressureTerm.f90:238-284): the right-hand side of the zone
+// solve, d/dx(gamma_phi d/dx phi) with the Dirichlet row (phi at the first
+// point) and the Neumann row (zero), and NuD = -gamma_eta eta over the row.
+// One block: the second derivative pass reads the whole zone of the first.
+__global__ void k_pd_rhs(PDampDev d, int Nxg, const double* E, const double* P) {
+    const int nd = d.nd, R = d.rank, a = (R - 1) / 2;
+    const double* p0 = P + (d.i1 - 1);
+    for (int i = threadIdx.x; i < nd; i += blockDim.x) {
+        const int s = (i < a) ? 0 : (i >= nd - a ? nd - R : i - a);   // DfDx_1D_Uneven.f90:18-29
+        const double* w = d.D1 + (size_t)i * R;
+        double acc = 0.0;
+        for (int m = 0; m < R; ++m) acc += p0[s + m] * w[m];
+        d.f[i] = d.gamPhi[d.i1 - 1 + i] * acc;
+    }
+    for (int i = threadIdx.x; i < Nxg; i += blockDim.x) d.NuD[i] = -d.gamEta[i] * E[i];
+    __syncthreads();
+    for (int i = threadIdx.x; i < nd; i += blockDim.x) {
+        double v = 0.0;
+        if (i == 0) {
+            v = p0[0];
+        } else if (i < nd - 1) {
+            const int s = (i < a) ? 0 : (i >= nd - a ? nd - R : i - a);
+            const double* w = d.D1 + (size_t)i * R;
+            for (int m = 0; m < R; ++m) v += d.f[s + m] * w[m];
+        }
+        d.r[i] = v;
+    }
+}
+
+// x = L^-1 r, a warp per row.
+__global__ void k_pd_solve(PDampDev d) {
+    const int lane = threadIdx.x & 31;
+    const int nd = d.nd;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nd; i += nw) {
+        const double* row = d.Linv + (size_t)i * nd;
+        double acc = 0.0;
+        for (int k = lane; k < nd; k += 32) acc += row[k] * d.r[k];
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) d.x[i] = acc;
+    }
+}
+
+// Pd over the zone, zero at its first point (funPressureTerm.f90:286-291);
+// Pd stays zero outside the zone.
+__global__ void k_pd_apply(PDampDev d) {
+    const double x0 = d.x[0];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < d.nd; i += gridDim.x * blockDim.x)
+        d.Pd[d.i1 - 1 + i] = -(d.x[i] - x0);
+}
+
+// Other types (funPressureTerm.f90:299-310): friction on eta and phi.
+__global__ void k_pd_friction(PDampDev d, int64_t C, const double* E, const double* P) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < C; p += (int64_t)gridDim.x * blockDim.x) {
+        d.NuD[p] = -d.gamEta[p] * E[p];
+        d.Pd[p] = -d.gamPhi[p] * P[p];
     }
 }
 
@@ -277,9 +339,20 @@ __global__ void k_unstable(FsArgs a, const double* __restrict__ E, double hmax10
 
 void fs_stage(const FsArgs& a, const double* E, const double* P, const double* W, const double* Ex, const double* Px,
               const double* Ey, const double* Py, const double* E0, const double* P0, double c, double* kE,
-              double* kP, double* tE, double* tP, cudaStream_t st) {
+              double* kP, double* tE, double* tP, const double* NuD, const double* Pd, cudaStream_t st) {
     int64_t C = (int64_t)a.Nxg * a.Nyg;
-    note_launch(), k_fs_stage<<<nb(C), 256, 0, st>>>(a, E, P, W, Ex, Px, Ey, Py, E0, P0, c, kE, kP, tE, tP);
+    note_launch(), k_fs_stage<<<nb(C), 256, 0, st>>>(a, E, P, W, Ex, Px, Ey, Py, E0, P0, c, kE, kP, tE, tP, NuD, Pd);
+}
+void fs_pdamp(const FsArgs& a, const PDampDev& d, const double* E, const double* P, cudaStream_t st) {
+    const int64_t C = (int64_t)a.Nxg * a.Nyg;
+    if (d.type != 0) {
+        note_launch(), k_pd_friction<<<nb(C), 256, 0, st>>>(d, C, E, P);
+        return;
+    }
+    note_launch(), k_pd_rhs<<<1, 256, 0, st>>>(d, a.Nxg, E, P);
+    const int blocks = (int)((d.nd + 7) / 8 < 148 * 4 ? (d.nd + 7) / 8 : 148 * 4);   // 8 rows (warps) a block
+    note_launch(), k_pd_solve<<<blocks, 256, 0, st>>>(d);
+    note_launch(), k_pd_apply<<<nb(d.nd), 256, 0, st>>>(d);
 }
 void fs_rk_final(const FsArgs& a, double* E, double* P, double* const* kE, double* const* kP, double dt,
                  cudaStream_t st) {

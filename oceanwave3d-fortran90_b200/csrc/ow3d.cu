@@ -89,6 +89,10 @@ struct ow3d_handle {
     // relaxation and filtering
     std::vector<RelaxZoneDev> zones;
     double *fc = nullptr, *F2 = nullptr;
+    // pressure damping (2-D decks)
+    PDampHost pd_h;
+    PDampDev pd{};
+    bool pd_on = false;
     int* flag = nullptr;
     int* flag_host = nullptr;
     double hmax = 0;
@@ -665,6 +669,28 @@ int create_impl(const ow3d_params* p, const double* h, const double* hx, const d
         d.gam = g; d.tmode = 0; d.nt = 0; d.tdt = 1.0; d.eta = nullptr; d.phis = nullptr;
         H->zones.push_back(d);
     }
+    if (p->PDampingONOFF != 0) {
+        std::string e;
+        if (int r = build_pdamp(*p, G, H->pd_h, &e)) { g_last_error = "ow3d_create: " + e; return r; }
+        PDampDev& d = H->pd;
+        const PDampHost& ph = H->pd_h;
+        d.type = ph.type; d.i1 = ph.i1; d.nd = ph.nd; d.rank = ph.rank;
+        double *gp, *ge;
+        TRY(upload(H.get(), &gp, ph.gamPhi)); TRY(upload(H.get(), &ge, ph.gamEta));
+        d.gamPhi = gp; d.gamEta = ge;
+        if (d.type == 0) {
+            double *w, *li;
+            TRY(upload(H.get(), &w, ph.D1)); TRY(upload(H.get(), &li, ph.Linv));
+            d.D1 = w; d.Linv = li;
+            TRY(dalloc(H.get(), &d.f, (size_t)ph.nd)); TRY(dalloc(H.get(), &d.r, (size_t)ph.nd));
+            TRY(dalloc(H.get(), &d.x, (size_t)ph.nd));
+        }
+        TRY(dalloc(H.get(), &d.NuD, (size_t)G.C)); TRY(dalloc(H.get(), &d.Pd, (size_t)G.C));
+        CK(cudaMemset(d.NuD, 0, sizeof(double) * (size_t)G.C));
+        CK(cudaMemset(d.Pd, 0, sizeof(double) * (size_t)G.C));
+        H->pd_h.L.clear(); H->pd_h.L.shrink_to_fit(); H->pd_h.Linv.clear(); H->pd_h.Linv.shrink_to_fit();
+        H->pd_on = true;
+    }
     if (p->filteringONOFF > 0) {
         std::vector<double> fc, F2;
         filter_coeffs(*p, fc, F2);
@@ -733,8 +759,18 @@ int rk4_step(ow3d_handle* H) {
     auto surf = [&](const double* E, const double* Ex, const double* Exx, const double* Ey, const double* Eyy) {
         return nl ? Surface{E, Ex, Exx, Ey, Eyy} : Surface{nullptr, nullptr, nullptr, nullptr, nullptr};
     };
+    // funPressureTerm at each stage (Runge_Kutta_4.f90:50,159,239,334): the
+    // damping terms of the stage's state when its time is positive; at
+    // t <= 0 they keep their last values
+    const double* NuD = H->pd_on ? H->pd.NuD : nullptr;
+    const double* Pd = H->pd_on ? H->pd.Pd : nullptr;
+    auto pdamp = [&](const double* E, const double* P, double t) {
+        if (H->pd_on && t > 0) fs_pdamp(fa, H->pd, E, P, st);
+    };
     // stage 1
-    fs_stage(fa, H->E, H->P, H->W, H->Ex, H->Px, H->Ey, H->Py, H->E, H->P, half * dt, H->kE[0], H->kP[0], H->tE, H->tP, st);
+    pdamp(H->E, H->P, time);
+    fs_stage(fa, H->E, H->P, H->W, H->Ex, H->Px, H->Ey, H->Py, H->E, H->P, half * dt, H->kE[0], H->kP[0], H->tE, H->tP,
+             NuD, Pd, st);
     relax(H->tE, H->tP, time + half * dt);
     derivs(H->tE, H->tP, H->tEx, H->tExx, H->tPx, H->tEy, H->tEyy, H->tPy);
     fs_set_rhs(fa, H->tP, H->RHS, st);
@@ -742,14 +778,18 @@ int rk4_step(ow3d_handle* H) {
     TRY(solve(surf(H->tE, H->tEx, H->tExx, H->tEy, H->tEyy)));
     fs_wvel(fa, H->PHI, H->tE, H->tW, st);
     // stage 2
-    fs_stage(fa, H->tE, H->tP, H->tW, H->tEx, H->tPx, H->tEy, H->tPy, H->E, H->P, half * dt, H->kE[1], H->kP[1], H->tE, H->tP, st);
+    pdamp(H->tE, H->tP, time + half * dt);
+    fs_stage(fa, H->tE, H->tP, H->tW, H->tEx, H->tPx, H->tEy, H->tPy, H->E, H->P, half * dt, H->kE[1], H->kP[1], H->tE,
+             H->tP, NuD, Pd, st);
     relax(H->tE, H->tP, time + half * dt);
     derivs(H->tE, H->tP, H->tEx, H->tExx, H->tPx, H->tEy, H->tEyy, H->tPy);
     fs_set_rhs(fa, H->tP, H->RHS, st);
     TRY(solve(surf(H->tE, H->tEx, H->tExx, H->tEy, H->tEyy)));
     fs_wvel(fa, H->PHI, H->tE, H->tW, st);
     // stage 3
-    fs_stage(fa, H->tE, H->tP, H->tW, H->tEx, H->tPx, H->tEy, H->tPy, H->E, H->P, dt, H->kE[2], H->kP[2], H->tE, H->tP, st);
+    pdamp(H->tE, H->tP, time + half * dt);
+    fs_stage(fa, H->tE, H->tP, H->tW, H->tEx, H->tPx, H->tEy, H->tPy, H->E, H->P, dt, H->kE[2], H->kP[2], H->tE, H->tP,
+             NuD, Pd, st);
     relax(H->tE, H->tP, time + dt);
     derivs(H->tE, H->tP, H->tEx, H->tExx, H->tPx, H->tEy, H->tEyy, H->tPy);
     fs_set_rhs(fa, H->tP, H->RHS, st);
@@ -757,7 +797,9 @@ int rk4_step(ow3d_handle* H) {
     TRY(solve(surf(H->tE, H->tEx, H->tExx, H->tEy, H->tEyy)));
     fs_wvel(fa, H->PHI, H->tE, H->tW, st);
     // stage 4 and the new time level
-    fs_stage(fa, H->tE, H->tP, H->tW, H->tEx, H->tPx, H->tEy, H->tPy, nullptr, nullptr, 0.0, H->kE[3], H->kP[3], nullptr, nullptr, st);
+    pdamp(H->tE, H->tP, time + dt);
+    fs_stage(fa, H->tE, H->tP, H->tW, H->tEx, H->tPx, H->tEy, H->tPy, nullptr, nullptr, 0.0, H->kE[3], H->kP[3], nullptr,
+             nullptr, NuD, Pd, st);
     fs_rk_final(fa, H->E, H->P, H->kE, H->kP, dt, st);
     if (H->p.filteringONOFF > 0 && (tstep % H->p.filteringONOFF) == 0) {
         FilterDev f{H->p.filterALPHA, H->fc, H->F2};
@@ -948,6 +990,8 @@ int ow3d_estimate_bytes(const ow3d_params* p, size_t* bytes) {
     const int m = p->GMRESmaxiterations;
     double b = 8.0 * N * (m + 1) + s * N * m + 8.0 * N * 5 + 3.0 * s * N * 1.6 + 8.0 * C * 60 +
                s * (double)kDenseMaxPoints * (double)kDenseMaxPoints * 2.0;
+    // the inverse of a type-0 pressure-damping zone matrix: at most a row squared
+    if (p->PDampingONOFF != 0 && p->pd_type == 0) b += 8.0 * (double)(p->Nx + 2) * (double)(p->Nx + 2);
     *bytes = (size_t)(b * 1.05) + ((size_t)64 << 20);
     return OW3D_OK;
 }
@@ -1503,6 +1547,29 @@ int ow3d_test_surface_derivs(ow3d_handle* H, double* Ex, double* Ey) {
     if (Ex) CK(cudaMemcpyAsync(Ex, H->Ex, cb, cudaMemcpyDeviceToHost, H->st));
     if (Ey) CK(cudaMemcpyAsync(Ey, H->Ey, cb, cudaMemcpyDeviceToHost, H->st));
     CK(cudaStreamSynchronize(H->st));
+    return OW3D_OK;
+}
+
+int ow3d_test_pdamp_setup(const ow3d_params* p, int* i1, int* nd, double* gamPhi, double* gamEta, double* L,
+                          double* Linv) {
+    if (!p) return OW3D_ERR_BAD_INPUT;
+    std::string e;
+    if (check_supported(*p, &e)) { g_last_error = e; return OW3D_ERR_UNSUPPORTED; }
+    const size_t C = (size_t)(p->Nx + 2) * (size_t)(p->Ny > 1 ? p->Ny + 2 : 1);
+    const std::vector<double> one(C, 1.0), zero(C, 0.0);
+    GridHost G;
+    if (int r = build_grid(*p, one.data(), zero.data(), zero.data(), zero.data(), zero.data(), G, &e)) {
+        g_last_error = e;
+        return r;
+    }
+    PDampHost d;
+    if (int r = build_pdamp(*p, G, d, &e)) { g_last_error = e; return r; }
+    if (i1) *i1 = d.i1;
+    if (nd) *nd = d.nd;
+    if (gamPhi) std::copy(d.gamPhi.begin(), d.gamPhi.end(), gamPhi);
+    if (gamEta) std::copy(d.gamEta.begin(), d.gamEta.end(), gamEta);
+    if (L) std::copy(d.L.begin(), d.L.end(), L);
+    if (Linv) std::copy(d.Linv.begin(), d.Linv.end(), Linv);
     return OW3D_OK;
 }
 

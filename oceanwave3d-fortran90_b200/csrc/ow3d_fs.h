@@ -33,9 +33,23 @@ struct FilterDev {
     const double* F2;        // (2*alpha+1) x alpha boundary weights, column-major
 };
 
+// The pressure-damping zone of a 2-D deck (funPressureTerm.f90:218-311).
+struct PDampDev {
+    int type, i1, nd, rank;  // i1: 1-based first point of the zone, nd points
+    const double* gamPhi;    // Nxg
+    const double* gamEta;    // Nxg
+    const double* D1;        // nd x rank first-derivative weights (type 0)
+    const double* Linv;      // nd x nd inverse of the zone matrix, row-major (type 0)
+    double *f, *r, *x;       // nd each: gamma * phi_x, the zone right-hand side, its solution
+    double *NuD, *Pd;        // Nxg each: the kinematic and dynamic damping terms
+};
+
+// NuD and Pd of the state (E, P): the damping terms the next fs_stage adds.
+void fs_pdamp(const FsArgs& a, const PDampDev& d, const double* E, const double* P, cudaStream_t st);
+// NuD and Pd may be null (no pressure damping).
 void fs_stage(const FsArgs& a, const double* E, const double* P, const double* W, const double* Ex, const double* Px,
               const double* Ey, const double* Py, const double* E0, const double* P0, double c, double* kE,
-              double* kP, double* tE, double* tP, cudaStream_t st);
+              double* kP, double* tE, double* tP, const double* NuD, const double* Pd, cudaStream_t st);
 void fs_rk_final(const FsArgs& a, double* E, double* P, double* const* kE, double* const* kP, double dt,
                  cudaStream_t st);
 void fs_relax(const FsArgs& a, const RelaxZoneDev* zones, int nz, double* E, double* P, double RKtime, double time,

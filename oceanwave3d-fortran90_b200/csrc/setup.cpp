@@ -150,7 +150,12 @@ int check_supported(const ow3d_params& p, std::string* err) {
     if (p.i_breaking != 0) return no("the breaking model (deck line 12) is not built");
     if (p.accel_tol_fact > 0.0 && p.accel_tol_fact < 10.0)
         return no("local filtering by the vertical acceleration (deck line 2) is not built");
-    if (p.PDampingONOFF != 0) return no("pressure-damping zones are not built");
+    if (p.PDampingONOFF != 0) {
+        // BuildPDampMatrices.f90:37-40 stops for Ny > 1; the friction form
+        // (type != 0) spreads its gamma over y lines inconsistently there
+        if (p.Ny > 1 || p.Nx < 2) return no("pressure damping is built for x-directed zones of 2-D decks (Ny = 1)");
+        if (p.NDampZones != 1) return no("one pressure-damping zone per deck (the reference stops on more)");
+    }
     if (p.swenseONOFF != 0) return no("SWENSE is not built");
     if (p.curvilinearONOFF != 0 && p.Nx > 1 && p.Ny > 1) return no("curvilinear grids are not built");
     return 0;
@@ -310,6 +315,95 @@ static std::vector<double> gamma_fn(const double* x, int n, int dir, int ftype, 
     if (dir == -1) std::reverse(g.begin(), g.end());
     return g;
 }
+// ------------------------------------------------- pressure-damping zone
+// PreprocessPDampingZones.f90:24-70 and BuildPDampMatrices.f90:17-86 for the
+// one zone of a 2-D deck.
+int build_pdamp(const ow3d_params& p, const GridHost& G, PDampHost& d, std::string* err) {
+    d = PDampHost{};
+    if (p.PDampingONOFF == 0) return 0;
+    auto bad = [&](const char* m) { if (err) *err = m; return OW3D_ERR_BAD_INPUT; };
+    const int nx = (int)G.x.size();
+    const int i1 = trace_position(G.x, p.pd_x0), i2 = trace_position(G.x, p.pd_x1);
+    if (i2 < i1) return bad("pressure-damping zone: x1 < x0");
+    const int nd = i2 - i1 + 1;
+    d.type = p.pd_type; d.i1 = i1; d.nd = nd;
+    // Gaussian gamma (GammaFunctions.f90 type 12, parameter 0.25): 1 at the
+    // zone's last point
+    const std::vector<double> gt = gamma_fn(&G.x[(size_t)i1 - 1], nd, 1, 12, 0.25);
+    const double two_pi = 2.0 * M_PI;
+    d.gamPhi.assign((size_t)nx, 0.0); d.gamEta.assign((size_t)nx, 0.0);
+    for (int i = 0; i < nd; ++i) {
+        d.gamPhi[(size_t)i1 - 1 + i] = two_pi * p.pd_g0Phi * gt[(size_t)i];
+        d.gamEta[(size_t)i1 - 1 + i] = two_pi * p.pd_g0Eta * gt[(size_t)i];
+    }
+    if (d.type != 0) return 0;
+    const int a = p.alpha, rank = 2 * a + 1;
+    d.rank = rank;
+    if (nd < rank) return bad("pressure-damping zone: a type-0 zone needs at least 2*alpha+1 points");
+    // 1st and 2nd derivative weights on nd nodes: the reference takes the
+    // first nd nodes of the row, x(1:nd) (BuildPDampMatrices.f90:25), which
+    // on these uniform grids gives the weights of the zone's own nodes
+    const Stencil s = stencils_xy(std::vector<double>(G.x.begin(), G.x.begin() + nd), a);
+    auto w = [&](int order, int i, int m) { return s.w[((size_t)(order - 1) * nd + i) * rank + m]; };
+    d.D1.resize((size_t)nd * rank); d.start.resize((size_t)nd);
+    for (int i = 0; i < nd; ++i) {
+        d.start[(size_t)i] = (i < a) ? 0 : (i >= nd - a ? nd - rank : i - a);
+        for (int m = 0; m < rank; ++m) d.D1[(size_t)i * rank + m] = w(1, i, m);
+    }
+    // Dirichlet at the first point, the Laplacian inside, Neumann at the last
+    d.L.assign((size_t)nd * nd, 0.0);
+    d.L[0] = 1.0;
+    for (int r = 1; r < nd; ++r)
+        for (int m = 0; m < rank; ++m)
+            d.L[(size_t)r * nd + d.start[(size_t)r] + m] = (r == nd - 1) ? w(1, r, m) : w(2, r, m);
+    // its inverse: LU with partial pivoting confined to the band (kl below
+    // the diagonal, kl + ku above after row exchanges), then nd solves
+    int kl = 0, ku = 0;
+    for (int r = 1; r < nd; ++r) {
+        kl = std::max(kl, r - d.start[(size_t)r]);
+        ku = std::max(ku, d.start[(size_t)r] + rank - 1 - r);
+    }
+    const int ub = kl + ku;
+    std::vector<double> A = d.L;
+    std::vector<int> piv((size_t)nd);
+    for (int k = 0; k < nd; ++k) {
+        const int rmax = std::min(nd - 1, k + kl), cmax = std::min(nd - 1, k + ub);
+        int pr = k;
+        for (int r = k + 1; r <= rmax; ++r)
+            if (std::fabs(A[(size_t)r * nd + k]) > std::fabs(A[(size_t)pr * nd + k])) pr = r;
+        piv[(size_t)k] = pr;
+        if (A[(size_t)pr * nd + k] == 0.0) return bad("pressure-damping zone: the zone Laplacian is singular");
+        if (pr != k)
+            for (int c = k; c <= cmax; ++c) std::swap(A[(size_t)k * nd + c], A[(size_t)pr * nd + c]);
+        const double pv = A[(size_t)k * nd + k];
+        for (int r = k + 1; r <= rmax; ++r) {
+            const double f = A[(size_t)r * nd + k] / pv;
+            A[(size_t)r * nd + k] = f;
+            if (f != 0.0)
+                for (int c = k + 1; c <= cmax; ++c) A[(size_t)r * nd + c] -= f * A[(size_t)k * nd + c];
+        }
+    }
+    d.Linv.assign((size_t)nd * nd, 0.0);
+    std::vector<double> b((size_t)nd);
+    for (int col = 0; col < nd; ++col) {
+        std::fill(b.begin(), b.end(), 0.0);
+        b[(size_t)col] = 1.0;
+        for (int k = 0; k < nd; ++k) {
+            std::swap(b[(size_t)k], b[(size_t)piv[(size_t)k]]);
+            const double bk = b[(size_t)k];
+            if (bk != 0.0)
+                for (int r = k + 1; r <= std::min(nd - 1, k + kl); ++r) b[(size_t)r] -= A[(size_t)r * nd + k] * bk;
+        }
+        for (int k = nd - 1; k >= 0; --k) {
+            double acc = b[(size_t)k];
+            for (int c = k + 1; c <= std::min(nd - 1, k + ub); ++c) acc -= A[(size_t)k * nd + c] * b[(size_t)c];
+            b[(size_t)k] = acc / A[(size_t)k * nd + k];
+        }
+        for (int r = 0; r < nd; ++r) d.Linv[(size_t)r * nd + col] = b[(size_t)r];
+    }
+    return 0;
+}
+
 std::vector<ZoneHost> build_zones(const ow3d_params& p, const GridHost& G) {
     std::vector<ZoneHost> out;
     if (p.relaxONOFF != 1) return out;
@@ -922,7 +1016,18 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
         };
         if (integer(0) && integer(1)) {
             p->PDampingONOFF = q.n(0);
-            if (q.n(0) != 0) for (int z = 0; z < q.n(1); ++z) next();   // pressure-damping zone lines
+            p->NDampZones = q.n(1);
+            // the zone lines x0 x1 y0 y1 g0Phi g0Eta type (:539-545); the
+            // first is kept (the reference runs one zone)
+            if (q.n(0) != 0)
+                for (int z = 0; z < q.n(1); ++z) {
+                    Record r = next();
+                    if (r.nnum() < 7) { if (err) *err = "pressure-damping zone line: 7 numbers expected"; return OW3D_ERR_BAD_INPUT; }
+                    if (z == 0) {
+                        p->pd_x0 = r.d(0); p->pd_x1 = r.d(1); p->pd_y0 = r.d(2); p->pd_y1 = r.d(3);
+                        p->pd_g0Phi = r.d(4); p->pd_g0Eta = r.d(5); p->pd_type = r.n(6);
+                    }
+                }
         } else {
             --li;   // not a pressure-damping line (the reference backspaces, :555-562)
         }

@@ -57,6 +57,22 @@ int check_supported(const ow3d_params& p, std::string* err);
 int build_grid(const ow3d_params& p, const double* h, const double* hx, const double* hxx, const double* hy,
                const double* hyy, GridHost& G, std::string* err);
 std::vector<ZoneHost> build_zones(const ow3d_params& p, const GridHost& G);
+
+// The pressure-damping zone of a 2-D deck (PreprocessPDampingZones.f90:24-70,
+// BuildPDampMatrices.f90:17-86). gamPhi and gamEta span the Nxg points of
+// the row; type 0 adds the first-derivative weights over the zone's nd
+// points (DfDx_1D_Uneven: 2a+1 weights per point from node start[i]) and
+// the zone's Dirichlet-Laplacian-Neumann matrix L (nd x nd, row-major) with
+// its inverse, which the device applies in place of the reference's sparse
+// LU solve.
+struct PDampHost {
+    int type = 0, i1 = 0, nd = 0, rank = 0;   // i1: 1-based first point of the zone
+    std::vector<double> gamPhi, gamEta;
+    std::vector<double> D1;                  // nd x rank
+    std::vector<int> start;                  // nd
+    std::vector<double> L, Linv;             // nd x nd
+};
+int build_pdamp(const ow3d_params& p, const GridHost& G, PDampHost& d, std::string* err);
 void filter_coeffs(const ow3d_params& p, std::vector<double>& fc, std::vector<double>& F2);
 
 int default_params(ow3d_params* p);

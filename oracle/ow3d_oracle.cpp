@@ -66,6 +66,11 @@ struct Sim {
     vector<double> dsig;                 // 5*N, dsigmanew(k,i,j,1..5) for the current stage
     double time = 0; int64_t tstep = 0;
     vector<Zone> zones;
+    // pressure damping (PreprocessPDampingZones.f90, BuildPDampMatrices.f90)
+    int pd_i1 = 0, pd_nd = 0;
+    vector<double> gamPhi, gamEta, NuD, Pd;
+    Stencil1D pdGrad;                    // BuildStencil_1D_Uneven over x(1:nd)
+    vector<double> pdLU; vector<int> pdPiv;
     vector<double> fc, fc2;              // filter: centre (NP) and boundary view (NP*alpha)
     int NP = 0;
     // stats
@@ -1010,6 +1015,7 @@ static void fs_rhs(const Sim& s, const vector<double>& E, const vector<double>& 
             kP[c] = -g * E[c] - half * (Px[c] * Px[c] + Py[c] * Py[c] - W[c] * W[c] * (one + Ex[c] * Ex[c] + Ey[c] * Ey[c]));
         }
     }
+    for (int c = 0; c < s.C; ++c) { kE[c] += s.NuD[c]; kP[c] += s.Pd[c]; }   // rhsFreeSurface3D.f90:27-28
     if (s.gx + s.gy == 2) {  // Zero_Corners.f90
         int Nx = s.Nxg, Ny = s.Nyg;
         size_t cs4[4] = {0, (size_t)Nx - 1, (size_t)Nx * (Ny - 1), (size_t)Nx * Ny - 1};
@@ -1166,6 +1172,93 @@ static int trace(const vector<double>& x, double x0) {
     for (size_t i = 0; i < x.size(); ++i) if (x0 <= x[i]) return (int)i + 1;
     return (int)x.size();
 }
+// PreprocessPDampingZones.f90:24-70 and BuildPDampMatrices.f90:17-86 (one
+// x-directed zone, 2-D).
+static void setup_pdamp(Sim& s) {
+    s.NuD.assign(s.C, 0.0); s.Pd.assign(s.C, 0.0);
+    if (s.p.PDampingONOFF == 0) return;
+    const int nx = s.Nxg;
+    int i1 = trace(s.fine.x, s.p.pd_x0), i2 = trace(s.fine.x, s.p.pd_x1), nd = i2 - i1 + 1;
+    s.pd_i1 = i1; s.pd_nd = nd;
+    vector<double> gt = gamma_fn(&s.fine.x[i1 - 1], nd, 1, 12, 0.25);
+    s.gamPhi.assign(nx, 0.0); s.gamEta.assign(nx, 0.0);
+    for (int i = 1; i <= nd; ++i) {
+        s.gamPhi[i1 + i - 2] = 2.0 * M_PI * s.p.pd_g0Phi * gt[i - 1];
+        s.gamEta[i1 + i - 2] = 2.0 * M_PI * s.p.pd_g0Eta * gt[i - 1];
+    }
+    if (s.p.pd_type != 0) return;
+    const int a = s.p.alpha, rank = 2 * a + 1;
+    s.pdGrad = orc::build_stencils_xy(vector<double>(s.fine.x.begin(), s.fine.x.begin() + nd), a);
+    const Stencil1D& G = s.pdGrad;
+    vector<double>& A = s.pdLU;
+    A.assign((size_t)nd * nd, 0.0);
+    auto put = [&](int i, int col, double v) { A[(size_t)(i - 1) * nd + (col - 1)] = v; };   // 1-based
+    put(1, 1, 1.0);
+    for (int i = 2; i <= a; ++i)
+        for (int m = 1; m <= rank; ++m) put(i, m, G.at(2, i - 1, m - 1));
+    for (int i = a + 1; i <= nd - a; ++i)
+        for (int m = 1; m <= rank; ++m) put(i, i - a - 1 + m, G.at(2, i - 1, m - 1));
+    for (int i = nd - a + 1; i <= nd - 1; ++i)
+        for (int m = 1; m <= rank; ++m) put(i, nd - rank + m, G.at(2, i - 1, m - 1));
+    for (int m = 1; m <= rank; ++m) put(nd, nd - rank + m, G.at(1, nd - 1, m - 1));
+    // dense LU with partial pivoting in place of the reference's MA41
+    s.pdPiv.assign(nd, 0);
+    for (int k = 0; k < nd; ++k) {
+        int pr = k;
+        for (int r = k + 1; r < nd; ++r) if (std::fabs(A[(size_t)r * nd + k]) > std::fabs(A[(size_t)pr * nd + k])) pr = r;
+        s.pdPiv[k] = pr;
+        if (pr != k) for (int c = 0; c < nd; ++c) std::swap(A[(size_t)k * nd + c], A[(size_t)pr * nd + c]);
+        for (int r = k + 1; r < nd; ++r) {
+            double f = A[(size_t)r * nd + k] / A[(size_t)k * nd + k];
+            A[(size_t)r * nd + k] = f;
+            if (f != 0.0) for (int c = k + 1; c < nd; ++c) A[(size_t)r * nd + c] -= f * A[(size_t)k * nd + c];
+        }
+    }
+}
+// DfDx_1D_Uneven.f90:17-29
+static void pd_dfdx(const Sim& s, const vector<double>& f, vector<double>& fx) {
+    const int nd = s.pd_nd, a = s.p.alpha, rank = 2 * a + 1;
+    for (int i = 1; i <= nd; ++i) {
+        int lo = (i <= a) ? 1 : (i <= nd - a ? i - a : nd - rank + 1);
+        double acc = 0.0;
+        for (int m = 1; m <= rank; ++m) acc += f[lo + m - 2] * s.pdGrad.at(1, i - 1, m - 1);
+        fx[i - 1] = acc;
+    }
+}
+// funPressureTerm.f90:218-311: NuD and Pd of the state (E, P) at time t > 0;
+// they keep their values otherwise.
+static void pressure_term(Sim& s, const vector<double>& E, const vector<double>& P, double t) {
+    if (s.p.PDampingONOFF == 0 || !(t > 0)) return;
+    const int nx = s.Nxg;
+    if (s.p.pd_type == 0) {
+        const int nd = s.pd_nd, id0 = s.pd_i1;
+        vector<double> tmp(nd), rhs(nd);
+        for (int i = 1; i <= nd; ++i) tmp[i - 1] = P[id0 + i - 2];
+        pd_dfdx(s, tmp, rhs);
+        for (int i = 1; i <= nd; ++i) tmp[i - 1] = s.gamPhi[id0 + i - 2] * (rhs[i - 1] - 0.0);   // no current
+        pd_dfdx(s, tmp, rhs);
+        rhs[0] = P[id0 - 1]; rhs[nd - 1] = 0.0;
+        const double* A = s.pdLU.data();
+        for (int k = 0; k < nd; ++k) if (s.pdPiv[k] != k) std::swap(rhs[k], rhs[s.pdPiv[k]]);
+        for (int r = 0; r < nd; ++r) { double v = rhs[r]; for (int c = 0; c < r; ++c) v -= A[(size_t)r * nd + c] * rhs[c]; rhs[r] = v; }
+        for (int r = nd - 1; r >= 0; --r) {
+            double v = rhs[r];
+            for (int c = r + 1; c < nd; ++c) v -= A[(size_t)r * nd + c] * rhs[c];
+            rhs[r] = v / A[(size_t)r * nd + r];
+        }
+        for (int i = 1; i <= nx; ++i) s.NuD[i - 1] = -s.gamEta[i - 1] * E[i - 1];
+        std::fill(s.Pd.begin(), s.Pd.end(), 0.0);
+        for (int i = 1; i <= nd; ++i) s.Pd[id0 + i - 2] = -(rhs[i - 1] - rhs[0]);
+    } else {
+        for (int j = 1; j <= s.Nyg; ++j)
+            for (int i = 1; i <= nx; ++i) {
+                size_t k = (size_t)(j - 1) * nx + (i - 1);
+                s.NuD[k] = -s.gamEta[k] * E[k];
+                s.Pd[k] = -s.gamPhi[k] * P[k];
+            }
+    }
+}
+
 static void setup_zones(Sim& s) {
     s.zones.clear();
     if (s.p.relaxONOFF != 1) return;
@@ -1212,6 +1305,7 @@ static int rk4_step(Sim& s) {
     };
     auto zero_src = [&]() { std::fill(s.sPx.begin(), s.sPx.end(), 0.0); };
     // stage 1
+    pressure_term(s, s.E, s.P, time);
     fs_rhs(s, s.E, s.P, s.W, s.Ex, s.Px, s.Ey, s.Py, k1E, k1P);
     for (size_t c = 0; c < C; ++c) { s.tE[c] = s.E[c] + half * dt * k1E[c]; s.tP[c] = s.P[c] + half * dt * k1P[c]; }
     double RKtime = time + half * dt;
@@ -1225,6 +1319,7 @@ static int rk4_step(Sim& s) {
     do_solve();
     vertical_velocity(s, s.tW);
     // stage 2
+    pressure_term(s, s.tE, s.tP, RKtime);
     fs_rhs(s, s.tE, s.tP, s.tW, s.tEx, s.tPx, s.tEy, s.tPy, k2E, k2P);
     for (size_t c = 0; c < C; ++c) { s.tE[c] = s.E[c] + half * dt * k2E[c]; s.tP[c] = s.P[c] + half * dt * k2P[c]; }
     RKtime = time + half * dt;
@@ -1235,6 +1330,7 @@ static int rk4_step(Sim& s) {
     do_solve();
     vertical_velocity(s, s.tW);
     // stage 3
+    pressure_term(s, s.tE, s.tP, RKtime);
     fs_rhs(s, s.tE, s.tP, s.tW, s.tEx, s.tPx, s.tEy, s.tPy, k3E, k3P);
     for (size_t c = 0; c < C; ++c) { s.tE[c] = s.E[c] + dt * k3E[c]; s.tP[c] = s.P[c] + dt * k3P[c]; }
     RKtime = time + dt;
@@ -1248,6 +1344,7 @@ static int rk4_step(Sim& s) {
     do_solve();
     vertical_velocity(s, s.tW);
     // stage 4
+    pressure_term(s, s.tE, s.tP, RKtime);
     fs_rhs(s, s.tE, s.tP, s.tW, s.tEx, s.tPx, s.tEy, s.tPy, k4E, k4P);
     const double six = 6.0, two = 2.0;
     for (size_t c = 0; c < C; ++c) {
@@ -1302,6 +1399,7 @@ static Sim* create(const ow3d_params* p, const double* h, const double* hx, cons
     update_sigma(*s, nullptr, nullptr, nullptr, nullptr, nullptr);
     if (p->filteringONOFF > 0) filter_init(*s);
     setup_zones(*s);
+    setup_pdamp(*s);
     s->time = p->time0;
     return s.release();
 }

@@ -142,8 +142,8 @@ def test_reference_example_decks_parse(ow3d):
 
 def test_decks_needing_unbuilt_features_are_refused(ow3d, tmp_path):
     """A deck that turns on a feature outside this library's path (breaking
-    model, pressure damping, SWENSE, flux wave generation, local filtering by
-    acceleration) is refused with OW3D_ERR_UNSUPPORTED by ow3d_create and
+    model, pressure damping in 3-D, SWENSE, flux wave generation, local
+    filtering by acceleration) is refused with OW3D_ERR_UNSUPPORTED by ow3d_create and
     ow3d_estimate_bytes instead of running without it."""
     import ctypes as C
     L = ow3d.lib()

@@ -77,11 +77,12 @@ REF = pathlib.Path(os.environ.get("OW3D_REFERENCE_DECKS", "/root/reference/examp
 
 @pytest.mark.skipif(not REF.is_dir(), reason="reference example decks not on this machine")
 @pytest.mark.parametrize("name", ["LinearTravellingWave", "RandomWave2D", "NLStanding", "RandomWave2DShoaling",
-                                  "ObliqueRegular1Beach"])
+                                  "ObliqueRegular1Beach", "StreamFuncWave"])
 def test_reference_decks_run_on_oracle(ow3d, oracle, name):
     """The reference's own example decks set up and step (two steps on the
     oracle) with bounded surfaces: incident waves of several kinds, a
-    formula IC, a bathymetry file, directional generation zones."""
+    formula IC, a bathymetry file, directional generation zones, pressure
+    damping."""
     from ow3d_b200 import driver
     sim, s, st = driver.run(REF / f"OceanWave3D.inp.{name}", steps=2, backend=_oracle_backend(oracle))
     E = sim.get_state()[0]
