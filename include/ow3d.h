@@ -158,7 +158,7 @@ typedef struct ow3d_params {
     char   bathymetry_file[256];
     /* deck features outside this library's path, kept so that ow3d_create
      * can refuse a deck that needs them instead of running without them */
-    double accel_tol_fact;            /* line 2: local filtering by acceleration (1e30 when absent) */
+    double accel_tol_fact;            /* line 2: local filtering by acceleration, on for (0, 100] (1e30 when absent) */
     int    i_breaking;                /* line 12: breaking model on */
     int    PDampingONOFF;             /* pressure-damping zones on */
     int    swenseONOFF;               /* SWENSE on */

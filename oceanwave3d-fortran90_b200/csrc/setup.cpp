@@ -141,14 +141,14 @@ static void level_colours(LevelHost& L) {
 
 // Deck features that change the physics but lie outside this library's path:
 // a deck that turns one on is refused (OW3D_ERR_UNSUPPORTED) rather than run
-// without it. The acceleration limit of line 2 counts as on between 0 and
-// 10 g (accelerations of these flows stay far below 10 g; decks write 1000
-// to turn it off, and 0 is no limit).
+// without it. The acceleration limit of line 2 turns the filter on up to
+// 100 g (LocalSmoothing2D.f90:37; decks write 1000 to turn it off); 0, the
+// value of a zero-initialised ow3d_params, counts as off.
 int check_supported(const ow3d_params& p, std::string* err) {
     auto no = [&](const char* m) { if (err) *err = m; return OW3D_ERR_UNSUPPORTED; };
     if (p.IncWaveType == 3) return no("IncWaveType 3 (flux wave generation at the boundary) is not built");
     if (p.i_breaking != 0) return no("the breaking model (deck line 12) is not built");
-    if (p.accel_tol_fact > 0.0 && p.accel_tol_fact < 10.0)
+    if (p.accel_tol_fact > 0.0 && p.accel_tol_fact <= 100.0)
         return no("local filtering by the vertical acceleration (deck line 2) is not built");
     if (p.PDampingONOFF != 0) {
         // BuildPDampMatrices.f90:37-40 stops for Ny > 1; the friction form

@@ -161,6 +161,7 @@ def test_decks_needing_unbuilt_features_are_refused(ow3d, tmp_path):
         "breaking": base.replace("1 6 10 0.08 0.08 0.4", "1 6 10 0.08 0.08 0.4\n1 1.0 0.6 0.2 0.1 0.8 0.5"),
         "IncWaveType 3": base.replace("-1 0  ", "-1 3  "),
         "acceleration": base.replace("-1 0  ", "-1 0 0.5 "),
+        "acceleration, 100 g": base.replace("-1 0  ", "-1 0 100. "),
     }
     for what, text in cases_.items():
         st, p = status(text)
