@@ -48,6 +48,16 @@ def test_struct_layouts_match(ow3d):
     assert L.ow3d_test_sizeof(99) == -1
 
 
+def test_fortran_binding_size(ow3d):
+    """The Fortran side of the binding holds ow3d_params as an opaque byte
+    array whose length must be the struct's size."""
+    import re
+    from conftest import ROOT
+    text = (ROOT / "INTEGRATION.md").read_text()
+    sizes = [int(n) for n in re.findall(r"raw\((\d+)\)\s+! opaque to Fortran: sizeof\(ow3d_params\)", text)]
+    assert sizes == [C.sizeof(ow3d.capi.Params)]
+
+
 def test_default_params_match_mirror(ow3d):
     L = ow3d.lib()
     q = ow3d.capi.Params()
