@@ -9,7 +9,8 @@ prepare() does the host set-up (no device): the deck, the geometry and
 initial state (a bathymetry file when Lz <= 0, the formula initial conditions,
 a hot start from OceanWave3D.init for IC -1) and the relaxation-zone targets of
 the incident wave (IncWaveType 1: the stream-function wave at every RK stage
-time; 2: the reference's linear or random wave series). run() creates the
+time; 2: the reference's linear or random wave series). A pressure-damping
+zone needs no host step: ow3d_create sets it up from the deck. run() creates the
 simulation, applies the output schedule of the deck at step 0 and after every
 step (EP / ASCII files, OceanWave3D.end, Kinematics files) and takes the
 Nsteps - 1 steps of the reference's time loop. run() takes any backend with
@@ -116,6 +117,10 @@ def prepare(deck, deck_dir=None):
                 phis = np.array([np.tile(f, rows) for _, f in line])
                 targets[z] = (1, nt, 0.5 * p.dt, eta, phis)
                 notes.append(f"zone {z}: stream-function wave at every RK stage time")
+    if p.PDampingONOFF:
+        # set up on the device by ow3d_create (PreprocessPDampingZones.f90)
+        notes.append(f"pressure-damping zone x = {p.pd_x0:g} .. {p.pd_x1:g}, type {p.pd_type}, "
+                     f"g0 {p.pd_g0Phi:g} (phi) {p.pd_g0Eta:g} (eta)")
     return Setup(p, geometry, E0, P0, targets, notes)
 
 
