@@ -82,7 +82,8 @@ typedef struct ow3d_zone {
  * restricted to the fields the hot path reads, plus build-only knobs. */
 typedef struct ow3d_params {
     /* line 2 */
-    int    IC, IncWaveType;
+    int    IC, IncWaveType;       /* as the deck writes it: 4 and 5 (a wave with a
+                                     constant-flux current) are refused by ow3d_create */
     /* line 3 */
     double Lx, Ly, Lz;
     int    Nx, Ny, Nz;
@@ -169,6 +170,17 @@ typedef struct ow3d_params {
     int    pd_type;                   /* 0: damp the velocity through p_d (a 1-D solve over the zone), else phi */
     double pd_x0, pd_x1, pd_y0, pd_y1;/* zone box BBox(1:4) */
     double pd_g0Phi, pd_g0Eta;        /* strengths: gamma = 2 pi g0 exp(-((x - x1)/(x1 - x0))^2 / 0.125) */
+    /* 1 when ow3d_read_deck read accel_tol_fact from line 2: the reference
+     * then smooths locally for every value up to 100 g, 0 and negative values
+     * included (LocalSmoothing2D.f90:37); 0 for parameters built by a caller,
+     * where accel_tol_fact = 0 means no local smoothing */
+    int    accel_from_deck;
+    /* build-only knob, no counterpart in the reference (whose lateral rows
+     * are walls, BuildLinearSystem.f90:149-216): 1 = periodic in x. The Nx
+     * points span one period including both ends, x_1 = 0 and x_Nx = Lx,
+     * which hold the same value; the Nx - 1 distinct columns are coupled
+     * cyclically in every stencil, the ghost columns are unused. */
+    int    periodic_x;
 } ow3d_params;
 
 typedef struct ow3d_handle ow3d_handle;
@@ -255,11 +267,12 @@ int ow3d_matvec(ow3d_handle* h, const double* phi, double* y,
  * memory of the handle's device (d_Ey, d_Eyy may be NULL in 2-D; the surface
  * is ignored for a linear run). The call allocates nothing: its only scratch
  * is a fixed file-scope device array (1024 partial sums) whose address is
- * looked up once per device on the first call -- make one call before
- * capturing the handle's stream into a graph. Vectors longer than 2^31-1
- * elements are rejected with OW3D_ERR_UNSUPPORTED. Calls that overlap in time
- * on one device share that scratch and must be serialised by the caller.
- * Runs on the handle's stream and returns after the norm is on the host. */
+ * looked up once per device on the first call on that device; that first
+ * call should come before any stream capture begins. Vectors longer than
+ * 2^31-1 elements are rejected with OW3D_ERR_UNSUPPORTED. Calls that overlap
+ * in time on one device share that scratch and must be serialised by the
+ * caller. Runs on the handle's stream and synchronises it: it returns after
+ * the norm is on the host. */
 int ow3d_residual_device_noalloc(ow3d_handle* h, const double* d_rhs, const double* d_phi,
                                  const double* d_E, const double* d_Ex, const double* d_Exx,
                                  const double* d_Ey, const double* d_Eyy,

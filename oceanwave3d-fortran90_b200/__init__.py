@@ -3,8 +3,8 @@ the RK4 free-surface update, as CUDA kernels for sm_100a behind the C ABI of
 include/ow3d.h.
 
 This module is the Python host side of that ABI (the reference's driver is
-Fortran; a Fortran host binds the same symbols through iso_c_binding, see
-INTEGRATION.md). It mirrors the reference's split into a set-up call
+Fortran; a Fortran host binds the same symbols through the iso_c_binding
+module include/ow3d_iface.f90). It mirrors the reference's split into a set-up call
 (OceanWave3DT0Setup) and a time-step call (OceanWave3DTakeATimeStep) and
 exposes the drop-in Laplace solve (iterative_solution).
 

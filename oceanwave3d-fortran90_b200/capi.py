@@ -72,6 +72,7 @@ class Params(C.Structure):
         ("NDampZones", C.c_int), ("pd_type", C.c_int),
         ("pd_x0", C.c_double), ("pd_x1", C.c_double), ("pd_y0", C.c_double), ("pd_y1", C.c_double),
         ("pd_g0Phi", C.c_double), ("pd_g0Eta", C.c_double),
+        ("accel_from_deck", C.c_int), ("periodic_x", C.c_int),
     ]
 
 

@@ -14,10 +14,11 @@
 //                 resets it,
 //   g_na_result   the reduced value read back by the host.
 // Their addresses are looked up with cudaGetSymbolAddress once per device, on
-// the first call made on that device, so a caller that later captures its
-// stream into a CUDA graph should make one call before capturing. Two calls
-// that overlap in time on one device (different streams or host threads)
-// share this scratch and race; callers serialise them.
+// the first call made on that device: that first call should come before any
+// stream capture begins. Every call reads its result back to the host and
+// synchronises the handle's stream before it returns. Two calls that overlap
+// in time on one device (different streams or host threads) share this
+// scratch and race; callers serialise them.
 #include "ow3d_internal.h"
 
 #include <mutex>

@@ -141,15 +141,21 @@ static void level_colours(LevelHost& L) {
 
 // Deck features that change the physics but lie outside this library's path:
 // a deck that turns one on is refused (OW3D_ERR_UNSUPPORTED) rather than run
-// without it. The acceleration limit of line 2 turns the filter on up to
-// 100 g (LocalSmoothing2D.f90:37; decks write 1000 to turn it off); 0, the
-// value of a zero-initialised ow3d_params, counts as off.
+// without it. The acceleration limit of line 2 turns the filter on for every
+// value up to 100 g (LocalSmoothing2D.f90:37; decks write 1000 to turn it
+// off); for parameters that did not come from a deck, 0, the value of a
+// zero-initialised ow3d_params, counts as off. IncWaveType 4 and 5 add a
+// constant-flux current to the wave (ReadInputFileParameters.f90:42-49),
+// which enters the right-hand side and the lateral Neumann rows.
 int check_supported(const ow3d_params& p, std::string* err) {
     auto no = [&](const char* m) { if (err) *err = m; return OW3D_ERR_UNSUPPORTED; };
     if (p.IncWaveType == 3) return no("IncWaveType 3 (flux wave generation at the boundary) is not built");
+    if (p.IncWaveType == 4 || p.IncWaveType == 5)
+        return no("IncWaveType 4 and 5 (a wave with a constant-flux current) are not built");
     if (p.i_breaking != 0) return no("the breaking model (deck line 12) is not built");
-    if (p.accel_tol_fact > 0.0 && p.accel_tol_fact <= 100.0)
-        return no("local filtering by the vertical acceleration (deck line 2) is not built");
+    const bool smoothing = p.accel_from_deck ? p.accel_tol_fact <= 100.0
+                                             : (p.accel_tol_fact > 0.0 && p.accel_tol_fact <= 100.0);
+    if (smoothing) return no("local filtering by the vertical acceleration (deck line 2) is not built");
     if (p.PDampingONOFF != 0) {
         // BuildPDampMatrices.f90:37-40 stops for Ny > 1; the friction form
         // (type != 0) spreads its gamma over y lines inconsistently there
@@ -184,6 +190,7 @@ int check_params(const ow3d_params& p, std::string* err) {
     if (p.precision != OW3D_PREC_FP64 && p.precision != OW3D_PREC_MIXED) return fail("precision must be 0 or 1");
     if (p.krylov != OW3D_KRYLOV_FGMRES && p.krylov != OW3D_KRYLOV_LGMRES) return fail("krylov must be 0 or 1");
     if (p.GMRESmaxiterations < 1) return fail("GMRESmaxiterations must be >= 1");
+    if (p.periodic_x != 0) return fail("periodic_x: the periodic lateral boundary is not built");
     return 0;
 }
 
@@ -899,9 +906,8 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
     Record r = next();  // IC [IncWaveType [accel_tol_fact]]
     if (!r.num(0)) return fail("line 2: IC expected");
     p->IC = r.n(0);
-    p->IncWaveType = r.num(1) ? r.n(1) : 0;
-    if (p->IncWaveType == 4) p->IncWaveType = 1;
-    if (r.num(2)) p->accel_tol_fact = r.d(2);
+    p->IncWaveType = r.num(1) ? r.n(1) : 0;   // 4 and 5 kept as written: ow3d_create refuses them
+    if (r.num(2)) { p->accel_tol_fact = r.d(2); p->accel_from_deck = 1; }
     r = next();  // Lx Ly Lz Nx Ny Nz GridX GridY GridZ GhostGridX GhostGridY GhostGridZ
     if (r.nnum() < 12) return fail("line 3: 12 grid values expected");
     p->Lx = r.d(0); p->Ly = r.d(1); p->Lz = r.d(2);

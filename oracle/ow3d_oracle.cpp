@@ -430,6 +430,9 @@ static void dm_pass(const Level& Lv, int colour, double* x, const double* b) {
         for (int k = k0; k <= k1; ++k) gs_row(Lv.A, (k - 1) + Nzg * ((i - 1) + Nxg * (j - 1)), x, b);
     };
     const int j0 = three ? 2 : 1, j1 = three ? Nyg - 1 : 1;
+    // the tasks of one colour read nothing another task of the colour writes,
+    // so rows of tasks run in parallel with the same result as in sequence
+#pragma omp parallel for schedule(static) if (three)
     for (int j = j0; j <= j1; ++j)
         for (int i = 2; i <= Nxg - 1; ++i) {
             const int col = (Lv.ncolor == 4) ? ((i & 1) + 2 * (j & 1)) : ((i + j) & 1);
@@ -486,7 +489,9 @@ static void restrict_(const Sim& s, const Level& Fl, const Level& Cl, const doub
     vector<double> t(rf, rf + (size_t)F.Nxg * F.Nyg * F.Nzg);
     auto I = [&](int k, int i, int j) -> size_t { return (size_t)(k - 1) + (size_t)F.Nzg * ((size_t)(i - 1) + (size_t)F.Nxg * (j - 1)); };
     const double half = 0.5, one = 1.0;
+    // each sweep writes the points of one parity from the other parity only
     if (xc) {
+#pragma omp parallel for schedule(static)
         for (int ifn = 1 + s.gx; ifn <= Nxf + s.gx; ifn += 2) {
             double dW = F.x[ifn - 1] - F.x[ifn - 2], dE = F.x[ifn] - F.x[ifn - 1];
             double dxc = one / (dW + dE);
@@ -496,6 +501,7 @@ static void restrict_(const Sim& s, const Level& Fl, const Level& Cl, const doub
         }
     }
     if (yc) {
+#pragma omp parallel for schedule(static)
         for (int jf = 1 + s.gy; jf <= Nyf + s.gy; jf += 2) {
             double dS = F.y[jf - 1] - F.y[jf - 2], dN = F.y[jf] - F.y[jf - 1];
             double dyc = one / (dS + dN);
@@ -508,12 +514,14 @@ static void restrict_(const Sim& s, const Level& Fl, const Level& Cl, const doub
         for (int kf = 1 + s.gz; kf <= Nzf + s.gz - 1; kf += 2) {
             double dU = F.z[kf] - F.z[kf - 1], dD = F.z[kf - 1] - F.z[kf - 2];
             double dzc = one / (dD + dU);
+#pragma omp parallel for schedule(static)
             for (int ifn = 1 + s.gx; ifn <= Nxf + s.gx; ifn += 1 + xc)
                 for (int jf = 1 + s.gy; jf <= Nyf + s.gy; jf += 1 + yc)
                     t[I(kf, ifn, jf)] = (half * dzc) * (dD * t[I(kf - 1, ifn, jf)] + dU * t[I(kf + 1, ifn, jf)]) + half * t[I(kf, ifn, jf)];
         }
     }
     std::fill(rc, rc + (size_t)Cg.Nxg * Cg.Nyg * Cg.Nzg, 0.0);
+#pragma omp parallel for schedule(static)
     for (int jc = 1 + s.gy; jc <= Nyc + s.gy; ++jc)
         for (int ic = 1 + s.gx; ic <= Nxc + s.gx; ++ic)
             for (int kc = 1 + s.gz; kc <= Nzc + s.gz; ++kc) {
@@ -531,12 +539,14 @@ static void prolong_(const Sim& s, const Level& Fl, const Level& Cl, double* pf,
     auto I = [&](int k, int i, int j) -> size_t { return (size_t)(k - 1) + (size_t)F.Nzg * ((size_t)(i - 1) + (size_t)F.Nxg * (j - 1)); };
     auto Ic = [&](int k, int i, int j) -> size_t { return (size_t)(k - 1) + (size_t)Cg.Nzg * ((size_t)(i - 1) + (size_t)Cg.Nxg * (j - 1)); };
     std::fill(pf, pf + (size_t)F.Nxg * F.Nyg * F.Nzg, 0.0);
+#pragma omp parallel for schedule(static)
     for (int jc = 1 + s.gy; jc <= Nyc + s.gy; ++jc)
         for (int ic = 1 + s.gx; ic <= Nxc + s.gx; ++ic)
             for (int kc = 1 + s.gz; kc <= Nzc + s.gz - 1; ++kc)
                 pf[I(1 + s.gz + (kc - 1 - s.gz) * ZF, 1 + s.gx + (ic - 1 - s.gx) * XF, 1 + s.gy + (jc - 1 - s.gy) * YF)] = pc[Ic(kc, ic, jc)];
     const double one = 1.0;
     if (XF == 2) {
+#pragma omp parallel for schedule(static)
         for (int jf = 1 + s.gy; jf <= Nyf + s.gy; jf += YF)
             for (int ifn = 2 + s.gx; ifn <= Nxf + s.gx; ifn += XF) {
                 double dW = F.x[ifn - 1] - F.x[ifn - 2], dE = F.x[ifn] - F.x[ifn - 1], dxf = one / (dW + dE);
@@ -545,6 +555,7 @@ static void prolong_(const Sim& s, const Level& Fl, const Level& Cl, double* pf,
             }
     }
     if (YF == 2) {
+#pragma omp parallel for schedule(static)
         for (int ifn = 1 + s.gx; ifn <= Nxf + s.gx; ++ifn)
             for (int jf = 2 + s.gy; jf <= Nyf + s.gy; jf += YF) {
                 double dS = F.y[jf - 1] - F.y[jf - 2], dN = F.y[jf] - F.y[jf - 1], dyf = one / (dS + dN);
@@ -555,6 +566,7 @@ static void prolong_(const Sim& s, const Level& Fl, const Level& Cl, double* pf,
     if (ZF == 2) {
         for (int kf = 2 + s.gz; kf <= Nzf + s.gz - 1; kf += ZF) {
             double dD = F.z[kf - 1] - F.z[kf - 2], dU = F.z[kf] - F.z[kf - 1], dzf = one / (dD + dU);
+#pragma omp parallel for schedule(static)
             for (int jf = 1 + s.gy; jf <= Nyf + s.gy; ++jf)
                 for (int ifn = 1 + s.gx; ifn <= Nxf + s.gx; ++ifn)
                     pf[I(kf, ifn, jf)] = (dU * pf[I(kf - 1, ifn, jf)] + dD * pf[I(kf + 1, ifn, jf)]) * dzf;
@@ -579,13 +591,15 @@ static void mg_solver(Sim& s, int k, double* x, const double* b) {
     size_t n = Lv.A.n;
     vector<double> Ax(n), r(n);
     csr_mv(Lv.A, x, Ax.data());
-    for (size_t t = 0; t < n; ++t) r[t] = b[t] - Ax[t];
+#pragma omp parallel for schedule(static)
+    for (long t = 0; t < (long)n; ++t) r[t] = b[t] - Ax[t];
     Level& Cl = s.lev[k - 1];
     vector<double> rc(Cl.A.n), dxc(Cl.A.n, 0.0), dxf(n);
     restrict_(s, Lv, Cl, r.data(), rc.data());
     mg_solver(s, k - 1, dxc.data(), rc.data());
     prolong_(s, Lv, Cl, dxf.data(), dxc.data());
-    for (size_t t = 0; t < n; ++t) x[t] += dxf[t];
+#pragma omp parallel for schedule(static)
+    for (long t = 0; t < (long)n; ++t) x[t] += dxf[t];
     smooth(s.p.nu2);
 }
 
@@ -604,6 +618,7 @@ static void precond(Sim& s, const double* r, double* u) {
 // DiffXEven.f90, DiffYEven.f90, DiffZArbitrary.f90 on a (Nz,Nx,Ny) array.
 static void diff_x(const Sim& s, const double* v, double* o, int order, int Nz) {
     int a = s.p.alpha, rank = 2 * a + 1, Nx = s.Nxg, Ny = s.Nyg;
+#pragma omp parallel for schedule(static) if (Ny > 1)
     for (int j = 1; j <= Ny; ++j)
         for (int i = 1; i <= Nx; ++i) {
             int st = (i <= a) ? 1 : (i <= Nx - a ? i - a : Nx + 1 - rank);
@@ -616,6 +631,7 @@ static void diff_x(const Sim& s, const double* v, double* o, int order, int Nz) 
 }
 static void diff_y(const Sim& s, const double* v, double* o, int order, int Nz) {
     int b = s.p.beta, rank = 2 * b + 1, Nx = s.Nxg, Ny = s.Nyg;
+#pragma omp parallel for schedule(static)
     for (int j = 1; j <= Ny; ++j) {
         int st = (j <= b) ? 1 : (j <= Ny - b ? j - b : Ny + 1 - rank);
         for (int i = 1; i <= Nx; ++i)
@@ -885,7 +901,8 @@ static int solve_fgmres(Sim& s, const double* rhs, double* sol, int& iters, doub
         std::fill(Hr.begin(), Hr.end(), 0.0);
         int k = 0;
         for (int j = 0;; ++j) {
-            for (size_t t = 0; t < n; ++t) vin[t] = V[j][t] * sc[j];
+#pragma omp parallel for schedule(static)
+            for (long t = 0; t < (long)n; ++t) vin[t] = V[j][t] * sc[j];
             precond(s, vin.data(), Z[j].data());
             matvec_ho(s, Z[j].data(), W.data()); ++mv;
             for (int i = 0; i < j; ++i) a[i] = dot(V[i].data(), V[j].data(), n);
@@ -907,7 +924,8 @@ static int solve_fgmres(Sim& s, const double* rhs, double* sol, int& iters, doub
             HR(j, j) = hj;
             // update: V_j <- V_j - sum sigma_i s_i V_i ; W <- W - sum h_i s_i V_i - h_j s_j V_j(new)
             double ww = 0;
-            for (size_t t = 0; t < n; ++t) {
+#pragma omp parallel for reduction(+ : ww) schedule(static)
+            for (long t = 0; t < (long)n; ++t) {
                 double vj = V[j][t], w = W[t];
                 for (int i = 0; i < j; ++i) { vj -= sig[i] * sc[i] * V[i][t]; w -= hq[i] * sc[i] * V[i][t]; }
                 w -= hj * sc[j] * vj;
@@ -932,7 +950,8 @@ static int solve_fgmres(Sim& s, const double* rhs, double* sol, int& iters, doub
             for (int j = i + 1; j < kk; ++j) t -= RR(j, i) * y[j];
             y[i] = t / RR(i, i);
         }
-        for (size_t t = 0; t < n; ++t) { double acc = sol[t]; for (int i = 0; i < kk; ++i) acc += y[i] * Z[i][t]; sol[t] = acc; }
+#pragma omp parallel for schedule(static)
+        for (long t = 0; t < (long)n; ++t) { double acc = sol[t]; for (int i = 0; i < kk; ++i) acc += y[i] * Z[i][t]; sol[t] = acc; }
         if (resid <= tol) { iters = mv; return OW3D_OK; }
         if (mv >= maxmv) { iters = mv; return OW3D_NOT_CONVERGED; }
     }

@@ -84,3 +84,41 @@ def fs_rhs(p, P):
     P2 = np.asarray(P).reshape(Nyg, Nxg)
     r[gy:Nyg - gy, 1:Nxg - 1, -1] = P2[gy:Nyg - gy, 1:Nxg - 1]
     return r.ravel()
+
+
+def shoal_generation(W, nsteps, **kw):
+    """The 257 x 33 x 9 shoal basin with its generation zone (0-3 m, the
+    linear regular wave T = 1 s, H = 0.01 m at the 0.45 m depth, sampled
+    every half step) and its sponge (30-35 m); GMRES reltol 1e-8 with the
+    example decks' abstol 1e-6. Returns params, geometry and a function of
+    the zone-0 box (i0, i1, j0, j1) that gives the zone's target
+    (mode, nt, dt_sample, eta, phis) for nsteps steps."""
+    zones = [dict(x1=0.0, x2=3.0, y1=0.0, y2=6.0, ftype=-10, param=3.5, wavegen=1),
+             dict(x1=30.0, x2=35.0, y1=0.0, y2=6.0, ftype=9, param=3.5)]
+    p, geo = W.shoal(relaxONOFF=1, relaxNo=2, relaxTransientTime=1.0, zones=zones, reltol=1e-8, abstol=1e-6, **kw)
+    x, _ = W.grid_xy(p)
+
+    def target(box):
+        i0, i1, j0, j1 = box
+        xs = x[i0 - 1:i1]
+        T, H, h = 1.0, 0.01, 0.45
+        om = 2 * np.pi / T
+        k = W.dispersion_k(om, h)
+        nt = 2 * nsteps + 2
+        tt = np.arange(nt) * (0.5 * p.dt)
+        ny = j1 - j0 + 1
+        eta = np.array([np.tile(0.5 * H * np.cos(k * xs - om * t), ny) for t in tt])
+        phis = np.array([np.tile(0.5 * H * W.G / om * np.sin(k * xs - om * t), ny) for t in tt])
+        return (0, nt, 0.5 * p.dt, eta, phis)
+    return p, geo, target
+
+
+def run_steps(sim, nsteps):
+    """Step one step at a time; returns the matvec count of each step."""
+    its = []
+    for _ in range(nsteps):
+        a = sim.stats()["total_iterations"]
+        st = sim.step(1)
+        assert st >= 0, st
+        its.append(sim.stats()["total_iterations"] - a)
+    return np.array(its, dtype=np.int64)

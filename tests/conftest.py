@@ -20,6 +20,15 @@ def load_package():
     return mod
 
 
+def reference_decks():
+    """Folder of the reference's example input decks, from the
+    OW3D_REFERENCE_DECKS environment variable (None when unset: the tests
+    that read those decks are then skipped)."""
+    import os
+    d = os.environ.get("OW3D_REFERENCE_DECKS")
+    return pathlib.Path(d) if d else None
+
+
 def load_oracle():
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle  # noqa: E402

@@ -1,6 +1,7 @@
 """Generate the golden vectors in this folder from the CPU oracle.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py             # the fast set
+    python tests/golden/make_golden.py --fullrun   # also the whole runs (run_*)
 
 The reference has no Fortran compiler or SPARSKIT2/HSL libraries here and no
 stored outputs of its own, so these vectors come from the oracle (the CPU
@@ -84,6 +85,48 @@ def host_setup_cases():
     return out
 
 
+def fullrun_cases():
+    """Whole runs of the benchmark configurations the oracle can finish here
+    in minutes (too slow to regenerate inside the test suite): the final
+    state and the matvec count of every step, in the device ordering (_dev)
+    and the reference ordering (_ref).
+
+      run_shoal_257x33x9_1000   the shoal basin with its generation zone and
+                                sponge, 1000 RK4 steps (reltol 1e-8, abstol 1e-6)
+      run_sfwave_257x9_200      the 2-D stream-function wave (kh = 1, half the
+                                breaking steepness) in the wall-bounded flume
+                                with generation and sponge, 200 RK4 steps
+    """
+    import cases
+    import oracle
+    from conftest import load_package
+    W = load_package().workloads
+    out = {}
+    for mode, tag in ((oracle.MODE_DEVICE, "dev"), (oracle.MODE_REFERENCE, "ref")):
+        p, geo, target = cases.shoal_generation(W, 1000)
+        o = oracle.Oracle(p, **geo, mode=mode)
+        o.set_relax_target(0, *target(o.zone_box(0)))
+        o.set_state(np.zeros(o.C), np.zeros(o.C))
+        its = cases.run_steps(o, 1000)
+        out[f"run_shoal_257x33x9_1000_{tag}"] = _final(o, its)
+        p, geo, E0, P0, targets = W.stream_function_2d(ppw=32, steps=200)
+        o = oracle.Oracle(p, **geo, mode=mode)
+        o.set_state(E0, P0)
+        o.set_relax_target(0, *targets[0])
+        its = cases.run_steps(o, 200)
+        out[f"run_sfwave_257x9_200_{tag}"] = _final(o, its)
+    return out
+
+
+def _final(o, its):
+    E, P, W, phi, t = o.get_state()
+    return dict(E=E, P=P, W=W, phi=phi, t=np.array([t]), step_iterations=its)
+
+
+def is_fullrun(name):
+    return name.startswith("run_")
+
+
 def generate():
     import oracle
     out = host_setup_cases()
@@ -100,7 +143,13 @@ def main():
     from conftest import load_package
     load_package()
     sets = generate()
+    if "--fullrun" in sys.argv:
+        sets.update(fullrun_cases())
     lines = []
+    # whole-run fixtures not regenerated this time keep their entries
+    for f in sorted(HERE.glob("run_*.npz")):
+        if f.stem not in sets:
+            lines.append(f"{hashlib.sha256(f.read_bytes()).hexdigest()}  {f.name}")
     for name, arrs in sorted(sets.items()):
         f = HERE / f"{name}.npz"
         if f.exists():
@@ -114,6 +163,7 @@ def main():
                 continue
         np.savez_compressed(f, **arrs)
         lines.append(f"{hashlib.sha256(f.read_bytes()).hexdigest()}  {f.name}")
+    lines.sort(key=lambda ln: ln.split()[1])
     (HERE / "MANIFEST.txt").write_text("\n".join(lines) + "\n")
     print("\n".join(lines))
 

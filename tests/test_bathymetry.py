@@ -9,6 +9,7 @@ import pathlib
 
 import numpy as np
 import pytest
+from conftest import reference_decks
 
 DECK = """bathymetry from a file
 0 0
@@ -93,7 +94,7 @@ def test_errors(ow3d, tmp_path):
         ow3d.read_bathymetry(p, deck_dir=tmp_path)
 
 
-REF = pathlib.Path(os.environ.get("OW3D_REFERENCE_DECKS", "/root/reference/examples/inputfiles"))
+REF = reference_decks() or pathlib.Path("/nonexistent")
 
 
 @pytest.mark.skipif(not (REF / "beach_137").exists(), reason="reference example files not on this machine")

@@ -49,13 +49,15 @@ def test_struct_layouts_match(ow3d):
 
 
 def test_fortran_binding_size(ow3d):
-    """The Fortran side of the binding holds ow3d_params as an opaque byte
-    array whose length must be the struct's size."""
-    import re
-    from conftest import ROOT
-    text = (ROOT / "INTEGRATION.md").read_text()
+    """The Fortran module of the binding (include/ow3d_iface.f90) holds
+    ow3d_params as an opaque byte array whose length must be the struct's
+    size, and binds only names the C header declares."""
+    text = (ROOT / "include" / "ow3d_iface.f90").read_text()
     sizes = [int(n) for n in re.findall(r"raw\((\d+)\)\s+! opaque to Fortran: sizeof\(ow3d_params\)", text)]
     assert sizes == [C.sizeof(ow3d.capi.Params)]
+    bound = set(re.findall(r'BIND\(C, name="(ow3d_\w+)"\)', text))
+    assert {"ow3d_read_deck", "ow3d_create", "ow3d_solve", "ow3d_step", "ow3d_get_state"} <= bound
+    assert bound <= declared_functions()
 
 
 def test_default_params_match_mirror(ow3d):

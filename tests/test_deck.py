@@ -6,6 +6,7 @@ import os
 import pathlib
 
 import pytest
+from conftest import reference_decks
 
 DECK_3D = """synthetic 3-D basin with two relaxation zones
 -1 0                                   <- IC, IncWaveType
@@ -112,7 +113,7 @@ def test_parsed_deck_builds_a_valid_estimate(ow3d, tmp_path):
     assert ow3d.lib().ow3d_estimate_bytes(C.byref(p), C.byref(b)) == 0 and b.value > 0
 
 
-REF_DECKS = pathlib.Path(os.environ.get("OW3D_REFERENCE_DECKS", "/root/reference/examples/inputfiles"))
+REF_DECKS = reference_decks() or pathlib.Path("/nonexistent")
 
 
 @pytest.mark.skipif(not REF_DECKS.is_dir(), reason="reference example decks not on this machine")
@@ -162,9 +163,23 @@ def test_decks_needing_unbuilt_features_are_refused(ow3d, tmp_path):
         "IncWaveType 3": base.replace("-1 0  ", "-1 3  "),
         "acceleration": base.replace("-1 0  ", "-1 0 0.5 "),
         "acceleration, 100 g": base.replace("-1 0  ", "-1 0 100. "),
+        # LocalSmoothing2D.f90:37 smooths for every limit up to 100 g when a deck gives one
+        "acceleration, 0": base.replace("-1 0  ", "-1 0 0. "),
+        "acceleration, negative": base.replace("-1 0  ", "-1 0 -5. "),
+        # a stream-function or flux wave with a constant-flux current (ReadInputFileParameters.f90:42-49)
+        "IncWaveType 4": base.replace("-1 0  ", "-1 4  "),
+        "IncWaveType 5": base.replace("-1 0  ", "-1 5  "),
     }
     for what, text in cases_.items():
         st, p = status(text)
         assert st == ow3d.capi.ERR_UNSUPPORTED, (what, st)
     msg = L.ow3d_last_error().decode()
-    assert "acceleration" in msg
+    assert "IncWaveType 4 and 5" in msg
+    st, p = status(base.replace("-1 0  ", "-1 0 1000. "))
+    assert st == 0 and p.accel_from_deck == 1
+    # parameters built by a caller: accel_tol_fact = 0 (zero-initialised) means no smoothing
+    q = ow3d.default_params(Nx=33, Ny=17, Nz=9)
+    q.accel_tol_fact = 0.0
+    assert L.ow3d_estimate_bytes(C.byref(q), C.byref(C.c_size_t())) == 0
+    q.accel_tol_fact = 50.0
+    assert L.ow3d_estimate_bytes(C.byref(q), C.byref(C.c_size_t())) == ow3d.capi.ERR_UNSUPPORTED

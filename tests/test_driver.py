@@ -11,6 +11,7 @@ import pathlib
 
 import numpy as np
 import pytest
+from conftest import reference_decks
 
 DECK = """driver test: 2-D flume, mono-chromatic incident wave, sponge
 0 2
@@ -72,7 +73,7 @@ def test_run_with_oracle_and_hot_start(ow3d, oracle, tmp_path):
     assert s2.params.time0 == t and np.array_equal(s2.E0[1:-1], Ei) and np.array_equal(s2.P0[1:-1], Pi)
 
 
-REF = pathlib.Path(os.environ.get("OW3D_REFERENCE_DECKS", "/root/reference/examples/inputfiles"))
+REF = reference_decks() or pathlib.Path("/nonexistent")
 
 
 @pytest.mark.skipif(not REF.is_dir(), reason="reference example decks not on this machine")

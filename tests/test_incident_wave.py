@@ -15,6 +15,7 @@ import pathlib
 
 import numpy as np
 import pytest
+from conftest import reference_decks
 
 DECK = """incident wave, mono-chromatic, x-directed generation zone
 0 2
@@ -122,7 +123,7 @@ def test_incident_wave_errors(ow3d, tmp_path):
         ow3d.incident_wave(p, 0)
 
 
-REF_DECKS = pathlib.Path(os.environ.get("OW3D_REFERENCE_DECKS", "/root/reference/examples/inputfiles"))
+REF_DECKS = reference_decks() or pathlib.Path("/nonexistent")
 
 
 @pytest.mark.skipif(not REF_DECKS.is_dir(), reason="reference example decks not on this machine")

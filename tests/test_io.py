@@ -17,8 +17,9 @@ import numpy as np
 import pytest
 
 import cases  # noqa: F401  (puts tests/ on the path for the package loader)
+from conftest import reference_decks
 
-REF_INPUTS = pathlib.Path("/root/reference/examples/inputfiles")
+REF_INPUTS = reference_decks() or pathlib.Path("/nonexistent")
 
 
 def fortran_e16_6e3(v):

@@ -17,8 +17,9 @@ import pytest
 
 import cases
 from test_driver import DECK
+from conftest import reference_decks
 
-REF = pathlib.Path(os.environ.get("OW3D_REFERENCE_DECKS", "/root/reference/examples/inputfiles"))
+REF = reference_decks() or pathlib.Path("/nonexistent")
 
 
 def _zone(p, typ=0, x0=6.0, x1=8.0, g0=1.0):

@@ -13,6 +13,7 @@ import pathlib
 
 import numpy as np
 import pytest
+from conftest import reference_decks
 
 
 def _params(ow3d, kd, kH, nmodes=20, nsteps=4, period=None):
@@ -88,7 +89,7 @@ def test_errors(ow3d):
         ow3d.stream_function_wave(p, np.zeros(3))
 
 
-REF_DECKS = pathlib.Path(os.environ.get("OW3D_REFERENCE_DECKS", "/root/reference/examples/inputfiles"))
+REF_DECKS = reference_decks() or pathlib.Path("/nonexistent")
 
 
 @pytest.mark.skipif(not REF_DECKS.is_dir(), reason="reference example decks not on this machine")
