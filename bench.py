@@ -154,6 +154,7 @@ def run_gpu(args, rank, world):
         launches = lib.ow3d_launch_count() - n0
         ms = max_over_ranks(ms, world, "cuda")
         s = sim.stats()
+        s["status"] = st
         E, P, Wv, phi, tt = sim.get_state()
         states[prec] = (E, phi)
         pb, pinfo = path_bytes_per_step(sim, s, args.steps, 8 if prec == "fp64" else 4)
@@ -173,6 +174,7 @@ def run_gpu(args, rank, world):
     outW = torch.empty(C, dtype=torch.float64).pin_memory().numpy()
     E, P, Wv, phi, tt = sim.get_state()
     hostE[:] = E; hostP[:] = P
+    sim.reset_stats()
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -184,6 +186,7 @@ def run_gpu(args, rank, world):
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     e2e_s = max_over_ranks(e2e_s, world, "cuda")
+    res["e2e_stats"] = sim.stats()
     sim.close()
     # eta / phi error of the mixed path against the FP64 path after the same steps
     Ef, phif = states["fp64"]; Em, phim = states["mixed"]
@@ -226,6 +229,17 @@ def path_bytes_per_step(sim, stats, steps, s):
         "iterations_min_max": [stats["min_iterations"], stats["max_iterations"]]}
 
 
+def solver_report(st, p):
+    """The stopping test of the timed solves: GMRES stops at
+    |r| <= reltol*|r0| + abstol (iterative_solution.f90:24,44-45), so the
+    report states both terms for the last timed solve, which of them set the
+    threshold, and how many solves hit the matvec limit."""
+    r0, tol = st["last_initial_residual"], st["last_tolerance"]
+    return {"not_converged": st["not_converged"], "reltol": p.reltol, "abstol": p.abstol,
+            "last_solve": {"initial_residual": r0, "threshold": tol, "final_residual": st["last_residual"],
+                           "threshold_set_by": "abstol" if p.abstol > p.reltol * r0 else "reltol"}}
+
+
 def kernel_roofline(pkg, p, dev):
     """Per-launch device time of the finest-level colour pass (the smoother,
     the largest kernel class of the step) and of the high-order operator,
@@ -236,6 +250,7 @@ def kernel_roofline(pkg, p, dev):
     p2 = pkg.default_params(Nx=p.Nx, Ny=p.Ny, Nz=p.Nz, Lx=p.Lx, Ly=p.Ly, Lz=p.Lz, GridZ=1, device=dev)
     Nxg, Nyg, Nzg = pkg.dims(p2)
     sim = pkg.Simulation(p2, np.ones(Nxg * Nyg))
+    ncolor = sim.level_dims(sim.level_count() - 1)[3]
     reps = 20
     out = {}
     for which, name in ((2, "colour"), (0, "operator")):
@@ -244,10 +259,11 @@ def kernel_roofline(pkg, p, dev):
             out[name] = ms.value / reps
     sim.close()
     N, Cc = Nxg * Nyg * Nzg, Nxg * Nyg
-    # colour pass: x read at every point (own and neighbour columns), b read
-    # and x written at the points of one colour
-    alg = {"colour": 2 * 8 * N, "operator": 2 * 8 * N + 10 * 8 * Cc}
-    return {k: (v, alg[k]) for k, v in out.items()}
+    # one Gauss-Seidel sweep of a level moves 3*s*N_l + 5*s*C_l bytes (x read
+    # and written, b read, the column coefficients); a sweep is `ncolor`
+    # colour passes, each covering 1/ncolor of the columns
+    alg = {"colour": (3 * 8 * N + 5 * 8 * Cc) / ncolor, "operator": 2 * 8 * N + 10 * 8 * Cc}
+    return {k: (v, alg[k]) for k, v in out.items()}, ncolor
 
 
 def profiled_traffic(kernel):
@@ -290,7 +306,13 @@ def serving_sample(n=16, seed=2024):
     }
 
 
-def cpu_baseline(threads, steps=1):
+def cpu_baseline(threads, warmup=1, steps=None, budget_s=15.0, max_steps=8):
+    """The reference-ordered oracle (lexicographic Gauss-Seidel multigrid,
+    left-preconditioned GMRES) on `threads` host threads, on a bounded
+    sample of the workload: one instance on the CPU_SAMPLE sub-basin of the
+    same sea, `warmup` untimed steps, then consecutive RK4 steps timed
+    together -- `steps` of them, or as many as fit in budget_s (at most
+    max_steps). Returns DOF-timesteps/s, seconds, steps timed, params."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
     pkg = package()
@@ -299,10 +321,18 @@ def cpu_baseline(threads, steps=1):
     p, geo, E0, P0 = W.irregular_sea(**CPU_SAMPLE, precision=0, seed=1234)
     orc = O.Oracle(p, **geo, mode=O.MODE_REFERENCE)
     orc.set_state(E0, P0)
+    if warmup > 0:
+        orc.step(warmup)
+    n = 0
     t0 = time.perf_counter()
-    orc.step(steps)
-    dt = time.perf_counter() - t0
-    return dof(p) * steps / dt, dt, p
+    while True:
+        orc.step(1)
+        n += 1
+        dt = time.perf_counter() - t0
+        if (steps and n >= steps) or (not steps and (dt >= budget_s or n >= max_steps)):
+            break
+    s = orc.stats()
+    return dof(p) * n / dt, dt, n, p, s["total_iterations"] / max(s["solves"], 1)
 
 
 def profile_step(args):
@@ -325,7 +355,8 @@ def profile_step(args):
 
 def largest_instance(args):
     """The largest single instance, 2049 x 513 x 9 (flat 1 m, seeded JONSWAP
-    sea): FP64 and mixed precision at GMRES rtol 1e-6, 1e-8 and 1e-10, one
+    sea): FP64 and mixed precision at GMRES rtol 1e-6, 1e-8 and 1e-10 with
+    abstol 0 (so that the relative term alone sets each threshold), one
     JSON line per tolerance with both precisions' DOF-timesteps/s, iterations
     per solve and the mixed path's eta error against FP64. Timed like the
     main line (device events around the steps, after warm-up steps)."""
@@ -337,7 +368,7 @@ def largest_instance(args):
         res, states = {}, {}
         for prec in ("fp64", "mixed"):
             p, geo, E0, P0 = W.irregular_sea(Nx=2049, Ny=513, Nz=9, precision=(1 if prec == "mixed" else 0),
-                                             reltol=rtol, seed=1234)
+                                             reltol=rtol, abstol=0.0, seed=1234)
             sim = pkg.Simulation(p, **geo)
             sim.set_state(E0, P0)
             sim.step(args.warmup)
@@ -349,10 +380,10 @@ def largest_instance(args):
             states[prec] = E
             res[prec] = dict(value=dof(p) * args.steps / (ms / 1e3), ms_per_step=ms / args.steps,
                              iterations_per_solve=s["total_iterations"] / max(s["solves"], 1),
-                             not_converged=s["not_converged"])
+                             **solver_report(s, p))
             sim.close()
         err = float(np.max(np.abs(states["mixed"] - states["fp64"])) / np.max(np.abs(states["fp64"])))
-        print(json.dumps({"config": "largest instance 2049x513x9, flat 1 m, JONSWAP", "rtol": rtol,
+        print(json.dumps({"config": "largest instance 2049x513x9, flat 1 m, JONSWAP, GMRES(23) abstol 0", "rtol": rtol,
                           "unit": UNIT, "steps": args.steps, "warmup": args.warmup, "fp64": res["fp64"],
                           "mixed": res["mixed"], "speedup_mixed_vs_fp64": res["mixed"]["value"] / res["fp64"]["value"],
                           "eta_rel_err_mixed_vs_fp64": err}))
@@ -384,18 +415,14 @@ def main():
         if rank != 0:
             return
         nthreads = os.cpu_count() or 1
-        vals = []
-        for _ in range(args.warmup):
-            pass
-        for _ in range(max(args.steps, 1)):
-            v, dt, p = cpu_baseline(nthreads, 1)
-            vals.append(v)
-        v = float(np.median(vals))
-        sample = (f"{p.Nx}x{p.Ny}x{p.Nz} sub-basin of the irregular-sea workload (same dx, Nz, spectrum), 1 RK4 step "
-                  f"per sample, reference-ordered oracle (lexicographic Gauss-Seidel, left GMRES)")
+        v, dt, n, p, it = cpu_baseline(nthreads, warmup=args.warmup, steps=max(args.steps, 1))
+        sample = (f"{p.Nx}x{p.Ny}x{p.Nz} sub-basin of the irregular-sea workload (same dx, Nz, spectrum): "
+                  f"{args.warmup} warm-up steps, then {n} consecutive RK4 steps of one instance timed together "
+                  f"({dt:.1f} s, {it:.1f} matvecs per solve), reference-ordered oracle (lexicographic "
+                  f"Gauss-Seidel, left GMRES), {nthreads} OpenMP threads")
         print(json.dumps({
             "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / n * 1e3, "higher_is_better": True,
             "config": {"workload": "irregular sea 1025x257x17 (sampled on host)", "sample": sample},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -417,7 +444,7 @@ def main():
     v_fp64 = job_throughput(D, args.steps, world, ms_fp64)
     peak, peak_kind = peaks()
     roof = None
-    kr = kernel_roofline(pkg, pm, int(os.environ.get("LOCAL_RANK", "0")))
+    kr, ncolor = kernel_roofline(pkg, pm, int(os.environ.get("LOCAL_RANK", "0")))
     roof_op = None
     if "colour" in kr:
         kms, alg = kr["colour"]
@@ -425,6 +452,7 @@ def main():
         roof = {"bound": "hbm", "kernel": "k_lo_colour (one colour pass of the finest multigrid level, FP64)",
                 "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                 "traffic": profiled_traffic("k_lo_colour"), "peak_kind": peak_kind, "alg_bytes_per_launch": alg,
+                "alg_bytes_rule": f"(3*8*N + 5*8*C) / {ncolor} colours: one sweep's bytes per colour pass",
                 "ms_per_launch": kms}
     if "operator" in kr:
         kms, alg = kr["operator"]
@@ -444,10 +472,15 @@ def main():
     cpu = None
     if not args.no_cpu:
         nthreads = os.cpu_count() or 1
-        v, dt, p = cpu_baseline(nthreads, 4)
+        v, dt, n, p, it = cpu_baseline(nthreads)
         cpu = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port",
-               "sample": f"{p.Nx}x{p.Ny}x{p.Nz} sub-basin of the same workload, 4 RK4 steps ({dt:.1f} s), "
-                         f"reference-ordered oracle (lexicographic Gauss-Seidel, left GMRES)"}
+               "sample": f"{p.Nx}x{p.Ny}x{p.Nz} sub-basin of the same workload: 1 warm-up step, then {n} consecutive "
+                         f"RK4 steps of one instance ({dt:.1f} s, {it:.1f} matvecs per solve), reference-ordered "
+                         f"oracle (lexicographic Gauss-Seidel, left GMRES), {nthreads} OpenMP threads"}
+        v1, dt1, n1, _, it1 = cpu_baseline(1, budget_s=15.0, max_steps=4)
+        cpu["serial"] = {"value": v1, "unit": UNIT, "cores": 1, "kind": "port",
+                         "sample": f"same sub-basin, 1 warm-up step, then {n1} consecutive RK4 steps on one thread "
+                                   f"({dt1:.1f} s): the like-for-like figure of the serial Fortran reference"}
     serve = None
     if not args.no_serve and world == 1:
         serve = serving_sample()
@@ -458,17 +491,22 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_mixed / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 (FP32 multigrid)", "data": "synthetic (seeded JONSWAP sea)",
         "config": {"workload": "irregular sea 1025x257x17, flat 1 m, JONSWAP Hs=0.05 Tp=1.5 gamma=3.3, "
-                               "GMRES rtol 1e-8, Courant 0.5", "DOF": D, "parallelism": f"replicas x{world}",
+                               "GMRES(23) reltol 1e-8 abstol 1e-6 (the example decks' solver line), Courant 0.5",
+                   "DOF": D, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (phi 38 MB + Krylov basis ~1.8 GB per replica)"},
         "fp64": {"value": v_fp64, "ms_per_step": ms_fp64 / args.steps,
-                 "avg_iterations": sf["total_iterations"] / max(sf["solves"], 1)},
+                 "avg_iterations": sf["total_iterations"] / max(sf["solves"], 1), **solver_report(sf, pm)},
         "mixed": {"value": v_mixed, "ms_per_step": ms_mixed / args.steps,
                   "avg_iterations": sm["total_iterations"] / max(sm["solves"], 1),
-                  "eta_rel_err_vs_fp64": err_eta, "phi_rel_err_vs_fp64": err_phi},
+                  "eta_rel_err_vs_fp64": err_eta, "phi_rel_err_vs_fp64": err_phi, **solver_report(sm, pm)},
         "speedup_mixed_vs_fp64": v_mixed / v_fp64,
         "laplace_solves_per_s": sm["solves"] * world / (ms_mixed / 1e3),
         "e2e": {"value": job_throughput(D, args.steps, world, e2e_s * 1e3), "unit": UNIT,
-                "h2d_bytes_per_step": 2 * 8 * C, "d2h_bytes_per_step": 3 * 8 * C},
+                "h2d_bytes_per_step": 2 * 8 * C, "d2h_bytes_per_step": 3 * 8 * C,
+                "path": "mixed precision; per step ow3d_put_surface (E, P from pinned host memory), ow3d_step, "
+                        "ow3d_get_state (E, P, W to pinned host memory); host wall clock around the steps",
+                "avg_iterations": res["e2e_stats"]["total_iterations"] / max(res["e2e_stats"]["solves"], 1),
+                "not_converged": res["e2e_stats"]["not_converged"]},
         "roofline": roof, "roofline_operator": roof_op, "roofline_path": path_roof, "cpu_baseline": cpu, "clocks": res["mixed"]["clocks"], "serving": serve,
         "gpu_launches": res["mixed"]["launches"],
     }

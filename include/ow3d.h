@@ -197,6 +197,10 @@ typedef struct ow3d_stats {
     double  last_residual;        /* final residual estimate of the last solve */
     double  time;                 /* simulation time                           */
     int64_t tstep;                /* number of completed time steps            */
+    double  last_initial_residual;/* |rhs - A phi0| of the last solve (FGMRES; the
+                                     preconditioned residual for left GMRES)     */
+    double  last_tolerance;       /* its stopping threshold reltol*|r0| + abstol
+                                     (iterative_solution.f90:24,44-45)          */
 } ow3d_stats;
 
 /* ------------------------------------------------------------- set-up */

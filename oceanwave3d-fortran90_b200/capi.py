@@ -82,6 +82,7 @@ class Stats(C.Structure):
         ("min_iterations", C.c_int), ("max_iterations", C.c_int), ("last_iterations", C.c_int),
         ("not_converged", C.c_int64), ("last_residual", C.c_double),
         ("time", C.c_double), ("tstep", C.c_int64),
+        ("last_initial_residual", C.c_double), ("last_tolerance", C.c_double),
     ]
 
 

@@ -160,9 +160,40 @@ __global__ void k_relax(FsArgs a, RelaxZoneDev z, double* E, double* P, double F
     }
 }
 
-// Ghost values so that the boundary one-sided d/dx equals S (zero).
+// Periodic x: the distinct column whose values image column i (1-based)
+// carries -- 1 <- Nxg-2, Nxg-1 <- 2, Nxg <- 3 -- or i itself.
+__device__ __forceinline__ int src_col(int i, int Nxg) {
+    return i == 1 ? Nxg - 2 : (i == Nxg - 1 ? 2 : (i == Nxg ? 3 : i));
+}
+
+// Periodic x: image columns of a field with nz values per column copied
+// from the distinct columns (zero = 1: set to zero instead).
+__global__ void k_images(FsArgs a, double* v, int nz, int zero) {
+    const int Nx = a.Nxg;
+    const int64_t n = (int64_t)a.Nyg * 3 * nz;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const int k = (int)(t % nz);
+        const int64_t q = t / nz;
+        const int w = (int)(q % 3), j = (int)(q / 3);
+        const int i = w == 0 ? 1 : (w == 1 ? Nx - 1 : Nx);   // 1-based image column
+        double* r = v + (int64_t)nz * Nx * j;
+        r[(int64_t)nz * (i - 1) + k] = zero ? 0.0 : r[(int64_t)nz * (src_col(i, Nx) - 1) + k];
+    }
+}
+
+// Ghost values so that the boundary one-sided d/dx equals S (zero); with
+// periodic x, the image columns instead.
 __global__ void k_ghost_x(FsArgs a, double* v1, double* v2) {
     const int Nx = a.Nxg;
+    if (a.per) {
+        for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < a.Nyg; j += gridDim.x * blockDim.x) {
+            double* r1 = v1 + (int64_t)Nx * j;
+            double* r2 = v2 + (int64_t)Nx * j;
+            r1[0] = r1[Nx - 3]; r1[Nx - 2] = r1[1]; r1[Nx - 1] = r1[2];
+            r2[0] = r2[Nx - 3]; r2[Nx - 2] = r2[1]; r2[Nx - 1] = r2[2];
+        }
+        return;
+    }
     for (int j = blockIdx.x * blockDim.x + threadIdx.x + 1; j <= a.Nyg; j += gridDim.x * blockDim.x) {
         if (a.three && (j == 1 || j == a.Nyg)) continue;
         double* vs[2] = {v1, v2};
@@ -208,13 +239,24 @@ __global__ void k_diff_x(FsArgs a, const double* E, const double* P, double* Ex,
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < C; p += (int64_t)gridDim.x * blockDim.x) {
         const int i = (int)(p % a.Nxg) + 1;
         const int64_t rb = p - (i - 1);
-        const int ws = ws7(i, a.Nxg);
         double dx = 0, dxx = 0, px = 0;
-        for (int m = 0; m < kHoRank; ++m) {
-            const double e = E[rb + ws - 1 + m];
-            dx += S1[(i - 1) * kHoRank + m] * e;
-            dxx += S2[(i - 1) * kHoRank + m] * e;
-            px += S1[(i - 1) * kHoRank + m] * P[rb + ws - 1 + m];
+        if (a.per) {
+            // centred on the distinct column the point stands for, cyclic
+            const int ic = src_col(i, a.Nxg);
+            for (int m = 0; m < kHoRank; ++m) {
+                const int64_t q = rb + wrap_x(ic - 3 + m, a.Nxg) - 1;
+                dx += S1[(ic - 1) * kHoRank + m] * E[q];
+                dxx += S2[(ic - 1) * kHoRank + m] * E[q];
+                px += S1[(ic - 1) * kHoRank + m] * P[q];
+            }
+        } else {
+            const int ws = ws7(i, a.Nxg);
+            for (int m = 0; m < kHoRank; ++m) {
+                const double e = E[rb + ws - 1 + m];
+                dx += S1[(i - 1) * kHoRank + m] * e;
+                dxx += S2[(i - 1) * kHoRank + m] * e;
+                px += S1[(i - 1) * kHoRank + m] * P[rb + ws - 1 + m];
+            }
         }
         Ex[p] = dx; Exx[p] = dxx; Px[p] = px;
     }
@@ -258,6 +300,7 @@ __global__ void k_set_rhs(FsArgs a, const double* __restrict__ P, double* __rest
         const int i = (int)(p % a.Nxg), j = (int)(p / a.Nxg);
         const bool ghost = i == 0 || i == a.Nxg - 1 || (a.three && (j == 0 || j == a.Nyg - 1));
         if (ghost) continue;
+        if (a.per && i == a.Nxg - 2) continue;   // the repeated column: identity rows, zero
         rhs[p * a.Nzg + a.Nzg - 1] = P[p];
     }
 }
@@ -279,7 +322,14 @@ __global__ void k_filter_x(FsArgs a, FilterDev f, const double* __restrict__ src
         const double* row = src + (p - (i - 1));
         double v = src[p];
         const bool rowok = !a.three || (j >= 2 && j <= a.Nyg - 1);
-        if (rowok && i >= 2 && i <= Nx - 1) {
+        if (rowok && a.per) {
+            // periodic x: the centred filter at the distinct column the point
+            // stands for, cyclic
+            const int ic = src_col(i, Nx);
+            double acc = 0;
+            for (int m = 1; m <= NP; ++m) acc += row[wrap_x(ic - al + m - 1, Nx) - 1] * f.fc[m - 1];
+            v = acc;
+        } else if (rowok && i >= 2 && i <= Nx - 1) {
             // the reference writes left block, centre, right block in that order
             if (i >= Nx - 1 - al + 1) {  // i = Nx-1-al+ib
                 const int ib = i - (Nx - 1 - al);
@@ -380,6 +430,11 @@ void fs_derivs(const FsArgs& a, double* E, double* P, double* Ex, double* Exx, d
 void fs_wvel(const FsArgs& a, const double* phi, const double* E, double* W, cudaStream_t st) {
     int64_t C = (int64_t)a.Nxg * a.Nyg;
     note_launch(), k_wvel<<<nb(C), 256, 0, st>>>(a, phi, E, W);
+    if (a.per) fs_images(a, W, 1, 0, st);
+}
+void fs_images(const FsArgs& a, double* v, int nz, int zero, cudaStream_t st) {
+    const int64_t n = (int64_t)a.Nyg * 3 * nz;
+    note_launch(), k_images<<<nb(n), 256, 0, st>>>(a, v, nz, zero);
 }
 void fs_set_rhs(const FsArgs& a, const double* P, double* rhs, cudaStream_t st) {
     int64_t C = (int64_t)a.Nxg * a.Nyg;

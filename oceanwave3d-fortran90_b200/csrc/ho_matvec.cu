@@ -147,6 +147,11 @@ __device__ void ho_column_general(const HoGrid& g, const Surface& s, const TIN* 
     };
     const bool ghost_x = (i == 1 || i == Nxg);
     const bool ghost_y = THREE && (j == 1 || j == Nyg);
+    if (g.per && (ghost_x || i == Nxg - 1)) {
+        // periodic x: ghost and repeated columns are identity rows
+        for (int k = 1; k <= Nzg; ++k) emit(k, P(k, i, j));
+        return;
+    }
     if (ghost_x || ghost_y) {
         // Lateral Neumann rows and identity corners (BuildLinearSystem.f90:150-284)
         const bool corner = ghost_x && ghost_y;
@@ -166,14 +171,15 @@ __device__ void ho_column_general(const HoGrid& g, const Surface& s, const TIN* 
         }
         return;
     }
-    // pass 1: horizontal derivatives at every level
+    // pass 1: horizontal derivatives at every level (periodic x: the centred
+    // window, its columns taken cyclically)
     double tx[kZMax], ty[kZMax], lap[kZMax], pc[kZMax];
-    const int wsx = win_start(i, Nxg);
+    const int wsx = g.per ? i - 3 : win_start(i, Nxg);
     const int wsy = THREE ? win_start(j, Nyg) : 1;
     for (int k = 1; k <= Nzg; ++k) {
         double dx = 0, dxx = 0;
         for (int m = 0; m < kHoRank; ++m) {
-            const double v = P(k, wsx + m, j);
+            const double v = P(k, g.per ? wrap_x(wsx + m, Nxg) : wsx + m, j);
             dx += SX1[(i - 1) * kHoRank + m] * v;
             dxx += SX2[(i - 1) * kHoRank + m] * v;
         }
@@ -192,8 +198,8 @@ __device__ void ho_column_general(const HoGrid& g, const Surface& s, const TIN* 
     // derivative avoids the ghost corner columns (ConstructTableCrossDerivatives.f90:173-186,231-235).
     {
         int sh = 0;
-        if (wsx == 1) sh = 1;
-        if (wsx + 6 == Nxg) sh = -1;
+        if (!g.per && wsx == 1) sh = 1;
+        if (!g.per && wsx + 6 == Nxg) sh = -1;
         if (sh != 0) {
             double dx = 0;
             for (int m = 0; m < kHoRank; ++m) dx += SX1[(i - sh - 1) * kHoRank + m] * P(1, wsx + sh + m, j);

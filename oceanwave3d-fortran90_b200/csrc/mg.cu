@@ -379,7 +379,7 @@ void launch_lo_matvec(const LevelDev<T>& L, const T* x, T* y, cudaStream_t st) {
 template <typename T, int S>
 static bool colour_tile_launch(const LevelDev<T>& L, int c, cudaStream_t st) {
     const int min_tiles = g_colour_tiles.load(std::memory_order_relaxed);
-    if (S < 4 || L.cross || L.ncolor != 2 || L.Nxg < 12 || L.Nyg < 12 || min_tiles <= 0) return false;
+    if (S < 4 || L.cross || L.per || L.ncolor != 2 || L.Nxg < 12 || L.Nyg < 12 || min_tiles <= 0) return false;
     const int ntx = (L.Nxg - 6 + kCTX - 1) / kCTX, nty = (L.Nyg - 6 + kCTY - 1) / kCTY;
     if (ntx * nty < min_tiles) return false;
     const TileShape<T> sh = tile_shape<T>(L.Nxg, L.Nzg);

@@ -69,6 +69,21 @@ __device__ __forceinline__ T sy(const LevelDev<T>& L, int o, int j, int m) { ret
 template <typename T>
 __device__ __forceinline__ T sz(const LevelDev<T>& L, int o, int k, int m) { return __ldg(L.SZ + ((o - 1) * L.Nzg + (k - 1)) * 3 + m); }
 
+// x-neighbour column index: cyclic on a periodic level.
+template <typename T>
+__device__ __forceinline__ int xcol(const LevelDev<T>& L, int i) { return L.per ? wrap_x(i, L.Nxg) : i; }
+// Column offsets (in elements) of the left and right x-neighbours of column
+// i, for addressing relative to the column: +-Nzg, or across the period on
+// a periodic level.
+template <typename T>
+__device__ __forceinline__ int xoff_l(const LevelDev<T>& L, int i) {
+    return (L.per && i == 2) ? (L.Nxg - 4) * L.Nzg : -L.Nzg;
+}
+template <typename T>
+__device__ __forceinline__ int xoff_r(const LevelDev<T>& L, int i) {
+    return (L.per && i == L.Nxg - 2) ? -(L.Nxg - 4) * L.Nzg : L.Nzg;
+}
+
 // Interior row (2 <= k <= Nzg-1, interior column). Returns A x at the row and
 // the diagonal coefficient.
 template <typename T, bool THREE, bool CROSS = true>
@@ -85,7 +100,7 @@ __device__ T lo_interior(const LevelDev<T>& L, const T* x, int k, int i, int j, 
     T acc = 0;
     // d2/dx2, d2/dy2 (centred 3-point, PrepareFullOperatorStencils.f90:213-231)
 #pragma unroll
-    for (int m = 0; m < 3; ++m) acc += sx(L, 2, i, m) * x[IX(L, k, i - 1 + m, j)];
+    for (int m = 0; m < 3; ++m) acc += sx(L, 2, i, m) * x[IX(L, k, xcol(L, i - 1 + m), j)];
     if (THREE) {
 #pragma unroll
         for (int m = 0; m < 3; ++m) acc += sy(L, 2, j, m) * x[IX(L, k, i, j - 1 + m)];
@@ -155,7 +170,7 @@ __device__ T lo_bottom(const LevelDev<T>& L, const T* x, int i, int j, T& diag) 
     for (int m = 0; m < 3; ++m) dz += sz(L, 1, 2, m) * x[IX(L, 1 + m, i, j)];
     T dx = 0;
 #pragma unroll
-    for (int m = 0; m < 3; ++m) dx += sx(L, 1, i, m) * x[IX(L, 2, i - 1 + m, j)];
+    for (int m = 0; m < 3; ++m) dx += sx(L, 1, i, m) * x[IX(L, 2, xcol(L, i - 1 + m), j)];
     T acc = f * dz + hx * dx;
     if (THREE) {
         T dy = 0;
@@ -171,7 +186,9 @@ __device__ T lo_bottom(const LevelDev<T>& L, const T* x, int i, int j, T& diag) 
 template <typename T, bool THREE>
 __device__ T lo_ghost(const LevelDev<T>& L, const T* x, int k, int i, int j, T& diag) {
     const bool gxx = (i == 1 || i == L.Nxg), gyy = THREE && (j == 1 || j == L.Nyg);
-    if ((gxx && gyy) || k == 1) { diag = T(1); return x[IX(L, k, i, j)]; }
+    // periodic x: the ghost and repeated columns are identity rows
+    const bool pid = L.per && (gxx || i == L.Nxg - 1);
+    if ((gxx && gyy) || k == 1 || pid) { diag = T(1); return x[IX(L, k, i, j)]; }
     T acc = 0;
     if (gxx) {
         const int ia = (i == 1) ? 2 : L.Nxg - 1;
@@ -189,7 +206,7 @@ __device__ T lo_ghost(const LevelDev<T>& L, const T* x, int k, int i, int j, T& 
 
 template <typename T, bool THREE>
 __device__ __forceinline__ bool is_ghost_col(const LevelDev<T>& L, int i, int j) {
-    return i == 1 || i == L.Nxg || (THREE && (j == 1 || j == L.Nyg));
+    return i == 1 || i == L.Nxg || (L.per && i == L.Nxg - 1) || (THREE && (j == 1 || j == L.Nyg));
 }
 
 template <typename T, bool THREE, bool CROSS = true>
@@ -243,7 +260,7 @@ __device__ __forceinline__ void residual_point(const LevelDev<T>& L, int64_t p) 
         const bool bot = (k == 1), top = (k == Nzg);
         const int kk = bot ? 2 : (top ? Nzg - 1 : k);
         const T* xp = L.xv + c * Nzg + (kk - 1);
-        const int ox = Nzg, oy = Nzg * Nxg;
+        const int oy = Nzg * Nxg;
         // interior-row coefficients of row kk
         T ih, ca, cb, c3;
         load_cf(L.cf, c, ih, ca, cb, c3);
@@ -268,7 +285,7 @@ __device__ __forceinline__ void residual_point(const LevelDev<T>& L, int64_t p) 
         load_bt8(L.bt, c, bt);
         if (bot) { cm = bt[7]; c0 = bt[0]; cq = bt[1]; cl = bt[2]; cr = bt[3]; cd = bt[4]; cu = bt[5]; }
         if (top) { cm = 0; c0 = 0; cq = 1; cl = 0; cr = 0; cd = 0; cu = 0; }
-        v = cm * xp[-1] + c0 * xp[0] + cq * xp[1] + cl * xp[-ox] + cr * xp[ox];
+        v = cm * xp[-1] + c0 * xp[0] + cq * xp[1] + cl * xp[xoff_l(L, i)] + cr * xp[xoff_r(L, i)];
         if (THREE) v += cd * xp[-oy] + cu * xp[oy];
     }
     L.rv[p] = L.bv[p] - v;
@@ -350,7 +367,7 @@ __device__ __forceinline__ void bottom_item(const LevelDev<T>& L, int64_t q) {
 // `base` (the first column index of the warp).
 template <typename T, bool THREE>
 __device__ __forceinline__ int64_t colour_count(const LevelDev<T>& L) {
-    const int nxi = L.Nxg - 2, nyi = THREE ? L.Nyg - 2 : 1;
+    const int nxi = L.Nxg - 2 - L.per, nyi = THREE ? L.Nyg - 2 : 1;   // periodic: the distinct columns
     const int ni = (nxi + 1) / 2, nj = (L.ncolor == 4) ? (nyi + 1) / 2 : nyi;
     return (int64_t)ni * nj;
 }
@@ -374,7 +391,7 @@ template <typename T, bool THREE, int S, bool CROSS>
 __device__ void colour_warp(const LevelDev<T>& L, int colour, int base, const RowConst<T>& rk) {
     const int Nxg = L.Nxg, Nyg = L.Nyg, Nzg = L.Nzg, R = Nzg - 2;
     const int lane = threadIdx.x & 31, r = lane & (S - 1);
-    const int nxi = Nxg - 2, nyi = THREE ? Nyg - 2 : 1;
+    const int nxi = Nxg - 2 - L.per, nyi = THREE ? Nyg - 2 : 1;
     // columns of this colour: every other i (and every other j with 4 colours)
     const bool four = (L.ncolor == 4);
     const int ni = (nxi + 1) / 2;
@@ -396,7 +413,7 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int base, const Ro
             j = THREE ? 2 + tj : 1;
             i = 2 + 2 * ti + ((colour + j) & 1);    // (i + j) & 1 == colour
         }
-        act = (i <= Nxg - 1) && (!THREE || j <= Nyg - 1);
+        act = (i <= Nxg - 1 - L.per) && (!THREE || j <= Nyg - 1);
     }
     const bool rowact = act && (r < R);
     const int k = r + 2;
@@ -428,10 +445,11 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int base, const Ro
     // the four ghost columns that can touch column (i, j); `pre` selects the
     // ones this column reads, otherwise the ones whose stencil contains it
     auto ghosts = [&](bool post, T xnew, T xfsn) {
-        if (i == 2 || (post && i == 3))
+        // periodic x has no x ghost columns to relax
+        if (!L.per && (i == 2 || (post && i == 3)))
             relax_ghost(colidx(1, j), colidx(2, j), sx(L, 1, 2, 1), colidx(3, j), sx(L, 1, 2, 2), sx(L, 1, 2, 0),
                         i == 2 ? 1 : 2, post, xnew, xfsn);
-        if (i == Nxg - 1 || (post && i == Nxg - 2))
+        if (!L.per && (i == Nxg - 1 || (post && i == Nxg - 2)))
             relax_ghost(colidx(Nxg, j), colidx(Nxg - 2, j), sx(L, 1, Nxg - 1, 0), colidx(Nxg - 1, j),
                         sx(L, 1, Nxg - 1, 1), sx(L, 1, Nxg - 1, 2), i == Nxg - 1 ? 2 : 1, post, xnew, xfsn);
         if (THREE) {
@@ -445,7 +463,7 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int base, const Ro
     };
     if (edge) {
         // 1. identity corner column diagonal to (i, j) (3-D; at most one)
-        if (THREE && (i == 2 || i == Nxg - 1) && (j == 2 || j == Nyg - 1)) {
+        if (THREE && !L.per && (i == 2 || i == Nxg - 1) && (j == 2 || j == Nyg - 1)) {
             const int64_t cc = colidx(i == 2 ? 1 : Nxg, j == 2 ? 1 : Nyg);
             for (int kk = r; kk < Nzg; kk += S) X[cc * Nzg + kk] = B[cc * Nzg + kk];
         }
@@ -466,7 +484,8 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int base, const Ro
     if (act) {
         T ih, ca, cb, c3;
         load_cf(L.cf, (int64_t)c, ih, ca, cb, c3);
-        const T xl = xc[o - ox], xr = xc[o + ox];
+        const int oxl = xoff_l(L, i), oxr = xoff_r(L, i);
+        const T xl = xc[o + oxl], xr = xc[o + oxr];
         const T xd = THREE ? xc[o - oy] : T(0), xu = THREE ? xc[o + oy] : T(0);
         const T x0 = xc[o];
         const T xp = xc[o + 1];                // old value of the row above (row Nzg: free surface)
@@ -477,7 +496,7 @@ __device__ void colour_warp(const LevelDev<T>& L, int colour, int base, const Ro
             load_bt(L.bt, (int64_t)c, btv);
             t0 = btv[0]; t1 = btv[1]; t2 = btv[2]; t3 = btv[3]; t4 = btv[4]; t5 = btv[5]; t6 = btv[6];
             x2o = xc[1]; x3o = xc[2]; bb1 = bc[0];
-            bl = xc[1 - ox]; br = xc[1 + ox];
+            bl = xc[1 + oxl]; br = xc[1 + oxr];
             if (THREE) { bd = xc[1 - oy]; bu = xc[1 + oy]; }
         } else {
             x1 = xc[0];                        // bottom rows are fixed during this pass
@@ -646,10 +665,11 @@ __device__ __forceinline__ void colour_col2(const LevelDev<T>& L, int i, int j, 
         if (!CROSS && r == 0) X[cg * Nzg] = B[cg * Nzg];   // identity level-1 row
     };
     auto ghosts = [&](bool post, T xna, T xnb, T xfsn) {
-        if (i == 2 || (post && i == 3))
+        // periodic x has no x ghost columns to relax
+        if (!L.per && (i == 2 || (post && i == 3)))
             relax_ghost(colidx(1, j), colidx(2, j), sx(L, 1, 2, 1), colidx(3, j), sx(L, 1, 2, 2), sx(L, 1, 2, 0),
                         i == 2 ? 1 : 2, post, xna, xnb, xfsn);
-        if (i == Nxg - 1 || (post && i == Nxg - 2))
+        if (!L.per && (i == Nxg - 1 || (post && i == Nxg - 2)))
             relax_ghost(colidx(Nxg, j), colidx(Nxg - 2, j), sx(L, 1, Nxg - 1, 0), colidx(Nxg - 1, j),
                         sx(L, 1, Nxg - 1, 1), sx(L, 1, Nxg - 1, 2), i == Nxg - 1 ? 2 : 1, post, xna, xnb, xfsn);
         if (THREE) {
@@ -663,7 +683,7 @@ __device__ __forceinline__ void colour_col2(const LevelDev<T>& L, int i, int j, 
     };
     if (!TILE) {
         if (edge) {
-            if (THREE && (i == 2 || i == Nxg - 1) && (j == 2 || j == Nyg - 1)) {
+            if (THREE && !L.per && (i == 2 || i == Nxg - 1) && (j == 2 || j == Nyg - 1)) {
                 const int64_t cc = colidx(i == 2 ? 1 : Nxg, j == 2 ? 1 : Nyg);
                 for (int kk = r; kk < Nzg; kk += S) X[cc * Nzg + kk] = B[cc * Nzg + kk];
             }
@@ -689,9 +709,10 @@ __device__ __forceinline__ void colour_col2(const LevelDev<T>& L, int i, int j, 
             wyd = __ldg(syp); wyc = __ldg(syp + 1); wyu = __ldg(syp + 2);
         }
         // q, g of row kr (x_kr = q - g x_{kr-1})
+        const int oxl = xoff_l(L, i), oxr = xoff_r(L, i);
         auto rowq = [&](int kr, const RowConst<T>& rk, T x0, T xp, T& qo, T& go) {
             const int o = kr - 1;
-            const T xl = xr[o - ox], xrr = xr[o + ox];
+            const T xl = xr[o + oxl], xrr = xr[o + oxr];
             const T xd = THREE ? xr[o - oy] : T(0), xu = THREE ? xr[o + oy] : T(0);
             const T bk = bc[o];
             const T om = rk.om;
@@ -771,7 +792,7 @@ __device__ __forceinline__ void colour_col2(const LevelDev<T>& L, int i, int j, 
                 t0 = btv[0]; t1 = btv[1]; t2 = btv[2]; t3 = btv[3]; t4 = btv[4]; t5 = btv[5]; t6 = btv[6];
             }
             bb1 = bc[0];
-            bl = xr[1 - ox]; br1 = xr[1 + ox];
+            bl = xr[1 + oxl]; br1 = xr[1 + oxr];
             if (THREE) { bd = xr[1 - oy]; bu = xr[1 + oy]; }
             T boff = t0 * xr[1] + t1 * xr[2] + t2 * bl + t3 * br1;
             if (THREE) boff += t4 * bd + t5 * bu;
@@ -815,7 +836,7 @@ __device__ void colour_warp2(const LevelDev<T>& L, int colour, int base, const R
                              const RowConst<T>& rkb) {
     const int Nxg = L.Nxg, Nyg = L.Nyg, Nzg = L.Nzg;
     const int lane = threadIdx.x & 31;
-    const int nxi = Nxg - 2, nyi = THREE ? Nyg - 2 : 1;
+    const int nxi = Nxg - 2 - L.per, nyi = THREE ? Nyg - 2 : 1;   // periodic: the distinct columns
     const bool four = (L.ncolor == 4);
     const int ni = (nxi + 1) / 2;
     const int nj = four ? (nyi + 1) / 2 : nyi;
@@ -832,7 +853,7 @@ __device__ void colour_warp2(const LevelDev<T>& L, int colour, int base, const R
             j = THREE ? 2 + tj : 1;
             i = 2 + 2 * ti + ((colour + j) & 1);
         }
-        act = (i <= Nxg - 1) && (!THREE || j <= Nyg - 1);
+        act = (i <= Nxg - 1 - L.per) && (!THREE || j <= Nyg - 1);
     }
     const int64_t c = (int64_t)(i - 1) + (int64_t)Nxg * (j - 1);
     colour_col2<T, THREE, S, CROSS, false>(L, i, j, act, rka, rkb, L.xv + c * Nzg, Nzg * Nxg, L.bv + c * Nzg,
@@ -887,7 +908,8 @@ __device__ void restrict_item(const LevelDev<T>& F, const LevelDev<T>& Cc, const
         int64_t cc;
         decomp(Cc, p, kc, cc, ic, jc);
         xc[p] = T(0);
-        const bool ghost = kc == 1 || ic == 1 || ic == Cc.Nxg || (gy && (jc == 1 || jc == Cc.Nyg));
+        const bool ghost = kc == 1 || ic == 1 || ic == Cc.Nxg || (Cc.per && ic == Cc.Nxg - 1) ||
+                           (gy && (jc == 1 || jc == Cc.Nyg));
         if (ghost) { rc[p] = T(0); return; }
         const int kf = 2 + (kc - 2) * (1 + zcz), ifn = 2 + (ic - 2) * (1 + xcz), jf = gy ? 2 + (jc - 2) * (1 + ycz) : 1;
         // fine values by 32-bit offsets from (kf, ifn, jf) (levels have < 2^31 points)
@@ -900,7 +922,9 @@ __device__ void restrict_item(const LevelDev<T>& F, const LevelDev<T>& Cc, const
             if (!xcz || k < 2 || k > Nzf || (gy && (j < 2 || j > Nyf + 1))) return R(k, ifn, j);
             const double dW = F.x[ifn - 1] - F.x[ifn - 2], dE = F.x[ifn] - F.x[ifn - 1];
             const T dxc = T(F.ix[ifn - 1]);
-            return (T(0.5) * dxc) * (T(dW) * R(k, ifn - 1, j) + T(dW + dE) * R(k, ifn, j) + T(dE) * R(k, ifn + 1, j));
+            // periodic x: the west neighbour of the first column is the last distinct one
+            const int iw = F.per ? wrap_x(ifn - 1, F.Nxg) : ifn - 1;
+            return (T(0.5) * dxc) * (T(dW) * R(k, iw, j) + T(dW + dE) * R(k, ifn, j) + T(dE) * R(k, ifn + 1, j));
         };
         auto Sxy = [&](int k) -> T {
             if (!ycz || k < 2 || k > Nzf) return Sx(k, jf);
@@ -931,6 +955,7 @@ __device__ void prolong_item(const LevelDev<T>& F, const LevelDev<T>& Cc, const 
     int64_t cfl;
     decomp(F, p, kf, cfl, ifn, jf);
     if (kf == 1 || kf == F.Nzg || ifn == 1 || ifn == F.Nxg || (gy && (jf == 1 || jf == F.Nyg))) return;
+    if (F.per && ifn == F.Nxg - 1) return;   // periodic x: the repeated column stays zero
     const int2 zi = __ldg(reinterpret_cast<const int2*>(F.piz) + (kf - 1));
     const int2 xi = __ldg(reinterpret_cast<const int2*>(F.pix) + (ifn - 1));
     const int2 yi = __ldg(reinterpret_cast<const int2*>(F.piy) + (gy ? jf - 1 : 0));

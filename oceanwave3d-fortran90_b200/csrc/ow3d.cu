@@ -151,6 +151,7 @@ int build_levels(ow3d_handle* H, MgSet<T>& S, bool alloc_fine_x) {
         d.Nx = h.Nx; d.Ny = h.Ny; d.Nz = h.Nz; d.Nxg = h.Nxg; d.Nyg = h.Nyg; d.Nzg = h.Nzg;
         d.N = (int64_t)h.Nxg * h.Nyg * h.Nzg;
         d.ncolor = h.ncolor; d.xc = h.xc; d.yc = h.yc; d.zc = h.zc;
+        d.per = H->G.per;
         d.cross = 0;
         for (size_t q = 0; q < h.hx.size(); ++q) if (h.hx[q] != 0.0 || h.hy[q] != 0.0) { d.cross = 1; break; }
         T *sx, *sy, *sz, *zs, *hh, *hx, *hxx, *hy, *hyy;
@@ -252,6 +253,14 @@ int build_levels(ow3d_handle* H, MgSet<T>& S, bool alloc_fine_x) {
             std::vector<int> ix_, iy_, iz_;
             std::vector<double> wx_, wy_, wz_;
             table(h.x, h.Nxg, hc.xc, false, ix_, wx_);
+            if (H->G.per) {
+                // periodic x: the coarse repeated column holds zero, so the
+                // last distinct fine column interpolates towards coarse
+                // column 2; the fine repeated column takes nothing
+                for (size_t q = 0; q < ix_.size(); ++q)
+                    if (ix_[q] == hc.Nxg - 1) ix_[q] = 2;
+                wx_[2 * (size_t)(h.Nxg - 2)] = 0.0; wx_[2 * (size_t)(h.Nxg - 2) + 1] = 0.0;
+            }
             if (h.Nyg > 1) table(h.y, h.Nyg, hc.yc, false, iy_, wy_);
             else { iy_.assign(2, 1); wy_.assign(2, 0.0); wy_[0] = 1.0; }
             table(h.z, h.Nzg, hc.zc, true, iz_, wz_);
@@ -505,6 +514,7 @@ int solve_device(ow3d_handle* H, const double* rhs, double* phi, const Surface& 
     const bool left = (H->p.krylov == OW3D_KRYLOV_LGMRES);
     launch_krylov_reset(H->ks, H->st);
     int status = OW3D_OK;
+    double r0 = 0, tol = 0;
     for (int cycle = 0; cycle < 1000; ++cycle) {
         // initial residual
         if (!left) {
@@ -515,6 +525,7 @@ int solve_device(ow3d_handle* H, const double* rhs, double* phi, const Surface& 
         }
         launch_norm_init(H->V, N, H->dsc, H->ks, H->p.reltol, H->p.abstol, H->st);
         TRY(sync_ks_small(H));
+        if (cycle == 0) { r0 = H->ks_host->beta; tol = H->ks_host->tol; }
         int j = 0;
         while (!H->ks_host->done) {
             if (!left && H->nlev > 0 && H->graphs && !H->graphs_failed && H->stats.solves > 0) {
@@ -580,6 +591,8 @@ int solve_device(ow3d_handle* H, const double* rhs, double* phi, const Surface& 
     S.max_iterations = std::max(S.max_iterations, it);
     S.last_iterations = it;
     S.last_residual = H->ks_host->resid;
+    S.last_initial_residual = r0;
+    S.last_tolerance = tol;
     if (status == OW3D_NOT_CONVERGED) S.not_converged++;
     CK(cudaGetLastError());
     return status;
@@ -606,6 +619,10 @@ int create_impl(const ow3d_params* p, const double* h, const double* hx, const d
     H->mixed = (p->precision == OW3D_PREC_MIXED);
     int r = build_grid(*p, h, hx, hxx, hy, hyy, H->G, &err);
     if (r) { g_last_error = err; return r; }
+    // the inputs are checked before any device work, so a bad deck is
+    // reported as such on a machine without a GPU too
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { g_last_error = "no CUDA device"; return OW3D_ERR_NO_DEVICE; }
     H->dev = p->device;
     CK(cudaSetDevice(H->dev));
     CK(cudaStreamCreateWithFlags(&H->st, cudaStreamNonBlocking));
@@ -618,11 +635,12 @@ int create_impl(const ow3d_params* p, const double* h, const double* hx, const d
     TRY(upload(H.get(), &H->hy, G.hy)); TRY(upload(H.get(), &H->hyy, G.hyy));
     HoGrid& hg = H->hg;
     hg.Nxg = G.Nxg; hg.Nyg = G.Nyg; hg.Nzg = G.Nzg; hg.gx = G.gx; hg.gy = G.gy; hg.three = G.three;
-    hg.nonlinear = (p->LinearONOFF == 1); hg.SX = H->SX; hg.SY = H->SY; hg.SZ = H->SZ; hg.zs = H->zs;
+    hg.nonlinear = (p->LinearONOFF == 1); hg.per = G.per; hg.SX = H->SX; hg.SY = H->SY; hg.SZ = H->SZ; hg.zs = H->zs;
     hg.h = H->h; hg.hx = H->hx; hg.hxx = H->hxx; hg.hy = H->hy; hg.hyy = H->hyy;
     hg.hSX = G.SX.w.data(); hg.hSY = G.SY.w.data(); hg.hSZ = G.SZ.w.data(); hg.hzs = G.zs.data();
     FsArgs& fa = H->fa;
     fa.Nxg = G.Nxg; fa.Nyg = G.Nyg; fa.Nzg = G.Nzg; fa.three = G.three; fa.nonlinear = hg.nonlinear; fa.g = p->g;
+    fa.per = G.per;
     fa.SX = H->SX; fa.SY = H->SY; fa.SZ = H->SZ; fa.h = H->h;
     H->hmax = *std::max_element(G.h.begin(), G.h.end());
     // multigrid
@@ -948,8 +966,6 @@ int ow3d_create(const ow3d_params* p, const double* h, const double* hx, const d
                 const double* hyy, ow3d_handle** out) {
     if (!out) return OW3D_ERR_BAD_INPUT;
     *out = nullptr;
-    int n = 0;
-    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) { g_last_error = "no CUDA device"; return OW3D_ERR_NO_DEVICE; }
     return create_impl(p, h, hx, hxx, hy, hyy, out);
 }
 
@@ -1080,6 +1096,12 @@ int ow3d_set_state(ow3d_handle* H, const double* E, const double* P, const doubl
     if (P) CK(cudaMemcpyAsync(H->P, P, cb, cudaMemcpyHostToDevice, H->st)); else CK(cudaMemsetAsync(H->P, 0, cb, H->st));
     if (W) CK(cudaMemcpyAsync(H->W, W, cb, cudaMemcpyHostToDevice, H->st)); else CK(cudaMemsetAsync(H->W, 0, cb, H->st));
     if (phi) CK(cudaMemcpyAsync(H->PHI, phi, nb, cudaMemcpyHostToDevice, H->st)); else CK(cudaMemsetAsync(H->PHI, 0, nb, H->st));
+    if (H->G.per) {
+        // periodic x: the image columns of phi stay zero inside the solves
+        // (identity rows), those of W hold the distinct columns' values
+        fs_images(H->fa, H->PHI, H->G.Nzg, 1, H->st);
+        fs_images(H->fa, H->W, 1, 0, H->st);
+    }
     CK(cudaMemsetAsync(H->LP[0], 0, nb, H->st));
     CK(cudaMemsetAsync(H->LP[1], 0, nb, H->st));
     CK(cudaMemsetAsync(H->RHS, 0, nb, H->st));
@@ -1113,6 +1135,17 @@ int ow3d_get_state(ow3d_handle* H, double* E, double* P, double* W, double* phi,
     if (W) CK(cudaMemcpyAsync(W, H->W, cb, cudaMemcpyDeviceToHost, H->st));
     if (phi) CK(cudaMemcpyAsync(phi, H->PHI, nb, cudaMemcpyDeviceToHost, H->st));
     CK(cudaStreamSynchronize(H->st));
+    if (phi && H->G.per) {
+        // periodic x: phi's image columns are filled on output (column 1 <-
+        // Nxg-2, Nxg-1 <- 2, Nxg <- 3); on the device they stay zero
+        const int Nx = H->G.Nxg, Nz = H->G.Nzg;
+        for (int j = 0; j < H->G.Nyg; ++j) {
+            double* r = phi + (size_t)Nz * Nx * j;
+            std::memcpy(r, r + (size_t)Nz * (Nx - 3), sizeof(double) * Nz);
+            std::memcpy(r + (size_t)Nz * (Nx - 2), r + (size_t)Nz * 1, sizeof(double) * Nz);
+            std::memcpy(r + (size_t)Nz * (Nx - 1), r + (size_t)Nz * 2, sizeof(double) * Nz);
+        }
+    }
     if (t) *t = H->time;
     return OW3D_OK;
 }
@@ -1272,6 +1305,7 @@ int kinematics_fields(ow3d_handle* H, double** out) {
 
 int ow3d_kinematics(ow3d_handle* H, double* u, double* v, double* w, double* grads) {
     if (!H) return OW3D_ERR_BAD_INPUT;
+    if (H->G.per) { g_last_error = "ow3d_kinematics: built for wall boundaries, not periodic_x"; return OW3D_ERR_UNSUPPORTED; }
     CK(cudaSetDevice(H->dev));
     double* d = nullptr;
     TRY(kinematics_fields(H, &d));

@@ -7,6 +7,7 @@ namespace ow3d {
 struct FsArgs {
     int Nxg, Nyg, Nzg;
     int three, nonlinear;
+    int per;            // periodic in x: image columns instead of ghost layers
     double g;
     const double* SX;   // [2][Nxg][7]
     const double* SY;   // [2][Nyg][7]
@@ -57,6 +58,9 @@ void fs_relax(const FsArgs& a, const RelaxZoneDev* zones, int nz, double* E, dou
 void fs_derivs(const FsArgs& a, double* E, double* P, double* Ex, double* Exx, double* Px, double* Ey, double* Eyy,
                double* Py, cudaStream_t st);
 void fs_wvel(const FsArgs& a, const double* phi, const double* E, double* W, cudaStream_t st);
+// Periodic x: copy the distinct columns into the image columns of a field
+// with nz values per column (1 <- Nxg-2, Nxg-1 <- 2, Nxg <- 3), or zero them.
+void fs_images(const FsArgs& a, double* v, int nz, int zero, cudaStream_t st);
 void fs_set_rhs(const FsArgs& a, const double* P, double* rhs, cudaStream_t st);
 void fs_extrap(double* phi, const double* lnew, const double* llast, int64_t n, int stage3, cudaStream_t st);
 void fs_filter(const FsArgs& a, const FilterDev& f, double* U, double* tmp, cudaStream_t st);

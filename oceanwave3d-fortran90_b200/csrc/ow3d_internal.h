@@ -40,6 +40,8 @@ struct HoGrid {
     int gx, gy;             // ghost layers present in x / y (0 in a 2-D direction)
     int three;              // 1: 3-D (Nx>1 and Ny>1); 0: 2-D in x (Ny == 1)
     int nonlinear;          // sigma coefficients from eta (LinearONOFF == 1)
+    int per;                // periodic in x: distinct columns 2..Nxg-2, the
+                            // others identity rows (see wrap_x)
     // per-position stencils, [order-1][pos][7], order 1 and 2 (BuildStencilsGridX.f90)
     const double* SX;       // 2*Nxg*7
     const double* SY;       // 2*Nyg*7 (unused in 2-D)
@@ -80,6 +82,7 @@ struct LevelDev {
     int64_t N;
     int ncolor;             // 2 or 4 (multicolour column Gauss-Seidel)
     int cross;              // mixed-derivative terms present (h_x or h_y nonzero on the level)
+    int per;                // periodic in x (never together with cross)
     int xc, yc, zc;         // this level is coarsened w.r.t. the next finer one
     const T* SX;            // [2][Nxg][3]
     const T* SY;            // [2][Nyg][3]
@@ -109,6 +112,16 @@ struct LevelDev {
     T* bv;                  // right-hand side
     T* rv;                  // residual
 };
+
+// Periodic x: the Nx points of a row span one period with both ends, so
+// column Nxg-1 repeats column 2; the distinct columns are 2..Nxg-2 and a
+// column index outside that range is taken cyclically. Ghost column 1,
+// the repeated column Nxg-1 and ghost column Nxg carry identity rows with a
+// zero right-hand side inside every solve.
+__host__ __device__ __forceinline__ int wrap_x(int i, int Nxg) {
+    const int M = Nxg - 3;
+    return i < 2 ? i + M : (i > Nxg - 2 ? i - M : i);
+}
 
 // n / d as a 64-bit multiply-high with m = floor((2^64-1)/d) + 1: exact for
 // every n < 2^48 and 2 <= d < 2^16 (the error term n*(m*d - 2^64) / 2^64 stays

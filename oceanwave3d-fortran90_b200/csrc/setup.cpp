@@ -77,6 +77,23 @@ Stencil stencils_xy(const std::vector<double>& x, int a) {
     return s;
 }
 
+// Periodic direction (no counterpart in the reference): every position takes
+// the centred stencil of half width a, from the exact offsets q*dx.
+Stencil stencils_periodic(const std::vector<double>& x, int a) {
+    Stencil s;
+    s.n = (int)x.size();
+    s.rank = 2 * a + 1;
+    s.w.assign((size_t)2 * s.n * s.rank, 0.0);
+    const double dx = (x[(size_t)s.n - 1] - x[0]) / (double)(s.n - 1);
+    std::vector<double> nodes(s.rank), w(s.rank);
+    for (int m = 0; m < s.rank; ++m) nodes[m] = (double)(m - a) * dx;
+    for (int order = 1; order <= 2; ++order) {
+        fd_weights(0.0, nodes.data(), s.rank - 1, order, w.data());
+        for (int i = 0; i < s.n; ++i) std::copy(w.begin(), w.end(), s.w.begin() + ((size_t)(order - 1) * s.n + i) * s.rank);
+    }
+    return s;
+}
+
 // sigma stencils, one-sided near the free surface and the bottom ghost
 // (PreProcessDiffStencils.f90:108-132).
 Stencil stencils_z(const std::vector<double>& z, int Nz, int gz, int g) {
@@ -190,7 +207,11 @@ int check_params(const ow3d_params& p, std::string* err) {
     if (p.precision != OW3D_PREC_FP64 && p.precision != OW3D_PREC_MIXED) return fail("precision must be 0 or 1");
     if (p.krylov != OW3D_KRYLOV_FGMRES && p.krylov != OW3D_KRYLOV_LGMRES) return fail("krylov must be 0 or 1");
     if (p.GMRESmaxiterations < 1) return fail("GMRESmaxiterations must be >= 1");
-    if (p.periodic_x != 0) return fail("periodic_x: the periodic lateral boundary is not built");
+    if (p.periodic_x != 0) {
+        if (p.Nx < 9) return fail("periodic_x: at least 8 distinct points per period (Nx >= 9)");
+        if (p.PDampingONOFF != 0) return fail("periodic_x: pressure-damping zones need the wall boundaries");
+        if (p.iKinematics != 0) return fail("periodic_x: the kinematics output is built for wall boundaries");
+    }
     return 0;
 }
 
@@ -225,7 +246,14 @@ int build_grid(const ow3d_params& p, const double* h, const double* hx, const do
     cp(h, G.h); cp(hx, G.hx); cp(hxx, G.hxx); cp(hy, G.hy); cp(hyy, G.hyy);
     if (!h) return fail("bathymetry h is required");
     for (size_t c = 0; c < C; ++c) if (!(G.h[c] > 0)) return fail("depth h must be positive everywhere (ghosts included)");
-    G.SX = stencils_xy(G.x, 3);
+    if (p.periodic_x != 0)
+        for (size_t c = 0; c < C; ++c)
+            if (G.hx[c] != 0.0 || G.hy[c] != 0.0) {
+                if (err) *err = "periodic_x: a flat bottom (h_x = h_y = 0) is required";
+                return OW3D_ERR_UNSUPPORTED;
+            }
+    G.per = p.periodic_x != 0 ? 1 : 0;
+    G.SX = G.per ? stencils_periodic(G.x, 3) : stencils_xy(G.x, 3);
     G.SY = stencils_xy(G.y, G.three ? 3 : 0);
     G.SZ = stencils_z(G.z, p.Nz, 1, 3);
     // multigrid hierarchy (MGPreProcess.f90:31-318)
@@ -289,7 +317,7 @@ int build_grid(const ow3d_params& p, const double* h, const double* hx, const do
     for (auto& Lv : G.levels) {
         level_sigma(Lv);
         level_colours(Lv);
-        Lv.SX = stencils_xy(Lv.x, 1);
+        Lv.SX = G.per ? stencils_periodic(Lv.x, 1) : stencils_xy(Lv.x, 1);
         Lv.SY = stencils_xy(Lv.y, G.three ? 1 : 0);
         Lv.SZ = stencils_z(Lv.z, Lv.Nz, 1, 1);
         if (Lv.Nxg < 4 || (G.three && Lv.Nyg < 4) || Lv.Nzg < 4) return fail("multigrid level too small");

@@ -31,6 +31,7 @@ struct GridHost {
     int Nx, Ny, Nz, gx, gy, gz, Nxg, Nyg, Nzg;
     int64_t N, C;
     int three;
+    int per = 0;                    // periodic in x
     std::vector<double> x, y, z, zs;
     std::vector<double> h, hx, hxx, hy, hyy;
     Stencil SX, SY, SZ;             // half width 3
@@ -45,6 +46,7 @@ struct ZoneHost {
 
 void fd_weights(double z, const double* x, int n, int order, double* w);
 Stencil stencils_xy(const std::vector<double>& x, int a);
+Stencil stencils_periodic(const std::vector<double>& x, int a);
 Stencil stencils_z(const std::vector<double>& z, int Nz, int gz, int g);
 
 // Returns 0 or an OW3D_ERR_* code with a message in *err.

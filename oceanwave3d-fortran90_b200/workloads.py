@@ -170,3 +170,28 @@ def stream_function_2d(n_waves=8, ppw=64, Nz=9, kh=1.0, h0=1.0, steepness=0.5, c
     eta = np.array([stream_function_wave(p, x[i0 - 1:i1], t)[0] for t in tt])
     phis = np.array([stream_function_wave(p, x[i0 - 1:i1], t)[1] for t in tt])
     return p, geo, E0, P0, {0: (1, nt, 0.5 * p.dt, eta, phis)}
+
+
+def periodic_wave_2d(Nx=65, Nz=9, kh=1.0, h0=1.0, steepness=0.5, courant=0.5, **kw):
+    """The 2-D periodic stream-function wave: one wavelength L = 2 pi h0 / kh
+    (kh = 1, depth 1 m) periodic in x with Nx points including both ends
+    (x_1 = 0 and x_Nx = L hold the same value), Nz sin-clustered sigma
+    levels, the nonlinear stream-function wave of height steepness x the
+    breaking limit at t = 0, flat bottom, time step at Courant number
+    `courant` on the phase speed. Returns params, geometry, E0, P0 and the
+    wave's (k, L, T, c); the exact solution at time t is the same wave
+    translated, stream_function_wave(params, x, t)."""
+    from . import stream_function_wave
+    L = 2 * np.pi * h0 / kh
+    p = default_params(Nx=Nx, Ny=1, Nz=Nz, Lx=L, Ly=1.0, Lz=h0, GridZ=1, periodic_x=1, **kw)
+    p.IncWaveType = 1
+    p.g = G
+    p.sf_H, p.sf_h, p.sf_L = steepness * breaking_steepness(kh) * L, h0, L
+    p.sf_T, p.sf_wavel_or_per, p.sf_uEorS, p.sf_euler_or_stokes = 0.0, 0, 0.0, 0
+    p.sf_nsteps, p.sf_nmodes = 6, 24
+    _, _, info = stream_function_wave(p, np.zeros(1))
+    p.dt = courant * (L / (Nx - 1)) / info[3]
+    Nxg, Nyg, _ = dims(p)
+    x = (np.arange(Nxg) - 1) * (L / (Nx - 1))
+    E0, P0, _ = stream_function_wave(p, x, 0.0)
+    return p, dict(h=np.full(Nxg * Nyg, h0)), E0, P0, info

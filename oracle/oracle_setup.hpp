@@ -85,6 +85,32 @@ inline Stencil1D build_stencils_xy(const vector<double>& x, int a) {
     return s;
 }
 
+// Periodic direction (no counterpart in the reference, whose lateral rows
+// are walls): every position takes the centred stencil of half width a,
+// formed on the nodes around the middle position of the uniform grid.
+inline Stencil1D build_stencils_periodic(const vector<double>& x, int a) {
+    Stencil1D s; s.n = (int)x.size(); s.rank = 2 * a + 1;
+    s.w.assign((size_t)2 * s.n * s.rank, 0.0);
+    vector<double> w(s.rank);
+    const int mid = s.n / 2;
+    for (int order = 1; order <= 2; ++order) {
+        fd_weights(x[mid], &x[mid - a], s.rank - 1, order, w.data());
+        for (int i = 0; i < s.n; ++i)
+            for (int m = 0; m < s.rank; ++m) s.at(order, i, m) = w[m];
+    }
+    return s;
+}
+
+// Periodic x: the distinct columns are 2..Nxg-2 (1-based, ghosts counted);
+// column Nxg-1 repeats column 2 and the ghost columns 1 and Nxg are unused.
+// wrap_x maps any column index into the distinct range.
+inline int wrap_x(int i, int Nxg) {
+    const int M = Nxg - 3;
+    while (i < 2) i += M;
+    while (i > Nxg - 2) i -= M;
+    return i;
+}
+
 // TaylorFDStencils1DArbitrary (src/functions/TaylorFDStencils1DArbitrary.f90:1-14):
 // alp+bet+1 nodes, expansion at node alp.
 inline void taylor(int alp, int bet, int order, const double* x, double* w) {

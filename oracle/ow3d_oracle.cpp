@@ -37,6 +37,7 @@ struct Level {
     vector<double> LU; vector<int> piv;  // coarsest level dense LU
     int ncolor = 0;
     int cross = 0;            // mixed-derivative terms present (h_x or h_y nonzero)
+    int per = 0;              // periodic in x
     // work vectors for the V-cycle
     vector<double> x, b, r;
 };
@@ -53,6 +54,7 @@ struct Zone {
 struct Sim {
     ow3d_params p;
     int mode = 0;
+    int per = 0;                         // periodic in x (params.periodic_x)
     int gx, gy, gz, Nxg, Nyg, Nzg, N, C, dimcase;
     LevelGrid fine;                      // fine grid + bathymetry
     Stencil1D SX, SY, SZ;                // high-order stencils
@@ -80,6 +82,27 @@ struct Sim {
 
 static inline size_t gid(const Sim& s, int k, int i, int j) {  // 1-based -> 0-based
     return (size_t)(k - 1) + (size_t)s.Nzg * ((size_t)(i - 1) + (size_t)s.Nxg * (size_t)(j - 1));
+}
+
+// Periodic x: copy the distinct columns into the image columns of a field of
+// nz values per column -- column 1 <- Nxg-2, Nxg-1 <- 2, Nxg <- 3.
+static void images_x(const Sim& s, double* v, int nz) {
+    const int Nx = s.Nxg;
+    for (int j = 1; j <= s.Nyg; ++j) {
+        double* r = v + (size_t)nz * Nx * (j - 1);
+        for (int k = 0; k < nz; ++k) {
+            r[(size_t)nz * 0 + k] = r[(size_t)nz * (Nx - 3) + k];
+            r[(size_t)nz * (Nx - 2) + k] = r[(size_t)nz * 1 + k];
+            r[(size_t)nz * (Nx - 1) + k] = r[(size_t)nz * 2 + k];
+        }
+    }
+}
+static void zero_images_x(const Sim& s, double* v, int nz) {
+    const int Nx = s.Nxg;
+    for (int j = 1; j <= s.Nyg; ++j) {
+        double* r = v + (size_t)nz * Nx * (j - 1);
+        for (int k = 0; k < nz; ++k) r[k] = r[(size_t)nz * (Nx - 2) + k] = r[(size_t)nz * (Nx - 1) + k] = 0.0;
+    }
 }
 
 // ---------------------------------------------------------------- grids
@@ -204,7 +227,7 @@ static void assemble_level(const Sim& s, Level& Lv) {
     const LevelGrid& G = Lv.G;
     const int a = p.alphaprecond, b = p.betaprecond, g = p.gammaprecond;
     const int Nxg = G.Nxg, Nyg = G.Nyg, Nzg = G.Nzg;
-    Lv.SX = build_stencils_xy(G.x, a);
+    Lv.SX = s.per ? build_stencils_periodic(G.x, a) : build_stencils_xy(G.x, a);
     Lv.SY = build_stencils_xy(G.y, b);
     Lv.SZ = build_stencils_z(G.z, G.Nz, s.gz, g);
     CrossTables T = build_cross_tables(G, Lv.SX, Lv.SY, Lv.SZ, g, s.gx, s.gy, s.gz);
@@ -220,6 +243,10 @@ static void assemble_level(const Sim& s, Level& Lv) {
     // Full-rank 1-D stencils of PrepareFullOperatorStencils, as (col,val) lists.
     auto DX = [&](int k, int i, int j, int order, double f, RowAcc& R) {
         if (Nxg == 1) return;
+        if (s.per) {   // centred, cyclic
+            for (int m = 0; m <= 2 * a; ++m) R.add(L(k, wrap_x(i + (m - a), Nxg), j), f * Lv.SX.at(order, i - 1, m));
+            return;
+        }
         int da = diff(i, a, Nxg);
         for (int m = 0; m <= 2 * a; ++m) R.add(L(k, i + (m - a) + da, j), f * Lv.SX.at(order, i - 1, m));
     };
@@ -303,6 +330,7 @@ static void assemble_level(const Sim& s, Level& Lv) {
                     DZ(k, i, j, 2, sg[3] * sg[3] + sg[4] * sg[4], P);
                 }
                 for (size_t t = 0; t < P.cols.size(); ++t) R.add(P.cols[t], P.vals[t]);
+                if (s.per) continue;   // periodic levels have no mixed-derivative terms (flat bottom)
                 if (three || xonly) DXZ(k, i, j, 2.0 * sg[1], R);
                 if (three || yonly) DYZ(k, i, j, 2.0 * sg[3], R);
             }
@@ -330,6 +358,10 @@ static void assemble_level(const Sim& s, Level& Lv) {
     } else if (gy == 1 && Nxg == 1) {
         ident(1, 1, 1); ident(1, 1, Nyg);
     }
+    if (s.per)   // ghost columns and the repeated column: identity rows
+        for (int j = 1; j <= Nyg; ++j)
+            for (int k = 1; k <= Nzg; ++k)
+                for (int i : {1, Nxg - 1, Nxg}) { rows[L(k, i, j) - 1].clear(); ident(k, i, j); }
     // CSR, diagonal first
     CSR& A = Lv.A; A.n = n; A.rp.assign(n + 1, 0);
     for (int r = 0; r < n; ++r) A.rp[r + 1] = A.rp[r] + (int)rows[r].cols.size();
@@ -345,6 +377,7 @@ static void assemble_level(const Sim& s, Level& Lv) {
     double hmax = 0; for (size_t c = 0; c < G.hx.size(); ++c) hmax = std::max(hmax, std::max(std::fabs(G.hx[c]), std::fabs(G.hy[c])));
     Lv.ncolor = (Nyg > 1 && Nxg > 1) ? (hmax > 0 ? 4 : 2) : 2;
     Lv.cross = hmax > 0 ? 1 : 0;
+    Lv.per = s.per;
 }
 
 static void dense_lu(Level& Lv) {
@@ -430,13 +463,26 @@ static void dm_pass(const Level& Lv, int colour, double* x, const double* b) {
         for (int k = k0; k <= k1; ++k) gs_row(Lv.A, (k - 1) + Nzg * ((i - 1) + Nxg * (j - 1)), x, b);
     };
     const int j0 = three ? 2 : 1, j1 = three ? Nyg - 1 : 1;
+    const bool per = Lv.per != 0;
+    const int ilast = per ? Nxg - 2 : Nxg - 1;   // periodic: the distinct columns only
     // the tasks of one colour read nothing another task of the colour writes,
     // so rows of tasks run in parallel with the same result as in sequence
 #pragma omp parallel for schedule(static) if (three)
     for (int j = j0; j <= j1; ++j)
-        for (int i = 2; i <= Nxg - 1; ++i) {
+        for (int i = 2; i <= ilast; ++i) {
             const int col = (Lv.ncolor == 4) ? ((i & 1) + 2 * (j & 1)) : ((i + j) & 1);
             if (col != colour) continue;
+            if (per) {
+                // no x ghost columns; the y ghost columns as usual
+                const int g0 = fuse_bottom ? 1 : 2;
+                if (three && j == 2) col_rows(i, 1, g0, Nzg);
+                if (three && j == Nyg - 1) col_rows(i, Nyg, g0, Nzg);
+                col_rows(i, j, fuse_bottom ? 1 : 2, Nzg);
+                if (fuse_bottom) col_rows(i, j, 1, 1);
+                if (three && (j == 2 || j == 3)) col_rows(i, 1, g0, Nzg);
+                if (three && (j == Nyg - 1 || j == Nyg - 2)) col_rows(i, Nyg, g0, Nzg);
+                continue;
+            }
             if (three) {
                 const int cis[2] = {i == 2 ? 1 : 0, i == Nxg - 1 ? Nxg : 0};
                 const int cjs[2] = {j == 2 ? 1 : 0, j == Nyg - 1 ? Nyg : 0};
@@ -491,13 +537,17 @@ static void restrict_(const Sim& s, const Level& Fl, const Level& Cl, const doub
     const double half = 0.5, one = 1.0;
     // each sweep writes the points of one parity from the other parity only
     if (xc) {
+        // periodic x: the west neighbour of the first column is the last
+        // distinct column (same spacing), and the repeated column is skipped
+        const int ilast = s.per ? Nxf + s.gx - 1 : Nxf + s.gx;
 #pragma omp parallel for schedule(static)
-        for (int ifn = 1 + s.gx; ifn <= Nxf + s.gx; ifn += 2) {
+        for (int ifn = 1 + s.gx; ifn <= ilast; ifn += 2) {
             double dW = F.x[ifn - 1] - F.x[ifn - 2], dE = F.x[ifn] - F.x[ifn - 1];
             double dxc = one / (dW + dE);
+            const int iw = s.per ? wrap_x(ifn - 1, F.Nxg) : ifn - 1;
             for (int kf = 1 + s.gz; kf <= Nzf + s.gz - 1; ++kf)
                 for (int jf = 1 + s.gy; jf <= Nyf + s.gy; ++jf)
-                    t[I(kf, ifn, jf)] = (half * dxc) * (dW * t[I(kf, ifn - 1, jf)] + (dW + dE) * t[I(kf, ifn, jf)] + dE * t[I(kf, ifn + 1, jf)]);
+                    t[I(kf, ifn, jf)] = (half * dxc) * (dW * t[I(kf, iw, jf)] + (dW + dE) * t[I(kf, ifn, jf)] + dE * t[I(kf, ifn + 1, jf)]);
         }
     }
     if (yc) {
@@ -526,7 +576,8 @@ static void restrict_(const Sim& s, const Level& Fl, const Level& Cl, const doub
         for (int ic = 1 + s.gx; ic <= Nxc + s.gx; ++ic)
             for (int kc = 1 + s.gz; kc <= Nzc + s.gz; ++kc) {
                 int kf = 1 + s.gz + (kc - 1 - s.gz) * (1 + zc), ifn = 1 + s.gx + (ic - 1 - s.gx) * (1 + xc), jf = 1 + s.gy + (jc - 1 - s.gy) * (1 + yc);
-                rc[(size_t)(kc - 1) + (size_t)Cg.Nzg * ((size_t)(ic - 1) + (size_t)Cg.Nxg * (jc - 1))] = t[I(kf, ifn, jf)];
+                rc[(size_t)(kc - 1) + (size_t)Cg.Nzg * ((size_t)(ic - 1) + (size_t)Cg.Nxg * (jc - 1))] =
+                    (s.per && ic == Cg.Nxg - 1) ? 0.0 : t[I(kf, ifn, jf)];
             }
 }
 
@@ -550,8 +601,10 @@ static void prolong_(const Sim& s, const Level& Fl, const Level& Cl, double* pf,
         for (int jf = 1 + s.gy; jf <= Nyf + s.gy; jf += YF)
             for (int ifn = 2 + s.gx; ifn <= Nxf + s.gx; ifn += XF) {
                 double dW = F.x[ifn - 1] - F.x[ifn - 2], dE = F.x[ifn] - F.x[ifn - 1], dxf = one / (dW + dE);
+                // periodic x: the repeated column holds zero, its value is column 2's
+                const int ie = (s.per && ifn + 1 == F.Nxg - 1) ? 2 : ifn + 1;
                 for (int kf = 1 + s.gz; kf <= Nzf + s.gz - 1; kf += ZF)
-                    pf[I(kf, ifn, jf)] = (dE * pf[I(kf, ifn - 1, jf)] + dW * pf[I(kf, ifn + 1, jf)]) * dxf;
+                    pf[I(kf, ifn, jf)] = (dE * pf[I(kf, ifn - 1, jf)] + dW * pf[I(kf, ie, jf)]) * dxf;
             }
     }
     if (YF == 2) {
@@ -618,6 +671,19 @@ static void precond(Sim& s, const double* r, double* u) {
 // DiffXEven.f90, DiffYEven.f90, DiffZArbitrary.f90 on a (Nz,Nx,Ny) array.
 static void diff_x(const Sim& s, const double* v, double* o, int order, int Nz) {
     int a = s.p.alpha, rank = 2 * a + 1, Nx = s.Nxg, Ny = s.Nyg;
+    if (s.per) {
+        // centred stencils on the distinct columns, indices taken cyclically
+        for (int j = 1; j <= Ny; ++j)
+            for (int i = 2; i <= Nx - 2; ++i)
+                for (int k = 1; k <= Nz; ++k) {
+                    double acc = 0;
+                    for (int m = 0; m < rank; ++m)
+                        acc += s.SX.at(order, i - 1, m) * v[(size_t)(k - 1) + (size_t)Nz * ((size_t)(wrap_x(i - a + m, Nx) - 1) + (size_t)Nx * (j - 1))];
+                    o[(size_t)(k - 1) + (size_t)Nz * ((size_t)(i - 1) + (size_t)Nx * (j - 1))] = acc;
+                }
+        images_x(s, o, Nz);
+        return;
+    }
 #pragma omp parallel for schedule(static) if (Ny > 1)
     for (int j = 1; j <= Ny; ++j)
         for (int i = 1; i <= Nx; ++i) {
@@ -661,7 +727,12 @@ static void matvec_ho(Sim& s, const double* phi, double* out) {
     vector<double> dpdx(N, 0), ddpdxx(N, 0), dpdy(N, 0), ddpdyy(N, 0), dpds(N), ddpdss(N), tmp(N), ddpdsdx(N, 0), ddpdsdy(N, 0);
     const double* dsg = s.dsig.data();
     auto DS = [&](int k, int i, int j, int c) { return dsg[gid(s, k, i, j) * 5 + (c - 1)]; };
-    if (Nx > 1) {
+    if (Nx > 1 && s.per) {
+        // no lateral walls: the mixed derivative is D_sigma(D_x phi) with the
+        // centred x stencil at every level (no shifted windows)
+        diff_x(s, phi, dpdx.data(), 1, Nz); diff_x(s, phi, ddpdxx.data(), 2, Nz);
+        diff_z(s, dpdx.data(), ddpdsdx.data(), 1);
+    } else if (Nx > 1) {
         diff_x(s, phi, dpdx.data(), 1, Nz); diff_x(s, phi, ddpdxx.data(), 2, Nz);
 #pragma omp parallel for schedule(static)
         for (int j = 1; j <= Ny; ++j) for (int i = 1; i <= Nx; ++i) for (int k = 1; k <= Nz; ++k) {
@@ -746,6 +817,9 @@ static void matvec_ho(Sim& s, const double* phi, double* out) {
     }
     if (gx == 1 && Ny == 1) { id_(1, 1, 1); id_(1, Nx, 1); }
     if (gy == 1 && Nx == 1) { id_(1, 1, 1); id_(1, 1, Ny); }
+    if (s.per)   // the ghost columns and the repeated column are identity rows
+        for (int j = 1; j <= Ny; ++j)
+            for (int k = 1; k <= Nz; ++k) { id_(k, 1, j); id_(k, Nx - 1, j); id_(k, Nx, j); }
 }
 
 // DetermineTransformationConstantsArray for the surface state (E..Eyy).
@@ -998,7 +1072,11 @@ static void ghost_y(const Sim& s, double* v, const double* S) {
 // DifferentiationsFreeSurfacePlane.f90:13-32 (Cartesian branch)
 static void fs_derivs(Sim& s, vector<double>& E, vector<double>& P, vector<double>& Ex, vector<double>& Exx,
                       vector<double>& Px, vector<double>& Ey, vector<double>& Eyy, vector<double>& Py) {
-    if (s.p.Nx > 1) {
+    if (s.per) {
+        // periodic x: image columns in place of the ghost-layer update
+        images_x(s, E.data(), 1); dx2(s, E.data(), Ex.data(), 1); dx2(s, E.data(), Exx.data(), 2);
+        images_x(s, P.data(), 1); dx2(s, P.data(), Px.data(), 1);
+    } else if (s.p.Nx > 1) {
         ghost_x(s, E.data(), s.sEx.data()); dx2(s, E.data(), Ex.data(), 1); dx2(s, E.data(), Exx.data(), 2);
         ghost_x(s, P.data(), s.sPx.data()); dx2(s, P.data(), Px.data(), 1);
     }
@@ -1015,6 +1093,7 @@ static void vertical_velocity(Sim& s, vector<double>& W) {
         for (int m = 0; m < rank; ++m) acc += s.SZ.at(1, Nz - 1, m) * s.PHI[(size_t)c * Nz + (Nz - 2 * g + m) - 1];
         W[c] = s.dsig[((size_t)c * Nz + Nz - 1) * 5 + 4] * acc;
     }
+    if (s.per) images_x(s, W.data(), 1);
 }
 // rhsFreeSurface3D.f90:12-28, rhsLinearFreeSurface3D.f90
 static void fs_rhs(const Sim& s, const vector<double>& E, const vector<double>& P, const vector<double>& W,
@@ -1091,7 +1170,17 @@ static void relax(Sim& s, vector<double>& E, vector<double>& P, double RKtime, d
 static void filter(Sim& s, vector<double>& U) {
     int Nx = s.Nxg, Ny = s.Nyg, al = s.p.filterALPHA, NP = s.NP, gx = s.gx, gy = s.gy;
     auto F2 = [&](int m, int i) { return s.fc2[(size_t)(i - 1) * NP + (m - 1)]; };  // (NP x alpha) view
-    if (Nx > 1) {
+    if (Nx > 1 && s.per) {
+        // periodic x: the centred filter on every distinct column, cyclic
+        vector<double> t = U;
+        for (int j = 1 + gy; j <= Ny - gy; ++j)
+            for (int i = 2; i <= Nx - 2; ++i) {
+                double a = 0;
+                for (int m = 1; m <= NP; ++m) a += t[(size_t)(wrap_x(i - al + m - 1, Nx) - 1) + (size_t)Nx * (j - 1)] * s.fc[m - 1];
+                U[(size_t)(i - 1) + (size_t)Nx * (j - 1)] = a;
+            }
+        images_x(s, U.data(), 1);
+    } else if (Nx > 1) {
         vector<double> t = U;
         for (int j = 1 + gy; j <= Ny - gy; ++j) {
             auto T = [&](int i) { return t[(size_t)(i - 1) + (size_t)Nx * (j - 1)]; };
@@ -1312,6 +1401,7 @@ static int rk4_step(Sim& s) {
         if (s.gx == 1)
             for (int j = 1 + s.gy; j <= s.Nyg - s.gy; ++j)
                 for (int k = 1; k <= Nz; ++k) { s.RHS[gid(s, k, 1, j)] = 0.0; s.RHS[gid(s, k, s.Nxg, j)] = 0.0; }
+        if (s.per) zero_images_x(s, s.RHS.data(), Nz);   // identity rows of the image columns
     };
     auto sigma_for = [&](const vector<double>& E, const vector<double>& Ex, const vector<double>& Exx,
                          const vector<double>& Ey, const vector<double>& Eyy) {
@@ -1400,7 +1490,8 @@ static Sim* create(const ow3d_params* p, const double* h, const double* hx, cons
     LevelGrid& G = s->fine;
     G.h.assign(h, h + s->C); G.hx.assign(hx, hx + s->C); G.hxx.assign(hxx, hxx + s->C);
     G.hy.assign(hy, hy + s->C); G.hyy.assign(hyy, hyy + s->C);
-    s->SX = build_stencils_xy(G.x, p->alpha);
+    s->per = (p->periodic_x != 0) ? 1 : 0;
+    s->SX = s->per ? build_stencils_periodic(G.x, p->alpha) : build_stencils_xy(G.x, p->alpha);
     s->SY = build_stencils_xy(G.y, p->beta);
     s->SZ = build_stencils_z(G.z, p->Nz, s->gz, p->gamma);
     s->T = build_cross_tables(G, s->SX, s->SY, s->SZ, p->gamma, s->gx, s->gy, s->gz);
@@ -1486,6 +1577,7 @@ void orc_set_state(void* sv, const double* E, const double* P, const double* W, 
     Sim* s = (Sim*)sv;
     if (E) s->E.assign(E, E + s->C); if (P) s->P.assign(P, P + s->C); if (W) s->W.assign(W, W + s->C);
     if (phi) s->PHI.assign(phi, phi + s->N); else std::fill(s->PHI.begin(), s->PHI.end(), 0.0);
+    if (s->per) { zero_images_x(*s, s->PHI.data(), s->Nzg); if (W) images_x(*s, s->W.data(), 1); }
     std::fill(s->LASTPHI0.begin(), s->LASTPHI0.end(), 0.0); std::fill(s->LASTPHI1.begin(), s->LASTPHI1.end(), 0.0);
     s->time = t; s->tstep = 0;
     // OceanWave3DT0Setup.f90:444,564-569: surface derivatives; linear case keeps eta = 0 coefficients.
@@ -1495,7 +1587,11 @@ void orc_set_state(void* sv, const double* E, const double* P, const double* W, 
 void orc_get_state(void* sv, double* E, double* P, double* W, double* phi, double* t) {
     Sim* s = (Sim*)sv;
     if (E) std::copy(s->E.begin(), s->E.end(), E); if (P) std::copy(s->P.begin(), s->P.end(), P);
-    if (W) std::copy(s->W.begin(), s->W.end(), W); if (phi) std::copy(s->PHI.begin(), s->PHI.end(), phi);
+    if (W) std::copy(s->W.begin(), s->W.end(), W);
+    if (phi) {
+        std::copy(s->PHI.begin(), s->PHI.end(), phi);
+        if (s->per) images_x(*s, phi, s->Nzg);   // periodic: image columns filled on output
+    }
     if (t) *t = s->time;
 }
 void orc_get_derivs(void* sv, double* Ex, double* Exx, double* Px, double* Ey, double* Eyy, double* Py) {

@@ -1,0 +1,110 @@
+"""Whole runs of the benchmark configurations on the device against the
+oracle's whole-run fixtures (tests/golden/run_*.npz, made by
+``make_golden.py --fullrun``; the oracle needs minutes for them, so they are
+stored rather than recomputed here):
+
+* the shoal basin, 257 x 33 x 9, 1000 RK4 steps with its generation zone and
+  sponge (reltol 1e-8, abstol 1e-6 as in the example decks), FP64;
+* the 2-D stream-function wave (kh = 1, half the breaking steepness) in the
+  wall-bounded flume with generation and sponge, 257 x 9, 200 RK4 steps.
+
+Against the device-ordered oracle (_dev: the same multicolour smoother and
+FGMRES variant): 1e-10 relative L-infinity on eta, P and phi after the whole
+run, and every step's matvec count within 4 (one per solve) of the oracle's.
+
+Against the reference-ordered oracle (_ref: lexicographic Gauss-Seidel and
+left-preconditioned GMRES with modified Gram-Schmidt, the order of
+GaussSeidel.f90 and iterative_solution.f90): the two algorithms stop at the
+same tolerance from different iterates, so the whole-run difference is of
+the order of the solver tolerance, not of rounding. The tests bound it
+(REF_TOL) and check the matvec totals of the whole run against the
+reference's (REF_ITER_FRAC).
+"""
+import pathlib
+
+import numpy as np
+import pytest
+
+import cases
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = pathlib.Path(__file__).resolve().parent / "golden"
+RTOL_RUN = 1e-10
+# reference ordering: relative L-infinity bound after the whole run, and the
+# relative difference of the run's matvec total (measured values are stated
+# in the assertion messages)
+REF_TOL = {"shoal": 1e-5, "sfwave": 1e-5}
+REF_ITER_FRAC = 0.6
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def load(name):
+    with np.load(GOLDEN / f"{name}.npz") as z:
+        return {k: z[k] for k in z.files}
+
+
+def _check_dev(sim, g, its):
+    E, P, W, phi, t = sim.get_state()
+    assert abs(t - float(g["t"][0])) < 1e-9
+    errs = {"E": rel(E, g["E"]), "P": rel(P, g["P"]), "phi": rel(phi, g["phi"])}
+    assert max(errs.values()) < RTOL_RUN, errs
+    d = np.abs(its - g["step_iterations"])
+    assert np.all(d <= 4), (int(d.max()), int(np.argmax(d)))
+
+
+def _check_ref(sim, g, its, tol):
+    E, P, W, phi, t = sim.get_state()
+    errs = {"E": rel(E, g["E"]), "P": rel(P, g["P"]), "phi": rel(phi, g["phi"])}
+    assert max(errs.values()) < tol, errs
+    tot, ref = int(its.sum()), int(g["step_iterations"].sum())
+    assert abs(tot - ref) <= REF_ITER_FRAC * ref, (tot, ref)
+    return errs, tot, ref
+
+
+def _shoal(ow3d, krylov=0):
+    W = ow3d.workloads
+    p, geo, target = cases.shoal_generation(W, 1000, krylov=krylov)
+    sim = ow3d.Simulation(p, **geo)
+    sim.set_relax_target(0, *target(sim.zone_box(0)))
+    sim.set_state(np.zeros(sim.C), np.zeros(sim.C))
+    return sim, cases.run_steps(sim, 1000)
+
+
+def _sfwave(ow3d, krylov=0):
+    W = ow3d.workloads
+    p, geo, E0, P0, targets = W.stream_function_2d(ppw=32, steps=200, krylov=krylov)
+    sim = ow3d.Simulation(p, **geo)
+    sim.set_state(E0, P0)
+    sim.set_relax_target(0, *targets[0])
+    return sim, cases.run_steps(sim, 200)
+
+
+def test_shoal_1000_steps_matches_device_ordered_oracle(ow3d):
+    sim, its = _shoal(ow3d)
+    _check_dev(sim, load("run_shoal_257x33x9_1000_dev"), its)
+    assert np.max(np.abs(sim.get_state()[0])) > 1e-3     # the wave crossed the basin
+
+
+def test_sfwave_200_steps_matches_device_ordered_oracle(ow3d):
+    sim, its = _sfwave(ow3d)
+    _check_dev(sim, load("run_sfwave_257x9_200_dev"), its)
+
+
+@pytest.mark.parametrize("krylov", [0, 1], ids=["fgmres", "left_gmres"])
+def test_shoal_1000_steps_against_reference_ordering(ow3d, krylov):
+    sim, its = _shoal(ow3d, krylov)
+    errs, tot, ref = _check_ref(sim, load("run_shoal_257x33x9_1000_ref"), its, REF_TOL["shoal"])
+    print(f"shoal 1000 steps, {'FGMRES' if krylov == 0 else 'left GMRES'} vs reference ordering: "
+          f"rel err {errs}, matvecs {tot} vs {ref}")
+
+
+@pytest.mark.parametrize("krylov", [0, 1], ids=["fgmres", "left_gmres"])
+def test_sfwave_200_steps_against_reference_ordering(ow3d, krylov):
+    sim, its = _sfwave(ow3d, krylov)
+    errs, tot, ref = _check_ref(sim, load("run_sfwave_257x9_200_ref"), its, REF_TOL["sfwave"])
+    print(f"stream-function flume 200 steps, {'FGMRES' if krylov == 0 else 'left GMRES'} vs reference "
+          f"ordering: rel err {errs}, matvecs {tot} vs {ref}")
