@@ -342,9 +342,23 @@ def profile_step(args):
     kw = dict(WORKLOAD)
     if args.grid:
         kw = dict(zip(("Nx", "Ny", "Nz"), (int(v) for v in args.grid.lower().split("x"))))
-    p, geo, E0, P0 = pkg.workloads.irregular_sea(**kw, precision=(1 if args.profile == "mixed" else 0))
-    sim = pkg.Simulation(p, **geo)
-    sim.set_state(E0, P0)
+    prec = 1 if args.profile == "mixed" else 0
+    if args.profile_workload == "shoal":
+        # sloping bottom: multigrid levels with mixed-derivative terms, the
+        # generation zone and the sponge
+        sys.path.insert(0, str(ROOT / "tests"))
+        import cases
+        p, geo, target = cases.shoal_generation(pkg.workloads, 4, precision=prec)
+        sim = pkg.Simulation(p, **geo)
+        sim.set_relax_target(0, *target(sim.zone_box(0)))
+        Nxg, Nyg, _ = pkg.dims(p)
+        x, y = pkg.workloads.grid_xy(p)
+        E0 = np.tile(0.004 * np.cos(2 * np.pi * x / 1.56), Nyg)
+        sim.set_state(E0, np.zeros_like(E0))
+    else:
+        p, geo, E0, P0 = pkg.workloads.irregular_sea(**kw, precision=prec)
+        sim = pkg.Simulation(p, **geo)
+        sim.set_state(E0, P0)
     sim.step(1)
     st, ms = sim.step_timed(1)
     s = sim.stats()
@@ -400,6 +414,8 @@ def main():
     ap.add_argument("--profile", choices=["fp64", "mixed"], default=None,
                     help="profiling driver: one warm-up step then one step of the workload, no JSON line")
     ap.add_argument("--grid", default=None, help="NXxNYxNZ override for --profile (e.g. 257x65x17)")
+    ap.add_argument("--profile-workload", choices=["sea", "shoal"], default="sea",
+                    help="--profile workload: the irregular sea, or the 257x33x9 shoal basin (sloping bottom)")
     ap.add_argument("--config", choices=["sea", "largest"], default="sea",
                     help="largest: the 2049x513x9 instance at three GMRES tolerances (one JSON line each)")
     args = ap.parse_args()

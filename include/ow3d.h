@@ -385,22 +385,31 @@ int ow3d_step_timed(ow3d_handle* h, int nsteps, double* device_ms);
 
 /* Advance n independent simulations together -- no counterpart in the
  * reference, which runs one simulation per process. Handle i takes nsteps[i]
- * RK4 steps; one host thread drives each handle's stream, so their kernels
- * overlap on the device. status[i] and wall_ms[i] (either may be NULL)
- * receive each handle's ow3d_step status and host wall time in milliseconds.
- * The handles must be distinct. Returns the most severe status. Each result
- * is the same as ow3d_step on that handle alone (handles share no state). */
+ * RK4 steps, in lock-step rounds driven by the calling thread: each round
+ * launches one step of every handle with steps left as that handle's step
+ * graph on its own stream (see ow3d_set_graphs; handles that cannot use
+ * graphs step directly meanwhile), then waits for them, so the simulations'
+ * kernels overlap on the device. status[i] and wall_ms[i] (either may be
+ * NULL) receive each handle's ow3d_step status and the host time in
+ * milliseconds from the call's start to the end of its last step. The
+ * handles must be distinct. Returns the most severe status. Each result is
+ * the same as ow3d_step on that handle alone (handles share no state). */
 int ow3d_step_batch(ow3d_handle* const* hs, int n, const int* nsteps, int* status, double* wall_ms);
 
 int ow3d_get_stats(const ow3d_handle* h, ow3d_stats* s);
 int ow3d_reset_stats(ow3d_handle* h);
 
-/* 1 (the default): from the handle's second solve on, each Arnoldi step of
- * the FGMRES solve with the multigrid preconditioner (V-cycle, operator,
- * orthogonalisation) is one CUDA graph launch, captured on first use per
- * step index and surface arrays; 0: kernels are launched one by one. The
- * left-preconditioned variant always launches directly. Results are the
- * same either way. */
+/* 1 (the default): with FGMRES and the multigrid preconditioner, from the
+ * second RK4 step on every step is one CUDA graph launch (one graph per
+ * parity of the step number, captured on first use): each of its four
+ * solves is the initial residual, one conditional node per Arnoldi step --
+ * enabled on the device by the previous step's stopping test -- and the
+ * solution update, so the host waits once per step. Before that (and in
+ * ow3d_solve), from the handle's second solve on, each Arnoldi step is one
+ * graph launch. 0: kernels are launched one by one. The left-preconditioned
+ * variant and decks with a pressure-damping zone always launch directly;
+ * ow3d_set_relax_target drops the step graphs (they hold the target table).
+ * Results are bitwise the same either way. */
 int ow3d_set_graphs(ow3d_handle* h, int on);
 
 /* Zone-box of relaxation zone `zone` in 1-based ghost-inclusive indices. */

@@ -67,6 +67,10 @@ int ow3d_test_set_colour_tiles(int min_tiles);
  * capture failed and the handle launches kernels directly. */
 int ow3d_test_graph_count(const ow3d_handle* h);
 
+/* Number of whole-step graphs the handle holds (0..2, one per step parity),
+ * or -1 when a step capture failed and the handle steps directly. */
+int ow3d_test_step_graph_count(const ow3d_handle* h);
+
 /* Device time of `reps` launches of one kernel on this handle's stream,
  * measured with CUDA events around each launch; before each launch a write of
  * the Krylov basis (larger than L2) evicts the inputs from L2, outside the

@@ -62,6 +62,7 @@ def lib():
         L.ow3d_test_set_coop_max_points.restype = _C.c_longlong
         L.ow3d_test_set_colour_tiles.argtypes = [_C.c_int]
         L.ow3d_test_graph_count.argtypes = [_C.c_void_p]
+        L.ow3d_test_step_graph_count.argtypes = [_C.c_void_p]
         _lib = L
     return _lib
 

@@ -121,7 +121,10 @@ __global__ void k_rk_final(FsArgs a, double* E, double* P, const double* k1E, co
     }
 }
 
-__global__ void k_relax(FsArgs a, RelaxZoneDev z, double* E, double* P, double FAC, double RKtime, double time) {
+__global__ void k_relax(FsArgs a, RelaxZoneDev z, double* E, double* P, const StepDev* sd, double off,
+                        double transient) {
+    const double time = sd->time, RKtime = time + off;
+    const double FAC = (RKtime < transient) ? RKtime / transient : 1.0;   // RelaxationModule_new.f90:23-27
     const int bx = z.i1 - z.i0 + 1, by = z.j1 - z.j0 + 1;
     const int64_t box = (int64_t)bx * by;
     const double* te = nullptr; const double* tp = nullptr;
@@ -306,17 +309,30 @@ __global__ void k_set_rhs(FsArgs a, const double* __restrict__ P, double* __rest
 }
 
 __global__ void k_extrap(double* __restrict__ phi, const double* __restrict__ lnew, const double* __restrict__ llast,
-                         int64_t n, int stage3) {
+                         int64_t n, int stage3, const StepDev* sd) {
+    if (stage3 && sd->tstep <= 1) return;   // Runge_Kutta_4.f90:294 (tstep > 1)
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
         if (!stage3) phi[p] = 1.5 * lnew[p] - llast[p] * 0.5;
         else phi[p] = 2.66667 * phi[p] - 2.0 * lnew[p] + 0.333333 * llast[p];
     }
 }
 
+// Filtering happens on steps that are multiples of `every` (every <= 0:
+// always); on the other steps the passes copy src to dst unchanged.
+__device__ __forceinline__ bool filter_step(const StepDev* sd, int every) {
+    return every <= 0 || (sd->tstep % every) == 0;
+}
+
 // FILTERING.f90 x pass over interior rows (reads src, writes dst).
-__global__ void k_filter_x(FsArgs a, FilterDev f, const double* __restrict__ src, double* __restrict__ dst) {
+__global__ void k_filter_x(FsArgs a, FilterDev f, const double* __restrict__ src, double* __restrict__ dst,
+                           const StepDev* sd, int every) {
     const int Nx = a.Nxg, al = f.alpha, NP = 2 * f.alpha + 1;
     const int64_t C = (int64_t)a.Nxg * a.Nyg;
+    if (!filter_step(sd, every)) {
+        for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < C; p += (int64_t)gridDim.x * blockDim.x)
+            dst[p] = src[p];
+        return;
+    }
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < C; p += (int64_t)gridDim.x * blockDim.x) {
         const int i = (int)(p % Nx) + 1, j = (int)(p / Nx) + 1;
         const double* row = src + (p - (i - 1));
@@ -350,9 +366,15 @@ __global__ void k_filter_x(FsArgs a, FilterDev f, const double* __restrict__ src
         dst[p] = v;
     }
 }
-__global__ void k_filter_y(FsArgs a, FilterDev f, const double* __restrict__ src, double* __restrict__ dst) {
+__global__ void k_filter_y(FsArgs a, FilterDev f, const double* __restrict__ src, double* __restrict__ dst,
+                           const StepDev* sd, int every) {
     const int Nx = a.Nxg, Ny = a.Nyg, al = f.alpha, NP = 2 * f.alpha + 1;
     const int64_t C = (int64_t)a.Nxg * a.Nyg;
+    if (!filter_step(sd, every)) {
+        for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < C; p += (int64_t)gridDim.x * blockDim.x)
+            dst[p] = src[p];
+        return;
+    }
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < C; p += (int64_t)gridDim.x * blockDim.x) {
         const int i = (int)(p % Nx) + 1, j = (int)(p / Nx) + 1;
         auto T = [&](int jj) { return src[(int64_t)(i - 1) + (int64_t)Nx * (jj - 1)]; };
@@ -376,6 +398,13 @@ __global__ void k_filter_y(FsArgs a, FilterDev f, const double* __restrict__ src
         }
         dst[p] = v;
     }
+}
+
+__global__ void k_step_begin(StepDev* sd) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) sd->tstep += 1;
+}
+__global__ void k_step_end(StepDev* sd, double dt) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) sd->time = sd->time + dt;
 }
 
 // max |E| for the instability test; writes flag = 1 when max|E| > 10 max h.
@@ -409,14 +438,15 @@ void fs_rk_final(const FsArgs& a, double* E, double* P, double* const* kE, doubl
     int64_t C = (int64_t)a.Nxg * a.Nyg;
     note_launch(), k_rk_final<<<nb(C), 256, 0, st>>>(a, E, P, kE[0], kE[1], kE[2], kE[3], kP[0], kP[1], kP[2], kP[3], dt);
 }
-void fs_relax(const FsArgs& a, const RelaxZoneDev* zones, int nz, double* E, double* P, double RKtime, double time,
+void fs_relax(const FsArgs& a, const RelaxZoneDev* zones, int nz, double* E, double* P, const StepDev* sd, double off,
               double transient, cudaStream_t st) {
-    const double FAC = (RKtime < transient) ? RKtime / transient : 1.0;
     for (int z = 0; z < nz; ++z) {
         int64_t box = (int64_t)(zones[z].i1 - zones[z].i0 + 1) * (zones[z].j1 - zones[z].j0 + 1);
-        note_launch(), k_relax<<<nb(box), 256, 0, st>>>(a, zones[z], E, P, FAC, RKtime, time);
+        note_launch(), k_relax<<<nb(box), 256, 0, st>>>(a, zones[z], E, P, sd, off, transient);
     }
 }
+void fs_step_begin(StepDev* sd, cudaStream_t st) { note_launch(), k_step_begin<<<1, 32, 0, st>>>(sd); }
+void fs_step_end(StepDev* sd, double dt, cudaStream_t st) { note_launch(), k_step_end<<<1, 32, 0, st>>>(sd, dt); }
 void fs_derivs(const FsArgs& a, double* E, double* P, double* Ex, double* Exx, double* Px, double* Ey, double* Eyy,
                double* Py, cudaStream_t st) {
     int64_t C = (int64_t)a.Nxg * a.Nyg;
@@ -440,13 +470,15 @@ void fs_set_rhs(const FsArgs& a, const double* P, double* rhs, cudaStream_t st) 
     int64_t C = (int64_t)a.Nxg * a.Nyg;
     note_launch(), k_set_rhs<<<nb(C), 256, 0, st>>>(a, P, rhs);
 }
-void fs_extrap(double* phi, const double* lnew, const double* llast, int64_t n, int stage3, cudaStream_t st) {
-    note_launch(), k_extrap<<<nb(n), 256, 0, st>>>(phi, lnew, llast, n, stage3);
+void fs_extrap(double* phi, const double* lnew, const double* llast, int64_t n, int stage3, const StepDev* sd,
+               cudaStream_t st) {
+    note_launch(), k_extrap<<<nb(n), 256, 0, st>>>(phi, lnew, llast, n, stage3, sd);
 }
-void fs_filter(const FsArgs& a, const FilterDev& f, double* U, double* tmp, cudaStream_t st) {
+void fs_filter(const FsArgs& a, const FilterDev& f, double* U, double* tmp, const StepDev* sd, int every,
+               cudaStream_t st) {
     int64_t C = (int64_t)a.Nxg * a.Nyg;
-    note_launch(), k_filter_x<<<nb(C), 256, 0, st>>>(a, f, U, tmp);
-    if (a.three) note_launch(), k_filter_y<<<nb(C), 256, 0, st>>>(a, f, tmp, U);
+    note_launch(), k_filter_x<<<nb(C), 256, 0, st>>>(a, f, U, tmp, sd, every);
+    if (a.three) note_launch(), k_filter_y<<<nb(C), 256, 0, st>>>(a, f, tmp, U, sd, every);
     else cudaMemcpyAsync(U, tmp, sizeof(double) * C, cudaMemcpyDeviceToDevice, st);
 }
 void fs_unstable(const FsArgs& a, const double* E, double hmax10, int* flag, cudaStream_t st) {

@@ -239,9 +239,11 @@ __global__ void __launch_bounds__(kThreads) k_project(const double* __restrict__
 }
 
 // Initial residual norm: beta = |v|, tolerance rtol*beta + atol.
+// hnext (nonzero only inside a captured step graph): the condition of the
+// graph node that runs the next Arnoldi step, set to "not done".
 __global__ void __launch_bounds__(kThreads) k_norm_init(const double* __restrict__ v, int64_t n, double* partial,
                                                         unsigned int* counter, int nblocks, KrylovState* ks,
-                                                        double rtol, double atol) {
+                                                        double rtol, double atol, cudaGraphConditionalHandle hnext) {
     double acc[1] = {0.0};
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += stride) acc[0] += v[t] * v[t];
@@ -260,6 +262,7 @@ __global__ void __launch_bounds__(kThreads) k_norm_init(const double* __restrict
             ks->k = 0;
             ks->reorth = 0;
             if (beta <= ks->tol) { ks->done = 1; ks->converged = 1; }
+            if (hnext) cudaGraphSetConditional(hnext, ks->done ? 0u : 1u);
         }
     }
 }
@@ -459,7 +462,7 @@ __global__ void __launch_bounds__(kThreads) k_dcgs_reduce(const double* __restri
 __global__ void __launch_bounds__(kThreads) k_dcgs_update(double* __restrict__ V, int64_t ldv, int j,
                                                           double* __restrict__ W, int64_t n, double* partial,
                                                           unsigned int* counter, int nblocks, KrylovState* ks,
-                                                          int maxmv, int m) {
+                                                          int maxmv, int m, cudaGraphConditionalHandle hnext) {
     if (ks->done) return;
     __shared__ double cA[kMaxDots], cB[kMaxDots + 1];
     for (int v = threadIdx.x; v <= j; v += blockDim.x) { cB[v] = ks->coefB[v]; if (v < j) cA[v] = ks->coefA[v]; }
@@ -503,8 +506,18 @@ __global__ void __launch_bounds__(kThreads) k_dcgs_update(double* __restrict__ V
             const bool conv = ks->resid <= ks->tol;
             if (conv) ks->converged = 1;
             if (conv || j + 1 >= m || ks->iters >= maxmv || nrm == 0.0) ks->done = 1;
+            if (hnext) cudaGraphSetConditional(hnext, ks->done ? 0u : 1u);
         }
     }
+}
+
+__global__ void k_solve_log(const KrylovState* ks, SolveLog* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    out->iters = ks->iters;
+    out->converged = ks->converged;
+    out->resid = ks->resid;
+    out->beta = ks->beta;
+    out->tol = ks->tol;
 }
 
 }  // namespace
@@ -522,9 +535,12 @@ void launch_dcgs_reduce(const double* V, int64_t ldv, int j, const double* W, in
 }
 
 void launch_dcgs_update(double* V, int64_t ldv, int j, double* W, int64_t n, const DotScratch& sc, KrylovState* ks,
-                        int maxmv, int m, cudaStream_t st) {
+                        int maxmv, int m, cudaStream_t st, cudaGraphConditionalHandle hnext) {
     note_launch(), k_dcgs_update<<<sc.nblocks, kThreads, 0, st>>>(V, ldv, j, W, n, sc.partial, sc.counter, sc.nblocks,
-                                                                  ks, maxmv, m);
+                                                                  ks, maxmv, m, hnext);
+}
+void launch_solve_log(const KrylovState* ks, SolveLog* out, cudaStream_t st) {
+    note_launch(), k_solve_log<<<1, 32, 0, st>>>(ks, out);
 }
 
 void launch_multidot(const double* V, int64_t ldv, int k, const double* w, int64_t n, const DotScratch& sc,
@@ -548,8 +564,9 @@ void launch_arnoldi_finish(KrylovState* ks, int maxmv, int m, cudaStream_t st) {
 }
 
 void launch_norm_init(const double* v, int64_t n, const DotScratch& sc, KrylovState* ks, double rtol, double atol,
-                      cudaStream_t st) {
-    note_launch(), k_norm_init<<<sc.nblocks, kThreads, 0, st>>>(v, n, sc.partial, sc.counter, sc.nblocks, ks, rtol, atol);
+                      cudaStream_t st, cudaGraphConditionalHandle hnext) {
+    note_launch(), k_norm_init<<<sc.nblocks, kThreads, 0, st>>>(v, n, sc.partial, sc.counter, sc.nblocks, ks, rtol, atol,
+                                                                hnext);
 }
 
 void launch_backsolve(KrylovState* ks, cudaStream_t st, int rotated_R) {

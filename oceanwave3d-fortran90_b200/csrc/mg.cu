@@ -320,12 +320,14 @@ __device__ void coop_smooth(const LevelDev<T>& L, int nu, SY& sy) {
 // phases are separated by the barrier SY; level ld is solved with the dense
 // operator M (the coarsest level's inverse when ld = 0, otherwise the V cycle
 // below ld as one precomputed map). Level lc's right-hand side is set and its
-// iterate zeroed on entry.
+// iterate zeroed on entry. Level lc is read from `top` (the table's entry with
+// the iterate and right-hand side of this launch), the others from the table.
 template <typename T, bool THREE, typename SY>
-__device__ void coarse_body(const LevelDev<T>* __restrict__ P, int lc, int ld, const T* __restrict__ M, int nu1,
-                            int nu2, SY& sy) {
+__device__ void coarse_body(const LevelDev<T>* __restrict__ P, const LevelDev<T>& top, int lc, int ld,
+                            const T* __restrict__ M, int nu1, int nu2, SY& sy) {
+    auto lv = [&](int l) -> const LevelDev<T>& { return l == lc ? top : P[l]; };
     for (int l = lc; l > ld; --l) {
-        const LevelDev<T>& L = P[l];
+        const LevelDev<T>& L = lv(l);
         const LevelDev<T>& Cc = P[l - 1];
         coop_smooth<T, THREE>(L, nu1, sy);
         if (L.cross) { OW3D_GRID_STRIDE(p, L.N) residual_point<T, THREE, true>(L, p); }
@@ -340,7 +342,7 @@ __device__ void coarse_body(const LevelDev<T>* __restrict__ P, int lc, int ld, c
         sy.sync();
     }
     for (int l = ld + 1; l <= lc; ++l) {
-        const LevelDev<T>& L = P[l];
+        const LevelDev<T>& L = lv(l);
         const LevelDev<T>& Cc = P[l - 1];
         OW3D_GRID_STRIDE(p, L.N) prolong_item<T>(L, Cc, Cc.xv, L.xv, p);
         sy.sync();
@@ -350,9 +352,17 @@ __device__ void coarse_body(const LevelDev<T>* __restrict__ P, int lc, int ld, c
 
 template <typename T, bool THREE>
 __global__ void __launch_bounds__(kCoopThreads) k_mg_coarse_cycle(const LevelDev<T>* __restrict__ P, int lc, int ld,
-                                                                  const T* __restrict__ M, int nu1, int nu2) {
+                                                                  const T* __restrict__ M, int nu1, int nu2, T* xtop,
+                                                                  T* btop) {
+    __shared__ LevelDev<T> top;
+    if (threadIdx.x == 0) {
+        top = P[lc];
+        top.xv = xtop;
+        top.bv = btop;
+    }
+    __syncthreads();
     GridSync sy{cg::this_grid()};
-    coarse_body<T, THREE>(P, lc, ld, M, nu1, nu2, sy);
+    coarse_body<T, THREE>(P, top, lc, ld, M, nu1, nu2, sy);
 }
 
 inline int nblk(int64_t n, int t = 256) {
@@ -525,8 +535,15 @@ static void coarse_cycle(const LevelDev<T>* lev, int lc, int ld, const T* M, int
     if (cap > 0 && cap < grid) grid = cap;
     // the level table lives in device memory (a by-value parameter indexed
     // by a run-time level would be copied to every thread's stack); upload it
-    // only when a level's pointers or sizes changed since the last launch
-    if (std::memcmp(pack.host, lev, sizeof(LevelDev<T>) * (size_t)(lc + 1)) != 0) {
+    // only when a level's pointers or sizes changed since the last launch.
+    // The top level's iterate and right-hand side are launch arguments (they
+    // change between Arnoldi steps when the top level is the finest), so the
+    // table holds them as null and stays the same.
+    LevelDev<T> cur[kMaxLevels];
+    std::memcpy(cur, lev, sizeof(LevelDev<T>) * (size_t)(lc + 1));
+    cur[lc].xv = nullptr;
+    cur[lc].bv = nullptr;
+    if (std::memcmp(pack.host, cur, sizeof(LevelDev<T>) * (size_t)(lc + 1)) != 0) {
         // Inside a stream capture this copy would replay from a host buffer
         // that later calls overwrite: mark the capture unusable and leave the
         // host image as it was, so that the direct launches that replace the
@@ -536,12 +553,14 @@ static void coarse_cycle(const LevelDev<T>* lev, int lc, int ld, const T* M, int
         if (cs != cudaStreamCaptureStatusNone) {
             g_capture_unsafe = true;
         } else {
-            std::memcpy(pack.host, lev, sizeof(LevelDev<T>) * (size_t)(lc + 1));
+            std::memcpy(pack.host, cur, sizeof(LevelDev<T>) * (size_t)(lc + 1));
             cudaMemcpyAsync(pack.dev, pack.host, sizeof(LevelDev<T>) * (size_t)(lc + 1), cudaMemcpyHostToDevice, st);
         }
     }
     const LevelDev<T>* P = pack.dev;
-    void* args[] = {(void*)&P, (void*)&lc, (void*)&ld, (void*)&M, (void*)&nu1, (void*)&nu2};
+    T* xtop = lev[lc].xv;
+    T* btop = lev[lc].bv;
+    void* args[] = {(void*)&P, (void*)&lc, (void*)&ld, (void*)&M, (void*)&nu1, (void*)&nu2, (void*)&xtop, (void*)&btop};
     note_launch();
     cudaLaunchCooperativeKernel((const void*)k_mg_coarse_cycle<T, THREE>, dim3(grid), dim3(kCoopThreads), args, 0, st);
 }

@@ -111,6 +111,23 @@ struct ow3d_handle {
     std::vector<IterGraph> iter_graphs;
     int graphs = 1;
     bool graphs_failed = false;
+    // One CUDA graph per RK4 step (from the second step on), by the parity of
+    // the step number (the extrapolation history alternates between two
+    // buffers). Each of the step's four solves is its initial residual, one
+    // conditional node per Arnoldi step whose condition the previous step's
+    // stopping test sets on the device, and the solution update; no host
+    // round trip happens inside a step.
+    struct StepGraph {
+        cudaGraphExec_t exec = nullptr;
+        unsigned long long base = 0;       // kernels outside the Arnoldi steps
+        unsigned long long per_step = 0;   // kernels of one Arnoldi step
+        bool failed = false;
+    };
+    StepGraph step_graph[2];
+    cudaStream_t st2 = nullptr;            // captures the conditional bodies
+    StepDev* sd = nullptr;                 // device time level
+    SolveLog* slog = nullptr;              // the four solves of the last graph step
+    SolveLog* slog_host = nullptr;         // pinned copy
 };
 
 namespace {
@@ -444,7 +461,8 @@ int sync_ks_small(ow3d_handle* H) {
 
 // The kernels of FGMRES Arnoldi step j with the multigrid preconditioner:
 // z_j = M^{-1} v_j, w = A z_j into V_{j+1}, DCGS2 reduction and update.
-void fgmres_step_launches(ow3d_handle* H, const Surface& s, int j, int maxmv, int m) {
+void fgmres_step_launches(ow3d_handle* H, const Surface& s, int j, int maxmv, int m,
+                          cudaGraphConditionalHandle hnext = 0) {
     const int64_t N = H->G.N;
     double* Vj = H->V + (int64_t)j * H->ldv;
     double* Vn = H->V + (int64_t)(j + 1) * H->ldv;
@@ -459,7 +477,7 @@ void fgmres_step_launches(ow3d_handle* H, const Surface& s, int j, int maxmv, in
         launch_ho_matvec<float>(H->hg, s, Zj, nullptr, nullptr, Vn, 0, H->st);
     }
     launch_dcgs_reduce(H->V, H->ldv, j, Vn, N, H->dsc, H->ks, H->st);
-    launch_dcgs_update(H->V, H->ldv, j, Vn, N, H->dsc, H->ks, maxmv, m, H->st);
+    launch_dcgs_update(H->V, H->ldv, j, Vn, N, H->dsc, H->ks, maxmv, m, H->st, hnext);
 }
 
 // Step j as a CUDA graph: captured on its first use (the handle has finished
@@ -505,6 +523,20 @@ int fgmres_step_graph(ow3d_handle* H, const Surface& s, int j, int maxmv, int m)
     CK(cudaGraphLaunch(g->exec, H->st));
     g_kernel_launches.fetch_add(g->kernels, std::memory_order_relaxed);
     return OW3D_OK;
+}
+
+// The counters of OceanWave3DTakeATimeStep.f90:76-122 for one solve.
+void record_solve(ow3d_handle* H, int it, double resid, double r0, double tol, bool not_converged) {
+    ow3d_stats& S = H->stats;
+    S.solves++;
+    S.total_iterations += it;
+    S.min_iterations = (S.solves == 1) ? it : std::min(S.min_iterations, it);
+    S.max_iterations = std::max(S.max_iterations, it);
+    S.last_iterations = it;
+    S.last_residual = resid;
+    S.last_initial_residual = r0;
+    S.last_tolerance = tol;
+    if (not_converged) S.not_converged++;
 }
 
 // One Laplace solve on the device: phi <- A^{-1} rhs, initial guess in phi.
@@ -584,16 +616,7 @@ int solve_device(ow3d_handle* H, const double* rhs, double* phi, const Surface& 
     }
     const int it = H->ks_host->iters;
     if (iters_out) *iters_out = it;
-    ow3d_stats& S = H->stats;
-    S.solves++;
-    S.total_iterations += it;
-    S.min_iterations = (S.solves == 1) ? it : std::min(S.min_iterations, it);
-    S.max_iterations = std::max(S.max_iterations, it);
-    S.last_iterations = it;
-    S.last_residual = H->ks_host->resid;
-    S.last_initial_residual = r0;
-    S.last_tolerance = tol;
-    if (status == OW3D_NOT_CONVERGED) S.not_converged++;
+    record_solve(H, it, H->ks_host->resid, r0, tol, status == OW3D_NOT_CONVERGED);
     CK(cudaGetLastError());
     return status;
 }
@@ -626,6 +649,7 @@ int create_impl(const ow3d_params* p, const double* h, const double* hx, const d
     H->dev = p->device;
     CK(cudaSetDevice(H->dev));
     CK(cudaStreamCreateWithFlags(&H->st, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&H->st2, cudaStreamNonBlocking));
     GridHost& G = H->G;
     TRY(upload(H.get(), &H->SX, G.SX.w));
     TRY(upload(H.get(), &H->SY, G.SY.w.empty() ? std::vector<double>(1, 0.0) : G.SY.w));
@@ -717,6 +741,13 @@ int create_impl(const ow3d_params* p, const double* h, const double* hx, const d
     TRY(dalloc(H.get(), &H->flag, 1));
     CK(cudaMemset(H->flag, 0, sizeof(int)));
     CK(cudaMallocHost(&H->flag_host, sizeof(int)));
+    TRY(dalloc(H.get(), &H->slog, 4));
+    CK(cudaMallocHost(&H->slog_host, 4 * sizeof(SolveLog)));
+    TRY(dalloc(H.get(), &H->sd, 1));
+    {
+        const StepDev s0{p->time0, 0};
+        CK(cudaMemcpy(H->sd, &s0, sizeof(StepDev), cudaMemcpyHostToDevice));
+    }
     H->time = p->time0;
     H->stats.time = H->time;
     CK(cudaStreamSynchronize(H->st));
@@ -747,31 +778,28 @@ int stage_surface(ow3d_handle* H, const double* E, const double* Ex, const doubl
 }
 
 // ------------------------------------------------------------- RK4 step
-// Runge_Kutta_4.f90:1-429 with the stage sequence of the reference.
-int rk4_step(ow3d_handle* H) {
+// The kernels of RK4 step number `tstep` (Runge_Kutta_4.f90:1-429, the
+// reference's stage sequence) on the handle's stream. solve(surface, k)
+// performs or enqueues the k-th Laplace solve of the step (k = 0..3). With
+// `graph` set the step is being captured: the records the host reads after
+// the step (instability flag, the solves' outcomes) are copied to pinned
+// memory at its end.
+template <typename SolveF>
+int enqueue_step(ow3d_handle* H, int64_t tstep, bool graph, SolveF&& solve) {
     cudaStream_t st = H->st;
     const double dt = H->p.dt, half = 0.5, time = H->time;
     const int64_t N = H->G.N;
-    H->tstep++;
-    const int64_t tstep = H->tstep;
     double* LPnew = H->LP[(tstep - 1) % 2];
     double* LPlast = H->LP[tstep % 2];
+    fs_step_begin(H->sd, st);
     CK(cudaMemcpyAsync(LPnew, H->PHI, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
     const FsArgs& fa = H->fa;
-    int status = OW3D_OK;
-    auto relax = [&](double* E, double* P, double RKtime) {
+    auto relax = [&](double* E, double* P, double off) {
         if (H->p.relaxONOFF == 1)
-            fs_relax(fa, H->zones.data(), (int)H->zones.size(), E, P, RKtime, time, H->p.relaxTransientTime, st);
+            fs_relax(fa, H->zones.data(), (int)H->zones.size(), E, P, H->sd, off, H->p.relaxTransientTime, st);
     };
     auto derivs = [&](double* E, double* P, double* Ex, double* Exx, double* Px, double* Ey, double* Eyy, double* Py) {
         fs_derivs(fa, E, P, Ex, Exx, Px, Ey, Eyy, Py, st);
-    };
-    auto solve = [&](const Surface& s) -> int {
-        int it = 0;
-        int r = solve_device(H, H->RHS, H->PHI, s, &it);
-        if (r < 0) return r;
-        if (r == OW3D_NOT_CONVERGED) status = OW3D_NOT_CONVERGED;
-        return OW3D_OK;
     };
     const bool nl = H->p.LinearONOFF == 1;
     auto surf = [&](const double* E, const double* Ex, const double* Exx, const double* Ey, const double* Eyy) {
@@ -779,7 +807,8 @@ int rk4_step(ow3d_handle* H) {
     };
     // funPressureTerm at each stage (Runge_Kutta_4.f90:50,159,239,334): the
     // damping terms of the stage's state when its time is positive; at
-    // t <= 0 they keep their last values
+    // t <= 0 they keep their last values (steps with pressure damping are
+    // never captured, so the host time is the step's)
     const double* NuD = H->pd_on ? H->pd.NuD : nullptr;
     const double* Pd = H->pd_on ? H->pd.Pd : nullptr;
     auto pdamp = [&](const double* E, const double* P, double t) {
@@ -789,56 +818,225 @@ int rk4_step(ow3d_handle* H) {
     pdamp(H->E, H->P, time);
     fs_stage(fa, H->E, H->P, H->W, H->Ex, H->Px, H->Ey, H->Py, H->E, H->P, half * dt, H->kE[0], H->kP[0], H->tE, H->tP,
              NuD, Pd, st);
-    relax(H->tE, H->tP, time + half * dt);
+    relax(H->tE, H->tP, half * dt);
     derivs(H->tE, H->tP, H->tEx, H->tExx, H->tPx, H->tEy, H->tEyy, H->tPy);
     fs_set_rhs(fa, H->tP, H->RHS, st);
-    if (H->p.extrapolationONOFF == 1) fs_extrap(H->PHI, LPnew, LPlast, N, 0, st);
-    TRY(solve(surf(H->tE, H->tEx, H->tExx, H->tEy, H->tEyy)));
+    if (H->p.extrapolationONOFF == 1) fs_extrap(H->PHI, LPnew, LPlast, N, 0, H->sd, st);
+    TRY(solve(surf(H->tE, H->tEx, H->tExx, H->tEy, H->tEyy), 0));
     fs_wvel(fa, H->PHI, H->tE, H->tW, st);
     // stage 2
     pdamp(H->tE, H->tP, time + half * dt);
     fs_stage(fa, H->tE, H->tP, H->tW, H->tEx, H->tPx, H->tEy, H->tPy, H->E, H->P, half * dt, H->kE[1], H->kP[1], H->tE,
              H->tP, NuD, Pd, st);
-    relax(H->tE, H->tP, time + half * dt);
+    relax(H->tE, H->tP, half * dt);
     derivs(H->tE, H->tP, H->tEx, H->tExx, H->tPx, H->tEy, H->tEyy, H->tPy);
     fs_set_rhs(fa, H->tP, H->RHS, st);
-    TRY(solve(surf(H->tE, H->tEx, H->tExx, H->tEy, H->tEyy)));
+    TRY(solve(surf(H->tE, H->tEx, H->tExx, H->tEy, H->tEyy), 1));
     fs_wvel(fa, H->PHI, H->tE, H->tW, st);
     // stage 3
     pdamp(H->tE, H->tP, time + half * dt);
     fs_stage(fa, H->tE, H->tP, H->tW, H->tEx, H->tPx, H->tEy, H->tPy, H->E, H->P, dt, H->kE[2], H->kP[2], H->tE, H->tP,
              NuD, Pd, st);
-    relax(H->tE, H->tP, time + dt);
+    relax(H->tE, H->tP, dt);
     derivs(H->tE, H->tP, H->tEx, H->tExx, H->tPx, H->tEy, H->tEyy, H->tPy);
     fs_set_rhs(fa, H->tP, H->RHS, st);
-    if (H->p.extrapolationONOFF == 1 && tstep > 1) fs_extrap(H->PHI, LPnew, LPlast, N, 1, st);
-    TRY(solve(surf(H->tE, H->tEx, H->tExx, H->tEy, H->tEyy)));
+    // Runge_Kutta_4.f90:294-303, from the second step on (checked on the device)
+    if (H->p.extrapolationONOFF == 1) fs_extrap(H->PHI, LPnew, LPlast, N, 1, H->sd, st);
+    TRY(solve(surf(H->tE, H->tEx, H->tExx, H->tEy, H->tEyy), 2));
     fs_wvel(fa, H->PHI, H->tE, H->tW, st);
     // stage 4 and the new time level
     pdamp(H->tE, H->tP, time + dt);
     fs_stage(fa, H->tE, H->tP, H->tW, H->tEx, H->tPx, H->tEy, H->tPy, nullptr, nullptr, 0.0, H->kE[3], H->kP[3], nullptr,
              nullptr, NuD, Pd, st);
     fs_rk_final(fa, H->E, H->P, H->kE, H->kP, dt, st);
-    if (H->p.filteringONOFF > 0 && (tstep % H->p.filteringONOFF) == 0) {
+    if (H->p.filteringONOFF > 0) {
+        // every filteringONOFF steps (Runge_Kutta_4.f90:355-362; the step number is checked on the device)
         FilterDev f{H->p.filterALPHA, H->fc, H->F2};
-        fs_filter(fa, f, H->E, H->ftmp, st);
-        fs_filter(fa, f, H->P, H->ftmp, st);
+        fs_filter(fa, f, H->E, H->ftmp, H->sd, H->p.filteringONOFF, st);
+        fs_filter(fa, f, H->P, H->ftmp, H->sd, H->p.filteringONOFF, st);
     }
-    relax(H->E, H->P, time + dt);
+    relax(H->E, H->P, dt);
     derivs(H->E, H->P, H->Ex, H->Exx, H->Px, H->Ey, H->Eyy, H->Py);
     fs_set_rhs(fa, H->P, H->RHS, st);
-    TRY(solve(surf(H->E, H->Ex, H->Exx, H->Ey, H->Eyy)));
+    TRY(solve(surf(H->E, H->Ex, H->Exx, H->Ey, H->Eyy), 3));
     fs_wvel(fa, H->PHI, H->E, H->W, st);
+    fs_step_end(H->sd, dt, st);
     // OceanWave3DTakeATimeStep.f90:54-70
     fs_unstable(fa, H->E, 10.0 * H->hmax, H->flag, st);
     CK(cudaMemcpyAsync(H->flag_host, H->flag, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    if (graph) CK(cudaMemcpyAsync(H->slog_host, H->slog, 4 * sizeof(SolveLog), cudaMemcpyDeviceToHost, st));
+    return OW3D_OK;
+}
+
+// Host bookkeeping after step number tstep completed on the device.
+int finish_step(ow3d_handle* H, int64_t tstep) {
     if (*H->flag_host) { g_last_error = "max|eta| > 10 max h: the solution went unstable"; return OW3D_ERR_UNSTABLE; }
-    H->time = time + dt;
+    H->tstep = tstep;
+    H->time = H->time + H->p.dt;
     H->stats.time = H->time;
     H->stats.tstep = H->tstep;
+    return OW3D_OK;
+}
+
+// One RK4 step with host-driven solves (per Arnoldi step graphs where they apply).
+int rk4_step(ow3d_handle* H) {
+    const int64_t tstep = H->tstep + 1;
+    int status = OW3D_OK;
+    auto solve = [&](const Surface& s, int) -> int {
+        int it = 0;
+        int r = solve_device(H, H->RHS, H->PHI, s, &it);
+        if (r < 0) return r;
+        if (r == OW3D_NOT_CONVERGED) status = OW3D_NOT_CONVERGED;
+        return OW3D_OK;
+    };
+    TRY(enqueue_step(H, tstep, false, solve));
+    CK(cudaStreamSynchronize(H->st));
+    TRY(finish_step(H, tstep));
     CK(cudaGetLastError());
     return status;
+}
+
+// One solve of a captured step: the initial residual, then one conditional
+// node per Arnoldi step (FGMRES with the multigrid preconditioner): node j
+// runs step j when its condition, set by the stopping test of step j-1 (or
+// of the initial residual), says the solve is not done. The subspace holds
+// m = GMRESmaxiterations vectors and the matvec limit is the same m, so a
+// solve never restarts. kin / bodies count the kernels and the nodes of the
+// Arnoldi steps.
+int enqueue_solve_graph(ow3d_handle* H, const Surface& s, int slot, unsigned long long& kin, int& bodies) {
+    cudaStream_t st = H->st;
+    const int m = H->m, maxmv = H->p.GMRESmaxiterations;
+    launch_krylov_reset(H->ks, st);
+    launch_ho_matvec<double>(H->hg, s, H->PHI, nullptr, H->RHS, H->V, 1, st);
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    CK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+    std::vector<cudaGraphConditionalHandle> hc((size_t)m, 0);
+    for (int j = 0; j < m; ++j) CK(cudaGraphConditionalHandleCreate(&hc[(size_t)j], g, 0, cudaGraphCondAssignDefault));
+    launch_norm_init(H->V, H->G.N, H->dsc, H->ks, H->p.reltol, H->p.abstol, st, hc[0]);
+    for (int j = 0; j < m; ++j) {
+        CK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+        // the parameter block has no default constructor (its union holds
+        // kernel parameters with dim3 members): zeroed raw storage instead
+        alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)] = {};
+        cudaGraphNodeParams& np = *reinterpret_cast<cudaGraphNodeParams*>(raw);
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = hc[(size_t)j];
+        np.conditional.type = cudaGraphCondTypeIf;
+        np.conditional.size = 1;
+        cudaGraphNode_t node = nullptr;
+        CK(cudaGraphAddNode(&node, g, deps, nd, &np));
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+        CK(cudaStreamBeginCaptureToGraph(H->st2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        const unsigned long long k0 = g_kernel_launches.load(std::memory_order_relaxed);
+        H->st = H->st2;   // the step's launches go to the body's capture
+        fgmres_step_launches(H, s, j, maxmv, m, j + 1 < m ? hc[(size_t)j + 1] : 0);
+        H->st = st;
+        kin += g_kernel_launches.load(std::memory_order_relaxed) - k0;
+        ++bodies;
+        cudaGraph_t bout = nullptr;
+        CK(cudaStreamEndCapture(H->st2, &bout));
+    }
+    launch_backsolve(H->ks, st, 1);
+    if (!H->mixed) launch_solution_update<double>(H->PHI, (const double*)H->Z, H->ldv, H->G.N, H->ks, 0, st);
+    else launch_solution_update<float>(H->PHI, (const float*)H->Z, H->ldv, H->G.N, H->ks, 0, st);
+    launch_solve_log(H->ks, H->slog + slot, st);
+    return OW3D_OK;
+}
+
+// Whether the next step may run as a captured graph: FGMRES with the
+// multigrid preconditioner, no pressure damping (its terms are gated on the
+// host time), graphs on, and the first step done directly (it performs the
+// one-time set-ups of the launches and uploads the level tables).
+bool step_graph_eligible(const ow3d_handle* H) {
+    return H->graphs && H->p.krylov == OW3D_KRYLOV_FGMRES && H->nlev > 0 && !H->pd_on && H->tstep >= 1 &&
+           !H->step_graph[(H->tstep + 1) & 1].failed;
+}
+
+// Capture the graph of steps with the parity of `tstep`.
+int capture_step_graph(ow3d_handle* H, int64_t tstep) {
+    ow3d_handle::StepGraph& G = H->step_graph[tstep & 1];
+    cudaStream_t st = H->st;
+    g_capture_unsafe = false;
+    const unsigned long long k0 = g_kernel_launches.load(std::memory_order_relaxed);
+    unsigned long long kin = 0;
+    int bodies = 0;
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    int err = OW3D_OK;
+    if (e == cudaSuccess) {
+        auto solve = [&](const Surface& s, int slot) -> int { return enqueue_solve_graph(H, s, slot, kin, bodies); };
+        err = enqueue_step(H, tstep, true, solve);
+        H->st = st;
+        e = cudaStreamEndCapture(st, &graph);
+        if (e == cudaSuccess && (err != OW3D_OK || g_capture_unsafe)) e = cudaErrorStreamCaptureUnsupported;
+    }
+    // the captured launches did not run: they are counted per replay instead
+    const unsigned long long nk = g_kernel_launches.load(std::memory_order_relaxed) - k0;
+    g_kernel_launches.fetch_sub(nk, std::memory_order_relaxed);
+    cudaGraphExec_t ex = nullptr;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&ex, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        G.failed = true;
+        return OW3D_ERR_UNSUPPORTED;   // the caller steps directly
+    }
+    G.exec = ex;
+    G.per_step = bodies > 0 ? kin / (unsigned long long)bodies : 0;
+    G.base = nk - kin;
+    return OW3D_OK;
+}
+
+// Launch the next step as a graph (capturing it first if needed); the host
+// work after it is finish_graph_step. Returns OW3D_ERR_UNSUPPORTED when the
+// step has to run directly.
+int launch_graph_step(ow3d_handle* H) {
+    if (!step_graph_eligible(H)) return OW3D_ERR_UNSUPPORTED;
+    const int64_t tstep = H->tstep + 1;
+    ow3d_handle::StepGraph& G = H->step_graph[tstep & 1];
+    if (!G.exec) TRY(capture_step_graph(H, tstep));
+    CK(cudaGraphLaunch(G.exec, H->st));
+    return OW3D_OK;
+}
+
+int finish_graph_step(ow3d_handle* H) {
+    const int64_t tstep = H->tstep + 1;
+    const ow3d_handle::StepGraph& G = H->step_graph[tstep & 1];
+    CK(cudaStreamSynchronize(H->st));
+    int status = OW3D_OK;
+    unsigned long long kernels = G.base;
+    const int maxmv = H->p.GMRESmaxiterations;
+    for (int q = 0; q < 4; ++q) {
+        const SolveLog& l = H->slog_host[q];
+        // iterative_solution.f90:117-134: the limit reached without convergence
+        const bool nc = !l.converged && l.iters >= maxmv;
+        record_solve(H, l.iters, l.resid, l.beta, l.tol, nc);
+        if (nc) status = OW3D_NOT_CONVERGED;
+        kernels += (unsigned long long)(l.iters > 1 ? l.iters - 1 : 0) * G.per_step;
+    }
+    g_kernel_launches.fetch_add(kernels, std::memory_order_relaxed);
+    TRY(finish_step(H, tstep));
+    CK(cudaGetLastError());
+    return status;
+}
+
+// The next step, as a graph where it applies, directly otherwise.
+int next_step(ow3d_handle* H) {
+    int r = launch_graph_step(H);
+    if (r == OW3D_ERR_UNSUPPORTED) return rk4_step(H);
+    if (r < 0) return r;
+    return finish_graph_step(H);
+}
+
+void drop_step_graphs(ow3d_handle* H) {
+    for (auto& g : H->step_graph) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g = ow3d_handle::StepGraph{};
+    }
 }
 
 }  // namespace
@@ -914,6 +1112,16 @@ int ow3d_test_graph_count(const ow3d_handle* H) {
     return H->graphs_failed ? -1 : (int)H->iter_graphs.size();
 }
 
+int ow3d_test_step_graph_count(const ow3d_handle* H) {
+    if (!H) return OW3D_ERR_BAD_INPUT;
+    int n = 0;
+    for (const auto& g : H->step_graph) {
+        if (g.failed) return -1;
+        if (g.exec) ++n;
+    }
+    return n;
+}
+
 int ow3d_default_params(ow3d_params* p) { return default_params(p); }
 
 int ow3d_read_deck(const char* path, ow3d_params* p) {
@@ -974,10 +1182,13 @@ int ow3d_destroy(ow3d_handle* H) {
     cudaSetDevice(H->dev);
     if (H->st) cudaStreamSynchronize(H->st);
     for (auto& g : H->iter_graphs) cudaGraphExecDestroy(g.exec);
+    for (auto& g : H->step_graph) if (g.exec) cudaGraphExecDestroy(g.exec);
     for (void* q : H->allocs) cudaFree(q);
     if (H->ks_host) cudaFreeHost(H->ks_host);
     if (H->flag_host) cudaFreeHost(H->flag_host);
+    if (H->slog_host) cudaFreeHost(H->slog_host);
     if (H->st) cudaStreamDestroy(H->st);
+    if (H->st2) cudaStreamDestroy(H->st2);
     delete H;
     return OW3D_OK;
 }
@@ -1107,6 +1318,11 @@ int ow3d_set_state(ow3d_handle* H, const double* E, const double* P, const doubl
     CK(cudaMemsetAsync(H->RHS, 0, nb, H->st));
     // OceanWave3DT0Setup.f90:444 -- surface derivatives of the initial state
     fs_derivs(H->fa, H->E, H->P, H->Ex, H->Exx, H->Px, H->Ey, H->Eyy, H->Py, H->st);
+    {
+        const StepDev s0{t, 0};
+        CK(cudaMemcpyAsync(H->sd, &s0, sizeof(StepDev), cudaMemcpyHostToDevice, H->st));
+        CK(cudaStreamSynchronize(H->st));   // s0 lives on this stack frame
+    }
     H->time = t;
     H->tstep = 0;
     H->stats.time = t;
@@ -1160,6 +1376,7 @@ int ow3d_set_relax_target(ow3d_handle* H, int zone, int mode, int nt, double dts
     CK(cudaMemcpy(de, eta, box * nt * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(dp, phis, box * nt * sizeof(double), cudaMemcpyHostToDevice));
     z.eta = de; z.phis = dp; z.nt = nt; z.tdt = dts; z.tmode = mode;
+    drop_step_graphs(H);   // the captured relaxation launches hold the old table
     return OW3D_OK;
 }
 
@@ -1449,7 +1666,7 @@ int ow3d_step(ow3d_handle* H, int nsteps) {
     CK(cudaSetDevice(H->dev));
     int st = OW3D_OK;
     for (int i = 0; i < nsteps; ++i) {
-        int r = rk4_step(H);
+        int r = next_step(H);
         if (r < 0) return r;
         if (r > 0) st = r;
     }
@@ -1463,25 +1680,37 @@ int ow3d_step_batch(ow3d_handle* const* hs, int n, const int* nsteps, int* statu
         for (int q = 0; q < i; ++q)
             if (hs[q] == hs[i]) { g_last_error = "ow3d_step_batch: a handle appears twice"; return OW3D_ERR_BAD_INPUT; }
     }
-    // One host thread per handle: each drives its handle's stream (the GMRES
-    // control loop synchronises with its own stream only), so the device runs
-    // the simulations' kernels concurrently.
-    std::vector<int> st(n, OW3D_OK);
+    // Lock-step rounds driven by this one host thread: in each round every
+    // handle with steps left launches its step graph on its own stream
+    // (no host work inside a step), the handles that cannot run graphs
+    // step directly meanwhile, then the launched steps are finished. The
+    // simulations' kernels so run concurrently on the device.
+    std::vector<int> st(n, OW3D_OK), left(nsteps, nsteps + n);
     std::vector<double> ms(n, 0.0);
     std::vector<std::string> errs(n);
-    auto work = [&](int i) {
-        const auto t0 = std::chrono::steady_clock::now();
-        st[i] = ow3d_step(hs[i], nsteps[i]);
-        const auto t1 = std::chrono::steady_clock::now();
-        ms[i] = std::chrono::duration<double, std::milli>(t1 - t0).count();
-        if (st[i] < 0) errs[i] = g_last_error;
+    const auto t0 = std::chrono::steady_clock::now();
+    auto done_at = [&](int i) {
+        ms[i] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     };
-    if (n == 1) work(0);
-    else {
-        std::vector<std::thread> th;
-        th.reserve(n);
-        for (int i = 0; i < n; ++i) th.emplace_back(work, i);
-        for (auto& t : th) t.join();
+    auto note = [&](int i, int r) {
+        if (r < 0) { st[i] = r; errs[i] = g_last_error; left[i] = 0; done_at(i); return; }
+        if (r > 0 && st[i] == OW3D_OK) st[i] = r;
+        if (--left[i] == 0) done_at(i);
+    };
+    for (int i = 0; i < n; ++i) if (left[i] == 0) done_at(i);
+    for (;;) {
+        std::vector<int> launched, direct;
+        for (int i = 0; i < n; ++i) {
+            if (left[i] <= 0) continue;
+            if (cudaSetDevice(hs[i]->dev) != cudaSuccess) { note(i, OW3D_ERR_CUDA); continue; }
+            const int r = launch_graph_step(hs[i]);
+            if (r == OW3D_OK) launched.push_back(i);
+            else if (r == OW3D_ERR_UNSUPPORTED) direct.push_back(i);
+            else note(i, r);
+        }
+        if (launched.empty() && direct.empty()) break;
+        for (int i : direct) { cudaSetDevice(hs[i]->dev); note(i, rk4_step(hs[i])); }
+        for (int i : launched) { cudaSetDevice(hs[i]->dev); note(i, finish_graph_step(hs[i])); }
     }
     int worst = OW3D_OK;
     for (int i = 0; i < n; ++i) {
@@ -1501,7 +1730,7 @@ int ow3d_step_timed(ow3d_handle* H, int nsteps, double* device_ms) {
     CK(cudaEventRecord(a, H->st));
     int st = OW3D_OK;
     for (int i = 0; i < nsteps; ++i) {
-        int r = rk4_step(H);
+        int r = next_step(H);
         if (r < 0) { cudaEventDestroy(a); cudaEventDestroy(b); return r; }
         if (r > 0) st = r;
     }
@@ -1533,6 +1762,7 @@ int ow3d_reset_stats(ow3d_handle* H) {
 int ow3d_set_graphs(ow3d_handle* H, int on) {
     if (!H) return OW3D_ERR_BAD_INPUT;
     H->graphs = on ? 1 : 0;
+    if (!on) drop_step_graphs(H);
     return OW3D_OK;
 }
 

@@ -15,6 +15,15 @@ struct FsArgs {
     const double* h;
 };
 
+// The time level on the device: the simulation time at the start of the
+// current step and the step number (1 for the first step). The kernels whose
+// work depends on them read this instead of taking the values as launch
+// parameters, so that a captured step replays correctly at every step.
+struct StepDev {
+    double time;
+    long long tstep;
+};
+
 // One relaxation zone on the device (PreprocessRelaxationZones.f90).
 struct RelaxZoneDev {
     int i0, i1, j0, j1;      // 1-based, ghost-inclusive box
@@ -53,8 +62,12 @@ void fs_stage(const FsArgs& a, const double* E, const double* P, const double* W
               double* kP, double* tE, double* tP, const double* NuD, const double* Pd, cudaStream_t st);
 void fs_rk_final(const FsArgs& a, double* E, double* P, double* const* kE, double* const* kP, double dt,
                  cudaStream_t st);
-void fs_relax(const FsArgs& a, const RelaxZoneDev* zones, int nz, double* E, double* P, double RKtime, double time,
+// Relaxation at RK time = (device time) + off.
+void fs_relax(const FsArgs& a, const RelaxZoneDev* zones, int nz, double* E, double* P, const StepDev* sd, double off,
               double transient, cudaStream_t st);
+// Start of a step: tstep += 1. End of a step: time += dt.
+void fs_step_begin(StepDev* sd, cudaStream_t st);
+void fs_step_end(StepDev* sd, double dt, cudaStream_t st);
 void fs_derivs(const FsArgs& a, double* E, double* P, double* Ex, double* Exx, double* Px, double* Ey, double* Eyy,
                double* Py, cudaStream_t st);
 void fs_wvel(const FsArgs& a, const double* phi, const double* E, double* W, cudaStream_t st);
@@ -62,8 +75,12 @@ void fs_wvel(const FsArgs& a, const double* phi, const double* E, double* W, cud
 // with nz values per column (1 <- Nxg-2, Nxg-1 <- 2, Nxg <- 3), or zero them.
 void fs_images(const FsArgs& a, double* v, int nz, int zero, cudaStream_t st);
 void fs_set_rhs(const FsArgs& a, const double* P, double* rhs, cudaStream_t st);
-void fs_extrap(double* phi, const double* lnew, const double* llast, int64_t n, int stage3, cudaStream_t st);
-void fs_filter(const FsArgs& a, const FilterDev& f, double* U, double* tmp, cudaStream_t st);
+// stage3: the stage-3 form, applied only from the second step on (sd->tstep > 1).
+void fs_extrap(double* phi, const double* lnew, const double* llast, int64_t n, int stage3, const StepDev* sd,
+               cudaStream_t st);
+// every > 0: filter only when sd->tstep is a multiple of `every` (U unchanged otherwise).
+void fs_filter(const FsArgs& a, const FilterDev& f, double* U, double* tmp, const StepDev* sd, int every,
+               cudaStream_t st);
 void fs_unstable(const FsArgs& a, const double* E, double hmax10, int* flag, cudaStream_t st);
 
 }  // namespace ow3d

@@ -227,15 +227,24 @@ void launch_multidot(const double* V, int64_t ldv, int k, const double* w, int64
 // reduction pass and the one update pass; W = A z_j sits in V_{j+1}.
 void launch_dcgs_reduce(const double* V, int64_t ldv, int j, const double* W, int64_t n, const DotScratch& sc,
                         KrylovState* ks, cudaStream_t st);
+// hnext: inside a captured step graph, the condition of the node that runs
+// Arnoldi step j+1 (set to "not done" by the step's stopping test); 0 otherwise.
 void launch_dcgs_update(double* V, int64_t ldv, int j, double* W, int64_t n, const DotScratch& sc, KrylovState* ks,
-                        int maxmv, int m, cudaStream_t st);
+                        int maxmv, int m, cudaStream_t st, cudaGraphConditionalHandle hnext = 0);
 // Projection pass; the last block finishes the Arnoldi step (Givens rotation,
 // stopping test) when no re-orthogonalisation pass follows.
 void launch_project(const double* V, int64_t ldv, int k, double* w, int64_t n, const DotScratch& sc, KrylovState* ks,
                     int cond, int maxmv, int m, cudaStream_t st);
 void launch_arnoldi_finish(KrylovState* ks, int maxmv, int m, cudaStream_t st);
 void launch_norm_init(const double* v, int64_t n, const DotScratch& sc, KrylovState* ks, double rtol, double atol,
-                      cudaStream_t st);
+                      cudaStream_t st, cudaGraphConditionalHandle hnext = 0);
+// The outcome of one solve, copied from the Krylov state when it ends (the
+// step graph's record of its four solves).
+struct SolveLog {
+    int iters, converged;
+    double resid, beta, tol;
+};
+void launch_solve_log(const KrylovState* ks, SolveLog* out, cudaStream_t st);
 void launch_backsolve(KrylovState* ks, cudaStream_t st, int rotated_R = 0);
 template <typename TZ>
 void launch_solution_update(double* x, const TZ* Z, int64_t ldz, int64_t n, const KrylovState* ks, int use_scale,

@@ -5,8 +5,11 @@ simulation -- its own grid, bathymetry and sea state -- that must be advanced
 a given number of RK4 steps. The server keeps every admitted simulation
 resident on the device (state, Krylov workspace and multigrid hierarchy live
 in its handle) and advances all of them together, one step per round, through
-ow3d_step_batch: one host thread per handle, so the simulations' kernels
-overlap on the GPU. A request is admitted as soon as it has arrived, a slot is
+ow3d_step_batch: one host thread launches every simulation's RK4 step as one
+CUDA graph on the simulation's own stream (the Arnoldi steps of each solve are
+conditional nodes the device enables, so no host round trip happens inside a
+step) and then waits for them, so the simulations' kernels overlap on the
+GPU. A request is admitted as soon as it has arrived, a slot is
 free and its estimated device memory (ow3d_estimate_bytes) fits in what the
 running simulations leave of the memory budget; finished simulations release
 their handle (and memory) at the end of the round in which they finish.

@@ -232,4 +232,93 @@ def test_graph_launched_steps_match_direct_launches(ow3d, precision):
     (sg, ng, ig), (sd, nd, idd) = out
     for a, b in zip(sg[:4], sd[:4]):
         assert np.array_equal(a, b)
-    assert ng == nd and ig == idd
+    # the whole-step graphs of steps 2 and 3 add one record kernel per solve
+    # and always run the back-substitution and update
+    assert ig == idd and 0 <= ng - nd <= 3 * 4 * 3
+
+
+def _step_case(ow3d, name):
+    """Cases for the whole-step graphs: 3-D bump (FP64 and mixed; finest
+    level outside the fused coarse kernel), the shoal basin with its
+    generation zone, sponge and a filter every other step (sloping bottom:
+    four colours and the level-1 passes), the periodic wave (finest level
+    inside the fused coarse kernel) and the stream-function flume
+    (relaxation targets at every stage time)."""
+    W = ow3d.workloads
+    if name in ("bump3d_fp64", "bump3d_mixed"):
+        p, geo = cases.bump_3d(Nx=129, Ny=33, Nz=17, Lx=8.0, Ly=2.0, dt=0.02)
+        p.precision = 1 if name.endswith("mixed") else 0
+        x = (np.arange(p.Nx + 2) - 1) / (p.Nx - 1) * p.Lx
+        E0 = np.tile(0.01 * np.cos(np.pi * x / p.Lx), p.Ny + 2)
+        return p, geo, E0, np.zeros_like(E0), None
+    if name == "shoal_filter":
+        p, geo, target = cases.shoal_generation(W, 8, filteringONOFF=2)
+        return p, geo, np.zeros((p.Nx + 2) * (p.Ny + 2)), np.zeros((p.Nx + 2) * (p.Ny + 2)), target
+    if name == "periodic":
+        p, geo, E0, P0, info = W.periodic_wave_2d()
+        return p, geo, E0, P0, None
+    p, geo, E0, P0, targets = W.stream_function_2d(ppw=16, steps=8)
+    return p, geo, E0, P0, (lambda box: targets[0])
+
+
+@pytest.mark.parametrize("name", ["bump3d_fp64", "bump3d_mixed", "shoal_filter", "periodic", "sfwave"])
+def test_step_graphs_match_direct_steps(ow3d, name):
+    """Steps replayed as one CUDA graph each (the default from the second
+    step on: each solve's Arnoldi steps as conditional nodes that the device
+    enables, the time level read on the device) give bitwise the state, the
+    matvec counts and the solver records of direct launches."""
+    L = ow3d.lib()
+    out = []
+    for graphs in (1, 0):
+        p, geo, E0, P0, target = _step_case(ow3d, name)
+        sim = ow3d.Simulation(p, **geo)
+        assert L.ow3d_set_graphs(sim.h, graphs) == 0
+        if target is not None:
+            sim.set_relax_target(0, *target(sim.zone_box(0)))
+        sim.set_state(E0, P0)
+        its = cases.run_steps(sim, 6)
+        st = sim.stats()
+        out.append((sim.get_state(), its, st))
+        n = L.ow3d_test_step_graph_count(sim.h)
+        assert (n == 2) if graphs else (n == 0), n
+        sim.close()
+    (sg, ig, tg), (sd, idd, td) = out
+    for a, b in zip(sg[:4], sd[:4]):
+        assert np.array_equal(a, b)
+    assert sg[4] == sd[4]
+    assert np.array_equal(ig, idd)
+    for k in ("solves", "total_iterations", "min_iterations", "max_iterations", "not_converged",
+              "last_residual", "last_initial_residual", "last_tolerance"):
+        assert tg[k] == td[k], k
+
+
+def test_step_batch_matches_single_steps(ow3d):
+    """ow3d_step_batch (one host thread, the handles' step graphs launched
+    together each round) gives each simulation bitwise the state of stepping
+    it alone."""
+    import ctypes as C
+    L = ow3d.lib()
+    W = ow3d.workloads
+    specs = [W.periodic_wave_2d(), W.periodic_wave_2d(Nx=129, Nz=9)]
+    alone, sims = [], []
+    for p, geo, E0, P0, info in specs:
+        s = ow3d.Simulation(p, **geo)
+        s.set_state(E0, P0)
+        assert s.step(5) >= 0
+        alone.append(s.get_state())
+        s.close()
+    for p, geo, E0, P0, info in specs:
+        s = ow3d.Simulation(p, **geo)
+        s.set_state(E0, P0)
+        sims.append(s)
+    hs = (C.c_void_p * 2)(*[s.h.value for s in sims])
+    ns = (C.c_int * 2)(5, 3)
+    stv = (C.c_int * 2)()
+    assert L.ow3d_step_batch(hs, 2, ns, stv, None) >= 0
+    ns2 = (C.c_int * 2)(0, 2)
+    assert L.ow3d_step_batch(hs, 2, ns2, stv, None) >= 0
+    for s, a in zip(sims, alone):
+        b = s.get_state()
+        for x, y in zip(a[:4], b[:4]):
+            assert np.array_equal(x, y)
+        s.close()
