@@ -276,16 +276,16 @@ def profiled_traffic(kernel):
     return None
 
 
-def serving_sample(n=16, seed=2024):
+def serving_sample(n=16, seed=2024, rate=50.0, nx=(65, 129, 257), ny=(1, 33, 65), nz=(9, 13, 17), steps=(10, 40),
+                   note="sizes capped to keep the run short"):
     """Bounded sample of the serving stream: n seeded requests (Poisson
-    arrivals at 50/s; Nx in {65,129,257}, Ny in {1,33,65}, Nz in {9,13,17};
-    10-40 steps each), served (a) one at a time with the plain FP64 path and
-    (b) by the memory-gated continuous-batching server with the mixed path."""
+    arrivals at `rate`/s, sizes drawn from nx, ny, nz, step counts from
+    `steps`), served (a) one at a time with the plain FP64 path and (b) by the
+    memory-gated continuous-batching server with the mixed path."""
     import torch
     pkg = package()
     S = pkg.serving
-    mk = lambda: S.request_stream(n=n, rate=50.0, seed=seed, nx=(65, 129, 257), ny=(1, 33, 65),
-                                  nz=(9, 13, 17), steps=(10, 40))
+    mk = lambda: S.request_stream(n=n, rate=rate, seed=seed, nx=nx, ny=ny, nz=nz, steps=steps)
     # warm-up: one small simulation per precision (module load, first launches)
     for prec in (pkg.capi.PREC_FP64, pkg.capi.PREC_MIXED):
         be = S.DeviceBackend(pkg, precision=prec)
@@ -298,8 +298,9 @@ def serving_sample(n=16, seed=2024):
     keys = ("dof_timesteps_per_s", "step_ms_p50", "step_ms_p99", "request_latency_s_p50", "request_latency_s_p99",
             "wall_s", "completed", "steps")
     return {
-        "sample": f"{n} requests of the seeded serving stream (Poisson 50/s; Nx 65-257, Ny 1-65, Nz 9-17; "
-                  f"10-40 steps each instead of 100-2000, sizes capped to keep the run short)",
+        "sample": f"{n} requests of the seeded serving stream (Poisson {rate:g}/s; Nx {min(nx)}-{max(nx)}, "
+                  f"Ny {min(ny)}-{max(ny)}, Nz {min(nz)}-{max(nz)}; {steps[0]}-{steps[1]} steps each instead of "
+                  f"100-2000, {note})",
         "batched_mixed": {k: bat[k] for k in keys} | {"peak_slots": bat["peak_slots"]},
         "sequential_fp64": {k: seq[k] for k in keys},
         "throughput_ratio": bat["dof_timesteps_per_s"] / max(seq["dof_timesteps_per_s"], 1e-30),
@@ -416,14 +417,26 @@ def main():
     ap.add_argument("--grid", default=None, help="NXxNYxNZ override for --profile (e.g. 257x65x17)")
     ap.add_argument("--profile-workload", choices=["sea", "shoal"], default="sea",
                     help="--profile workload: the irregular sea, or the 257x33x9 shoal basin (sloping bottom)")
-    ap.add_argument("--config", choices=["sea", "largest"], default="sea",
-                    help="largest: the 2049x513x9 instance at three GMRES tolerances (one JSON line each)")
+    ap.add_argument("--config", choices=["sea", "largest", "serving"], default="sea",
+                    help="largest: the 2049x513x9 instance at three GMRES tolerances (one JSON line each); "
+                         "serving: the serving stream with the configuration's size sets (one JSON line)")
+    ap.add_argument("--requests", type=int, default=48, help="--config serving: number of requests")
     args = ap.parse_args()
     if args.profile:
         profile_step(args)
         return
     if args.config == "largest":
         largest_instance(args)
+        return
+    if args.config == "serving":
+        # the serving stream with the configuration's size sets (Nx 65-1025,
+        # Ny 1-257, Nz 9-17), step counts scaled down 10x to bound the run
+        import torch
+        torch.cuda.set_device(0)
+        S = package().serving
+        out = serving_sample(n=args.requests, seed=2024, rate=4.0, nx=S.NX_SET, ny=S.NY_SET, nz=S.NZ_SET,
+                             steps=(10, 200), note="the configuration's size sets, step counts scaled down 10x")
+        print(json.dumps({"config": "serving stream", "unit": UNIT, **out}))
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

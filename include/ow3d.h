@@ -385,15 +385,16 @@ int ow3d_step_timed(ow3d_handle* h, int nsteps, double* device_ms);
 
 /* Advance n independent simulations together -- no counterpart in the
  * reference, which runs one simulation per process. Handle i takes nsteps[i]
- * RK4 steps, in lock-step rounds driven by the calling thread: each round
- * launches one step of every handle with steps left as that handle's step
- * graph on its own stream (see ow3d_set_graphs; handles that cannot use
- * graphs step directly meanwhile), then waits for them, so the simulations'
- * kernels overlap on the device. status[i] and wall_ms[i] (either may be
- * NULL) receive each handle's ow3d_step status and the host time in
- * milliseconds from the call's start to the end of its last step. The
- * handles must be distinct. Returns the most severe status. Each result is
- * the same as ow3d_step on that handle alone (handles share no state). */
+ * RK4 steps, each simulation at its own pace, driven by the calling thread:
+ * every handle with steps left has its next step in flight as its step
+ * graph on its own stream (see ow3d_set_graphs), and as soon as one
+ * completes the thread launches that handle's next step (handles that
+ * cannot use graphs step directly in between). The simulations' kernels so
+ * overlap on the device. status[i] and wall_ms[i] (either may be NULL)
+ * receive each handle's ow3d_step status and the host time in milliseconds
+ * from the call's start to the end of its last step. The handles must be
+ * distinct. Returns the most severe status. Each result is the same as
+ * ow3d_step on that handle alone (handles share no state). */
 int ow3d_step_batch(ow3d_handle* const* hs, int n, const int* nsteps, int* status, double* wall_ms);
 
 int ow3d_get_stats(const ow3d_handle* h, ow3d_stats* s);

@@ -1680,12 +1680,15 @@ int ow3d_step_batch(ow3d_handle* const* hs, int n, const int* nsteps, int* statu
         for (int q = 0; q < i; ++q)
             if (hs[q] == hs[i]) { g_last_error = "ow3d_step_batch: a handle appears twice"; return OW3D_ERR_BAD_INPUT; }
     }
-    // Lock-step rounds driven by this one host thread: in each round every
-    // handle with steps left launches its step graph on its own stream
-    // (no host work inside a step), the handles that cannot run graphs
-    // step directly meanwhile, then the launched steps are finished. The
-    // simulations' kernels so run concurrently on the device.
+    // One host thread, each simulation at its own pace: every handle with
+    // steps left has its next step graph in flight on its own stream; the
+    // thread polls the streams and, as soon as one step completes, does its
+    // bookkeeping and launches that handle's next step. Handles that cannot
+    // use graphs (their first step, left GMRES, pressure damping) step
+    // directly in between. The simulations' kernels so overlap on the device
+    // and a small simulation is not held back by a large one.
     std::vector<int> st(n, OW3D_OK), left(nsteps, nsteps + n);
+    std::vector<char> inflight(n, 0);
     std::vector<double> ms(n, 0.0);
     std::vector<std::string> errs(n);
     const auto t0 = std::chrono::steady_clock::now();
@@ -1699,18 +1702,36 @@ int ow3d_step_batch(ow3d_handle* const* hs, int n, const int* nsteps, int* statu
     };
     for (int i = 0; i < n; ++i) if (left[i] == 0) done_at(i);
     for (;;) {
-        std::vector<int> launched, direct;
+        // launch the next step of every idle handle; direct steps run here
+        bool work = false;
         for (int i = 0; i < n; ++i) {
-            if (left[i] <= 0) continue;
+            if (left[i] <= 0 || inflight[i]) continue;
+            work = true;
             if (cudaSetDevice(hs[i]->dev) != cudaSuccess) { note(i, OW3D_ERR_CUDA); continue; }
             const int r = launch_graph_step(hs[i]);
-            if (r == OW3D_OK) launched.push_back(i);
-            else if (r == OW3D_ERR_UNSUPPORTED) direct.push_back(i);
+            if (r == OW3D_OK) inflight[i] = 1;
+            else if (r == OW3D_ERR_UNSUPPORTED) note(i, rk4_step(hs[i]));
             else note(i, r);
         }
-        if (launched.empty() && direct.empty()) break;
-        for (int i : direct) { cudaSetDevice(hs[i]->dev); note(i, rk4_step(hs[i])); }
-        for (int i : launched) { cudaSetDevice(hs[i]->dev); note(i, finish_graph_step(hs[i])); }
+        bool any = false;
+        for (int i = 0; i < n; ++i) any = any || inflight[i];
+        if (!any) {
+            if (!work) break;
+            continue;
+        }
+        // wait for the first in-flight step to complete, then finish it
+        for (bool got = false; !got;) {
+            for (int i = 0; i < n; ++i) {
+                if (!inflight[i]) continue;
+                cudaSetDevice(hs[i]->dev);
+                const cudaError_t e = cudaStreamQuery(hs[i]->st);
+                if (e == cudaErrorNotReady) continue;
+                inflight[i] = 0;
+                got = true;
+                note(i, e == cudaSuccess ? finish_graph_step(hs[i]) : OW3D_ERR_CUDA);
+            }
+            if (!got) std::this_thread::yield();
+        }
     }
     int worst = OW3D_OK;
     for (int i = 0; i < n; ++i) {

@@ -5,17 +5,21 @@ simulation -- its own grid, bathymetry and sea state -- that must be advanced
 a given number of RK4 steps. The server keeps every admitted simulation
 resident on the device (state, Krylov workspace and multigrid hierarchy live
 in its handle) and advances all of them together, one step per round, through
-ow3d_step_batch: one host thread launches every simulation's RK4 step as one
-CUDA graph on the simulation's own stream (the Arnoldi steps of each solve are
-conditional nodes the device enables, so no host round trip happens inside a
-step) and then waits for them, so the simulations' kernels overlap on the
-GPU. A request is admitted as soon as it has arrived, a slot is
+ow3d_step_batch: one host thread keeps every simulation's next RK4 step in
+flight as one CUDA graph on the simulation's own stream (the Arnoldi steps of
+each solve are conditional nodes the device enables, so no host round trip
+happens inside a step) and launches a simulation's next step as soon as its
+previous one completes, so the simulations' kernels overlap on the GPU. In a
+round, a simulation takes as many steps as fit in the longest single step of
+the round (from the step times measured in the previous round), so small
+simulations are not held back by large ones. A request is admitted as soon as it has arrived, a slot is
 free and its estimated device memory (ow3d_estimate_bytes) fits in what the
 running simulations leave of the memory budget; finished simulations release
 their handle (and memory) at the end of the round in which they finish.
 
-Reported: per-step latency percentiles over every step of every request (the
-host wall time of that request's step inside its round), request latency
+Reported: per-step latency percentiles over every step of every request (a
+request's host time inside its round divided by the steps it took in the
+round), request latency
 (arrival to completion), and aggregate DOF-timesteps/s of the whole run.
 
 The reference advances one simulation per process; this module has no
@@ -134,10 +138,10 @@ class DeviceBackend:
         sim.set_state(eta, phis)
         return sim
 
-    def step_batch(self, sims):
+    def step_batch(self, sims, nsteps=None):
         n = len(sims)
         hs = (C.c_void_p * n)(*[s.h for s in sims])
-        steps = (C.c_int * n)(*([1] * n))
+        steps = (C.c_int * n)(*(nsteps if nsteps is not None else [1] * n))
         status = (C.c_int * n)()
         ms = (C.c_double * n)()
         self.lib.ow3d_step_batch(hs, n, steps, status, ms)
@@ -193,14 +197,23 @@ class Server:
                         self.sleep(wait)
                 continue
             peak_slots = max(peak_slots, len(active))
-            status, ms = self.backend.step_batch([a[1] for a in active])
+            # steps per simulation in this round: as many as fit in the
+            # round's longest single step, from the last measured step times
+            est = [a[0].step_ms[-1] if a[0].step_ms else None for a in active]
+            known = [e for e in est if e]
+            longest = max(known) if known else None
+            nst = []
+            for a, e in zip(active, est):
+                k = 1 if (longest is None or not e) else max(1, int(longest // e))
+                nst.append(min(k, a[0].steps - a[3]))
+            status, ms = self.backend.step_batch([a[1] for a in active], nst)
             rounds += 1
             now = self.clock() - t0
             still = []
-            for a, st, m in zip(active, status, ms):
+            for a, st, m, k in zip(active, status, ms, nst):
                 req = a[0]
-                req.step_ms.append(m)
-                a[3] += 1
+                req.step_ms.extend([m / k] * k)
+                a[3] += k
                 if st < 0 or a[3] >= req.steps:
                     req.status = st
                     req.finished = now
@@ -223,7 +236,7 @@ def run_sequential(backend, requests, keep_eta=False, clock=time.perf_counter):
         sim = backend.create(req)
         req.admitted = clock() - t0
         for _ in range(req.steps):
-            st, ms = backend.step_batch([sim])
+            st, ms = backend.step_batch([sim], [1])
             req.step_ms.append(ms[0])
             if st[0] < 0:
                 break

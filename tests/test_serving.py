@@ -40,9 +40,11 @@ class FakeBackend:
         self.created.append(req.rid)
         return req
 
-    def step_batch(self, sims):
-        self.clock.t += 1e-3 * (1 + 0.1 * len(sims))
-        return [0] * len(sims), [1.0 + 0.1 * len(sims)] * len(sims)
+    def step_batch(self, sims, nsteps):
+        # a step costs (1 + 0.1 * slots) ms; the round lasts the longest run
+        c = 1.0 + 0.1 * len(sims)
+        self.clock.t += 1e-3 * c * max(nsteps)
+        return [0] * len(sims), [c * k for k in nsteps]
 
     def finish(self, sim, req):
         del self.resident[req.rid]
