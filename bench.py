@@ -344,6 +344,9 @@ def profile_step(args):
     if args.grid:
         kw = dict(zip(("Nx", "Ny", "Nz"), (int(v) for v in args.grid.lower().split("x"))))
     prec = 1 if args.profile == "mixed" else 0
+    def graphs_off(sim):
+        if args.no_graphs:
+            pkg.lib().ow3d_set_graphs(sim.h, 0)
     if args.profile_workload == "shoal":
         # sloping bottom: multigrid levels with mixed-derivative terms, the
         # generation zone and the sponge
@@ -351,6 +354,7 @@ def profile_step(args):
         import cases
         p, geo, target = cases.shoal_generation(pkg.workloads, 4, precision=prec)
         sim = pkg.Simulation(p, **geo)
+        graphs_off(sim)
         sim.set_relax_target(0, *target(sim.zone_box(0)))
         Nxg, Nyg, _ = pkg.dims(p)
         x, y = pkg.workloads.grid_xy(p)
@@ -359,6 +363,7 @@ def profile_step(args):
     else:
         p, geo, E0, P0 = pkg.workloads.irregular_sea(**kw, precision=prec)
         sim = pkg.Simulation(p, **geo)
+        graphs_off(sim)
         sim.set_state(E0, P0)
     sim.step(1)
     st, ms = sim.step_timed(1)
@@ -415,6 +420,8 @@ def main():
     ap.add_argument("--profile", choices=["fp64", "mixed"], default=None,
                     help="profiling driver: one warm-up step then one step of the workload, no JSON line")
     ap.add_argument("--grid", default=None, help="NXxNYxNZ override for --profile (e.g. 257x65x17)")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="--profile: launch every kernel directly (no CUDA graphs), for per-launch profiling")
     ap.add_argument("--profile-workload", choices=["sea", "shoal"], default="sea",
                     help="--profile workload: the irregular sea, or the 257x33x9 shoal basin (sloping bottom)")
     ap.add_argument("--config", choices=["sea", "largest", "serving"], default="sea",
