@@ -277,7 +277,7 @@ def profiled_traffic(kernel):
 
 
 def serving_sample(n=16, seed=2024, rate=50.0, nx=(65, 129, 257), ny=(1, 33, 65), nz=(9, 13, 17), steps=(10, 40),
-                   note="sizes capped to keep the run short"):
+                   note="sizes capped to keep the run short", slots=(None,)):
     """Bounded sample of the serving stream: n seeded requests (Poisson
     arrivals at `rate`/s, sizes drawn from nx, ny, nz, step counts from
     `steps`), served (a) one at a time with the plain FP64 path and (b) by the
@@ -293,17 +293,24 @@ def serving_sample(n=16, seed=2024, rate=50.0, nx=(65, 129, 257), ny=(1, 33, 65)
         sim = be.create(w); be.step_batch([sim]); be.finish(sim, w)
     seq = S.run_sequential(S.DeviceBackend(pkg, precision=pkg.capi.PREC_FP64), mk())
     free, _ = torch.cuda.mem_get_info()
-    srv = S.Server(S.DeviceBackend(pkg, precision=pkg.capi.PREC_MIXED), budget_bytes=int(0.5 * free), max_slots=n)
-    bat = srv.run(mk())
     keys = ("dof_timesteps_per_s", "step_ms_p50", "step_ms_p99", "request_latency_s_p50", "request_latency_s_p99",
             "wall_s", "completed", "steps")
+    runs = {}
+    for cap in slots:
+        srv = S.Server(S.DeviceBackend(pkg, precision=pkg.capi.PREC_MIXED), budget_bytes=int(0.5 * free),
+                       max_slots=cap or n)
+        r = srv.run(mk())
+        runs[cap or n] = {k: r[k] for k in keys} | {"peak_slots": r["peak_slots"],
+                                                   "throughput_ratio": r["dof_timesteps_per_s"] / max(seq["dof_timesteps_per_s"], 1e-30)}
+    bat = runs[slots[0] or n]
     return {
         "sample": f"{n} requests of the seeded serving stream (Poisson {rate:g}/s; Nx {min(nx)}-{max(nx)}, "
                   f"Ny {min(ny)}-{max(ny)}, Nz {min(nz)}-{max(nz)}; {steps[0]}-{steps[1]} steps each instead of "
                   f"100-2000, {note})",
-        "batched_mixed": {k: bat[k] for k in keys} | {"peak_slots": bat["peak_slots"]},
+        "batched_mixed": bat,
         "sequential_fp64": {k: seq[k] for k in keys},
-        "throughput_ratio": bat["dof_timesteps_per_s"] / max(seq["dof_timesteps_per_s"], 1e-30),
+        "throughput_ratio": bat["throughput_ratio"],
+        **({"batched_mixed_by_slot_cap": runs} if len(slots) > 1 else {}),
     }
 
 
@@ -352,7 +359,8 @@ def profile_step(args):
         # generation zone and the sponge
         sys.path.insert(0, str(ROOT / "tests"))
         import cases
-        p, geo, target = cases.shoal_generation(pkg.workloads, 4, precision=prec)
+        gkw = dict(zip(("Nx", "Ny", "Nz"), (int(v) for v in args.grid.lower().split("x")))) if args.grid else {}
+        p, geo, target = cases.shoal_generation(pkg.workloads, 4, precision=prec, **gkw)
         sim = pkg.Simulation(p, **geo)
         graphs_off(sim)
         sim.set_relax_target(0, *target(sim.zone_box(0)))
@@ -428,6 +436,7 @@ def main():
                     help="largest: the 2049x513x9 instance at three GMRES tolerances (one JSON line each); "
                          "serving: the serving stream with the configuration's size sets (one JSON line)")
     ap.add_argument("--requests", type=int, default=48, help="--config serving: number of requests")
+    ap.add_argument("--slots", default=None, help="--config serving: comma-separated slot caps (default: no cap)")
     args = ap.parse_args()
     if args.profile:
         profile_step(args)
@@ -441,8 +450,10 @@ def main():
         import torch
         torch.cuda.set_device(0)
         S = package().serving
+        caps = tuple(int(c) for c in args.slots.split(",")) if args.slots else (None,)
         out = serving_sample(n=args.requests, seed=2024, rate=4.0, nx=S.NX_SET, ny=S.NY_SET, nz=S.NZ_SET,
-                             steps=(10, 200), note="the configuration's size sets, step counts scaled down 10x")
+                             steps=(10, 200), note="the configuration's size sets, step counts scaled down 10x",
+                             slots=caps)
         print(json.dumps({"config": "serving stream", "unit": UNIT, **out}))
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))

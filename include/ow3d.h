@@ -363,6 +363,21 @@ int ow3d_stream_function_wave(const ow3d_params* p, int n, const double* x, doub
  * OW3D_ERR_UNSUPPORTED. */
 int ow3d_incident_wave(const ow3d_params* p, int zone, int nt, double* eta, double* phis, int* box);
 
+/* The incident wave of IncWaveType 2 on generation zone `zone` (0-based),
+ * synthesised on the device and installed as the zone's relaxation target
+ * (mode 0: sampled every dt, mid-stage targets averaged), without the series
+ * crossing the host: the same wave as ow3d_incident_wave followed by
+ * ow3d_set_relax_target(h, zone, 0, nt, dt, ...), to rounding. The
+ * amplitudes, wavenumbers and headings (the reference's sequential random
+ * generator, a few thousand numbers) are set up on the host; every sample at
+ * every point of the zone is formed on the device -- the mono-chromatic wave
+ * in closed form, random waves as the sum over their modes that the
+ * reference's inverse real transform evaluates (random_wave_signal.f90:48-172,
+ * random_wave_signal_3D.f90). nt: the samples to build, at most the count
+ * ow3d_incident_wave reports in box[4] for random waves. Replaces: the
+ * RandomWave(i)%eta, %Phis set-up of OceanWave3DT0Setup.f90:176-255. */
+int ow3d_incident_wave_device(ow3d_handle* h, int zone, int nt);
+
 /* Relaxation-zone target signal for generation zone `zone` (0-based):
  * nt samples of eta and surface phi on the zone rectangle (i fastest, then j,
  * ghost-inclusive index box of the zone), sampled every dt_sample from t=0.

@@ -63,6 +63,13 @@ long long ow3d_test_set_coop_max_points(long long points);
  * previous value. Process-wide. */
 int ow3d_test_set_colour_tiles(int min_tiles);
 
+/* Per-level colour pass launch form: 0 (the default) one pass over the
+ * columns with up to 32 blocks per SM; 1 the grid capped at the 4 resident
+ * blocks per SM, each warp prefetching its next group of columns into L1;
+ * 2 the capped grid alone. Results are bitwise the same. Returns the
+ * previous value. Process-wide. */
+int ow3d_test_set_colour_prefetch(int mode);
+
 /* Number of captured Arnoldi-step graphs the handle holds, or -1 when a
  * capture failed and the handle launches kernels directly. */
 int ow3d_test_graph_count(const ow3d_handle* h);
@@ -70,6 +77,10 @@ int ow3d_test_graph_count(const ow3d_handle* h);
 /* Number of whole-step graphs the handle holds (0..2, one per step parity),
  * or -1 when a step capture failed and the handle steps directly. */
 int ow3d_test_step_graph_count(const ow3d_handle* h);
+
+/* The relaxation target of generation zone `zone` as the device holds it:
+ * nt x box samples each of eta and phis (either may be NULL). */
+int ow3d_test_relax_target(const ow3d_handle* h, int zone, double* eta, double* phis);
 
 /* Device time of `reps` launches of one kernel on this handle's stream,
  * measured with CUDA events around each launch; before each launch a write of

@@ -61,8 +61,10 @@ def lib():
         L.ow3d_test_set_coop_max_points.argtypes = [_C.c_longlong]
         L.ow3d_test_set_coop_max_points.restype = _C.c_longlong
         L.ow3d_test_set_colour_tiles.argtypes = [_C.c_int]
+        L.ow3d_test_set_colour_prefetch.argtypes = [_C.c_int]
         L.ow3d_test_graph_count.argtypes = [_C.c_void_p]
         L.ow3d_test_step_graph_count.argtypes = [_C.c_void_p]
+        L.ow3d_test_relax_target.argtypes = [_C.c_void_p, _C.c_int, D, D]
         _lib = L
     return _lib
 
@@ -309,6 +311,20 @@ class Simulation:
     def set_relax_target(self, zone, mode, nt, dt_sample, eta, phis):
         _check(lib().ow3d_set_relax_target(self.h, zone, mode, nt, float(dt_sample), _d(_f64(eta).ravel()),
                                            _d(_f64(phis).ravel())), "ow3d_set_relax_target")
+
+    def incident_wave_device(self, zone, nt):
+        """Synthesise the deck's IncWaveType 2 incident wave for generation zone
+        `zone` on the device and install it as the zone's relaxation target
+        (ow3d_incident_wave_device)."""
+        _check(lib().ow3d_incident_wave_device(self.h, zone, int(nt)), "ow3d_incident_wave_device")
+
+    def relax_target(self, zone, nt):
+        """The zone's relaxation target as the device holds it: (nt, box) eta, phis."""
+        i0, i1, j0, j1 = self.zone_box(zone)
+        box = (i1 - i0 + 1) * (j1 - j0 + 1)
+        e, f = _np.zeros(nt * box), _np.zeros(nt * box)
+        _check(lib().ow3d_test_relax_target(self.h, zone, _d(e), _d(f)), "ow3d_test_relax_target")
+        return e.reshape(nt, box), f.reshape(nt, box)
 
     def zone_box(self, zone):
         a, b, c, d = (_C.c_int() for _ in range(4))

@@ -166,6 +166,7 @@ def declare(lib):
         "ow3d_step_timed": (C.c_int, [H, C.c_int, _D]),
         "ow3d_last_error": (C.c_char_p, []),
         "ow3d_set_relax_target": (C.c_int, [H, C.c_int, C.c_int, C.c_int, C.c_double, _D, _D]),
+        "ow3d_incident_wave_device": (C.c_int, [H, C.c_int, C.c_int]),
         "ow3d_step": (C.c_int, [H, C.c_int]),
         "ow3d_step_batch": (C.c_int, [C.POINTER(H), C.c_int, _I, _I, _D]),
         "ow3d_get_stats": (C.c_int, [H, C.POINTER(Stats)]),

@@ -62,15 +62,21 @@ __global__ void k_lo_bottom(LevelDev<T> L) {
 }
 
 // Per-level colour pass: two rows per lane (colour_warp2), S lanes per column.
+// With prefetch set, each warp asks for the next group's column data (its
+// rows of x in the column and the four neighbour columns, and of b) to be
+// brought into L1 before it solves the current group.
 template <typename T, bool THREE, int S, bool CROSS>
-__global__ void __launch_bounds__(128, 4) k_lo_colour(LevelDev<T> L, int colour) {
+__global__ void __launch_bounds__(128, 4) k_lo_colour(LevelDev<T> L, int colour, int prefetch) {
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t total = colour_count<T, THREE>(L);
     const int r = (threadIdx.x & 31) & (S - 1);
     const RowConst<T> rka = row_const_k<T>(L, 2 + 2 * r), rkb = row_const_k<T>(L, 3 + 2 * r);
-    for (int base = (int)warp * (32 / S); base < (int)total; base += (int)nwarps * (32 / S))
+    const int step = (int)nwarps * (32 / S);
+    for (int base = (int)warp * (32 / S); base < (int)total; base += step) {
+        if (prefetch && base + step < (int)total) colour_prefetch<T, THREE, S>(L, colour, base + step);
         colour_warp2<T, THREE, S, CROSS>(L, colour, base, rka, rkb);
+    }
 }
 
 // ------------------------------------------------- tiled colour pass
@@ -414,10 +420,16 @@ static void colour_launch(const LevelDev<T>& L, int c, cudaStream_t st) {
     const int64_t cols = (int64_t)((L.Nxg - 1) / 2) * (THREE ? L.Nyg - 2 : 1);
     const int64_t warps = (cols + (32 / S) - 1) / (32 / S);
     int64_t blocks = (warps * 32 + 127) / 128;
-    if (blocks > 148 * 32) blocks = 148 * 32;
+    // g_colour_prefetch: 0 = one pass over the columns with up to 32 blocks
+    // per SM; 1 = the grid capped at the resident 4 blocks per SM, each warp
+    // prefetching its next group into L1; 2 = the capped grid alone
+    const int pf = g_colour_prefetch.load(std::memory_order_relaxed);
+    const int64_t cap = pf ? 148 * 4 : 148 * 32;
+    if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
-    if (L.cross) note_launch(), k_lo_colour<T, THREE, S, true><<<(int)blocks, 128, 0, st>>>(L, c);
-    else note_launch(), k_lo_colour<T, THREE, S, false><<<(int)blocks, 128, 0, st>>>(L, c);
+    const int pre = pf == 1 ? 1 : 0;
+    if (L.cross) note_launch(), k_lo_colour<T, THREE, S, true><<<(int)blocks, 128, 0, st>>>(L, c, pre);
+    else note_launch(), k_lo_colour<T, THREE, S, false><<<(int)blocks, 128, 0, st>>>(L, c, pre);
 }
 // Lanes per column of the two-rows-per-lane pass.
 inline int seg_width2(int Nzg) {
@@ -513,6 +525,7 @@ std::atomic<int64_t> g_coop_max_points{160000};
 // default: inside the solve the per-column pass measured faster, see the
 // launcher).
 std::atomic<int> g_colour_tiles{0};
+std::atomic<int> g_colour_prefetch{0};
 
 thread_local bool g_capture_unsafe = false;
 

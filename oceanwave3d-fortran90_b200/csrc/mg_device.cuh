@@ -829,6 +829,34 @@ __device__ __forceinline__ void colour_col2(const LevelDev<T>& L, int i, int j, 
     if (!TILE && edge) ghosts(true, xna, xnb, xfs);
 }
 
+// Ask for the column data of the group a warp solves from `base` on to be
+// brought into L1 (the rows of x this lane reads in the column and its four
+// neighbours, and of b): one prefetch per 32-byte sector the lane touches.
+template <typename T, bool THREE, int S>
+__device__ __forceinline__ void colour_prefetch(const LevelDev<T>& L, int colour, int base) {
+    const int Nxg = L.Nxg, Nyg = L.Nyg, Nzg = L.Nzg;
+    const int lane = threadIdx.x & 31, r = lane & (S - 1);
+    const int nxi = Nxg - 2 - L.per, nyi = THREE ? Nyg - 2 : 1;
+    const bool four = (L.ncolor == 4);
+    const int ni = (nxi + 1) / 2, nj = four ? (nyi + 1) / 2 : nyi;
+    const int q = base + (lane / S);
+    if (q >= ni * nj) return;
+    const int tj = q / ni, ti = q - tj * ni;
+    int i, j;
+    if (four) { j = THREE ? 2 + 2 * tj + (colour >> 1) : 1; i = 2 + 2 * ti + (colour & 1); }
+    else { j = THREE ? 2 + tj : 1; i = 2 + 2 * ti + ((colour + j) & 1); }
+    if (i > Nxg - 1 - L.per || (THREE && j > Nyg - 1)) return;
+    const int64_t c = (int64_t)(i - 1) + (int64_t)Nxg * (j - 1);
+    const int k = min(2 + 2 * r, Nzg - 1) - 1;
+    const T* x = L.xv + c * Nzg + k;
+    auto pf = [](const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); };
+    pf(x);
+    pf(x + xoff_l(L, i));
+    pf(x + xoff_r(L, i));
+    if (THREE) { pf(x - (int64_t)Nzg * Nxg); pf(x + (int64_t)Nzg * Nxg); }
+    pf(L.bv + c * Nzg + k);
+}
+
 // The colour's columns in order (rows of constant j, i fastest), 32/S per
 // warp from column `base` on.
 template <typename T, bool THREE, int S, bool CROSS>

@@ -1103,6 +1103,7 @@ unsigned long long ow3d_launch_count(void) { return g_kernel_launches.load(std::
 
 int ow3d_test_set_coarse_blocks(int blocks) { return g_coarse_blocks.exchange(blocks < 0 ? 0 : blocks); }
 int ow3d_test_set_colour_tiles(int min_tiles) { return g_colour_tiles.exchange(min_tiles < 0 ? 0 : min_tiles); }
+int ow3d_test_set_colour_prefetch(int mode) { return g_colour_prefetch.exchange(mode < 0 ? 0 : mode); }
 long long ow3d_test_set_coop_max_points(long long points) {
     return g_coop_max_points.exchange(points < 0 ? 0 : (int64_t)points);
 }
@@ -1377,6 +1378,80 @@ int ow3d_set_relax_target(ow3d_handle* H, int zone, int mode, int nt, double dts
     CK(cudaMemcpy(dp, phis, box * nt * sizeof(double), cudaMemcpyHostToDevice));
     z.eta = de; z.phis = dp; z.nt = nt; z.tdt = dts; z.tmode = mode;
     drop_step_graphs(H);   // the captured relaxation launches hold the old table
+    return OW3D_OK;
+}
+
+int ow3d_incident_wave_device(ow3d_handle* H, int zone, int nt) {
+    if (!H) return OW3D_ERR_BAD_INPUT;
+    if (zone < 0 || zone >= (int)H->zones.size()) { g_last_error = "ow3d_incident_wave_device: no such zone"; return OW3D_ERR_BAD_INPUT; }
+    CK(cudaSetDevice(H->dev));
+    IncidentWave w;
+    std::string err;
+    if (int r = incident_wave_setup(H->p, zone, nt, w, nullptr, nullptr, &err)) { g_last_error = err; return r; }
+    RelaxZoneDev& z = H->zones[(size_t)zone];
+    const size_t box = (size_t)(z.i1 - z.i0 + 1) * (z.j1 - z.j0 + 1);
+    if (box != (size_t)w.bx * w.by) { g_last_error = "ow3d_incident_wave_device: zone box mismatch"; return OW3D_ERR_BAD_INPUT; }
+    // the series, kept as the zone's target for the handle's lifetime
+    double *de, *dp;
+    TRY(dalloc(H, &de, box * (size_t)nt)); TRY(dalloc(H, &dp, box * (size_t)nt));
+    // the components and work arrays, freed at the end of the call
+    std::vector<void*> tmp;
+    auto put = [&](const void* src, size_t bytes) -> void* {
+        void* d = nullptr;
+        if (cudaMalloc(&d, bytes ? bytes : 16) != cudaSuccess) return nullptr;
+        tmp.push_back(d);
+        if (bytes) cudaMemcpy(d, src, bytes, cudaMemcpyHostToDevice);
+        return d;
+    };
+    auto release = [&]() { for (void* q : tmp) cudaFree(q); };
+    const double pi = std::acos(-1.0);
+    std::vector<double> dy_rows((size_t)w.by, 0.0);
+    if (w.heading) dy_rows = w.dy;
+    IncidentWaveDev d{};
+    d.bx = w.bx; d.by = w.by; d.nt = nt; d.ny_eval = w.ny_eval; d.N = w.N; d.kmax = w.kmax;
+    d.heading = w.heading ? 1 : 0; d.mono = w.mono ? 1 : 0;
+    d.cosb = w.cosb; d.sinb = w.sinb; d.g = w.g; d.domega = w.domega;
+    d.amp = w.amp; d.nu = w.nu; d.omega = w.omega; d.phifact = w.phifact; d.t0 = w.t0; d.dt = w.dt;
+    d.dx = (const double*)put(w.dx.data(), w.dx.size() * sizeof(double));
+    d.dy = (const double*)put(w.dy.data(), w.dy.size() * sizeof(double));
+    d.dy_rows = (const double*)put(dy_rows.data(), dy_rows.size() * sizeof(double));
+    if (!w.mono) {
+        std::vector<double2> c((size_t)w.kmax), W((size_t)w.N);
+        for (int k = 0; k < w.kmax; ++k) c[(size_t)k] = make_double2(w.c[(size_t)k].real(), w.c[(size_t)k].imag());
+        for (int m = 0; m < w.N; ++m) {
+            const double a = -2.0 * pi * (double)m / (double)w.N;
+            W[(size_t)m] = make_double2(std::cos(a), std::sin(a));
+        }
+        d.c = (const double2*)put(c.data(), c.size() * sizeof(double2));
+        d.W = (const double2*)put(W.data(), W.size() * sizeof(double2));
+        d.nus = (const double*)put(w.nus.data(), w.nus.size() * sizeof(double));
+        if (!w.kcos.empty()) {
+            d.kcos = (const double*)put(w.kcos.data(), w.kcos.size() * sizeof(double));
+            d.ksin = (const double*)put(w.ksin.data(), w.ksin.size() * sizeof(double));
+        }
+        const size_t modes = (size_t)w.bx * w.ny_eval * (size_t)w.kmax;
+        d.A = (double2*)put(nullptr, modes * sizeof(double2));
+        d.B = (double2*)put(nullptr, modes * sizeof(double2));
+    }
+    for (void* q : tmp)
+        if (!q) { release(); g_last_error = "ow3d_incident_wave_device: device allocation failed"; return OW3D_ERR_OOM; }
+    int r = launch_incident_wave(d, de, dp, H->st);
+    if (r == OW3D_OK && cudaStreamSynchronize(H->st) != cudaSuccess) r = OW3D_ERR_CUDA;
+    release();
+    if (r) { g_last_error = "ow3d_incident_wave_device: kernel failed"; return r; }
+    z.eta = de; z.phis = dp; z.nt = nt; z.tdt = H->p.dt; z.tmode = 0;
+    drop_step_graphs(H);   // the captured relaxation launches hold the old table
+    return OW3D_OK;
+}
+
+int ow3d_test_relax_target(const ow3d_handle* H, int zone, double* eta, double* phis) {
+    if (!H || zone < 0 || zone >= (int)H->zones.size()) return OW3D_ERR_BAD_INPUT;
+    const RelaxZoneDev& z = H->zones[(size_t)zone];
+    if (!z.eta || z.nt <= 0) return OW3D_ERR_BAD_INPUT;
+    CK(cudaSetDevice(H->dev));
+    const size_t n = (size_t)(z.i1 - z.i0 + 1) * (z.j1 - z.j0 + 1) * (size_t)z.nt * sizeof(double);
+    if (eta) CK(cudaMemcpy(eta, z.eta, n, cudaMemcpyDeviceToHost));
+    if (phis) CK(cudaMemcpy(phis, z.phis, n, cudaMemcpyDeviceToHost));
     return OW3D_OK;
 }
 

@@ -23,6 +23,7 @@ extern std::atomic<unsigned long long> g_kernel_launches;
 extern std::atomic<int> g_coarse_blocks;
 extern std::atomic<int64_t> g_coop_max_points;
 extern std::atomic<int> g_colour_tiles;
+extern std::atomic<int> g_colour_prefetch;
 // Set (on the capturing thread) when a launch sequence under stream capture
 // issued a host-to-device copy whose source the host later overwrites.
 extern thread_local bool g_capture_unsafe;
@@ -142,6 +143,20 @@ inline void div_magic32(uint32_t d, uint32_t& m, int& sh) {
 #ifdef __CUDACC__
 __device__ __forceinline__ uint32_t div32(uint32_t n, uint32_t m, int sh) { return __umulhi(n, m) >> sh; }
 #endif
+
+// The incident wave of a generation zone on the device (incwave.cu): the
+// components set up on the host (incident_wave_setup), device copies.
+struct IncidentWaveDev {
+    int bx, by, nt, ny_eval, N, kmax, heading, mono;
+    double cosb, sinb, g, domega;
+    double amp, nu, omega, phifact, t0, dt;   // mono-chromatic wave
+    const double *dx, *dy, *dy_rows;          // [bx], [ny_eval], [by]
+    const double *nus, *kcos, *ksin;          // [kmax]; kcos, ksin null unless spread
+    const double2 *c, *W;                     // amplitudes [kmax], twiddles [N]
+    double2 *A, *B;                           // per point and mode [ny_eval*bx][kmax]
+};
+// eta, phis: nt x (bx*by) samples (i fastest, then j), the zone's target layout.
+int launch_incident_wave(const IncidentWaveDev& w, double* eta, double* phis, cudaStream_t st);
 
 // sqrt(sum y^2) of a device vector using only fixed file-scope device scratch
 // (noalloc.cu); result written to host memory, stream synchronised.

@@ -629,8 +629,10 @@ int incident_wave_samples(const ow3d_params& p) {
 //    and summed over the N = nt_ref samples t = n dt as the inverse real
 //    transform does: eta_n = sum_k Re(c_k e^(i nu_k d) e^(-2 pi i k n / N)),
 //    phiS likewise with g/omega_k (-i) c_k.
-int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* phis, int* box, std::string* err) {
+int incident_wave_setup(const ow3d_params& p, int zone, int nt, IncidentWave& w, int* box, bool* query_only,
+                        std::string* err) {
     auto fail = [&](const std::string& m, int code) { if (err) *err = m; return code; };
+    if (query_only) *query_only = false;
     if (p.relaxONOFF != 1 || zone < 0 || zone >= p.relaxNo || zone >= OW3D_MAX_ZONES)
         return fail("incident_wave: no such relaxation zone", OW3D_ERR_BAD_INPUT);
     const ow3d_zone& d = p.zones[zone];
@@ -648,7 +650,7 @@ int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* p
     const ZoneHost& z = Z[(size_t)zone];
     const int nref = incident_wave_samples(p);
     if (box) { box[0] = z.i0; box[1] = z.i1; box[2] = z.j0; box[3] = z.j1; box[4] = nref; }
-    if (!eta && !phis) return OW3D_OK;   // the box query works for every deck
+    if (query_only) { *query_only = true; return OW3D_OK; }
     if (p.IncWaveType != 2) return fail("incident_wave: the deck's IncWaveType is not 2", OW3D_ERR_BAD_INPUT);
     if (!(p.ispec == -1 || p.ispec == 0 || p.ispec == 1 || p.ispec == 3 || p.ispec == -30 || p.ispec == 30 ||
           p.ispec == 31 || p.ispec == 33 || p.ispec == 34))
@@ -662,96 +664,121 @@ int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* p
     if (p.ispec >= 0 && nt > nref)
         return fail("incident_wave: a random wave has " + std::to_string(nref) + " samples", OW3D_ERR_BAD_INPUT);
     const double pi = std::acos(-1.0), two = 2.0, twopi = two * pi;
-    const int bx = z.i1 - z.i0 + 1, by = z.j1 - z.j0 + 1;
+    w = IncidentWave{};
+    w.bx = z.i1 - z.i0 + 1;
+    w.by = z.j1 - z.j0 + 1;
+    w.nt = nt;
+    w.g = p.g;
     // long-crested along x (|ispec| < 30): one x line, repeated on the rows;
     // at heading beta0 (random_wave_signal_3D.f90): every point of the box
-    const bool heading = std::abs(p.ispec) >= 30;
-    const int ny_eval = heading ? by : 1;
-    const double cosb = heading ? std::cos(pi / 180.0 * p.beta0) : 1.0;
-    const double sinb = heading ? std::sin(pi / 180.0 * p.beta0) : 0.0;
-    auto dist_of = [&](int i, int j) {
-        const double dx = G.x[(size_t)(z.i0 - 1 + i)] - p.x0;
-        const double dy = heading ? G.y[(size_t)(z.j0 - 1 + j)] - p.y0 : 0.0;
-        return cosb * dx + sinb * dy;
-    };
-    // per-frequency headings of a spread sea (ispec 34), cos and sin, index k
-    std::vector<double> kcos, ksin;
+    w.heading = std::abs(p.ispec) >= 30;
+    w.ny_eval = w.heading ? w.by : 1;
+    w.cosb = w.heading ? std::cos(pi / 180.0 * p.beta0) : 1.0;
+    w.sinb = w.heading ? std::sin(pi / 180.0 * p.beta0) : 0.0;
+    w.dx.resize((size_t)w.bx);
+    w.dy.assign((size_t)w.ny_eval, 0.0);
+    for (int i = 0; i < w.bx; ++i) w.dx[(size_t)i] = G.x[(size_t)(z.i0 - 1 + i)] - p.x0;
+    if (w.heading)
+        for (int j = 0; j < w.ny_eval; ++j) w.dy[(size_t)j] = G.y[(size_t)(z.j0 - 1 + j)] - p.y0;
+    if (p.ispec < 0) {
+        w.mono = true;
+        w.omega = twopi / p.Tp;
+        w.nu = fd_wavenumber(p.h0, w.omega, p.g);
+        w.amp = p.Hs / two;
+        w.phifact = p.g / w.omega;
+        w.t0 = p.time0;
+        w.dt = p.dt;
+        return OW3D_OK;
+    }
+    const int N = nref;
+    w.N = N;
+    const double df = 1.0 / (N * p.dt), cst = std::sqrt(df);
+    w.domega = twopi / (N * p.dt);
+    const bool pm = (p.ispec == 0 || p.ispec == 30);   // the others: JONSWAP
+    std::vector<std::complex<double>> c((size_t)N / 2, 0.0);
+    std::vector<double>& kcos = w.kcos;
+    std::vector<double>& ksin = w.ksin;
+    Ran1 rng;
+    int seed2 = p.seed2;
+    if (p.ispec == 34) {
+        // build_coeff_3D_Cos.f90:38-52: the headings take the first N/2
+        // deviates; converted to degrees and back for the phase
+        const std::vector<double> b = spread_headings(rng, seed2, p.s0, p.beta0, N / 2);
+        kcos.assign((size_t)N / 2, 0.0); ksin.assign((size_t)N / 2, 0.0);
+        const double rad2deg = 1.0 / (pi / 180.0), deg2rad = pi / 180.0;
+        for (int k = 1; k < N / 2; ++k) {
+            const double deg = b[(size_t)(k + 1)] * rad2deg;   // beta(i) with i = k + 1
+            kcos[(size_t)k] = std::cos(deg2rad * deg);
+            ksin[(size_t)k] = std::sin(deg2rad * deg);
+        }
+    }
+    for (int i = 2; i <= N / 2; ++i) {
+        const double freq = (i - 1) * df;
+        const double psi = (double)rng.next(seed2);
+        const float cr = (float)std::cos(twopi * psi), ci = (float)std::sin(twopi * psi);
+        const double spec = pm ? pm_spectrum(freq, p.Hs, p.Tp) : jonswap_spectrum(freq, p.Hs, p.Tp, p.gamma_jonswap);
+        const double a = std::sqrt(two * spec) * cst;
+        c[(size_t)(i - 1)] = std::complex<double>(a * (double)cr, a * (double)ci);
+        if (p.ispec == 33) {
+            // build_coeff_3D.f90:44-58: a normally spread heading from the
+            // same deviate; the reference's InvErf returns -1 for a
+            // negative argument (ErfReal.f90:406-409), kept as it is
+            const double rad2deg = 180.0 / pi, fp = 1.0 / p.Tp;
+            const double sigma = 0.2 * std::pow(freq / fp, 2.5);
+            const double erf1 = std::erf(pi / (two * std::sqrt(two * sigma)));
+            const double arg = (two * psi - 1.0) * erf1;
+            const double erf2 = arg >= 0.0 ? inverse_erf(arg) : -1.0;
+            const double deg = p.beta0 + rad2deg * std::sqrt(2.0 * sigma) * erf2;
+            if (kcos.empty()) { kcos.assign((size_t)N / 2, 0.0); ksin.assign((size_t)N / 2, 0.0); }
+            kcos[(size_t)(i - 1)] = std::cos(pi / 180.0 * deg);
+            ksin[(size_t)(i - 1)] = std::sin(pi / 180.0 * deg);
+        }
+    }
+    // truncation at kh_max (random_wave_coefficients.f90:92-100): the
+    // coefficients from index n_cut - 1 on are zero
+    const int n_cut = (int)std::lround(std::sqrt(p.g * p.kh_max / p.h0 * std::tanh(p.kh_max)) / w.domega) + 1;
+    for (int k = std::max(n_cut - 1, 1); k < N / 2; ++k) c[(size_t)k] = 0.0;
+    w.kmax = std::min(n_cut, N / 2);
+    w.c.assign(c.begin(), c.begin() + std::max(w.kmax, 1));
+    w.nus.assign((size_t)std::max(w.kmax, 1), 0.0);
+    for (int k = 1; k < w.kmax; ++k) w.nus[(size_t)k] = fd_wavenumber(p.h0, k * w.domega, p.g);
+    return OW3D_OK;
+}
+
+int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* phis, int* box, std::string* err) {
+    IncidentWave w;
+    bool query = false;
+    const int r = incident_wave_setup(p, zone, nt, w, box, (!eta && !phis) ? &query : nullptr, err);
+    if (r || query) return r;   // the box query works for every deck
+    const int bx = w.bx, by = w.by, ny_eval = w.ny_eval;
     std::vector<double> le((size_t)nt * bx * ny_eval), lp(le.size());   // [n][j][i]
     auto at = [&](int n, int j, int i) { return ((size_t)n * ny_eval + j) * bx + i; };
-    if (p.ispec < 0) {
-        const double omega = twopi / p.Tp;
-        const double nu = fd_wavenumber(p.h0, omega, p.g);
-        const double amp = p.Hs / two, phifact = p.g / omega;
+    auto dist_of = [&](int i, int j) { return w.cosb * w.dx[(size_t)i] + w.sinb * w.dy[(size_t)j]; };
+    if (w.mono) {
+        // random_wave_signal.f90:151-172
         for (int n = 0; n < nt; ++n) {
-            const double t = p.time0 + n * p.dt;
+            const double t = w.t0 + n * w.dt;
             for (int j = 0; j < ny_eval; ++j)
                 for (int i = 0; i < bx; ++i) {
                     const double dist = dist_of(i, j);
-                    le[at(n, j, i)] = amp * std::cos(nu * dist - omega * t);
-                    lp[at(n, j, i)] = phifact * amp * std::sin(nu * dist - omega * t);
+                    le[at(n, j, i)] = w.amp * std::cos(w.nu * dist - w.omega * t);
+                    lp[at(n, j, i)] = w.phifact * w.amp * std::sin(w.nu * dist - w.omega * t);
                 }
         }
     } else {
-        const int N = nref;
-        const double df = 1.0 / (N * p.dt), cst = std::sqrt(df), domega = twopi / (N * p.dt);
-        const bool pm = (p.ispec == 0 || p.ispec == 30);   // the others: JONSWAP
-        std::vector<std::complex<double>> c((size_t)N / 2, 0.0);
-        Ran1 rng;
-        int seed2 = p.seed2;
-        if (p.ispec == 34) {
-            // build_coeff_3D_Cos.f90:38-52: the headings take the first N/2
-            // deviates; converted to degrees and back for the phase
-            const std::vector<double> b = spread_headings(rng, seed2, p.s0, p.beta0, N / 2);
-            kcos.assign((size_t)N / 2, 0.0); ksin.assign((size_t)N / 2, 0.0);
-            const double rad2deg = 1.0 / (pi / 180.0), deg2rad = pi / 180.0;
-            for (int k = 1; k < N / 2; ++k) {
-                const double deg = b[(size_t)(k + 1)] * rad2deg;   // beta(i) with i = k + 1
-                kcos[(size_t)k] = std::cos(deg2rad * deg);
-                ksin[(size_t)k] = std::sin(deg2rad * deg);
-            }
-        }
-        for (int i = 2; i <= N / 2; ++i) {
-            const double freq = (i - 1) * df;
-            const double psi = (double)rng.next(seed2);
-            const float cr = (float)std::cos(twopi * psi), ci = (float)std::sin(twopi * psi);
-            const double spec = pm ? pm_spectrum(freq, p.Hs, p.Tp) : jonswap_spectrum(freq, p.Hs, p.Tp, p.gamma_jonswap);
-            const double a = std::sqrt(two * spec) * cst;
-            c[(size_t)(i - 1)] = std::complex<double>(a * (double)cr, a * (double)ci);
-            if (p.ispec == 33) {
-                // build_coeff_3D.f90:44-58: a normally spread heading from the
-                // same deviate; the reference's InvErf returns -1 for a
-                // negative argument (ErfReal.f90:406-409), kept as it is
-                const double rad2deg = 180.0 / pi, fp = 1.0 / p.Tp;
-                const double sigma = 0.2 * std::pow(freq / fp, 2.5);
-                const double erf1 = std::erf(pi / (two * std::sqrt(two * sigma)));
-                const double arg = (two * psi - 1.0) * erf1;
-                const double erf2 = arg >= 0.0 ? inverse_erf(arg) : -1.0;
-                const double deg = p.beta0 + rad2deg * std::sqrt(2.0 * sigma) * erf2;
-                if (kcos.empty()) { kcos.assign((size_t)N / 2, 0.0); ksin.assign((size_t)N / 2, 0.0); }
-                kcos[(size_t)(i - 1)] = std::cos(pi / 180.0 * deg);
-                ksin[(size_t)(i - 1)] = std::sin(pi / 180.0 * deg);
-            }
-        }
-        // truncation at kh_max (random_wave_coefficients.f90:92-100): the
-        // coefficients from index n_cut - 1 on are zero
-        const int n_cut = (int)std::lround(std::sqrt(p.g * p.kh_max / p.h0 * std::tanh(p.kh_max)) / domega) + 1;
-        for (int k = std::max(n_cut - 1, 1); k < N / 2; ++k) c[(size_t)k] = 0.0;
-        const int kmax = std::min(n_cut, N / 2);
-        std::vector<double> nus((size_t)std::max(kmax, 1), 0.0);
-        for (int k = 1; k < kmax; ++k) nus[(size_t)k] = fd_wavenumber(p.h0, k * domega, p.g);
+        const int N = w.N;
         std::vector<std::complex<double>> ZE((size_t)N), ZP((size_t)N);
         for (int j = 0; j < ny_eval; ++j)
             for (int i = 0; i < bx; ++i) {
-                const double dx = G.x[(size_t)(z.i0 - 1 + i)] - p.x0;
-                const double dy = heading ? G.y[(size_t)(z.j0 - 1 + j)] - p.y0 : 0.0;
                 std::fill(ZE.begin(), ZE.end(), 0.0);
                 std::fill(ZP.begin(), ZP.end(), 0.0);
-                for (int k = 1; k < kmax; ++k) {
-                    const double omega = k * domega, nu = nus[(size_t)k];
-                    const double dist = kcos.empty() ? dist_of(i, j) : kcos[(size_t)k] * dx + ksin[(size_t)k] * dy;
+                for (int k = 1; k < w.kmax; ++k) {
+                    const double omega = k * w.domega, nu = w.nus[(size_t)k];
+                    const double dist = w.kcos.empty() ? dist_of(i, j)
+                                                       : w.kcos[(size_t)k] * w.dx[(size_t)i] + w.ksin[(size_t)k] * w.dy[(size_t)j];
                     const std::complex<double> e =
-                        c[(size_t)k] * std::complex<double>(std::cos(nu * dist), std::sin(nu * dist));
-                    const std::complex<double> v = (p.g / omega) * std::complex<double>(e.imag(), -e.real());
+                        w.c[(size_t)k] * std::complex<double>(std::cos(nu * dist), std::sin(nu * dist));
+                    const std::complex<double> v = (w.g / omega) * std::complex<double>(e.imag(), -e.real());
                     ZE[(size_t)k] = e; ZE[(size_t)(N - k)] = std::conj(e);
                     ZP[(size_t)k] = v; ZP[(size_t)(N - k)] = std::conj(v);
                 }
@@ -767,7 +794,7 @@ int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* p
         for (int j = 0; j < by; ++j)
             for (int i = 0; i < bx; ++i) {
                 const size_t q = (size_t)n * bx * by + (size_t)j * bx + i;
-                const size_t src = at(n, heading ? j : 0, i);
+                const size_t src = at(n, w.heading ? j : 0, i);
                 if (eta) eta[q] = le[src];
                 if (phis) phis[q] = lp[src];
             }

@@ -2,6 +2,7 @@
 // relaxation zones and filter coefficients (the device-relevant half of
 // OceanWave3DT0Setup, src/main/OceanWave3DT0Setup.f90:35-444).
 #pragma once
+#include <complex>
 #include <string>
 #include <vector>
 #include "../../include/ow3d.h"
@@ -101,6 +102,30 @@ void stream_function_eval(const SFWave& w, int nx, const double* x, double t, do
 int initial_condition(const ow3d_params& p, double* h, double* hx, double* hxx, double* hy, double* hyy, double* E,
                       double* P, std::string* err);
 int incident_wave(const ow3d_params& p, int zone, int nt, double* eta, double* phis, int* box, std::string* err);
+
+// The incident wave of a generation zone as its components, shared by the
+// host synthesis (incident_wave) and the device kernels (incwave.cu). The
+// series is evaluated on the zone box's points: long-crested waves on one x
+// line (ny_eval = 1, repeated on the rows), waves at a heading on every row.
+// The point (i, j) lies at dx[i], dy[j] from the wave's origin; the
+// mono-chromatic wave is amp cos(nu d - omega t) with d = cosb dx + sinb dy
+// and t = t0 + n dt; a random wave is, at sample n,
+//   sum_{k=1}^{kmax-1} Re(c_k e^(i nu_k d_k) e^(-2 pi i k n / N)),
+// d_k = kcos_k dx + ksin_k dy for spread seas (kcos non-empty), else d, and
+// its surface potential likewise with (g / (k domega)) (-i) c_k.
+struct IncidentWave {
+    int bx = 0, by = 0, nt = 0, ny_eval = 1, N = 0, kmax = 0;
+    bool heading = false, mono = false;
+    double cosb = 1, sinb = 0, g = 9.81;
+    double omega = 0, nu = 0, amp = 0, phifact = 0, t0 = 0, dt = 0;   // mono-chromatic
+    double domega = 0;
+    std::vector<double> dx, dy;
+    std::vector<std::complex<double>> c;   // [kmax]
+    std::vector<double> nus, kcos, ksin;   // [kmax] ([N/2] for kcos, ksin)
+};
+// With query_only non-null the call only fills box (any deck) and sets *query_only.
+int incident_wave_setup(const ow3d_params& p, int zone, int nt, IncidentWave& w, int* box, bool* query_only,
+                        std::string* err);
 int read_deck(const char* path, ow3d_params* p, std::string* err);
 
 }  // namespace ow3d

@@ -380,3 +380,48 @@ def test_normally_spread_sea(ow3d, tmp_path):
         ce = np.conj(np.fft.fft(eta[:, cj, ci])[1:N // 2]) * 2 / N
         w = want * np.exp(1j * nu * (np.cos(beta) * dx + np.sin(beta) * dy))
         assert np.max(np.abs(ce - w)) < 1e-6 * np.abs(want).max(), (ci, cj)
+
+
+# ----------------------------------------------------------------- device
+
+_DEVICE_CASES = {
+    "mono": ("-1 1.25 0.04 0.8 35. 4 -34 1.5 0. run06.el 0.0", "400"),
+    "jonswap": ("1 1.25 0.04 0.8 20. 4 -34 0. 0. run06.el", "1000"),
+    "pm": ("0 1.25 0.04 0.8 20. 4 -34 0. 0. run06.el", "1000"),
+    "mono_heading": ("-30 1.25 0.04 0.8 35. 4 -34 1.5 0.5 run06.el 22.5 1.0 3.3", "400"),
+    "jonswap_heading": ("31 1.25 0.04 0.8 20. 4 -34 0. 0. run06.el 30.0 1.0 3.3", "1000"),
+    "normal_spread": ("33 1.25 0.04 0.8 20. 4 -34 0. 0.5 run06.el 0 1.0 3.3", "1000"),
+    "cos2s_spread": ("34 1.25 0.04 0.8 20. 4 -34 0. 0.5 run06.el 0 8.0 3.3", "1000"),
+}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", sorted(_DEVICE_CASES))
+def test_device_incident_wave_matches_host(ow3d, tmp_path, case):
+    """ow3d_incident_wave_device forms the series on the device (closed form
+    for the mono-chromatic wave, the direct sum over the modes for random
+    waves) and installs it as the zone's target: the same samples as the
+    host synthesis (ow3d_incident_wave, an FFT for random waves) to 1e-12 of
+    the wave's amplitude, and the same RK4 steps to 1e-12."""
+    line, nsteps = _DEVICE_CASES[case]
+    p = _heading_deck(tmp_path, line, nsteps=nsteps)
+    eta, phis, box = ow3d.incident_wave(p, 0)
+    nt = eta.shape[0]
+    Nxg, Nyg, _ = ow3d.dims(p)
+    geo = dict(h=np.full(Nxg * Nyg, p.h0))
+    dev = ow3d.Simulation(p, **geo)
+    dev.incident_wave_device(0, nt)
+    de, dp = dev.relax_target(0, nt)
+    he, hp = eta.reshape(nt, -1), phis.reshape(nt, -1)
+    assert np.max(np.abs(de - he)) <= 1e-12 * np.max(np.abs(he)), np.max(np.abs(de - he))
+    assert np.max(np.abs(dp - hp)) <= 1e-12 * np.max(np.abs(hp)), np.max(np.abs(dp - hp))
+    # the same steps with the host-built target
+    host = ow3d.Simulation(p, **geo)
+    host.set_relax_target(0, 0, nt, p.dt, eta, phis)
+    for s in (dev, host):
+        s.set_state(np.zeros(Nxg * Nyg), np.zeros(Nxg * Nyg))
+        assert s.step(6) >= 0
+    E1, E2 = dev.get_state()[0], host.get_state()[0]
+    assert np.max(np.abs(E2)) > 0
+    assert np.max(np.abs(E1 - E2)) <= 1e-12 * np.max(np.abs(E2))
+    dev.close(); host.close()
