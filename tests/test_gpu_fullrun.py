@@ -16,9 +16,15 @@ Against the reference-ordered oracle (_ref: lexicographic Gauss-Seidel and
 left-preconditioned GMRES with modified Gram-Schmidt, the order of
 GaussSeidel.f90 and iterative_solution.f90): the two algorithms stop at the
 same tolerance from different iterates, so the whole-run difference is of
-the order of the solver tolerance, not of rounding. The tests bound it
-(REF_TOL) and check the matvec totals of the whole run against the
-reference's (REF_ITER_FRAC).
+the order of the solver tolerance, not of rounding. Between the two oracle
+orderings themselves it is 5.5e-5 (eta, shoal, 1000 steps) and 1.0e-6 /
+6.4e-6 (eta / phi, flume, 200 steps), and the device-ordered FGMRES takes
+1.49x (shoal) and 1.32x (flume) the reference-ordered matvecs: its stopping
+test is on the true residual, the reference's on the preconditioned one. The
+tests bound the device's difference from the reference ordering (REF_TOL,
+about three times the oracle-to-oracle figure) and its matvec totals
+(REF_ITER_FRAC for FGMRES; the left-preconditioned device variant, with the
+reference's stopping test, within REF_ITER_FRAC_LEFT).
 """
 import pathlib
 
@@ -34,8 +40,9 @@ RTOL_RUN = 1e-10
 # reference ordering: relative L-infinity bound after the whole run, and the
 # relative difference of the run's matvec total (measured values are stated
 # in the assertion messages)
-REF_TOL = {"shoal": 1e-5, "sfwave": 1e-5}
+REF_TOL = {"shoal": 2e-4, "sfwave": 3e-5}
 REF_ITER_FRAC = 0.6
+REF_ITER_FRAC_LEFT = 0.25
 
 
 def rel(a, b):
@@ -56,12 +63,12 @@ def _check_dev(sim, g, its):
     assert np.all(d <= 4), (int(d.max()), int(np.argmax(d)))
 
 
-def _check_ref(sim, g, its, tol):
+def _check_ref(sim, g, its, tol, frac):
     E, P, W, phi, t = sim.get_state()
     errs = {"E": rel(E, g["E"]), "P": rel(P, g["P"]), "phi": rel(phi, g["phi"])}
     assert max(errs.values()) < tol, errs
     tot, ref = int(its.sum()), int(g["step_iterations"].sum())
-    assert abs(tot - ref) <= REF_ITER_FRAC * ref, (tot, ref)
+    assert abs(tot - ref) <= frac * ref, (tot, ref)
     return errs, tot, ref
 
 
@@ -97,7 +104,8 @@ def test_sfwave_200_steps_matches_device_ordered_oracle(ow3d):
 @pytest.mark.parametrize("krylov", [0, 1], ids=["fgmres", "left_gmres"])
 def test_shoal_1000_steps_against_reference_ordering(ow3d, krylov):
     sim, its = _shoal(ow3d, krylov)
-    errs, tot, ref = _check_ref(sim, load("run_shoal_257x33x9_1000_ref"), its, REF_TOL["shoal"])
+    errs, tot, ref = _check_ref(sim, load("run_shoal_257x33x9_1000_ref"), its, REF_TOL["shoal"],
+                                REF_ITER_FRAC if krylov == 0 else REF_ITER_FRAC_LEFT)
     print(f"shoal 1000 steps, {'FGMRES' if krylov == 0 else 'left GMRES'} vs reference ordering: "
           f"rel err {errs}, matvecs {tot} vs {ref}")
 
@@ -105,6 +113,7 @@ def test_shoal_1000_steps_against_reference_ordering(ow3d, krylov):
 @pytest.mark.parametrize("krylov", [0, 1], ids=["fgmres", "left_gmres"])
 def test_sfwave_200_steps_against_reference_ordering(ow3d, krylov):
     sim, its = _sfwave(ow3d, krylov)
-    errs, tot, ref = _check_ref(sim, load("run_sfwave_257x9_200_ref"), its, REF_TOL["sfwave"])
+    errs, tot, ref = _check_ref(sim, load("run_sfwave_257x9_200_ref"), its, REF_TOL["sfwave"],
+                                REF_ITER_FRAC if krylov == 0 else REF_ITER_FRAC_LEFT)
     print(f"stream-function flume 200 steps, {'FGMRES' if krylov == 0 else 'left GMRES'} vs reference "
           f"ordering: rel err {errs}, matvecs {tot} vs {ref}")
