@@ -160,7 +160,7 @@ typedef struct ow3d_params {
     /* deck features outside this library's path, kept so that ow3d_create
      * can refuse a deck that needs them instead of running without them */
     double accel_tol_fact;            /* line 2: local filtering by acceleration, on for (0, 100] (1e30 when absent) */
-    int    i_breaking;                /* line 12: breaking model on */
+    int    i_breaking;                /* line 12: breaking model (see T_half below) */
     int    PDampingONOFF;             /* pressure-damping zones on */
     int    swenseONOFF;               /* SWENSE on */
     int    curvilinearONOFF;          /* curvilinear grid on */
@@ -181,6 +181,15 @@ typedef struct ow3d_params {
      * which hold the same value; the Nx - 1 distinct columns are coupled
      * cyclically in every stencil, the ghost columns are unused. */
     int    periodic_x;
+    /* line 12, the roller breaking model of x flumes (DetectBreaking.f90;
+     * ReadInputFileParameters.f90:478-479), after i_breaking above: 1 = rollers
+     * found and their flux slope Qr_x subtracted from the kinematic condition
+     * at every RK stage, 2 (or any other positive value) = rollers found and
+     * reported only. Applied when Ny = 1, as in the reference; ignored in 3-D. */
+    double T_half;                    /* s over which tan(phi) relaxes to tan(phi_0); > 0 */
+    double phi_b, phi_0;              /* breaking and terminal roller angles, degrees */
+    double del_fac;                   /* roller thickness factor f_delta */
+    double cel_fac, gamma_break;      /* read and kept; the reference computes nothing from them */
 } ow3d_params;
 
 typedef struct ow3d_handle ow3d_handle;
@@ -393,6 +402,21 @@ int ow3d_set_relax_target(ow3d_handle* h, int zone, int mode, int nt,
  * OceanWave3DTakeATimeStep.f90:27. Returns OW3D_ERR_UNSTABLE on the
  * reference's instability test; OW3D_NOT_CONVERGED if any solve hit the limit. */
 int ow3d_step(ow3d_handle* h, int nsteps);
+
+/* The rollers of the roller breaking model (i_breaking > 0, Ny = 1) after
+ * the last completed step, as the reference writes them to roller.dat each
+ * step (DetectBreaking.f90:205-211): *n_rollers receives their number (0
+ * when the model is off), and for the first min(n, cap) rollers, in the
+ * order found (from the right end of the flume): npts = grid points the
+ * roller covers, toe = the 1-based, ghost-inclusive column just ahead of the
+ * toe, x = the toe's position measured as the reference does, (j - 1) dx
+ * from the ghost column, eta = the elevation at the toe, thickness = the
+ * roller thickness one column behind the toe, tan_phi = tan(phi) at the toe
+ * column after the step's update. Any array may be NULL. The reference
+ * holds at most Nxg / 10 rollers; this library holds all. Synchronises the
+ * handle's stream. Replaces: the roller.dat record of detect_breaking. */
+int ow3d_rollers(ow3d_handle* h, int cap, int* n_rollers, int* npts, int* toe, double* x, double* eta,
+                 double* thickness, double* tan_phi);
 
 /* ow3d_step, plus the device time of the steps measured with CUDA events on
  * the handle's stream (milliseconds). */

@@ -38,7 +38,7 @@ MODULE ow3d_iface
   ! ow3d_params mirrors the deck (include/ow3d.h); filled by ow3d_read_deck
   ! and opaque to Fortran
   TYPE, BIND(C) :: ow3d_params_t
-     INTEGER(c_int8_t) :: raw(2144)         ! opaque to Fortran: sizeof(ow3d_params)
+     INTEGER(c_int8_t) :: raw(2192)         ! opaque to Fortran: sizeof(ow3d_params)
   END TYPE
 
   INTERFACE
@@ -123,6 +123,25 @@ MODULE ow3d_iface
        INTEGER(c_int), VALUE :: zone, nt
        REAL(c_double), DIMENSION(*), INTENT(OUT) :: eta, phis
        INTEGER(c_int), DIMENSION(5), INTENT(OUT) :: box
+     END FUNCTION
+
+     ! the same wave synthesised on the device and installed as the zone's target
+     INTEGER(c_int) FUNCTION ow3d_incident_wave_device(handle, zone, nt) BIND(C, name="ow3d_incident_wave_device")
+       IMPORT :: c_int, c_ptr
+       TYPE(c_ptr), VALUE :: handle
+       INTEGER(c_int), VALUE :: zone, nt
+     END FUNCTION
+
+     ! the rollers of the breaking model after the last step (the roller.dat
+     ! record of detect_breaking); pass cap = 0 to query n_rollers only
+     INTEGER(c_int) FUNCTION ow3d_rollers(handle, cap, n_rollers, npts, toe, x, eta, thickness, tan_phi) &
+          BIND(C, name="ow3d_rollers")
+       IMPORT :: c_int, c_double, c_ptr
+       TYPE(c_ptr), VALUE :: handle
+       INTEGER(c_int), VALUE :: cap
+       INTEGER(c_int), INTENT(OUT) :: n_rollers
+       INTEGER(c_int), DIMENSION(*), INTENT(OUT) :: npts, toe
+       REAL(c_double), DIMENSION(*), INTENT(OUT) :: x, eta, thickness, tan_phi
      END FUNCTION
 
      ! the reference's output schedule (StoreDataONOFF of the deck): EP_#####.bin

@@ -82,6 +82,15 @@ int ow3d_test_step_graph_count(const ow3d_handle* h);
  * nt x box samples each of eta and phis (either may be NULL). */
 int ow3d_test_relax_target(const ow3d_handle* h, int zone, double* eta, double* phis);
 
+/* The roller breaking model's state: tan(phi) per column (the angle carried
+ * between steps) and the Qr_x of its last call, Nxg each (either may be NULL).
+ * OW3D_ERR_BAD_INPUT when the handle runs no breaking model. */
+int ow3d_test_breaking_state(ow3d_handle* h, double* tan_phi, double* Qr_x);
+/* One call of the breaking model on the surface E (Nxg values; update: the
+ * call after a step, with the roller-angle update and the roller record).
+ * Uses the handle's stage buffer for E. */
+int ow3d_test_detect_breaking(ow3d_handle* h, const double* E, int update);
+
 /* Device time of `reps` launches of one kernel on this handle's stream,
  * measured with CUDA events around each launch; before each launch a write of
  * the Krylov basis (larger than L2) evicts the inputs from L2, outside the

@@ -65,6 +65,8 @@ def lib():
         L.ow3d_test_graph_count.argtypes = [_C.c_void_p]
         L.ow3d_test_step_graph_count.argtypes = [_C.c_void_p]
         L.ow3d_test_relax_target.argtypes = [_C.c_void_p, _C.c_int, D, D]
+        L.ow3d_test_breaking_state.argtypes = [_C.c_void_p, D, D]
+        L.ow3d_test_detect_breaking.argtypes = [_C.c_void_p, D, _C.c_int]
         _lib = L
     return _lib
 
@@ -325,6 +327,32 @@ class Simulation:
         e, f = _np.zeros(nt * box), _np.zeros(nt * box)
         _check(lib().ow3d_test_relax_target(self.h, zone, _d(e), _d(f)), "ow3d_test_relax_target")
         return e.reshape(nt, box), f.reshape(nt, box)
+
+    def rollers(self):
+        """The roller breaking model's rollers after the last step (ow3d_rollers):
+        a dict of arrays npts, toe, x, eta, thickness, tan_phi, one entry per
+        roller in the order found; empty arrays when the model is off."""
+        n = _C.c_int()
+        _check(lib().ow3d_rollers(self.h, 0, _C.byref(n), None, None, None, None, None, None), "ow3d_rollers")
+        k = n.value
+        ints = [_np.zeros(max(k, 1), dtype=_np.int32) for _ in range(2)]
+        dbl = [_np.zeros(max(k, 1)) for _ in range(4)]
+        I = _C.POINTER(_C.c_int)
+        _check(lib().ow3d_rollers(self.h, k, _C.byref(n), *(a.ctypes.data_as(I) for a in ints), *(_d(a) for a in dbl)),
+               "ow3d_rollers")
+        names = ("npts", "toe", "x", "eta", "thickness", "tan_phi")
+        return {nm: a[:k].copy() for nm, a in zip(names, ints + dbl)}
+
+    def detect_breaking(self, E, update=False):
+        """One call of the breaking model on the surface E (a test hook)."""
+        E = _f64(E).ravel()
+        _check(lib().ow3d_test_detect_breaking(self.h, _d(E), 1 if update else 0), "ow3d_test_detect_breaking")
+
+    def breaking_state(self):
+        """(tan_phi, Qr_x) per column of the roller breaking model."""
+        t, q = _np.zeros(self.Nxg * self.Nyg), _np.zeros(self.Nxg * self.Nyg)
+        _check(lib().ow3d_test_breaking_state(self.h, _d(t), _d(q)), "ow3d_test_breaking_state")
+        return t, q
 
     def zone_box(self, zone):
         a, b, c, d = (_C.c_int() for _ in range(4))

@@ -73,6 +73,8 @@ class Params(C.Structure):
         ("pd_x0", C.c_double), ("pd_x1", C.c_double), ("pd_y0", C.c_double), ("pd_y1", C.c_double),
         ("pd_g0Phi", C.c_double), ("pd_g0Eta", C.c_double),
         ("accel_from_deck", C.c_int), ("periodic_x", C.c_int),
+        ("T_half", C.c_double), ("phi_b", C.c_double), ("phi_0", C.c_double),
+        ("del_fac", C.c_double), ("cel_fac", C.c_double), ("gamma_break", C.c_double),
     ]
 
 
@@ -167,6 +169,7 @@ def declare(lib):
         "ow3d_last_error": (C.c_char_p, []),
         "ow3d_set_relax_target": (C.c_int, [H, C.c_int, C.c_int, C.c_int, C.c_double, _D, _D]),
         "ow3d_incident_wave_device": (C.c_int, [H, C.c_int, C.c_int]),
+        "ow3d_rollers": (C.c_int, [H, C.c_int, _I, _I, _I, _D, _D, _D, _D]),
         "ow3d_step": (C.c_int, [H, C.c_int]),
         "ow3d_step_batch": (C.c_int, [C.POINTER(H), C.c_int, _I, _I, _D]),
         "ow3d_get_stats": (C.c_int, [H, C.POINTER(Stats)]),

@@ -26,7 +26,7 @@ inline int nb(int64_t n, int t = 256) {
 __global__ void k_fs_stage(FsArgs a, const double* E, const double* P, const double* W, const double* Ex,
                            const double* Px, const double* Ey, const double* Py, const double* E0,
                            const double* P0, double c, double* kE, double* kP, double* tE, double* tP,
-                           const double* NuD, const double* Pd) {
+                           const double* NuD, const double* Pd, const double* Qr_x) {
     const int64_t C = (int64_t)a.Nxg * a.Nyg;
     const double g = a.g, one = 1.0, half = 0.5;
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < C; p += (int64_t)gridDim.x * blockDim.x) {
@@ -36,6 +36,7 @@ __global__ void k_fs_stage(FsArgs a, const double* E, const double* P, const dou
             kp = -g * E[p];
         } else if (!a.three) {
             ke = -Ex[p] * Px[p] + W[p] * (one + Ex[p] * Ex[p]);
+            if (Qr_x) ke -= Qr_x[p];   // rhsFreeSurface3D.f90:17, the roller term
             kp = -g * E[p] - half * (Px[p] * Px[p] - W[p] * W[p] * (one + Ex[p] * Ex[p]));
         } else {
             ke = -Ex[p] * Px[p] - Ey[p] * Py[p] + W[p] * (one + Ex[p] * Ex[p] + Ey[p] * Ey[p]);
@@ -418,9 +419,11 @@ __global__ void k_unstable(FsArgs a, const double* __restrict__ E, double hmax10
 
 void fs_stage(const FsArgs& a, const double* E, const double* P, const double* W, const double* Ex, const double* Px,
               const double* Ey, const double* Py, const double* E0, const double* P0, double c, double* kE,
-              double* kP, double* tE, double* tP, const double* NuD, const double* Pd, cudaStream_t st) {
+              double* kP, double* tE, double* tP, const double* NuD, const double* Pd, const double* Qr_x,
+              cudaStream_t st) {
     int64_t C = (int64_t)a.Nxg * a.Nyg;
-    note_launch(), k_fs_stage<<<nb(C), 256, 0, st>>>(a, E, P, W, Ex, Px, Ey, Py, E0, P0, c, kE, kP, tE, tP, NuD, Pd);
+    note_launch(), k_fs_stage<<<nb(C), 256, 0, st>>>(a, E, P, W, Ex, Px, Ey, Py, E0, P0, c, kE, kP, tE, tP, NuD, Pd,
+                                                     Qr_x);
 }
 void fs_pdamp(const FsArgs& a, const PDampDev& d, const double* E, const double* P, cudaStream_t st) {
     const int64_t C = (int64_t)a.Nxg * a.Nyg;

@@ -93,6 +93,9 @@ struct ow3d_handle {
     PDampHost pd_h;
     PDampDev pd{};
     bool pd_on = false;
+    // roller breaking model (x flumes with i_breaking > 0)
+    BreakDev brk{};
+    bool brk_on = false;
     int* flag = nullptr;
     int* flag_host = nullptr;
     double hmax = 0;
@@ -733,6 +736,26 @@ int create_impl(const ow3d_params* p, const double* h, const double* hx, const d
         H->pd_h.L.clear(); H->pd_h.L.shrink_to_fit(); H->pd_h.Linv.clear(); H->pd_h.Linv.shrink_to_fit();
         H->pd_on = true;
     }
+    if (breaking_on(*p)) {
+        // DetectBreaking.f90:38-70 (its first call): tan(phi) starts at tan(phi_b)
+        BreakDev& b = H->brk;
+        const int nfx = G.Nxg;
+        b.nfx = nfx; b.cap = nfx; b.dynamics = p->i_breaking == 1 ? 1 : 0;
+        b.dx = p->Lx / ((double)p->Nx - 1.0); b.dx_inv = 1.0 / b.dx;
+        b.g = p->g; b.del_fac = p->del_fac; b.dt = p->dt; b.T_half = p->T_half;
+        const double deg2rad = std::acos(-1.0) / 180.0;   // Initialize.f90:7-8
+        b.tan_b = std::tan(deg2rad * p->phi_b); b.tan_0 = std::tan(deg2rad * p->phi_0);
+        TRY(upload(H.get(), &b.tan_phi, std::vector<double>((size_t)nfx, b.tan_b)));
+        TRY(dalloc(H.get(), &b.tan_old, (size_t)nfx)); TRY(dalloc(H.get(), &b.eta_x, (size_t)nfx + 1));
+        TRY(dalloc(H.get(), &b.thick, (size_t)nfx + 1)); TRY(dalloc(H.get(), &b.Qr_x, (size_t)nfx));
+        TRY(dalloc(H.get(), &b.n_rollers, 1));
+        TRY(dalloc(H.get(), &b.npts, (size_t)nfx)); TRY(dalloc(H.get(), &b.toe, (size_t)nfx));
+        TRY(dalloc(H.get(), &b.xr, (size_t)nfx)); TRY(dalloc(H.get(), &b.sr, (size_t)nfx));
+        TRY(dalloc(H.get(), &b.r_thick, (size_t)nfx)); TRY(dalloc(H.get(), &b.r_tan, (size_t)nfx));
+        CK(cudaMemset(b.Qr_x, 0, sizeof(double) * (size_t)nfx));
+        CK(cudaMemset(b.n_rollers, 0, sizeof(int)));
+        H->brk_on = true;
+    }
     if (p->filteringONOFF > 0) {
         std::vector<double> fc, F2;
         filter_coeffs(*p, fc, F2);
@@ -814,10 +837,19 @@ int enqueue_step(ow3d_handle* H, int64_t tstep, bool graph, SolveF&& solve) {
     auto pdamp = [&](const double* E, const double* P, double t) {
         if (H->pd_on && t > 0) fs_pdamp(fa, H->pd, E, P, st);
     };
+    // detect_breaking at each stage (Runge_Kutta_4.f90:55-57,164-166,241-243,
+    // 336-338): the stage's rollers give the Qr_x its fs_stage subtracts; it
+    // only changes the dynamics with i_breaking == 1
+    const bool brk_dyn = H->brk_on && H->brk.dynamics;
+    const double* Qr = brk_dyn ? H->brk.Qr_x : nullptr;
+    auto breaking = [&](const double* E) {
+        if (brk_dyn) fs_breaking(H->brk, E, 0, st);
+    };
     // stage 1
     pdamp(H->E, H->P, time);
+    breaking(H->E);
     fs_stage(fa, H->E, H->P, H->W, H->Ex, H->Px, H->Ey, H->Py, H->E, H->P, half * dt, H->kE[0], H->kP[0], H->tE, H->tP,
-             NuD, Pd, st);
+             NuD, Pd, Qr, st);
     relax(H->tE, H->tP, half * dt);
     derivs(H->tE, H->tP, H->tEx, H->tExx, H->tPx, H->tEy, H->tEyy, H->tPy);
     fs_set_rhs(fa, H->tP, H->RHS, st);
@@ -826,8 +858,9 @@ int enqueue_step(ow3d_handle* H, int64_t tstep, bool graph, SolveF&& solve) {
     fs_wvel(fa, H->PHI, H->tE, H->tW, st);
     // stage 2
     pdamp(H->tE, H->tP, time + half * dt);
+    breaking(H->tE);
     fs_stage(fa, H->tE, H->tP, H->tW, H->tEx, H->tPx, H->tEy, H->tPy, H->E, H->P, half * dt, H->kE[1], H->kP[1], H->tE,
-             H->tP, NuD, Pd, st);
+             H->tP, NuD, Pd, Qr, st);
     relax(H->tE, H->tP, half * dt);
     derivs(H->tE, H->tP, H->tEx, H->tExx, H->tPx, H->tEy, H->tEyy, H->tPy);
     fs_set_rhs(fa, H->tP, H->RHS, st);
@@ -835,8 +868,9 @@ int enqueue_step(ow3d_handle* H, int64_t tstep, bool graph, SolveF&& solve) {
     fs_wvel(fa, H->PHI, H->tE, H->tW, st);
     // stage 3
     pdamp(H->tE, H->tP, time + half * dt);
+    breaking(H->tE);
     fs_stage(fa, H->tE, H->tP, H->tW, H->tEx, H->tPx, H->tEy, H->tPy, H->E, H->P, dt, H->kE[2], H->kP[2], H->tE, H->tP,
-             NuD, Pd, st);
+             NuD, Pd, Qr, st);
     relax(H->tE, H->tP, dt);
     derivs(H->tE, H->tP, H->tEx, H->tExx, H->tPx, H->tEy, H->tEyy, H->tPy);
     fs_set_rhs(fa, H->tP, H->RHS, st);
@@ -846,8 +880,9 @@ int enqueue_step(ow3d_handle* H, int64_t tstep, bool graph, SolveF&& solve) {
     fs_wvel(fa, H->PHI, H->tE, H->tW, st);
     // stage 4 and the new time level
     pdamp(H->tE, H->tP, time + dt);
+    breaking(H->tE);
     fs_stage(fa, H->tE, H->tP, H->tW, H->tEx, H->tPx, H->tEy, H->tPy, nullptr, nullptr, 0.0, H->kE[3], H->kP[3], nullptr,
-             nullptr, NuD, Pd, st);
+             nullptr, NuD, Pd, Qr, st);
     fs_rk_final(fa, H->E, H->P, H->kE, H->kP, dt, st);
     if (H->p.filteringONOFF > 0) {
         // every filteringONOFF steps (Runge_Kutta_4.f90:355-362; the step number is checked on the device)
@@ -860,6 +895,9 @@ int enqueue_step(ow3d_handle* H, int64_t tstep, bool graph, SolveF&& solve) {
     fs_set_rhs(fa, H->P, H->RHS, st);
     TRY(solve(surf(H->E, H->Ex, H->Exx, H->Ey, H->Eyy), 3));
     fs_wvel(fa, H->PHI, H->E, H->W, st);
+    // the rollers of the new state and the roller-angle update
+    // (OceanWave3DTakeATimeStep.f90:45-49)
+    if (H->brk_on) fs_breaking(H->brk, H->E, 1, st);
     fs_step_end(H->sd, dt, st);
     // OceanWave3DTakeATimeStep.f90:54-70
     fs_unstable(fa, H->E, 10.0 * H->hmax, H->flag, st);
@@ -1396,11 +1434,15 @@ int ow3d_incident_wave_device(ow3d_handle* H, int zone, int nt) {
     TRY(dalloc(H, &de, box * (size_t)nt)); TRY(dalloc(H, &dp, box * (size_t)nt));
     // the components and work arrays, freed at the end of the call
     std::vector<void*> tmp;
+    // src = nullptr: an uninitialised work array
     auto put = [&](const void* src, size_t bytes) -> void* {
         void* d = nullptr;
-        if (cudaMalloc(&d, bytes ? bytes : 16) != cudaSuccess) return nullptr;
+        if (cudaMalloc(&d, bytes ? bytes : 16) != cudaSuccess) { tmp.push_back(nullptr); return nullptr; }
         tmp.push_back(d);
-        if (bytes) cudaMemcpy(d, src, bytes, cudaMemcpyHostToDevice);
+        if (src && bytes && cudaMemcpy(d, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+            tmp.push_back(nullptr);
+            return nullptr;
+        }
         return d;
     };
     auto release = [&]() { for (void* q : tmp) cudaFree(q); };
@@ -1434,13 +1476,71 @@ int ow3d_incident_wave_device(ow3d_handle* H, int zone, int nt) {
         d.B = (double2*)put(nullptr, modes * sizeof(double2));
     }
     for (void* q : tmp)
-        if (!q) { release(); g_last_error = "ow3d_incident_wave_device: device allocation failed"; return OW3D_ERR_OOM; }
+        if (!q) {
+            release();
+            (void)cudaGetLastError();
+            g_last_error = "ow3d_incident_wave_device: device allocation or upload failed";
+            return OW3D_ERR_OOM;
+        }
     int r = launch_incident_wave(d, de, dp, H->st);
     if (r == OW3D_OK && cudaStreamSynchronize(H->st) != cudaSuccess) r = OW3D_ERR_CUDA;
     release();
-    if (r) { g_last_error = "ow3d_incident_wave_device: kernel failed"; return r; }
+    if (r) {
+        g_last_error = "ow3d_incident_wave_device: kernel launch or execution failed";
+        return r;
+    }
     z.eta = de; z.phis = dp; z.nt = nt; z.tdt = H->p.dt; z.tmode = 0;
     drop_step_graphs(H);   // the captured relaxation launches hold the old table
+    return OW3D_OK;
+}
+
+int ow3d_rollers(ow3d_handle* H, int cap, int* n_rollers, int* npts, int* toe, double* x, double* eta,
+                 double* thickness, double* tan_phi) {
+    if (!H || !n_rollers) { g_last_error = "ow3d_rollers: null argument"; return OW3D_ERR_BAD_INPUT; }
+    if (!H->brk_on) { *n_rollers = 0; return OW3D_OK; }
+    int n = 0;
+    CK(cudaSetDevice(H->dev));
+    CK(cudaMemcpyAsync(&n, H->brk.n_rollers, sizeof(int), cudaMemcpyDeviceToHost, H->st));
+    CK(cudaStreamSynchronize(H->st));
+    *n_rollers = n;
+    const int k = n < cap ? n : (cap > 0 ? cap : 0);
+    if (k > 0) {
+        const BreakDev& b = H->brk;
+        auto get = [&](void* dst, const void* src, size_t sz) -> int {
+            if (dst) CK(cudaMemcpyAsync(dst, src, sz * (size_t)k, cudaMemcpyDeviceToHost, H->st));
+            return OW3D_OK;
+        };
+        TRY(get(npts, b.npts, sizeof(int))); TRY(get(toe, b.toe, sizeof(int)));
+        TRY(get(x, b.xr, sizeof(double))); TRY(get(eta, b.sr, sizeof(double)));
+        TRY(get(thickness, b.r_thick, sizeof(double))); TRY(get(tan_phi, b.r_tan, sizeof(double)));
+        CK(cudaStreamSynchronize(H->st));
+    }
+    return OW3D_OK;
+}
+
+int ow3d_test_detect_breaking(ow3d_handle* H, const double* E, int update) {
+    if (!H || !H->brk_on || !E) {
+        g_last_error = "ow3d_test_detect_breaking: no breaking model on this handle";
+        return OW3D_ERR_BAD_INPUT;
+    }
+    CK(cudaSetDevice(H->dev));
+    CK(cudaMemcpyAsync(H->tE, E, sizeof(double) * (size_t)H->G.C, cudaMemcpyHostToDevice, H->st));
+    fs_breaking(H->brk, H->tE, update, H->st);
+    CK(cudaStreamSynchronize(H->st));
+    CK(cudaGetLastError());
+    return OW3D_OK;
+}
+
+int ow3d_test_breaking_state(ow3d_handle* H, double* tan_phi, double* Qr_x) {
+    if (!H || !H->brk_on) {
+        g_last_error = "ow3d_test_breaking_state: no breaking model on this handle";
+        return OW3D_ERR_BAD_INPUT;
+    }
+    CK(cudaSetDevice(H->dev));
+    const size_t n = (size_t)H->brk.nfx;
+    if (tan_phi) CK(cudaMemcpyAsync(tan_phi, H->brk.tan_phi, sizeof(double) * n, cudaMemcpyDeviceToHost, H->st));
+    if (Qr_x) CK(cudaMemcpyAsync(Qr_x, H->brk.Qr_x, sizeof(double) * n, cudaMemcpyDeviceToHost, H->st));
+    CK(cudaStreamSynchronize(H->st));
     return OW3D_OK;
 }
 

@@ -54,12 +54,36 @@ struct PDampDev {
     double *NuD, *Pd;        // Nxg each: the kinematic and dynamic damping terms
 };
 
+// The roller breaking model of an x flume (DetectBreaking.f90). Columns are
+// 1-based in thick and eta_x (nfx + 1 entries), 0-based elsewhere.
+struct BreakDev {
+    int nfx;                 // Nxg
+    int cap;                 // roller records held (nfx)
+    int dynamics;            // i_breaking == 1: Qr_x enters the kinematic condition
+    double dx, dx_inv, g, del_fac, dt, T_half;
+    double tan_b, tan_0;     // tan(phi_b), tan(phi_0)
+    double* tan_phi;         // nfx: the roller angle, carried from step to step
+    double* tan_old;         // nfx: its value at the start of the call
+    double* eta_x;           // nfx + 1
+    double* thick;           // nfx + 1: roller thickness
+    double* Qr_x;            // nfx: the term the next fs_stage subtracts
+    int* n_rollers;          // rollers found by the last update call
+    int *npts, *toe;         // cap each: points covered, toe column (1-based)
+    double *xr, *sr;         // cap each: toe position (x = (j-1) dx) and elevation
+    double *r_thick, *r_tan; // cap each: thickness behind the toe, tan(phi) at the toe
+};
+
+// Rollers of the surface E and Qr_x; update: also the roller-angle update and
+// the roller records (the call after the step).
+void fs_breaking(const BreakDev& b, const double* E, int update, cudaStream_t st);
+
 // NuD and Pd of the state (E, P): the damping terms the next fs_stage adds.
 void fs_pdamp(const FsArgs& a, const PDampDev& d, const double* E, const double* P, cudaStream_t st);
-// NuD and Pd may be null (no pressure damping).
+// NuD and Pd may be null (no pressure damping), Qr_x likewise (no breaking).
 void fs_stage(const FsArgs& a, const double* E, const double* P, const double* W, const double* Ex, const double* Px,
               const double* Ey, const double* Py, const double* E0, const double* P0, double c, double* kE,
-              double* kP, double* tE, double* tP, const double* NuD, const double* Pd, cudaStream_t st);
+              double* kP, double* tE, double* tP, const double* NuD, const double* Pd, const double* Qr_x,
+              cudaStream_t st);
 void fs_rk_final(const FsArgs& a, double* E, double* P, double* const* kE, double* const* kP, double dt,
                  cudaStream_t st);
 // Relaxation at RK time = (device time) + off.

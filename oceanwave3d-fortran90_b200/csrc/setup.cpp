@@ -156,6 +156,8 @@ static void level_colours(LevelHost& L) {
     L.ncolor = (L.Nxg > 1 && L.Nyg > 1 && m > 0) ? 4 : 2;
 }
 
+bool breaking_on(const ow3d_params& p) { return p.i_breaking > 0 && p.Ny == 1 && p.Nx > 1; }
+
 // Deck features that change the physics but lie outside this library's path:
 // a deck that turns one on is refused (OW3D_ERR_UNSUPPORTED) rather than run
 // without it. The acceleration limit of line 2 turns the filter on for every
@@ -169,7 +171,6 @@ int check_supported(const ow3d_params& p, std::string* err) {
     if (p.IncWaveType == 3) return no("IncWaveType 3 (flux wave generation at the boundary) is not built");
     if (p.IncWaveType == 4 || p.IncWaveType == 5)
         return no("IncWaveType 4 and 5 (a wave with a constant-flux current) are not built");
-    if (p.i_breaking != 0) return no("the breaking model (deck line 12) is not built");
     const bool smoothing = p.accel_from_deck ? p.accel_tol_fact <= 100.0
                                              : (p.accel_tol_fact > 0.0 && p.accel_tol_fact <= 100.0);
     if (smoothing) return no("local filtering by the vertical acceleration (deck line 2) is not built");
@@ -207,6 +208,12 @@ int check_params(const ow3d_params& p, std::string* err) {
     if (p.precision != OW3D_PREC_FP64 && p.precision != OW3D_PREC_MIXED) return fail("precision must be 0 or 1");
     if (p.krylov != OW3D_KRYLOV_FGMRES && p.krylov != OW3D_KRYLOV_LGMRES) return fail("krylov must be 0 or 1");
     if (p.GMRESmaxiterations < 1) return fail("GMRESmaxiterations must be >= 1");
+    if (breaking_on(p)) {
+        // the roller-angle update divides by T_half (DetectBreaking.f90:181)
+        if (!(p.T_half > 0.0)) return fail("breaking model: T_half > 0 required");
+        if (!(p.del_fac >= 0.0)) return fail("breaking model: f_delta >= 0 required");
+        if (p.periodic_x != 0) return fail("periodic_x: the breaking model is built for wall boundaries");
+    }
     if (p.periodic_x != 0) {
         if (p.Nx < 9) return fail("periodic_x: at least 8 distinct points per period (Nx >= 9)");
         if (p.PDampingONOFF != 0) return fail("periodic_x: pressure-damping zones need the wall boundaries");
@@ -902,6 +909,7 @@ int default_params(ow3d_params* p) {
     p->sf_wavel_or_per = p->sf_euler_or_stokes = 0; p->sf_nsteps = 1; p->sf_nmodes = 0;
     std::memset(p->bathymetry_file, 0, sizeof p->bathymetry_file);
     p->accel_tol_fact = 1e30; p->i_breaking = 0; p->PDampingONOFF = 0; p->swenseONOFF = 0; p->curvilinearONOFF = 0;
+    p->T_half = 0; p->phi_b = 0; p->phi_0 = 0; p->del_fac = 0; p->cel_fac = 0; p->gamma_break = 0;
     return OW3D_OK;
 }
 
@@ -1046,7 +1054,12 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
     p->filteringONOFF = r.n(0); p->filterALPHA = r.n(1); p->filterORDER = r.n(2);
     for (int q = 0; q < 3; ++q) p->sigma_filt[q] = r.num(3 + q) ? r.d(3 + q) : 0.0;
     r = next();  // optional breaking line (7 numbers), else the relaxation line
-    if (r.nnum() >= 7) { p->i_breaking = r.n(0); r = next(); }
+    if (r.nnum() >= 7) {
+        // i_breaking, T_half, phi_b, phi_0, f_delta, f_cel, gamma_break
+        p->i_breaking = r.n(0); p->T_half = r.d(1); p->phi_b = r.d(2); p->phi_0 = r.d(3);
+        p->del_fac = r.d(4); p->cel_fac = r.d(5); p->gamma_break = r.d(6);
+        r = next();
+    }
     // relaxONOFF relaxTransientTime relaxNo relaxXorY relaxDegrees
     if (r.nnum() < 3) return fail("line 13: relaxation line expected");
     p->relaxONOFF = r.n(0); p->relaxTransientTime = r.d(1); p->relaxNo = r.n(2);

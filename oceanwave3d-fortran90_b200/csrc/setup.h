@@ -56,6 +56,9 @@ int check_params(const ow3d_params& p, std::string* err);
 // Deck features outside the path (breaking, pressure damping, SWENSE, ...):
 // 0, or OW3D_ERR_UNSUPPORTED with a message.
 int check_supported(const ow3d_params& p, std::string* err);
+// The roller breaking model runs: i_breaking > 0 on an x flume (Ny = 1),
+// where the reference calls detect_breaking (Runge_Kutta_4.f90:55).
+bool breaking_on(const ow3d_params& p);
 
 int build_grid(const ow3d_params& p, const double* h, const double* hx, const double* hxx, const double* hy,
                const double* hyy, GridHost& G, std::string* err);

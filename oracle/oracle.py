@@ -84,6 +84,9 @@ def lib():
         L.orc_step.argtypes = [V, C.c_int]
         L.orc_stats.argtypes = [V, C.POINTER(C.c_int64), C.POINTER(C.c_int64), I, I, I, D, C.POINTER(C.c_int64)]
         L.orc_reset_stats.argtypes = [V]
+        L.orc_rollers.argtypes = [V, C.c_int, I, I, D, D, D, D]
+        L.orc_breaking_state.argtypes = [V, D, D]
+        L.orc_detect_breaking.argtypes = [V, D, C.c_int]
         _lib = L
     return _lib
 
@@ -247,6 +250,29 @@ class Oracle:
 
     def reset_stats(self):
         lib().orc_reset_stats(self.h)
+
+    def rollers(self):
+        """The rollers of the last step (DetectBreaking.f90:205-211), as
+        Simulation.rollers returns them."""
+        cap = self.Nxg
+        ints = [np.zeros(cap, dtype=np.int32) for _ in range(2)]
+        dbl = [np.zeros(cap) for _ in range(4)]
+        I = C.POINTER(C.c_int)
+        n = lib().orc_rollers(self.h, cap, *(a.ctypes.data_as(I) for a in ints), *(_p(a) for a in dbl))
+        names = ("npts", "toe", "x", "eta", "thickness", "tan_phi")
+        return {nm: a[:n].copy() for nm, a in zip(names, ints + dbl)}
+
+    def detect_breaking(self, E, update=False):
+        """One detect_breaking call on the surface E (DetectBreaking.f90);
+        update: the call after a step (roller-angle update, roller record)."""
+        E = _c(E)
+        if lib().orc_detect_breaking(self.h, _p(E), 1 if update else 0) != 0:
+            raise ValueError("oracle: no breaking model in this simulation")
+
+    def breaking_state(self):
+        t, q = np.zeros(self.C), np.zeros(self.C)
+        lib().orc_breaking_state(self.h, _p(t), _p(q))
+        return t, q
 
 
 def set_threads(n):

@@ -75,6 +75,12 @@ struct Sim {
     vector<double> pdLU; vector<int> pdPiv;
     vector<double> fc, fc2;              // filter: centre (NP) and boundary view (NP*alpha)
     int NP = 0;
+    // the roller breaking model of x flumes (DetectBreaking.f90)
+    int brk = 0;                         // i_breaking > 0 and Ny == 1
+    double tan_b = 0, tan_0 = 0;         // tan(phi_b), tan(phi_0)
+    vector<double> tan_phi, Qr_x;        // per column: roller angle state, roller flux slope
+    vector<int> r_npts, r_toe;           // rollers of the last completed step
+    vector<double> r_x, r_eta, r_thick, r_tan;
     // stats
     int64_t solves = 0, totit = 0, notconv = 0; int minit = 1 << 30, maxit = 0, lastit = 0;
     double lastres = 0;
@@ -1106,7 +1112,7 @@ static void fs_rhs(const Sim& s, const vector<double>& E, const vector<double>& 
             kE[c] = -Ey[c] * Py[c] + W[c] * (one + Ey[c] * Ey[c]);
             kP[c] = -g * E[c] - half * (Py[c] * Py[c] - W[c] * W[c] * (one + Ey[c] * Ey[c]));
         } else if (s.p.Ny == 1) {
-            kE[c] = -Ex[c] * Px[c] + W[c] * (one + Ex[c] * Ex[c]);
+            kE[c] = -Ex[c] * Px[c] + W[c] * (one + Ex[c] * Ex[c]) - s.Qr_x[c];
             kP[c] = -g * E[c] - half * (Px[c] * Px[c] - W[c] * W[c] * (one + Ex[c] * Ex[c]));
         } else {
             kE[c] = -Ex[c] * Px[c] - Ey[c] * Py[c] + W[c] * (one + Ex[c] * Ex[c] + Ey[c] * Ey[c]);
@@ -1382,6 +1388,70 @@ static void setup_zones(Sim& s) {
     }
 }
 
+// ------------------------------------------------------------- breaking
+// DetectBreaking.f90:72-211 on the surface elevation E of an x flume (1-based
+// column j, nfx = Nxg columns). Rollers are searched from the right end: a
+// toe lies between j-1 and j where the slope eta_x (forward differences at
+// j+1/2) crosses -tan(phi(j)) and no roller covers j yet; its sub-grid
+// position comes from the local quadratic, and the roller extends back while
+// the surface stays above the tangent line from the toe, with thickness
+// del_fac times that height (capped at eta - eta_toe). Qr_x, the 1-2-1
+// smoothed g * thickness, enters the kinematic condition when i_breaking is 1
+// (rhsFreeSurface3D.f90:17). With update (the call after the step, :175-186)
+// tan(phi) returns to tan(phi_b) everywhere except from three points ahead of
+// each toe to the back of its roller, where it moves linearly toward
+// tan(phi_0) by dt / T_half of the way from the toe's previous value, and the
+// rollers are recorded as the reference writes them to roller.dat
+// (:205-211). Rollers are not capped at nfx/10 (the reference's arrays) and
+// angle updates past the last column are dropped (the reference writes
+// them out of bounds).
+static void detect_breaking(Sim& s, const vector<double>& E, bool update) {
+    const int nfx = s.Nxg;
+    const double half = 0.5, two = 2.0, quart = 0.25, g = s.p.g;
+    const double dx = s.p.Lx / ((double)s.p.Nx - 1.0), dx_inv = 1.0 / dx;
+    auto et = [&](int j) { return E[(size_t)j - 1]; };
+    vector<double> tan_old(s.tan_phi), thick(nfx + 1, 0.0), eta_x(nfx + 1, 0.0), Qr(nfx + 1, 0.0);
+    std::fill(s.Qr_x.begin(), s.Qr_x.end(), 0.0);
+    for (int j = 2; j <= nfx - 2; ++j) eta_x[j] = dx_inv * (et(j + 1) - et(j));
+    vector<int> npts, toe; vector<double> xr_l, sr_l;
+    for (int j = nfx - 2; j >= 3; --j) {
+        const double tphib = s.tan_phi[(size_t)j - 1];
+        if (!(eta_x[j - 1] < -tphib && eta_x[j] >= -tphib && thick[j] <= 0.0)) continue;
+        const double a = half * dx_inv * (eta_x[j] - eta_x[j - 1]);
+        const double b = half * (eta_x[j] + eta_x[j - 1]);
+        const double c = et(j);
+        const double dxr = -(tphib + b) / (two * a);
+        const double xr = (double)(j - 1) * dx + dxr;
+        const int jr = (int)(xr * dx_inv) + 2;
+        const double sr = a * dxr * dxr + b * dxr + c;
+        int n = 0;
+        for (int i = jr - 1; i >= 3; --i) {
+            double d = s.p.del_fac * (et(i) - (sr + tphib * (xr - (double)(i - 1) * dx)));
+            if (d < 0.0) break;
+            if (d > et(i) - sr) d = et(i) - sr;
+            thick[i] = d; ++n;
+            Qr[i] = g * thick[i];
+        }
+        npts.push_back(n); toe.push_back(jr); xr_l.push_back(xr); sr_l.push_back(sr);
+    }
+    const int nr = (int)npts.size();
+    if (update) {
+        std::fill(s.tan_phi.begin(), s.tan_phi.end(), s.tan_b);
+        for (int r = 0; r < nr; ++r) {
+            const double tphib = tan_old[(size_t)toe[r] - 1];
+            for (int i = 1; i <= npts[r] + 3; ++i) {
+                const int idx = toe[r] + 4 - i;
+                if (idx >= 1 && idx <= nfx) s.tan_phi[(size_t)idx - 1] = tphib + s.p.dt / s.p.T_half * (s.tan_0 - tphib);
+            }
+        }
+        s.r_npts = npts; s.r_toe = toe; s.r_x = xr_l; s.r_eta = sr_l;
+        s.r_thick.assign(nr, 0.0); s.r_tan.assign(nr, 0.0);
+        for (int r = 0; r < nr; ++r) { s.r_thick[r] = thick[toe[r] - 1]; s.r_tan[r] = s.tan_phi[(size_t)toe[r] - 1]; }
+    }
+    if (nr > 0 && s.p.i_breaking == 1)
+        for (int j = 3; j <= nfx - 2; ++j) s.Qr_x[(size_t)j - 1] = quart * Qr[j + 1] + half * Qr[j] + quart * Qr[j - 1];
+}
+
 // ------------------------------------------------------------- RK4 step
 // Runge_Kutta_4.f90:1-429 (nonlinear or linear FSBC, no SWENSE, no pressure).
 static int rk4_step(Sim& s) {
@@ -1413,8 +1483,10 @@ static int rk4_step(Sim& s) {
         if (st == OW3D_NOT_CONVERGED) status = OW3D_NOT_CONVERGED;
     };
     auto zero_src = [&]() { std::fill(s.sPx.begin(), s.sPx.end(), 0.0); };
+    auto breaking = [&](const vector<double>& Ef) { if (s.brk && s.p.i_breaking == 1) detect_breaking(s, Ef, false); };
     // stage 1
     pressure_term(s, s.E, s.P, time);
+    breaking(s.E);
     fs_rhs(s, s.E, s.P, s.W, s.Ex, s.Px, s.Ey, s.Py, k1E, k1P);
     for (size_t c = 0; c < C; ++c) { s.tE[c] = s.E[c] + half * dt * k1E[c]; s.tP[c] = s.P[c] + half * dt * k1P[c]; }
     double RKtime = time + half * dt;
@@ -1429,6 +1501,7 @@ static int rk4_step(Sim& s) {
     vertical_velocity(s, s.tW);
     // stage 2
     pressure_term(s, s.tE, s.tP, RKtime);
+    breaking(s.tE);
     fs_rhs(s, s.tE, s.tP, s.tW, s.tEx, s.tPx, s.tEy, s.tPy, k2E, k2P);
     for (size_t c = 0; c < C; ++c) { s.tE[c] = s.E[c] + half * dt * k2E[c]; s.tP[c] = s.P[c] + half * dt * k2P[c]; }
     RKtime = time + half * dt;
@@ -1440,6 +1513,7 @@ static int rk4_step(Sim& s) {
     vertical_velocity(s, s.tW);
     // stage 3
     pressure_term(s, s.tE, s.tP, RKtime);
+    breaking(s.tE);
     fs_rhs(s, s.tE, s.tP, s.tW, s.tEx, s.tPx, s.tEy, s.tPy, k3E, k3P);
     for (size_t c = 0; c < C; ++c) { s.tE[c] = s.E[c] + dt * k3E[c]; s.tP[c] = s.P[c] + dt * k3P[c]; }
     RKtime = time + dt;
@@ -1454,6 +1528,7 @@ static int rk4_step(Sim& s) {
     vertical_velocity(s, s.tW);
     // stage 4
     pressure_term(s, s.tE, s.tP, RKtime);
+    breaking(s.tE);
     fs_rhs(s, s.tE, s.tP, s.tW, s.tEx, s.tPx, s.tEy, s.tPy, k4E, k4P);
     const double six = 6.0, two = 2.0;
     for (size_t c = 0; c < C; ++c) {
@@ -1469,6 +1544,8 @@ static int rk4_step(Sim& s) {
     set_rhs(s.P);
     do_solve();
     vertical_velocity(s, s.W);
+    // rollers of the new state and the roller-angle update (OceanWave3DTakeATimeStep.f90:45-49)
+    if (s.brk) detect_breaking(s, s.E, true);
     // instability check and time advance (OceanWave3DTakeATimeStep.f90:54-70)
     double me = 0, mh = 0;
     for (size_t c = 0; c < C; ++c) { me = std::max(me, std::fabs(s.E[c])); mh = std::max(mh, s.fine.h[c]); }
@@ -1510,6 +1587,14 @@ static Sim* create(const ow3d_params* p, const double* h, const double* hx, cons
     if (p->filteringONOFF > 0) filter_init(*s);
     setup_zones(*s);
     setup_pdamp(*s);
+    // DetectBreaking.f90:38-70 (the first call): tan(phi) starts at tan(phi_b); Initialize.f90:7-8
+    s->brk = (p->i_breaking > 0 && p->Ny == 1 && p->Nx > 1) ? 1 : 0;
+    s->Qr_x.assign(C, 0.0);
+    if (s->brk) {
+        const double deg2rad = std::acos(-1.0) / 180.0;
+        s->tan_b = std::tan(deg2rad * p->phi_b); s->tan_0 = std::tan(deg2rad * p->phi_0);
+        s->tan_phi.assign(C, s->tan_b);
+    }
     s->time = p->time0;
     return s.release();
 }
@@ -1622,6 +1707,27 @@ int orc_step(void* sv, int nsteps) {
 void orc_stats(void* sv, int64_t* solves, int64_t* totit, int* minit, int* maxit, int* lastit, double* lastres, int64_t* notconv) {
     Sim* s = (Sim*)sv; *solves = s->solves; *totit = s->totit; *minit = s->minit; *maxit = s->maxit; *lastit = s->lastit;
     *lastres = s->lastres; *notconv = s->notconv;
+}
+// the rollers of the last completed step: count, and per roller the points
+// it covers, the toe column, its position (x = (j-1) dx), the elevation at
+// the toe, the thickness one column behind the toe and tan(phi) at the toe
+int orc_rollers(void* sv, int cap, int* npts, int* toe, double* x, double* eta, double* thick, double* tanphi) {
+    Sim* s = (Sim*)sv; const int n = (int)s->r_npts.size();
+    for (int r = 0; r < n && r < cap; ++r) {
+        npts[r] = s->r_npts[r]; toe[r] = s->r_toe[r]; x[r] = s->r_x[r]; eta[r] = s->r_eta[r];
+        thick[r] = s->r_thick[r]; tanphi[r] = s->r_tan[r];
+    }
+    return n;
+}
+// one detect_breaking call on the surface E (update: the call after a step)
+int orc_detect_breaking(void* sv, const double* E, int update) {
+    Sim* s = (Sim*)sv; if (!s->brk) return -1;
+    vector<double> e(E, E + s->C); detect_breaking(*s, e, update != 0); return 0;
+}
+void orc_breaking_state(void* sv, double* tan_phi, double* Qr_x) {
+    Sim* s = (Sim*)sv;
+    if (tan_phi && !s->tan_phi.empty()) std::copy(s->tan_phi.begin(), s->tan_phi.end(), tan_phi);
+    if (Qr_x) std::copy(s->Qr_x.begin(), s->Qr_x.end(), Qr_x);
 }
 void orc_reset_stats(void* sv) { Sim* s = (Sim*)sv; s->solves = s->totit = s->notconv = 0; s->minit = 1 << 30; s->maxit = 0; }
 }

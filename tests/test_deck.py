@@ -86,6 +86,19 @@ def test_deck_2d_optional_fields(ow3d, tmp_path):
     assert p.filteringONOFF == 0 and p.relaxONOFF == 0
 
 
+def test_deck_breaking_line(ow3d, tmp_path):
+    """Line 12 (ReadInputFileParameters.f90:478-479): i_breaking, T_1/2,
+    phi_b, phi_0, f_delta, f_cel, gamma_break, as the roller-breaking decks
+    of the reference write it."""
+    text = DECK_2D_CFL.replace("0.1 0.2 0.3 0.4 0.5 0.6 1", "1 .8 32. 20. 1.5 1.3 1.0")
+    p = ow3d.read_deck(write(tmp_path, "rb.inp", text))
+    assert (p.i_breaking, p.T_half, p.phi_b, p.phi_0) == (1, 0.8, 32.0, 20.0)
+    assert (p.del_fac, p.cel_fac, p.gamma_break) == (1.5, 1.3, 1.0)
+    assert p.relaxONOFF == 0
+    p = ow3d.read_deck(write(tmp_path, "nb.inp", DECK_3D))
+    assert (p.i_breaking, p.T_half) == (0, 0.0)
+
+
 def test_deck_errors(ow3d, tmp_path):
     with pytest.raises(ow3d.OW3DError) as e:
         ow3d.read_deck(tmp_path / "missing.inp")
@@ -142,8 +155,8 @@ def test_reference_example_decks_parse(ow3d):
 
 
 def test_decks_needing_unbuilt_features_are_refused(ow3d, tmp_path):
-    """A deck that turns on a feature outside this library's path (breaking
-    model, pressure damping in 3-D, SWENSE, flux wave generation, local
+    """A deck that turns on a feature outside this library's path (pressure
+    damping in 3-D, SWENSE, flux wave generation, local
     filtering by acceleration) is refused with OW3D_ERR_UNSUPPORTED by ow3d_create and
     ow3d_estimate_bytes instead of running without it."""
     import ctypes as C
@@ -159,7 +172,6 @@ def test_decks_needing_unbuilt_features_are_refused(ow3d, tmp_path):
     cases_ = {
         "pressure": base.replace("0 0\n0 2.0 2", "1 1\n0. 5. 0. 10. 0.1 0.1 0\n0 2.0 2"),
         "SWENSE": base.replace("0 2.0 2 0 0 1 0", "1 2.0 2 0 0 1 0"),
-        "breaking": base.replace("1 6 10 0.08 0.08 0.4", "1 6 10 0.08 0.08 0.4\n1 1.0 0.6 0.2 0.1 0.8 0.5"),
         "IncWaveType 3": base.replace("-1 0  ", "-1 3  "),
         "acceleration": base.replace("-1 0  ", "-1 0 0.5 "),
         "acceleration, 100 g": base.replace("-1 0  ", "-1 0 100. "),
@@ -177,6 +189,10 @@ def test_decks_needing_unbuilt_features_are_refused(ow3d, tmp_path):
     assert "IncWaveType 4 and 5" in msg
     st, p = status(base.replace("-1 0  ", "-1 0 1000. "))
     assert st == 0 and p.accel_from_deck == 1
+    # the breaking model acts on x flumes only (Runge_Kutta_4.f90:55): a 3-D
+    # deck with it on runs without it, as in the reference
+    st, p = status(base.replace("1 6 10 0.08 0.08 0.4", "1 6 10 0.08 0.08 0.4\n1 1.0 32. 20. 1.5 1.3 1.0"))
+    assert st == 0 and p.i_breaking == 1
     # parameters built by a caller: accel_tol_fact = 0 (zero-initialised) means no smoothing
     q = ow3d.default_params(Nx=33, Ny=17, Nz=9)
     q.accel_tol_fact = 0.0
