@@ -55,6 +55,11 @@ int ow3d_test_set_coarse_blocks(int blocks);
  * applies to handles created after the change (and to captures made after
  * it). Returns the previous value. Process-wide. */
 long long ow3d_test_set_coop_max_points(long long points);
+/* Levels of at most `points` points run in the cluster (tail) kernel of the
+ * fused coarse cycle (0: no tail), and the cluster's block count (8 or 16);
+ * each returns the previous value. Process-wide. */
+long long ow3d_test_set_tail_max_points(long long points);
+int ow3d_test_set_tail_cluster(int blocks);
 
 /* Levels without mixed-derivative terms that cover at least `min_tiles`
  * tiles of 32 x 8 columns take the tiled colour pass (columns away from the

@@ -301,10 +301,16 @@ __device__ void coop_colour(const LevelDev<T>& L, int colour) {
 #undef OW3D_CC
 }
 
-// Barrier of the fused coarse kernel: the whole cooperative grid.
+// Barriers of the fused coarse kernels: the whole cooperative grid, or the
+// one thread-block cluster of the tail kernel (a hardware barrier among the
+// cluster's SMs, with release / acquire ordering of their global-memory
+// accesses at cluster scope).
 struct GridSync {
     cg::grid_group g;
     __device__ void sync() { g.sync(); }
+};
+struct ClusterSync {
+    __device__ void sync() { cg::this_cluster().sync(); }
 };
 
 template <typename T, bool THREE, typename SY>
@@ -322,44 +328,54 @@ __device__ void coop_smooth(const LevelDev<T>& L, int nu, SY& sy) {
     }
 }
 
+// Parts of the V cycle over levels lc..ld that one launch of a fused kernel
+// runs: all of it, the descent from lc to level lo (ending with lo's
+// right-hand side restricted and its iterate zeroed), or the ascent from lo.
+enum CoarsePart : int { kWhole = 0, kDown = 1, kUp = 2 };
+
 // V cycle over levels lc..ld (MultiGridSolver.f90:5-192) in one launch whose
 // phases are separated by the barrier SY; level ld is solved with the dense
 // operator M (the coarsest level's inverse when ld = 0, otherwise the V cycle
 // below ld as one precomputed map). Level lc's right-hand side is set and its
 // iterate zeroed on entry. Level lc is read from `top` (the table's entry with
 // the iterate and right-hand side of this launch), the others from the table.
+// part / lo select the piece of the cycle (CoarsePart); lo = ld for kWhole.
 template <typename T, bool THREE, typename SY>
-__device__ void coarse_body(const LevelDev<T>* __restrict__ P, const LevelDev<T>& top, int lc, int ld,
-                            const T* __restrict__ M, int nu1, int nu2, SY& sy) {
+__device__ void coarse_body(const LevelDev<T>* __restrict__ P, const LevelDev<T>& top, int lc, int ld, int lo,
+                            int part, const T* __restrict__ M, int nu1, int nu2, SY& sy) {
     auto lv = [&](int l) -> const LevelDev<T>& { return l == lc ? top : P[l]; };
-    for (int l = lc; l > ld; --l) {
-        const LevelDev<T>& L = lv(l);
-        const LevelDev<T>& Cc = P[l - 1];
-        coop_smooth<T, THREE>(L, nu1, sy);
-        if (L.cross) { OW3D_GRID_STRIDE(p, L.N) residual_point<T, THREE, true>(L, p); }
-        else { OW3D_GRID_STRIDE(p, L.N) residual_point<T, THREE, false>(L, p); }
-        sy.sync();
-        OW3D_GRID_STRIDE(p, Cc.N) restrict_item<T>(L, Cc, L.rv, Cc.bv, Cc.xv, p);
-        sy.sync();
+    if (part != kUp) {
+        for (int l = lc; l > lo; --l) {
+            const LevelDev<T>& L = lv(l);
+            const LevelDev<T>& Cc = P[l - 1];
+            coop_smooth<T, THREE>(L, nu1, sy);
+            if (L.cross) { OW3D_GRID_STRIDE(p, L.N) residual_point<T, THREE, true>(L, p); }
+            else { OW3D_GRID_STRIDE(p, L.N) residual_point<T, THREE, false>(L, p); }
+            sy.sync();
+            OW3D_GRID_STRIDE(p, Cc.N) restrict_item<T>(L, Cc, L.rv, Cc.bv, Cc.xv, p);
+            sy.sync();
+        }
     }
-    {
+    if (part == kWhole) {
         const LevelDev<T>& Ld = P[ld];
         dense_rows<T>((int)Ld.N, M, Ld.bv, Ld.xv);
         sy.sync();
     }
-    for (int l = ld + 1; l <= lc; ++l) {
-        const LevelDev<T>& L = lv(l);
-        const LevelDev<T>& Cc = P[l - 1];
-        OW3D_GRID_STRIDE(p, L.N) prolong_item<T>(L, Cc, Cc.xv, L.xv, p);
-        sy.sync();
-        coop_smooth<T, THREE>(L, nu2, sy);
+    if (part != kDown) {
+        for (int l = lo + 1; l <= lc; ++l) {
+            const LevelDev<T>& L = lv(l);
+            const LevelDev<T>& Cc = P[l - 1];
+            OW3D_GRID_STRIDE(p, L.N) prolong_item<T>(L, Cc, Cc.xv, L.xv, p);
+            sy.sync();
+            coop_smooth<T, THREE>(L, nu2, sy);
+        }
     }
 }
 
 template <typename T, bool THREE>
 __global__ void __launch_bounds__(kCoopThreads) k_mg_coarse_cycle(const LevelDev<T>* __restrict__ P, int lc, int ld,
-                                                                  const T* __restrict__ M, int nu1, int nu2, T* xtop,
-                                                                  T* btop) {
+                                                                  int lo, int part, const T* __restrict__ M, int nu1,
+                                                                  int nu2, T* xtop, T* btop) {
     __shared__ LevelDev<T> top;
     if (threadIdx.x == 0) {
         top = P[lc];
@@ -368,7 +384,25 @@ __global__ void __launch_bounds__(kCoopThreads) k_mg_coarse_cycle(const LevelDev
     }
     __syncthreads();
     GridSync sy{cg::this_grid()};
-    coarse_body<T, THREE>(P, top, lc, ld, M, nu1, nu2, sy);
+    coarse_body<T, THREE>(P, top, lc, ld, lo, part, M, nu1, nu2, sy);
+}
+
+// The small coarse levels (the tail of the cycle) in one thread-block
+// cluster: a cluster barrier costs a fraction of a grid-wide one, and these
+// levels have fewer points than the cluster has threads.
+template <typename T, bool THREE>
+__global__ void __launch_bounds__(kCoopThreads) k_mg_tail_cycle(const LevelDev<T>* __restrict__ P, int lc, int ld,
+                                                                const T* __restrict__ M, int nu1, int nu2, T* xtop,
+                                                                T* btop) {
+    __shared__ LevelDev<T> top;
+    if (threadIdx.x == 0) {
+        top = P[lc];
+        top.xv = xtop;
+        top.bv = btop;
+    }
+    __syncthreads();
+    ClusterSync sy;
+    coarse_body<T, THREE>(P, top, lc, ld, ld, kWhole, M, nu1, nu2, sy);
 }
 
 inline int nblk(int64_t n, int t = 256) {
@@ -521,6 +555,11 @@ void launch_dense_apply(const LevelDev<T>& L, const T* M, cudaStream_t st) {
 std::atomic<int> g_coarse_blocks{0};
 // Levels with at most this many points run in the fused coarse kernel.
 std::atomic<int64_t> g_coop_max_points{160000};
+// Levels with at most this many points run in the cluster (tail) kernel (0: none).
+std::atomic<int64_t> g_tail_max_points{8192};
+// Blocks of the tail kernel's cluster (16 needs the non-portable cluster
+// size; the launcher falls back to 8 where 16 cannot be resident).
+std::atomic<int> g_tail_cluster{16};
 // Levels of at least this many tiles take the tiled colour pass (0: none, the
 // default: inside the solve the per-column pass measured faster, see the
 // launcher).
@@ -529,7 +568,48 @@ std::atomic<int> g_colour_prefetch{0};
 
 thread_local bool g_capture_unsafe = false;
 
-// Launch the fused coarse cycle over levels lc..ld with a fully co-resident grid.
+// Cluster size the tail kernel can run with on this device (0: none):
+// the requested size if a cluster of it can be resident, else 8, else 0.
+template <typename T, bool THREE>
+static int tail_cluster_size(int want) {
+    static std::atomic<int> cached[64][17];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (want < 1 || want > 16) return 0;
+    std::atomic<int>& c = cached[dev & 63][want];
+    int v = c.load(std::memory_order_relaxed);
+    if (v != 0) return v > 0 ? v : 0;
+    auto fits = [&](int cl) {
+        if (cl > 8 && cudaFuncSetAttribute((const void*)k_mg_tail_cycle<T, THREE>,
+                                           cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return false;
+        }
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = (unsigned)cl;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3((unsigned)cl);
+        cfg.blockDim = dim3(kCoopThreads);
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, (const void*)k_mg_tail_cycle<T, THREE>, &cfg) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return false;
+        }
+        return n >= 1;
+    };
+    v = fits(want) ? want : (want > 8 && fits(8) ? 8 : -1);
+    c.store(v, std::memory_order_relaxed);
+    return v > 0 ? v : 0;
+}
+
+// Launch the fused coarse cycle over levels lc..ld: the levels of at most
+// g_tail_max_points points in one thread-block cluster, the larger ones with
+// a fully co-resident grid (its descent, then the tail, then its ascent).
 template <typename T, bool THREE>
 static void coarse_cycle(const LevelDev<T>* lev, int lc, int ld, const T* M, int nu1, int nu2, LevelTable<T>& pack,
                          cudaStream_t st) {
@@ -571,11 +651,42 @@ static void coarse_cycle(const LevelDev<T>* lev, int lc, int ld, const T* M, int
         }
     }
     const LevelDev<T>* P = pack.dev;
-    T* xtop = lev[lc].xv;
-    T* btop = lev[lc].bv;
-    void* args[] = {(void*)&P, (void*)&lc, (void*)&ld, (void*)&M, (void*)&nu1, (void*)&nu2, (void*)&xtop, (void*)&btop};
-    note_launch();
-    cudaLaunchCooperativeKernel((const void*)k_mg_coarse_cycle<T, THREE>, dim3(grid), dim3(kCoopThreads), args, 0, st);
+    // the tail: levels ld+1..lt of at most g_tail_max_points points
+    const int64_t tmax = g_tail_max_points.load(std::memory_order_relaxed);
+    const int cl = tmax > 0 ? tail_cluster_size<T, THREE>(g_tail_cluster.load(std::memory_order_relaxed)) : 0;
+    int lt = ld;
+    if (cl > 0)
+        for (int l = ld + 1; l <= lc && lev[l].N <= tmax; ++l) lt = l;
+    auto coop = [&](int lo, int part) {
+        T* xtop = lev[lc].xv;
+        T* btop = lev[lc].bv;
+        void* args[] = {(void*)&P, (void*)&lc, (void*)&ld, (void*)&lo, (void*)&part, (void*)&M,
+                        (void*)&nu1, (void*)&nu2, (void*)&xtop, (void*)&btop};
+        note_launch();
+        cudaLaunchCooperativeKernel((const void*)k_mg_coarse_cycle<T, THREE>, dim3(grid), dim3(kCoopThreads), args, 0,
+                                    st);
+    };
+    if (lt == ld) {
+        coop(ld, kWhole);
+        return;
+    }
+    if (lt < lc) coop(lt, kDown);
+    {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = (unsigned)cl;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3((unsigned)cl);
+        cfg.blockDim = dim3(kCoopThreads);
+        cfg.stream = st;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        note_launch();
+        cudaLaunchKernelEx(&cfg, k_mg_tail_cycle<T, THREE>, P, lt, ld, M, nu1, nu2, lev[lt].xv, lev[lt].bv);
+    }
+    if (lt < lc) coop(lt, kUp);
 }
 
 template <typename T>

@@ -1142,6 +1142,10 @@ unsigned long long ow3d_launch_count(void) { return g_kernel_launches.load(std::
 int ow3d_test_set_coarse_blocks(int blocks) { return g_coarse_blocks.exchange(blocks < 0 ? 0 : blocks); }
 int ow3d_test_set_colour_tiles(int min_tiles) { return g_colour_tiles.exchange(min_tiles < 0 ? 0 : min_tiles); }
 int ow3d_test_set_colour_prefetch(int mode) { return g_colour_prefetch.exchange(mode < 0 ? 0 : mode); }
+long long ow3d_test_set_tail_max_points(long long points) {
+    return g_tail_max_points.exchange(points < 0 ? 0 : (int64_t)points);
+}
+int ow3d_test_set_tail_cluster(int blocks) { return g_tail_cluster.exchange(blocks < 0 ? 0 : blocks); }
 long long ow3d_test_set_coop_max_points(long long points) {
     return g_coop_max_points.exchange(points < 0 ? 0 : (int64_t)points);
 }

@@ -22,6 +22,8 @@ extern std::atomic<unsigned long long> g_kernel_launches;
 // Block count cap of the fused coarse-level kernel (0: one block per SM).
 extern std::atomic<int> g_coarse_blocks;
 extern std::atomic<int64_t> g_coop_max_points;
+extern std::atomic<int64_t> g_tail_max_points;
+extern std::atomic<int> g_tail_cluster;
 extern std::atomic<int> g_colour_tiles;
 extern std::atomic<int> g_colour_prefetch;
 // Set (on the capturing thread) when a launch sequence under stream capture

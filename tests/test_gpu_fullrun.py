@@ -24,7 +24,11 @@ test is on the true residual, the reference's on the preconditioned one. The
 tests bound the device's difference from the reference ordering (REF_TOL,
 about three times the oracle-to-oracle figure) and its matvec totals
 (REF_ITER_FRAC for FGMRES; the left-preconditioned device variant, with the
-reference's stopping test, within REF_ITER_FRAC_LEFT).
+reference's stopping test, within REF_ITER_FRAC_LEFT). Measured on a B200:
+FGMRES 5.5e-5 (shoal, eta) and 9.7e-7 / 6.4e-6 (flume, eta / phi) with
+75,335 and 12,580 matvecs; left GMRES 9.0e-5 / 1.0e-4 (shoal, eta / phi)
+and 6.9e-7 / 2.2e-6 (flume) with 51,728 and 9,540 matvecs against the
+reference ordering's 50,605 and 9,565.
 """
 import pathlib
 
@@ -42,7 +46,7 @@ RTOL_RUN = 1e-10
 # in the assertion messages)
 REF_TOL = {"shoal": 2e-4, "sfwave": 3e-5}
 REF_ITER_FRAC = 0.6
-REF_ITER_FRAC_LEFT = 0.25
+REF_ITER_FRAC_LEFT = 0.05
 
 
 def rel(a, b):
