@@ -95,6 +95,10 @@ int ow3d_test_breaking_state(ow3d_handle* h, double* tan_phi, double* Qr_x);
  * call after a step, with the roller-angle update and the roller record).
  * Uses the handle's stage buffer for E. */
 int ow3d_test_detect_breaking(ow3d_handle* h, const double* E, int update);
+/* The last step's local smoothing (accel_tol_fact <= 100): the surface
+ * Lagrangian dw/dt and the flags of the points where -dw/dt reached the
+ * limit, Nxg*Nyg each (either may be NULL; both zero before the third step). */
+int ow3d_test_accel_state(ow3d_handle* h, double* Wt, int* flags);
 
 /* Device time of `reps` launches of one kernel on this handle's stream,
  * measured with CUDA events around each launch; before each launch a write of

@@ -70,6 +70,7 @@ def lib():
         L.ow3d_test_relax_target.argtypes = [_C.c_void_p, _C.c_int, D, D]
         L.ow3d_test_breaking_state.argtypes = [_C.c_void_p, D, D]
         L.ow3d_test_detect_breaking.argtypes = [_C.c_void_p, D, _C.c_int]
+        L.ow3d_test_accel_state.argtypes = [_C.c_void_p, D, _C.POINTER(_C.c_int)]
         _lib = L
     return _lib
 
@@ -350,6 +351,15 @@ class Simulation:
         """One call of the breaking model on the surface E (a test hook)."""
         E = _f64(E).ravel()
         _check(lib().ow3d_test_detect_breaking(self.h, _d(E), 1 if update else 0), "ow3d_test_detect_breaking")
+
+    def accel_state(self):
+        """The last step's local smoothing: (surface dw/dt, 0-based columns
+        where -dw/dt reached the limit) -- a test hook."""
+        Wt = _np.zeros(self.C)
+        fl = _np.zeros(self.C, dtype=_np.int32)
+        _check(lib().ow3d_test_accel_state(self.h, _d(Wt), fl.ctypes.data_as(_C.POINTER(_C.c_int))),
+               "ow3d_test_accel_state")
+        return Wt, _np.flatnonzero(fl).astype(_np.int32)
 
     def breaking_state(self):
         """(tan_phi, Qr_x) per column of the roller breaking model."""

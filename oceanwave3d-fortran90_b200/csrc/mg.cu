@@ -556,7 +556,7 @@ std::atomic<int> g_coarse_blocks{0};
 // Levels with at most this many points run in the fused coarse kernel.
 std::atomic<int64_t> g_coop_max_points{160000};
 // Levels with at most this many points run in the cluster (tail) kernel (0: none).
-std::atomic<int64_t> g_tail_max_points{8192};
+std::atomic<int64_t> g_tail_max_points{0};
 // Blocks of the tail kernel's cluster (16 needs the non-portable cluster
 // size; the launcher falls back to 8 where 16 cannot be resident).
 std::atomic<int> g_tail_cluster{16};

@@ -96,6 +96,9 @@ struct ow3d_handle {
     // roller breaking model (x flumes with i_breaking > 0)
     BreakDev brk{};
     bool brk_on = false;
+    // local smoothing by the vertical acceleration (accel_tol_fact <= 100)
+    SmoothDev sm{};
+    bool sm_on = false;
     int* flag = nullptr;
     int* flag_host = nullptr;
     double hmax = 0;
@@ -736,6 +739,21 @@ int create_impl(const ow3d_params* p, const double* h, const double* hx, const d
         H->pd_h.L.clear(); H->pd_h.L.shrink_to_fit(); H->pd_h.Linv.clear(); H->pd_h.Linv.shrink_to_fit();
         H->pd_on = true;
     }
+    if (smoothing_on(*p)) {
+        SmoothDev& m = H->sm;
+        m.tol = p->accel_tol_fact * p->g;
+        m.dt_inv = 1.0 / p->dt;
+        m.z = H->zs; m.hx = H->hx; m.hy = H->hy;
+        for (int q = 0; q < 3; ++q) {
+            TRY(dalloc(H.get(), &m.WH[q], (size_t)G.C));
+            CK(cudaMemset(m.WH[q], 0, sizeof(double) * (size_t)G.C));
+        }
+        TRY(dalloc(H.get(), &m.Wt, (size_t)G.C)); TRY(dalloc(H.get(), &m.flag, (size_t)G.C));
+        TRY(dalloc(H.get(), &m.any, 1)); TRY(dalloc(H.get(), &m.sE, (size_t)G.C)); TRY(dalloc(H.get(), &m.sP, (size_t)G.C));
+        CK(cudaMemset(m.Wt, 0, sizeof(double) * (size_t)G.C));
+        CK(cudaMemset(m.flag, 0, sizeof(int) * (size_t)G.C));
+        H->sm_on = true;
+    }
     if (breaking_on(*p)) {
         // DetectBreaking.f90:38-70 (its first call): tan(phi) starts at tan(phi_b)
         BreakDev& b = H->brk;
@@ -895,6 +913,9 @@ int enqueue_step(ow3d_handle* H, int64_t tstep, bool graph, SolveF&& solve) {
     fs_set_rhs(fa, H->P, H->RHS, st);
     TRY(solve(surf(H->E, H->Ex, H->Exx, H->Ey, H->Eyy), 3));
     fs_wvel(fa, H->PHI, H->E, H->W, st);
+    // OceanWave3DTakeATimeStep.f90:33-39: local smoothing (from the third
+    // step on; the step number is read on the device)
+    if (H->sm_on) TRY(fs_local_smoothing(fa, H->sm, H->PHI, H->E, H->P, H->Ex, H->Ey, H->W, H->kE, H->sd, st));
     // the rollers of the new state and the roller-angle update
     // (OceanWave3DTakeATimeStep.f90:45-49)
     if (H->brk_on) fs_breaking(H->brk, H->E, 1, st);
@@ -1262,6 +1283,10 @@ int ow3d_estimate_bytes(const ow3d_params* p, size_t* bytes) {
                s * (double)kDenseMaxPoints * (double)kDenseMaxPoints * 2.0;
     // the inverse of a type-0 pressure-damping zone matrix: at most a row squared
     if (p->PDampingONOFF != 0 && p->pd_type == 0) b += 8.0 * (double)(p->Nx + 2) * (double)(p->Nx + 2);
+    // local smoothing: the W history, dw/dt, flags and two scratch fields;
+    // the breaking model: its per-column state and roller records
+    if (smoothing_on(*p)) b += 8.0 * C * 7;
+    if (breaking_on(*p)) b += 8.0 * C * 12;
     *bytes = (size_t)(b * 1.05) + ((size_t)64 << 20);
     return OW3D_OK;
 }
@@ -1532,6 +1557,19 @@ int ow3d_test_detect_breaking(ow3d_handle* H, const double* E, int update) {
     fs_breaking(H->brk, H->tE, update, H->st);
     CK(cudaStreamSynchronize(H->st));
     CK(cudaGetLastError());
+    return OW3D_OK;
+}
+
+int ow3d_test_accel_state(ow3d_handle* H, double* Wt, int* flags) {
+    if (!H || !H->sm_on) {
+        g_last_error = "ow3d_test_accel_state: no local smoothing on this handle";
+        return OW3D_ERR_BAD_INPUT;
+    }
+    CK(cudaSetDevice(H->dev));
+    const size_t n = (size_t)H->G.C;
+    if (Wt) CK(cudaMemcpyAsync(Wt, H->sm.Wt, sizeof(double) * n, cudaMemcpyDeviceToHost, H->st));
+    if (flags) CK(cudaMemcpyAsync(flags, H->sm.flag, sizeof(int) * n, cudaMemcpyDeviceToHost, H->st));
+    CK(cudaStreamSynchronize(H->st));
     return OW3D_OK;
 }
 

@@ -77,6 +77,26 @@ struct BreakDev {
 // the roller records (the call after the step).
 void fs_breaking(const BreakDev& b, const double* E, int update, cudaStream_t st);
 
+// Local smoothing by the surface's vertical acceleration (LocalSmoothing2D.f90,
+// LocalSmoothing3D.f90), after each step.
+struct SmoothDev {
+    double tol;              // accel_tol_fact * g
+    double dt_inv;
+    const double* z;         // Nzg sigma levels
+    const double *hx, *hy;
+    double* WH[3];           // W after step t is filed in WH[t % 3]
+    double* Wt;              // C: the surface dw/dt of the last step
+    int* flag;               // C: -dw/dt reached the limit at a point i = 6..Nxg-5
+    int* any;                // some point of the step did
+    double *sE, *sP;         // C each: the filtered fields before the copy back
+};
+
+// From the third step on: dw/dt, the flags, and the filter of E and P where
+// they call for it; every step: W filed in the history ring.
+int fs_local_smoothing(const FsArgs& a, const SmoothDev& s, const double* phi, double* E, double* P,
+                       const double* Ex, const double* Ey, const double* W, double* const* kE, const StepDev* sd,
+                       cudaStream_t st);
+
 // NuD and Pd of the state (E, P): the damping terms the next fs_stage adds.
 void fs_pdamp(const FsArgs& a, const PDampDev& d, const double* E, const double* P, cudaStream_t st);
 // NuD and Pd may be null (no pressure damping), Qr_x likewise (no breaking).

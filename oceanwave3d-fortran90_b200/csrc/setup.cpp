@@ -158,12 +158,13 @@ static void level_colours(LevelHost& L) {
 
 bool breaking_on(const ow3d_params& p) { return p.i_breaking > 0 && p.Ny == 1 && p.Nx > 1; }
 
+bool smoothing_on(const ow3d_params& p) {
+    return p.accel_from_deck ? p.accel_tol_fact <= 100.0 : (p.accel_tol_fact > 0.0 && p.accel_tol_fact <= 100.0);
+}
+
 // Deck features that change the physics but lie outside this library's path:
 // a deck that turns one on is refused (OW3D_ERR_UNSUPPORTED) rather than run
-// without it. The acceleration limit of line 2 turns the filter on for every
-// value up to 100 g (LocalSmoothing2D.f90:37; decks write 1000 to turn it
-// off); for parameters that did not come from a deck, 0, the value of a
-// zero-initialised ow3d_params, counts as off. IncWaveType 4 and 5 add a
+// without it. IncWaveType 4 and 5 add a
 // constant-flux current to the wave (ReadInputFileParameters.f90:42-49),
 // which enters the right-hand side and the lateral Neumann rows.
 int check_supported(const ow3d_params& p, std::string* err) {
@@ -171,9 +172,6 @@ int check_supported(const ow3d_params& p, std::string* err) {
     if (p.IncWaveType == 3) return no("IncWaveType 3 (flux wave generation at the boundary) is not built");
     if (p.IncWaveType == 4 || p.IncWaveType == 5)
         return no("IncWaveType 4 and 5 (a wave with a constant-flux current) are not built");
-    const bool smoothing = p.accel_from_deck ? p.accel_tol_fact <= 100.0
-                                             : (p.accel_tol_fact > 0.0 && p.accel_tol_fact <= 100.0);
-    if (smoothing) return no("local filtering by the vertical acceleration (deck line 2) is not built");
     if (p.PDampingONOFF != 0) {
         // BuildPDampMatrices.f90:37-40 stops for Ny > 1; the friction form
         // (type != 0) spreads its gamma over y lines inconsistently there
@@ -208,6 +206,8 @@ int check_params(const ow3d_params& p, std::string* err) {
     if (p.precision != OW3D_PREC_FP64 && p.precision != OW3D_PREC_MIXED) return fail("precision must be 0 or 1");
     if (p.krylov != OW3D_KRYLOV_FGMRES && p.krylov != OW3D_KRYLOV_LGMRES) return fail("krylov must be 0 or 1");
     if (p.GMRESmaxiterations < 1) return fail("GMRESmaxiterations must be >= 1");
+    if (smoothing_on(p) && p.periodic_x != 0)
+        return fail("periodic_x: local smoothing by the vertical acceleration is built for wall boundaries");
     if (breaking_on(p)) {
         // the roller-angle update divides by T_half (DetectBreaking.f90:181)
         if (!(p.T_half > 0.0)) return fail("breaking model: T_half > 0 required");

@@ -59,6 +59,11 @@ int check_supported(const ow3d_params& p, std::string* err);
 // The roller breaking model runs: i_breaking > 0 on an x flume (Ny = 1),
 // where the reference calls detect_breaking (Runge_Kutta_4.f90:55).
 bool breaking_on(const ow3d_params& p);
+// Local smoothing by the vertical acceleration runs (LocalSmoothing2D.f90:37):
+// every acceleration limit up to 100 g that a deck gives (decks write 1000 to
+// turn it off), or a limit in (0, 100] that a caller sets (0, the value of a
+// zero-initialised ow3d_params, counts as off).
+bool smoothing_on(const ow3d_params& p);
 
 int build_grid(const ow3d_params& p, const double* h, const double* hx, const double* hxx, const double* hy,
                const double* hyy, GridHost& G, std::string* err);

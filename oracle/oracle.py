@@ -87,6 +87,7 @@ def lib():
         L.orc_rollers.argtypes = [V, C.c_int, I, I, D, D, D, D]
         L.orc_breaking_state.argtypes = [V, D, D]
         L.orc_detect_breaking.argtypes = [V, D, C.c_int]
+        L.orc_accel_state.argtypes = [V, D, C.c_int, I]
         _lib = L
     return _lib
 
@@ -268,6 +269,15 @@ class Oracle:
         E = _c(E)
         if lib().orc_detect_breaking(self.h, _p(E), 1 if update else 0) != 0:
             raise ValueError("oracle: no breaking model in this simulation")
+
+    def accel_state(self):
+        """The last local-smoothing call (LocalSmoothing2D/3D.f90): the surface
+        dw/dt per column and the 0-based columns where -dw/dt reached the
+        limit; None when the filter is off."""
+        Wt = np.zeros(self.C)
+        cols = np.zeros(self.C, dtype=np.int32)
+        n = lib().orc_accel_state(self.h, _p(Wt), self.C, cols.ctypes.data_as(C.POINTER(C.c_int)))
+        return None if n < 0 else (Wt, cols[:n].copy())
 
     def breaking_state(self):
         t, q = np.zeros(self.C), np.zeros(self.C)

@@ -81,6 +81,11 @@ struct Sim {
     vector<double> tan_phi, Qr_x;        // per column: roller angle state, roller flux slope
     vector<int> r_npts, r_toe;           // rollers of the last completed step
     vector<double> r_x, r_eta, r_thick, r_tan;
+    // local smoothing by the vertical acceleration (LocalSmoothing2D/3D.f90)
+    int smooth = 0;
+    vector<double> WHist[3], EtatHist1;  // W after the last three steps; eta_t of the last step
+    vector<double> accel_Wt;             // the last call's Lagrangian dw/dt at the surface
+    vector<int> accel_pts;               // columns (0-based) where it exceeded the limit
     // stats
     int64_t solves = 0, totit = 0, notconv = 0; int minit = 1 << 30, maxit = 0, lastit = 0;
     double lastres = 0;
@@ -1452,6 +1457,78 @@ static void detect_breaking(Sim& s, const vector<double>& E, bool update) {
         for (int j = 3; j <= nfx - 2; ++j) s.Qr_x[(size_t)j - 1] = quart * Qr[j + 1] + half * Qr[j] + quart * Qr[j - 1];
 }
 
+// --------------------------------------------------- local smoothing
+// LocalSmoothing2D.f90:37-145 (x flumes) and LocalSmoothing3D.f90 (3-D),
+// called after each step from OceanWave3DTakeATimeStep.f90:33-39 with the
+// step number: from the third step on, the Lagrangian vertical acceleration
+// of the surface, dw/dt = (3 W^n - 4 W^(n-1) + W^(n-2)) / (2 dt) - w_z eta_t
+// + u w_x (+ v w_y) + w w_z, is formed from the last solution (the velocity
+// and its gradients in physical space by the sigma chain rule, as the
+// reference takes them on the whole grid); where -dw/dt >= accel_tol_fact g
+// at a point i = 6..Nxg-5 of a row, the points i-5..i+5 of that row get the
+// weight 1/4, and if any point did, eta and the surface potential of every
+// row are filtered with [a, 1-2a, a] over i = 2..Nxg-1. As in the reference
+// the 3-D v takes the x derivative of phi (DiffXEven called with beta).
+static void local_smoothing(Sim& s) {
+    if (!s.smooth || s.tstep < 3) return;
+    const int Nx = s.Nxg, Ny = s.Nyg, Nz = s.Nzg;
+    const size_t N = s.N, C = s.C;
+    const bool three = s.dimcase == 3;
+    const double one = 1.0, half = 0.5, two = 2.0, three_ = 3.0, four = 4.0;
+    const vector<double>& z = s.fine.z;
+    vector<double> d(C), U(N), V(three ? N : 0), W(N), Wz(N), Wx(N), Wy(three ? N : 0);
+    for (size_t c = 0; c < C; ++c) d[c] = s.fine.h[c] + s.E[c];
+    diff_x(s, s.PHI.data(), U.data(), 1, Nz);
+    if (three) diff_x(s, s.PHI.data(), V.data(), 1, Nz);
+    diff_z(s, s.PHI.data(), W.data(), 1);
+    for (size_t c = 0; c < C; ++c)
+        for (int k = 1; k <= Nz; ++k) {
+            const size_t q = c * Nz + (size_t)k - 1;
+            W[q] = W[q] / d[c];
+            U[q] = U[q] + ((one - z[k - 1]) * s.fine.hx[c] - z[k - 1] * s.Ex[c]) * W[q];
+            if (three) V[q] = V[q] + ((one - z[k - 1]) * s.fine.hy[c] - z[k - 1] * s.Ey[c]) * W[q];
+        }
+    diff_z(s, W.data(), Wz.data(), 1);
+    diff_x(s, W.data(), Wx.data(), 1, Nz);
+    if (three) diff_y(s, W.data(), Wy.data(), 1, Nz);
+    for (size_t c = 0; c < C; ++c)
+        for (int k = 1; k <= Nz; ++k) {
+            const size_t q = c * Nz + (size_t)k - 1;
+            Wz[q] = Wz[q] / d[c];
+            Wx[q] = Wx[q] + ((one - z[k - 1]) * s.fine.hx[c] - z[k - 1] * s.Ex[c]) * Wz[q];
+            if (three) Wy[q] = Wy[q] + ((one - z[k - 1]) * s.fine.hy[c] - z[k - 1] * s.Ey[c]) * Wz[q];
+        }
+    const double dt_inv = one / s.p.dt;
+    vector<double>& Wt = s.accel_Wt;
+    Wt.assign(C, 0.0);
+    for (size_t c = 0; c < C; ++c) {
+        const size_t q = c * Nz + (size_t)Nz - 1;
+        Wt[c] = half * dt_inv * (three_ * s.WHist[0][c] - four * s.WHist[1][c] + s.WHist[2][c]) - Wz[q] * s.EtatHist1[c];
+        if (three) Wt[c] = Wt[c] + U[q] * Wx[q] + V[q] * Wy[q] + W[q] * Wz[q];
+        else Wt[c] = Wt[c] + U[q] * Wx[q] + W[q] * Wz[q];
+    }
+    const double accel_tol = s.p.accel_tol_fact * s.p.g;
+    vector<double> alpha_s(C, 0.0);
+    s.accel_pts.clear();
+    for (int j = 1; j <= Ny; ++j)
+        for (int i = 6; i <= Nx - 5; ++i) {
+            const size_t c = (size_t)(i - 1) + (size_t)Nx * (j - 1);
+            if (-Wt[c] >= accel_tol) {
+                s.accel_pts.push_back((int)c);
+                for (int ii = i - 5; ii <= i + 5; ++ii) alpha_s[(size_t)(ii - 1) + (size_t)Nx * (j - 1)] = 0.25;
+            }
+        }
+    if (s.accel_pts.empty()) return;
+    const vector<double> et(s.E), ph(s.P);
+    for (int j = 1; j <= Ny; ++j)
+        for (int i = 2; i <= Nx - 1; ++i) {
+            const size_t c = (size_t)(i - 1) + (size_t)Nx * (j - 1);
+            const double a = alpha_s[c];
+            s.E[c] = a * et[c - 1] + (one - two * a) * et[c] + a * et[c + 1];
+            s.P[c] = a * ph[c - 1] + (one - two * a) * ph[c] + a * ph[c + 1];
+        }
+}
+
 // ------------------------------------------------------------- RK4 step
 // Runge_Kutta_4.f90:1-429 (nonlinear or linear FSBC, no SWENSE, no pressure).
 static int rk4_step(Sim& s) {
@@ -1535,6 +1612,9 @@ static int rk4_step(Sim& s) {
         s.E[c] = s.E[c] + dt / six * (k1E[c] + two * k2E[c] + two * k3E[c] + k4E[c]);
         s.P[c] = s.P[c] + dt / six * (k1P[c] + two * k2P[c] + two * k3P[c] + k4P[c]);
     }
+    if (s.smooth) {   // Runge_Kutta_4.f90:347-348
+        for (size_t c = 0; c < C; ++c) s.EtatHist1[c] = 1.0 / six * (k1E[c] + two * k2E[c] + two * k3E[c] + k4E[c]);
+    }
     RKtime = time + dt;
     if (s.p.filteringONOFF > 0 && (tstep % s.p.filteringONOFF) == 0) { filter(s, s.E); filter(s, s.P); }
     relax(s, s.E, s.P, RKtime, time);
@@ -1544,6 +1624,12 @@ static int rk4_step(Sim& s) {
     set_rhs(s.P);
     do_solve();
     vertical_velocity(s, s.W);
+    if (s.smooth) {   // Runge_Kutta_4.f90:426-427
+        std::swap(s.WHist[2], s.WHist[1]); std::swap(s.WHist[1], s.WHist[0]);
+        s.WHist[0] = s.W;
+    }
+    // OceanWave3DTakeATimeStep.f90:33-39
+    local_smoothing(s);
     // rollers of the new state and the roller-angle update (OceanWave3DTakeATimeStep.f90:45-49)
     if (s.brk) detect_breaking(s, s.E, true);
     // instability check and time advance (OceanWave3DTakeATimeStep.f90:54-70)
@@ -1588,6 +1674,11 @@ static Sim* create(const ow3d_params* p, const double* h, const double* hx, cons
     setup_zones(*s);
     setup_pdamp(*s);
     // DetectBreaking.f90:38-70 (the first call): tan(phi) starts at tan(phi_b); Initialize.f90:7-8
+    // local smoothing on for limits up to 100 g (LocalSmoothing2D.f90:37): any
+    // value a deck gives, or a positive one set by a caller
+    s->smooth = (p->accel_from_deck ? p->accel_tol_fact <= 100.0
+                                    : (p->accel_tol_fact > 0.0 && p->accel_tol_fact <= 100.0)) ? 1 : 0;
+    if (s->smooth) { for (auto& v : s->WHist) v.assign(C, 0.0); s->EtatHist1.assign(C, 0.0); }
     s->brk = (p->i_breaking > 0 && p->Ny == 1 && p->Nx > 1) ? 1 : 0;
     s->Qr_x.assign(C, 0.0);
     if (s->brk) {
@@ -1723,6 +1814,15 @@ int orc_rollers(void* sv, int cap, int* npts, int* toe, double* x, double* eta, 
 int orc_detect_breaking(void* sv, const double* E, int update) {
     Sim* s = (Sim*)sv; if (!s->brk) return -1;
     vector<double> e(E, E + s->C); detect_breaking(*s, e, update != 0); return 0;
+}
+// the last local-smoothing call: dw/dt at the surface (C values) and the
+// columns where it exceeded the limit; returns their count (-1: off)
+int orc_accel_state(void* sv, double* Wt, int cap, int* cols) {
+    Sim* s = (Sim*)sv; if (!s->smooth) return -1;
+    if (Wt && !s->accel_Wt.empty()) std::copy(s->accel_Wt.begin(), s->accel_Wt.end(), Wt);
+    const int n = (int)s->accel_pts.size();
+    for (int q = 0; q < n && q < cap; ++q) cols[q] = s->accel_pts[q];
+    return n;
 }
 void orc_breaking_state(void* sv, double* tan_phi, double* Qr_x) {
     Sim* s = (Sim*)sv;

@@ -156,8 +156,8 @@ def test_reference_example_decks_parse(ow3d):
 
 def test_decks_needing_unbuilt_features_are_refused(ow3d, tmp_path):
     """A deck that turns on a feature outside this library's path (pressure
-    damping in 3-D, SWENSE, flux wave generation, local
-    filtering by acceleration) is refused with OW3D_ERR_UNSUPPORTED by ow3d_create and
+    damping in 3-D, SWENSE, flux wave generation, a constant-flux current) is
+    refused with OW3D_ERR_UNSUPPORTED by ow3d_create and
     ow3d_estimate_bytes instead of running without it."""
     import ctypes as C
     L = ow3d.lib()
@@ -173,11 +173,6 @@ def test_decks_needing_unbuilt_features_are_refused(ow3d, tmp_path):
         "pressure": base.replace("0 0\n0 2.0 2", "1 1\n0. 5. 0. 10. 0.1 0.1 0\n0 2.0 2"),
         "SWENSE": base.replace("0 2.0 2 0 0 1 0", "1 2.0 2 0 0 1 0"),
         "IncWaveType 3": base.replace("-1 0  ", "-1 3  "),
-        "acceleration": base.replace("-1 0  ", "-1 0 0.5 "),
-        "acceleration, 100 g": base.replace("-1 0  ", "-1 0 100. "),
-        # LocalSmoothing2D.f90:37 smooths for every limit up to 100 g when a deck gives one
-        "acceleration, 0": base.replace("-1 0  ", "-1 0 0. "),
-        "acceleration, negative": base.replace("-1 0  ", "-1 0 -5. "),
         # a stream-function or flux wave with a constant-flux current (ReadInputFileParameters.f90:42-49)
         "IncWaveType 4": base.replace("-1 0  ", "-1 4  "),
         "IncWaveType 5": base.replace("-1 0  ", "-1 5  "),
@@ -193,9 +188,9 @@ def test_decks_needing_unbuilt_features_are_refused(ow3d, tmp_path):
     # deck with it on runs without it, as in the reference
     st, p = status(base.replace("1 6 10 0.08 0.08 0.4", "1 6 10 0.08 0.08 0.4\n1 1.0 32. 20. 1.5 1.3 1.0"))
     assert st == 0 and p.i_breaking == 1
-    # parameters built by a caller: accel_tol_fact = 0 (zero-initialised) means no smoothing
-    q = ow3d.default_params(Nx=33, Ny=17, Nz=9)
-    q.accel_tol_fact = 0.0
-    assert L.ow3d_estimate_bytes(C.byref(q), C.byref(C.c_size_t())) == 0
-    q.accel_tol_fact = 50.0
-    assert L.ow3d_estimate_bytes(C.byref(q), C.byref(C.c_size_t())) == ow3d.capi.ERR_UNSUPPORTED
+    # local smoothing by the vertical acceleration is built: every limit up to
+    # 100 g that a deck gives turns it on (LocalSmoothing2D.f90:37), 0 and
+    # negative values included
+    for text in ("-1 0 0.5 ", "-1 0 100. ", "-1 0 0. ", "-1 0 -5. "):
+        st, p = status(base.replace("-1 0  ", text))
+        assert st == 0 and p.accel_from_deck == 1, text
