@@ -297,8 +297,8 @@ def serving_sample(n=16, seed=2024, rate=50.0, nx=(65, 129, 257), ny=(1, 33, 65)
             "wall_s", "completed", "steps")
     runs = {}
     for cap in slots:
-        srv = S.Server(S.DeviceBackend(pkg, precision=pkg.capi.PREC_MIXED), budget_bytes=int(0.5 * free),
-                       max_slots=cap or n)
+        srv = S.Server(S.DeviceBackend(pkg, precision=pkg.capi.PREC_MIXED, coarse_cluster=True),
+                       budget_bytes=int(0.5 * free), max_slots=cap or n)
         r = srv.run(mk())
         runs[cap or n] = {k: r[k] for k in keys} | {"peak_slots": r["peak_slots"],
                                                    "throughput_ratio": r["dof_timesteps_per_s"] / max(seq["dof_timesteps_per_s"], 1e-30)}

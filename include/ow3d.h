@@ -82,8 +82,9 @@ typedef struct ow3d_zone {
  * restricted to the fields the hot path reads, plus build-only knobs. */
 typedef struct ow3d_params {
     /* line 2 */
-    int    IC, IncWaveType;       /* as the deck writes it: 4 and 5 (a wave with a
-                                     constant-flux current) are refused by ow3d_create */
+    int    IC, IncWaveType;       /* ow3d_read_deck reads 4 as 1 with current_flag = 1
+                                     (see current_Q); 3 and 5 (the flux wavemaker, alone
+                                     or with a current) are refused by ow3d_create */
     /* line 3 */
     double Lx, Ly, Lz;
     int    Nx, Ny, Nz;
@@ -190,6 +191,14 @@ typedef struct ow3d_params {
     double phi_b, phi_0;              /* breaking and terminal roller angles, degrees */
     double del_fac;                   /* roller thickness factor f_delta */
     double cel_fac, gamma_break;      /* read and kept; the reference computes nothing from them */
+    /* the constant-flux current of IncWaveType 4 (ReadInputFileParameters.f90:42-49,
+     * 655-690): ow3d_read_deck reads IncWaveType 4 as 1 (the stream-function
+     * wave) with current_flag = 1 and the flux Q from the line after the
+     * curvilinear line. The lateral Neumann rows then carry u = Q/h at the
+     * west and east walls (Runge_Kutta_4.f90:112,207,291,412) and the surface
+     * potential's ghost points the same flux (:85-88). */
+    int    current_flag;
+    double current_Q;                 /* m^2/s */
 } ow3d_params;
 
 typedef struct ow3d_handle ow3d_handle;
@@ -402,6 +411,17 @@ int ow3d_set_relax_target(ow3d_handle* h, int zone, int mode, int nt,
  * OceanWave3DTakeATimeStep.f90:27. Returns OW3D_ERR_UNSTABLE on the
  * reference's instability test; OW3D_NOT_CONVERGED if any solve hit the limit. */
 int ow3d_step(ow3d_handle* h, int nsteps);
+
+/* on = 1: the coarse levels of every V-cycle run in one thread-block
+ * cluster of 16 SMs (8 where 16 cannot be resident) instead of a cooperative
+ * grid over every SM -- no counterpart in the reference. For handles stepped
+ * together (ow3d_step_batch): the coarse cycles of different simulations then
+ * overlap, where a grid-wide cycle takes the whole device for its duration.
+ * Measured on a B200 over a stream of the serving configuration's sizes: 1.55x
+ * the batched throughput and half the step latency; a handle stepped alone is
+ * 10-30% slower with it, so the default is off. Results are bitwise the same
+ * either way. Drops the handle's captured graphs. */
+int ow3d_set_coarse_cluster(ow3d_handle* h, int on);
 
 /* The rollers of the roller breaking model (i_breaking > 0, Ny = 1) after
  * the last completed step, as the reference writes them to roller.dat each

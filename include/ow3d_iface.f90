@@ -38,7 +38,7 @@ MODULE ow3d_iface
   ! ow3d_params mirrors the deck (include/ow3d.h); filled by ow3d_read_deck
   ! and opaque to Fortran
   TYPE, BIND(C) :: ow3d_params_t
-     INTEGER(c_int8_t) :: raw(2192)         ! opaque to Fortran: sizeof(ow3d_params)
+     INTEGER(c_int8_t) :: raw(2208)         ! opaque to Fortran: sizeof(ow3d_params)
   END TYPE
 
   INTERFACE

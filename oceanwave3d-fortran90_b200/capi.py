@@ -75,6 +75,7 @@ class Params(C.Structure):
         ("accel_from_deck", C.c_int), ("periodic_x", C.c_int),
         ("T_half", C.c_double), ("phi_b", C.c_double), ("phi_0", C.c_double),
         ("del_fac", C.c_double), ("cel_fac", C.c_double), ("gamma_break", C.c_double),
+        ("current_flag", C.c_int), ("current_Q", C.c_double),
     ]
 
 
@@ -175,6 +176,7 @@ def declare(lib):
         "ow3d_get_stats": (C.c_int, [H, C.POINTER(Stats)]),
         "ow3d_reset_stats": (C.c_int, [H]),
         "ow3d_set_graphs": (C.c_int, [H, C.c_int]),
+        "ow3d_set_coarse_cluster": (C.c_int, [H, C.c_int]),
         "ow3d_zone_box": (C.c_int, [H, C.c_int, _I, _I, _I, _I]),
         "ow3d_strerror": (C.c_char_p, [C.c_int]),
         "ow3d_version": (C.c_char_p, []),

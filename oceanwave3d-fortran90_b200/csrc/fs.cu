@@ -185,9 +185,10 @@ __global__ void k_images(FsArgs a, double* v, int nz, int zero) {
     }
 }
 
-// Ghost values so that the boundary one-sided d/dx equals S (zero); with
-// periodic x, the image columns instead.
-__global__ void k_ghost_x(FsArgs a, double* v1, double* v2) {
+// Ghost values so that the boundary one-sided d/dx equals S: zero for E, the
+// current's flux Ul / Ur for P when src is set, else zero
+// (UpdateGhostLayerX.f90:15-20); with periodic x, the image columns instead.
+__global__ void k_ghost_x(FsArgs a, double* v1, double* v2, int src) {
     const int Nx = a.Nxg;
     if (a.per) {
         for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < a.Nyg; j += gridDim.x * blockDim.x) {
@@ -205,12 +206,13 @@ __global__ void k_ghost_x(FsArgs a, double* v1, double* v2) {
             double* r = vs[q] + (int64_t)Nx * (j - 1);
             const double* s0 = a.SX + (int64_t)(2 - 1) * kHoRank;          // stencil of point i = 2
             const double* s1 = a.SX + (int64_t)(Nx - 1 - 1) * kHoRank;     // stencil of point i = Nx-1
+            const double sw = (q == 1 && src) ? a.Ul : 0.0, se = (q == 1 && src) ? a.Ur : 0.0;
             double acc = 0;
             for (int m = 1; m < kHoRank; ++m) acc += s0[m] * r[m];
-            r[0] = (0.0 - acc) / s0[0];
+            r[0] = (sw - acc) / s0[0];
             acc = 0;
             for (int m = 0; m < kHoRank - 1; ++m) acc += s1[m] * r[Nx - kHoRank + m];
-            r[Nx - 1] = (0.0 - acc) / s1[kHoRank - 1];
+            r[Nx - 1] = (se - acc) / s1[kHoRank - 1];
         }
     }
 }
@@ -297,12 +299,20 @@ __global__ void k_wvel(FsArgs a, const double* __restrict__ phi, const double* _
     }
 }
 
-// RHS free-surface row = P at the interior columns (Runge_Kutta_4.f90:106-107).
+// RHS free-surface row = P at the interior columns (Runge_Kutta_4.f90:106-107);
+// the x-ghost columns' Neumann rows = the current's Ul (west) and Ur (east)
+// at every level of the interior rows (:108-113), zero without a current.
 __global__ void k_set_rhs(FsArgs a, const double* __restrict__ P, double* __restrict__ rhs) {
     const int64_t C = (int64_t)a.Nxg * a.Nyg;
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < C; p += (int64_t)gridDim.x * blockDim.x) {
         const int i = (int)(p % a.Nxg), j = (int)(p / a.Nxg);
-        const bool ghost = i == 0 || i == a.Nxg - 1 || (a.three && (j == 0 || j == a.Nyg - 1));
+        const bool yghost = a.three && (j == 0 || j == a.Nyg - 1);
+        if (!a.per && !yghost && (i == 0 || i == a.Nxg - 1)) {
+            const double u = i == 0 ? a.Ul : a.Ur;
+            for (int k = 0; k < a.Nzg; ++k) rhs[p * a.Nzg + k] = u;
+            continue;
+        }
+        const bool ghost = i == 0 || i == a.Nxg - 1 || yghost;
         if (ghost) continue;
         if (a.per && i == a.Nxg - 2) continue;   // the repeated column: identity rows, zero
         rhs[p * a.Nzg + a.Nzg - 1] = P[p];
@@ -451,9 +461,9 @@ void fs_relax(const FsArgs& a, const RelaxZoneDev* zones, int nz, double* E, dou
 void fs_step_begin(StepDev* sd, cudaStream_t st) { note_launch(), k_step_begin<<<1, 32, 0, st>>>(sd); }
 void fs_step_end(StepDev* sd, double dt, cudaStream_t st) { note_launch(), k_step_end<<<1, 32, 0, st>>>(sd, dt); }
 void fs_derivs(const FsArgs& a, double* E, double* P, double* Ex, double* Exx, double* Px, double* Ey, double* Eyy,
-               double* Py, cudaStream_t st) {
+               double* Py, int src, cudaStream_t st) {
     int64_t C = (int64_t)a.Nxg * a.Nyg;
-    note_launch(), k_ghost_x<<<nb(a.Nyg, 128), 128, 0, st>>>(a, E, P);
+    note_launch(), k_ghost_x<<<nb(a.Nyg, 128), 128, 0, st>>>(a, E, P, src);
     note_launch(), k_diff_x<<<nb(C), 256, 0, st>>>(a, E, P, Ex, Exx, Px);
     if (a.three) {
         note_launch(), k_ghost_y<<<nb(a.Nxg, 128), 128, 0, st>>>(a, E, P);

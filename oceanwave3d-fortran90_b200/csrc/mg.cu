@@ -652,7 +652,7 @@ static void coarse_cycle(const LevelDev<T>* lev, int lc, int ld, const T* M, int
     }
     const LevelDev<T>* P = pack.dev;
     // the tail: levels ld+1..lt of at most g_tail_max_points points
-    const int64_t tmax = g_tail_max_points.load(std::memory_order_relaxed);
+    const int64_t tmax = pack.cluster ? INT64_MAX : g_tail_max_points.load(std::memory_order_relaxed);
     const int cl = tmax > 0 ? tail_cluster_size<T, THREE>(g_tail_cluster.load(std::memory_order_relaxed)) : 0;
     int lt = ld;
     if (cl > 0)

@@ -672,6 +672,9 @@ int create_impl(const ow3d_params* p, const double* h, const double* hx, const d
     fa.Nxg = G.Nxg; fa.Nyg = G.Nyg; fa.Nzg = G.Nzg; fa.three = G.three; fa.nonlinear = hg.nonlinear; fa.g = p->g;
     fa.per = G.per;
     fa.SX = H->SX; fa.SY = H->SY; fa.SZ = H->SZ; fa.h = H->h;
+    // OceanWave3DT0Setup.f90:325-326: Ul = Q / h(1,1), Ur = Q / h(Nx+GhostGridX,1)
+    fa.Ul = p->current_flag ? p->current_Q / G.h[0] : 0.0;
+    fa.Ur = p->current_flag ? p->current_Q / G.h[(size_t)G.Nxg - 2] : 0.0;
     H->hmax = *std::max_element(G.h.begin(), G.h.end());
     // multigrid
     H->nlev = (int)G.levels.size();
@@ -840,7 +843,7 @@ int enqueue_step(ow3d_handle* H, int64_t tstep, bool graph, SolveF&& solve) {
             fs_relax(fa, H->zones.data(), (int)H->zones.size(), E, P, H->sd, off, H->p.relaxTransientTime, st);
     };
     auto derivs = [&](double* E, double* P, double* Ex, double* Exx, double* Px, double* Ey, double* Eyy, double* Py) {
-        fs_derivs(fa, E, P, Ex, Exx, Px, Ey, Eyy, Py, st);
+        fs_derivs(fa, E, P, Ex, Exx, Px, Ey, Eyy, Py, 1, st);
     };
     const bool nl = H->p.LinearONOFF == 1;
     auto surf = [&](const double* E, const double* Ex, const double* Exx, const double* Ey, const double* Eyy) {
@@ -1385,7 +1388,8 @@ int ow3d_set_state(ow3d_handle* H, const double* E, const double* P, const doubl
     CK(cudaMemsetAsync(H->LP[1], 0, nb, H->st));
     CK(cudaMemsetAsync(H->RHS, 0, nb, H->st));
     // OceanWave3DT0Setup.f90:444 -- surface derivatives of the initial state
-    fs_derivs(H->fa, H->E, H->P, H->Ex, H->Exx, H->Px, H->Ey, H->Eyy, H->Py, H->st);
+    // (the current's ghost source is still zero there)
+    fs_derivs(H->fa, H->E, H->P, H->Ex, H->Exx, H->Px, H->Ey, H->Eyy, H->Py, 0, H->st);
     {
         const StepDev s0{t, 0};
         CK(cudaMemcpyAsync(H->sd, &s0, sizeof(StepDev), cudaMemcpyHostToDevice, H->st));
@@ -1405,7 +1409,8 @@ int ow3d_put_surface(ow3d_handle* H, const double* E, const double* P) {
     const size_t cb = sizeof(double) * (size_t)H->G.C;
     CK(cudaMemcpyAsync(H->E, E, cb, cudaMemcpyHostToDevice, H->st));
     CK(cudaMemcpyAsync(H->P, P, cb, cudaMemcpyHostToDevice, H->st));
-    fs_derivs(H->fa, H->E, H->P, H->Ex, H->Exx, H->Px, H->Ey, H->Eyy, H->Py, H->st);
+    // after a step the surface potential's ghost source holds the current's flux
+    fs_derivs(H->fa, H->E, H->P, H->Ex, H->Exx, H->Px, H->Ey, H->Eyy, H->Py, H->tstep > 0 ? 1 : 0, H->st);
     CK(cudaGetLastError());
     return OW3D_OK;
 }
@@ -1994,6 +1999,21 @@ int ow3d_reset_stats(ow3d_handle* H) {
     std::memset(&H->stats, 0, sizeof(H->stats));
     H->stats.time = t;
     H->stats.tstep = ts;
+    return OW3D_OK;
+}
+
+int ow3d_set_coarse_cluster(ow3d_handle* H, int on) {
+    if (!H) return OW3D_ERR_BAD_INPUT;
+    const bool c = on != 0;
+    if (H->mg64.table.cluster == c && H->mg32.table.cluster == c) return OW3D_OK;
+    CK(cudaSetDevice(H->dev));
+    CK(cudaStreamSynchronize(H->st));
+    H->mg64.table.cluster = c;
+    H->mg32.table.cluster = c;
+    // the captured launches hold the other coarse kernel
+    drop_step_graphs(H);
+    for (auto& g : H->iter_graphs) cudaGraphExecDestroy(g.exec);
+    H->iter_graphs.clear();
     return OW3D_OK;
 }
 

@@ -13,6 +13,9 @@ struct FsArgs {
     const double* SY;   // [2][Nyg][7]
     const double* SZ;   // [2][Nzg][7]
     const double* h;
+    // the constant-flux current (IncWaveType 4): u = Q/h at the west and east
+    // walls (OceanWave3DT0Setup.f90:325-326), 0 without one
+    double Ul, Ur;
 };
 
 // The time level on the device: the simulation time at the start of the
@@ -112,8 +115,11 @@ void fs_relax(const FsArgs& a, const RelaxZoneDev* zones, int nz, double* E, dou
 // Start of a step: tstep += 1. End of a step: time += dt.
 void fs_step_begin(StepDev* sd, cudaStream_t st);
 void fs_step_end(StepDev* sd, double dt, cudaStream_t st);
+// src: the surface potential's ghost points carry the current's flux (the
+// RK stages' sourcePx, Runge_Kutta_4.f90:85-88); 0 at set-up, where the
+// reference's source is still zero (OceanWave3DT0Setup.f90:444).
 void fs_derivs(const FsArgs& a, double* E, double* P, double* Ex, double* Exx, double* Px, double* Ey, double* Eyy,
-               double* Py, cudaStream_t st);
+               double* Py, int src, cudaStream_t st);
 void fs_wvel(const FsArgs& a, const double* phi, const double* E, double* W, cudaStream_t st);
 // Periodic x: copy the distinct columns into the image columns of a field
 // with nz values per column (1 <- Nxg-2, Nxg-1 <- 2, Nxg <- 3), or zero them.

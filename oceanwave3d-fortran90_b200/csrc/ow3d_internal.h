@@ -199,6 +199,9 @@ template <typename T>
 struct LevelTable {
     LevelDev<T>* dev = nullptr;
     LevelDev<T> host[kMaxLevels];
+    // the whole fused coarse cycle in one thread-block cluster instead of a
+    // cooperative grid over every SM (ow3d_set_coarse_cluster)
+    bool cluster = false;
 };
 
 // M: dense operator of level ld (the coarsest level's inverse when ld = 0).

@@ -164,14 +164,17 @@ bool smoothing_on(const ow3d_params& p) {
 
 // Deck features that change the physics but lie outside this library's path:
 // a deck that turns one on is refused (OW3D_ERR_UNSUPPORTED) rather than run
-// without it. IncWaveType 4 and 5 add a
-// constant-flux current to the wave (ReadInputFileParameters.f90:42-49),
-// which enters the right-hand side and the lateral Neumann rows.
+// without it. IncWaveType 3 and 5 generate waves by a boundary flux read from
+// a paddle-signal file (waveGenerationFromPaddleSignal.f90), 5 with a
+// constant-flux current (ReadInputFileParameters.f90:42-49); a raw 4 is the
+// deck's code for what the parser stores as 1 plus current_flag.
 int check_supported(const ow3d_params& p, std::string* err) {
     auto no = [&](const char* m) { if (err) *err = m; return OW3D_ERR_UNSUPPORTED; };
     if (p.IncWaveType == 3) return no("IncWaveType 3 (flux wave generation at the boundary) is not built");
-    if (p.IncWaveType == 4 || p.IncWaveType == 5)
-        return no("IncWaveType 4 and 5 (a wave with a constant-flux current) are not built");
+    if (p.IncWaveType == 4)
+        return no("IncWaveType 4: give IncWaveType 1 with current_flag = 1, as ow3d_read_deck reads it");
+    if (p.IncWaveType == 5)
+        return no("IncWaveType 5 (the flux wavemaker with a constant-flux current) is not built");
     if (p.PDampingONOFF != 0) {
         // BuildPDampMatrices.f90:37-40 stops for Ny > 1; the friction form
         // (type != 0) spreads its gamma over y lines inconsistently there
@@ -206,6 +209,8 @@ int check_params(const ow3d_params& p, std::string* err) {
     if (p.precision != OW3D_PREC_FP64 && p.precision != OW3D_PREC_MIXED) return fail("precision must be 0 or 1");
     if (p.krylov != OW3D_KRYLOV_FGMRES && p.krylov != OW3D_KRYLOV_LGMRES) return fail("krylov must be 0 or 1");
     if (p.GMRESmaxiterations < 1) return fail("GMRESmaxiterations must be >= 1");
+    if (p.current_flag != 0 && p.current_Q != 0.0 && p.periodic_x != 0)
+        return fail("periodic_x: the constant-flux current enters through the walls");
     if (smoothing_on(p) && p.periodic_x != 0)
         return fail("periodic_x: local smoothing by the vertical acceleration is built for wall boundaries");
     if (breaking_on(p)) {
@@ -910,6 +915,7 @@ int default_params(ow3d_params* p) {
     std::memset(p->bathymetry_file, 0, sizeof p->bathymetry_file);
     p->accel_tol_fact = 1e30; p->i_breaking = 0; p->PDampingONOFF = 0; p->swenseONOFF = 0; p->curvilinearONOFF = 0;
     p->T_half = 0; p->phi_b = 0; p->phi_0 = 0; p->del_fac = 0; p->cel_fac = 0; p->gamma_break = 0;
+    p->current_flag = 0; p->current_Q = 0;
     return OW3D_OK;
 }
 
@@ -969,7 +975,12 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
     Record r = next();  // IC [IncWaveType [accel_tol_fact]]
     if (!r.num(0)) return fail("line 2: IC expected");
     p->IC = r.n(0);
-    p->IncWaveType = r.num(1) ? r.n(1) : 0;   // 4 and 5 kept as written: ow3d_create refuses them
+    p->IncWaveType = r.num(1) ? r.n(1) : 0;
+    // IncWaveType 4 is the stream-function wave on a constant-flux current
+    // (ReadInputFileParameters.f90:45-46); 5, the flux wavemaker with one, is
+    // kept as written (ow3d_create refuses it)
+    if (p->IncWaveType == 4) { p->IncWaveType = 1; p->current_flag = 1; }
+    if (p->IncWaveType == 5) p->current_flag = 1;
     if (r.num(2)) { p->accel_tol_fact = r.d(2); p->accel_from_deck = 1; }
     r = next();  // Lx Ly Lz Nx Ny Nz GridX GridY GridZ GhostGridX GhostGridY GhostGridZ
     if (r.nnum() < 12) return fail("line 3: 12 grid values expected");
@@ -1118,7 +1129,9 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
         Record q = next();  // curvilinearONOFF
         if (q.num(0)) p->curvilinearONOFF = q.n(0);
     }
-    if (p->IncWaveType == 2) {
+    if (p->IncWaveType == 3 || p->IncWaveType == 5) {
+        next();   // ramp time, order, paddle-signal file of the flux wavemaker (:579-589)
+    } else if (p->IncWaveType == 2) {
         Record q = next();
         if (q.nnum() < 1) return fail("incident-wave line expected for IncWaveType 2");
         p->ispec = q.n(0);
@@ -1137,6 +1150,15 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
         }
         if (p->seed >= 0) p->seed = -p->seed;     // :632-647
         if (p->seed2 >= 0) p->seed2 = -p->seed2;
+    }
+    if (p->current_flag) {
+        // the current's flux Q (:655-665); a line that does not read as a
+        // number turns the current off (Q = 0)
+        while (li < lines.size() && blank(li)) ++li;
+        if (li < lines.size()) {
+            Record q = next();
+            p->current_Q = q.num(0) ? q.d(0) : 0.0;
+        }
     }
     return OW3D_OK;
 }

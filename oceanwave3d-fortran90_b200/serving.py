@@ -12,7 +12,10 @@ happens inside a step) and launches a simulation's next step as soon as its
 previous one completes, so the simulations' kernels overlap on the GPU. In a
 round, a simulation takes as many steps as fit in the longest single step of
 the round (from the step times measured in the previous round), so small
-simulations are not held back by large ones. A request is admitted as soon as it has arrived, a slot is
+simulations are not held back by large ones. Each simulation's coarse
+multigrid levels run in one thread-block cluster (ow3d_set_coarse_cluster)
+rather than a cooperative grid over every SM, so that the coarse cycles of
+the simulations overlap too. A request is admitted as soon as it has arrived, a slot is
 free and its estimated device memory (ow3d_estimate_bytes) fits in what the
 running simulations leave of the memory budget; finished simulations release
 their handle (and memory) at the end of the round in which they finish.
@@ -119,10 +122,15 @@ def request_case(req, precision=capi.PREC_MIXED, dx=0.1, Hs=0.02, Tp=1.5, gamma=
 class DeviceBackend:
     """The device calls the server makes, through the C ABI."""
 
-    def __init__(self, pkg, precision=capi.PREC_MIXED):
+    def __init__(self, pkg, precision=capi.PREC_MIXED, coarse_cluster=False):
+        """coarse_cluster: each simulation's coarse multigrid levels run in
+        one thread-block cluster (ow3d_set_coarse_cluster), so that the
+        coarse cycles of simulations stepped together overlap; for batched
+        serving, not for one simulation at a time."""
         self.pkg = pkg
         self.lib = pkg.lib()
         self.precision = precision
+        self.coarse_cluster = coarse_cluster
 
     def estimate_bytes(self, req):
         p = capi.default_params(Nx=req.Nx, Ny=req.Ny, Nz=req.Nz, precision=self.precision)
@@ -135,6 +143,10 @@ class DeviceBackend:
     def create(self, req):
         p, geo, eta, phis = request_case(req, precision=self.precision)
         sim = self.pkg.Simulation(p, **geo)
+        if self.coarse_cluster:
+            st = self.lib.ow3d_set_coarse_cluster(sim.h, 1)
+            if st != 0:
+                raise self.pkg.OW3DError(st, "ow3d_set_coarse_cluster")
         sim.set_state(eta, phis)
         return sim
 

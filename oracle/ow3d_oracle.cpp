@@ -76,6 +76,7 @@ struct Sim {
     vector<double> fc, fc2;              // filter: centre (NP) and boundary view (NP*alpha)
     int NP = 0;
     // the roller breaking model of x flumes (DetectBreaking.f90)
+    double Ul = 0, Ur = 0;               // constant-flux current at the west and east walls
     int brk = 0;                         // i_breaking > 0 and Ny == 1
     double tan_b = 0, tan_0 = 0;         // tan(phi_b), tan(phi_0)
     vector<double> tan_phi, Qr_x;        // per column: roller angle state, roller flux slope
@@ -1545,9 +1546,9 @@ static int rk4_step(Sim& s) {
         const int Nz = s.Nzg;
         for (int j = 1 + s.gy; j <= s.Nyg - s.gy; ++j)
             for (int i = 1 + s.gx; i <= s.Nxg - s.gx; ++i) s.RHS[gid(s, Nz, i, j)] = Pf[(size_t)(i - 1) + (size_t)s.Nxg * (j - 1)];
-        if (s.gx == 1)
+        if (s.gx == 1)   // Runge_Kutta_4.f90:108-113: Uneumann (zero) + the current
             for (int j = 1 + s.gy; j <= s.Nyg - s.gy; ++j)
-                for (int k = 1; k <= Nz; ++k) { s.RHS[gid(s, k, 1, j)] = 0.0; s.RHS[gid(s, k, s.Nxg, j)] = 0.0; }
+                for (int k = 1; k <= Nz; ++k) { s.RHS[gid(s, k, 1, j)] = s.Ul; s.RHS[gid(s, k, s.Nxg, j)] = s.Ur; }
         if (s.per) zero_images_x(s, s.RHS.data(), Nz);   // identity rows of the image columns
     };
     auto sigma_for = [&](const vector<double>& E, const vector<double>& Ex, const vector<double>& Exx,
@@ -1559,7 +1560,16 @@ static int rk4_step(Sim& s) {
         int st = solve(s, s.RHS.data(), s.PHI.data(), it, res);
         if (st == OW3D_NOT_CONVERGED) status = OW3D_NOT_CONVERGED;
     };
-    auto zero_src = [&]() { std::fill(s.sPx.begin(), s.sPx.end(), 0.0); };
+    // Runge_Kutta_4.f90:82-88: the ghost source of the surface potential, zero
+    // plus the constant-flux current at the west and east boundary columns
+    auto zero_src = [&]() {
+        std::fill(s.sPx.begin(), s.sPx.end(), 0.0);
+        if (s.gx == 1)
+            for (int j = 1; j <= s.Nyg; ++j) {
+                s.sPx[(size_t)(1 + s.gx - 1) + (size_t)s.Nxg * (j - 1)] += s.Ul;
+                s.sPx[(size_t)(s.p.Nx + s.gx - 1) + (size_t)s.Nxg * (j - 1)] += s.Ur;
+            }
+    };
     auto breaking = [&](const vector<double>& Ef) { if (s.brk && s.p.i_breaking == 1) detect_breaking(s, Ef, false); };
     // stage 1
     pressure_term(s, s.E, s.P, time);
@@ -1673,6 +1683,8 @@ static Sim* create(const ow3d_params* p, const double* h, const double* hx, cons
     if (p->filteringONOFF > 0) filter_init(*s);
     setup_zones(*s);
     setup_pdamp(*s);
+    // OceanWave3DT0Setup.f90:325-326
+    if (p->current_flag) { s->Ul = p->current_Q / G.h[0]; s->Ur = p->current_Q / G.h[(size_t)s->Nxg - 2]; }
     // DetectBreaking.f90:38-70 (the first call): tan(phi) starts at tan(phi_b); Initialize.f90:7-8
     // local smoothing on for limits up to 100 g (LocalSmoothing2D.f90:37): any
     // value a deck gives, or a positive one set by a caller
@@ -1756,6 +1768,7 @@ void orc_set_state(void* sv, const double* E, const double* P, const double* W, 
     if (s->per) { zero_images_x(*s, s->PHI.data(), s->Nzg); if (W) images_x(*s, s->W.data(), 1); }
     std::fill(s->LASTPHI0.begin(), s->LASTPHI0.end(), 0.0); std::fill(s->LASTPHI1.begin(), s->LASTPHI1.end(), 0.0);
     s->time = t; s->tstep = 0;
+    std::fill(s->sPx.begin(), s->sPx.end(), 0.0);   // the set-up's source is zero
     // OceanWave3DT0Setup.f90:444,564-569: surface derivatives; linear case keeps eta = 0 coefficients.
     fs_derivs(*s, s->E, s->P, s->Ex, s->Exx, s->Px, s->Ey, s->Eyy, s->Py);
     update_sigma(*s, nullptr, nullptr, nullptr, nullptr, nullptr);

@@ -173,15 +173,18 @@ def test_decks_needing_unbuilt_features_are_refused(ow3d, tmp_path):
         "pressure": base.replace("0 0\n0 2.0 2", "1 1\n0. 5. 0. 10. 0.1 0.1 0\n0 2.0 2"),
         "SWENSE": base.replace("0 2.0 2 0 0 1 0", "1 2.0 2 0 0 1 0"),
         "IncWaveType 3": base.replace("-1 0  ", "-1 3  "),
-        # a stream-function or flux wave with a constant-flux current (ReadInputFileParameters.f90:42-49)
-        "IncWaveType 4": base.replace("-1 0  ", "-1 4  "),
+        # the flux wavemaker with a constant-flux current (ReadInputFileParameters.f90:42-49)
         "IncWaveType 5": base.replace("-1 0  ", "-1 5  "),
     }
     for what, text in cases_.items():
         st, p = status(text)
         assert st == ow3d.capi.ERR_UNSUPPORTED, (what, st)
     msg = L.ow3d_last_error().decode()
-    assert "IncWaveType 4 and 5" in msg
+    assert "IncWaveType 5" in msg
+    # IncWaveType 4, the stream-function wave on a current, is read as 1 with
+    # the current flag (tests/test_current.py)
+    st, p = status(base.replace("-1 0  ", "-1 4  "))
+    assert st == 0 and (p.IncWaveType, p.current_flag) == (1, 1)
     st, p = status(base.replace("-1 0  ", "-1 0 1000. "))
     assert st == 0 and p.accel_from_deck == 1
     # the breaking model acts on x flumes only (Runge_Kutta_4.f90:55): a 3-D

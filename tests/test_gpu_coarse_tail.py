@@ -49,3 +49,23 @@ def test_tail_cluster_is_bitwise_the_grid_cycle(ow3d, case, prec):
         got = _run(ow3d, make, tail, cluster)    # 1 << 40: the whole fused cycle in the cluster
         for a, b in zip(got[:4], ref[:4]):
             assert np.array_equal(a, b), (tail, cluster)
+
+
+def test_coarse_cluster_mode_per_handle(ow3d):
+    """ow3d_set_coarse_cluster: the whole fused coarse cycle of one handle in
+    a cluster, switched on and off between steps (the captured graphs are
+    dropped and captured again), bitwise the grid cycle throughout."""
+    make = _sea(ow3d, 0)
+    runs = []
+    for schedule in ((0, 0, 0), (1, 1, 1), (1, 0, 1)):
+        p, geo, E0, P0 = make()
+        sim = ow3d.Simulation(p, **geo)
+        sim.set_state(E0, P0)
+        for on in schedule:
+            assert ow3d.lib().ow3d_set_coarse_cluster(sim.h, on) == 0
+            sim.step(2)
+        runs.append(sim.get_state())
+        sim.close()
+    for got in runs[1:]:
+        for a, b in zip(got[:4], runs[0][:4]):
+            assert np.array_equal(a, b)
