@@ -83,8 +83,7 @@ typedef struct ow3d_zone {
 typedef struct ow3d_params {
     /* line 2 */
     int    IC, IncWaveType;       /* ow3d_read_deck reads 4 as 1 with current_flag = 1
-                                     (see current_Q); 3 and 5 (the flux wavemaker, alone
-                                     or with a current) are refused by ow3d_create */
+                                     (see current_Q) and 5 as 3 with current_flag = 1 */
     /* line 3 */
     double Lx, Ly, Lz;
     int    Nx, Ny, Nz;
@@ -199,6 +198,13 @@ typedef struct ow3d_params {
      * potential's ghost points the same flux (:85-88). */
     int    current_flag;
     double current_Q;                 /* m^2/s */
+    /* the flux wavemaker of IncWaveType 3 (and 5): the deck line after the
+     * curvilinear line (ReadInputFileParameters.f90:579-589). The paddle
+     * signal itself is read with ow3d_read_paddle_signal and installed with
+     * ow3d_set_paddle_signal before the first step. */
+    double flux_ramp;                 /* ramp time of the boundary flux, s */
+    int    flux_order;                /* points of the interpolation in y (1..10) */
+    char   flux_file[256];            /* paddle-signal file named by the deck */
 } ow3d_params;
 
 typedef struct ow3d_handle ow3d_handle;
@@ -411,6 +417,26 @@ int ow3d_set_relax_target(ow3d_handle* h, int zone, int mode, int nt,
  * OceanWave3DTakeATimeStep.f90:27. Returns OW3D_ERR_UNSTABLE on the
  * reference's instability test; OW3D_NOT_CONVERGED if any solve hit the limit. */
 int ow3d_step(ow3d_handle* h, int nsteps);
+
+/* The paddle-signal file of the flux wavemaker (setupWavePaddle.f90:43-67): a
+ * header line, `dt nt n2`, the n2 y positions of the signal points, then nt
+ * records `time flux(1..n2)`. Call with y = flux = NULL (or cap too small)
+ * to get dt, nt and n2; then with y (n2) and flux (nt * n2, time-major) of
+ * at least cap = nt * n2 values. Host-only. */
+int ow3d_read_paddle_signal(const char* path, int cap, double* dt, int* nt, int* n2, double* y, double* flux);
+
+/* Install the flux wavemaker's signal on a handle of IncWaveType 3 (or 5):
+ * the boundary flux u(t, y) at the n2 points y (uniformly spaced from dy/2)
+ * every dt, and eta_x = -u_t / g from its 5-point time derivative
+ * (setupWavePaddle.f90:89-122). Each RK stage then imposes, on the west
+ * wall, the flux ramped over flux_ramp and interpolated linearly in time and
+ * with flux_order points in y (waveGenerationFromPaddleSignal.f90:43-111):
+ * in the Neumann rows of every level above the bottom, and in the ghost
+ * points of the surface potential and elevation at the end of each step.
+ * Replaces: setupWavePaddle. Required before the first ow3d_step of such a
+ * handle; OW3D_ERR_BAD_INPUT for unevenly spaced points or a signal shorter
+ * than Nsteps * dt. */
+int ow3d_set_paddle_signal(ow3d_handle* h, int nt, int n2, double dt, const double* y, const double* flux);
 
 /* on = 1: the coarse levels of every V-cycle run in one thread-block
  * cluster of 16 SMs (8 where 16 cannot be resident) instead of a cooperative

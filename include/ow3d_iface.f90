@@ -38,7 +38,7 @@ MODULE ow3d_iface
   ! ow3d_params mirrors the deck (include/ow3d.h); filled by ow3d_read_deck
   ! and opaque to Fortran
   TYPE, BIND(C) :: ow3d_params_t
-     INTEGER(c_int8_t) :: raw(2208)         ! opaque to Fortran: sizeof(ow3d_params)
+     INTEGER(c_int8_t) :: raw(2480)         ! opaque to Fortran: sizeof(ow3d_params)
   END TYPE
 
   INTERFACE
@@ -142,6 +142,28 @@ MODULE ow3d_iface
        INTEGER(c_int), INTENT(OUT) :: n_rollers
        INTEGER(c_int), DIMENSION(*), INTENT(OUT) :: npts, toe
        REAL(c_double), DIMENSION(*), INTENT(OUT) :: x, eta, thickness, tan_phi
+     END FUNCTION
+
+     ! the flux wavemaker's paddle-signal file (setupWavePaddle): call with
+     ! cap = 0 for dt, nt, n2, then with y(n2) and flux(n2, nt) (time-major in C)
+     INTEGER(c_int) FUNCTION ow3d_read_paddle_signal(path, cap, dt, nt, n2, y, flux) &
+          BIND(C, name="ow3d_read_paddle_signal")
+       IMPORT :: c_int, c_double, c_char
+       CHARACTER(kind=c_char), DIMENSION(*), INTENT(IN) :: path
+       INTEGER(c_int), VALUE :: cap
+       REAL(c_double), INTENT(OUT) :: dt
+       INTEGER(c_int), INTENT(OUT) :: nt, n2
+       REAL(c_double), DIMENSION(*), INTENT(OUT) :: y, flux
+     END FUNCTION
+
+     ! install it on a handle of IncWaveType 3 (or 5) before the first step
+     INTEGER(c_int) FUNCTION ow3d_set_paddle_signal(handle, nt, n2, dt, y, flux) &
+          BIND(C, name="ow3d_set_paddle_signal")
+       IMPORT :: c_int, c_double, c_ptr
+       TYPE(c_ptr), VALUE :: handle
+       INTEGER(c_int), VALUE :: nt, n2
+       REAL(c_double), VALUE :: dt
+       REAL(c_double), DIMENSION(*), INTENT(IN) :: y, flux
      END FUNCTION
 
      ! the reference's output schedule (StoreDataONOFF of the deck): EP_#####.bin

@@ -136,6 +136,18 @@ def stream_function_wave(params, x, t=0.0):
     return eta, phis, tuple(info)
 
 
+def read_paddle_signal(path):
+    """The flux wavemaker's paddle-signal file (ow3d_read_paddle_signal):
+    (dt, y (n2,), flux (nt, n2))."""
+    dt, nt, n2 = _C.c_double(), _C.c_int(), _C.c_int()
+    _check(lib().ow3d_read_paddle_signal(_b(path), 0, _C.byref(dt), _C.byref(nt), _C.byref(n2), None, None),
+           "ow3d_read_paddle_signal")
+    y, flux = _np.zeros(n2.value), _np.zeros(nt.value * n2.value)
+    _check(lib().ow3d_read_paddle_signal(_b(path), flux.size, _C.byref(dt), _C.byref(nt), _C.byref(n2), _d(y),
+                                         _d(flux)), "ow3d_read_paddle_signal")
+    return dt.value, y, flux.reshape(nt.value, n2.value)
+
+
 def incident_wave(params, zone, nt=None):
     """The incident wave of IncWaveType 2 on generation zone `zone` (0-based):
     eta and surface phi as (nt, rows, columns) arrays every dt (nt defaults
@@ -331,6 +343,15 @@ class Simulation:
         e, f = _np.zeros(nt * box), _np.zeros(nt * box)
         _check(lib().ow3d_test_relax_target(self.h, zone, _d(e), _d(f)), "ow3d_test_relax_target")
         return e.reshape(nt, box), f.reshape(nt, box)
+
+    def set_paddle_signal(self, dt, y, flux):
+        """Install the flux wavemaker's signal: flux (nt, n2) at y every dt
+        (ow3d_set_paddle_signal)."""
+        y = _f64(y).ravel()
+        flux = _np.ascontiguousarray(flux, dtype=_np.float64)
+        nt, n2 = flux.shape
+        _check(lib().ow3d_set_paddle_signal(self.h, nt, n2, float(dt), _d(y), _d(flux.ravel())),
+               "ow3d_set_paddle_signal")
 
     def rollers(self):
         """The roller breaking model's rollers after the last step (ow3d_rollers):

@@ -76,6 +76,7 @@ class Params(C.Structure):
         ("T_half", C.c_double), ("phi_b", C.c_double), ("phi_0", C.c_double),
         ("del_fac", C.c_double), ("cel_fac", C.c_double), ("gamma_break", C.c_double),
         ("current_flag", C.c_int), ("current_Q", C.c_double),
+        ("flux_ramp", C.c_double), ("flux_order", C.c_int), ("flux_file", C.c_char * 256),
     ]
 
 
@@ -116,6 +117,7 @@ def default_params(**kw):
     p.ispec = -1; p.gamma_jonswap = 3.3; p.s0 = 1.0
     p.sf_nsteps = 1
     p.accel_tol_fact = 1e30
+    p.flux_order = 1
     for k, v in kw.items():
         if k == "zones":
             for i, z in enumerate(v):
@@ -177,6 +179,8 @@ def declare(lib):
         "ow3d_reset_stats": (C.c_int, [H]),
         "ow3d_set_graphs": (C.c_int, [H, C.c_int]),
         "ow3d_set_coarse_cluster": (C.c_int, [H, C.c_int]),
+        "ow3d_read_paddle_signal": (C.c_int, [C.c_char_p, C.c_int, _D, _I, _I, _D, _D]),
+        "ow3d_set_paddle_signal": (C.c_int, [H, C.c_int, C.c_int, C.c_double, _D, _D]),
         "ow3d_zone_box": (C.c_int, [H, C.c_int, _I, _I, _I, _I]),
         "ow3d_strerror": (C.c_char_p, [C.c_int]),
         "ow3d_version": (C.c_char_p, []),

@@ -206,7 +206,13 @@ __global__ void k_ghost_x(FsArgs a, double* v1, double* v2, int src) {
             double* r = vs[q] + (int64_t)Nx * (j - 1);
             const double* s0 = a.SX + (int64_t)(2 - 1) * kHoRank;          // stencil of point i = 2
             const double* s1 = a.SX + (int64_t)(Nx - 1 - 1) * kHoRank;     // stencil of point i = Nx-1
-            const double sw = (q == 1 && src) ? a.Ul : 0.0, se = (q == 1 && src) ? a.Ur : 0.0;
+            double sw = 0.0, se = 0.0;
+            if (q == 1 && src) {
+                sw = (src == 2 && a.Uw) ? a.Uw[j - 1] + a.Ul : a.Ul;
+                se = a.Ur;
+            } else if (q == 0 && src == 2 && a.Es) {
+                sw = a.Es[j - 1];
+            }
             double acc = 0;
             for (int m = 1; m < kHoRank; ++m) acc += s0[m] * r[m];
             r[0] = (sw - acc) / s0[0];
@@ -308,8 +314,15 @@ __global__ void k_set_rhs(FsArgs a, const double* __restrict__ P, double* __rest
         const int i = (int)(p % a.Nxg), j = (int)(p / a.Nxg);
         const bool yghost = a.three && (j == 0 || j == a.Nyg - 1);
         if (!a.per && !yghost && (i == 0 || i == a.Nxg - 1)) {
-            const double u = i == 0 ? a.Ul : a.Ur;
-            for (int k = 0; k < a.Nzg; ++k) rhs[p * a.Nzg + k] = u;
+            if (i == 0 && a.Uw) {
+                // Uneumann (zero in the bottom row, FAC u above) + the current
+                rhs[p * a.Nzg] = 0.0 + a.Ul;
+                const double u = a.Uw[j] + a.Ul;
+                for (int k = 1; k < a.Nzg; ++k) rhs[p * a.Nzg + k] = u;
+            } else {
+                const double u = i == 0 ? a.Ul : a.Ur;
+                for (int k = 0; k < a.Nzg; ++k) rhs[p * a.Nzg + k] = u;
+            }
             continue;
         }
         const bool ghost = i == 0 || i == a.Nxg - 1 || yghost;
@@ -411,6 +424,29 @@ __global__ void k_filter_y(FsArgs a, FilterDev f, const double* __restrict__ src
     }
 }
 
+// waveGenerationFromPaddleSignal.f90:43-111 at RK time t = (device time) +
+// off: the signal levels itime and itime + 1 around t (1-based, itime =
+// floor(t / dt) + 1; kept inside the table, where the reference would read
+// past its end), their linear weights, the cubic ramp over the first `ramp`
+// seconds, and per interior row the west wall's flux FAC u and eta_x.
+__global__ void k_paddle(PaddleDev d, const StepDev* sd, double off) {
+    const double t = sd->time + off;
+    int it = (int)floor(t / d.dt) + 1;
+    if (it < 1) it = 1;
+    if (it > d.nt - 1) it = d.nt - 1;
+    const double dl1 = t - (it - 1) * d.dt, dl2 = it * d.dt - t;
+    const double w1 = dl2 / (dl1 + dl2), w2 = dl1 / (dl1 + dl2);
+    double fac = 1.0;
+    if (t < d.ramp) fac = -2.0 / (d.ramp * d.ramp * d.ramp) * (t * t * t) + 3.0 / (d.ramp * d.ramp) * (t * t);
+    for (int j = d.j0 + (int)(blockIdx.x * blockDim.x + threadIdx.x); j <= d.j1; j += gridDim.x * blockDim.x) {
+        const int64_t r0 = (int64_t)(it - 1) * d.Nyg + (j - 1), r1 = (int64_t)it * d.Nyg + (j - 1);
+        const double flux = w1 * d.F[r0] + w2 * d.F[r1];
+        const double etax = w1 * d.X[r0] + w2 * d.X[r1];
+        d.Uw[j - 1] = fac * flux;
+        d.Es[j - 1] = etax;
+    }
+}
+
 __global__ void k_step_begin(StepDev* sd) {
     if (blockIdx.x == 0 && threadIdx.x == 0) sd->tstep += 1;
 }
@@ -460,6 +496,9 @@ void fs_relax(const FsArgs& a, const RelaxZoneDev* zones, int nz, double* E, dou
 }
 void fs_step_begin(StepDev* sd, cudaStream_t st) { note_launch(), k_step_begin<<<1, 32, 0, st>>>(sd); }
 void fs_step_end(StepDev* sd, double dt, cudaStream_t st) { note_launch(), k_step_end<<<1, 32, 0, st>>>(sd, dt); }
+void fs_paddle(const PaddleDev& d, const StepDev* sd, double off, cudaStream_t st) {
+    note_launch(), k_paddle<<<nb(d.j1 - d.j0 + 1, 128), 128, 0, st>>>(d, sd, off);
+}
 void fs_derivs(const FsArgs& a, double* E, double* P, double* Ex, double* Exx, double* Px, double* Ey, double* Eyy,
                double* Py, int src, cudaStream_t st) {
     int64_t C = (int64_t)a.Nxg * a.Nyg;

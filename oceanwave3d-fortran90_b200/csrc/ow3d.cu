@@ -99,6 +99,10 @@ struct ow3d_handle {
     // local smoothing by the vertical acceleration (accel_tol_fact <= 100)
     SmoothDev sm{};
     bool sm_on = false;
+    // the flux wavemaker (IncWaveType 3): its signal tables, installed by
+    // ow3d_set_paddle_signal before the first step
+    PaddleDev pad{};
+    bool pad_on = false, pad_set = false;
     int* flag = nullptr;
     int* flag_host = nullptr;
     double hmax = 0;
@@ -742,6 +746,15 @@ int create_impl(const ow3d_params* p, const double* h, const double* hx, const d
         H->pd_h.L.clear(); H->pd_h.L.shrink_to_fit(); H->pd_h.Linv.clear(); H->pd_h.Linv.shrink_to_fit();
         H->pd_on = true;
     }
+    if (p->IncWaveType == 3) {
+        PaddleDev& d = H->pad;
+        d.Nyg = G.Nyg; d.j0 = 1 + G.gy; d.j1 = G.Ny + G.gy; d.ramp = p->flux_ramp;
+        TRY(dalloc(H.get(), &d.Uw, (size_t)G.Nyg)); TRY(dalloc(H.get(), &d.Es, (size_t)G.Nyg));
+        CK(cudaMemset(d.Uw, 0, sizeof(double) * (size_t)G.Nyg));
+        CK(cudaMemset(d.Es, 0, sizeof(double) * (size_t)G.Nyg));
+        H->fa.Uw = d.Uw; H->fa.Es = d.Es;
+        H->pad_on = true;
+    }
     if (smoothing_on(*p)) {
         SmoothDev& m = H->sm;
         m.tol = p->accel_tol_fact * p->g;
@@ -830,6 +843,10 @@ int stage_surface(ow3d_handle* H, const double* E, const double* Ex, const doubl
 // memory at its end.
 template <typename SolveF>
 int enqueue_step(ow3d_handle* H, int64_t tstep, bool graph, SolveF&& solve) {
+    if (H->pad_on && !H->pad_set) {
+        g_last_error = "IncWaveType 3: install the paddle signal (ow3d_set_paddle_signal) before stepping";
+        return OW3D_ERR_BAD_INPUT;
+    }
     cudaStream_t st = H->st;
     const double dt = H->p.dt, half = 0.5, time = H->time;
     const int64_t N = H->G.N;
@@ -842,8 +859,13 @@ int enqueue_step(ow3d_handle* H, int64_t tstep, bool graph, SolveF&& solve) {
         if (H->p.relaxONOFF == 1)
             fs_relax(fa, H->zones.data(), (int)H->zones.size(), E, P, H->sd, off, H->p.relaxTransientTime, st);
     };
-    auto derivs = [&](double* E, double* P, double* Ex, double* Exx, double* Px, double* Ey, double* Eyy, double* Py) {
-        fs_derivs(fa, E, P, Ex, Exx, Px, Ey, Eyy, Py, 1, st);
+    auto derivs = [&](double* E, double* P, double* Ex, double* Exx, double* Px, double* Ey, double* Eyy, double* Py,
+                      int src) { fs_derivs(fa, E, P, Ex, Exx, Px, Ey, Eyy, Py, src, st); };
+    // waveGenerationFromPaddleSignal at RK time (step start) + off: stages 1
+    // and 3 (Runge_Kutta_4.f90:83-85,264-266); the last stage's call, at the
+    // same time as stage 3's, gives the same values
+    auto paddle = [&](double off) {
+        if (H->pad_on) fs_paddle(H->pad, H->sd, off, st);
     };
     const bool nl = H->p.LinearONOFF == 1;
     auto surf = [&](const double* E, const double* Ex, const double* Exx, const double* Ey, const double* Eyy) {
@@ -872,7 +894,8 @@ int enqueue_step(ow3d_handle* H, int64_t tstep, bool graph, SolveF&& solve) {
     fs_stage(fa, H->E, H->P, H->W, H->Ex, H->Px, H->Ey, H->Py, H->E, H->P, half * dt, H->kE[0], H->kP[0], H->tE, H->tP,
              NuD, Pd, Qr, st);
     relax(H->tE, H->tP, half * dt);
-    derivs(H->tE, H->tP, H->tEx, H->tExx, H->tPx, H->tEy, H->tEyy, H->tPy);
+    paddle(half * dt);
+    derivs(H->tE, H->tP, H->tEx, H->tExx, H->tPx, H->tEy, H->tEyy, H->tPy, 1);
     fs_set_rhs(fa, H->tP, H->RHS, st);
     if (H->p.extrapolationONOFF == 1) fs_extrap(H->PHI, LPnew, LPlast, N, 0, H->sd, st);
     TRY(solve(surf(H->tE, H->tEx, H->tExx, H->tEy, H->tEyy), 0));
@@ -883,7 +906,7 @@ int enqueue_step(ow3d_handle* H, int64_t tstep, bool graph, SolveF&& solve) {
     fs_stage(fa, H->tE, H->tP, H->tW, H->tEx, H->tPx, H->tEy, H->tPy, H->E, H->P, half * dt, H->kE[1], H->kP[1], H->tE,
              H->tP, NuD, Pd, Qr, st);
     relax(H->tE, H->tP, half * dt);
-    derivs(H->tE, H->tP, H->tEx, H->tExx, H->tPx, H->tEy, H->tEyy, H->tPy);
+    derivs(H->tE, H->tP, H->tEx, H->tExx, H->tPx, H->tEy, H->tEyy, H->tPy, 1);
     fs_set_rhs(fa, H->tP, H->RHS, st);
     TRY(solve(surf(H->tE, H->tEx, H->tExx, H->tEy, H->tEyy), 1));
     fs_wvel(fa, H->PHI, H->tE, H->tW, st);
@@ -893,7 +916,8 @@ int enqueue_step(ow3d_handle* H, int64_t tstep, bool graph, SolveF&& solve) {
     fs_stage(fa, H->tE, H->tP, H->tW, H->tEx, H->tPx, H->tEy, H->tPy, H->E, H->P, dt, H->kE[2], H->kP[2], H->tE, H->tP,
              NuD, Pd, Qr, st);
     relax(H->tE, H->tP, dt);
-    derivs(H->tE, H->tP, H->tEx, H->tExx, H->tPx, H->tEy, H->tEyy, H->tPy);
+    paddle(dt);
+    derivs(H->tE, H->tP, H->tEx, H->tExx, H->tPx, H->tEy, H->tEyy, H->tPy, 1);
     fs_set_rhs(fa, H->tP, H->RHS, st);
     // Runge_Kutta_4.f90:294-303, from the second step on (checked on the device)
     if (H->p.extrapolationONOFF == 1) fs_extrap(H->PHI, LPnew, LPlast, N, 1, H->sd, st);
@@ -912,7 +936,7 @@ int enqueue_step(ow3d_handle* H, int64_t tstep, bool graph, SolveF&& solve) {
         fs_filter(fa, f, H->P, H->ftmp, H->sd, H->p.filteringONOFF, st);
     }
     relax(H->E, H->P, dt);
-    derivs(H->E, H->P, H->Ex, H->Exx, H->Px, H->Ey, H->Eyy, H->Py);
+    derivs(H->E, H->P, H->Ex, H->Exx, H->Px, H->Ey, H->Eyy, H->Py, 2);
     fs_set_rhs(fa, H->P, H->RHS, st);
     TRY(solve(surf(H->E, H->Ex, H->Exx, H->Ey, H->Eyy), 3));
     fs_wvel(fa, H->PHI, H->E, H->W, st);
@@ -1409,8 +1433,9 @@ int ow3d_put_surface(ow3d_handle* H, const double* E, const double* P) {
     const size_t cb = sizeof(double) * (size_t)H->G.C;
     CK(cudaMemcpyAsync(H->E, E, cb, cudaMemcpyHostToDevice, H->st));
     CK(cudaMemcpyAsync(H->P, P, cb, cudaMemcpyHostToDevice, H->st));
-    // after a step the surface potential's ghost source holds the current's flux
-    fs_derivs(H->fa, H->E, H->P, H->Ex, H->Exx, H->Px, H->Ey, H->Eyy, H->Py, H->tstep > 0 ? 1 : 0, H->st);
+    // after a step the ghost sources hold the current's flux and the
+    // wavemaker's values of the step's end
+    fs_derivs(H->fa, H->E, H->P, H->Ex, H->Exx, H->Px, H->Ey, H->Eyy, H->Py, H->tstep > 0 ? 2 : 0, H->st);
     CK(cudaGetLastError());
     return OW3D_OK;
 }
@@ -1999,6 +2024,47 @@ int ow3d_reset_stats(ow3d_handle* H) {
     std::memset(&H->stats, 0, sizeof(H->stats));
     H->stats.time = t;
     H->stats.tstep = ts;
+    return OW3D_OK;
+}
+
+int ow3d_read_paddle_signal(const char* path, int cap, double* dt, int* nt, int* n2, double* y, double* flux) {
+    PaddleSignal ps;
+    std::string err;
+    if (int r = read_paddle_signal(path, ps, &err)) { g_last_error = err; return r; }
+    if (dt) *dt = ps.dt;
+    if (nt) *nt = ps.nt;
+    if (n2) *n2 = ps.n2;
+    if (y && flux && cap >= ps.nt * ps.n2) {
+        std::copy(ps.y.begin(), ps.y.end(), y);
+        std::copy(ps.flux.begin(), ps.flux.end(), flux);
+    }
+    return OW3D_OK;
+}
+
+int ow3d_set_paddle_signal(ow3d_handle* H, int nt, int n2, double dt, const double* y, const double* flux) {
+    if (!H || !y || !flux || nt < 5 || n2 < 1 || !(dt > 0)) {
+        g_last_error = "ow3d_set_paddle_signal: bad arguments";
+        return OW3D_ERR_BAD_INPUT;
+    }
+    if (!H->pad_on) {
+        g_last_error = "ow3d_set_paddle_signal: the handle's IncWaveType is not 3";
+        return OW3D_ERR_BAD_INPUT;
+    }
+    PaddleSignal ps;
+    ps.dt = dt; ps.nt = nt; ps.n2 = n2;
+    ps.y.assign(y, y + n2);
+    ps.flux.assign(flux, flux + (size_t)nt * n2);
+    std::vector<double> F, X;
+    std::string err;
+    if (int r = paddle_tables(H->p, H->G, ps, F, X, &err)) { g_last_error = err; return r; }
+    CK(cudaSetDevice(H->dev));
+    CK(cudaStreamSynchronize(H->st));
+    double *dF, *dX;
+    TRY(upload(H, &dF, F));
+    TRY(upload(H, &dX, X));
+    H->pad.F = dF; H->pad.X = dX; H->pad.nt = nt; H->pad.dt = dt;
+    H->pad_set = true;
+    drop_step_graphs(H);   // captured wavemaker launches hold the old table
     return OW3D_OK;
 }
 

@@ -16,7 +16,21 @@ struct FsArgs {
     // the constant-flux current (IncWaveType 4): u = Q/h at the west and east
     // walls (OceanWave3DT0Setup.f90:325-326), 0 without one
     double Ul, Ur;
+    // the flux wavemaker (IncWaveType 3): per row, the west wall's flux
+    // FAC u (Uneumann) and eta_x source of the last k_paddle; null without one
+    const double* Uw;
+    const double* Es;
 };
+
+// The flux wavemaker's signal on the device (waveGenerationFromPaddleSignal.f90).
+struct PaddleDev {
+    int nt, Nyg, j0, j1;     // time levels; rows; interior rows j0..j1 (1-based)
+    double dt, ramp;
+    const double* F;         // nt x Nyg: the flux interpolated onto the rows
+    const double* X;         // nt x Nyg: eta_x = -u_t / g likewise
+    double *Uw, *Es;         // Nyg each: the values at the last RK time
+};
+
 
 // The time level on the device: the simulation time at the start of the
 // current step and the step number (1 for the first step). The kernels whose
@@ -26,6 +40,9 @@ struct StepDev {
     double time;
     long long tstep;
 };
+
+// The wavemaker's values at RK time (device time) + off.
+void fs_paddle(const PaddleDev& d, const StepDev* sd, double off, cudaStream_t st);
 
 // One relaxation zone on the device (PreprocessRelaxationZones.f90).
 struct RelaxZoneDev {
@@ -115,9 +132,12 @@ void fs_relax(const FsArgs& a, const RelaxZoneDev* zones, int nz, double* E, dou
 // Start of a step: tstep += 1. End of a step: time += dt.
 void fs_step_begin(StepDev* sd, cudaStream_t st);
 void fs_step_end(StepDev* sd, double dt, cudaStream_t st);
-// src: the surface potential's ghost points carry the current's flux (the
-// RK stages' sourcePx, Runge_Kutta_4.f90:85-88); 0 at set-up, where the
-// reference's source is still zero (OceanWave3DT0Setup.f90:444).
+// src: the ghost sources of the surface derivatives. 0 at set-up, where the
+// reference's sources are still zero (OceanWave3DT0Setup.f90:444); 1 in the
+// RK stages, whose fields carry the current's flux in the potential's source
+// (Runge_Kutta_4.f90:85-88); 2 at the end of a step, whose field also carries
+// the flux wavemaker's west-wall flux and eta_x (waveGenerationFromPaddleSignal.f90:
+// 107-110 writes them to the step's own field only).
 void fs_derivs(const FsArgs& a, double* E, double* P, double* Ex, double* Exx, double* Px, double* Ey, double* Eyy,
                double* Py, int src, cudaStream_t st);
 void fs_wvel(const FsArgs& a, const double* phi, const double* E, double* W, cudaStream_t st);

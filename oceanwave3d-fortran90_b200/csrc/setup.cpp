@@ -9,6 +9,7 @@
 #include <cmath>
 #include <complex>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <sstream>
@@ -164,17 +165,12 @@ bool smoothing_on(const ow3d_params& p) {
 
 // Deck features that change the physics but lie outside this library's path:
 // a deck that turns one on is refused (OW3D_ERR_UNSUPPORTED) rather than run
-// without it. IncWaveType 3 and 5 generate waves by a boundary flux read from
-// a paddle-signal file (waveGenerationFromPaddleSignal.f90), 5 with a
-// constant-flux current (ReadInputFileParameters.f90:42-49); a raw 4 is the
-// deck's code for what the parser stores as 1 plus current_flag.
+// without it. A raw IncWaveType 4 or 5 is the deck's code for what the parser
+// stores as 1 or 3 plus current_flag (ReadInputFileParameters.f90:42-49).
 int check_supported(const ow3d_params& p, std::string* err) {
     auto no = [&](const char* m) { if (err) *err = m; return OW3D_ERR_UNSUPPORTED; };
-    if (p.IncWaveType == 3) return no("IncWaveType 3 (flux wave generation at the boundary) is not built");
-    if (p.IncWaveType == 4)
-        return no("IncWaveType 4: give IncWaveType 1 with current_flag = 1, as ow3d_read_deck reads it");
-    if (p.IncWaveType == 5)
-        return no("IncWaveType 5 (the flux wavemaker with a constant-flux current) is not built");
+    if (p.IncWaveType == 4 || p.IncWaveType == 5)
+        return no("IncWaveType 4 / 5: give IncWaveType 1 / 3 with current_flag = 1, as ow3d_read_deck reads them");
     if (p.PDampingONOFF != 0) {
         // BuildPDampMatrices.f90:37-40 stops for Ny > 1; the friction form
         // (type != 0) spreads its gamma over y lines inconsistently there
@@ -209,6 +205,10 @@ int check_params(const ow3d_params& p, std::string* err) {
     if (p.precision != OW3D_PREC_FP64 && p.precision != OW3D_PREC_MIXED) return fail("precision must be 0 or 1");
     if (p.krylov != OW3D_KRYLOV_FGMRES && p.krylov != OW3D_KRYLOV_LGMRES) return fail("krylov must be 0 or 1");
     if (p.GMRESmaxiterations < 1) return fail("GMRESmaxiterations must be >= 1");
+    if (p.IncWaveType == 3) {
+        if (p.periodic_x != 0) return fail("periodic_x: the flux wavemaker is the west wall's flux");
+        if (p.flux_order < 1 || p.flux_order > 10) return fail("flux wavemaker: interpolation order 1..10 required");
+    }
     if (p.current_flag != 0 && p.current_Q != 0.0 && p.periodic_x != 0)
         return fail("periodic_x: the constant-flux current enters through the walls");
     if (smoothing_on(p) && p.periodic_x != 0)
@@ -916,6 +916,7 @@ int default_params(ow3d_params* p) {
     p->accel_tol_fact = 1e30; p->i_breaking = 0; p->PDampingONOFF = 0; p->swenseONOFF = 0; p->curvilinearONOFF = 0;
     p->T_half = 0; p->phi_b = 0; p->phi_0 = 0; p->del_fac = 0; p->cel_fac = 0; p->gamma_break = 0;
     p->current_flag = 0; p->current_Q = 0;
+    p->flux_ramp = 0; p->flux_order = 1; std::memset(p->flux_file, 0, sizeof p->flux_file);
     return OW3D_OK;
 }
 
@@ -976,11 +977,10 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
     if (!r.num(0)) return fail("line 2: IC expected");
     p->IC = r.n(0);
     p->IncWaveType = r.num(1) ? r.n(1) : 0;
-    // IncWaveType 4 is the stream-function wave on a constant-flux current
-    // (ReadInputFileParameters.f90:45-46); 5, the flux wavemaker with one, is
-    // kept as written (ow3d_create refuses it)
+    // IncWaveType 4 and 5 are the stream-function wave and the flux
+    // wavemaker on a constant-flux current (ReadInputFileParameters.f90:45-48)
     if (p->IncWaveType == 4) { p->IncWaveType = 1; p->current_flag = 1; }
-    if (p->IncWaveType == 5) p->current_flag = 1;
+    if (p->IncWaveType == 5) { p->IncWaveType = 3; p->current_flag = 1; }
     if (r.num(2)) { p->accel_tol_fact = r.d(2); p->accel_from_deck = 1; }
     r = next();  // Lx Ly Lz Nx Ny Nz GridX GridY GridZ GhostGridX GhostGridY GhostGridZ
     if (r.nnum() < 12) return fail("line 3: 12 grid values expected");
@@ -1129,8 +1129,12 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
         Record q = next();  // curvilinearONOFF
         if (q.num(0)) p->curvilinearONOFF = q.n(0);
     }
-    if (p->IncWaveType == 3 || p->IncWaveType == 5) {
-        next();   // ramp time, order, paddle-signal file of the flux wavemaker (:579-589)
+    if (p->IncWaveType == 3) {
+        // ramp time, interpolation order, paddle-signal file (:579-589)
+        Record q = next();
+        if (q.nnum() < 2 || q.t.size() < 3) return fail("flux-wavemaker line: ramp time, order and file expected");
+        p->flux_ramp = q.d(0); p->flux_order = q.n(1);
+        std::snprintf(p->flux_file, sizeof p->flux_file, "%s", q.t[2].c_str());
     } else if (p->IncWaveType == 2) {
         Record q = next();
         if (q.nnum() < 1) return fail("incident-wave line expected for IncWaveType 2");
@@ -1158,6 +1162,123 @@ int read_deck(const char* path, ow3d_params* p, std::string* err) {
         if (li < lines.size()) {
             Record q = next();
             p->current_Q = q.num(0) ? q.d(0) : 0.0;
+        }
+    }
+    return OW3D_OK;
+}
+
+// ------------------------------------------------------ paddle signal
+// setupWavePaddle.f90:43-67: a header line, "dt nt n2", the n2 y positions,
+// then nt records "time flux(1..n2)" (list-directed: a record may span lines).
+int read_paddle_signal(const char* path, PaddleSignal& ps, std::string* err) {
+    auto fail = [&](const std::string& m, int code) { if (err) *err = m; return code; };
+    if (!path) return fail("read_paddle_signal: no file", OW3D_ERR_BAD_INPUT);
+    std::ifstream f(path);
+    if (!f) return fail(std::string("read_paddle_signal: cannot open ") + path, OW3D_ERR_IO);
+    std::string header;
+    if (!std::getline(f, header)) return fail("read_paddle_signal: no header line", OW3D_ERR_IO);
+    std::vector<double> v;
+    std::string tok;
+    while (f >> tok) {
+        for (char& ch : tok) if (ch == 'D' || ch == 'd') ch = 'e';
+        char* end = nullptr;
+        const double x = std::strtod(tok.c_str(), &end);
+        if (end == tok.c_str()) break;
+        v.push_back(x);
+    }
+    if (v.size() < 3) return fail("read_paddle_signal: dt nt n2 expected", OW3D_ERR_IO);
+    ps.dt = v[0]; ps.nt = (int)v[1]; ps.n2 = (int)v[2];
+    if (ps.nt < 5 || ps.n2 < 1) return fail("read_paddle_signal: at least 5 times and 1 point required", OW3D_ERR_BAD_INPUT);
+    const size_t need = 3 + (size_t)ps.n2 + (size_t)ps.nt * (1 + (size_t)ps.n2);
+    if (v.size() < need) return fail("read_paddle_signal: error reading wave flux data (file too short)", OW3D_ERR_IO);
+    ps.y.assign(v.begin() + 3, v.begin() + 3 + ps.n2);
+    ps.flux.resize((size_t)ps.nt * ps.n2);
+    for (int i = 0; i < ps.nt; ++i)
+        for (int j = 0; j < ps.n2; ++j) ps.flux[(size_t)i * ps.n2 + j] = v[3 + (size_t)ps.n2 + (size_t)i * (1 + ps.n2) + 1 + j];
+    return OW3D_OK;
+}
+
+// Neville's algorithm: the value at x of the polynomial through (xa[i],
+// ya[i]), i < n, built column by column of the difference tableau from the
+// entry nearest x, the correction path kept as central as it can be -- the
+// published algorithm of the reference's polint (polint.f90).
+static double neville(const double* xa, const double* ya, int n, double x) {
+    double c[10], d[10];
+    int ns = 1;   // 1-based, as the path rule is written
+    double dif = std::fabs(x - xa[0]);
+    for (int i = 1; i <= n; ++i) {
+        const double dift = std::fabs(x - xa[i - 1]);
+        if (dift < dif) { ns = i; dif = dift; }
+        c[i - 1] = ya[i - 1];
+        d[i - 1] = ya[i - 1];
+    }
+    double y = ya[ns - 1];
+    ns = ns - 1;
+    for (int m = 1; m <= n - 1; ++m) {
+        for (int i = 1; i <= n - m; ++i) {
+            const double ho = xa[i - 1] - x, hp = xa[i + m - 1] - x;
+            const double w = c[i] - d[i - 1];
+            const double den = w / (ho - hp);
+            d[i - 1] = hp * den;
+            c[i - 1] = ho * den;
+        }
+        double dy;
+        if (2 * ns < n - m) dy = c[ns];
+        else { dy = d[ns - 1]; ns = ns - 1; }
+        y = y + dy;
+    }
+    return y;
+}
+
+// The signal on the rows of the grid (setupWavePaddle.f90:77-122 and the
+// y interpolation of waveGenerationFromPaddleSignal.f90:65-96, which does not
+// depend on time): F[i * Nyg + j] = u and X[...] = eta_x = -u_t / g at time
+// level i (0-based) and row j, interior rows only.
+int paddle_tables(const ow3d_params& p, const GridHost& G, const PaddleSignal& ps, std::vector<double>& F,
+                  std::vector<double>& X, std::string* err) {
+    auto fail = [&](const std::string& m) { if (err) *err = m; return OW3D_ERR_BAD_INPUT; };
+    const int nt = ps.nt, n2 = ps.n2, order = p.flux_order;
+    if (order < 1 || order > 10 || order > n2) return fail("paddle signal: the interpolation order must be 1..min(10, n2)");
+    const double dy_local = 2.0 * ps.y[0];
+    for (int i = 2; i <= n2 - 1; ++i)
+        if (std::fabs(ps.y[(size_t)i - 1] - (ps.y[(size_t)i - 2] + dy_local)) >= 1e-5)
+            return fail("paddle signal: the points must be uniformly spaced from y = dy/2 to ymax - dy/2");
+    if ((double)nt * ps.dt < (double)p.Nsteps * p.dt)
+        return fail("paddle signal: the time series is shorter than Nsteps * dt");
+    // eta_x = -1/g u_t, 5-point derivative weights at each of 5 uniform times
+    double tt[5], w[5][5];
+    for (int q = 0; q < 5; ++q) tt[q] = q * ps.dt;
+    for (int q = 0; q < 5; ++q) fd_weights(tt[q], tt, 4, 1, w[q]);
+    const double gfac = -1.0 / p.g;
+    std::vector<double> ex((size_t)nt * n2);
+    for (int j = 0; j < n2; ++j) {
+        auto fl = [&](int i) { return ps.flux[(size_t)i * n2 + j]; };   // 0-based time
+        for (int i = 0; i < nt; ++i) {
+            int row, base;
+            if (i < 2) { row = i; base = 0; }
+            else if (i < nt - 2) { row = 2; base = i - 2; }
+            else { row = 4 - (nt - 1 - i); base = nt - 5; }
+            double acc = 0;
+            for (int q = 0; q < 5; ++q) acc += w[row][q] * fl(base + q);
+            ex[(size_t)i * n2 + j] = gfac * acc;
+        }
+    }
+    const int Nyg = G.Nyg;
+    F.assign((size_t)nt * Nyg, 0.0);
+    X.assign((size_t)nt * Nyg, 0.0);
+    for (int j = 1 + G.gy; j <= G.Ny + G.gy; ++j) {
+        const double y0 = G.y[(size_t)j - 1];
+        int nny = (int)std::lround(y0 / dy_local) + 1 - order / 2;   // NINT: half away from zero
+        if (nny < 1) nny = 1;
+        else if (nny + order - 1 > n2) nny = n2 - order + 1;
+        std::vector<double> a((size_t)order), b((size_t)order);
+        for (int i = 0; i < nt; ++i) {
+            for (int q = 0; q < order; ++q) {
+                a[(size_t)q] = ps.flux[(size_t)i * n2 + nny - 1 + q];
+                b[(size_t)q] = ex[(size_t)i * n2 + nny - 1 + q];
+            }
+            F[(size_t)i * Nyg + j - 1] = neville(&ps.y[(size_t)nny - 1], a.data(), order, y0);
+            X[(size_t)i * Nyg + j - 1] = neville(&ps.y[(size_t)nny - 1], b.data(), order, y0);
         }
     }
     return OW3D_OK;

@@ -65,6 +65,16 @@ bool breaking_on(const ow3d_params& p);
 // zero-initialised ow3d_params, counts as off).
 bool smoothing_on(const ow3d_params& p);
 
+// The flux wavemaker's paddle signal (setupWavePaddle.f90): flux time-major, nt x n2.
+struct PaddleSignal {
+    double dt = 0;
+    int nt = 0, n2 = 0;
+    std::vector<double> y, flux;
+};
+int read_paddle_signal(const char* path, PaddleSignal& ps, std::string* err);
+int paddle_tables(const ow3d_params& p, const GridHost& G, const PaddleSignal& ps, std::vector<double>& F,
+                  std::vector<double>& X, std::string* err);
+
 int build_grid(const ow3d_params& p, const double* h, const double* hx, const double* hxx, const double* hy,
                const double* hyy, GridHost& G, std::string* err);
 std::vector<ZoneHost> build_zones(const ow3d_params& p, const GridHost& G);

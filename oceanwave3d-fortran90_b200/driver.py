@@ -9,8 +9,10 @@ prepare() does the host set-up (no device): the deck, the geometry and
 initial state (a bathymetry file when Lz <= 0, the formula initial conditions,
 a hot start from OceanWave3D.init for IC -1) and the relaxation-zone targets of
 the incident wave (IncWaveType 1: the stream-function wave at every RK stage
-time; 2: the reference's linear or random wave series). A pressure-damping
-zone needs no host step: ow3d_create sets it up from the deck. run() creates the
+time; 2: the reference's linear or random wave series; 3: the paddle signal
+of the flux wavemaker, read from the file the deck names). A pressure-damping
+zone, the current of IncWaveType 4 / 5, the breaking model and the local
+smoothing need no host step: ow3d_create sets them up from the deck. run() creates the
 simulation, applies the output schedule of the deck at step 0 and after every
 step (EP / ASCII files, OceanWave3D.end, Kinematics files) and takes the
 Nsteps - 1 steps of the reference's time loop. run() takes any backend with
@@ -22,7 +24,7 @@ import numpy as np
 
 from . import capi
 from . import (Simulation, dims, incident_wave, initial_condition, lib, read_bathymetry, read_deck, read_init_file,
-               stream_function_wave)
+               read_paddle_signal, stream_function_wave)
 
 
 def zone_box(p, zone):
@@ -39,10 +41,11 @@ def zone_box(p, zone):
 class Setup:
     """Everything a run needs before the device is involved."""
 
-    def __init__(self, params, geometry, E0, P0, targets, notes):
+    def __init__(self, params, geometry, E0, P0, targets, notes, paddle=None):
         self.params, self.geometry, self.E0, self.P0 = params, geometry, E0, P0
         self.targets = targets          # {zone: (mode, nt, dt_sample, eta, phis)}
         self.notes = notes              # how each part was built, for the log
+        self.paddle = paddle            # flux wavemaker: (dt, y, flux) or None
 
 
 def prepare(deck, deck_dir=None):
@@ -117,11 +120,20 @@ def prepare(deck, deck_dir=None):
                 phis = np.array([np.tile(f, rows) for _, f in line])
                 targets[z] = (1, nt, 0.5 * p.dt, eta, phis)
                 notes.append(f"zone {z}: stream-function wave at every RK stage time")
+    paddle = None
+    if p.IncWaveType == 3:
+        # the flux wavemaker's paddle signal (setupWavePaddle.f90), named by the deck
+        f = deck_dir / p.flux_file.decode()
+        paddle = read_paddle_signal(f)
+        notes.append(f"flux wavemaker: {f.name}, {paddle[2].shape[0]} times every {paddle[0]:g} s, "
+                     f"{paddle[2].shape[1]} points in y, ramp {p.flux_ramp:g} s, order {p.flux_order}")
+    if p.current_flag:
+        notes.append(f"constant-flux current Q = {p.current_Q:g} m^2/s")
     if p.PDampingONOFF:
         # set up on the device by ow3d_create (PreprocessPDampingZones.f90)
         notes.append(f"pressure-damping zone x = {p.pd_x0:g} .. {p.pd_x1:g}, type {p.pd_type}, "
                      f"g0 {p.pd_g0Phi:g} (phi) {p.pd_g0Eta:g} (eta)")
-    return Setup(p, geometry, E0, P0, targets, notes)
+    return Setup(p, geometry, E0, P0, targets, notes, paddle)
 
 
 def run(deck, outdir=None, steps=None, backend=Simulation, deck_dir=None):
@@ -136,6 +148,8 @@ def run(deck, outdir=None, steps=None, backend=Simulation, deck_dir=None):
     sim.set_state(s.E0, s.P0, t=p.time0)
     for z, t in s.targets.items():
         sim.set_relax_target(z, *t)
+    if s.paddle is not None and hasattr(sim, "set_paddle_signal"):
+        sim.set_paddle_signal(*s.paddle)
     out = None if outdir is None else str(outdir)
     writes = out is not None and hasattr(sim, "store_data")
     if out is not None:

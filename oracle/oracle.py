@@ -88,6 +88,7 @@ def lib():
         L.orc_breaking_state.argtypes = [V, D, D]
         L.orc_detect_breaking.argtypes = [V, D, C.c_int]
         L.orc_accel_state.argtypes = [V, D, C.c_int, I]
+        L.orc_set_paddle.argtypes = [V, C.c_int, C.c_int, C.c_double, D, D]
         _lib = L
     return _lib
 
@@ -269,6 +270,16 @@ class Oracle:
         E = _c(E)
         if lib().orc_detect_breaking(self.h, _p(E), 1 if update else 0) != 0:
             raise ValueError("oracle: no breaking model in this simulation")
+
+    def set_paddle(self, dt, y, flux):
+        """The flux wavemaker's signal (setupWavePaddle.f90): flux (nt, n2) at
+        the n2 positions y every dt."""
+        y, flux = _c(y), _c(flux)
+        nt, n2 = flux.shape
+        if lib().orc_set_paddle(self.h, nt, n2, float(dt), _p(y), _p(flux)) != 0:
+            raise ValueError("oracle: not a flux-wavemaker simulation, or a signal shorter than 5 times")
+
+    set_paddle_signal = set_paddle
 
     def accel_state(self):
         """The last local-smoothing call (LocalSmoothing2D/3D.f90): the surface

@@ -63,7 +63,13 @@ struct Sim {
     // state
     vector<double> E, P, W, Ex, Exx, Ey, Eyy, Px, Py;
     vector<double> tE, tP, tW, tEx, tExx, tEy, tEyy, tPx, tPy;
-    vector<double> sEx, sPx, sEy, sPy;   // ghost source terms (zero)
+    vector<double> sEx, sPx, sEy, sPy;   // ghost source terms of Wavefield
+    vector<double> tsEx, tsPx;           // those of Wavefield_tmp (the RK stages)
+    // the flux wavemaker (IncWaveType 3; setupWavePaddle.f90)
+    int pad = 0, pad_nt = 0, pad_n2 = 0;
+    double pad_dt = 0;
+    vector<double> pad_y, pad_flux, pad_etax;   // nt x n2, time-major
+    vector<double> Uneu;                 // per row: the west wall's flux FAC u (Uneumann, k >= 2)
     vector<double> PHI, LASTPHI0, LASTPHI1, RHS;
     vector<double> dsig;                 // 5*N, dsigmanew(k,i,j,1..5) for the current stage
     double time = 0; int64_t tstep = 0;
@@ -1082,15 +1088,16 @@ static void ghost_y(const Sim& s, double* v, const double* S) {
     }
 }
 // DifferentiationsFreeSurfacePlane.f90:13-32 (Cartesian branch)
+// tmp: the RK stages' field (Wavefield_tmp), whose x sources are its own
 static void fs_derivs(Sim& s, vector<double>& E, vector<double>& P, vector<double>& Ex, vector<double>& Exx,
-                      vector<double>& Px, vector<double>& Ey, vector<double>& Eyy, vector<double>& Py) {
+                      vector<double>& Px, vector<double>& Ey, vector<double>& Eyy, vector<double>& Py, bool tmp = false) {
     if (s.per) {
         // periodic x: image columns in place of the ghost-layer update
         images_x(s, E.data(), 1); dx2(s, E.data(), Ex.data(), 1); dx2(s, E.data(), Exx.data(), 2);
         images_x(s, P.data(), 1); dx2(s, P.data(), Px.data(), 1);
     } else if (s.p.Nx > 1) {
-        ghost_x(s, E.data(), s.sEx.data()); dx2(s, E.data(), Ex.data(), 1); dx2(s, E.data(), Exx.data(), 2);
-        ghost_x(s, P.data(), s.sPx.data()); dx2(s, P.data(), Px.data(), 1);
+        ghost_x(s, E.data(), tmp ? s.tsEx.data() : s.sEx.data()); dx2(s, E.data(), Ex.data(), 1); dx2(s, E.data(), Exx.data(), 2);
+        ghost_x(s, P.data(), tmp ? s.tsPx.data() : s.sPx.data()); dx2(s, P.data(), Px.data(), 1);
     }
     if (s.p.Ny > 1) {
         ghost_y(s, E.data(), s.sEy.data()); dy2(s, E.data(), Ey.data(), 1); dy2(s, E.data(), Eyy.data(), 2);
@@ -1530,6 +1537,71 @@ static void local_smoothing(Sim& s) {
         }
 }
 
+// ------------------------------------------------------- flux wavemaker
+// polint.f90 (Neville's algorithm, the published method): the value at x of
+// the polynomial through (xa[i], ya[i]), i < n.
+static double polint(const double* xa, const double* ya, int n, double x) {
+    vector<double> c(ya, ya + n), d(ya, ya + n);
+    int ns = 1;
+    double dif = std::fabs(x - xa[0]);
+    for (int i = 1; i <= n; ++i) {
+        double dift = std::fabs(x - xa[i - 1]);
+        if (dift < dif) { ns = i; dif = dift; }
+    }
+    double y = ya[ns - 1];
+    ns = ns - 1;
+    for (int m = 1; m <= n - 1; ++m) {
+        for (int i = 1; i <= n - m; ++i) {
+            double ho = xa[i - 1] - x, hp = xa[i + m - 1] - x;
+            double w = c[i] - d[i - 1];
+            double den = ho - hp;
+            den = w / den;
+            d[i - 1] = hp * den;
+            c[i - 1] = ho * den;
+        }
+        double dy;
+        if (2 * ns < n - m) dy = c[ns];
+        else { dy = d[ns - 1]; ns = ns - 1; }
+        y = y + dy;
+    }
+    return y;
+}
+
+// waveGenerationFromPaddleSignal.f90:43-111 at RKtime: the flux and eta_x of
+// the two signal levels around it (itime = floor(RKtime / dt) + 1, kept
+// inside the table), interpolated in y with `order` points, linearly in time,
+// the flux ramped; Uneumann per row, and the west-wall sources of Wavefield.
+static void paddle_signal(Sim& s, double RKtime) {
+    const int n2 = s.pad_n2, order = s.p.flux_order, Nx = s.Nxg;
+    int itime = (int)std::floor(RKtime / s.pad_dt) + 1;
+    if (itime < 1) itime = 1;
+    if (itime > s.pad_nt - 1) itime = s.pad_nt - 1;
+    double dl1 = RKtime - (itime - 1) * s.pad_dt, dl2 = itime * s.pad_dt - RKtime;
+    double tw1 = dl2 / (dl1 + dl2), tw2 = dl1 / (dl1 + dl2);
+    const double r = s.p.flux_ramp;
+    double FAC = 1.0;
+    if (RKtime < r) FAC = -2.0 / (r * r * r) * (RKtime * RKtime * RKtime) + 3.0 / (r * r) * (RKtime * RKtime);
+    const double dy_local = s.pad_y[0] * 2;
+    for (int j = 1 + s.gy; j <= s.p.Ny + s.gy; ++j) {
+        double y0 = s.fine.y[(size_t)j - 1];
+        int NNY = (int)std::lround(y0 / dy_local) + 1 - order / 2;
+        if (NNY < 1) NNY = 1;
+        else if (NNY + order - 1 > n2) NNY = n2 - order + 1;
+        auto at = [&](const vector<double>& tab, int it) {
+            vector<double> v((size_t)order);
+            for (int q = 0; q < order; ++q) v[(size_t)q] = tab[(size_t)(it - 1) * n2 + NNY - 1 + q];
+            return polint(&s.pad_y[(size_t)NNY - 1], v.data(), order, y0);
+        };
+        double flux0 = at(s.pad_flux, itime), etax0 = at(s.pad_etax, itime);
+        double flux1 = at(s.pad_flux, itime + 1), etax1 = at(s.pad_etax, itime + 1);
+        double flux = tw1 * flux0 + tw2 * flux1;
+        double etax = tw1 * etax0 + tw2 * etax1;
+        s.Uneu[(size_t)j - 1] = FAC * flux;
+        s.sPx[(size_t)(1 + s.gx - 1) + (size_t)Nx * (j - 1)] = FAC * flux;
+        s.sEx[(size_t)(1 + s.gx - 1) + (size_t)Nx * (j - 1)] = etax;
+    }
+}
+
 // ------------------------------------------------------------- RK4 step
 // Runge_Kutta_4.f90:1-429 (nonlinear or linear FSBC, no SWENSE, no pressure).
 static int rk4_step(Sim& s) {
@@ -1546,9 +1618,13 @@ static int rk4_step(Sim& s) {
         const int Nz = s.Nzg;
         for (int j = 1 + s.gy; j <= s.Nyg - s.gy; ++j)
             for (int i = 1 + s.gx; i <= s.Nxg - s.gx; ++i) s.RHS[gid(s, Nz, i, j)] = Pf[(size_t)(i - 1) + (size_t)s.Nxg * (j - 1)];
-        if (s.gx == 1)   // Runge_Kutta_4.f90:108-113: Uneumann (zero) + the current
+        if (s.gx == 1)   // Runge_Kutta_4.f90:108-113: Uneumann (the wavemaker's flux above the bottom row) + the current
             for (int j = 1 + s.gy; j <= s.Nyg - s.gy; ++j)
-                for (int k = 1; k <= Nz; ++k) { s.RHS[gid(s, k, 1, j)] = s.Ul; s.RHS[gid(s, k, s.Nxg, j)] = s.Ur; }
+                for (int k = 1; k <= Nz; ++k) {
+                    const double un = (s.pad && k >= 1 + s.gz) ? s.Uneu[(size_t)j - 1] : 0.0;
+                    s.RHS[gid(s, k, 1, j)] = un + s.Ul;
+                    s.RHS[gid(s, k, s.Nxg, j)] = s.Ur;
+                }
         if (s.per) zero_images_x(s, s.RHS.data(), Nz);   // identity rows of the image columns
     };
     auto sigma_for = [&](const vector<double>& E, const vector<double>& Ex, const vector<double>& Exx,
@@ -1560,14 +1636,19 @@ static int rk4_step(Sim& s) {
         int st = solve(s, s.RHS.data(), s.PHI.data(), it, res);
         if (st == OW3D_NOT_CONVERGED) status = OW3D_NOT_CONVERGED;
     };
-    // Runge_Kutta_4.f90:82-88: the ghost source of the surface potential, zero
-    // plus the constant-flux current at the west and east boundary columns
-    auto zero_src = [&]() {
-        std::fill(s.sPx.begin(), s.sPx.end(), 0.0);
+    // Runge_Kutta_4.f90:80-88 (and :261-268, :382-389): the potential's ghost
+    // source of the stage's field set to zero, the flux wavemaker called at
+    // RK time (it writes Uneumann and the sources of Wavefield, whichever
+    // field the stage uses, waveGenerationFromPaddleSignal.f90:107-110), then
+    // the constant-flux current added at the west and east boundary columns
+    auto zero_src = [&](bool tmp, double RKt) {
+        vector<double>& px = tmp ? s.tsPx : s.sPx;
+        std::fill(px.begin(), px.end(), 0.0);
+        if (s.pad) paddle_signal(s, RKt);
         if (s.gx == 1)
             for (int j = 1; j <= s.Nyg; ++j) {
-                s.sPx[(size_t)(1 + s.gx - 1) + (size_t)s.Nxg * (j - 1)] += s.Ul;
-                s.sPx[(size_t)(s.p.Nx + s.gx - 1) + (size_t)s.Nxg * (j - 1)] += s.Ur;
+                px[(size_t)(1 + s.gx - 1) + (size_t)s.Nxg * (j - 1)] += s.Ul;
+                px[(size_t)(s.p.Nx + s.gx - 1) + (size_t)s.Nxg * (j - 1)] += s.Ur;
             }
     };
     auto breaking = [&](const vector<double>& Ef) { if (s.brk && s.p.i_breaking == 1) detect_breaking(s, Ef, false); };
@@ -1578,8 +1659,8 @@ static int rk4_step(Sim& s) {
     for (size_t c = 0; c < C; ++c) { s.tE[c] = s.E[c] + half * dt * k1E[c]; s.tP[c] = s.P[c] + half * dt * k1P[c]; }
     double RKtime = time + half * dt;
     relax(s, s.tE, s.tP, RKtime, time);
-    zero_src();
-    fs_derivs(s, s.tE, s.tP, s.tEx, s.tExx, s.tPx, s.tEy, s.tEyy, s.tPy);
+    zero_src(true, RKtime);
+    fs_derivs(s, s.tE, s.tP, s.tEx, s.tExx, s.tPx, s.tEy, s.tEyy, s.tPy, true);
     sigma_for(s.tE, s.tEx, s.tExx, s.tEy, s.tEyy);
     set_rhs(s.tP);
     if (s.p.extrapolationONOFF == 1)
@@ -1593,7 +1674,7 @@ static int rk4_step(Sim& s) {
     for (size_t c = 0; c < C; ++c) { s.tE[c] = s.E[c] + half * dt * k2E[c]; s.tP[c] = s.P[c] + half * dt * k2P[c]; }
     RKtime = time + half * dt;
     relax(s, s.tE, s.tP, RKtime, time);
-    fs_derivs(s, s.tE, s.tP, s.tEx, s.tExx, s.tPx, s.tEy, s.tEyy, s.tPy);
+    fs_derivs(s, s.tE, s.tP, s.tEx, s.tExx, s.tPx, s.tEy, s.tEyy, s.tPy, true);
     sigma_for(s.tE, s.tEx, s.tExx, s.tEy, s.tEyy);
     set_rhs(s.tP);
     do_solve();
@@ -1605,8 +1686,8 @@ static int rk4_step(Sim& s) {
     for (size_t c = 0; c < C; ++c) { s.tE[c] = s.E[c] + dt * k3E[c]; s.tP[c] = s.P[c] + dt * k3P[c]; }
     RKtime = time + dt;
     relax(s, s.tE, s.tP, RKtime, time);
-    zero_src();
-    fs_derivs(s, s.tE, s.tP, s.tEx, s.tExx, s.tPx, s.tEy, s.tEyy, s.tPy);
+    zero_src(true, RKtime);
+    fs_derivs(s, s.tE, s.tP, s.tEx, s.tExx, s.tPx, s.tEy, s.tEyy, s.tPy, true);
     sigma_for(s.tE, s.tEx, s.tExx, s.tEy, s.tEyy);
     set_rhs(s.tP);
     if (s.p.extrapolationONOFF == 1 && tstep > 1)
@@ -1628,7 +1709,7 @@ static int rk4_step(Sim& s) {
     RKtime = time + dt;
     if (s.p.filteringONOFF > 0 && (tstep % s.p.filteringONOFF) == 0) { filter(s, s.E); filter(s, s.P); }
     relax(s, s.E, s.P, RKtime, time);
-    zero_src();
+    zero_src(false, RKtime);
     fs_derivs(s, s.E, s.P, s.Ex, s.Exx, s.Px, s.Ey, s.Eyy, s.Py);
     sigma_for(s.E, s.Ex, s.Exx, s.Ey, s.Eyy);
     set_rhs(s.P);
@@ -1676,7 +1757,8 @@ static Sim* create(const ow3d_params* p, const double* h, const double* hx, cons
     }
     size_t C = s->C, N = s->N;
     for (auto* v : {&s->E, &s->P, &s->W, &s->Ex, &s->Exx, &s->Ey, &s->Eyy, &s->Px, &s->Py, &s->tE, &s->tP, &s->tW,
-                    &s->tEx, &s->tExx, &s->tEy, &s->tEyy, &s->tPx, &s->tPy, &s->sEx, &s->sPx, &s->sEy, &s->sPy})
+                    &s->tEx, &s->tExx, &s->tEy, &s->tEyy, &s->tPx, &s->tPy, &s->sEx, &s->sPx, &s->sEy, &s->sPy,
+                    &s->tsEx, &s->tsPx})
         v->assign(C, 0.0);
     for (auto* v : {&s->PHI, &s->LASTPHI0, &s->LASTPHI1, &s->RHS}) v->assign(N, 0.0);
     update_sigma(*s, nullptr, nullptr, nullptr, nullptr, nullptr);
@@ -1691,6 +1773,8 @@ static Sim* create(const ow3d_params* p, const double* h, const double* hx, cons
     s->smooth = (p->accel_from_deck ? p->accel_tol_fact <= 100.0
                                     : (p->accel_tol_fact > 0.0 && p->accel_tol_fact <= 100.0)) ? 1 : 0;
     if (s->smooth) { for (auto& v : s->WHist) v.assign(C, 0.0); s->EtatHist1.assign(C, 0.0); }
+    s->pad = p->IncWaveType == 3 ? 1 : 0;
+    s->Uneu.assign((size_t)s->Nyg, 0.0);
     s->brk = (p->i_breaking > 0 && p->Ny == 1 && p->Nx > 1) ? 1 : 0;
     s->Qr_x.assign(C, 0.0);
     if (s->brk) {
@@ -1768,7 +1852,8 @@ void orc_set_state(void* sv, const double* E, const double* P, const double* W, 
     if (s->per) { zero_images_x(*s, s->PHI.data(), s->Nzg); if (W) images_x(*s, s->W.data(), 1); }
     std::fill(s->LASTPHI0.begin(), s->LASTPHI0.end(), 0.0); std::fill(s->LASTPHI1.begin(), s->LASTPHI1.end(), 0.0);
     s->time = t; s->tstep = 0;
-    std::fill(s->sPx.begin(), s->sPx.end(), 0.0);   // the set-up's source is zero
+    std::fill(s->sPx.begin(), s->sPx.end(), 0.0);   // the set-up's sources are zero
+    std::fill(s->sEx.begin(), s->sEx.end(), 0.0);
     // OceanWave3DT0Setup.f90:444,564-569: surface derivatives; linear case keeps eta = 0 coefficients.
     fs_derivs(*s, s->E, s->P, s->Ex, s->Exx, s->Px, s->Ey, s->Eyy, s->Py);
     update_sigma(*s, nullptr, nullptr, nullptr, nullptr, nullptr);
@@ -1827,6 +1912,26 @@ int orc_rollers(void* sv, int cap, int* npts, int* toe, double* x, double* eta, 
 int orc_detect_breaking(void* sv, const double* E, int update) {
     Sim* s = (Sim*)sv; if (!s->brk) return -1;
     vector<double> e(E, E + s->C); detect_breaking(*s, e, update != 0); return 0;
+}
+// setupWavePaddle.f90:89-122: the signal (flux time-major, nt x n2) and
+// eta_x = -u_t / g from the 5-point time derivative (one-sided at the ends)
+int orc_set_paddle(void* sv, int nt, int n2, double dt, const double* y, const double* flux) {
+    Sim* s = (Sim*)sv; if (!s->pad || nt < 5 || n2 < 1) return -1;
+    s->pad_nt = nt; s->pad_n2 = n2; s->pad_dt = dt;
+    s->pad_y.assign(y, y + n2); s->pad_flux.assign(flux, flux + (size_t)nt * n2);
+    s->pad_etax.assign((size_t)nt * n2, 0.0);
+    double ft[5], fc[5][5];
+    for (int i = 0; i < 5; ++i) ft[i] = i * dt;
+    for (int i = 0; i < 5; ++i) fd_weights(ft[i], ft, 4, 1, fc[i]);
+    const double gfac = -1.0 / s->p.g;
+    for (int j = 1; j <= n2; ++j) {
+        auto F = [&](int i) { return s->pad_flux[(size_t)(i - 1) * n2 + j - 1]; };
+        auto dot = [&](int row, int i0) { double a = 0; for (int q = 0; q < 5; ++q) a += fc[row - 1][q] * F(i0 + q); return a; };
+        for (int i = 1; i <= 2; ++i) s->pad_etax[(size_t)(i - 1) * n2 + j - 1] = gfac * dot(i, 1);
+        for (int i = 3; i <= nt - 2; ++i) s->pad_etax[(size_t)(i - 1) * n2 + j - 1] = gfac * dot(3, i - 2);
+        for (int i = nt - 1; i <= nt; ++i) s->pad_etax[(size_t)(i - 1) * n2 + j - 1] = gfac * dot(5 - (nt - i), nt - 4);
+    }
+    return 0;
 }
 // the last local-smoothing call: dw/dt at the surface (C values) and the
 // columns where it exceeded the limit; returns their count (-1: off)

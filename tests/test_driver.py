@@ -78,12 +78,14 @@ REF = reference_decks() or pathlib.Path("/nonexistent")
 
 @pytest.mark.skipif(not REF.is_dir(), reason="reference example decks not on this machine")
 @pytest.mark.parametrize("name", ["LinearTravellingWave", "RandomWave2D", "NLStanding", "RandomWave2DShoaling",
-                                  "ObliqueRegular1Beach", "StreamFuncWave"])
+                                  "ObliqueRegular1Beach", "StreamFuncWave", "FluxWavemaker2D",
+                                  "RollerBreakingModel2D", "FilterBreakingModel2D"])
 def test_reference_decks_run_on_oracle(ow3d, oracle, name):
     """The reference's own example decks set up and step (two steps on the
     oracle) with bounded surfaces: incident waves of several kinds, a
     formula IC, a bathymetry file, directional generation zones, pressure
-    damping."""
+    damping, the flux wavemaker with its paddle-signal file, the roller
+    breaking model and the local smoothing."""
     from ow3d_b200 import driver
     sim, s, st = driver.run(REF / f"OceanWave3D.inp.{name}", steps=2, backend=_oracle_backend(oracle))
     E = sim.get_state()[0]
