@@ -569,6 +569,20 @@ const char* ow3d_strerror(int status);
 const char* ow3d_last_error(void);
 const char* ow3d_version(void);
 
+/* ------------------------------------------------------ measurement */
+
+/* Number of kernels this library has launched since it was loaded, over all
+ * handles and threads (the cooperative coarse-grid kernel counts as one). */
+unsigned long long ow3d_launch_count(void);
+
+/* Device time of `reps` launches of one kernel on this handle's stream,
+ * measured with CUDA events around each launch; before each launch a write of
+ * the Krylov basis (larger than L2) evicts the inputs from L2, outside the
+ * timed interval. which 0 = high-order operator, 1 = one preconditioner
+ * application (V-cycle), 2 = one colour pass of the finest multigrid level
+ * (FP64 handles). Returns the total milliseconds of the launches. */
+int ow3d_bench_kernel(ow3d_handle* h, int which, int reps, double* ms_total);
+
 #ifdef __cplusplus
 }
 #endif

@@ -3,6 +3,9 @@
  * set-up tables and the individual multigrid components of a handle so that
  * each can be compared with the CPU restatement of the reference; they have no
  * counterpart in the reference program and are not part of the drop-in API.
+ * They are exported only by the testing build of the library
+ * (libow3d_dev.so, the same objects linked without the product's export
+ * list); libow3d.so exports the functions of ow3d.h alone.
  */
 #ifndef OW3D_TEST_H
 #define OW3D_TEST_H
@@ -40,9 +43,6 @@ int ow3d_test_filter_coeffs(const ow3d_handle* h, double* centre, double* bounda
  * op 5: out = in1 after one smoother phase with rhs in2: colour pass `nu`, or
  *       the bottom-row pass when nu < 0 (levels with mixed-derivative terms). */
 int ow3d_test_level_op(ow3d_handle* h, int level, int op, int nu, const double* in1, const double* in2, double* out);
-/* Number of kernels this library has launched since it was loaded, over all
- * handles and threads (the cooperative coarse-grid kernel counts as one). */
-unsigned long long ow3d_launch_count(void);
 
 /* Tuning knob for measurements: cap on the number of blocks of the fused
  * coarse-level multigrid kernel (0 = one block per SM, the default). Returns
@@ -100,13 +100,6 @@ int ow3d_test_detect_breaking(ow3d_handle* h, const double* E, int update);
  * limit, Nxg*Nyg each (either may be NULL; both zero before the third step). */
 int ow3d_test_accel_state(ow3d_handle* h, double* Wt, int* flags);
 
-/* Device time of `reps` launches of one kernel on this handle's stream,
- * measured with CUDA events around each launch; before each launch a write of
- * the Krylov basis (larger than L2) evicts the inputs from L2, outside the
- * timed interval. which 0 = high-order operator, 1 = one preconditioner
- * application (V-cycle), 2 = one colour pass of the finest multigrid level
- * (FP64 handles). Returns the total milliseconds of the launches. */
-int ow3d_bench_kernel(ow3d_handle* h, int which, int reps, double* ms_total);
 /* sizeof the C structs: 0 ow3d_params, 1 ow3d_zone, 2 ow3d_stats. */
 int ow3d_test_sizeof(int which);
 

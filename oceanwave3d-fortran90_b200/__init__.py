@@ -14,6 +14,7 @@ points included. numpy arrays of shape (Nyg, Nxg, Nzg) / (Nyg, Nxg) in C order
 have exactly that memory layout.
 """
 import ctypes as _C
+import os as _os
 import pathlib as _pathlib
 
 import numpy as _np
@@ -22,7 +23,11 @@ from . import capi
 from . import workloads  # noqa: F401
 from .capi import Params, Zone, Stats, default_params, dims, set_zone  # noqa: F401
 
-LIB_PATH = _pathlib.Path(__file__).resolve().parent / "libow3d.so"
+# libow3d.so exports the functions of include/ow3d.h; the testing build,
+# libow3d_dev.so (same objects), also the probes of include/ow3d_test.h that
+# the parity tests call. OW3D_TEST_BUILD=1 selects the testing build.
+LIB_PATH = _pathlib.Path(__file__).resolve().parent / (
+    "libow3d_dev.so" if _os.environ.get("OW3D_TEST_BUILD") == "1" else "libow3d.so")
 _lib = None
 
 
@@ -44,6 +49,12 @@ def lib():
         L = _C.CDLL(str(LIB_PATH))
         capi.declare(L)
         D = _C.POINTER(_C.c_double)
+        L.ow3d_bench_kernel.argtypes = [_C.c_void_p, _C.c_int, _C.c_int, D]
+        L.ow3d_launch_count.argtypes = []
+        L.ow3d_launch_count.restype = _C.c_ulonglong
+        if not hasattr(L, "ow3d_test_level_count"):   # the product build: no probes
+            _lib = L
+            return _lib
         L.ow3d_test_level_count.argtypes = [_C.c_void_p]
         L.ow3d_test_level_dims.argtypes = [_C.c_void_p, _C.c_int] + [_C.POINTER(_C.c_int)] * 4
         L.ow3d_test_stencils.argtypes = [_C.c_void_p, D, D, D]
@@ -54,9 +65,6 @@ def lib():
         L.ow3d_test_filter_coeffs.argtypes = [_C.c_void_p, D, D]
         L.ow3d_test_level_op.argtypes = [_C.c_void_p, _C.c_int, _C.c_int, _C.c_int, D, D, D]
         L.ow3d_test_sizeof.argtypes = [_C.c_int]
-        L.ow3d_bench_kernel.argtypes = [_C.c_void_p, _C.c_int, _C.c_int, D]
-        L.ow3d_launch_count.argtypes = []
-        L.ow3d_launch_count.restype = _C.c_ulonglong
         L.ow3d_test_set_coarse_blocks.argtypes = [_C.c_int]
         L.ow3d_test_set_coop_max_points.argtypes = [_C.c_longlong]
         L.ow3d_test_set_coop_max_points.restype = _C.c_longlong

@@ -3,10 +3,15 @@
     python oceanwave3d-fortran90_b200/build.py [--force] [--jobs N]
 
 Compiles every csrc/*.cu and csrc/*.cpp with nvcc for
-``-gencode arch=compute_100a,code=sm_100a`` and links one shared library
-next to this file, so that it travels with the source tree.
+``-gencode arch=compute_100a,code=sm_100a`` and links the objects twice, next
+to this file so that both travel with the source tree:
+* libow3d.so, the product: it exports exactly the functions that
+  include/ow3d.h declares (a linker version script built from the header);
+* libow3d_dev.so, the testing build: the same objects with every ow3d_*
+  symbol exported, the probes of include/ow3d_test.h included.
 """
 import argparse
+import re
 import concurrent.futures as cf
 import os
 import pathlib
@@ -17,6 +22,7 @@ import sys
 HERE = pathlib.Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 OUT = HERE / "libow3d.so"
+OUT_DEV = HERE / "libow3d_dev.so"
 BUILD = HERE / "_build"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -65,12 +71,37 @@ def build(force=False, jobs=None, verbose=False, extra=()):
             if verbose and err.strip():
                 print(err, file=sys.stderr)
     objs = [BUILD / (s.name + ".o") for s in srcs]
-    if force or not OUT.exists() or any(o.stat().st_mtime > OUT.stat().st_mtime for o in objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", str(OUT), *map(str, objs), "-lcudart"]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError(f"link failed:\n{r.stderr}")
+    api = HERE.parent / "include" / "ow3d.h"
+    for out, script in ((OUT_DEV, None), (OUT, api)):
+        stamp = [o.stat().st_mtime for o in objs] + ([api.stat().st_mtime] if script else [])
+        if force or not out.exists() or any(t > out.stat().st_mtime for t in stamp):
+            link(out, objs, export_list(script) if script else None)
     return OUT
+
+
+def api_functions(header):
+    """Names of the functions a C header declares (comments removed)."""
+    text = re.sub(r"/\*.*?\*/", " ", header.read_text(), flags=re.S)
+    text = re.sub(r"//[^\n]*", " ", text)
+    return sorted(set(re.findall(r"\b(ow3d_[A-Za-z0-9_]+)\s*\(", text)))
+
+
+def export_list(header):
+    names = api_functions(header)
+    if not names:
+        raise RuntimeError(f"no functions found in {header}")
+    script = BUILD / "ow3d_exports.map"
+    script.write_text("{\n  global:\n" + "".join(f"    {n};\n" for n in names) + "  local: *;\n};\n")
+    return script
+
+
+def link(out, objs, version_script=None):
+    cmd = [nvcc(), *ARCH, "-shared", "-o", str(out), *map(str, objs), "-lcudart"]
+    if version_script:
+        cmd += ["-Xlinker", f"--version-script={version_script}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"link failed:\n{r.stderr}")
 
 
 if __name__ == "__main__":

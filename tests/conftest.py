@@ -1,4 +1,5 @@
 import importlib.util
+import os
 import pathlib
 import sys
 
@@ -6,6 +7,9 @@ import pytest
 
 ROOT = pathlib.Path(__file__).resolve().parent.parent
 PKG_DIR = ROOT / "oceanwave3d-fortran90_b200"
+# the tests call the probes of include/ow3d_test.h: load the testing build of
+# the library (the same objects as libow3d.so, with the probes exported)
+os.environ.setdefault("OW3D_TEST_BUILD", "1")
 
 
 def load_package():

@@ -13,9 +13,9 @@ ROOT = pathlib.Path(__file__).resolve().parent.parent
 HEADERS = sorted((ROOT / "include").glob("*.h"))
 
 
-def declared_functions():
+def declared_functions(headers=None):
     names = set()
-    for h in HEADERS:
+    for h in headers or HEADERS:
         text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
         for m in re.finditer(r"^[A-Za-z_][\w\s\*]*?\b(ow3d_\w+)\s*\(", text, flags=re.M):
             names.add(m.group(1))
@@ -29,15 +29,24 @@ def test_headers_declare_the_api():
     assert len(names) >= 30
 
 
+def exported(path):
+    out = subprocess.run(["nm", "-D", "--defined-only", str(path)], capture_output=True, text=True).stdout
+    return {ln.split()[-1] for ln in out.splitlines() if ln.strip()}
+
+
 def test_library_exports_every_declared_symbol(ow3d):
-    lib_path = ow3d.LIB if hasattr(ow3d, "LIB") else None
+    """The product library exports exactly the functions of include/ow3d.h;
+    the testing build (the same objects) also the probes of ow3d_test.h,
+    which the tests load."""
     L = ow3d.lib()
     missing = [n for n in sorted(declared_functions()) if not hasattr(L, n)]
     assert not missing, missing
-    if lib_path:
-        out = subprocess.run(["nm", "-D", "--defined-only", str(lib_path)], capture_output=True, text=True).stdout
-        exported = {ln.split()[-1] for ln in out.splitlines() if ln.strip()}
-        assert declared_functions() <= exported
+    api = declared_functions([ROOT / "include" / "ow3d.h"])
+    probes = declared_functions([ROOT / "include" / "ow3d_test.h"])
+    product = exported(ow3d.LIB_PATH.parent / "libow3d.so")
+    assert api <= product and not (product & probes)
+    assert {n for n in product if n.startswith("ow3d_")} == api
+    assert (api | probes) <= exported(ow3d.LIB_PATH.parent / "libow3d_dev.so")
 
 
 def test_struct_layouts_match(ow3d):
