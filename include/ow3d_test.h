@@ -58,6 +58,11 @@ long long ow3d_test_set_coop_max_points(long long points);
 /* Levels of at most `points` points run in the cluster (tail) kernel of the
  * fused coarse cycle (0: no tail), and the cluster's block count (8 or 16);
  * each returns the previous value. Process-wide. */
+/* Programmatic dependent launch between the solver's kernels (1, the
+ * default) or plain launches (0). Applies to launches made after the call:
+ * captured graphs keep what they were captured with. Returns the previous
+ * value. Process-wide. */
+int ow3d_test_set_pdl(int on);
 long long ow3d_test_set_tail_max_points(long long points);
 int ow3d_test_set_tail_cluster(int blocks);
 

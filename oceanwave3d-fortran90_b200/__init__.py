@@ -72,6 +72,7 @@ def lib():
         L.ow3d_test_set_tail_max_points.argtypes = [_C.c_longlong]
         L.ow3d_test_set_tail_max_points.restype = _C.c_longlong
         L.ow3d_test_set_tail_cluster.argtypes = [_C.c_int]
+        L.ow3d_test_set_pdl.argtypes = [_C.c_int]
         L.ow3d_test_set_colour_prefetch.argtypes = [_C.c_int]
         L.ow3d_test_graph_count.argtypes = [_C.c_void_p]
         L.ow3d_test_step_graph_count.argtypes = [_C.c_void_p]

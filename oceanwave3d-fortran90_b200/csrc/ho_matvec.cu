@@ -340,6 +340,7 @@ __global__ void __launch_bounds__(THREE ? 256 : 256, 2)
                 const double* __restrict__ b, double* __restrict__ y, int mode,
                 const __grid_constant__ ZTab<(NZG > 0 ? NZG : kZMax)> zt, int band_blocks, int64_t nband, int all,
                 int tiles_x) {
+    pdl_entry();
     constexpr int BX = Tile<THREE>::BX, BY = Tile<THREE>::BY, HX = Tile<THREE>::HX, HY = Tile<THREE>::HY;
     const int Nxg = g.Nxg, Nyg = g.Nyg, Nzg = NZG > 0 ? NZG : g.Nzg;
     const double scale = dscale ? *dscale : 1.0;
@@ -452,7 +453,7 @@ void launch_impl(const HoGrid& g, const Surface& s, const TIN* phi, const double
         cudaFuncSetAttribute(k_ho_matvec<NZG, THREE, TIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         attr_set.fetch_or(bit, std::memory_order_relaxed);
     }
-    note_launch(), k_ho_matvec<NZG, THREE, TIN><<<band_blocks + tiles, threads, smem, st>>>(
+    launch_k(k_ho_matvec<NZG, THREE, TIN>, dim3(band_blocks + tiles), dim3(threads), smem, st, 
         g, s, phi, scale, b, y, mode, zt, band_blocks, nband, split ? 0 : 1, tiles_x);
 }
 

@@ -112,6 +112,7 @@ __device__ void arnoldi_finish_dev(KrylovState* ks, int maxmv, int m) {
 }
 
 __global__ void k_arnoldi_finish(KrylovState* ks, int maxmv, int m) {
+    pdl_entry();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     arnoldi_finish_dev(ks, maxmv, m);
 }
@@ -124,6 +125,7 @@ __global__ void k_arnoldi_finish(KrylovState* ks, int maxmv, int m) {
 __global__ void __launch_bounds__(kThreads) k_multidot(const double* __restrict__ V, int64_t ldv, int k,
                                                        const double* __restrict__ w, int64_t n, double* partial,
                                                        unsigned int* counter, int nbx, KrylovState* ks, int cond) {
+    pdl_entry();
     if (cond && !ks->reorth) return;
     if (ks->done) return;
     const int v = blockIdx.y;
@@ -202,6 +204,7 @@ __global__ void __launch_bounds__(kThreads) k_project(const double* __restrict__
                                                       double* __restrict__ w, int64_t n,
                                                       double* partial, unsigned int* counter, int nblocks,
                                                       KrylovState* ks, int cond, int maxmv, int m) {
+    pdl_entry();
     if (cond && !ks->reorth) return;
     if (ks->done) return;
     __shared__ double coef[kMaxDots];
@@ -244,6 +247,7 @@ __global__ void __launch_bounds__(kThreads) k_project(const double* __restrict__
 __global__ void __launch_bounds__(kThreads) k_norm_init(const double* __restrict__ v, int64_t n, double* partial,
                                                         unsigned int* counter, int nblocks, KrylovState* ks,
                                                         double rtol, double atol, cudaGraphConditionalHandle hnext) {
+    pdl_entry();
     double acc[1] = {0.0};
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += stride) acc[0] += v[t] * v[t];
@@ -270,6 +274,7 @@ __global__ void __launch_bounds__(kThreads) k_norm_init(const double* __restrict
 // Upper-triangular solve R y = g for the current k (1 thread); R is the
 // in-place rotated H (left GMRES) or the separate rotated copy (FGMRES).
 __global__ void k_backsolve(KrylovState* ks, int rotated_R) {
+    pdl_entry();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     auto Rv = [&](int col, int row) -> double { return rotated_R ? ks->R[col][row] : ks->H[col][row]; };
     int kk = ks->k;
@@ -288,6 +293,7 @@ template <typename TZ>
 __global__ void __launch_bounds__(kThreads) k_solution_update(double* __restrict__ x, const TZ* __restrict__ Z,
                                                               int64_t ldz, int64_t n,
                                                               const KrylovState* ks, int use_scale) {
+    pdl_entry();
     __shared__ double coef[kMaxDots];
     const int k = ks->k;
     for (int v = threadIdx.x; v < k; v += blockDim.x) coef[v] = ks->y[v] * (use_scale ? ks->scale[v] : 1.0);
@@ -301,6 +307,7 @@ __global__ void __launch_bounds__(kThreads) k_solution_update(double* __restrict
 }
 
 __global__ void k_krylov_reset(KrylovState* ks) {
+    pdl_entry();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     ks->k = 0; ks->done = 0; ks->converged = 0; ks->iters = 0; ks->reorth = 0; ks->status = 0;
     ks->tol = 0; ks->resid = 0; ks->beta = 0;
@@ -376,6 +383,7 @@ constexpr int kDotG = 4;   // vectors whose loads are issued together
 __global__ void __launch_bounds__(kThreads) k_dcgs_reduce(const double* __restrict__ V, int64_t ldv, int j,
                                                           const double* __restrict__ W, int64_t n, double* partial,
                                                           unsigned int* counter, int nbx, KrylovState* ks) {
+    pdl_entry();
     if (ks->done) return;
     __shared__ double acc[2 * kMaxDots][kThreads / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -463,6 +471,7 @@ __global__ void __launch_bounds__(kThreads) k_dcgs_update(double* __restrict__ V
                                                           double* __restrict__ W, int64_t n, double* partial,
                                                           unsigned int* counter, int nblocks, KrylovState* ks,
                                                           int maxmv, int m, cudaGraphConditionalHandle hnext) {
+    pdl_entry();
     if (ks->done) return;
     __shared__ double cA[kMaxDots], cB[kMaxDots + 1];
     for (int v = threadIdx.x; v <= j; v += blockDim.x) { cB[v] = ks->coefB[v]; if (v < j) cA[v] = ks->coefA[v]; }
@@ -512,6 +521,7 @@ __global__ void __launch_bounds__(kThreads) k_dcgs_update(double* __restrict__ V
 }
 
 __global__ void k_solve_log(const KrylovState* ks, SolveLog* out) {
+    pdl_entry();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     out->iters = ks->iters;
     out->converged = ks->converged;
@@ -531,16 +541,16 @@ void launch_dcgs_reduce(const double* V, int64_t ldv, int j, const double* W, in
     const int cap = (int)(((int64_t)(kMaxKrylov + 2) * sc.nblocks) / (2 * (j + 1)));   // scratch rows
     if (nb > cap) nb = cap;
     if (nb < 1) nb = 1;
-    note_launch(), k_dcgs_reduce<<<nb, kThreads, 0, st>>>(V, ldv, j, W, n, sc.partial, sc.counter, nb, ks);
+    launch_k(k_dcgs_reduce, dim3(nb), dim3(kThreads), 0, st, V, ldv, j, W, n, sc.partial, sc.counter, nb, ks);
 }
 
 void launch_dcgs_update(double* V, int64_t ldv, int j, double* W, int64_t n, const DotScratch& sc, KrylovState* ks,
                         int maxmv, int m, cudaStream_t st, cudaGraphConditionalHandle hnext) {
-    note_launch(), k_dcgs_update<<<sc.nblocks, kThreads, 0, st>>>(V, ldv, j, W, n, sc.partial, sc.counter, sc.nblocks,
+    launch_k(k_dcgs_update, dim3(sc.nblocks), dim3(kThreads), 0, st, V, ldv, j, W, n, sc.partial, sc.counter, sc.nblocks,
                                                                   ks, maxmv, m, hnext);
 }
 void launch_solve_log(const KrylovState* ks, SolveLog* out, cudaStream_t st) {
-    note_launch(), k_solve_log<<<1, 32, 0, st>>>(ks, out);
+    launch_k(k_solve_log, dim3(1), dim3(32), 0, st, ks, out);
 }
 
 void launch_multidot(const double* V, int64_t ldv, int k, const double* w, int64_t n, const DotScratch& sc,
@@ -551,26 +561,26 @@ void launch_multidot(const double* V, int64_t ldv, int k, const double* w, int64
     if (nbx > need) nbx = (int)need;
     if (nbx < 1) nbx = 1;
     if (nbx > sc.nblocks) nbx = sc.nblocks;
-    note_launch(), k_multidot<<<dim3(nbx, k + 1), kThreads, 0, st>>>(V, ldv, k, w, n, sc.partial, sc.counter, nbx, ks, cond);
+    launch_k(k_multidot, dim3(dim3(nbx, k + 1)), dim3(kThreads), 0, st, V, ldv, k, w, n, sc.partial, sc.counter, nbx, ks, cond);
 }
 
 void launch_project(const double* V, int64_t ldv, int k, double* w, int64_t n, const DotScratch& sc, KrylovState* ks,
                     int cond, int maxmv, int m, cudaStream_t st) {
-    note_launch(), k_project<<<sc.nblocks, kThreads, 0, st>>>(V, ldv, k, w, n, sc.partial, sc.counter, sc.nblocks, ks, cond, maxmv, m);
+    launch_k(k_project, dim3(sc.nblocks), dim3(kThreads), 0, st, V, ldv, k, w, n, sc.partial, sc.counter, sc.nblocks, ks, cond, maxmv, m);
 }
 
 void launch_arnoldi_finish(KrylovState* ks, int maxmv, int m, cudaStream_t st) {
-    note_launch(), k_arnoldi_finish<<<1, 32, 0, st>>>(ks, maxmv, m);
+    launch_k(k_arnoldi_finish, dim3(1), dim3(32), 0, st, ks, maxmv, m);
 }
 
 void launch_norm_init(const double* v, int64_t n, const DotScratch& sc, KrylovState* ks, double rtol, double atol,
                       cudaStream_t st, cudaGraphConditionalHandle hnext) {
-    note_launch(), k_norm_init<<<sc.nblocks, kThreads, 0, st>>>(v, n, sc.partial, sc.counter, sc.nblocks, ks, rtol, atol,
+    launch_k(k_norm_init, dim3(sc.nblocks), dim3(kThreads), 0, st, v, n, sc.partial, sc.counter, sc.nblocks, ks, rtol, atol,
                                                                 hnext);
 }
 
 void launch_backsolve(KrylovState* ks, cudaStream_t st, int rotated_R) {
-    note_launch(), k_backsolve<<<1, 32, 0, st>>>(ks, rotated_R);
+    launch_k(k_backsolve, dim3(1), dim3(32), 0, st, ks, rotated_R);
 }
 
 template <typename TZ>
@@ -579,20 +589,21 @@ void launch_solution_update(double* x, const TZ* Z, int64_t ldz, int64_t n, cons
     int nb = (int)((n + kThreads - 1) / kThreads);
     if (nb > 148 * 8) nb = 148 * 8;
     if (nb < 1) nb = 1;
-    note_launch(), k_solution_update<TZ><<<nb, kThreads, 0, st>>>(x, Z, ldz, n, ks, use_scale);
+    launch_k(k_solution_update<TZ>, dim3(nb), dim3(kThreads), 0, st, x, Z, ldz, n, ks, use_scale);
 }
 template void launch_solution_update<double>(double*, const double*, int64_t, int64_t, const KrylovState*, int,
                                              cudaStream_t);
 template void launch_solution_update<float>(double*, const float*, int64_t, int64_t, const KrylovState*, int,
                                             cudaStream_t);
 
-void launch_krylov_reset(KrylovState* ks, cudaStream_t st) { note_launch(), k_krylov_reset<<<1, 32, 0, st>>>(ks); }
+void launch_krylov_reset(KrylovState* ks, cudaStream_t st) { launch_k(k_krylov_reset, dim3(1), dim3(32), 0, st, ks); }
 
 // Restart after a full subspace: keep the matvec count and the tolerance.
 __global__ void k_krylov_restart(KrylovState* ks) {
+    pdl_entry();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     ks->k = 0; ks->done = 0; ks->converged = 0; ks->reorth = 0;
 }
-void launch_krylov_restart(KrylovState* ks, cudaStream_t st) { note_launch(), k_krylov_restart<<<1, 32, 0, st>>>(ks); }
+void launch_krylov_restart(KrylovState* ks, cudaStream_t st) { launch_k(k_krylov_restart, dim3(1), dim3(32), 0, st, ks); }
 
 }  // namespace ow3d

@@ -42,6 +42,7 @@ constexpr int kCoopThreads = 512;
 
 template <typename T, bool THREE>
 __global__ void k_lo_matvec(LevelDev<T> L, const T* __restrict__ x, T* __restrict__ y) {
+    pdl_entry();
     OW3D_GRID_STRIDE(p, L.N) {
         int k, i, j;
         int64_t c;
@@ -53,11 +54,13 @@ __global__ void k_lo_matvec(LevelDev<T> L, const T* __restrict__ x, T* __restric
 
 template <typename T, bool THREE, bool CROSS>
 __global__ void k_lo_residual(LevelDev<T> L) {
+    pdl_entry();
     OW3D_GRID_STRIDE(p, L.N) residual_point<T, THREE, CROSS>(L, p);
 }
 
 template <typename T, bool THREE>
 __global__ void k_lo_bottom(LevelDev<T> L) {
+    pdl_entry();
     OW3D_GRID_STRIDE(q, (bottom_count<T, THREE>(L))) bottom_item<T, THREE>(L, q);
 }
 
@@ -67,6 +70,7 @@ __global__ void k_lo_bottom(LevelDev<T> L) {
 // brought into L1 before it solves the current group.
 template <typename T, bool THREE, int S, bool CROSS>
 __global__ void __launch_bounds__(128, 4) k_lo_colour(LevelDev<T> L, int colour, int prefetch) {
+    pdl_entry();
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t total = colour_count<T, THREE>(L);
@@ -137,6 +141,7 @@ __device__ __forceinline__ int chunk_pad(const T* p) {
 template <typename T, int S>
 __global__ void __launch_bounds__(kCTThreads, 2) k_lo_colour_tile(LevelDev<T> L, int colour, int nband, int ntx,
                                                                   TileShape<T> sh) {
+    pdl_entry();
     extern __shared__ __align__(16) unsigned char ct_smem[];
     constexpr int V = 16 / (int)sizeof(T);
     constexpr int CPW = 32 / S;                       // columns per warp
@@ -221,11 +226,13 @@ __global__ void __launch_bounds__(kCTThreads, 2) k_lo_colour_tile(LevelDev<T> L,
 
 template <typename T>
 __global__ void k_restrict(LevelDev<T> F, LevelDev<T> Cc, const T* __restrict__ rf, T* __restrict__ rc, T* __restrict__ xc) {
+    pdl_entry();
     OW3D_GRID_STRIDE(p, Cc.N) restrict_item<T>(F, Cc, rf, rc, xc, p);
 }
 
 template <typename T>
 __global__ void k_prolong_add(LevelDev<T> F, LevelDev<T> Cc, const T* __restrict__ xc, T* __restrict__ xf) {
+    pdl_entry();
     OW3D_GRID_STRIDE(p, F.N) prolong_item<T>(F, Cc, xc, xf, p);
 }
 
@@ -233,6 +240,7 @@ __global__ void k_prolong_add(LevelDev<T> F, LevelDev<T> Cc, const T* __restrict
 // this matrix with HSL MA41 once, LUfactor.f90:20-66, and solves with it).
 template <typename T>
 __global__ void k_coarse(int n, const T* __restrict__ inv, const T* __restrict__ b, T* __restrict__ x) {
+    pdl_entry();
     OW3D_GRID_STRIDE(r, n) coarse_item<T>(n, inv, b, x, (int)r);
 }
 
@@ -255,23 +263,28 @@ __device__ __forceinline__ void dense_rows(int n, const T* __restrict__ M, const
 
 template <typename T>
 __global__ void k_dense_apply(int n, const T* __restrict__ M, const T* __restrict__ b, T* __restrict__ x) {
+    pdl_entry();
     dense_rows<T>(n, M, b, x);
 }
 
 template <typename T>
 __global__ void k_scale_copy(const double* __restrict__ src, double s, T* __restrict__ dst, int64_t n) {
+    pdl_entry();
     OW3D_GRID_STRIDE(p, n) dst[p] = T(s * src[p]);
 }
 template <typename T>
 __global__ void k_scale_copy_dev(const double* __restrict__ src, const double* __restrict__ ds, T* __restrict__ dst, int64_t n) {
+    pdl_entry();
     const double s = ds ? *ds : 1.0;
     OW3D_GRID_STRIDE(p, n) dst[p] = T(s * src[p]);
 }
 __global__ void k_convert(const float* __restrict__ src, double* __restrict__ dst, int64_t n) {
+    pdl_entry();
     OW3D_GRID_STRIDE(p, n) dst[p] = (double)src[p];
 }
 template <typename T>
 __global__ void k_fill(T* __restrict__ dst, T v, int64_t n) {
+    pdl_entry();
     OW3D_GRID_STRIDE(p, n) dst[p] = v;
 }
 
@@ -414,8 +427,8 @@ inline int nblk(int64_t n, int t = 256) {
 
 template <typename T>
 void launch_lo_matvec(const LevelDev<T>& L, const T* x, T* y, cudaStream_t st) {
-    if (L.Nyg > 1) note_launch(), k_lo_matvec<T, true><<<nblk(L.N), 256, 0, st>>>(L, x, y);
-    else note_launch(), k_lo_matvec<T, false><<<nblk(L.N), 256, 0, st>>>(L, x, y);
+    if (L.Nyg > 1) launch_k(k_lo_matvec<T, true>, dim3(nblk(L.N)), dim3(256), 0, st, L, x, y);
+    else launch_k(k_lo_matvec<T, false>, dim3(nblk(L.N)), dim3(256), 0, st, L, x, y);
 }
 
 // Tiled colour pass for the levels it covers (see k_lo_colour_tile); false
@@ -444,7 +457,7 @@ static bool colour_tile_launch(const LevelDev<T>& L, int c, cudaStream_t st) {
     }
     const int per_block = (kCTThreads / 32) * (32 / S);
     const int nband = (mgdev::wall_band_count(L) + per_block - 1) / per_block;
-    note_launch(), k_lo_colour_tile<T, S><<<nband + ntx * nty, kCTThreads, sh.bytes, st>>>(L, c, nband, ntx, sh);
+    launch_k(k_lo_colour_tile<T, S>, dim3(nband + ntx * nty), dim3(kCTThreads), sh.bytes, st, L, c, nband, ntx, sh);
     return true;
 }
 
@@ -462,8 +475,8 @@ static void colour_launch(const LevelDev<T>& L, int c, cudaStream_t st) {
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
     const int pre = pf == 1 ? 1 : 0;
-    if (L.cross) note_launch(), k_lo_colour<T, THREE, S, true><<<(int)blocks, 128, 0, st>>>(L, c, pre);
-    else note_launch(), k_lo_colour<T, THREE, S, false><<<(int)blocks, 128, 0, st>>>(L, c, pre);
+    if (L.cross) launch_k(k_lo_colour<T, THREE, S, true>, dim3((int)blocks), dim3(128), 0, st, L, c, pre);
+    else launch_k(k_lo_colour<T, THREE, S, false>, dim3((int)blocks), dim3(128), 0, st, L, c, pre);
 }
 // Lanes per column of the two-rows-per-lane pass.
 inline int seg_width2(int Nzg) {
@@ -492,8 +505,8 @@ template <typename T>
 static void bottoms(const LevelDev<T>& L, cudaStream_t st) {
     const int64_t nyi = L.Nyg > 1 ? L.Nyg - 2 : 1;
     const int64_t n = (int64_t)(L.Nxg - 2) * nyi + 2 * nyi + (L.Nyg > 1 ? 2 * (int64_t)(L.Nxg - 2) : 0);
-    if (L.Nyg > 1) note_launch(), k_lo_bottom<T, true><<<nblk(n), 256, 0, st>>>(L);
-    else note_launch(), k_lo_bottom<T, false><<<nblk(n), 256, 0, st>>>(L);
+    if (L.Nyg > 1) launch_k(k_lo_bottom<T, true>, dim3(nblk(n)), dim3(256), 0, st, L);
+    else launch_k(k_lo_bottom<T, false>, dim3(nblk(n)), dim3(256), 0, st, L);
 }
 
 template <typename T>
@@ -514,31 +527,31 @@ void launch_lo_smooth(const LevelDev<T>& L, int nu, cudaStream_t st) {
 
 template <typename T>
 void launch_restrict(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* rf, T* rc, cudaStream_t st) {
-    note_launch(), k_restrict<T><<<nblk(Cc.N), 256, 0, st>>>(F, Cc, rf, rc, Cc.xv);
+    launch_k(k_restrict<T>, dim3(nblk(Cc.N)), dim3(256), 0, st, F, Cc, rf, rc, Cc.xv);
 }
 template <typename T>
 void launch_prolong_add(const LevelDev<T>& F, const LevelDev<T>& Cc, const T* xc, T* xf, cudaStream_t st) {
-    note_launch(), k_prolong_add<T><<<nblk(F.N), 256, 0, st>>>(F, Cc, xc, xf);
+    launch_k(k_prolong_add<T>, dim3(nblk(F.N)), dim3(256), 0, st, F, Cc, xc, xf);
 }
 template <typename T>
 void launch_coarse_solve(const LevelDev<T>& Lc, const T* inv, cudaStream_t st) {
     int n = (int)Lc.N;
-    note_launch(), k_coarse<T><<<(n + 127) / 128, 128, 0, st>>>(n, inv, Lc.bv, Lc.xv);
+    launch_k(k_coarse<T>, dim3((n + 127) / 128), dim3(128), 0, st, n, inv, Lc.bv, Lc.xv);
 }
 template <typename T>
 void launch_scale_copy(const double* src, double s, T* dst, int64_t n, cudaStream_t st) {
-    note_launch(), k_scale_copy<T><<<nblk(n), 256, 0, st>>>(src, s, dst, n);
+    launch_k(k_scale_copy<T>, dim3(nblk(n)), dim3(256), 0, st, src, s, dst, n);
 }
 template <typename T>
 void launch_fill(T* dst, T v, int64_t n, cudaStream_t st) {
-    note_launch(), k_fill<T><<<nblk(n), 256, 0, st>>>(dst, v, n);
+    launch_k(k_fill<T>, dim3(nblk(n)), dim3(256), 0, st, dst, v, n);
 }
 template <typename T>
 void launch_scale_copy_dev(const double* src, const double* ds, T* dst, int64_t n, cudaStream_t st) {
-    note_launch(), k_scale_copy_dev<T><<<nblk(n), 256, 0, st>>>(src, ds, dst, n);
+    launch_k(k_scale_copy_dev<T>, dim3(nblk(n)), dim3(256), 0, st, src, ds, dst, n);
 }
 void launch_convert(const float* src, double* dst, int64_t n, cudaStream_t st) {
-    note_launch(), k_convert<<<nblk(n), 256, 0, st>>>(src, dst, n);
+    launch_k(k_convert, dim3(nblk(n)), dim3(256), 0, st, src, dst, n);
 }
 
 template <typename T>
@@ -547,7 +560,7 @@ void launch_dense_apply(const LevelDev<T>& L, const T* M, cudaStream_t st) {
     const int warps_per_block = 8;
     int blocks = (n + warps_per_block - 1) / warps_per_block;
     if (blocks > 148 * 8) blocks = 148 * 8;
-    note_launch(), k_dense_apply<T><<<blocks, 32 * warps_per_block, 0, st>>>(n, M, L.bv, L.xv);
+    launch_k(k_dense_apply<T>, dim3(blocks), dim3(32 * warps_per_block), 0, st, n, M, L.bv, L.xv);
 }
 
 // Block count of the fused coarse kernel: 0 = one block per SM, else at most
@@ -565,6 +578,8 @@ std::atomic<int> g_tail_cluster{16};
 // launcher).
 std::atomic<int> g_colour_tiles{0};
 std::atomic<int> g_colour_prefetch{0};
+// Programmatic dependent launch between the solver-path kernels (launch_k).
+std::atomic<int> g_pdl{1};
 
 thread_local bool g_capture_unsafe = false;
 
@@ -712,11 +727,11 @@ static void vcycle(LevelDev<T>* lev, int l, int lc, int ld, const T* M, int nu1,
     LevelDev<T>& Cc = lev[l - 1];
     launch_lo_smooth(F, nu1, st);
     if (F.Nyg > 1) {
-        if (F.cross) note_launch(), k_lo_residual<T, true, true><<<nblk(F.N), 256, 0, st>>>(F);
-        else note_launch(), k_lo_residual<T, true, false><<<nblk(F.N), 256, 0, st>>>(F);
+        if (F.cross) launch_k(k_lo_residual<T, true, true>, dim3(nblk(F.N)), dim3(256), 0, st, F);
+        else launch_k(k_lo_residual<T, true, false>, dim3(nblk(F.N)), dim3(256), 0, st, F);
     } else {
-        if (F.cross) note_launch(), k_lo_residual<T, false, true><<<nblk(F.N), 256, 0, st>>>(F);
-        else note_launch(), k_lo_residual<T, false, false><<<nblk(F.N), 256, 0, st>>>(F);
+        if (F.cross) launch_k(k_lo_residual<T, false, true>, dim3(nblk(F.N)), dim3(256), 0, st, F);
+        else launch_k(k_lo_residual<T, false, false>, dim3(nblk(F.N)), dim3(256), 0, st, F);
     }
     launch_restrict(F, Cc, (const T*)F.rv, Cc.bv, st);   // also zeroes Cc.xv
     vcycle(lev, l - 1, lc, ld, M, nu1, nu2, pack, st);

@@ -1193,6 +1193,7 @@ int ow3d_test_set_colour_prefetch(int mode) { return g_colour_prefetch.exchange(
 long long ow3d_test_set_tail_max_points(long long points) {
     return g_tail_max_points.exchange(points < 0 ? 0 : (int64_t)points);
 }
+int ow3d_test_set_pdl(int on) { return g_pdl.exchange(on ? 1 : 0); }
 int ow3d_test_set_tail_cluster(int blocks) { return g_tail_cluster.exchange(blocks < 0 ? 0 : blocks); }
 long long ow3d_test_set_coop_max_points(long long points) {
     return g_coop_max_points.exchange(points < 0 ? 0 : (int64_t)points);

@@ -8,6 +8,7 @@
 // Ghost points are included (one layer in x, y and below the bottom).
 #pragma once
 #include <atomic>
+#include <utility>
 #include <cstdint>
 #include <cstddef>
 #include <cstdio>
@@ -26,10 +27,44 @@ extern std::atomic<int64_t> g_tail_max_points;
 extern std::atomic<int> g_tail_cluster;
 extern std::atomic<int> g_colour_tiles;
 extern std::atomic<int> g_colour_prefetch;
+
 // Set (on the capturing thread) when a launch sequence under stream capture
 // issued a host-to-device copy whose source the host later overwrites.
 extern thread_local bool g_capture_unsafe;
 inline void note_launch() { g_kernel_launches.fetch_add(1ull, std::memory_order_relaxed); }
+
+// Programmatic dependent launch on the solver path: a kernel launched by
+// launch_k may start (its blocks resident, its launch latency spent) while
+// the kernel before it on the stream finishes; it waits at pdl_entry for
+// that kernel to complete and its writes to be visible, before touching any
+// memory, and lets its own successor start as soon as all its blocks run.
+// g_pdl = 0 launches plainly (the wait is then a no-op).
+extern std::atomic<int> g_pdl;
+#ifdef __CUDACC__
+__device__ __forceinline__ void pdl_entry() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+template <typename... KArgs, typename... Args>
+inline void launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args&&... args) {
+    note_launch();
+    if (g_pdl.load(std::memory_order_relaxed)) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = grid;
+        cfg.blockDim = block;
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+    } else {
+        kernel<<<grid, block, smem, st>>>(std::forward<Args>(args)...);
+    }
+}
+#endif  // __CUDACC__
 
 constexpr int kMaxLevels = 16;
 constexpr int kMaxKrylov = 64;     // maximum GMRESmaxiterations
