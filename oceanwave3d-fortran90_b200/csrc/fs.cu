@@ -64,7 +64,9 @@ __global__ void k_pd_rhs(PDampDev d, int Nxg, const double* E, const double* P) 
         const double* w = d.D1 + (size_t)i * R;
         double acc = 0.0;
         for (int m = 0; m < R; ++m) acc += p0[s + m] * w[m];
-        d.f[i] = d.gamPhi[d.i1 - 1 + i] * acc;
+        // the damping acts on the velocity relative to the constant-flux
+        // current, Ur = Q / h at the east wall (funPressureTerm.f90:249-252)
+        d.f[i] = d.gamPhi[d.i1 - 1 + i] * (acc - d.Ur);
     }
     for (int i = threadIdx.x; i < Nxg; i += blockDim.x) d.NuD[i] = -d.gamEta[i] * E[i];
     __syncthreads();

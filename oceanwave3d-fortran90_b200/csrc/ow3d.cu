@@ -730,6 +730,7 @@ int create_impl(const ow3d_params* p, const double* h, const double* hx, const d
         PDampDev& d = H->pd;
         const PDampHost& ph = H->pd_h;
         d.type = ph.type; d.i1 = ph.i1; d.nd = ph.nd; d.rank = ph.rank;
+        d.Ur = p->current_flag ? p->current_Q / G.h[(size_t)G.Nxg - 2] : 0.0;
         double *gp, *ge;
         TRY(upload(H.get(), &gp, ph.gamPhi)); TRY(upload(H.get(), &ge, ph.gamEta));
         d.gamPhi = gp; d.gamEta = ge;
@@ -1189,7 +1190,7 @@ unsigned long long ow3d_launch_count(void) { return g_kernel_launches.load(std::
 
 int ow3d_test_set_coarse_blocks(int blocks) { return g_coarse_blocks.exchange(blocks < 0 ? 0 : blocks); }
 int ow3d_test_set_colour_tiles(int min_tiles) { return g_colour_tiles.exchange(min_tiles < 0 ? 0 : min_tiles); }
-int ow3d_test_set_colour_prefetch(int mode) { return g_colour_prefetch.exchange(mode < 0 ? 0 : mode); }
+int ow3d_test_set_colour_prefetch(int mode) { return g_colour_prefetch.exchange(mode < 0 ? -1 : mode); }
 long long ow3d_test_set_tail_max_points(long long points) {
     return g_tail_max_points.exchange(points < 0 ? 0 : (int64_t)points);
 }

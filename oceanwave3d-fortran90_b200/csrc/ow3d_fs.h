@@ -72,6 +72,7 @@ struct PDampDev {
     const double* Linv;      // nd x nd inverse of the zone matrix, row-major (type 0)
     double *f, *r, *x;       // nd each: gamma * phi_x, the zone right-hand side, its solution
     double *NuD, *Pd;        // Nxg each: the kinematic and dynamic damping terms
+    double Ur;               // the current's velocity at the east wall (0 without one)
 };
 
 // The roller breaking model of an x flume (DetectBreaking.f90). Columns are

@@ -1362,7 +1362,7 @@ static void pressure_term(Sim& s, const vector<double>& E, const vector<double>&
         vector<double> tmp(nd), rhs(nd);
         for (int i = 1; i <= nd; ++i) tmp[i - 1] = P[id0 + i - 2];
         pd_dfdx(s, tmp, rhs);
-        for (int i = 1; i <= nd; ++i) tmp[i - 1] = s.gamPhi[id0 + i - 2] * (rhs[i - 1] - 0.0);   // no current
+        for (int i = 1; i <= nd; ++i) tmp[i - 1] = s.gamPhi[id0 + i - 2] * (rhs[i - 1] - s.Ur);   // relative to the current
         pd_dfdx(s, tmp, rhs);
         rhs[0] = P[id0 - 1]; rhs[nd - 1] = 0.0;
         const double* A = s.pdLU.data();
