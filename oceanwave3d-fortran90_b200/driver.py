@@ -48,8 +48,9 @@ class Setup:
         self.paddle = paddle            # flux wavemaker: (dt, y, flux) or None
 
 
-def prepare(deck, deck_dir=None):
-    """Host set-up of a deck (a path or a Params)."""
+def prepare(deck, deck_dir=None, steps=None):
+    """Host set-up of a deck (a path or a Params). steps: the time steps the
+    targets must cover (default: the deck's Nsteps)."""
     notes = []
     if isinstance(deck, capi.Params):
         p = deck
@@ -113,7 +114,8 @@ def prepare(deck, deck_dir=None):
                 i0, i1, j0, j1 = zone_box(p, z)
                 x = (np.arange(Nxg) - (1 if p.Nx > 1 else 0)) * (p.Lx / max(p.Nx - 1, 1))
                 xs = x[i0 - 1:i1]
-                nt = 2 * max(p.Nsteps, 1) + 2 + int(np.ceil(2 * max(p.time0, 0.0) / p.dt))
+                nsteps = max(p.Nsteps, 1) if steps is None else int(steps) + 1
+                nt = 2 * nsteps + 2 + int(np.ceil(2 * max(p.time0, 0.0) / p.dt))
                 line = [stream_function_wave(p, xs, n * 0.5 * p.dt)[:2] for n in range(nt)]
                 rows = j1 - j0 + 1
                 eta = np.array([np.tile(e, rows) for e, _ in line])
@@ -142,7 +144,7 @@ def run(deck, outdir=None, steps=None, backend=Simulation, deck_dir=None):
     default). Returns the simulation (still open: close it when done), the
     setup and the worst step status (1: some solve reached the matvec limit,
     which the reference accepts silently)."""
-    s = prepare(deck, deck_dir)
+    s = prepare(deck, deck_dir, steps)
     p = s.params
     sim = backend(p, **s.geometry)
     sim.set_state(s.E0, s.P0, t=p.time0)

@@ -94,6 +94,25 @@ def test_reference_decks_run_on_oracle(ow3d, oracle, name):
     assert st >= 0 and np.all(np.isfinite(E)) and np.max(np.abs(E)) < 5 * H, (name, np.max(np.abs(E)))
 
 
+@pytest.mark.skipif(not REF.is_dir(), reason="reference example decks not on this machine")
+@pytest.mark.parametrize("name", ["SFWaveAndFollowingCurrent", "SFWaveAndOpposingCurrent"])
+def test_reference_current_decks_run_on_oracle(ow3d, oracle, tmp_path, name):
+    """The stream-function wave on a following and an opposing current
+    (IncWaveType 4): a hot start from the deck's own .init file (copied to
+    the OceanWave3D.init the reference reads), the current's flux, the
+    pressure-damping zone relative to it and the local smoothing (deck line
+    2 gives 1 g), two steps on the oracle with bounded surfaces."""
+    import shutil
+    from ow3d_b200 import driver
+    shutil.copy(REF / f"OceanWave3D.inp.{name}", tmp_path / "case.inp")
+    shutil.copy(REF / f"{name}.init", tmp_path / "OceanWave3D.init")
+    sim, s, st = driver.run(tmp_path / "case.inp", steps=2, backend=_oracle_backend(oracle))
+    p = s.params
+    assert (p.IncWaveType, p.current_flag, p.PDampingONOFF) == (1, 1, 1) and p.accel_tol_fact == 1.0
+    E = sim.get_state()[0]
+    assert st >= 0 and np.all(np.isfinite(E)) and np.max(np.abs(E)) < 5 * p.sf_H
+
+
 @pytest.mark.gpu
 def test_run_on_device_matches_oracle_and_writes_files(ow3d, oracle, tmp_path):
     from ow3d_b200 import driver
