@@ -571,6 +571,12 @@ const char* ow3d_version(void);
 
 /* ------------------------------------------------------ measurement */
 
+/* The multigrid hierarchy of a handle (MGPreProcess.f90:95-215): the number
+ * of levels, and level `level`'s interior sizes (0 = coarsest) and the
+ * colours of its Gauss-Seidel smoother (2, or 4 with mixed-derivative terms). */
+int ow3d_level_count(const ow3d_handle* h);
+int ow3d_level_dims(const ow3d_handle* h, int level, int* Nx, int* Ny, int* Nz, int* ncolor);
+
 /* Number of kernels this library has launched since it was loaded, over all
  * handles and threads (the cooperative coarse-grid kernel counts as one). */
 unsigned long long ow3d_launch_count(void);

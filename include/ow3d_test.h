@@ -14,8 +14,6 @@
 extern "C" {
 #endif
 
-int ow3d_test_level_count(const ow3d_handle* h);
-int ow3d_test_level_dims(const ow3d_handle* h, int level, int* Nx, int* Ny, int* Nz, int* ncolor);
 /* n deviates of the incident-wave generator (Park-Miller with the
  * Bays-Durham shuffle, RAN1_b.f90) started from idum, and the final idum. */
 int ow3d_test_ran1(int idum, int n, float* out, int* idum_out);

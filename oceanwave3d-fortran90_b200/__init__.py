@@ -52,11 +52,11 @@ def lib():
         L.ow3d_bench_kernel.argtypes = [_C.c_void_p, _C.c_int, _C.c_int, D]
         L.ow3d_launch_count.argtypes = []
         L.ow3d_launch_count.restype = _C.c_ulonglong
-        if not hasattr(L, "ow3d_test_level_count"):   # the product build: no probes
+        L.ow3d_level_count.argtypes = [_C.c_void_p]
+        L.ow3d_level_dims.argtypes = [_C.c_void_p, _C.c_int] + [_C.POINTER(_C.c_int)] * 4
+        if not hasattr(L, "ow3d_test_stencils"):   # the product build: no probes
             _lib = L
             return _lib
-        L.ow3d_test_level_count.argtypes = [_C.c_void_p]
-        L.ow3d_test_level_dims.argtypes = [_C.c_void_p, _C.c_int] + [_C.POINTER(_C.c_int)] * 4
         L.ow3d_test_stencils.argtypes = [_C.c_void_p, D, D, D]
         L.ow3d_test_surface_derivs.argtypes = [_C.c_void_p, D, D]
         L.ow3d_test_ran1.argtypes = [_C.c_int, _C.c_int, _C.POINTER(_C.c_float), _C.POINTER(_C.c_int)]
@@ -438,11 +438,11 @@ class Simulation:
 
     # ---- probes (include/ow3d_test.h)
     def level_count(self):
-        return lib().ow3d_test_level_count(self.h)
+        return lib().ow3d_level_count(self.h)
 
     def level_dims(self, l):
         a, b, c, d = (_C.c_int() for _ in range(4))
-        _check(lib().ow3d_test_level_dims(self.h, l, _C.byref(a), _C.byref(b), _C.byref(c), _C.byref(d)), "level_dims")
+        _check(lib().ow3d_level_dims(self.h, l, _C.byref(a), _C.byref(b), _C.byref(c), _C.byref(d)), "level_dims")
         return a.value, b.value, c.value, d.value
 
     def level_size(self, l):

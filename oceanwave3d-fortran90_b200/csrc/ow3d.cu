@@ -2113,9 +2113,9 @@ const char* ow3d_version(void) { return "ow3d-b200 0.1 (sm_100a)"; }
 const char* ow3d_last_error(void) { return g_last_error.c_str(); }
 
 // --------------------------------------------------------- test hooks
-int ow3d_test_level_count(const ow3d_handle* H) { return H ? H->nlev : -1; }
+int ow3d_level_count(const ow3d_handle* H) { return H ? H->nlev : -1; }
 
-int ow3d_test_level_dims(const ow3d_handle* H, int l, int* Nx, int* Ny, int* Nz, int* ncolor) {
+int ow3d_level_dims(const ow3d_handle* H, int l, int* Nx, int* Ny, int* Nz, int* ncolor) {
     if (!H || l < 0 || l >= H->nlev) return OW3D_ERR_BAD_INPUT;
     const LevelHost& L = H->G.levels[l];
     *Nx = L.Nx; *Ny = L.Ny; *Nz = L.Nz; *ncolor = L.ncolor;
