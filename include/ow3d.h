@@ -60,6 +60,9 @@ extern "C" {
                                        preconditioned residual (SPARSKIT2 semantics
                                        used by iterative_solution.f90:23-24)            */
 
+#define OW3D_SMOOTHER_MULTICOLOUR     0   /* multicolour column Gauss-Seidel (default)  */
+#define OW3D_SMOOTHER_LEXICOGRAPHIC   1   /* the reference's row order (GaussSeidel.f90) */
+
 #define OW3D_MAX_ZONES          8
 #define OW3D_MAX_KIN_FILES     20   /* kinematics output slices (ReadInputFileParameters.f90:305) */
 
@@ -448,6 +451,26 @@ int ow3d_set_paddle_signal(ow3d_handle* h, int nt, int n2, double dt, const doub
  * 10-30% slower with it, so the default is off. Results are bitwise the same
  * either way. Drops the handle's captured graphs. */
 int ow3d_set_coarse_cluster(ow3d_handle* h, int on);
+
+/* Row order of the multigrid smoother's Gauss-Seidel steps.
+ * OW3D_SMOOTHER_MULTICOLOUR (default): interior columns in 2 or 4 colour
+ * classes, each column bottom to top with the ghost and bottom rows it
+ * borders -- a different ordering of the same relaxations, with about the
+ * reference's smoothing per step, that runs in parallel.
+ * OW3D_SMOOTHER_LEXICOGRAPHIC: the reference's order on every level, which
+ * gives the reference's iterates up to rounding: the special rows (bottom and
+ * lateral ghost rows, MGPreProcess.f90:376-439), then per smoothing step a
+ * sweep over all rows in index order and the special rows again
+ * (GaussSeidel.f90:15-26, GaussSeidelSpecialPoints.f90:43-53,
+ * MultiGridSolver.f90:118-126,174-181), run as wavefronts in one thread block
+ * per sweep; the V cycle then descends to the coarsest level's inverse on
+ * every application (no fused coarse cycle, no dense sub-cycle operator).
+ * Together with krylov = OW3D_KRYLOV_LGMRES this is the reference's
+ * preconditioned solver. Many times slower than the default: meant for
+ * checking results against the reference, not for production runs. Drops the
+ * handle's captured graphs. Replaces: the smoother choice of
+ * MultiGridSolver.f90 (the reference has only the lexicographic order). */
+int ow3d_set_smoother_order(ow3d_handle* h, int order);
 
 /* The rollers of the roller breaking model (i_breaking > 0, Ny = 1) after
  * the last completed step, as the reference writes them to roller.dat each

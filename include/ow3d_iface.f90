@@ -34,6 +34,7 @@ MODULE ow3d_iface
   INTEGER(c_int), PARAMETER :: OW3D_ERR_BAD_INPUT = -1, OW3D_ERR_CUDA = -2, OW3D_ERR_OOM = -3
   INTEGER(c_int), PARAMETER :: OW3D_ERR_UNSTABLE = -4, OW3D_ERR_TIMEOUT = -5, OW3D_ERR_NO_DEVICE = -6
   INTEGER(c_int), PARAMETER :: OW3D_ERR_IO = -7, OW3D_ERR_UNSUPPORTED = -8
+  INTEGER(c_int), PARAMETER :: OW3D_SMOOTHER_MULTICOLOUR = 0, OW3D_SMOOTHER_LEXICOGRAPHIC = 1
 
   ! ow3d_params mirrors the deck (include/ow3d.h); filled by ow3d_read_deck
   ! and opaque to Fortran
@@ -164,6 +165,14 @@ MODULE ow3d_iface
        INTEGER(c_int), VALUE :: nt, n2
        REAL(c_double), VALUE :: dt
        REAL(c_double), DIMENSION(*), INTENT(IN) :: y, flux
+     END FUNCTION
+
+     ! Gauss-Seidel row order of the multigrid smoother: OW3D_SMOOTHER_LEXICOGRAPHIC
+     ! gives the reference's own order (with krylov = 1, its solver's iterates)
+     INTEGER(c_int) FUNCTION ow3d_set_smoother_order(handle, order) BIND(C, name="ow3d_set_smoother_order")
+       IMPORT :: c_int, c_ptr
+       TYPE(c_ptr), VALUE :: handle
+       INTEGER(c_int), VALUE :: order
      END FUNCTION
 
      ! the reference's output schedule (StoreDataONOFF of the deck): EP_#####.bin

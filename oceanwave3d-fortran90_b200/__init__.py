@@ -353,6 +353,12 @@ class Simulation:
         _check(lib().ow3d_test_relax_target(self.h, zone, _d(e), _d(f)), "ow3d_test_relax_target")
         return e.reshape(nt, box), f.reshape(nt, box)
 
+    def set_smoother_order(self, order):
+        """Row order of the multigrid smoother (ow3d_set_smoother_order):
+        capi.SMOOTHER_MULTICOLOUR (default) or capi.SMOOTHER_LEXICOGRAPHIC,
+        the reference's order."""
+        _check(lib().ow3d_set_smoother_order(self.h, int(order)), "ow3d_set_smoother_order")
+
     def set_paddle_signal(self, dt, y, flux):
         """Install the flux wavemaker's signal: flux (nt, n2) at y every dt
         (ow3d_set_paddle_signal)."""

@@ -21,6 +21,8 @@ PREC_FP64 = 0
 PREC_MIXED = 1
 KRYLOV_FGMRES = 0
 KRYLOV_LGMRES = 1
+SMOOTHER_MULTICOLOUR = 0
+SMOOTHER_LEXICOGRAPHIC = 1
 MAX_ZONES = 8
 MAX_KIN_FILES = 20
 
@@ -179,6 +181,7 @@ def declare(lib):
         "ow3d_reset_stats": (C.c_int, [H]),
         "ow3d_set_graphs": (C.c_int, [H, C.c_int]),
         "ow3d_set_coarse_cluster": (C.c_int, [H, C.c_int]),
+        "ow3d_set_smoother_order": (C.c_int, [H, C.c_int]),
         "ow3d_read_paddle_signal": (C.c_int, [C.c_char_p, C.c_int, _D, _I, _I, _D, _D]),
         "ow3d_set_paddle_signal": (C.c_int, [H, C.c_int, C.c_int, C.c_double, _D, _D]),
         "ow3d_zone_box": (C.c_int, [H, C.c_int, _I, _I, _I, _I]),

@@ -15,7 +15,8 @@
 // borders -- so the reference's special rows (iGhost, MGPreProcess.f90:376-439,
 // relaxed by GaussSeidelSpecialPoints around each sweep in
 // MultiGridSolver.f90:118-126,174-181) are relaxed inside the colour passes
-// instead of in separate strided passes.
+// instead of in separate strided passes. A handle may ask for the reference's
+// own lexicographic order instead (mg_lex.cu, ow3d_set_smoother_order).
 //
 // Levels with few points run inside one cooperative kernel (k_mg_coarse_cycle)
 // that executes the phases of every coarse level back to back with grid-wide
@@ -729,7 +730,8 @@ static void vcycle(LevelDev<T>* lev, int l, int lc, int ld, const T* M, int nu1,
     }
     const LevelDev<T>& F = lev[l];
     LevelDev<T>& Cc = lev[l - 1];
-    launch_lo_smooth(F, nu1, st);
+    if (pack.lex) launch_lo_smooth_lex(F, nu1, st);
+    else launch_lo_smooth(F, nu1, st);
     if (F.Nyg > 1) {
         if (F.cross) launch_k(k_lo_residual<T, true, true>, dim3(nblk(F.N)), dim3(256), 0, st, F);
         else launch_k(k_lo_residual<T, true, false>, dim3(nblk(F.N)), dim3(256), 0, st, F);
@@ -740,7 +742,8 @@ static void vcycle(LevelDev<T>* lev, int l, int lc, int ld, const T* M, int nu1,
     launch_restrict(F, Cc, (const T*)F.rv, Cc.bv, st);   // also zeroes Cc.xv
     vcycle(lev, l - 1, lc, ld, M, nu1, nu2, pack, st);
     launch_prolong_add(F, Cc, (const T*)Cc.xv, F.xv, st);
-    launch_lo_smooth(F, nu2, st);
+    if (pack.lex) launch_lo_smooth_lex(F, nu2, st);
+    else launch_lo_smooth(F, nu2, st);
 }
 
 // One V cycle from level l (its b set, its x zeroed by the caller) down to the
@@ -748,7 +751,7 @@ static void vcycle(LevelDev<T>* lev, int l, int lc, int ld, const T* M, int nu1,
 template <typename T>
 void launch_mg_subcycle(LevelDev<T>* lev, int nlev, int l, int ld, const T* M, int nu1, int nu2, LevelTable<T>& pack,
                         cudaStream_t st) {
-    const int lc = (nlev > 1) ? coop_level(lev, nlev) : -1;
+    const int lc = (nlev > 1 && !pack.lex) ? coop_level(lev, nlev) : -1;
     vcycle(lev, l, lc, ld, M, nu1, nu2, pack, st);
 }
 
@@ -758,7 +761,7 @@ void launch_mg_vcycle(LevelDev<T>* lev, int nlev, const T* M, int ld, int nu1, i
                       cudaStream_t st) {
     LevelDev<T>& F = lev[nlev - 1];
     launch_fill<T>(F.xv, T(0), F.N, st);
-    const int lc = (nlev > 1) ? coop_level(lev, nlev) : -1;
+    const int lc = (nlev > 1 && !pack.lex) ? coop_level(lev, nlev) : -1;
     for (int it = 1; it <= maxit; ++it) {
         if (nlev == 1 && it > 1) break;
         vcycle(lev, nlev - 1, lc, ld, M, nu1, nu2, pack, st);

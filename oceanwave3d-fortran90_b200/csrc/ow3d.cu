@@ -438,7 +438,10 @@ void run_precond(ow3d_handle* H, MgSet<T>& S, const double* src, const double* d
     LevelDev<T>& F = lev[L - 1];
     launch_scale_copy_dev<T>(src, dscale, S.fine_b, F.N, H->st);
     F.xv = out;
-    launch_mg_vcycle<T>(lev, L, S.dense_op, S.dense_level, H->p.nu1, H->p.nu2, H->p.maxit, S.table, H->st);
+    if (S.table.lex)  // the recursion to the coarsest level, as the reference runs it
+        launch_mg_vcycle<T>(lev, L, S.coarse_inv, 0, H->p.nu1, H->p.nu2, H->p.maxit, S.table, H->st);
+    else
+        launch_mg_vcycle<T>(lev, L, S.dense_op, S.dense_level, H->p.nu1, H->p.nu2, H->p.maxit, S.table, H->st);
 }
 
 // Apply M^{-1} to src (times *dscale) into the FP64 vector dst.
@@ -1156,7 +1159,12 @@ int level_op_t(ow3d_handle* H, MgSet<T>& S, int l, int op, int nu, const double*
         if (!r) { launch_lo_matvec<T>(Lv, a, b, H->st); cudaStreamSynchronize(H->st); r = get(out, b, n); }
     } else if (op == 1) {  // smoothing: x <- S(x, b), nu steps
         r = put(a, in1, n); if (!r) r = put(b, in2, n);
-        if (!r) { Lv.xv = a; Lv.bv = b; launch_lo_smooth<T>(Lv, nu, H->st); cudaStreamSynchronize(H->st); r = get(out, a, n); }
+        if (!r) {
+            Lv.xv = a; Lv.bv = b;
+            if (S.table.lex) launch_lo_smooth_lex<T>(Lv, nu, H->st);
+            else launch_lo_smooth<T>(Lv, nu, H->st);
+            cudaStreamSynchronize(H->st); r = get(out, a, n);
+        }
     } else if (op == 2 && l > 0) {  // restriction of a fine residual to level l-1
         LevelDev<T> Cc = S.lev[l - 1];
         r = put(a, in1, n);
@@ -2079,6 +2087,21 @@ int ow3d_set_coarse_cluster(ow3d_handle* H, int on) {
     H->mg64.table.cluster = c;
     H->mg32.table.cluster = c;
     // the captured launches hold the other coarse kernel
+    drop_step_graphs(H);
+    for (auto& g : H->iter_graphs) cudaGraphExecDestroy(g.exec);
+    H->iter_graphs.clear();
+    return OW3D_OK;
+}
+
+int ow3d_set_smoother_order(ow3d_handle* H, int order) {
+    if (!H || (order != OW3D_SMOOTHER_MULTICOLOUR && order != OW3D_SMOOTHER_LEXICOGRAPHIC)) return OW3D_ERR_BAD_INPUT;
+    const bool lx = order == OW3D_SMOOTHER_LEXICOGRAPHIC;
+    if (H->mg64.table.lex == lx && H->mg32.table.lex == lx) return OW3D_OK;
+    CK(cudaSetDevice(H->dev));
+    CK(cudaStreamSynchronize(H->st));
+    H->mg64.table.lex = lx;
+    H->mg32.table.lex = lx;
+    // the captured launches hold the other smoother
     drop_step_graphs(H);
     for (auto& g : H->iter_graphs) cudaGraphExecDestroy(g.exec);
     H->iter_graphs.clear();

@@ -237,6 +237,10 @@ struct LevelTable {
     // the whole fused coarse cycle in one thread-block cluster instead of a
     // cooperative grid over every SM (ow3d_set_coarse_cluster)
     bool cluster = false;
+    // Gauss-Seidel in the reference's lexicographic order on every level
+    // (ow3d_set_smoother_order): no fused coarse cycle, no dense sub-cycle
+    // operator (the V cycle descends to the coarsest level's inverse)
+    bool lex = false;
 };
 
 // M: dense operator of level ld (the coarsest level's inverse when ld = 0).
@@ -252,6 +256,9 @@ template <typename T>
 void launch_lo_matvec(const LevelDev<T>& L, const T* x, T* y, cudaStream_t st);
 template <typename T>
 void launch_lo_smooth(const LevelDev<T>& L, int nu, cudaStream_t st);
+// the same smoothing steps in the reference's lexicographic order (mg_lex.cu)
+template <typename T>
+void launch_lo_smooth_lex(const LevelDev<T>& L, int nu, cudaStream_t st);
 // One smoother phase: colour pass `colour`, or the bottom-row pass (colour < 0).
 template <typename T>
 void launch_lo_pass(const LevelDev<T>& L, int colour, cudaStream_t st);
