@@ -34,8 +34,15 @@ CASES = [
     (cases.bump_3d, dict(Nx=17, Ny=9, Nz=9)),
     (cases.bump_3d, dict(Nx=33, Ny=17, Nz=9)),
     (cases.bump_3d, dict(Nx=65, Ny=33, Nz=9, amp=0.0)),
+    # finest level above the shared-memory size: a thread-block cluster
+    (cases.bump_3d, dict(Nx=129, Ny=33, Nz=9)),
+    # finest level whose window does not fit a cluster block, and a long 2-D
+    # level: one block from global memory
+    (cases.bump_3d, dict(Nx=1025, Ny=9, Nz=9)),
+    (cases.flat_2d, dict(Nx=4097, Nz=9, L=64.0)),
 ]
-IDS = ["flat2d", "slope2d", "bump3d-17x9", "bump3d-33x17", "flat3d-65x33"]
+IDS = ["flat2d", "slope2d", "bump3d-17x9", "bump3d-33x17", "flat3d-65x33", "bump3d-129x33-cluster",
+       "bump3d-1025x9-global", "flat2d-4097-global"]
 
 
 def make(ow3d, oracle, case, **kw):
