@@ -508,15 +508,15 @@ int ow3d_step_batch(ow3d_handle* const* hs, int n, const int* nsteps, int* statu
 int ow3d_get_stats(const ow3d_handle* h, ow3d_stats* s);
 int ow3d_reset_stats(ow3d_handle* h);
 
-/* 1 (the default): with FGMRES and the multigrid preconditioner, from the
- * second RK4 step on every step is one CUDA graph launch (one graph per
+/* 1 (the default): with the multigrid preconditioner (FGMRES or left GMRES),
+ * from the second RK4 step on every step is one CUDA graph launch (one graph per
  * parity of the step number, captured on first use): each of its four
  * solves is the initial residual, one conditional node per Arnoldi step --
  * enabled on the device by the previous step's stopping test -- and the
  * solution update, so the host waits once per step. Before that (and in
  * ow3d_solve), from the handle's second solve on, each Arnoldi step is one
- * graph launch. 0: kernels are launched one by one. The left-preconditioned
- * variant and decks with a pressure-damping zone always launch directly;
+ * graph launch. 0: kernels are launched one by one. Decks with a
+ * pressure-damping zone always launch directly;
  * ow3d_set_relax_target drops the step graphs (they hold the target table).
  * Results are bitwise the same either way. */
 int ow3d_set_graphs(ow3d_handle* h, int on);

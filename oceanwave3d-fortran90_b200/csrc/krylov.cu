@@ -2,11 +2,11 @@
 //
 // The reference drives SPARSKIT2's gmres through reverse communication
 // (src/wrappers/iterative_solution.f90:50-134); here the Arnoldi process,
-// the Givens rotations and the least-squares update stay on the device:
-//   multidot      h_i = s_i <V_i, w>, i < k, and |w|^2      (one pass over V, w)
-//   project       w -= sum_i h_i s_i V_i, and |w|^2         (one pass over V, w)
-//   arnoldi_finish: Hessenberg column, Givens rotation, residual estimate,
-//                   re-orthogonalisation decision and stopping test (1 thread)
+// the Givens rotations and the least-squares update stay on the device, for
+// right (flexible) and left preconditioning alike: each Arnoldi step is one
+// reduction pass and one update pass of delayed classical Gram-Schmidt
+// (DCGS2, below), whose last block forms the Hessenberg column, the Givens
+// rotation, the residual estimate and the stopping test.
 // Reductions are deterministic: every block writes a partial sum, the last
 // block to finish (atomic ticket) adds the partials in block order.
 // Basis vectors are stored unnormalised with a scale factor s_i = 1/|V_i|,
@@ -80,167 +80,6 @@ __device__ bool last_block_reduce(double* partial, int nv, int nblocks, unsigned
     return true;
 }
 
-// One thread: finish Arnoldi step k (1-based after increment).
-__device__ void arnoldi_finish_dev(KrylovState* ks, int maxmv, int m) {
-    if (ks->done) return;
-    const int k = ks->k + 1;           // this step's column index is ks->k (0-based)
-    double* hc = ks->H[ks->k];
-    const double nrm = sqrt(ks->w1);
-    hc[k] = nrm;
-    ks->scale[k] = nrm > 0 ? 1.0 / nrm : 0.0;
-    for (int i = 0; i < k - 1; ++i) {
-        const double a0 = hc[i];
-        hc[i] = ks->cs[i] * a0 + ks->sn[i] * hc[i + 1];
-        hc[i + 1] = ks->cs[i] * hc[i + 1] - ks->sn[i] * a0;
-    }
-    double x = hc[k - 1], yv = hc[k];
-    const double r = sqrt(x * x + yv * yv);
-    double c = 1.0, s = 0.0;
-    if (r != 0.0) { c = x / r; s = yv / r; }
-    hc[k - 1] = r; hc[k] = 0.0;
-    ks->cs[k - 1] = c; ks->sn[k - 1] = s;
-    const double al = -s * ks->g[k - 1];
-    ks->g[k - 1] = c * ks->g[k - 1];
-    ks->g[k] = al;
-    ks->resid = fabs(al);
-    ks->k = k;
-    ks->iters += 1;
-    ks->reorth = 0;
-    const bool conv = ks->resid <= ks->tol;
-    if (conv) ks->converged = 1;
-    if (conv || k >= m || ks->iters >= maxmv || nrm == 0.0) ks->done = 1;
-}
-
-__global__ void k_arnoldi_finish(KrylovState* ks, int maxmv, int m) {
-    pdl_entry();
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    arnoldi_finish_dev(ks, maxmv, m);
-}
-
-// Basis vectors are contiguous: V_i = V + i * ldv, ldv even and the padding
-// past n zero, so element pairs (16-byte loads) can run to n rounded up.
-// Grid (nbx, k+1): block (bx, v) forms a partial of <V_v, w> (v < k) or of
-// |w|^2 (v == k) over a slice of the elements; w is re-read per v from L2.
-// cond: 0 always run; 1 run only when ks->reorth is set (second CGS pass).
-__global__ void __launch_bounds__(kThreads) k_multidot(const double* __restrict__ V, int64_t ldv, int k,
-                                                       const double* __restrict__ w, int64_t n, double* partial,
-                                                       unsigned int* counter, int nbx, KrylovState* ks, int cond) {
-    pdl_entry();
-    if (cond && !ks->reorth) return;
-    if (ks->done) return;
-    const int v = blockIdx.y;
-    const int64_t n2 = (n + 1) / 2;
-    const double2* w2 = reinterpret_cast<const double2*>(w);
-    const double2* a2 = reinterpret_cast<const double2*>(v < k ? V + (int64_t)v * ldv : w);
-    const int64_t stride = (int64_t)nbx * blockDim.x;
-    double acc0 = 0, acc1 = 0, acc2 = 0, acc3 = 0;
-    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    for (; t + 3 * stride < n2; t += 4 * stride) {
-        const double2 x0 = a2[t], x1 = a2[t + stride], x2 = a2[t + 2 * stride], x3 = a2[t + 3 * stride];
-        const double2 y0 = w2[t], y1 = w2[t + stride], y2 = w2[t + 2 * stride], y3 = w2[t + 3 * stride];
-        acc0 += x0.x * y0.x + x0.y * y0.y;
-        acc1 += x1.x * y1.x + x1.y * y1.y;
-        acc2 += x2.x * y2.x + x2.y * y2.y;
-        acc3 += x3.x * y3.x + x3.y * y3.y;
-    }
-    for (; t < n2; t += stride) { const double2 x0 = a2[t], y0 = w2[t]; acc0 += x0.x * y0.x + x0.y * y0.y; }
-    double acc[1] = {(acc0 + acc1) + (acc2 + acc3)};
-    // block partial -> partial[v * nbx + bx]
-    __shared__ double red[kThreads / 32];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    double sm = warp_sum(acc[0]);
-    if (lane == 0) red[wid] = sm;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double tt = 0;
-        for (int q = 0; q < (int)(blockDim.x / 32); ++q) tt += red[q];
-        partial[(int64_t)v * nbx + blockIdx.x] = tt;
-    }
-    // last block over the whole grid reduces every vector's partials
-    __shared__ bool amlast;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const unsigned int total = gridDim.x * gridDim.y;
-        amlast = (atomicAdd(counter, 1u) == total - 1);
-    }
-    __syncthreads();
-    if (!amlast) return;
-    __threadfence();
-    __shared__ double res[kMaxDots];
-    const int nv = k + 1, nw = blockDim.x >> 5;
-    for (int u = wid; u < nv; u += nw) {
-        const double* pv = partial + (int64_t)u * nbx;
-        double s = 0;
-        int b = lane;
-        for (; b + 7 * 32 < nbx; b += 8 * 32) {
-            double q[8];
-#pragma unroll
-            for (int e = 0; e < 8; ++e) q[e] = __ldcg(pv + b + e * 32);
-#pragma unroll
-            for (int e = 0; e < 8; ++e) s += q[e];
-        }
-        for (; b < nbx; b += 32) s += __ldcg(pv + b);
-        s = warp_sum(s);
-        if (lane == 0) res[u] = s;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        *counter = 0u;
-        for (int u = 0; u < k; ++u) ks->dots[u] = ks->scale[u] * res[u];
-        if (cond) {
-            for (int u = 0; u < k; ++u) ks->H[ks->k][u] += ks->dots[u];
-        } else {
-            for (int u = 0; u < k; ++u) ks->H[ks->k][u] = ks->dots[u];
-            ks->w0 = res[k];
-        }
-    }
-}
-
-// w -= sum_v dots[v] * scale[v] * V_v ; |w|^2 -> ks->w1, and decide re-orthogonalisation.
-// The last block also finishes the Arnoldi step (Hessenberg column, Givens
-// rotation, stopping test) once no second Gram-Schmidt pass follows.
-__global__ void __launch_bounds__(kThreads) k_project(const double* __restrict__ V, int64_t ldv, int k,
-                                                      double* __restrict__ w, int64_t n,
-                                                      double* partial, unsigned int* counter, int nblocks,
-                                                      KrylovState* ks, int cond, int maxmv, int m) {
-    pdl_entry();
-    if (cond && !ks->reorth) return;
-    if (ks->done) return;
-    __shared__ double coef[kMaxDots];
-    for (int v = threadIdx.x; v < k; v += blockDim.x) coef[v] = ks->dots[v] * ks->scale[v];
-    __syncthreads();
-    double acc[1] = {0.0};
-    const int64_t n2 = (n + 1) / 2;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    double2* w2 = reinterpret_cast<double2*>(w);
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n2; t += stride) {
-        double2 a = w2[t];
-        for (int v0 = 0; v0 < k; v0 += 8) {
-            double2 vv[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u)
-                if (v0 + u < k) vv[u] = __ldcs(reinterpret_cast<const double2*>(V + (int64_t)(v0 + u) * ldv) + t);
-#pragma unroll
-            for (int u = 0; u < 8; ++u)
-                if (v0 + u < k) { a.x -= coef[v0 + u] * vv[u].x; a.y -= coef[v0 + u] * vv[u].y; }
-        }
-        w2[t] = a;
-        acc[0] += a.x * a.x + a.y * a.y;
-    }
-    block_store_partials(acc, 1, partial, nblocks);
-    __shared__ double res[1];
-    if (last_block_reduce(partial, 1, nblocks, counter, res)) {
-        if (threadIdx.x == 0) {
-            ks->w1 = res[0];
-            // Daniel-Gragg-Kaufman-Stewart test: re-orthogonalise once when the
-            // projection removed more than half of |w|^2.
-            ks->reorth = (!cond && res[0] < 0.5 * ks->w0) ? 1 : 0;
-            if (!ks->reorth) arnoldi_finish_dev(ks, maxmv, m);
-        }
-    }
-}
-
 // Initial residual norm: beta = |v|, tolerance rtol*beta + atol.
 // hnext (nonzero only inside a captured step graph): the condition of the
 // graph node that runs the next Arnoldi step, set to "not done".
@@ -273,7 +112,10 @@ __global__ void __launch_bounds__(kThreads) k_norm_init(const double* __restrict
 
 // Upper-triangular solve R y = g for the current k (1 thread); R is the
 // in-place rotated H (left GMRES) or the separate rotated copy (FGMRES).
-__global__ void k_backsolve(KrylovState* ks, int rotated_R) {
+// With in_basis set (left preconditioning), the coefficients of the vectors
+// the Arnoldi steps multiplied are taken to the final basis, y <- T y, so
+// that the update is x += sum_i y_i v_i.
+__global__ void k_backsolve(KrylovState* ks, int rotated_R, int in_basis) {
     pdl_entry();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     auto Rv = [&](int col, int row) -> double { return rotated_R ? ks->R[col][row] : ks->H[col][row]; };
@@ -283,6 +125,15 @@ __global__ void k_backsolve(KrylovState* ks, int rotated_R) {
         double t = ks->g[i];
         for (int j = i + 1; j < kk; ++j) t -= Rv(j, i) * ks->y[j];
         ks->y[i] = t / Rv(i, i);
+    }
+    if (in_basis) {
+        // T is upper triangular in (i, j): entry i of T y reads y[j >= i]
+        // only, so it can replace y[i] in increasing i
+        for (int i = 0; i < kk; ++i) {
+            double c = 0.0;
+            for (int j = i; j < kk; ++j) c += ks->T[j][i] * ks->y[j];
+            ks->y[i] = c;
+        }
     }
     for (int i = kk; i <= kMaxKrylov; ++i) ks->y[i] = 0.0;
     ks->k = kk;
@@ -314,7 +165,7 @@ __global__ void k_krylov_reset(KrylovState* ks) {
 }
 
 // ---------------------------------------------------------------- DCGS2
-// Flexible GMRES orthogonalisation by delayed classical Gram-Schmidt with
+// Arnoldi orthogonalisation by delayed classical Gram-Schmidt with
 // reorthogonalisation (Swirydowicz, Langou, Ananthan, Yang, Thomas, "Low
 // synchronization Gram-Schmidt and generalized minimal residual algorithms",
 // NLAA 2021): the second Gram-Schmidt pass of V_j rides on step j's single
@@ -343,20 +194,29 @@ __device__ double dcgs_rotate(KrylovState* ks, int col) {
 }
 
 // One thread, after step j's reduction: res[2i] = <V_i, V_j>, res[2i+1] = <V_i, W>, i <= j.
+// The vector step j multiplied, scale_j V_j with V_j after one pass and
+// scale_j its provisional scale, is scale_j (nu q_j + sum sigma_i q_i) in
+// the final basis: column j of T (used by left preconditioning, whose
+// solution is a combination of those vectors).
 __device__ void dcgs_column(KrylovState* ks, int j, const double* res) {
     double ss = 0.0, corr = 0.0;
     if (j >= 1) {
+        const double sp = ks->scale[j];
         for (int i = 0; i < j; ++i) {
             const double sig = ks->scale[i] * res[2 * i];
             ks->coefA[i] = sig;          // sigma_i, scaled below
+            ks->T[j][i] = sp * sig;
             ss += sig * sig;
         }
         const double nu = sqrt(fmax(res[2 * j] - ss, 0.0));
+        ks->T[j][j] = sp * nu;
         // complete column j-1: W_{j-1} = sum (h + sigma) q_i + nu q_j
         for (int i = 0; i < j; ++i) ks->H[j - 1][i] += ks->coefA[i];
         ks->H[j - 1][j] = nu;
         ks->scale[j] = nu > 0 ? 1.0 / nu : 0.0;
         ks->resid = dcgs_rotate(ks, j - 1);
+    } else {
+        ks->T[0][0] = 1.0;   // scale_0 V_0 is final: v_0
     }
     for (int i = 0; i < j; ++i) {
         const double hq = ks->scale[i] * res[2 * i + 1];
@@ -553,34 +413,14 @@ void launch_solve_log(const KrylovState* ks, SolveLog* out, cudaStream_t st) {
     launch_k(k_solve_log, dim3(1), dim3(32), 0, st, ks, out);
 }
 
-void launch_multidot(const double* V, int64_t ldv, int k, const double* w, int64_t n, const DotScratch& sc,
-                     KrylovState* ks, int cond, cudaStream_t st) {
-    // about 8 blocks per SM in total, split over the k+1 products
-    int nbx = (148 * 8 + k) / (k + 1);
-    const int64_t need = ((n + 1) / 2 + kThreads - 1) / kThreads;
-    if (nbx > need) nbx = (int)need;
-    if (nbx < 1) nbx = 1;
-    if (nbx > sc.nblocks) nbx = sc.nblocks;
-    launch_k(k_multidot, dim3(dim3(nbx, k + 1)), dim3(kThreads), 0, st, V, ldv, k, w, n, sc.partial, sc.counter, nbx, ks, cond);
-}
-
-void launch_project(const double* V, int64_t ldv, int k, double* w, int64_t n, const DotScratch& sc, KrylovState* ks,
-                    int cond, int maxmv, int m, cudaStream_t st) {
-    launch_k(k_project, dim3(sc.nblocks), dim3(kThreads), 0, st, V, ldv, k, w, n, sc.partial, sc.counter, sc.nblocks, ks, cond, maxmv, m);
-}
-
-void launch_arnoldi_finish(KrylovState* ks, int maxmv, int m, cudaStream_t st) {
-    launch_k(k_arnoldi_finish, dim3(1), dim3(32), 0, st, ks, maxmv, m);
-}
-
 void launch_norm_init(const double* v, int64_t n, const DotScratch& sc, KrylovState* ks, double rtol, double atol,
                       cudaStream_t st, cudaGraphConditionalHandle hnext) {
     launch_k(k_norm_init, dim3(sc.nblocks), dim3(kThreads), 0, st, v, n, sc.partial, sc.counter, sc.nblocks, ks, rtol, atol,
                                                                 hnext);
 }
 
-void launch_backsolve(KrylovState* ks, cudaStream_t st, int rotated_R) {
-    launch_k(k_backsolve, dim3(1), dim3(32), 0, st, ks, rotated_R);
+void launch_backsolve(KrylovState* ks, cudaStream_t st, int rotated_R, int in_basis) {
+    launch_k(k_backsolve, dim3(1), dim3(32), 0, st, ks, rotated_R, in_basis);
 }
 
 template <typename TZ>

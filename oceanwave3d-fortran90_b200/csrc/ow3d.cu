@@ -472,15 +472,20 @@ int sync_ks_small(ow3d_handle* H) {
     return OW3D_OK;
 }
 
-// The kernels of FGMRES Arnoldi step j with the multigrid preconditioner:
-// z_j = M^{-1} v_j, w = A z_j into V_{j+1}, DCGS2 reduction and update.
-void fgmres_step_launches(ow3d_handle* H, const Surface& s, int j, int maxmv, int m,
-                          cudaGraphConditionalHandle hnext = 0) {
+// The kernels of Arnoldi step j with the multigrid preconditioner, then the
+// DCGS2 reduction and update of the new vector V_{j+1}:
+//   FGMRES (right):  z_j = M^{-1} v_j, V_{j+1} = A z_j;
+//   left GMRES:      w = A v_j, V_{j+1} = M^{-1} w.
+void arnoldi_step_launches(ow3d_handle* H, const Surface& s, int j, int maxmv, int m,
+                           cudaGraphConditionalHandle hnext = 0) {
     const int64_t N = H->G.N;
     double* Vj = H->V + (int64_t)j * H->ldv;
     double* Vn = H->V + (int64_t)(j + 1) * H->ldv;
     const double* sj = &H->ks->scale[j];
-    if (!H->mixed) {
+    if (H->p.krylov == OW3D_KRYLOV_LGMRES) {
+        launch_ho_matvec<double>(H->hg, s, Vj, sj, nullptr, H->w, 0, H->st);
+        precond_into(H, H->w, nullptr, Vn);
+    } else if (!H->mixed) {
         double* Zj = (double*)H->Z + (int64_t)j * H->ldv;
         run_precond<double>(H, H->mg64, Vj, sj, Zj);
         launch_ho_matvec<double>(H->hg, s, Zj, nullptr, nullptr, Vn, 0, H->st);
@@ -493,12 +498,37 @@ void fgmres_step_launches(ow3d_handle* H, const Surface& s, int j, int maxmv, in
     launch_dcgs_update(H->V, H->ldv, j, Vn, N, H->dsc, H->ks, maxmv, m, H->st, hnext);
 }
 
-// Step j as a CUDA graph: captured on its first use (the handle has finished
+// The initial residual of a solve into V_0 (FGMRES: b - A phi; left GMRES:
+// M^{-1}(b - A phi)).
+void initial_residual_launches(ow3d_handle* H, const Surface& s, const double* rhs, const double* phi) {
+    if (H->p.krylov == OW3D_KRYLOV_LGMRES) {
+        launch_ho_matvec<double>(H->hg, s, phi, nullptr, rhs, H->w, 1, H->st);
+        precond_into(H, H->w, nullptr, H->V);
+    } else {
+        launch_ho_matvec<double>(H->hg, s, phi, nullptr, rhs, H->V, 1, H->st);
+    }
+}
+
+// phi += the solve's combination: of Z (FGMRES) or of the final basis V (left
+// GMRES, after the back-substitution took the coefficients there).
+void solution_update_launches(ow3d_handle* H, double* phi) {
+    const int64_t N = H->G.N;
+    if (H->p.krylov == OW3D_KRYLOV_LGMRES) {
+        launch_backsolve(H->ks, H->st, 1, 1);
+        launch_solution_update<double>(phi, H->V, H->ldv, N, H->ks, 1, H->st);
+    } else {
+        launch_backsolve(H->ks, H->st, 1, 0);
+        if (!H->mixed) launch_solution_update<double>(phi, (const double*)H->Z, H->ldv, N, H->ks, 0, H->st);
+        else launch_solution_update<float>(phi, (const float*)H->Z, H->ldv, N, H->ks, 0, H->st);
+    }
+}
+
+// Arnoldi step j as a CUDA graph: captured on its first use (the handle has finished
 // a solve by then, so every one-time set-up of the launches is done),
 // replayed afterwards. The launch sequence depends on j and on the surface
 // arrays only; everything else it touches is fixed for the handle's
 // lifetime. A capture that fails switches the handle to direct launches.
-int fgmres_step_graph(ow3d_handle* H, const Surface& s, int j, int maxmv, int m) {
+int arnoldi_step_graph(ow3d_handle* H, const Surface& s, int j, int maxmv, int m) {
     const double* key[5] = {s.E, s.Ex, s.Exx, s.Ey, s.Eyy};
     ow3d_handle::IterGraph* g = nullptr;
     for (auto& q : H->iter_graphs)
@@ -510,7 +540,7 @@ int fgmres_step_graph(ow3d_handle* H, const Surface& s, int j, int maxmv, int m)
         cudaError_t e = cudaStreamBeginCapture(H->st, cudaStreamCaptureModeThreadLocal);
         unsigned long long nk = 0;
         if (e == cudaSuccess) {
-            fgmres_step_launches(H, s, j, maxmv, m);
+            arnoldi_step_launches(H, s, j, maxmv, m);
             e = cudaStreamEndCapture(H->st, &graph);
             if (e == cudaSuccess && g_capture_unsafe) e = cudaErrorStreamCaptureUnsupported;
         }
@@ -523,7 +553,7 @@ int fgmres_step_graph(ow3d_handle* H, const Surface& s, int j, int maxmv, int m)
         if (e != cudaSuccess) {
             cudaGetLastError();
             H->graphs_failed = true;
-            fgmres_step_launches(H, s, j, maxmv, m);
+            arnoldi_step_launches(H, s, j, maxmv, m);
             CK(cudaGetLastError());
             return OW3D_OK;
         }
@@ -556,71 +586,35 @@ void record_solve(ow3d_handle* H, int it, double resid, double r0, double tol, b
 int solve_device(ow3d_handle* H, const double* rhs, double* phi, const Surface& s, int* iters_out) {
     const int64_t N = H->G.N;
     const int m = H->m, maxmv = H->p.GMRESmaxiterations;
-    const bool left = (H->p.krylov == OW3D_KRYLOV_LGMRES);
     launch_krylov_reset(H->ks, H->st);
     int status = OW3D_OK;
     double r0 = 0, tol = 0;
     for (int cycle = 0; cycle < 1000; ++cycle) {
-        // initial residual
-        if (!left) {
-            launch_ho_matvec<double>(H->hg, s, phi, nullptr, rhs, H->V, 1, H->st);
-        } else {
-            launch_ho_matvec<double>(H->hg, s, phi, nullptr, rhs, H->w, 1, H->st);
-            precond_into(H, H->w, nullptr, H->V);
-        }
+        initial_residual_launches(H, s, rhs, phi);
         launch_norm_init(H->V, N, H->dsc, H->ks, H->p.reltol, H->p.abstol, H->st);
         TRY(sync_ks_small(H));
         if (cycle == 0) { r0 = H->ks_host->beta; tol = H->ks_host->tol; }
         int j = 0;
         while (!H->ks_host->done) {
-            if (!left && H->nlev > 0 && H->graphs && !H->graphs_failed && H->stats.solves > 0) {
-                // FGMRES step j as one graph launch
-                TRY(fgmres_step_graph(H, s, j, maxmv, m));
-                TRY(sync_ks_small(H));
-                ++j;
-                continue;
-            }
-            double* Vj = H->V + (int64_t)j * H->ldv;
-            double* Vn = H->V + (int64_t)(j + 1) * H->ldv;
-            const double* sj = &H->ks->scale[j];
-            if (!left) {
-                if (H->nlev == 0) {
-                    launch_scale_copy_dev<double>(Vj, sj, (double*)H->Z + (int64_t)j * H->ldv, N, H->st);
-                    launch_ho_matvec<double>(H->hg, s, (double*)H->Z + (int64_t)j * H->ldv, nullptr, nullptr, Vn, 0, H->st);
-                } else if (!H->mixed) {
-                    double* Zj = (double*)H->Z + (int64_t)j * H->ldv;
-                    run_precond<double>(H, H->mg64, Vj, sj, Zj);
-                    launch_ho_matvec<double>(H->hg, s, Zj, nullptr, nullptr, Vn, 0, H->st);
-                } else {
-                    float* Zj = (float*)H->Z + (int64_t)j * H->ldv;
-                    run_precond<float>(H, H->mg32, Vj, sj, Zj);
-                    launch_ho_matvec<float>(H->hg, s, Zj, nullptr, nullptr, Vn, 0, H->st);
-                }
-            } else {
-                launch_ho_matvec<double>(H->hg, s, Vj, sj, nullptr, H->w, 0, H->st);
-                precond_into(H, H->w, nullptr, Vn);
-            }
-            if (!left) {
+            if (H->nlev > 0 && H->graphs && !H->graphs_failed && H->stats.solves > 0) {
+                // Arnoldi step j as one graph launch
+                TRY(arnoldi_step_graph(H, s, j, maxmv, m));
+            } else if (H->nlev == 0 && H->p.krylov != OW3D_KRYLOV_LGMRES) {
+                // FGMRES without a preconditioner: z_j = v_j
+                double* Vj = H->V + (int64_t)j * H->ldv;
+                double* Vn = H->V + (int64_t)(j + 1) * H->ldv;
+                double* Zj = (double*)H->Z + (int64_t)j * H->ldv;
+                launch_scale_copy_dev<double>(Vj, &H->ks->scale[j], Zj, N, H->st);
+                launch_ho_matvec<double>(H->hg, s, Zj, nullptr, nullptr, Vn, 0, H->st);
                 launch_dcgs_reduce(H->V, H->ldv, j, Vn, N, H->dsc, H->ks, H->st);
                 launch_dcgs_update(H->V, H->ldv, j, Vn, N, H->dsc, H->ks, maxmv, m, H->st);
             } else {
-                launch_multidot(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 0, H->st);
-                launch_project(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 0, maxmv, m, H->st);
-                launch_multidot(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 1, H->st);
-                launch_project(H->V, H->ldv, j + 1, Vn, N, H->dsc, H->ks, 1, maxmv, m, H->st);
+                arnoldi_step_launches(H, s, j, maxmv, m);
             }
             TRY(sync_ks_small(H));
             ++j;
         }
-        if (H->ks_host->k > 0) {
-            launch_backsolve(H->ks, H->st, left ? 0 : 1);
-            if (!left) {
-                if (!H->mixed) launch_solution_update<double>(phi, (const double*)H->Z, H->ldv, N, H->ks, 0, H->st);
-                else launch_solution_update<float>(phi, (const float*)H->Z, H->ldv, N, H->ks, 0, H->st);
-            } else {
-                launch_solution_update<double>(phi, H->V, H->ldv, N, H->ks, 1, H->st);
-            }
-        }
+        if (H->ks_host->k > 0) solution_update_launches(H, phi);
         TRY(sync_ks_small(H));
         if (H->ks_host->converged) break;
         if (H->ks_host->iters >= maxmv) { status = OW3D_NOT_CONVERGED; break; }
@@ -997,7 +991,7 @@ int enqueue_solve_graph(ow3d_handle* H, const Surface& s, int slot, unsigned lon
     cudaStream_t st = H->st;
     const int m = H->m, maxmv = H->p.GMRESmaxiterations;
     launch_krylov_reset(H->ks, st);
-    launch_ho_matvec<double>(H->hg, s, H->PHI, nullptr, H->RHS, H->V, 1, st);
+    initial_residual_launches(H, s, H->RHS, H->PHI);
     cudaStreamCaptureStatus cs;
     cudaGraph_t g = nullptr;
     const cudaGraphNode_t* deps = nullptr;
@@ -1023,27 +1017,25 @@ int enqueue_solve_graph(ow3d_handle* H, const Surface& s, int slot, unsigned lon
         CK(cudaStreamBeginCaptureToGraph(H->st2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
         const unsigned long long k0 = g_kernel_launches.load(std::memory_order_relaxed);
         H->st = H->st2;   // the step's launches go to the body's capture
-        fgmres_step_launches(H, s, j, maxmv, m, j + 1 < m ? hc[(size_t)j + 1] : 0);
+        arnoldi_step_launches(H, s, j, maxmv, m, j + 1 < m ? hc[(size_t)j + 1] : 0);
         H->st = st;
         kin += g_kernel_launches.load(std::memory_order_relaxed) - k0;
         ++bodies;
         cudaGraph_t bout = nullptr;
         CK(cudaStreamEndCapture(H->st2, &bout));
     }
-    launch_backsolve(H->ks, st, 1);
-    if (!H->mixed) launch_solution_update<double>(H->PHI, (const double*)H->Z, H->ldv, H->G.N, H->ks, 0, st);
-    else launch_solution_update<float>(H->PHI, (const float*)H->Z, H->ldv, H->G.N, H->ks, 0, st);
+    solution_update_launches(H, H->PHI);
     launch_solve_log(H->ks, H->slog + slot, st);
     return OW3D_OK;
 }
 
-// Whether the next step may run as a captured graph: FGMRES with the
-// multigrid preconditioner, no pressure damping (its terms are gated on the
-// host time), graphs on, and the first step done directly (it performs the
-// one-time set-ups of the launches and uploads the level tables).
+// Whether the next step may run as a captured graph: GMRES (either side)
+// with the multigrid preconditioner, no pressure damping (its terms are
+// gated on the host time), graphs on, and the first step done directly (it
+// performs the one-time set-ups of the launches and uploads the level
+// tables).
 bool step_graph_eligible(const ow3d_handle* H) {
-    return H->graphs && H->p.krylov == OW3D_KRYLOV_FGMRES && H->nlev > 0 && !H->pd_on && H->tstep >= 1 &&
-           !H->step_graph[(H->tstep + 1) & 1].failed;
+    return H->graphs && H->nlev > 0 && !H->pd_on && H->tstep >= 1 && !H->step_graph[(H->tstep + 1) & 1].failed;
 }
 
 // Capture the graph of steps with the parity of `tstep`.

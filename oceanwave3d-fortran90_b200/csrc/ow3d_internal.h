@@ -208,12 +208,16 @@ struct KrylovState {
     double coefB[kMaxKrylov + 2];               // FGMRES update: W -= coefB_i V_i (i <= j)
     double cs[kMaxKrylov + 1], sn[kMaxKrylov + 1], g[kMaxKrylov + 2];
     double scale[kMaxKrylov + 2];               // v_i = scale[i] * V_i (stored unnormalised)
+    // left preconditioning: T[j][i], i <= j, expresses the vector step j
+    // multiplied (V_j after one Gram-Schmidt pass, times its provisional
+    // scale) in the final basis v_0..v_j
+    double T[kMaxKrylov + 1][kMaxKrylov + 1];
     double y[kMaxKrylov + 1];
-    double dots[kMaxKrylov + 2];                // result of the last multi-dot
-    double w0, w1;                              // |w|^2 before / after projection
+    // the scalars from here on are what the host reads after each Arnoldi step
+    double w0, w1;                              // spare
     double beta, tol, resid;
     int k;                                      // Arnoldi steps done
-    int reorth;                                 // re-orthogonalise this step
+    int reorth;                                 // spare
     int done;                                   // converged / stopped
     int converged;
     int iters;                                  // matvec count
@@ -283,21 +287,15 @@ struct DotScratch {
     unsigned int* counter;
     int nblocks;
 };
-void launch_multidot(const double* V, int64_t ldv, int k, const double* w, int64_t n, const DotScratch& sc,
-                     KrylovState* ks, int cond, cudaStream_t st);
-// FGMRES Arnoldi step j with delayed classical Gram-Schmidt (DCGS2): the one
-// reduction pass and the one update pass; W = A z_j sits in V_{j+1}.
+// Arnoldi step j with delayed classical Gram-Schmidt (DCGS2): the one
+// reduction pass and the one update pass; the new vector W (A z_j, or
+// M^{-1} A v_j with left preconditioning) sits in V_{j+1}.
 void launch_dcgs_reduce(const double* V, int64_t ldv, int j, const double* W, int64_t n, const DotScratch& sc,
                         KrylovState* ks, cudaStream_t st);
 // hnext: inside a captured step graph, the condition of the node that runs
 // Arnoldi step j+1 (set to "not done" by the step's stopping test); 0 otherwise.
 void launch_dcgs_update(double* V, int64_t ldv, int j, double* W, int64_t n, const DotScratch& sc, KrylovState* ks,
                         int maxmv, int m, cudaStream_t st, cudaGraphConditionalHandle hnext = 0);
-// Projection pass; the last block finishes the Arnoldi step (Givens rotation,
-// stopping test) when no re-orthogonalisation pass follows.
-void launch_project(const double* V, int64_t ldv, int k, double* w, int64_t n, const DotScratch& sc, KrylovState* ks,
-                    int cond, int maxmv, int m, cudaStream_t st);
-void launch_arnoldi_finish(KrylovState* ks, int maxmv, int m, cudaStream_t st);
 void launch_norm_init(const double* v, int64_t n, const DotScratch& sc, KrylovState* ks, double rtol, double atol,
                       cudaStream_t st, cudaGraphConditionalHandle hnext = 0);
 // The outcome of one solve, copied from the Krylov state when it ends (the
@@ -307,7 +305,7 @@ struct SolveLog {
     double resid, beta, tol;
 };
 void launch_solve_log(const KrylovState* ks, SolveLog* out, cudaStream_t st);
-void launch_backsolve(KrylovState* ks, cudaStream_t st, int rotated_R = 0);
+void launch_backsolve(KrylovState* ks, cudaStream_t st, int rotated_R = 0, int in_basis = 0);
 template <typename TZ>
 void launch_solution_update(double* x, const TZ* Z, int64_t ldz, int64_t n, const KrylovState* ks, int use_scale,
                             cudaStream_t st);

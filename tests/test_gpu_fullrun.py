@@ -65,6 +65,7 @@ def _check_dev(sim, g, its):
     assert max(errs.values()) < RTOL_RUN, errs
     d = np.abs(its - g["step_iterations"])
     assert np.all(d <= 4), (int(d.max()), int(np.argmax(d)))
+    return errs, int(d.max()), int(its.sum()), int(g["step_iterations"].sum())
 
 
 def _check_ref(sim, g, its, tol, frac):
@@ -134,9 +135,13 @@ def test_shoal_1000_steps_in_reference_order_matches_reference_ordered_oracle(ow
     """Left GMRES with the lexicographic smoother: the reference's own solver,
     held to the device-ordered bar (1e-10, matvecs within one per solve)."""
     sim, its = _shoal(ow3d, krylov=1, lex=True)
-    _check_dev(sim, load("run_shoal_257x33x9_1000_ref"), its)
+    errs, dmax, tot, ref = _check_dev(sim, load("run_shoal_257x33x9_1000_ref"), its)
+    print(f"shoal 1000 steps in the reference order: rel err {errs}, largest per-step matvec "
+          f"difference {dmax}, matvecs {tot} vs {ref}")
 
 
 def test_sfwave_200_steps_in_reference_order_matches_reference_ordered_oracle(ow3d):
     sim, its = _sfwave(ow3d, krylov=1, lex=True)
-    _check_dev(sim, load("run_sfwave_257x9_200_ref"), its)
+    errs, dmax, tot, ref = _check_dev(sim, load("run_sfwave_257x9_200_ref"), its)
+    print(f"stream-function flume 200 steps in the reference order: rel err {errs}, largest per-step "
+          f"matvec difference {dmax}, matvecs {tot} vs {ref}")

@@ -245,14 +245,15 @@ def _step_case(ow3d, name):
     inside the fused coarse kernel) and the stream-function flume
     (relaxation targets at every stage time)."""
     W = ow3d.workloads
-    if name in ("bump3d_fp64", "bump3d_mixed"):
+    if name.startswith("bump3d"):
         p, geo = cases.bump_3d(Nx=129, Ny=33, Nz=17, Lx=8.0, Ly=2.0, dt=0.02)
-        p.precision = 1 if name.endswith("mixed") else 0
+        p.precision = 1 if "mixed" in name else 0
+        p.krylov = 1 if name.endswith("left") else 0
         x = (np.arange(p.Nx + 2) - 1) / (p.Nx - 1) * p.Lx
         E0 = np.tile(0.01 * np.cos(np.pi * x / p.Lx), p.Ny + 2)
         return p, geo, E0, np.zeros_like(E0), None
-    if name == "shoal_filter":
-        p, geo, target = cases.shoal_generation(W, 8, filteringONOFF=2)
+    if name.startswith("shoal_filter"):
+        p, geo, target = cases.shoal_generation(W, 8, filteringONOFF=2, krylov=1 if name.endswith("left") else 0)
         return p, geo, np.zeros((p.Nx + 2) * (p.Ny + 2)), np.zeros((p.Nx + 2) * (p.Ny + 2)), target
     if name == "periodic":
         p, geo, E0, P0, info = W.periodic_wave_2d()
@@ -261,12 +262,14 @@ def _step_case(ow3d, name):
     return p, geo, E0, P0, (lambda box: targets[0])
 
 
-@pytest.mark.parametrize("name", ["bump3d_fp64", "bump3d_mixed", "shoal_filter", "periodic", "sfwave"])
+@pytest.mark.parametrize("name", ["bump3d_fp64", "bump3d_mixed", "shoal_filter", "periodic", "sfwave",
+                                  "bump3d_fp64_left", "bump3d_mixed_left", "shoal_filter_left"])
 def test_step_graphs_match_direct_steps(ow3d, name):
     """Steps replayed as one CUDA graph each (the default from the second
     step on: each solve's Arnoldi steps as conditional nodes that the device
     enables, the time level read on the device) give bitwise the state, the
-    matvec counts and the solver records of direct launches."""
+    matvec counts and the solver records of direct launches, for FGMRES and
+    for left-preconditioned GMRES."""
     L = ow3d.lib()
     out = []
     for graphs in (1, 0):
