@@ -591,7 +591,7 @@ def main():
                                    f"({dt1:.1f} s): the like-for-like figure of the serial Fortran reference"}
     serve = None
     if not args.no_serve and world == 1:
-        serve = serving_sample()
+        serve = serving_sample(slots=(4, None))
     C = (pm.Nx + 2) * (pm.Ny + 2)
     sm = res["mixed"]["stats"]; sf = res["fp64"]["stats"]
     out = {
