@@ -438,16 +438,23 @@ def profile_step(args):
 
 
 def largest_instance(args):
+    """--config largest: one JSON line per tolerance (largest_sweep)."""
+    for line in largest_sweep(args.steps, args.warmup):
+        print(json.dumps(line))
+
+
+def largest_sweep(steps, warmup):
     """The largest single instance, 2049 x 513 x 9 (flat 1 m, seeded JONSWAP
     sea): FP64 and mixed precision at GMRES rtol 1e-6, 1e-8 and 1e-10 with
     abstol 0 (so that the relative term alone sets each threshold), one
-    JSON line per tolerance with both precisions' DOF-timesteps/s, iterations
+    record per tolerance with both precisions' DOF-timesteps/s, iterations
     per solve and the mixed path's eta error against FP64. Timed like the
     main line (device events around the steps, after warm-up steps)."""
     import torch
     pkg = package()
     W = pkg.workloads
     torch.cuda.set_device(0)
+    out = []
     for rtol in (1e-6, 1e-8, 1e-10):
         res, states = {}, {}
         for prec in ("fp64", "mixed"):
@@ -455,22 +462,23 @@ def largest_instance(args):
                                              reltol=rtol, abstol=0.0, seed=1234)
             sim = pkg.Simulation(p, **geo)
             sim.set_state(E0, P0)
-            sim.step(args.warmup)
+            sim.step(warmup)
             sim.reset_stats()
             torch.cuda.synchronize()
-            st, ms = sim.step_timed(args.steps)
+            st, ms = sim.step_timed(steps)
             s = sim.stats()
             E, P, Wv, phi, t = sim.get_state()
             states[prec] = E
-            res[prec] = dict(value=dof(p) * args.steps / (ms / 1e3), ms_per_step=ms / args.steps,
+            res[prec] = dict(value=dof(p) * steps / (ms / 1e3), ms_per_step=ms / steps,
                              iterations_per_solve=s["total_iterations"] / max(s["solves"], 1),
                              **solver_report(s, p))
             sim.close()
         err = float(np.max(np.abs(states["mixed"] - states["fp64"])) / np.max(np.abs(states["fp64"])))
-        print(json.dumps({"config": "largest instance 2049x513x9, flat 1 m, JONSWAP, GMRES(23) abstol 0", "rtol": rtol,
-                          "unit": UNIT, "steps": args.steps, "warmup": args.warmup, "fp64": res["fp64"],
-                          "mixed": res["mixed"], "speedup_mixed_vs_fp64": res["mixed"]["value"] / res["fp64"]["value"],
-                          "eta_rel_err_mixed_vs_fp64": err}))
+        out.append({"config": "largest instance 2049x513x9, flat 1 m, JONSWAP, GMRES(23) abstol 0", "rtol": rtol,
+                    "unit": UNIT, "steps": steps, "warmup": warmup, "fp64": res["fp64"],
+                    "mixed": res["mixed"], "speedup_mixed_vs_fp64": res["mixed"]["value"] / res["fp64"]["value"],
+                    "eta_rel_err_mixed_vs_fp64": err})
+    return out
 
 
 def main():
@@ -481,6 +489,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop sample")
+    ap.add_argument("--no-largest", action="store_true",
+                    help="skip the largest-instance sweep (2049x513x9 at three tolerances, 3 timed steps each)")
     ap.add_argument("--profile", choices=["fp64", "mixed"], default=None,
                     help="profiling driver: one warm-up step then one step of the workload, no JSON line")
     ap.add_argument("--grid", default=None, help="NXxNYxNZ override for --profile (e.g. 257x65x17)")
@@ -592,6 +602,9 @@ def main():
     serve = None
     if not args.no_serve and world == 1:
         serve = serving_sample(slots=(4, None))
+    largest = None
+    if not args.no_largest and world == 1:
+        largest = largest_sweep(3, 3)
     C = (pm.Nx + 2) * (pm.Ny + 2)
     sm = res["mixed"]["stats"]; sf = res["fp64"]["stats"]
     out = {
@@ -617,6 +630,7 @@ def main():
                 "avg_iterations": res["e2e_stats"]["total_iterations"] / max(res["e2e_stats"]["solves"], 1),
                 "not_converged": res["e2e_stats"]["not_converged"]},
         "roofline": roof, "roofline_operator": roof_op, "roofline_path": path_roof, "cpu_baseline": cpu, "clocks": res["mixed"]["clocks"], "serving": serve,
+        "largest_instance": largest,
         "gpu_launches": res["mixed"]["launches"],
     }
     print(json.dumps(out))
