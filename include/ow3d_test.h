@@ -72,7 +72,7 @@ int ow3d_test_set_tail_cluster(int blocks);
 int ow3d_test_set_colour_tiles(int min_tiles);
 
 /* Per-level colour pass launch form: 0 one pass over the columns with up to
- * 32 blocks per SM; 1 the grid capped at the 4 resident blocks per SM, each
+ * 32 blocks per SM; 1 the grid capped at the resident blocks per SM, each
  * warp prefetching its next group of columns into L1; 2 the capped grid
  * alone; -1 (the default) 2 on FP64 levels and 0 on FP32 ones. Results are
  * bitwise the same. Returns the previous value. Process-wide. */

@@ -69,8 +69,15 @@ __global__ void k_lo_bottom(LevelDev<T> L) {
 // With prefetch set, each warp asks for the next group's column data (its
 // rows of x in the column and the four neighbour columns, and of b) to be
 // brought into L1 before it solves the current group.
+// Resident blocks per SM: 5 without mixed-derivative terms (at most 96
+// registers, a few spilled: measured on a B200 at 1025x257x17 FP64, the
+// finest pass 51.8 against 57.6 us and the step 78.8 against 79.6 ms; 6
+// blocks spill more and are slower), 4 with them (their larger rows would
+// spill far more under the same cap).
+constexpr int colour_blocks_per_sm(bool cross) { return cross ? 4 : 5; }
+
 template <typename T, bool THREE, int S, bool CROSS>
-__global__ void __launch_bounds__(128, 4) k_lo_colour(LevelDev<T> L, int colour, int prefetch) {
+__global__ void __launch_bounds__(128, colour_blocks_per_sm(CROSS)) k_lo_colour(LevelDev<T> L, int colour, int prefetch) {
     pdl_entry();
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -469,14 +476,14 @@ static void colour_launch(const LevelDev<T>& L, int c, cudaStream_t st) {
     const int64_t warps = (cols + (32 / S) - 1) / (32 / S);
     int64_t blocks = (warps * 32 + 127) / 128;
     // g_colour_prefetch: 0 = one pass over the columns with up to 32 blocks
-    // per SM; 1 = the grid capped at the resident 4 blocks per SM, each warp
+    // per SM; 1 = the grid capped at the resident blocks per SM, each warp
     // prefetching its next group into L1; 2 = the capped grid alone; -1 (the
     // default) = 2 for FP64 levels, 0 for FP32 ones, the faster of each
     // measured on a B200 (1025x257x17: FP64 step 80.7 against 82.4 ms, mixed
     // 65.7 against 68.1 ms)
     int pf = g_colour_prefetch.load(std::memory_order_relaxed);
     if (pf < 0) pf = sizeof(T) == 8 ? 2 : 0;
-    const int64_t cap = pf ? 148 * 4 : 148 * 32;
+    const int64_t cap = pf ? 148 * colour_blocks_per_sm(L.cross != 0) : 148 * 32;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
     const int pre = pf == 1 ? 1 : 0;
