@@ -69,15 +69,17 @@ __global__ void k_lo_bottom(LevelDev<T> L) {
 // With prefetch set, each warp asks for the next group's column data (its
 // rows of x in the column and the four neighbour columns, and of b) to be
 // brought into L1 before it solves the current group.
-// Resident blocks per SM: 5 without mixed-derivative terms (at most 96
-// registers, a few spilled: measured on a B200 at 1025x257x17 FP64, the
-// finest pass 51.8 against 57.6 us and the step 78.8 against 79.6 ms; 6
-// blocks spill more and are slower), 4 with them (their larger rows would
-// spill far more under the same cap).
-constexpr int colour_blocks_per_sm(bool cross) { return cross ? 4 : 5; }
+// Resident blocks per SM. Without mixed-derivative terms: FP64 5 (at most
+// 96 registers, a few spilled: measured on a B200 at 1025x257x17, the finest
+// pass 51.8 against 57.6 us and the FP64 step 78.8 against 79.6 ms; 6 blocks
+// spill more and are slower), FP32 7 (72 registers, none spilled: the mixed
+// step 62.9 against 63.4 ms; 8 blocks spill and gain less). With them 4
+// (their larger rows would spill far more under the same caps).
+constexpr int colour_blocks_per_sm(bool cross, bool fp32) { return cross ? 4 : (fp32 ? 7 : 5); }
 
 template <typename T, bool THREE, int S, bool CROSS>
-__global__ void __launch_bounds__(128, colour_blocks_per_sm(CROSS)) k_lo_colour(LevelDev<T> L, int colour, int prefetch) {
+__global__ void __launch_bounds__(128, colour_blocks_per_sm(CROSS, sizeof(T) == 4))
+    k_lo_colour(LevelDev<T> L, int colour, int prefetch) {
     pdl_entry();
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -483,7 +485,7 @@ static void colour_launch(const LevelDev<T>& L, int c, cudaStream_t st) {
     // 65.7 against 68.1 ms)
     int pf = g_colour_prefetch.load(std::memory_order_relaxed);
     if (pf < 0) pf = sizeof(T) == 8 ? 2 : 0;
-    const int64_t cap = pf ? 148 * colour_blocks_per_sm(L.cross != 0) : 148 * 32;
+    const int64_t cap = pf ? 148 * colour_blocks_per_sm(L.cross != 0, sizeof(T) == 4) : 148 * 32;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
     const int pre = pf == 1 ? 1 : 0;
