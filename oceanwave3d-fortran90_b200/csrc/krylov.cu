@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(kThreads) k_solution_update(double* __restrict
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += stride) {
         double a = x[t];
-        for (int v = 0; v < k; ++v) a += coef[v] * (double)Z[(int64_t)v * ldz + t];
+        for (int v = 0; v < k; ++v) a += coef[v] * (double)__ldcs(Z + (int64_t)v * ldz + t);
         x[t] = a;
     }
 }
@@ -264,7 +264,10 @@ __global__ void __launch_bounds__(kThreads) k_dcgs_reduce(const double* __restri
             if (t < n2) { q[e] = q2[t]; w[e] = w2[t]; }
             else { q[e] = make_double2(0.0, 0.0); w[e] = make_double2(0.0, 0.0); }
         }
-        // vectors in groups of kDotG, all their loads in flight together
+        // vectors in groups of kDotG, all their loads in flight together; the
+        // older basis vectors are read once per pass, so they are streamed
+        // (evict-first) rather than let them push the multigrid levels and
+        // their coefficient tables out of L2 before the next V-cycle
         for (int v0 = 0; v0 <= j; v0 += kDotG) {
             double2 x[kDotG][kDotE];
 #pragma unroll
@@ -274,7 +277,7 @@ __global__ void __launch_bounds__(kThreads) k_dcgs_reduce(const double* __restri
 #pragma unroll
                 for (int e = 0; e < kDotE; ++e) {
                     const int64_t t = t0 + (int64_t)e * blockDim.x;
-                    x[g][e] = (v < j && t < n2) ? a2[t] : make_double2(0.0, 0.0);
+                    x[g][e] = (v < j && t < n2) ? __ldcs(a2 + t) : make_double2(0.0, 0.0);
                 }
             }
 #pragma unroll
