@@ -346,7 +346,9 @@ __global__ void __launch_bounds__(kThreads) k_dcgs_update(double* __restrict__ V
     double2* vj2 = reinterpret_cast<double2*>(V + (int64_t)j * ldv);
     double2* w2 = reinterpret_cast<double2*>(W);
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n2; t += stride) {
-        double2 q = vj2[t], a = w2[t];
+        // v_j is next read as an older vector of the following reduction
+        // (streamed), so it is written back evict-first too
+        double2 q = __ldcs(vj2 + t), a = w2[t];
         for (int v0 = 0; v0 < j; v0 += 8) {
             double2 vv[8];
 #pragma unroll
@@ -360,7 +362,7 @@ __global__ void __launch_bounds__(kThreads) k_dcgs_update(double* __restrict__ V
                 }
         }
         a.x -= cBj * q.x; a.y -= cBj * q.y;
-        if (j > 0) vj2[t] = q;
+        if (j > 0) __stcs(vj2 + t, q);
         w2[t] = a;
         acc[0] += a.x * a.x + a.y * a.y;
     }
